@@ -1,0 +1,116 @@
+/* C-ABI of the B200 hot path of the MPCNS_Uns Hall-MHD step.
+ *
+ * One opaque handle (MhdMesh) holds a device copy of one rank's signed cell complex, its
+ * metric and boundary classification, plus the tables derived from them once (least-squares
+ * stencil inverses, cell-field reconstruction coefficients, face -> (L, R) cells).  Every
+ * entry point below replaces one function of the reference and keeps its meaning: same
+ * inputs, same outputs, same layout of the arrays (the reference's AoS order: value(i, comp)
+ * = a[i*ncomp + comp]).  Array arguments are DEVICE pointers unless the name says `host`;
+ * all work is ordered on the handle's CUDA stream (mhd_gpu_mesh_stream) and calls return
+ * when it is enqueued, except calls with host outputs, which synchronise.
+ *
+ * Status: 0 ok, MHD_EINVAL bad argument, MHD_ECUDA CUDA error, MHD_ESTATE non-finite or
+ * invalid state detected, MHD_ENOCONV GMRES stopped at max_it above rtol (the solution and
+ * its relative residual are still returned).  mhd_gpu_last_error() gives the message of the
+ * calling thread's last failure.  No C++ exception crosses this boundary.  A handle is used
+ * by one host thread at a time (the reference's one-rank-one-thread model).
+ */
+#ifndef MHD_GPU_H
+#define MHD_GPU_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MHD_OK 0
+#define MHD_EINVAL (-1)
+#define MHD_ECUDA (-2)
+#define MHD_ESTATE (-3)
+#define MHD_ENOCONV (-4)
+
+typedef struct MhdMesh MhdMesh;
+typedef struct MhdInduction MhdInduction;
+typedef struct MhdState MhdState;
+
+/* Host arrays of one rank's mesh, in the layout of the reference's uns::CellComplex
+ * (include/uns/complex/CellComplex.h:29-53: signed CSR, int64 ptr / int32 idx / int8 sgn),
+ * uns::Geometry (include/uns/geometry/Geometry.h:25-43; Vec3 = 3 doubles) and
+ * mhd::BoundaryInfo (Common/boundary/BoundaryInfo.h:21-29).  Copied at creation. */
+typedef struct MhdMeshDesc {
+    int32_t n_nodes, n_edges, n_faces, n_cells;
+    int32_t n_owned_cells, n_owned_edges; /* reference LocalMesh ent[3].n_owned / ent[1].n_owned */
+    const int64_t *c2f_ptr; const int32_t *c2f_idx; const int8_t *c2f_sgn;
+    const int64_t *f2e_ptr; const int32_t *f2e_idx; const int8_t *f2e_sgn;
+    const int64_t *e2f_ptr; const int32_t *e2f_idx; const int8_t *e2f_sgn;
+    const int64_t *f2c_ptr; const int32_t *f2c_idx; const int8_t *f2c_sgn;
+    const int32_t *cell_material;          /* 0 fluid, 1 solid */
+    const double *edge_vec, *edge_mid, *edge_len;
+    const double *face_area, *face_center, *face_area_mag;
+    const double *cell_center, *cell_volume;
+    const int64_t *ec_ptr; const int32_t *ec_cell; const double *ec_weight;
+    const double *ef_weight;               /* aligned with e2f */
+    const double *star1, *star2;
+    const int8_t *face_kind;               /* 0 Interior 1 Wall 2 Inflow 3 Outflow 4 Skip */
+    const int8_t *edge_mode;               /* 0 free 1 wall (E = 0) 2 inflow */
+} MhdMeshDesc;
+
+/* Primitive state W = (rho, u, v, w, p) of mhd::Prim (Common/physics/Euler.h:7-10). */
+typedef struct MhdPrim { double rho, u, v, w, p; } MhdPrim;
+
+const char *mhd_gpu_last_error(void);
+int mhd_gpu_device_info(char *name, size_t name_len, int *sm_count);
+
+/* Upload a mesh; replaces the reference's per-call use of LocalMesh + Geometry + BoundaryInfo
+ * and the one-time setup of mhd::Stencil::Stencil (Common/fluid/Reconstruction.cpp:26-78). */
+int mhd_gpu_mesh_create(const MhdMeshDesc *desc, MhdMesh **out);
+int mhd_gpu_mesh_destroy(MhdMesh *mesh);
+/* The CUDA stream (cudaStream_t) the handle's work is ordered on; may be replaced by the caller's. */
+void *mhd_gpu_mesh_stream(MhdMesh *mesh);
+int mhd_gpu_mesh_set_stream(MhdMesh *mesh, void *stream);
+int mhd_gpu_synchronize(MhdMesh *mesh);
+
+/* mhd::to_prim over n cells (Common/physics/Euler.h:13-21): U, W 5 per cell. */
+int mhd_gpu_to_prim(MhdMesh *mesh, const double *U, int32_t n, double gamma, double rho_floor, double p_floor, double *W);
+
+/* mhd::Stencil::limited_gradients (Common/fluid/Reconstruction.h:28-29, .cpp:80-142):
+ * W 5 per cell -> grad 15 per cell (3*m + axis), zero outside the valid owned fluid cells.
+ * species 1 is the absorbing wall species of ghost_state (Reconstruction.cpp:9-24). */
+int mhd_gpu_limited_gradients(MhdMesh *mesh, const double *W, int32_t species, const MhdPrim *freestream, int32_t limit,
+                              double rel_limit, double *grad);
+
+/* mhd::fluid_flux_rhs (Common/fluid/FluxRHS.h:10-12, .cpp:30-74): rhs 5 per cell, overwritten
+ * on the owned fluid cells, zero elsewhere. */
+int mhd_gpu_flux_rhs(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim *freestream, const double *W,
+                     const double *grad, double *rhs);
+
+/* uns::reconstruct_cell_vector (include/uns/geometry/Reconstruct.h:14, src/uns/geometry/Reconstruct.cpp:8-46):
+ * face flux (canonical orientation) -> 3 per cell for the cells [0, ncells). */
+int mhd_gpu_cell_vector(MhdMesh *mesh, const double *flux, int32_t ncells, double *out);
+
+/* mhd::add_ideal_emf (Common/induction/IdealEMF.h:40, .cpp:25-129): adds the ideal UCT EMF of
+ * every owned edge to E.  u, B_tot, B_ind: 3 per cell; phi_tot, phi_ind: 1 per face. */
+int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u_cell, const double *B_cell_tot, const double *B_cell_ind,
+                      const double *phi_tot, const double *phi_ind, double cuct, double *E);
+
+/* Boundary edge values of mercury::Solver::rhs (MercuryUns/driver/Solver.cpp:162-167):
+ * edge_mode 1 -> E = 0, edge_mode 2 -> E = (-u_inf x B_imf) . edge_vec, owned edges. */
+int mhd_gpu_edge_modes(MhdMesh *mesh, const double *u_inf, const double *B_imf, double *E);
+
+/* mhd::faraday_update / faraday_update_edge_dt (Common/induction/Faraday.h:17-19, .cpp:15-36)
+ * over mhd::active_faces (:7-13): B[f] -= dt * sum f2e.sgn * E, in FP64. */
+int mhd_gpu_faraday(MhdMesh *mesh, const double *E, double *B, double dt);
+int mhd_gpu_faraday_edge_dt(MhdMesh *mesh, const double *E, const double *dt_edge, double *B);
+
+/* mhd::div_b (Common/diagnostics/DivB.h:15, .cpp:8-24) over the owned cells, FP64.
+ * host_out[0] = max |d2 B|, host_out[1] = max relative, host_out[2] = id of the worst cell. */
+int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *host_out);
+
+/* mhd::cell_current (Common/induction/Current.cpp:9-31): B 3 per cell -> J 3 per cell. */
+int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,74 @@
+/* Host-side mesh services of the caller: the signed cell complex, its metric and its
+ * boundary classification, in exactly the layout the reference's uns::CellComplex,
+ * uns::Geometry and mhd::BoundaryInfo hold (signed CSR: int64 ptr, int32 idx, int8 sgn;
+ * Vec3 arrays as 3 doubles per entity).  These are the inputs of the device hot path
+ * (mhd_gpu.h); in a reference build they come from the reference itself, here they are
+ * produced natively so the library runs stand-alone.
+ *
+ * Numbering, orientation and classification follow the reference bit for bit:
+ *   builder      include/uns/complex/ComplexBuilder.h:14-41, src/uns/complex/ComplexBuilder.cpp:20-134
+ *   generators   src/uns/generate/BoxMesh.cpp:5-33, CubedSphereMesh.cpp:12-83, HexMesh.cpp:7-18
+ *   geometry     src/uns/geometry/Geometry.cpp:17-169 (+ check_geometry :171-205)
+ *   boundary     Common/boundary/BoundaryInfo.cpp:9-49
+ *   hash         src/uns/complex/CellComplex.cpp:56-70 (uns::topology_hash)
+ * The 6-tetrahedron split of hexahedral meshes (mhdm_split_tets) has no counterpart in the
+ * reference, which generates hexahedra only; it feeds tetrahedra to the same builder.
+ *
+ * Every function returns 0 on success and a negative status on error; the message of the
+ * last error of the calling thread is returned by mhdm_last_error(). */
+#ifndef MHD_MESH_H
+#define MHD_MESH_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct MhdHostMesh MhdHostMesh;
+
+const char *mhdm_last_error(void);
+
+/* Generic polyhedral cells (reference ComplexBuilder::add_cell + tag_face + finish).  Cell c
+ * owns the outward face loops cell_ptr[c] .. cell_ptr[c+1]-1; loop l has the nodes
+ * loop_nodes[loop_ptr[l] .. loop_ptr[l+1]-1] counter-clockwise seen from outside.  Tagged face
+ * t has the nodes tag_nodes[tag_ptr[t] .. tag_ptr[t+1]-1] in any order and the tag id tag_id[t];
+ * tag_names (n_names strings, [0] unused) name the tag ids. */
+int mhdm_from_cells(int32_t n_nodes, const double *x, int32_t n_cells, const int64_t *cell_ptr, const int64_t *loop_ptr,
+                    const int32_t *loop_nodes, const int32_t *material, int32_t n_tagged, const int64_t *tag_ptr,
+                    const int32_t *tag_nodes, const int32_t *tag_id, int32_t n_names, const char *const *tag_names,
+                    MhdHostMesh **out);
+
+/* Hexahedral generators (reference uns::make_box / make_cubed_sphere_shell + build_mesh).
+ * as_tets != 0 cuts every hexahedron into the 6 tetrahedra of its lattice body diagonal
+ * (Kuhn split: corner 0 -> corner 7 of the reference's local node order) before building;
+ * jitter > 0 moves every node not on the domain boundary by jitter*h uniformly in each
+ * coordinate (box only; h = cell size per axis) with the splitmix64 stream of `seed`. */
+int mhdm_box(int32_t nx, int32_t ny, int32_t nz, const double *lo, const double *hi, int32_t as_tets, double jitter,
+             uint64_t seed, MhdHostMesh **out);
+int mhdm_shell(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch, int32_t as_tets,
+               MhdHostMesh **out);
+
+void mhdm_free(MhdHostMesh *m);
+
+/* counts[0..3] = nodes, edges, faces, cells */
+void mhdm_counts(const MhdHostMesh *m, int32_t *counts);
+uint64_t mhdm_topology_hash(const MhdHostMesh *m);
+
+/* uns::compute_geometry on this mesh (idempotent). */
+int mhdm_compute_geometry(MhdHostMesh *m);
+/* mhd::BoundaryInfo::build: bc_default and per-tag-name types ("wall", "inflow", "outflow",
+ * "farfield"); u_inf decides farfield faces. */
+int mhdm_boundary(MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const char *const *tag_names,
+                  const char *const *types, const double *u_inf);
+
+/* Pointer to the named array and its element count (NULL / -1 if unknown or not computed).
+ * Names: x, e2n_ptr/idx/sgn, f2e_*, c2f_*, e2f_*, f2c_*, cell_material, face_tag, edge_vec,
+ * edge_mid, edge_len, face_area, face_center, face_area_mag, cell_center, cell_volume,
+ * cell_min_tet_volume, edge_dual_area, ec_ptr, ec_cell, ec_weight, ef_weight, ec_misoriented,
+ * star0..star3, face_kind, edge_mode.  The pointer stays valid until mhdm_free. */
+const void *mhdm_array(const MhdHostMesh *m, const char *name, int64_t *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

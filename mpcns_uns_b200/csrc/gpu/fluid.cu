@@ -1,0 +1,282 @@
+// nvcc-flags: -fmad=false
+// Fluid right-hand side on the device: primitives, limited least-squares gradients, Rusanov
+// face fluxes, and the deterministic (atomic-free) gather of face fluxes into cells.
+// FP64, reference-exact: every expression keeps the reference's operation order and this file
+// is compiled without multiply-add contraction, so results round exactly as the host code does.
+#include "fluid.cuh"
+
+namespace mhd
+{
+// mhd::to_prim over n cells
+__global__ void k_to_prim(SField<const double> U, SField<double> W, int32_t n, int nsp, double gamma, double rho_floor, double p_floor)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    for (int s = 0; s < nsp; ++s)
+    {
+        const Prim5 w = to_prim(U(s, c, 0), U(s, c, 1), U(s, c, 2), U(s, c, 3), U(s, c, 4), gamma, rho_floor, p_floor);
+        W(s, c, 0) = w.rho; W(s, c, 1) = w.u; W(s, c, 2) = w.v; W(s, c, 3) = w.w; W(s, c, 4) = w.p;
+    }
+}
+
+// mhd::Stencil::limited_gradients (Common/fluid/Reconstruction.cpp:80-142), one thread per cell,
+// all species of the launch: least-squares gradient of the 5 primitives from the precomputed
+// w*d and the symmetric inverse, Barth-Jespersen psi over all faces of the cell, optional relative
+// limiter on rho and p, clamp to [0, 1].  Cells without a valid stencil get zero.
+__global__ void __launch_bounds__(128) k_limited_gradients(MeshView m, FluidParams p, SField<const double> W, SField<double> G)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    if (c >= m.no_cells || !m.st_valid[c])
+    {
+        for (int s = 0; s < p.nsp; ++s)
+            for (int q = 0; q < 15; ++q) G(s, c, q) = 0.0;
+        return;
+    }
+    const int32_t k0 = m.c2f_ptr[c], k1 = m.c2f_ptr[c + 1];
+    const V3 xc = ld3(m.cell_center, c);
+    const double *Ip = m.st_inv + 6 * (int64_t)c;
+    const double I00 = Ip[0], I01 = Ip[1], I02 = Ip[2], I11 = Ip[3], I12 = Ip[4], I22 = Ip[5];
+    for (int s = 0; s < p.nsp; ++s)
+    {
+        double wc[5], lo[5], hi[5], g[5][3];
+        for (int q = 0; q < 5; ++q)
+        {
+            wc[q] = W(s, c, q);
+            lo[q] = hi[q] = wc[q];
+            g[q][0] = g[q][1] = g[q][2] = 0.0;
+        }
+        const Prim5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
+        for (int32_t k = k0; k < k1; ++k)
+        {
+            const int32_t nb = m.st_nb[k];
+            if (nb == INT32_MIN) continue;
+            double wn[5];
+            if (nb >= 0)
+            {
+                for (int q = 0; q < 5; ++q) wn[q] = W(s, nb, q);
+            }
+            else
+            {
+                const int32_t f = -(nb + 1);
+                const V3 n = (double(m.c2f_sgn[k]) / m.face_area_mag[f]) * ld3(m.face_area, f);
+                prim_arr(ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, n, p.fs[s]), wn);
+            }
+            const double wx = m.st_wd[3 * (int64_t)k], wy = m.st_wd[3 * (int64_t)k + 1], wz = m.st_wd[3 * (int64_t)k + 2];
+            for (int q = 0; q < 5; ++q)
+            {
+                const double dq = wn[q] - wc[q];
+                g[q][0] += wx * dq;
+                g[q][1] += wy * dq;
+                g[q][2] += wz * dq;
+                lo[q] = dmin(lo[q], wn[q]);
+                hi[q] = dmax(hi[q], wn[q]);
+            }
+        }
+        double psi[5];
+        for (int q = 0; q < 5; ++q)
+        {
+            const double r0 = g[q][0], r1 = g[q][1], r2 = g[q][2];
+            g[q][0] = I00 * r0 + I01 * r1 + I02 * r2;
+            g[q][1] = I01 * r0 + I11 * r1 + I12 * r2;
+            g[q][2] = I02 * r0 + I12 * r1 + I22 * r2;
+            psi[q] = 1.0;
+        }
+        if (p.limit)
+        {
+            for (int32_t k = k0; k < k1; ++k)
+            {
+                const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
+                for (int q = 0; q < 5; ++q)
+                {
+                    const double dl = g[q][0] * dx.x + g[q][1] * dx.y + g[q][2] * dx.z;
+                    if (dl > 1e-300) psi[q] = dmin(psi[q], (hi[q] - wc[q]) / dl);
+                    else if (dl < -1e-300) psi[q] = dmin(psi[q], (lo[q] - wc[q]) / dl);
+                }
+            }
+            if (p.rel_limit > 0)
+                for (int32_t k = k0; k < k1; ++k)
+                {
+                    const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
+                    for (int q = 0; q < 5; q += 4)
+                    {
+                        const double dl = fabs(g[q][0] * dx.x + g[q][1] * dx.y + g[q][2] * dx.z);
+                        if (dl > 1e-300) psi[q] = dmin(psi[q], p.rel_limit * wc[q] / dl);
+                    }
+                }
+        }
+        for (int q = 0; q < 5; ++q)
+        {
+            const double ps = dmax(0.0, dmin(1.0, psi[q]));
+            G(s, c, 3 * q) = ps * g[q][0];
+            G(s, c, 3 * q + 1) = ps * g[q][1];
+            G(s, c, 3 * q + 2) = ps * g[q][2];
+        }
+    }
+}
+
+// Face loop of mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:36-69): Rusanov flux of the
+// reconstructed face states times |A|, per face and species (SoA: F[(s*5 + m)*nf + f]).
+// Faces that the reference skips (Skip kind, no owned fluid cell) get zero.
+__global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SField<const double> W, SField<const double> G,
+                                                   double *__restrict__ F)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    const int64_t nf = m.nf;
+    const int kind = m.face_kind[f];
+    const int32_t p0 = m.f2c_ptr[f], cnt = m.f2c_ptr[f + 1] - p0;
+    bool any_owned = false;
+    for (int q = 0; q < cnt; ++q)
+    {
+        const int32_t cc = m.f2c_idx[p0 + q];
+        any_owned |= cc < m.no_cells && m.material[cc] == 0;
+    }
+    if (kind == 4 || !any_owned)
+    {
+        for (int s = 0; s < p.nsp; ++s)
+            for (int q = 0; q < 5; ++q) F[(s * 5 + q) * nf + f] = 0.0;
+        return;
+    }
+    const double A = m.face_area_mag[f];
+    const V3 n = (1.0 / A) * ld3(m.face_area, f);
+    const V3 xf = ld3(m.face_center, f);
+    const bool interior = cnt == 2 && kind == 0;
+    int32_t cL = -1, cR = -1, c = -1;
+    int sgn = 0;
+    if (interior)
+    {
+        cL = m.face_L[f];
+        cR = m.face_R[f];
+    }
+    else
+    {
+        c = m.f2c_idx[p0];
+        sgn = m.f2c_sgn[p0];
+        if (cnt == 2 && m.material[c] != 0)
+        {
+            c = m.f2c_idx[p0 + 1];
+            sgn = m.f2c_sgn[p0 + 1];
+        }
+    }
+    for (int s = 0; s < p.nsp; ++s)
+    {
+        Prim5 L, R;
+        double g[15];
+        auto state_of = [&](int32_t cc) {
+            const Prim5 w{W(s, cc, 0), W(s, cc, 1), W(s, cc, 2), W(s, cc, 3), W(s, cc, 4)};
+            for (int q = 0; q < 15; ++q) g[q] = G(s, cc, q);
+            return face_state(w, g, xf - ld3(m.cell_center, cc));
+        };
+        if (interior)
+        {
+            L = state_of(cL);
+            R = state_of(cR);
+        }
+        else
+        {
+            const Prim5 in = state_of(c);
+            const Prim5 gh = ghost_state(kind, p.absorb[s] != 0, in, double(sgn) * n, p.fs[s]);
+            if (sgn > 0) { L = in; R = gh; }
+            else { R = in; L = gh; }
+        }
+        double Fl[5];
+        rusanov(L, R, n, p.gamma, Fl);
+        for (int q = 0; q < 5; ++q) F[(s * 5 + q) * nf + f] = Fl[q] * A;
+    }
+}
+
+// Scatter of Common/fluid/FluxRHS.cpp:70-72 as a gather: rhs_c = sum_f -s_cf F_f / V_c over the
+// faces of each owned fluid cell, zero elsewhere.  The faces are visited in ascending id, the
+// order in which the reference's face loop scatters into the cell, so the sum rounds the same.
+__global__ void k_gather_rhs(MeshView m, int nsp, const double *__restrict__ F, SField<double> rhs)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int64_t nf = m.nf;
+    if (c >= m.no_cells || m.material[c] != 0)
+    {
+        for (int s = 0; s < nsp; ++s)
+            for (int q = 0; q < 5; ++q) rhs(s, c, q) = 0.0;
+        return;
+    }
+    const double V = m.cell_volume[c];
+    const int32_t k0 = m.c2f_ptr[c], k1 = m.c2f_ptr[c + 1];
+    for (int s = 0; s < nsp; ++s)
+    {
+        double r[5] = {0, 0, 0, 0, 0};
+        for (int32_t k = k0; k < k1; ++k)
+        {
+            const int32_t f = m.cfa_idx[k];
+            const bool out = m.cfa_sgn[k] > 0;
+            for (int q = 0; q < 5; ++q)
+            {
+                const double v = F[(s * 5 + q) * nf + f] / V;
+                r[q] = out ? r[q] - v : r[q] + v;
+            }
+        }
+        for (int q = 0; q < 5; ++q) rhs(s, c, q) = r[q];
+    }
+}
+
+static FluidParams single_species(int32_t species, const MhdPrim *fs, double gamma, int limit, double rel_limit)
+{
+    FluidParams p{};
+    p.nsp = 1;
+    p.limit = limit;
+    p.gamma = gamma;
+    p.rel_limit = rel_limit;
+    if (fs) p.fs[0] = Prim5{fs->rho, fs->u, fs->v, fs->w, fs->p};
+    p.absorb[0] = species == 1; // reference ghost_state: species 1 is absorbed at walls
+    return p;
+}
+} // namespace mhd
+
+using namespace mhd;
+
+extern "C" {
+
+int mhd_gpu_to_prim(MhdMesh *mesh, const double *U, int32_t n, double gamma, double rho_floor, double p_floor, double *W)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && U && W && n >= 0, "bad argument");
+        if (!n) return;
+        k_to_prim<<<grid_for(n, 256), 256, 0, mesh->stream>>>(SField<const double>{U, 0, 5, 1}, SField<double>{W, 0, 5, 1}, n, 1,
+                                                              gamma, rho_floor, p_floor);
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_limited_gradients(MhdMesh *mesh, const double *W, int32_t species, const MhdPrim *fs, int32_t limit, double rel_limit,
+                              double *grad)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && W && grad && fs, "bad argument");
+        MHD_REQUIRE(species >= 0, "negative species");
+        const MeshView &m = mesh->v;
+        if (!m.nc) return;
+        const FluidParams p = single_species(species, fs, 0.0, limit, rel_limit);
+        k_limited_gradients<<<grid_for(m.nc, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
+                                                                           SField<double>{grad, 0, 15, 1});
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_flux_rhs(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim *fs, const double *W, const double *grad, double *rhs)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && W && grad && rhs && fs, "bad argument");
+        MHD_REQUIRE(gamma > 1.0, "gamma must exceed 1");
+        const MeshView &m = mesh->v;
+        if (!m.nc) return;
+        const FluidParams p = single_species(species, fs, gamma, 1, 0.0);
+        mesh->scratch_face.alloc(5 * static_cast<size_t>(m.nf));
+        k_face_flux<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
+                                                                   SField<const double>{grad, 0, 15, 1}, mesh->scratch_face.p);
+        MHD_LAUNCH_CHECK();
+        k_gather_rhs<<<grid_for(m.nc, 256), 256, 0, mesh->stream>>>(m, 1, mesh->scratch_face.p, SField<double>{rhs, 0, 5, 1});
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+} // extern "C"

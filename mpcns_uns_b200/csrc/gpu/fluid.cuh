@@ -1,0 +1,98 @@
+// Finite-volume building blocks of the ion fluids (device functions shared by the
+// reference-signature entry points and the fused step).
+#pragma once
+#include <climits>
+
+#include "common.cuh"
+
+namespace mhd
+{
+constexpr int kMaxSpecies = 16;
+
+// Per-launch parameters of the fluid kernels (all species of one launch share the mesh).
+struct FluidParams
+{
+    int nsp;                        // species in this launch
+    int limit;                      // Barth-Jespersen on/off
+    double gamma, rel_limit, rho_floor, p_floor;
+    Prim5 fs[kMaxSpecies];          // free-stream (inflow ghost) state per species
+    int8_t absorb[kMaxSpecies];     // wall ghost: 1 = absorbing floor state, 0 = slip reflection
+};
+
+// Species-indexed strided field: value(s, i, m) = p[s * ss + i * si + m * sm]
+template <class T> struct SField
+{
+    T *p;
+    int64_t ss, si, sm;
+    __device__ __forceinline__ T &operator()(int s, int64_t i, int m) const { return p[s * ss + i * si + m * sm]; }
+};
+
+// mhd::to_prim (Common/physics/Euler.h:13-21)
+__device__ __forceinline__ Prim5 to_prim(double U0, double U1, double U2, double U3, double U4, double gamma, double rho_floor,
+                                         double p_floor)
+{
+    Prim5 W;
+    W.rho = dmax(U0, rho_floor);
+    W.u = U1 / W.rho;
+    W.v = U2 / W.rho;
+    W.w = U3 / W.rho;
+    const double ke = 0.5 * W.rho * (W.u * W.u + W.v * W.v + W.w * W.w);
+    W.p = dmax((gamma - 1.0) * (U4 - ke), p_floor);
+    return W;
+}
+
+// mhd::ghost_state (Common/fluid/Reconstruction.cpp:9-24): kind 1 wall, 2 inflow, else zero gradient
+__device__ __forceinline__ Prim5 ghost_state(int kind, bool absorb, const Prim5 &in, V3 n, const Prim5 &fs)
+{
+    if (kind == 1)
+    {
+        if (absorb) return Prim5{1e-12, 0, 0, 0, 1e-12};
+        const double un = in.u * n.x + in.v * n.y + in.w * n.z;
+        Prim5 g = in;
+        g.u -= 2 * un * n.x;
+        g.v -= 2 * un * n.y;
+        g.w -= 2 * un * n.z;
+        return g;
+    }
+    if (kind == 2) return fs;
+    return in;
+}
+
+__device__ __forceinline__ void prim_arr(const Prim5 &w, double *a)
+{
+    a[0] = w.rho; a[1] = w.u; a[2] = w.v; a[3] = w.w; a[4] = w.p;
+}
+
+// mhd::rusanov (Common/physics/Euler.h:30-49): flux per unit area through unit normal n (L -> R)
+__device__ __forceinline__ void rusanov(const Prim5 &L, const Prim5 &R, V3 n, double gamma, double *F)
+{
+    auto cons = [&](const Prim5 &W, double *U) {
+        U[0] = W.rho; U[1] = W.rho * W.u; U[2] = W.rho * W.v; U[3] = W.rho * W.w;
+        U[4] = W.p / (gamma - 1.0) + 0.5 * W.rho * (W.u * W.u + W.v * W.v + W.w * W.w);
+    };
+    double UL[5], UR[5];
+    cons(L, UL);
+    cons(R, UR);
+    const double unL = L.u * n.x + L.v * n.y + L.w * n.z, unR = R.u * n.x + R.v * n.y + R.w * n.z;
+    const double FL[5] = {L.rho * unL, L.rho * unL * L.u + L.p * n.x, L.rho * unL * L.v + L.p * n.y, L.rho * unL * L.w + L.p * n.z,
+                          unL * (UL[4] + L.p)};
+    const double FR[5] = {R.rho * unR, R.rho * unR * R.u + R.p * n.x, R.rho * unR * R.v + R.p * n.y, R.rho * unR * R.w + R.p * n.z,
+                          unR * (UR[4] + R.p)};
+    const double sL = fabs(unL) + sqrt(gamma * L.p / L.rho);
+    const double sR = fabs(unR) + sqrt(gamma * R.p / R.rho);
+    const double s = dmax(sL, sR);
+    for (int q = 0; q < 5; ++q) F[q] = 0.5 * (FL[q] + FR[q]) - 0.5 * s * (UR[q] - UL[q]);
+}
+
+// face_state of Common/fluid/FluxRHS.cpp:16-27: linear extrapolation with positivity fallback
+__device__ __forceinline__ Prim5 face_state(const Prim5 &w, const double *g, V3 dx)
+{
+    Prim5 r;
+    r.rho = w.rho + g[0] * dx.x + g[1] * dx.y + g[2] * dx.z;
+    r.u = w.u + g[3] * dx.x + g[4] * dx.y + g[5] * dx.z;
+    r.v = w.v + g[6] * dx.x + g[7] * dx.y + g[8] * dx.z;
+    r.w = w.w + g[9] * dx.x + g[10] * dx.y + g[11] * dx.z;
+    r.p = w.p + g[12] * dx.x + g[13] * dx.y + g[14] * dx.z;
+    return (r.rho > 0 && r.p > 0) ? r : w;
+}
+} // namespace mhd

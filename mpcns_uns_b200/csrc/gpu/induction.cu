@@ -1,0 +1,392 @@
+// nvcc-flags: -fmad=false
+// Magnetic-field side of the explicit step on the device: cell-field reconstruction, the ideal
+// UCT edge EMF, boundary edge values, constrained transport (FP64) and the div B diagnostic.
+// FP64, reference-exact (see fluid.cu): no multiply-add contraction, reference operation order.
+#include <cfloat>
+
+#include "common.cuh"
+
+namespace mhd
+{
+// uns::reconstruct_cell_vector (src/uns/geometry/Reconstruct.cpp:8-46): area-weighted least squares
+// b . n_f = flux_f / A_f, the 3x3 normal matrix built and inverted per cell.
+__device__ __forceinline__ V3 cell_vector(const MeshView &m, const double *__restrict__ flux, int32_t c)
+{
+    // the full (not symmetrised) matrix: its two triangles round differently and both enter det
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, r[3] = {0, 0, 0};
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        const double A = m.face_area_mag[f];
+        if (A <= 0) continue;
+        const double s = m.c2f_sgn[k];
+        const V3 n = (s / A) * ld3(m.face_area, f);
+        const double nv[3] = {n.x, n.y, n.z};
+        const double phi = s * flux[f];
+        for (int i = 0; i < 3; ++i)
+        {
+            r[i] += nv[i] * phi;
+            for (int j = 0; j < 3; ++j) M[i][j] += A * nv[i] * nv[j];
+        }
+    }
+    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    const double sc = dmax(dmax(dmax(M[0][0], M[1][1]), M[2][2]), 1e-300);
+    if (fabs(det) < 1e-12 * sc * sc * sc) return mk(0, 0, 0);
+    double I[3][3];
+    I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
+    I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+    I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
+    I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+    I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
+    I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+    I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det;
+    I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+    I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+    return mk(I[0][0] * r[0] + I[0][1] * r[1] + I[0][2] * r[2], I[1][0] * r[0] + I[1][1] * r[1] + I[1][2] * r[2],
+              I[2][0] * r[0] + I[2][1] * r[1] + I[2][2] * r[2]);
+}
+
+__global__ void k_cell_vector(MeshView m, const double *__restrict__ flux, int32_t ncells, double *__restrict__ out)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    st3(out, c, cell_vector(m, flux, c));
+}
+
+// Face candidate of mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:32-55):
+// E_f = -n x [ 1/2 (F_L + F_R) - 1/2 a_f (B_R^ind - B_L^ind) ],  F_X = (u_X.n) B_X^tot - u_X B_n^tot
+__global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const double *__restrict__ Bt, const double *__restrict__ Bi,
+                                 const double *__restrict__ phi_tot, double *__restrict__ Ef)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    const double A = m.face_area_mag[f];
+    const V3 n = (1.0 / A) * ld3(m.face_area, f);
+    const double Bn = phi_tot[f] / A;
+    auto flux = [&](int32_t c) {
+        const V3 uc = ld3(u, c);
+        return dot(uc, n) * ld3(Bt, c) - Bn * uc;
+    };
+    const int32_t p0 = m.f2c_ptr[f], cnt = m.f2c_ptr[f + 1] - p0;
+    V3 F;
+    if (cnt == 2)
+    {
+        const int32_t L = m.face_L[f], R = m.face_R[f];
+        const double a = dmax(fabs(dot(ld3(u, L), n)), fabs(dot(ld3(u, R), n)));
+        F = 0.5 * (flux(L) + flux(R)) - (0.5 * a) * (ld3(Bi, R) - ld3(Bi, L));
+    }
+    else
+        F = flux(m.f2c_idx[p0]);
+    st3(Ef, f, -1.0 * cross(n, F));
+}
+
+// Edge loop of mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:59-128), one thread per owned
+// edge: central part sum_f w_ef E_f . t, transverse upwind part with the weights omega corrected
+// by the 2x2 solve in the plane normal to the edge.
+__global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
+                                                   const double *__restrict__ phi_ind, double cuct, double *__restrict__ E)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.no_edges) return;
+    const int32_t f0 = m.e2f_ptr[e], nf = m.e2f_ptr[e + 1] - f0;
+    const double L = m.edge_len[e];
+    if (nf == 0 || L <= 0) return;
+    const int32_t q0 = m.ec_ptr[e], q1 = m.ec_ptr[e + 1];
+    bool any_fluid = false;
+    for (int32_t k = q0; k < q1 && !any_fluid; ++k) any_fluid = m.material[m.ec_cell[k]] == 0;
+    if (!any_fluid) return;
+    const V3 t = ld3(m.edge_vec, e);
+    const V3 th = (1.0 / L) * t;
+    const V3 mid = ld3(m.edge_mid, e);
+    // plane basis (IdealEMF.cpp:14-20)
+    const V3 ax = fabs(th.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
+    V3 e1 = cross(th, ax);
+    e1 = (1.0 / sqrt(dot(e1, e1))) * e1;
+    const V3 e2 = cross(th, e1);
+    double w[kMaxValence], aef[kMaxValence], sg[kMaxValence], qa[kMaxValence], qb[kMaxValence];
+    double Ec = 0, M11 = 0, M12 = 0, M22 = 0, g1 = 0, g2 = 0;
+    for (int i = 0; i < nf; ++i)
+    {
+        const int32_t f = m.e2f_idx[f0 + i];
+        w[i] = m.ef_weight[f0 + i];
+        Ec += w[i] * dot(ld3(Ef, f), t);
+        V3 v = ld3(m.face_center, f) - mid;
+        v = v - dot(v, th) * th;
+        const double nv = sqrt(dot(v, v));
+        const V3 mi = nv > 0 ? (1.0 / nv) * v : mk(0, 0, 0);
+        const V3 nrm = (1.0 / m.face_area_mag[f]) * ld3(m.face_area, f);
+        double a = 0;
+        for (int32_t k = q0; k < q1; ++k) a = dmax(a, fabs(dot(ld3(u, m.ec_cell[k]), mi)));
+        aef[i] = a;
+        sg[i] = dot(th, cross(mi, nrm));
+        const V3 qv = (a * sg[i]) * nrm;
+        qa[i] = dot(qv, e1);
+        qb[i] = dot(qv, e2);
+        M11 += w[i] * qa[i] * qa[i];
+        M12 += w[i] * qa[i] * qb[i];
+        M22 += w[i] * qb[i] * qb[i];
+        g1 += w[i] * qa[i];
+        g2 += w[i] * qb[i];
+    }
+    const double tr = M11 + M22;
+    const double eps = 1e-14 * tr;
+    const double det = (M11 + eps) * (M22 + eps) - M12 * M12;
+    double l1 = 0, l2 = 0;
+    if (tr > 0 && det > 0)
+    {
+        l1 = ((M22 + eps) * g1 - M12 * g2) / det;
+        l2 = ((M11 + eps) * g2 - M12 * g1) / det;
+    }
+    double Eu = 0;
+    for (int i = 0; i < nf; ++i)
+    {
+        const int32_t f = m.e2f_idx[f0 + i];
+        const double omega = w[i] * (1.0 - (qa[i] * l1 + qb[i] * l2));
+        Eu += omega * aef[i] * sg[i] * (phi_ind[f] / m.face_area_mag[f]);
+    }
+    E[e] += Ec + 2.0 * cuct * L * Eu;
+}
+
+// Boundary edge values of mercury::Solver::rhs (MercuryUns/driver/Solver.cpp:162-167)
+__global__ void k_edge_modes(MeshView m, V3 E_inf, double *__restrict__ E)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.no_edges) return;
+    const int mode = m.edge_mode[e];
+    if (mode == 1) E[e] = 0.0;
+    else if (mode == 2) E[e] = dot(E_inf, ld3(m.edge_vec, e));
+}
+
+// mhd::faraday_update (Common/induction/Faraday.cpp:15-24) over mhd::active_faces (:7-13), FP64
+__global__ void k_faraday(MeshView m, const double *__restrict__ E, const double *__restrict__ dt_edge, double dt, double *__restrict__ B)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    bool active = false;
+    for (int32_t k = m.f2c_ptr[f]; k < m.f2c_ptr[f + 1]; ++k) active |= m.f2c_idx[k] < m.no_cells;
+    if (!active) return;
+    double circ = 0.0;
+    if (dt_edge)
+    {
+        for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k)
+        {
+            const int32_t e = m.f2e_idx[k];
+            circ += m.f2e_sgn[k] * dt_edge[e] * E[e];
+        }
+        B[f] -= circ;
+    }
+    else
+    {
+        for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) circ += m.f2e_sgn[k] * E[m.f2e_idx[k]];
+        B[f] -= dt * circ;
+    }
+}
+
+// mhd::div_b (Common/diagnostics/DivB.cpp:8-24): block partial (max |s|, its cell, max rel)
+struct DivPart
+{
+    double max_abs, worst, max_rel;
+};
+__device__ __forceinline__ void div_combine(DivPart &a, const DivPart &b)
+{
+    // the reference keeps the first cell (lowest id) reaching the maximum
+    if (b.max_abs > a.max_abs || (b.max_abs == a.max_abs && b.worst >= 0 && (a.worst < 0 || b.worst < a.worst)))
+    {
+        a.max_abs = b.max_abs;
+        a.worst = b.worst;
+    }
+    a.max_rel = dmax(a.max_rel, b.max_rel);
+}
+__device__ __forceinline__ DivPart div_block_reduce(DivPart v)
+{
+    __shared__ DivPart sh[32];
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        DivPart w{__shfl_down_sync(0xffffffffu, v.max_abs, o), __shfl_down_sync(0xffffffffu, v.worst, o),
+                  __shfl_down_sync(0xffffffffu, v.max_rel, o)};
+        div_combine(v, w);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0)
+    {
+        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : DivPart{0.0, -1.0, 0.0};
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            DivPart w{__shfl_down_sync(0xffffffffu, v.max_abs, o), __shfl_down_sync(0xffffffffu, v.worst, o),
+                      __shfl_down_sync(0xffffffffu, v.max_rel, o)};
+            div_combine(v, w);
+        }
+    }
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_div_b_partial(MeshView m, const double *__restrict__ B, const double *__restrict__ extra,
+                                                        DivPart *__restrict__ part)
+{
+    DivPart v{0.0, -1.0, 0.0};
+    for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < m.no_cells; c += gridDim.x * blockDim.x)
+    {
+        double s = 0, a = 0;
+        for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m.c2f_idx[k];
+            s += m.c2f_sgn[k] * B[f];
+            a += fabs(B[f]) + (extra ? fabs(extra[f]) : 0.0);
+        }
+        const double rel = a > 0 ? fabs(s) / a : 0.0;
+        div_combine(v, DivPart{fabs(s), fabs(s) > 0 ? double(c) : -1.0, rel});
+    }
+    v = div_block_reduce(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+__global__ void __launch_bounds__(1024) k_div_b_final(const DivPart *__restrict__ part, int n, double *__restrict__ out)
+{
+    DivPart v{0.0, -1.0, 0.0};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) div_combine(v, part[i]);
+    v = div_block_reduce(v);
+    if (threadIdx.x == 0)
+    {
+        out[0] = v.max_abs;
+        out[1] = v.max_rel;
+        out[2] = v.worst;
+    }
+}
+
+// mhd::cell_current (Common/induction/Current.cpp:9-31)
+__global__ void k_cell_current(MeshView m, const double *__restrict__ B, double *__restrict__ J)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    if (c >= m.no_cells)
+    {
+        st3(J, c, mk(0, 0, 0));
+        return;
+    }
+    const V3 bc = ld3(B, c);
+    V3 sum = mk(0, 0, 0);
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        V3 bf = bc;
+        const int32_t p0 = m.f2c_ptr[f];
+        if (m.f2c_ptr[f + 1] - p0 == 2)
+        {
+            const int32_t o = m.f2c_idx[p0] == c ? m.f2c_idx[p0 + 1] : m.f2c_idx[p0];
+            bf = 0.5 * (bc + ld3(B, o));
+        }
+        sum = sum + cross(double(m.c2f_sgn[k]) * ld3(m.face_area, f), bf);
+    }
+    const double invV = 1.0 / m.cell_volume[c];
+    st3(J, c, mk(sum.x * invV, sum.y * invV, sum.z * invV));
+}
+
+int div_b_blocks(const MeshView &m) { return static_cast<int>(std::min<int64_t>(grid_for(m.no_cells, 256), 4 * 148)); }
+} // namespace mhd
+
+using namespace mhd;
+
+extern "C" {
+
+int mhd_gpu_cell_vector(MhdMesh *mesh, const double *flux, int32_t ncells, double *out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && flux && out, "bad argument");
+        MHD_REQUIRE(ncells >= 0 && ncells <= mesh->v.nc, "ncells out of range");
+        if (!ncells) return;
+        k_cell_vector<<<grid_for(ncells, 128), 128, 0, mesh->stream>>>(mesh->v, flux, ncells, out);
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const double *Bi, const double *phi_tot, const double *phi_ind,
+                      double cuct, double *E)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && u && Bt && Bi && phi_tot && phi_ind && E, "bad argument");
+        const MeshView &m = mesh->v;
+        if (!m.nf) return;
+        mesh->scratch_face3.alloc(3 * static_cast<size_t>(m.nf));
+        k_face_candidate<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, u, Bt, Bi, phi_tot, mesh->scratch_face3.p);
+        MHD_LAUNCH_CHECK();
+        if (m.no_edges)
+        {
+            k_edge_uct<<<grid_for(m.no_edges, 128), 128, 0, mesh->stream>>>(m, mesh->scratch_face3.p, u, phi_ind, cuct, E);
+            MHD_LAUNCH_CHECK();
+        }
+    });
+}
+
+int mhd_gpu_edge_modes(MhdMesh *mesh, const double *u_inf, const double *B_imf, double *E)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && u_inf && B_imf && E, "bad argument");
+        if (!mesh->v.no_edges) return;
+        const V3 ui = mk(u_inf[0], u_inf[1], u_inf[2]), bi = mk(B_imf[0], B_imf[1], B_imf[2]);
+        const V3 Einf = -1.0 * cross(ui, bi);
+        k_edge_modes<<<grid_for(mesh->v.no_edges, 256), 256, 0, mesh->stream>>>(mesh->v, Einf, E);
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_faraday(MhdMesh *mesh, const double *E, double *B, double dt)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && E && B, "bad argument");
+        if (!mesh->v.nf) return;
+        k_faraday<<<grid_for(mesh->v.nf, 256), 256, 0, mesh->stream>>>(mesh->v, E, nullptr, dt, B);
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_faraday_edge_dt(MhdMesh *mesh, const double *E, const double *dt_edge, double *B)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && E && B && dt_edge, "bad argument");
+        if (!mesh->v.nf) return;
+        k_faraday<<<grid_for(mesh->v.nf, 256), 256, 0, mesh->stream>>>(mesh->v, E, dt_edge, 0.0, B);
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *host_out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && B && host_out, "bad argument");
+        const MeshView &m = mesh->v;
+        if (!m.no_cells)
+        {
+            host_out[0] = host_out[1] = 0.0;
+            host_out[2] = -1.0;
+            return;
+        }
+        const int nb = div_b_blocks(m);
+        mesh->scratch_red.alloc(3 * static_cast<size_t>(nb) + 3);
+        DivPart *part = reinterpret_cast<DivPart *>(mesh->scratch_red.p);
+        double *res = mesh->scratch_red.p + 3 * nb;
+        k_div_b_partial<<<nb, 256, 0, mesh->stream>>>(m, B, extra, part);
+        MHD_LAUNCH_CHECK();
+        k_div_b_final<<<1, 1024, 0, mesh->stream>>>(part, nb, res);
+        MHD_LAUNCH_CHECK();
+        MHD_CUDA(cudaMemcpyAsync(mesh->pinned, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, mesh->stream));
+        MHD_CUDA(cudaStreamSynchronize(mesh->stream));
+        host_out[0] = mesh->pinned[0];
+        host_out[1] = mesh->pinned[1];
+        host_out[2] = mesh->pinned[2];
+    });
+}
+
+int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && B && J, "bad argument");
+        if (!mesh->v.nc) return;
+        k_cell_current<<<grid_for(mesh->v.nc, 128), 128, 0, mesh->stream>>>(mesh->v, B, J);
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+} // extern "C"

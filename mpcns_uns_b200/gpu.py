@@ -1,0 +1,281 @@
+"""Python mirror of the reference's hot-path interface, dispatching to libmhd_gpu.so (include/mhd_gpu.h).
+
+The names, argument meaning and layouts follow the reference functions they replace (AoS
+arrays: value(i, comp) = a[i * ncomp + comp]); torch CUDA tensors carry the device memory.
+There is no CPU fallback: without the built library or a CUDA device every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+
+MHD_OK, MHD_EINVAL, MHD_ECUDA, MHD_ESTATE, MHD_ENOCONV = 0, -1, -2, -3, -4
+
+
+class MhdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("n_nodes", i32), ("n_edges", i32), ("n_faces", i32), ("n_cells", i32),
+                ("n_owned_cells", i32), ("n_owned_edges", i32)] + \
+               [(n, vp) for n in ("c2f_ptr", "c2f_idx", "c2f_sgn", "f2e_ptr", "f2e_idx", "f2e_sgn",
+                                  "e2f_ptr", "e2f_idx", "e2f_sgn", "f2c_ptr", "f2c_idx", "f2c_sgn", "cell_material",
+                                  "edge_vec", "edge_mid", "edge_len", "face_area", "face_center", "face_area_mag",
+                                  "cell_center", "cell_volume", "ec_ptr", "ec_cell", "ec_weight", "ef_weight",
+                                  "star1", "star2", "face_kind", "edge_mode")]
+
+
+class Prim(ctypes.Structure):
+    """mhd::Prim (Common/physics/Euler.h:7-10)."""
+    _fields_ = [("rho", dbl), ("u", dbl), ("v", dbl), ("w", dbl), ("p", dbl)]
+
+
+_SIGS = {
+    "mhd_gpu_last_error": ([], ctypes.c_char_p),
+    "mhd_gpu_device_info": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "mhd_gpu_mesh_create": ([ctypes.POINTER(MeshDesc), ctypes.POINTER(vp)], ctypes.c_int),
+    "mhd_gpu_mesh_destroy": ([vp], ctypes.c_int),
+    "mhd_gpu_mesh_stream": ([vp], vp),
+    "mhd_gpu_mesh_set_stream": ([vp, vp], ctypes.c_int),
+    "mhd_gpu_synchronize": ([vp], ctypes.c_int),
+    "mhd_gpu_to_prim": ([vp, vp, i32, dbl, dbl, dbl, vp], ctypes.c_int),
+    "mhd_gpu_limited_gradients": ([vp, vp, i32, ctypes.POINTER(Prim), i32, dbl, vp], ctypes.c_int),
+    "mhd_gpu_flux_rhs": ([vp, dbl, i32, ctypes.POINTER(Prim), vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_cell_vector": ([vp, vp, i32, vp], ctypes.c_int),
+    "mhd_gpu_ideal_emf": ([vp, vp, vp, vp, vp, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_edge_modes": ([vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_faraday": ([vp, vp, vp, dbl], ctypes.c_int),
+    "mhd_gpu_faraday_edge_dt": ([vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_div_b": ([vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_cell_current": ([vp, vp, vp], ctypes.c_int),
+}
+
+
+def lib():
+    """The loaded C-ABI library (built in-tree on first use if missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_build.GPU_SO):
+            _build.build_gpu()
+        L = ctypes.CDLL(_build.GPU_SO)
+        for name, (args, res) in _SIGS.items():
+            f = getattr(L, name, None)
+            if f is None:
+                continue
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def register(name, args, res=ctypes.c_int):
+    """Declare a further C-ABI symbol (used by the modules that extend this one)."""
+    _SIGS[name] = (args, res)
+    if _lib is not None:
+        f = getattr(_lib, name)
+        f.argtypes = args
+        f.restype = res
+
+
+def check(rc):
+    if rc != MHD_OK:
+        raise MhdError(rc, lib().mhd_gpu_last_error().decode())
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise RuntimeError("mpcns_uns_b200.gpu needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+def dev(a, dtype=None):
+    """numpy array / tensor -> contiguous CUDA tensor (float64 unless an integer dtype is given)."""
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        t = a if dtype is None else a.to(dtype)
+        return t.contiguous().cuda()
+    a = np.ascontiguousarray(a)
+    t = torch.from_numpy(a)
+    if dtype is not None:
+        t = t.to(dtype)
+    elif t.dtype == torch.float32:
+        t = t.double()
+    return t.cuda()
+
+
+def ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class DeviceMesh:
+    """A device copy of one rank's mesh (MhdMesh handle)."""
+
+    def __init__(self, host_mesh):
+        torch = _torch()
+        hm = host_mesh
+        keep = {}
+
+        def arr(name, dtype):
+            a = np.ascontiguousarray(hm[name], dtype)
+            keep[name] = a
+            return ctypes.c_void_p(a.ctypes.data)
+
+        d = MeshDesc()
+        d.n_nodes, d.n_edges, d.n_faces, d.n_cells = hm.n_nodes, hm.n_edges, hm.n_faces, hm.n_cells
+        d.n_owned_cells, d.n_owned_edges = hm.n_cells, hm.n_edges
+        for t in ("c2f", "f2e", "e2f", "f2c"):
+            setattr(d, t + "_ptr", arr(t + "_ptr", np.int64))
+            setattr(d, t + "_idx", arr(t + "_idx", np.int32))
+            setattr(d, t + "_sgn", arr(t + "_sgn", np.int8))
+        d.cell_material = arr("cell_material", np.int32)
+        for n in ("edge_vec", "edge_mid", "edge_len", "face_area", "face_center", "face_area_mag", "cell_center",
+                  "cell_volume", "ec_weight", "ef_weight", "star1", "star2"):
+            setattr(d, n, arr(n, np.float64))
+        d.ec_ptr = arr("ec_ptr", np.int64)
+        d.ec_cell = arr("ec_cell", np.int32)
+        d.face_kind = arr("face_kind", np.int8)
+        d.edge_mode = arr("edge_mode", np.int8)
+        h = vp()
+        torch.cuda.init()
+        check(lib().mhd_gpu_mesh_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        self.host = hm
+        self.n_nodes, self.n_edges, self.n_faces, self.n_cells = hm.n_nodes, hm.n_edges, hm.n_faces, hm.n_cells
+        self._stream = torch.cuda.ExternalStream(lib().mhd_gpu_mesh_stream(self._h))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mhd_gpu_mesh_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self):
+        """torch view of the handle's CUDA stream."""
+        return self._stream
+
+    def synchronize(self):
+        check(lib().mhd_gpu_synchronize(self._h))
+
+    def _enter(self):
+        # the handle's stream must see every tensor that torch's current stream produced
+        self._stream.wait_stream(_torch().cuda.current_stream())
+
+    def _leave(self):
+        _torch().cuda.current_stream().wait_stream(self._stream)
+
+    # ------------------------------------------------------------- reference functions
+    def to_prim(self, U, gamma, rho_floor=1e-10, p_floor=1e-12):
+        """mhd::to_prim (Common/physics/Euler.h:13-21) for every cell."""
+        torch = _torch()
+        U = dev(U)
+        W = torch.empty_like(U)
+        self._enter()
+        check(lib().mhd_gpu_to_prim(self._h, ptr(U), U.numel() // 5, gamma, rho_floor, p_floor, ptr(W)))
+        self._leave()
+        return W
+
+    def limited_gradients(self, W, species, freestream, limit=True, rel_limit=0.0):
+        """Stencil::limited_gradients (Common/fluid/Reconstruction.cpp:80-142): 15 per cell."""
+        torch = _torch()
+        W = dev(W)
+        g = torch.empty(15 * self.n_cells, dtype=torch.float64, device="cuda")
+        fs = Prim(*[float(v) for v in freestream])
+        self._enter()
+        check(lib().mhd_gpu_limited_gradients(self._h, ptr(W), int(species), ctypes.byref(fs), int(bool(limit)),
+                                              float(rel_limit), ptr(g)))
+        self._leave()
+        return g
+
+    def fluid_flux_rhs(self, gamma, species, freestream, W, grad):
+        """mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:30-74): 5 per cell."""
+        torch = _torch()
+        W, grad = dev(W), dev(grad)
+        r = torch.empty(5 * self.n_cells, dtype=torch.float64, device="cuda")
+        fs = Prim(*[float(v) for v in freestream])
+        self._enter()
+        check(lib().mhd_gpu_flux_rhs(self._h, float(gamma), int(species), ctypes.byref(fs), ptr(W), ptr(grad), ptr(r)))
+        self._leave()
+        return r
+
+    def reconstruct_cell_vector(self, flux, ncells=None):
+        """uns::reconstruct_cell_vector (src/uns/geometry/Reconstruct.cpp:8-46): 3 per cell."""
+        torch = _torch()
+        flux = dev(flux)
+        n = self.n_cells if ncells is None else int(ncells)
+        out = torch.empty(3 * n, dtype=torch.float64, device="cuda")
+        self._enter()
+        check(lib().mhd_gpu_cell_vector(self._h, ptr(flux), n, ptr(out)))
+        self._leave()
+        return out
+
+    def add_ideal_emf(self, u_cell, B_cell_tot, B_cell_ind, phi_tot, phi_ind, cuct=0.5, E=None):
+        """mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:25-129): adds into E (zeros if None)."""
+        torch = _torch()
+        args = [dev(a) for a in (u_cell, B_cell_tot, B_cell_ind, phi_tot, phi_ind)]
+        E = torch.zeros(self.n_edges, dtype=torch.float64, device="cuda") if E is None else dev(E).clone()
+        self._enter()
+        check(lib().mhd_gpu_ideal_emf(self._h, *[ptr(a) for a in args], float(cuct), ptr(E)))
+        self._leave()
+        return E
+
+    def edge_modes(self, u_inf, B_imf, E):
+        """Boundary edge values of Solver::rhs (MercuryUns/driver/Solver.cpp:162-167), in place."""
+        u = np.asarray(u_inf, np.float64)
+        b = np.asarray(B_imf, np.float64)
+        self._enter()
+        check(lib().mhd_gpu_edge_modes(self._h, u.ctypes.data_as(vp), b.ctypes.data_as(vp), ptr(E)))
+        self._leave()
+        return E
+
+    def faraday_update(self, E, B, dt):
+        """mhd::faraday_update (Common/induction/Faraday.cpp:15-24); returns the updated copy of B."""
+        E = dev(E)
+        B = dev(B).clone()
+        self._enter()
+        check(lib().mhd_gpu_faraday(self._h, ptr(E), ptr(B), float(dt)))
+        self._leave()
+        return B
+
+    def faraday_update_edge_dt(self, E, dt_edge, B):
+        """mhd::faraday_update_edge_dt (Common/induction/Faraday.cpp:27-36)."""
+        E, d = dev(E), dev(dt_edge)
+        B = dev(B).clone()
+        self._enter()
+        check(lib().mhd_gpu_faraday_edge_dt(self._h, ptr(E), ptr(d), ptr(B)))
+        self._leave()
+        return B
+
+    def div_b(self, B, extra=None):
+        """mhd::div_b (Common/diagnostics/DivB.cpp:8-24) -> dict(max_abs, max_rel, worst_cell_gid)."""
+        B = dev(B)
+        ex = None if extra is None else dev(extra)
+        out = np.zeros(3)
+        self._enter()
+        check(lib().mhd_gpu_div_b(self._h, ptr(B), ptr(ex), out.ctypes.data_as(vp)))
+        return dict(max_abs=float(out[0]), max_rel=float(out[1]), worst_cell_gid=int(out[2]))
+
+    def cell_current(self, B):
+        """mhd::cell_current (Common/induction/Current.cpp:9-31): 3 per cell."""
+        torch = _torch()
+        B = dev(B)
+        J = torch.empty(3 * self.n_cells, dtype=torch.float64, device="cuda")
+        self._enter()
+        check(lib().mhd_gpu_cell_current(self._h, ptr(B), ptr(J)))
+        self._leave()
+        return J

@@ -1,0 +1,151 @@
+"""Seeded synthetic workloads: the meshes and initial states of the benchmark configurations.
+
+No public dataset is involved; every input is generated here from documented seeds.
+Random numbers come from numpy's PCG64 (`np.random.default_rng(seed)`); the node jitter of the
+box comes from the splitmix64 stream of the native mesh builder.
+
+  box(n)     unit cube, n^3 hexahedra x 6 tetrahedra, interior nodes jittered +-0.15 h (seed 0),
+             rho = 1, p = 0.1, u = (1, 0, 0) with 1% uniform noise, gamma = 5/3, B = d1(A)
+             with A = 8 Fourier modes of amplitude 0.05 plus the uniform B0 = (0.1, 0.2, 0)
+             (B0 enters the evolved flux, so d2 B = 0 holds as an integer identity), outflow
+             on every boundary.  n = 16 is the 24,576-cell configuration.
+  shell(...) cubed-sphere shells, 6 tetrahedra per hexahedron, geometric radial layers:
+             two ions (H+, Na+ of mass 23) upstream u = (-8, 0, 0), p = 0.05; Na+ density
+             1e-3 * lognormal(0, 0.5) * exp(-(r - 1)/0.2); IMF (0, 0, -0.5) and a dipole of
+             moment 1 at (0, 0, 0.2) in the static background flux; wall at the inner surface,
+             far field outside.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .mesh import HostMesh
+
+GAMMA = 5.0 / 3.0
+
+
+def to_cons(W, gamma):
+    """mhd::to_cons (Common/physics/Euler.h:22-26) on an (n, 5) array of primitives."""
+    W = np.asarray(W, np.float64).reshape(-1, 5)
+    U = np.empty_like(W)
+    U[:, 0] = W[:, 0]
+    U[:, 1:4] = W[:, :1] * W[:, 1:4]
+    U[:, 4] = W[:, 4] / (gamma - 1.0) + 0.5 * W[:, 0] * (W[:, 1:4] ** 2).sum(1)
+    return U
+
+
+def d1(mesh: HostMesh, A):
+    """(d1 A)_f = sum_e f2e[f,e] A_e."""
+    ptr, idx, sgn = mesh["f2e_ptr"], mesh["f2e_idx"], mesh["f2e_sgn"]
+    rows = np.repeat(np.arange(mesh.n_faces), np.diff(ptr))
+    out = np.zeros(mesh.n_faces)
+    np.add.at(out, rows, sgn * np.asarray(A)[idx])
+    return out
+
+
+def fourier_potential(mesh: HostMesh, seed, modes=8, amp=0.05, B0=(0.1, 0.2, 0.0)):
+    """Edge vector potential A_e = (a(x_mid) + 1/2 B0 x x_mid) . t_e, a = sum of seeded Fourier modes."""
+    rng = np.random.default_rng(seed)
+    x = np.asarray(mesh["edge_mid"])
+    t = np.asarray(mesh["edge_vec"])
+    a = np.zeros_like(x)
+    for _ in range(modes):
+        k = rng.integers(-2, 3, size=3)
+        while not k.any():
+            k = rng.integers(-2, 3, size=3)
+        d = rng.normal(size=3)
+        d *= amp / np.linalg.norm(d)
+        ph = rng.uniform(0, 2 * np.pi)
+        a += np.cos(2 * np.pi * x @ k + ph)[:, None] * d
+    a += 0.5 * np.cross(np.asarray(B0, np.float64), x)
+    return (a * t).sum(1)
+
+
+@dataclass
+class Workload:
+    name: str
+    mesh: HostMesh
+    n_species: int
+    gamma: float
+    U: list                     # per species (n_cells*5,) conservative AoS
+    Phi: np.ndarray             # induced face flux
+    PhiAdd: np.ndarray          # static background face flux
+    fs: list                    # free-stream primitives per species
+    mass: list
+    u_inf: tuple
+    B_imf: tuple
+    cfl: float = 0.4
+    steps: int = 20
+    extra: dict = field(default_factory=dict)
+
+
+def box(n=16, seed=0, jitter=0.15, tets=True):
+    m = HostMesh.box(n, n, n, tets=tets, jitter=jitter, seed=seed).compute_geometry().boundary("outflow")
+    rng = np.random.default_rng(seed + 1)
+    nc = m.n_cells
+    W = np.zeros((nc, 5))
+    W[:, 0] = 1.0 * (1 + 0.01 * rng.uniform(-1, 1, nc))
+    W[:, 1] = 1.0 * (1 + 0.01 * rng.uniform(-1, 1, nc))
+    W[:, 2] = 0.01 * rng.uniform(-1, 1, nc)
+    W[:, 3] = 0.01 * rng.uniform(-1, 1, nc)
+    W[:, 4] = 0.1 * (1 + 0.01 * rng.uniform(-1, 1, nc))
+    Phi = d1(m, fourier_potential(m, seed + 2))
+    return Workload(name=f"box{n}^3x6", mesh=m, n_species=1, gamma=GAMMA, U=[to_cons(W, GAMMA).ravel()], Phi=Phi,
+                    PhiAdd=np.zeros(m.n_faces), fs=[(1.0, 1.0, 0.0, 0.0, 0.1)], mass=[1.0], u_inf=(1.0, 0.0, 0.0),
+                    B_imf=(0.0, 0.0, 0.0), cfl=0.4, steps=20)
+
+
+def background(mesh: HostMesh, B_imf, dipole_m, dipole_c, soft=1e-3):
+    """Static background flux of mercury::set_background (MercuryUns/initial/Initial.cpp:66-84)."""
+    PhiAdd = np.asarray(mesh["face_area"]) @ np.asarray(B_imf, np.float64)
+    r = np.asarray(mesh["edge_mid"]) - np.asarray(dipole_c, np.float64)
+    d2 = (r * r).sum(1) + soft * soft
+    a = np.cross(np.asarray(dipole_m, np.float64), r) / (d2 * np.sqrt(d2))[:, None]
+    A = (a * np.asarray(mesh["edge_vec"])).sum(1)
+    return PhiAdd + d1(mesh, A)
+
+
+def geometric_stretch(nr, r_in, r_out, first):
+    """Ratio q of nr geometric layers between r_in and r_out with first layer thickness `first`."""
+    lo, hi = 1.0, 2.0
+    f = lambda q: first * (q ** nr - 1) / (q - 1) - (r_out - r_in)
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if f(mid) > 0:
+            hi = mid
+        else:
+            lo = mid
+    return 0.5 * (lo + hi)
+
+
+def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0)):
+    if stretch is None:
+        # first layer as thick as the angular spacing at r_in
+        stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
+    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry()
+    m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
+    rng = np.random.default_rng(seed)
+    nc = m.n_cells
+    r = np.linalg.norm(np.asarray(m["cell_center"]), axis=1)
+    masses = masses or ([1.0, 23.0] if n_species == 2 else [1.0] * n_species)
+    U, fs = [], []
+    for s in range(n_species):
+        W = np.zeros((nc, 5))
+        W[:, 1:4] = np.asarray(u_inf)
+        if s == 0:
+            W[:, 0] = 1.0
+            W[:, 4] = 0.05
+            fs.append((1.0, *u_inf, 0.05))
+        else:
+            rho0 = 1e-3 if n_species == 2 else 10 ** rng.uniform(-4, 0)
+            W[:, 0] = rho0 * rng.lognormal(0.0, 0.5, nc) * np.exp(-(r - r_in) / 0.2) + 1e-3 * rho0
+            W[:, 4] = 0.05 * W[:, 0]
+            fs.append((rho0 * 1e-3, *u_inf, 0.05 * rho0 * 1e-3))
+        U.append(to_cons(W, GAMMA).ravel())
+    B_imf = (0.0, 0.0, -0.5)
+    PhiAdd = background(m, B_imf, (0.0, 0.0, 1.0), (0.0, 0.0, 0.2))
+    return Workload(name=f"shell6x{ncube}x{ncube}x{nr}x6", mesh=m, n_species=n_species, gamma=GAMMA, U=U,
+                    Phi=np.zeros(m.n_faces), PhiAdd=PhiAdd, fs=fs, mass=masses, u_inf=tuple(u_inf), B_imf=B_imf,
+                    cfl=0.4, steps=100, extra=dict(stretch=stretch))

@@ -1,0 +1,622 @@
+// C entry points over the reference's own C++ code (compiled in place from the
+// reference tree by oracle/Makefile into oracle/_ref/libmhdref.so).
+//
+// Test infrastructure only: the parity tests, the golden-vector generator and
+// bench.py's CPU-baseline leg call these through ctypes.  Every function here
+// forwards to the reference implementation named in its comment; the only
+// code of this file's own is argument marshalling and the composition of the
+// hot-path sequence of one SSP-RK2 step (ref_rk2_step), which follows
+// MercuryUns/driver/Solver.cpp:94-125 (prepare), :132-169 (rhs),
+// :194-206 (advance), :481-516 (step) with the model sources left out.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "boundary/BoundaryInfo.h"
+#include "diagnostics/DivB.h"
+#include "fluid/FluxRHS.h"
+#include "fluid/MercurySources.h"
+#include "fluid/Reconstruction.h"
+#include "induction/Current.h"
+#include "induction/EdgeEMF.h"
+#include "induction/Faraday.h"
+#include "induction/IdealEMF.h"
+#include "uns/complex/ComplexBuilder.h"
+#include "uns/complex/Validate.h"
+#include "uns/generate/HexMesh.h"
+#include "uns/geometry/Geometry.h"
+#include "uns/geometry/Reconstruct.h"
+#include "uns/refine/Refine.h"
+// The per-edge resistivity of ImplicitInduction (m_) is only filled from its
+// built-in tanh window; the checker sets arbitrary per-edge profiles, so the
+// class is opened here (the layout is unchanged: GCC lays members out in
+// declaration order whatever their access).
+#define private public
+#include "induction/ImplicitInduction.h"
+#undef private
+
+using namespace uns;
+using namespace mhd;
+
+namespace
+{
+struct RefMesh
+{
+    LocalMesh lm;
+    Geometry geo;
+    bool have_geo = false;
+    BoundaryInfo bc;
+    bool have_bc = false;
+    Config cfg;
+    std::unique_ptr<Stencil> stencil;
+    std::vector<char> active;
+};
+
+thread_local std::string g_err;
+
+template <class F> int guarded(F &&f)
+{
+    try { f(); return 0; }
+    catch (const std::exception &e) { g_err = e.what(); return -1; }
+}
+
+RefMesh *wrap(Mesh &&m)
+{
+    auto *r = new RefMesh;
+    r->lm.mesh = std::move(m);
+    r->active = active_faces(r->lm.mesh.cx);
+    return r;
+}
+
+void ensure_geo(RefMesh *r)
+{
+    if (!r->have_geo) { r->geo = compute_geometry(r->lm.mesh); r->have_geo = true; }
+}
+
+template <class T> int64_t put(const std::vector<T> &v, void *out)
+{
+    if (out) std::memcpy(out, v.data(), v.size() * sizeof(T));
+    return static_cast<int64_t>(v.size());
+}
+int64_t put3(const std::vector<Vec3> &v, void *out)
+{
+    if (out)
+    {
+        double *o = static_cast<double *>(out);
+        for (size_t i = 0; i < v.size(); ++i) { o[3 * i] = v[i].x; o[3 * i + 1] = v[i].y; o[3 * i + 2] = v[i].z; }
+    }
+    return static_cast<int64_t>(3 * v.size());
+}
+int64_t put_inc(const Incidence &t, const std::string &part, void *out)
+{
+    if (part == "ptr") return put(t.ptr, out);
+    if (part == "idx") return put(t.idx, out);
+    if (part == "sgn") return put(t.sgn, out);
+    return -1;
+}
+} // namespace
+
+extern "C" {
+
+const char *ref_last_error() { return g_err.c_str(); }
+
+// ---------------------------------------------------------------- meshes
+// Generic polyhedral cells through ComplexBuilder::add_cell / tag_face / finish
+// (src/uns/complex/ComplexBuilder.cpp:45-76, :87-92, :102-134).  Cell c owns the
+// outward loops cell_ptr[c]..cell_ptr[c+1]; loop l has nodes loop_nodes[loop_ptr[l]..loop_ptr[l+1]].
+void *ref_mesh_from_cells(int32_t n_nodes, const double *x, int32_t n_cells, const int64_t *cell_ptr, const int64_t *loop_ptr,
+                          const int32_t *loop_nodes, const int32_t *material, int32_t n_tagged, const int64_t *tag_ptr,
+                          const int32_t *tag_nodes, const int32_t *tag_id, int32_t n_names, const char *const *names)
+{
+    RefMesh *out = nullptr;
+    guarded([&] {
+        ComplexBuilder b(n_nodes);
+        std::vector<std::vector<Id>> loops;
+        for (int32_t c = 0; c < n_cells; ++c)
+        {
+            loops.clear();
+            for (int64_t l = cell_ptr[c]; l < cell_ptr[c + 1]; ++l)
+                loops.emplace_back(loop_nodes + loop_ptr[l], loop_nodes + loop_ptr[l + 1]);
+            b.add_cell(loops, material ? material[c] : kFluid);
+        }
+        for (int32_t t = 0; t < n_tagged; ++t)
+            b.tag_face(std::vector<Id>(tag_nodes + tag_ptr[t], tag_nodes + tag_ptr[t + 1]), tag_id[t]);
+        Mesh m;
+        m.cx = b.finish();
+        m.x.resize(n_nodes);
+        for (int32_t i = 0; i < n_nodes; ++i) m.x[i] = {x[3 * i], x[3 * i + 1], x[3 * i + 2]};
+        m.tag_names.assign(names, names + n_names);
+        out = wrap(std::move(m));
+    });
+    return out;
+}
+
+// uns::make_box + build_mesh (src/uns/generate/BoxMesh.cpp:5-33, HexMesh.cpp:7-18)
+void *ref_mesh_box(int32_t nx, int32_t ny, int32_t nz, const double *lo, const double *hi)
+{
+    RefMesh *out = nullptr;
+    guarded([&] {
+        BoxSpec s;
+        s.nx = nx; s.ny = ny; s.nz = nz;
+        s.lo = {lo[0], lo[1], lo[2]}; s.hi = {hi[0], hi[1], hi[2]};
+        out = wrap(build_mesh(make_box(s)));
+    });
+    return out;
+}
+
+// uns::make_cubed_sphere_shell (src/uns/generate/CubedSphereMesh.cpp:12-83)
+void *ref_mesh_shell(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch)
+{
+    RefMesh *out = nullptr;
+    guarded([&] {
+        CubedSphereSpec s;
+        s.ncube = ncube; s.nr = nr; s.n_solid = n_solid; s.r_in = r_in; s.r_out = r_out; s.r_stretch = r_stretch;
+        out = wrap(build_mesh(make_cubed_sphere_shell(s)));
+    });
+    return out;
+}
+
+// Hanging-node polyhedra: a box refined inside a sphere, as in tests/test_ideal_emf.cpp:357-364
+// (uns::build_refined_mesh, src/uns/refine/RefineMesh.cpp).
+void *ref_mesh_hanging_box(int32_t nx, int32_t ny, int32_t nz, const double *hi, const double *sphere, int32_t level)
+{
+    RefMesh *out = nullptr;
+    guarded([&] {
+        BoxSpec bs;
+        bs.nx = nx; bs.ny = ny; bs.nz = nz; bs.hi = {hi[0], hi[1], hi[2]};
+        Mesh box = build_mesh(make_box(bs));
+        RefineSpec rs;
+        rs.max_level = level;
+        Region reg;
+        reg.kind = Region::Kind::Sphere;
+        reg.a = {sphere[0], sphere[1], sphere[2], sphere[3]};
+        reg.level = level;
+        rs.regions.push_back(reg);
+        out = wrap(build_refined_mesh(box, rs, std::vector<int>(box.cx.n_cells(), 0)).fine);
+    });
+    return out;
+}
+
+void ref_mesh_free(void *h) { delete static_cast<RefMesh *>(h); }
+
+void ref_mesh_counts(void *h, int32_t *out)
+{
+    const CellComplex &cx = static_cast<RefMesh *>(h)->lm.mesh.cx;
+    out[0] = cx.n_nodes(); out[1] = cx.n_edges(); out[2] = cx.n_faces(); out[3] = cx.n_cells();
+}
+
+uint64_t ref_topology_hash(void *h) { return topology_hash(static_cast<RefMesh *>(h)->lm.mesh.cx); }
+
+// uns::validate_topology (src/uns/complex/Validate.cpp:18-69): ok, euler, d1d0, d2d1, boundary faces
+void ref_validate(void *h, int64_t *out)
+{
+    const TopologyReport r = validate_topology(static_cast<RefMesh *>(h)->lm.mesh.cx);
+    out[0] = r.ok; out[1] = r.euler; out[2] = r.d1d0_violations; out[3] = r.d2d1_violations; out[4] = r.boundary_faces;
+}
+
+// uns::check_geometry (src/uns/geometry/Geometry.cpp:171-205)
+void ref_check_geometry(void *h, double *out)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    const GeometryReport g = check_geometry(r->lm.mesh, r->geo);
+    out[0] = g.ok; out[1] = g.min_volume; out[2] = g.max_volume; out[3] = g.min_tet; out[4] = g.max_closure;
+    out[5] = static_cast<double>(g.nonpositive_volume); out[6] = static_cast<double>(g.nonpositive_star);
+    out[7] = static_cast<double>(g.misoriented_dual);
+}
+
+// Copies the named array (topology, geometry or boundary classification) into out (if non-null); returns its
+// element count, or -1 for an unknown name.  Vec3 arrays are flattened x,y,z per entity.
+int64_t ref_array(void *h, const char *cname, void *out)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    const CellComplex &cx = r->lm.mesh.cx;
+    const std::string name(cname);
+    const auto us = name.find('_');
+    if (us != std::string::npos)
+    {
+        const std::string tab = name.substr(0, us), part = name.substr(us + 1);
+        if (tab == "e2n") return put_inc(cx.e2n, part, out);
+        if (tab == "f2e") return put_inc(cx.f2e, part, out);
+        if (tab == "c2f") return put_inc(cx.c2f, part, out);
+        if (tab == "e2f") return put_inc(cx.e2f, part, out);
+        if (tab == "f2c") return put_inc(cx.f2c, part, out);
+        if (tab == "n2e") return put_inc(cx.n2e, part, out);
+    }
+    if (name == "x") return put3(r->lm.mesh.x, out);
+    if (name == "cell_material") return put(cx.cell_material, out);
+    if (name == "face_tag") return put(cx.face_tag, out);
+    if (name == "face_kind" || name == "edge_mode")
+    {
+        if (!r->have_bc) return -1;
+        if (name == "edge_mode") return put(r->bc.edge_mode, out);
+        std::vector<int8_t> k(r->bc.face_kind.size());
+        for (size_t i = 0; i < k.size(); ++i) k[i] = static_cast<int8_t>(r->bc.face_kind[i]);
+        return put(k, out);
+    }
+    ensure_geo(r);
+    const Geometry &g = r->geo;
+    if (name == "edge_vec") return put3(g.edge_vec, out);
+    if (name == "edge_mid") return put3(g.edge_mid, out);
+    if (name == "edge_len") return put(g.edge_len, out);
+    if (name == "face_area") return put3(g.face_area, out);
+    if (name == "face_center") return put3(g.face_center, out);
+    if (name == "face_area_mag") return put(g.face_area_mag, out);
+    if (name == "cell_center") return put3(g.cell_center, out);
+    if (name == "cell_volume") return put(g.cell_volume, out);
+    if (name == "cell_min_tet_volume") return put(g.cell_min_tet_volume, out);
+    if (name == "edge_dual_area") return put3(g.edge_dual_area, out);
+    if (name == "ec_ptr") return put(g.ec_ptr, out);
+    if (name == "ec_cell") return put(g.ec_cell, out);
+    if (name == "ec_weight") return put(g.ec_weight, out);
+    if (name == "ef_weight") return put(g.ef_weight, out);
+    if (name == "ec_misoriented") return put(g.ec_misoriented, out);
+    if (name == "star0") return put(g.star0, out);
+    if (name == "star1") return put(g.star1, out);
+    if (name == "star2") return put(g.star2, out);
+    if (name == "star3") return put(g.star3, out);
+    return -1;
+}
+
+// mhd::BoundaryInfo::build (Common/boundary/BoundaryInfo.cpp:9-49) for a bc_default and per-tag types.
+int ref_boundary_build(void *h, const char *bc_default, int32_t n_pairs, const char *const *tags, const char *const *types,
+                       const double *u_inf)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        ensure_geo(r);
+        r->cfg.bc_default = bc_default;
+        r->cfg.bc_by_tag.clear();
+        for (int32_t i = 0; i < n_pairs; ++i) r->cfg.bc_by_tag[tags[i]] = types[i];
+        r->cfg.u_inf = {u_inf[0], u_inf[1], u_inf[2]};
+        r->bc = BoundaryInfo::build(r->lm, r->geo, r->cfg);
+        r->have_bc = true;
+        r->stencil.reset();
+    });
+}
+
+// ---------------------------------------------------------------- fluid
+// mhd::to_prim (Common/physics/Euler.h:13-21) on n cells of a 5-per-cell array.
+void ref_to_prim(const double *U, int64_t n, double gamma, double rho_floor, double p_floor, double *W)
+{
+    for (int64_t c = 0; c < n; ++c)
+    {
+        const Prim w = to_prim(U + 5 * c, gamma, rho_floor, p_floor);
+        W[5 * c] = w.rho; W[5 * c + 1] = w.u; W[5 * c + 2] = w.v; W[5 * c + 3] = w.w; W[5 * c + 4] = w.p;
+    }
+}
+
+static void ensure_stencil(RefMesh *r)
+{
+    if (!r->have_bc) throw std::runtime_error("boundary classification missing");
+    if (!r->stencil) r->stencil = std::make_unique<Stencil>(r->lm, r->geo, r->bc);
+}
+
+// mhd::Stencil::Stencil + limited_gradients (Common/fluid/Reconstruction.cpp:26-78, :80-142)
+int ref_limited_gradients(void *h, const double *W, int32_t species, const double *fs, int32_t limit, double rel_limit, double *grad)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        ensure_stencil(r);
+        r->stencil->set_rel_limit(rel_limit);
+        const Prim p{fs[0], fs[1], fs[2], fs[3], fs[4]};
+        r->stencil->limited_gradients(r->lm, r->geo, r->bc, W, species, p, limit != 0, grad);
+    });
+}
+
+// mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:30-74)
+int ref_flux_rhs(void *h, double gamma, int32_t species, const double *fs, const double *W, const double *grad, double *rhs)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        if (!r->have_bc) throw std::runtime_error("boundary classification missing");
+        r->cfg.sc.gamma = gamma;
+        const Prim p{fs[0], fs[1], fs[2], fs[3], fs[4]};
+        fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, species, p, W, grad, rhs);
+    });
+}
+
+// ---------------------------------------------------------------- induction
+// uns::reconstruct_cell_vector (src/uns/geometry/Reconstruct.cpp:8-46)
+void ref_cell_vector(void *h, const double *phi, double *out)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    const CellComplex &cx = r->lm.mesh.cx;
+    const auto b = reconstruct_cell_vector(cx, r->geo, phi, cx.n_cells());
+    for (Id c = 0; c < cx.n_cells(); ++c) { out[3 * c] = b[c].x; out[3 * c + 1] = b[c].y; out[3 * c + 2] = b[c].z; }
+}
+
+// mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:25-129); adds into E.
+void ref_ideal_emf(void *h, const double *u, const double *Btot, const double *Bind, const double *phitot, const double *phiind,
+                   double cuct, double *E)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    IdealInputs in;
+    in.u_cell = u; in.B_cell_tot = Btot; in.B_cell_ind = Bind; in.phi_tot = phitot; in.phi_ind = phiind;
+    IdealParams p;
+    p.cuct = cuct;
+    add_ideal_emf(r->lm, r->geo, in, p, E);
+}
+
+// mhd::faraday_update (Common/induction/Faraday.cpp:15-24) over active_faces (:7-13)
+void ref_faraday(void *h, const double *E, double *B, double dt)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    faraday_update(r->lm.mesh.cx, r->active, E, B, dt);
+}
+
+// mhd::faraday_update_edge_dt (Common/induction/Faraday.cpp:27-36)
+void ref_faraday_edge_dt(void *h, const double *E, const double *dt_edge, double *B)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    faraday_update_edge_dt(r->lm.mesh.cx, r->active, E, dt_edge, B);
+}
+
+// mhd::div_b (Common/diagnostics/DivB.cpp:8-24): max_abs, max_rel, worst gid
+void ref_div_b(void *h, const double *B, const double *extra, double *out)
+{
+    const DivBReport d = div_b(static_cast<RefMesh *>(h)->lm.mesh.cx, B, extra);
+    out[0] = d.max_abs; out[1] = d.max_rel; out[2] = static_cast<double>(d.worst_cell_gid);
+}
+
+// mhd::cell_current (Common/induction/Current.cpp:9-31)
+void ref_cell_current(void *h, const double *B, double *J)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    cell_current(r->lm, r->geo, B, J);
+}
+
+// mercury::local_time_step (MercuryUns/fluid/MercurySources.cpp:65-116), two species.
+double ref_local_time_step(void *h, double gamma, double cfl, double inver_MA2, double rho_floor_dt, const double *WH,
+                           const double *WNa, const double *B)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    Config c = r->cfg;
+    c.sc.gamma = gamma; c.cfl = cfl; c.sc.inver_MA2 = inver_MA2; c.rho_floor_dt = rho_floor_dt;
+    return mercury::local_time_step(r->lm, r->geo, c, WH, WNa, B);
+}
+
+struct RefIndParams
+{
+    int32_t resistive, hall, max_it, restart, ilu, pad;
+    double inver_Rem, eta_r_inner, eta_r_outer, eta_width, hall_coef, hall_r_min, hall_r_max, rtol, ilu_shift;
+};
+
+struct RefInd
+{
+    RefMesh *mesh;
+    comm::Exchanger ex;
+    std::unique_ptr<ImplicitInduction> ind;
+    RefInd(RefMesh *m) : mesh(m), ex(MPI_COMM_SELF, m->lm) {}
+};
+
+// mhd::ImplicitInduction::ImplicitInduction (Common/induction/ImplicitInduction.cpp:10-103)
+void *ref_ind_create(void *h, const RefIndParams *p)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    RefInd *out = nullptr;
+    guarded([&] {
+        ensure_geo(r);
+        Config c;
+        c.resistive = p->resistive != 0; c.sc.inver_Rem = p->inver_Rem;
+        c.eta_r_inner = p->eta_r_inner; c.eta_r_outer = p->eta_r_outer; c.eta_width = p->eta_width;
+        c.hall = p->hall != 0; c.sc.hall_coef = p->hall_coef; c.hall_r_min = p->hall_r_min; c.hall_r_max = p->hall_r_max;
+        c.ind_rtol = p->rtol; c.ind_max_it = p->max_it; c.ind_restart = p->restart; c.ind_ilu = p->ilu != 0;
+        c.ind_ilu_shift = p->ilu_shift;
+        auto *ri = new RefInd(r);
+        ri->ind = std::make_unique<ImplicitInduction>(r->lm, r->geo, ri->ex, c);
+        out = ri;
+    });
+    return out;
+}
+
+void ref_ind_free(void *h) { delete static_cast<RefInd *>(h); }
+
+// Per-edge resistive coefficient m_e (eta_e / star1_e) in place of the constructor's tanh window.
+void ref_ind_set_m(void *h, const double *m)
+{
+    RefInd *ri = static_cast<RefInd *>(h);
+    std::copy(m, m + ri->ind->m_.size(), ri->ind->m_.begin());
+    ri->ind->resistive_ = true;
+}
+
+int64_t ref_ind_array(void *h, const char *cname, void *out)
+{
+    ImplicitInduction &I = *static_cast<RefInd *>(h)->ind;
+    const std::string n(cname);
+    if (n == "m") return put(I.m_, out);
+    if (n == "d2") return put(I.d2_, out);
+    if (n == "recon") return put(I.recon_, out);
+    if (n == "taper") return put(I.taper_, out);
+    if (n == "alpha") return put(I.alpha_, out);
+    if (n == "ce_ptr") return put(I.ce_ptr_, out);
+    if (n == "ce_edge") return put(I.ce_edge_, out);
+    if (n == "ce_wt") return put3(I.ce_wt_, out);
+    if (n == "corr") return put(I.corr_, out);
+    return -1;
+}
+
+// ImplicitInduction::set_frozen_state (:105-111)
+void ref_ind_set_frozen(void *h, const double *B0, const double *ne) { static_cast<RefInd *>(h)->ind->set_frozen_state(B0, ne); }
+
+// ImplicitInduction::apply_F (:127-183)
+void ref_ind_apply_F(void *h, const double *phi, double *out) { static_cast<RefInd *>(h)->ind->apply_F(phi, out); }
+
+// ImplicitInduction::apply_A (:185-198): y = x + dt F(d1 x)
+void ref_ind_apply_A(void *h, const double *x, double dt, double *y)
+{
+    ImplicitInduction &I = *static_cast<RefInd *>(h)->ind;
+    const size_t ne = I.m_.size();
+    std::vector<double> xv(x, x + ne), yv(ne);
+    I.apply_A(xv, yv, dt);
+    std::copy(yv.begin(), yv.end(), y);
+}
+
+// ImplicitInduction::solve (:299-390).  use_guess = 0 clears the warm start first.
+int32_t ref_ind_solve(void *h, const double *Phi, const double *Eexpl, const int8_t *dir, double dt, int32_t use_guess, double *E,
+                      double *rel_res)
+{
+    ImplicitInduction &I = *static_cast<RefInd *>(h)->ind;
+    if (!use_guess) I.corr_.clear();
+    std::vector<char> d(I.m_.size());
+    for (size_t e = 0; e < d.size(); ++e) d[e] = dir[e];
+    return I.solve(Phi, Eexpl, d, dt, E, rel_res);
+}
+
+// ---------------------------------------------------------------- one SSP-RK2 step of the hot path
+struct RefStepParams
+{
+    int32_t n_species, second_order;
+    double gamma, rho_floor, p_floor, cuct, M_ref, ne_floor, rel_limit;
+    double u_inf[3], B_imf[3];
+    double mass[16];
+    double fs[16][5];
+};
+
+namespace
+{
+struct StepWork
+{
+    std::vector<std::vector<double>> W, grad, rhs, U1, U2;
+    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2;
+};
+
+// charge-weighted ion velocity of Solver::prepare (Solver.cpp:108-118) with mhd::Scales::numinfo (Scales.cpp:50-62)
+void uplus_of(const RefStepParams &p, const CellComplex &cx, const std::vector<std::vector<double>> &W, std::vector<double> &up)
+{
+    const Id nc = cx.n_cells();
+    up.assign(3 * static_cast<size_t>(nc), 0.0);
+    for (Id c = 0; c < nc; ++c)
+    {
+        if (cx.cell_material[c] != kFluid) continue;
+        if (p.n_species == 2)
+        {
+            Scales sc;
+            sc.M_ref = p.M_ref; sc.M_H = p.mass[0]; sc.M_Na = p.mass[1]; sc.ne_floor = p.ne_floor;
+            const NumInfo ni = sc.numinfo(W[0][5 * c], W[1][5 * c]);
+            for (int a = 0; a < 3; ++a) up[3 * c + a] = ni.chiH * W[0][5 * c + 1 + a] + ni.chiNa * W[1][5 * c + 1 + a];
+            continue;
+        }
+        double n[16], ne = 0;
+        for (int s = 0; s < p.n_species; ++s) { n[s] = std::max(W[s][5 * c], 0.0) / p.mass[s] * p.M_ref; ne += n[s]; }
+        for (int s = 0; s < p.n_species; ++s)
+        {
+            const double chi = ne > 1e-300 ? n[s] / ne : (s == 0 ? 1.0 : 0.0);
+            for (int a = 0; a < 3; ++a) up[3 * c + a] += chi * W[s][5 * c + 1 + a];
+        }
+    }
+}
+
+// Solver::enforce_floors (Solver.cpp:171-191) over all species
+void floors(const RefStepParams &p, const CellComplex &cx, std::vector<double *> &U)
+{
+    for (int k = 0; k < p.n_species; ++k)
+        for (Id c = 0; c < cx.ent[3].n_owned; ++c)
+        {
+            if (cx.cell_material[c] == kSolid) continue;
+            double *u = U[k] + 5 * static_cast<size_t>(c);
+            const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
+            if (!(u[0] >= p.rho_floor)) to_cons(Prim{p.rho_floor, 0, 0, 0, p.p_floor}, p.gamma, u);
+            else if ((p.gamma - 1.0) * (u[4] - ke) < p.p_floor) to_cons(to_prim(u, p.gamma, p.rho_floor, p.p_floor), p.gamma, u);
+        }
+}
+} // namespace
+
+// U[s]: 5 per cell (AoS) per species, updated in place; Phi: induced face flux, updated in place.
+int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        const RefStepParams &p = *pp;
+        ensure_stencil(r);
+        r->cfg.sc.gamma = p.gamma;
+        const CellComplex &cx = r->lm.mesh.cx;
+        const Id nc = cx.n_cells(), ne = cx.n_edges(), nf = cx.n_faces();
+        const int ns = p.n_species;
+        static thread_local StepWork w;
+        w.W.assign(ns, std::vector<double>(5 * static_cast<size_t>(nc)));
+        w.grad.assign(ns, std::vector<double>(15 * static_cast<size_t>(nc)));
+        w.rhs.assign(ns, std::vector<double>(5 * static_cast<size_t>(nc)));
+        w.U1.assign(ns, std::vector<double>());
+        w.U2.assign(ns, std::vector<double>());
+        w.E.assign(ne, 0.0);
+        w.PhiTot.assign(nf, 0.0);
+        r->stencil->set_rel_limit(p.rel_limit);
+        const Vec3 uinf(p.u_inf[0], p.u_inf[1], p.u_inf[2]), bimf(p.B_imf[0], p.B_imf[1], p.B_imf[2]);
+        const Vec3 E_inf = -1.0 * cross(uinf, bimf);
+
+        // prepare + rhs of one stage on (Us, phis); the stage result goes to (Uo, phio)
+        auto stage = [&](std::vector<double *> &Us, const double *phis, std::vector<double *> &Uo, double *phio) {
+            for (int k = 0; k < ns; ++k) ref_to_prim(Us[k], nc, p.gamma, p.rho_floor, p.p_floor, w.W[k].data());
+            const auto bi = reconstruct_cell_vector(cx, r->geo, phis, nc);
+            w.Bind.assign(3 * static_cast<size_t>(nc), 0.0);
+            w.Btot.assign(3 * static_cast<size_t>(nc), 0.0);
+            for (Id c = 0; c < nc; ++c)
+            {
+                const double b[3] = {bi[c].x, bi[c].y, bi[c].z};
+                for (int a = 0; a < 3; ++a) { w.Bind[3 * c + a] = b[a]; w.Btot[3 * c + a] = b[a] + BaddCell[3 * c + a]; }
+            }
+            uplus_of(p, cx, w.W, w.uplus);
+            for (Id f = 0; f < nf; ++f) w.PhiTot[f] = phis[f] + PhiAdd[f];
+            for (int k = 0; k < ns; ++k)
+            {
+                const Prim fs{p.fs[k][0], p.fs[k][1], p.fs[k][2], p.fs[k][3], p.fs[k][4]};
+                if (p.second_order) r->stencil->limited_gradients(r->lm, r->geo, r->bc, w.W[k].data(), k, fs, true, w.grad[k].data());
+                else std::fill(w.grad[k].begin(), w.grad[k].end(), 0.0);
+                fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, k, fs, w.W[k].data(), w.grad[k].data(), w.rhs[k].data());
+            }
+            std::fill(w.E.begin(), w.E.end(), 0.0);
+            IdealInputs in;
+            in.u_cell = w.uplus.data(); in.B_cell_tot = w.Btot.data(); in.B_cell_ind = w.Bind.data();
+            in.phi_tot = w.PhiTot.data(); in.phi_ind = phis;
+            IdealParams ip;
+            ip.cuct = p.cuct;
+            add_ideal_emf(r->lm, r->geo, in, ip, w.E.data());
+            for (Id e = 0; e < cx.ent[1].n_owned; ++e)
+            {
+                if (r->bc.edge_mode[e] == 1) w.E[e] = 0.0;
+                else if (r->bc.edge_mode[e] == 2) w.E[e] = dot(E_inf, r->geo.edge_vec[e]);
+            }
+            // advance: out = base + dt * rhs on the owned fluid cells, CT on the active faces, floors
+            for (int k = 0; k < ns; ++k)
+            {
+                std::copy(Us[k], Us[k] + 5 * static_cast<size_t>(nc), Uo[k]);
+                for (Id c = 0; c < cx.ent[3].n_owned; ++c)
+                {
+                    if (cx.cell_material[c] == kSolid) continue;
+                    for (int m = 0; m < 5; ++m) Uo[k][5 * static_cast<size_t>(c) + m] += dt * w.rhs[k][5 * static_cast<size_t>(c) + m];
+                }
+            }
+            std::copy(phis, phis + nf, phio);
+            faraday_update(cx, r->active, w.E.data(), phio, dt);
+            floors(p, cx, Uo);
+        };
+        std::vector<double *> U0(U, U + ns), U1(ns), U2(ns);
+        for (int k = 0; k < ns; ++k)
+        {
+            w.U1[k].resize(5 * static_cast<size_t>(nc));
+            w.U2[k].resize(5 * static_cast<size_t>(nc));
+            U1[k] = w.U1[k].data();
+            U2[k] = w.U2[k].data();
+        }
+        w.Phi1.resize(nf);
+        w.Phi2.resize(nf);
+        stage(U0, Phi, U1, w.Phi1.data());
+        stage(U1, w.Phi1.data(), U2, w.Phi2.data());
+        for (int k = 0; k < ns; ++k)
+            for (size_t i = 0; i < 5 * static_cast<size_t>(nc); ++i) U0[k][i] = 0.5 * (U0[k][i] + U2[k][i]);
+        for (Id f = 0; f < nf; ++f) Phi[f] = 0.5 * (Phi[f] + w.Phi2[f]);
+    });
+}
+
+} // extern "C"

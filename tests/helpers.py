@@ -1,0 +1,65 @@
+"""Shared helpers of the parity tests: test meshes in both worlds and comparison utilities."""
+from __future__ import annotations
+
+import numpy as np
+
+from mpcns_uns_b200.mesh import HostMesh
+
+BOX_TAGS = ("", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+SHELL_TAGS = ("", "inner", "outer")
+
+# boundary set-ups exercised by the tests: (bc_default, per-tag types, u_inf)
+MIXED_BOX_BC = ("outflow", {"xmin": "inflow", "xmax": "outflow", "ymin": "wall", "ymax": "wall",
+                            "zmin": "farfield", "zmax": "farfield"}, (0.5, 0.2, -0.3))
+SHELL_BC = ("outflow", {"inner": "wall", "outer": "farfield"}, (-8.0, 0.0, 0.0))
+
+
+def tagged_faces(m: HostMesh):
+    """(node loop, tag) of every tagged face of a built mesh."""
+    ft = np.asarray(m["face_tag"])
+    e2n = np.asarray(m["e2n_idx"]).reshape(-1, 2)
+    fp, fi, fs = m["f2e_ptr"], m["f2e_idx"], m["f2e_sgn"]
+    out = []
+    for f in np.nonzero(ft)[0]:
+        nodes = [int(e2n[e, 0] if s > 0 else e2n[e, 1]) for e, s in zip(fi[fp[f]:fp[f + 1]], fs[fp[f]:fp[f + 1]])]
+        out.append((nodes, int(ft[f])))
+    return out
+
+
+def ref_twin(m: HostMesh, tag_names):
+    """The same complex built by the reference's ComplexBuilder from this mesh's cells."""
+    from oracle.ref import RefMesh
+    return RefMesh.from_cells(np.asarray(m["x"]), m.outward_loops(), np.asarray(m["cell_material"]), tagged_faces(m),
+                              tag_names)
+
+
+def host_from_ref(r, tag_names):
+    """A HostMesh built natively from the cells of a reference mesh (e.g. its refined polyhedra)."""
+    x = r["x"]
+    e2n = r["e2n_idx"].reshape(-1, 2)
+    fp, fi, fs = r["f2e_ptr"], r["f2e_idx"], r["f2e_sgn"]
+    cp, ci, cs = r["c2f_ptr"], r["c2f_idx"], r["c2f_sgn"]
+    loops_of_face = []
+    for f in range(r.n_faces):
+        loops_of_face.append([int(e2n[e, 0] if s > 0 else e2n[e, 1]) for e, s in zip(fi[fp[f]:fp[f + 1]], fs[fp[f]:fp[f + 1]])])
+    cells = []
+    for c in range(r.n_cells):
+        cells.append([loops_of_face[ci[k]] if cs[k] > 0 else loops_of_face[ci[k]][::-1] for k in range(cp[c], cp[c + 1])])
+    ft = r["face_tag"]
+    tagged = [(loops_of_face[f], int(ft[f])) for f in np.nonzero(ft)[0]]
+    return HostMesh.from_cells(x, cells, r["cell_material"], tagged, tag_names)
+
+
+def rel_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    scale = max(float(np.max(np.abs(b))) if b.size else 0.0, 1e-300)
+    return float(np.max(np.abs(a - b))) / scale if a.size else 0.0
+
+
+def random_prims(n, rng, rho=(0.5, 1.5), p=(0.05, 0.15), u=1.0):
+    W = np.zeros((n, 5))
+    W[:, 0] = rng.uniform(*rho, n)
+    W[:, 1:4] = rng.uniform(-u, u, (n, 3))
+    W[:, 4] = rng.uniform(*p, n)
+    return W.ravel()

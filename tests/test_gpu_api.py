@@ -1,0 +1,176 @@
+"""Parity of every reference-signature entry point of the C-ABI against the reference's own code.
+
+Each device function runs on the same seeded inputs as the compiled reference
+(oracle/_ref) on meshes that cover the boundary kinds (interior, wall, inflow, outflow,
+far field, solid interfaces, skipped faces), tetrahedra, hexahedra and hanging-node
+polyhedra.  FP64 results must agree to 1e-12 relative to the largest reference value.
+"""
+import numpy as np
+import pytest
+
+from helpers import BOX_TAGS, MIXED_BOX_BC, SHELL_BC, SHELL_TAGS, host_from_ref, random_prims, ref_twin, rel_err
+from mpcns_uns_b200.mesh import HostMesh
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+ref = pytest.importorskip("oracle.ref")
+if not ref.available():
+    pytest.skip("reference checker not built (make -C oracle ref)", allow_module_level=True)
+
+
+def _mk(name):
+    if name == "cfg1":
+        h = HostMesh.box(16, 16, 16, tets=True, jitter=0.15, seed=0)
+        bc, tags = ("outflow", {}, (1.0, 0.0, 0.0)), BOX_TAGS
+    elif name == "box_hex_mixed":
+        h = HostMesh.box(4, 3, 5, hi=(2.0, 1.5, 2.5))
+        bc, tags = MIXED_BOX_BC, BOX_TAGS
+    elif name == "box_tets_mixed":
+        h = HostMesh.box(5, 4, 3, tets=True, jitter=0.1, seed=3)
+        bc, tags = MIXED_BOX_BC, BOX_TAGS
+    elif name == "shell_solid":
+        h = HostMesh.shell(4, 4, 0.8, 5.0, 1.2, n_solid=1, tets=True)
+        bc, tags = SHELL_BC, SHELL_TAGS
+    elif name == "hanging":
+        r0 = ref.RefMesh.hanging_box()
+        h = host_from_ref(r0, BOX_TAGS)
+        bc, tags = MIXED_BOX_BC, BOX_TAGS
+    else:
+        raise KeyError(name)
+    h.compute_geometry().boundary(bc[0], bc[1], bc[2])
+    r = ref_twin(h, tags).boundary(bc[0], bc[1], bc[2])
+    assert h.topology_hash() == r.topology_hash()
+    from mpcns_uns_b200.gpu import DeviceMesh
+    return h, r, DeviceMesh(h), bc
+
+
+MESHES = ["cfg1", "box_hex_mixed", "box_tets_mixed", "shell_solid", "hanging"]
+_cache = {}
+
+
+@pytest.fixture(params=MESHES)
+def meshes(request):
+    if request.param not in _cache:
+        _cache[request.param] = _mk(request.param)
+    return _cache[request.param]
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def test_boundary_classification_bit_exact(meshes):
+    h, r, d, bc = meshes
+    assert np.array_equal(np.asarray(h["face_kind"]), r["face_kind"])
+    assert np.array_equal(np.asarray(h["edge_mode"]), r["edge_mode"])
+
+
+def test_to_prim(meshes):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(11)
+    U = rng.uniform(-1, 1, 5 * h.n_cells)
+    U[0::5] = rng.uniform(-0.1, 1.0, h.n_cells)  # some below the floor
+    W = _np(d.to_prim(U, 5 / 3))
+    assert rel_err(W, r.to_prim(U, 5 / 3)) < TOL
+
+
+@pytest.mark.parametrize("species,limit,rel_limit", [(0, True, 0.0), (1, True, 0.0), (0, False, 0.0), (0, True, 0.5)])
+def test_limited_gradients(meshes, species, limit, rel_limit):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(100 + species)
+    W = random_prims(h.n_cells, rng)
+    fs = (1.1, 0.3, -0.2, 0.1, 0.12)
+    g = _np(d.limited_gradients(W, species, fs, limit, rel_limit))
+    gr = r.limited_gradients(W, species, fs, limit, rel_limit)
+    assert rel_err(g, gr) < TOL
+
+
+@pytest.mark.parametrize("species", [0, 1])
+def test_flux_rhs(meshes, species):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(200 + species)
+    W = random_prims(h.n_cells, rng)
+    fs = (1.1, 0.3, -0.2, 0.1, 0.12)
+    grad = r.limited_gradients(W, species, fs, True, 0.0)
+    rhs = _np(d.fluid_flux_rhs(5 / 3, species, fs, W, grad))
+    rr = r.flux_rhs(W, grad, species, fs, 5 / 3)
+    assert rel_err(rhs, rr) < TOL
+
+
+def test_cell_vector(meshes):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(300)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    assert rel_err(_np(d.reconstruct_cell_vector(phi)), r.cell_vector(phi)) < TOL
+
+
+@pytest.mark.parametrize("cuct", [0.5, 0.0])
+def test_ideal_emf(meshes, cuct):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(400)
+    u = rng.uniform(-1, 1, 3 * h.n_cells)
+    Bt = rng.uniform(-1, 1, 3 * h.n_cells)
+    Bi = rng.uniform(-1, 1, 3 * h.n_cells)
+    pt = rng.uniform(-1, 1, h.n_faces)
+    pi = rng.uniform(-1, 1, h.n_faces)
+    E0 = rng.uniform(-1, 1, h.n_edges)
+    E = _np(d.add_ideal_emf(u, Bt, Bi, pt, pi, cuct, E0))
+    Er = r.ideal_emf(u, Bt, Bi, pt, pi, cuct, E0)
+    assert rel_err(E, Er) < TOL
+
+
+def test_edge_modes(meshes):
+    h, r, d, bc = meshes
+    from mpcns_uns_b200.gpu import dev
+    rng = np.random.default_rng(450)
+    E0 = rng.uniform(-1, 1, h.n_edges)
+    u_inf, B_imf = (0.4, -0.2, 0.3), (0.3, 0.5, -0.2)
+    E = dev(E0)
+    d.edge_modes(u_inf, B_imf, E)
+    d.synchronize()
+    Eref = E0.copy()
+    mode = np.asarray(h["edge_mode"])
+    Einf = -np.cross(u_inf, B_imf)
+    Eref[mode == 1] = 0.0
+    Eref[mode == 2] = np.asarray(h["edge_vec"])[mode == 2] @ Einf
+    assert rel_err(_np(E), Eref) < TOL
+
+
+def test_faraday_and_div_b(meshes):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(500)
+    E = rng.uniform(-1, 1, h.n_edges)
+    B = rng.uniform(-1, 1, h.n_faces)
+    Bn = _np(d.faraday_update(E, B, 0.37))
+    Br = r.faraday(E, B, 0.37)
+    assert rel_err(Bn, Br) < TOL
+    dt_e = rng.uniform(0.1, 1.0, h.n_edges)
+    assert rel_err(_np(d.faraday_update_edge_dt(E, dt_e, B)), r.faraday_edge_dt(E, dt_e, B)) < TOL
+    extra = rng.uniform(-1, 1, h.n_faces)
+    for ex in (None, extra):
+        g = d.div_b(B, ex)
+        rr = r.div_b(B, ex)
+        assert abs(g["max_abs"] - rr["max_abs"]) <= TOL * rr["max_abs"]
+        assert abs(g["max_rel"] - rr["max_rel"]) <= TOL * rr["max_rel"]
+        assert g["worst_cell_gid"] == rr["worst_cell_gid"]
+
+
+def test_ct_keeps_div_b(meshes):
+    """B = d1 A stays divergence free under any number of CT updates (integer identity d2 d1 = 0)."""
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(600)
+    from mpcns_uns_b200.workloads import d1
+    B = d1(h, rng.uniform(-1, 1, h.n_edges))
+    from mpcns_uns_b200.gpu import dev
+    Bd = dev(B)
+    for _ in range(20):
+        Bd = d.faraday_update(rng.uniform(-1, 1, h.n_edges), Bd, 0.02)
+    assert d.div_b(Bd)["max_rel"] < 1e-13
+
+
+def test_cell_current(meshes):
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(700)
+    B = rng.uniform(-1, 1, 3 * h.n_cells)
+    assert rel_err(_np(d.cell_current(B)), r.cell_current(B)) < TOL
