@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the hot path: explicit SSP-RK2 steps of the two-ion shell workload on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (default): cubed-sphere shell r in [1, 6], 6 x 64 x 64 surface cells x 96 geometric
+radial layers, every hexahedron cut into 6 tetrahedra (14,155,776 cells), two ions (H+, Na+),
+inflow u = (-8, 0, 0), IMF (0, 0, -0.5), dipole at (0, 0, 0.2), wall at r = 1; seeded synthetic
+state (mpcns_uns_b200/workloads.py).  One step = the reference's Solver::step hot path:
+CFL step, two stages of primitives + limited gradients + Rusanov fluxes for both ions + ideal
+UCT EMF + CT, floors, SSP-RK2 average, all on the device.  Metric: cell-updates/s
+(cells x species x 2 stages per step).  Inputs exceed L2 (126 MB) many times over, so no
+flush is needed between steps.
+
+Under torchrun (N > 1) every rank runs an independent replica on its own GPU (the hot path
+has no data-path exchange on one mesh per GPU); value = all ranks' cell-updates / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per RK step + GMRES s/solve, mixed vs FP64 GPU at fixed error"
+UNIT = "cell-updates/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ algorithmic bytes per launch
+def mesh_counts(h):
+    return dict(nc=h.n_cells, nf=h.n_faces, ne=h.n_edges, c2f=len(h["c2f_idx"]), f2e=len(h["f2e_idx"]),
+                e2f=len(h["e2f_idx"]), ec=len(h["ec_cell"]), f2c=len(h["f2c_idx"]))
+
+
+def algorithmic_bytes(k, c, nsp, group, p=8):
+    """Compulsory bytes of one launch of kernel class k: every array the pass needs, counted once
+    (perfect reuse within the pass); FP64 values p bytes, indices 4, signs / flags 1."""
+    nc, nf, ne = c["nc"], c["nf"], c["ne"]
+    csr_c2f = c["c2f"] * 5 + nc * 4          # idx + sgn + ptr
+    if k == "prepare":
+        return (10 * nsp * nc + nf * 5 + 3 * nc + 9 * nc) * p + csr_c2f + nc
+    if k == "limited_gradients":
+        g = group
+        return (20 * g * nc + 6 * nc + 3 * c["c2f"] + 3 * nc + 3 * nf) * p + c["c2f"] * 8 + csr_c2f + 2 * nc
+    if k == "face_flux":
+        g = group
+        return (20 * g * nc + 3 * nc + 7 * nf + 5 * g * nf) * p + c["f2c"] * 5 + nf * 4 + 2 * nf * 4 + nf + nc
+    if k == "update":
+        g = group
+        return (5 * g * nf + 12.5 * g * nc + nc) * p + c["c2f"] * 5 + nc * 4 + nc   # stage 1 / 2 averaged (U0 read in stage 2)
+    if k == "face_candidate":
+        return (9 * nc + 4 * nf + 2 * nf + 3 * nf) * p + c["f2c"] * 5 + nf * 4 + 2 * nf * 4
+    if k == "edge_emf":
+        return (c["e2f"] + 7 * ne + 7 * nf + 3 * nf + nf + 3 * nc + ne) * p + c["e2f"] * 4 + ne * 8 + c["ec"] * 4 + nc + ne
+    if k == "ct":
+        return (ne + 2.5 * nf) * p + c["f2e"] * 5 + nf * 4 + c["f2c"] * 4 + nf * 4
+    if k == "cfl":
+        return (5 * nsp * nc + 3 * nc + 4 * nf + nc) * p + csr_c2f + nc
+    return 0.0
+
+
+# ------------------------------------------------------------------ clocks during the timed region
+class ClockSampler:
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fh:
+            for line in fh:
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ workload
+def make_workload(args):
+    from mpcns_uns_b200 import workloads
+    t = time.time()
+    if args.config == "box":
+        wl = workloads.box(args.ncube or 16)
+    else:
+        wl = workloads.shell(args.ncube or 64, args.nr or 96, r_in=1.0, r_out=6.0)
+    log(f"[bench] workload {wl.name}: {wl.mesh.n_cells} cells, {wl.mesh.n_faces} faces, {wl.mesh.n_edges} edges "
+        f"(setup {time.time() - t:.1f}s)")
+    return wl
+
+
+def cpu_sample(args):
+    """Bounded sample of the same workload for the CPU reference: the same shell construction at
+    6 x 16 x 16 x 24 (221,184 cells), two ions."""
+    from mpcns_uns_b200 import workloads
+    if args.config == "box":
+        return workloads.box(12)
+    return workloads.shell(16, 24, r_in=1.0, r_out=6.0)
+
+
+def time_reference(wl, steps, warmup):
+    """The reference's own hot-path step (oracle/_ref, np = 1, one core) on workload wl."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import ref
+    from helpers import BOX_TAGS, SHELL_TAGS, ref_twin
+    from mpcns_uns_b200 import gpu as _g
+    tags = SHELL_TAGS if wl.name.startswith("shell") else BOX_TAGS
+    bc = ("outflow", {"inner": "wall", "outer": "farfield"}, wl.u_inf) if tags is SHELL_TAGS else ("outflow", {}, wl.u_inf)
+    r = ref_twin(wl.mesh, tags).boundary(*bc)
+    p = ref.StepParams()
+    p.n_species, p.second_order = wl.n_species, 1
+    p.gamma, p.rho_floor, p.p_floor, p.cuct, p.M_ref, p.ne_floor, p.rel_limit = wl.gamma, 1e-10, 1e-12, 0.5, 1.0, 0.01, 0.0
+    p.u_inf[:] = list(wl.u_inf)
+    p.B_imf[:] = list(wl.B_imf)
+    for s in range(wl.n_species):
+        p.mass[s] = wl.mass[s]
+        p.fs[s][:] = list(wl.fs[s])
+    U = [np.array(u) for u in wl.U]
+    Phi = np.array(wl.Phi)
+    Badd = r.cell_vector(wl.PhiAdd)
+    dt = None
+    times = []
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        W = [r.to_prim(u, wl.gamma) for u in U]
+        Btot = r.cell_vector(Phi) + Badd
+        if wl.n_species == 2:
+            dt = r.local_time_step(wl.gamma, 0.4, 1.0, 1e-2, W[0], W[1], Btot)
+        else:
+            dt = dt or 0.2 * float(np.min(np.asarray(wl.mesh["edge_len"])))
+        r.rk2_step(p, U, Phi, wl.PhiAdd, Badd, dt)
+        if k >= warmup:
+            times.append(time.perf_counter() - t0)
+    per_step = float(np.median(times))
+    return wl.mesh.n_cells * wl.n_species * 2 / per_step, per_step
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="shell", choices=["shell", "box"])
+    ap.add_argument("--ncube", type=int, default=0)
+    ap.add_argument("--nr", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        wl = cpu_sample(args)
+        from oracle import ref
+        if not ref.available():
+            print(json.dumps({"impl": "reference", "unavailable": "reference checker oracle/_ref not built"}))
+            return
+        steps = max(1, min(args.steps, 5))
+        warm = 1 if args.warmup > 0 else 0
+        v, per = time_reference(wl, steps, warm)
+        cfgd = {"workload": wl.name + " (bounded sample of the 6x64x64x96x6 shell)", "n_species": wl.n_species,
+                "cells": wl.mesh.n_cells, "l2": "inputs > L2"}
+        print(json.dumps({"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+                          "steps": steps, "warmup": warm, "ms_per_step": per * 1e3, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfgd,
+                          "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                                           "sample": f"{wl.name}, {steps} steps, np=1"},
+                          "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from mpcns_uns_b200 import gpu
+    wl = make_workload(args)
+    h = wl.mesh
+    dm = gpu.DeviceMesh(h)
+    p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl)
+    st = gpu.ResidentState(dm, p)
+    st.set(wl.U, wl.Phi, wl.PhiAdd)
+    stream = dm.stream
+
+    for _ in range(args.warmup):
+        st.step(0.0, sync=True)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = st.launches()
+    st.profile(True)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st.step(0.0, sync=False)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    prof = st.profile_read()
+    st.profile(False)
+    launches = st.launches() - l0
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    clocks = sampler.stop() if sampler else None
+    dt_last = st.cfl_dt()
+    if not np.isfinite(dt_last):
+        raise RuntimeError("state became invalid")
+
+    cu_per_step = h.n_cells * wl.n_species * 2
+    value = cu_per_step * args.steps * world / (ms / 1e3)
+
+    # roofline of the dominant kernel (live CUDA-event timing on the handle's stream)
+    counts = mesh_counts(h)
+    peak, peak_kind = peaks()
+    kern = max(prof, key=lambda k: prof[k][0])
+    k_ms, k_n = prof[kern]
+    group = min(2, wl.n_species)
+    bytes_launch = algorithmic_bytes(kern, counts, wl.n_species, group)
+    achieved = bytes_launch / (k_ms / k_n / 1e3) / 1e9
+    breakdown = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
+                     "GBps": (algorithmic_bytes(k, counts, wl.n_species, group) / (v[0] / v[1] / 1e3) / 1e9) if v[1] else None}
+                 for k, v in prof.items() if v[1]}
+
+    # end to end through the C-ABI with host buffers (pinned), copies inside the timed region
+    pin_U = [torch.empty(5 * h.n_cells, dtype=torch.float64).pin_memory() for _ in range(wl.n_species)]
+    pin_P = torch.empty(h.n_faces, dtype=torch.float64).pin_memory()
+    for s in range(wl.n_species):
+        pin_U[s].numpy()[:] = st.U(s)
+    pin_P.numpy()[:] = st.Phi()
+    e2e_times = []
+    for _ in range(args.e2e_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in range(wl.n_species):
+            st.upload(gpu.FIELD_U, pin_U[s].numpy(), s)
+        st.upload(gpu.FIELD_PHI, pin_P.numpy())
+        st.step(0.0, sync=True)
+        for s in range(wl.n_species):
+            pin_U[s].numpy()[:] = st.U(s)
+        pin_P.numpy()[:] = st.Phi()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(e2e_times))
+    e2e_v = cu_per_step * world / e2e_s
+    io_bytes = (5 * h.n_cells * wl.n_species + h.n_faces) * 8
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            from oracle import ref
+            if ref.available():
+                swl = cpu_sample(args)
+                v, per = time_reference(swl, 3, 1)
+                cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
+                       "sample": f"{swl.name} ({swl.mesh.n_cells} cells, same construction), 3 steps after 1 warm-up, np=1"}
+        except Exception as e:  # the baseline is reported, never required
+            log(f"[bench] cpu baseline failed: {e}")
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "f64", "data": "synthetic",
+               "config": {"workload": wl.name, "cells": h.n_cells, "faces": h.n_faces, "edges": h.n_edges,
+                          "n_species": wl.n_species, "global_cells": h.n_cells * world,
+                          "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                          "dt": "CFL 0.4 on device", "l2": "inputs > L2 (no flush needed)", "precision": "fp64 reference-exact"},
+               "gpu_launches": launches,
+               "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                            "algorithmic_bytes_per_launch": bytes_launch},
+               "kernels": breakdown,
+               "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
+               "cpu_baseline": cpu, "clocks": clocks}
+        print(json.dumps(out))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

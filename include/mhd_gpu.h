@@ -110,6 +110,54 @@ int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *h
 /* mhd::cell_current (Common/induction/Current.cpp:9-31): B 3 per cell -> J 3 per cell. */
 int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);
 
+/* ------------------------------------------------------------------ resident state, fused step
+ * The explicit step of mercury::Solver::step (MercuryUns/driver/Solver.cpp:481-516) restricted to
+ * the hot path (prepare :94-125 without the current, rhs :132-169 without model sources, advance
+ * :194-206 with enforce_floors :171-191, the SSP-RK2 average :505-508), for n_species ion fluids.
+ * The state stays on the device between steps, species-major:
+ *   U[(s*5 + m)*n_cells + c]  (FP64 conservative variables), Phi[f] induced face flux (FP64). */
+typedef struct MhdStepParams {
+    int32_t n_species;                 /* 1 .. 16 */
+    int32_t second_order;              /* Config::second_order */
+    double gamma, rho_floor, p_floor;  /* Scales::gamma, Config::rho_floor / p_floor */
+    double cuct;                       /* IdealParams::cuct */
+    double M_ref, ne_floor;            /* Scales::M_ref / ne_floor (charge-weighted ion velocity) */
+    double rel_limit;                  /* Config::recon_rel_limit */
+    double cfl, inver_MA2, rho_floor_dt; /* CFL step of mercury::cell_time_steps (MercurySources.cpp:65-106) */
+    double u_inf[3], B_imf[3];         /* free stream (inflow edge EMF) */
+    double mass[16];                   /* molar mass per species (Scales::M_H, M_Na, ...) */
+    MhdPrim fs[16];                    /* free-stream (inflow ghost) state per species */
+    int8_t absorb[16];                 /* wall ghost absorbs the species (reference: species 1) */
+} MhdStepParams;
+
+#define MHD_FIELD_U 0      /* conservative state of one species, 5 per cell */
+#define MHD_FIELD_PHI 1    /* induced face flux */
+#define MHD_FIELD_PHIADD 2 /* static background face flux; uploading it also sets the background cell field */
+#define MHD_FIELD_BADD 3   /* background cell field (3 per cell), download only */
+
+int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *params, MhdState **out);
+int mhd_gpu_state_destroy(MhdState *state);
+/* Host transfers in the reference layout (AoS); `species` selects the fluid for MHD_FIELD_U. */
+int mhd_gpu_state_upload(MhdState *state, int32_t field, int32_t species, const double *host);
+int mhd_gpu_state_download(MhdState *state, int32_t field, int32_t species, double *host);
+/* Device pointer of a resident array (U: all species, species-major as above). */
+int mhd_gpu_state_device_ptr(MhdState *state, int32_t field, double **out);
+/* mercury::local_time_step (MercurySources.cpp:108-116) of the current state, min with dt_max. */
+int mhd_gpu_cfl_dt(MhdState *state, double dt_max, double *host_dt);
+/* One SSP-RK2 step.  dt_fixed > 0 is used as the step, otherwise the CFL step of the state
+ * capped by dt_max is computed on the device.  dt_used (host, may be NULL) receives the step
+ * and makes the call synchronous; with NULL the step is only enqueued (no host round trip). */
+int mhd_gpu_step_rk2(MhdState *state, double dt_fixed, double dt_max, double *dt_used);
+
+/* Live per-kernel timing of the fused step (CUDA events recorded on the handle's stream around
+ * every launch while enabled).  _read synchronises, returns per kernel class its name (32 chars
+ * each), summed milliseconds and launch count, and restarts the accumulation. */
+int mhd_gpu_state_profile(MhdState *state, int32_t enable);
+int mhd_gpu_state_profile_read(MhdState *state, int32_t max_kernels, char *names, double *ms_total, int64_t *count,
+                               int32_t *n_out);
+/* Number of kernels the fused step has launched since the state was created. */
+int mhd_gpu_state_launches(MhdState *state, int64_t *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -3,7 +3,7 @@
 // face fluxes, and the deterministic (atomic-free) gather of face fluxes into cells.
 // FP64, reference-exact: every expression keeps the reference's operation order and this file
 // is compiled without multiply-add contraction, so results round exactly as the host code does.
-#include "fluid.cuh"
+#include "kernels.cuh"
 
 namespace mhd
 {
@@ -217,6 +217,20 @@ __global__ void k_gather_rhs(MeshView m, int nsp, const double *__restrict__ F, 
         }
         for (int q = 0; q < 5; ++q) rhs(s, c, q) = r[q];
     }
+}
+
+void launch_limited_gradients(const MeshView &m, const FluidParams &p, SField<const double> W, SField<double> G, cudaStream_t s)
+{
+    if (!m.nc) return;
+    k_limited_gradients<<<grid_for(m.nc, 128), 128, 0, s>>>(m, p, W, G);
+    MHD_LAUNCH_CHECK();
+}
+
+void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const double> W, SField<const double> G, double *F, cudaStream_t s)
+{
+    if (!m.nf) return;
+    k_face_flux<<<grid_for(m.nf, 128), 128, 0, s>>>(m, p, W, G, F);
+    MHD_LAUNCH_CHECK();
 }
 
 static FluidParams single_species(int32_t species, const MhdPrim *fs, double gamma, int limit, double rel_limit)

@@ -4,49 +4,11 @@
 // FP64, reference-exact (see fluid.cu): no multiply-add contraction, reference operation order.
 #include <cfloat>
 
-#include "common.cuh"
+#include "induction.cuh"
+#include "kernels.cuh"
 
 namespace mhd
 {
-// uns::reconstruct_cell_vector (src/uns/geometry/Reconstruct.cpp:8-46): area-weighted least squares
-// b . n_f = flux_f / A_f, the 3x3 normal matrix built and inverted per cell.
-__device__ __forceinline__ V3 cell_vector(const MeshView &m, const double *__restrict__ flux, int32_t c)
-{
-    // the full (not symmetrised) matrix: its two triangles round differently and both enter det
-    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, r[3] = {0, 0, 0};
-    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
-    {
-        const int32_t f = m.c2f_idx[k];
-        const double A = m.face_area_mag[f];
-        if (A <= 0) continue;
-        const double s = m.c2f_sgn[k];
-        const V3 n = (s / A) * ld3(m.face_area, f);
-        const double nv[3] = {n.x, n.y, n.z};
-        const double phi = s * flux[f];
-        for (int i = 0; i < 3; ++i)
-        {
-            r[i] += nv[i] * phi;
-            for (int j = 0; j < 3; ++j) M[i][j] += A * nv[i] * nv[j];
-        }
-    }
-    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
-                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
-    const double sc = dmax(dmax(dmax(M[0][0], M[1][1]), M[2][2]), 1e-300);
-    if (fabs(det) < 1e-12 * sc * sc * sc) return mk(0, 0, 0);
-    double I[3][3];
-    I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
-    I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
-    I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
-    I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
-    I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
-    I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
-    I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det;
-    I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
-    I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
-    return mk(I[0][0] * r[0] + I[0][1] * r[1] + I[0][2] * r[2], I[1][0] * r[0] + I[1][1] * r[1] + I[1][2] * r[2],
-              I[2][0] * r[0] + I[2][1] * r[1] + I[2][2] * r[2]);
-}
-
 __global__ void k_cell_vector(MeshView m, const double *__restrict__ flux, int32_t ncells, double *__restrict__ out)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -56,14 +18,16 @@ __global__ void k_cell_vector(MeshView m, const double *__restrict__ flux, int32
 
 // Face candidate of mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:32-55):
 // E_f = -n x [ 1/2 (F_L + F_R) - 1/2 a_f (B_R^ind - B_L^ind) ],  F_X = (u_X.n) B_X^tot - u_X B_n^tot
+// phi_add (optional): static background flux, phi_tot = phi + phi_add as in Solver::prepare (Solver.cpp:119)
 __global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const double *__restrict__ Bt, const double *__restrict__ Bi,
-                                 const double *__restrict__ phi_tot, double *__restrict__ Ef)
+                                 const double *__restrict__ phi_tot, const double *__restrict__ phi_add, double *__restrict__ Ef)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf) return;
     const double A = m.face_area_mag[f];
     const V3 n = (1.0 / A) * ld3(m.face_area, f);
-    const double Bn = phi_tot[f] / A;
+    const double pt = phi_add ? phi_tot[f] + phi_add[f] : phi_tot[f];
+    const double Bn = pt / A;
     auto flux = [&](int32_t c) {
         const V3 uc = ld3(u, c);
         return dot(uc, n) * ld3(Bt, c) - Bn * uc;
@@ -84,18 +48,17 @@ __global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const
 // Edge loop of mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:59-128), one thread per owned
 // edge: central part sum_f w_ef E_f . t, transverse upwind part with the weights omega corrected
 // by the 2x2 solve in the plane normal to the edge.
-__global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
-                                                   const double *__restrict__ phi_ind, double cuct, double *__restrict__ E)
+// Returns false for the edges the reference skips (no faces, zero length, no fluid cell).
+__device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const double *__restrict__ Ef, const double *__restrict__ u,
+                                         const double *__restrict__ phi_ind, double cuct, double &out)
 {
-    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= m.no_edges) return;
     const int32_t f0 = m.e2f_ptr[e], nf = m.e2f_ptr[e + 1] - f0;
     const double L = m.edge_len[e];
-    if (nf == 0 || L <= 0) return;
+    if (nf == 0 || L <= 0) return false;
     const int32_t q0 = m.ec_ptr[e], q1 = m.ec_ptr[e + 1];
     bool any_fluid = false;
     for (int32_t k = q0; k < q1 && !any_fluid; ++k) any_fluid = m.material[m.ec_cell[k]] == 0;
-    if (!any_fluid) return;
+    if (!any_fluid) return false;
     const V3 t = ld3(m.edge_vec, e);
     const V3 th = (1.0 / L) * t;
     const V3 mid = ld3(m.edge_mid, e);
@@ -145,7 +108,52 @@ __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__re
         const double omega = w[i] * (1.0 - (qa[i] * l1 + qb[i] * l2));
         Eu += omega * aef[i] * sg[i] * (phi_ind[f] / m.face_area_mag[f]);
     }
-    E[e] += Ec + 2.0 * cuct * L * Eu;
+    out = Ec + 2.0 * cuct * L * Eu;
+    return true;
+}
+
+__global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
+                                                   const double *__restrict__ phi_ind, double cuct, double *__restrict__ E)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.no_edges) return;
+    double v;
+    if (edge_uct(m, e, Ef, u, phi_ind, cuct, v)) E[e] += v;
+}
+
+// EdgeEMF::begin (zero) + add_ideal_emf + the boundary edge values of Solver::rhs (Solver.cpp:150-167)
+__global__ void __launch_bounds__(128) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
+                                                          const double *__restrict__ phi_ind, double cuct, V3 E_inf,
+                                                          double *__restrict__ E)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    double val = 0.0;
+    if (e < m.no_edges)
+    {
+        double v;
+        if (edge_uct(m, e, Ef, u, phi_ind, cuct, v)) val += v;
+        const int mode = m.edge_mode[e];
+        if (mode == 1) val = 0.0;
+        else if (mode == 2) val = dot(E_inf, ld3(m.edge_vec, e));
+    }
+    E[e] = val;
+}
+
+void launch_face_candidate(const MeshView &m, const double *u, const double *Bt, const double *Bi, const double *phi_tot,
+                           const double *phi_add, double *Ef, cudaStream_t s)
+{
+    if (!m.nf) return;
+    k_face_candidate<<<grid_for(m.nf, 128), 128, 0, s>>>(m, u, Bt, Bi, phi_tot, phi_add, Ef);
+    MHD_LAUNCH_CHECK();
+}
+
+void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
+                            double *E, cudaStream_t s)
+{
+    if (!m.ne) return;
+    k_edge_emf_assign<<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, E);
+    MHD_LAUNCH_CHECK();
 }
 
 // Boundary edge values of mercury::Solver::rhs (MercuryUns/driver/Solver.cpp:162-167)
@@ -310,7 +318,7 @@ int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const do
         const MeshView &m = mesh->v;
         if (!m.nf) return;
         mesh->scratch_face3.alloc(3 * static_cast<size_t>(m.nf));
-        k_face_candidate<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, u, Bt, Bi, phi_tot, mesh->scratch_face3.p);
+        k_face_candidate<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, u, Bt, Bi, phi_tot, nullptr, mesh->scratch_face3.p);
         MHD_LAUNCH_CHECK();
         if (m.no_edges)
         {

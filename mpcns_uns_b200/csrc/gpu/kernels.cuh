@@ -1,0 +1,18 @@
+// Host-side launchers of the hot-path kernels, shared between the translation units that
+// define the kernels and the fused step.
+#pragma once
+#include "fluid.cuh"
+
+namespace mhd
+{
+// fluid.cu
+void launch_limited_gradients(const MeshView &m, const FluidParams &p, SField<const double> W, SField<double> G, cudaStream_t s);
+void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const double> W, SField<const double> G, double *F, cudaStream_t s);
+
+// induction.cu
+void launch_face_candidate(const MeshView &m, const double *u, const double *Bt, const double *Bi, const double *phi_tot,
+                           const double *phi_add, double *Ef, cudaStream_t s);
+// E = begin (0) + ideal UCT EMF of the owned edges, then the boundary edge values (wall 0, inflow E_inf . t)
+void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
+                            double *E, cudaStream_t s);
+} // namespace mhd

@@ -1,0 +1,603 @@
+// nvcc-flags: -fmad=false
+// Resident state and the fused explicit SSP-RK2 step of the hot path (FP64, reference-exact:
+// reference operation order, no multiply-add contraction).
+//
+// One stage on (Us, Phi_s) -> (Uo, Phi_o):
+//   k_prepare      per cell: primitives of every species, B_ind = cell fit of Phi_s, B_tot, u+
+//   [k_cfl_*]      stage 1, CFL mode: per-cell step, device-wide minimum (no host round trip)
+//   per species group: k_limited_gradients, k_face_flux, k_update (gather + U += dt rhs + floors)
+//   k_face_candidate, k_edge_emf_assign (begin + UCT + boundary edge values)
+//   k_ct           Phi_o = Phi_s - dt d1 E on the active faces
+// Stage 2 writes the SSP-RK2 averages U = (U0 + U2)/2, Phi = (Phi0 + Phi2)/2 in place.
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "induction.cuh"
+#include "kernels.cuh"
+
+namespace mhd
+{
+namespace
+{
+constexpr int kGroup = 2; // species whose gradients and face fluxes are held at once
+
+__device__ __forceinline__ void to_cons5(const Prim5 &W, double gamma, double *U)
+{
+    U[0] = W.rho;
+    U[1] = W.rho * W.u;
+    U[2] = W.rho * W.v;
+    U[3] = W.rho * W.w;
+    U[4] = W.p / (gamma - 1.0) + 0.5 * W.rho * (W.u * W.u + W.v * W.v + W.w * W.w);
+}
+
+// Solver::prepare (Solver.cpp:94-125) without the halo exchange and the cell current
+__global__ void __launch_bounds__(128) k_prepare(MeshView m, FluidParams p, const double *__restrict__ mass, double M_ref,
+                                                  SField<const double> U, SField<double> W, const double *__restrict__ phi,
+                                                  const double *__restrict__ Badd, double *__restrict__ Bind, double *__restrict__ Btot,
+                                                  double *__restrict__ up)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double rho[kMaxSpecies];
+    for (int s = 0; s < p.nsp; ++s)
+    {
+        const Prim5 w = to_prim(U(s, c, 0), U(s, c, 1), U(s, c, 2), U(s, c, 3), U(s, c, 4), p.gamma, p.rho_floor, p.p_floor);
+        W(s, c, 0) = w.rho; W(s, c, 1) = w.u; W(s, c, 2) = w.v; W(s, c, 3) = w.w; W(s, c, 4) = w.p;
+        rho[s] = w.rho;
+    }
+    const V3 b = cell_vector(m, phi, c);
+    st3(Bind, c, b);
+    st3(Btot, c, mk(b.x + Badd[3 * (int64_t)c], b.y + Badd[3 * (int64_t)c + 1], b.z + Badd[3 * (int64_t)c + 2]));
+    // charge-weighted ion velocity: mhd::Scales::numinfo (Common/physics/Scales.cpp:50-62) generalised to n species
+    double u[3] = {0, 0, 0};
+    if (m.material[c] == 0)
+    {
+        double n[kMaxSpecies], ne = 0;
+        for (int s = 0; s < p.nsp; ++s)
+        {
+            n[s] = dmax(rho[s], 0.0) / mass[s] * M_ref;
+            ne += n[s];
+        }
+        for (int s = 0; s < p.nsp; ++s)
+        {
+            const double chi = ne > 1e-300 ? n[s] / ne : (s == 0 ? 1.0 : 0.0);
+            for (int a = 0; a < 3; ++a) u[a] += chi * W(s, c, 1 + a);
+        }
+    }
+    st3(up, c, mk(u[0], u[1], u[2]));
+}
+
+// mercury::cell_time_steps (MercuryUns/fluid/MercurySources.cpp:65-106) without the optional gyration
+// limit, n species (the wave speeds use the summed density, as the reference does for its two ions).
+__global__ void __launch_bounds__(128) k_cfl_cells(MeshView m, FluidParams p, double cfl, double inver_MA2, double rho_floor_dt,
+                                                    SField<const double> W, const double *__restrict__ Btot,
+                                                    unsigned long long *__restrict__ dt_bits, int *__restrict__ flag)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.no_cells || m.material[c] != 0) return;
+    double dt = CUDART_INF;
+    const V3 b = ld3(Btot, c);
+    const double B2 = dot(b, b);
+    double rsum = W(0, c, 0);
+    for (int s = 1; s < p.nsp; ++s) rsum = rsum + W(s, c, 0);
+    const double rho_tot = dmax(rsum, rho_floor_dt);
+    const int32_t k0 = m.c2f_ptr[c], k1 = m.c2f_ptr[c + 1];
+    for (int s = 0; s < p.nsp; ++s)
+    {
+        const double cs2 = p.gamma * W(s, c, 4) / dmax(W(s, c, 0), 1e-30);
+        double denom = 0;
+        for (int32_t k = k0; k < k1; ++k)
+        {
+            const int32_t f = m.c2f_idx[k];
+            const double A = m.face_area_mag[f];
+            const V3 n = (1.0 / A) * ld3(m.face_area, f);
+            const double vA2 = inver_MA2 * B2 / rho_tot;
+            const double vAn2 = inver_MA2 * dot(b, n) * dot(b, n) / rho_tot;
+            const double term = cs2 + vA2;
+            const double cf = sqrt(0.5 * (term + sqrt(dmax(0.0, term * term - 4 * cs2 * vAn2))));
+            denom += (fabs(W(s, c, 1) * n.x + W(s, c, 2) * n.y + W(s, c, 3) * n.z) + cf) * A;
+        }
+        if (denom > 0) dt = dmin(dt, cfl * m.cell_volume[c] / denom);
+    }
+    if (!(dt > 0)) atomicOr(flag, 1); // zero, negative or NaN: the reference's "invalid time step"
+    else atomicMin(dt_bits, static_cast<unsigned long long>(__double_as_longlong(dt)));
+}
+
+__global__ void k_cfl_init(unsigned long long *dt_bits, int *flag)
+{
+    *dt_bits = static_cast<unsigned long long>(__double_as_longlong(CUDART_INF));
+    *flag = 0;
+}
+
+// gdt = min(gdt, dt_max); invalid unless finite and positive (Solver.cpp:233-236)
+__global__ void k_cfl_final(const unsigned long long *dt_bits, double dt_max, double *dt, int *flag)
+{
+    double g = __longlong_as_double(static_cast<long long>(*dt_bits));
+    g = dmin(g, dt_max);
+    if (!isfinite(g) || g <= 0) atomicOr(flag, 1);
+    *dt = g;
+}
+
+__global__ void k_set_dt(double *dt, double v, int *flag)
+{
+    *dt = v;
+    *flag = 0;
+}
+
+// Solver::advance (Solver.cpp:194-206) for one species group: rhs gathered from the face fluxes in the
+// reference's scatter order, U = U_base + dt rhs on the owned fluid cells, Solver::enforce_floors
+// (:171-191); stage 2 averages with U0 in place (Solver.cpp:505-506).
+__global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s0, int ng, const double *__restrict__ F,
+                                                 SField<const double> Ub, SField<double> Uo, const double *__restrict__ dtp, int stage2)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int64_t nf = m.nf;
+    const double dt = *dtp;
+    const bool live = c < m.no_cells && m.material[c] == 0;
+    const int32_t k0 = m.c2f_ptr[c], k1 = m.c2f_ptr[c + 1];
+    const double V = m.cell_volume[c];
+    for (int g = 0; g < ng; ++g)
+    {
+        const int s = s0 + g;
+        double u[5];
+        for (int q = 0; q < 5; ++q) u[q] = Ub(s, c, q);
+        if (live)
+        {
+            double r[5] = {0, 0, 0, 0, 0};
+            for (int32_t k = k0; k < k1; ++k)
+            {
+                const int32_t f = m.cfa_idx[k];
+                const bool out = m.cfa_sgn[k] > 0;
+                for (int q = 0; q < 5; ++q)
+                {
+                    const double v = F[(g * 5 + q) * nf + f] / V;
+                    r[q] = out ? r[q] - v : r[q] + v;
+                }
+            }
+            for (int q = 0; q < 5; ++q) u[q] += dt * r[q];
+            const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
+            if (!(u[0] >= p.rho_floor)) to_cons5(Prim5{p.rho_floor, 0, 0, 0, p.p_floor}, p.gamma, u);
+            else if ((p.gamma - 1.0) * (u[4] - ke) < p.p_floor)
+                to_cons5(to_prim(u[0], u[1], u[2], u[3], u[4], p.gamma, p.rho_floor, p.p_floor), p.gamma, u);
+        }
+        if (stage2)
+            for (int q = 0; q < 5; ++q) Uo(s, c, q) = 0.5 * (Uo(s, c, q) + u[q]);
+        else
+            for (int q = 0; q < 5; ++q) Uo(s, c, q) = u[q];
+    }
+}
+
+// mhd::faraday_update on the active faces (Faraday.cpp:15-24); stage 2 averages with Phi0 in place (Solver.cpp:507-508)
+__global__ void __launch_bounds__(256) k_ct(MeshView m, const double *__restrict__ E, const double *__restrict__ phis,
+                                             double *__restrict__ phio, const double *__restrict__ dtp, int stage2)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    bool active = false;
+    for (int32_t k = m.f2c_ptr[f]; k < m.f2c_ptr[f + 1]; ++k) active |= m.f2c_idx[k] < m.no_cells;
+    double v = phis[f];
+    if (active)
+    {
+        double circ = 0.0;
+        for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) circ += m.f2e_sgn[k] * E[m.f2e_idx[k]];
+        v -= *dtp * circ;
+    }
+    phio[f] = stage2 ? 0.5 * (phio[f] + v) : v;
+}
+
+__global__ void k_aos_to_soa(const double *__restrict__ in, double *__restrict__ out, int32_t n, int ncomp)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * ncomp) return;
+    const int64_t c = i / ncomp, q = i % ncomp;
+    out[q * n + c] = in[i];
+}
+
+__global__ void k_soa_to_aos(const double *__restrict__ in, double *__restrict__ out, int32_t n, int ncomp)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * ncomp) return;
+    const int64_t c = i / ncomp, q = i % ncomp;
+    out[i] = in[q * n + c];
+}
+
+__global__ void k_cell_vector_all(MeshView m, const double *__restrict__ flux, double *__restrict__ out)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    st3(out, c, cell_vector(m, flux, c));
+}
+} // namespace
+} // namespace mhd
+
+namespace mhd
+{
+// Kernel classes of the step, timed with CUDA events on the handle's stream when profiling is on.
+enum StepKernel { KP_PREPARE = 0, KP_CFL, KP_GRAD, KP_FLUX, KP_UPDATE, KP_FACE_CAND, KP_EDGE_EMF, KP_CT, KP_COUNT };
+static const char *const kStepKernelNames[KP_COUNT] = {"prepare", "cfl", "limited_gradients", "face_flux",
+                                                        "update",  "face_candidate", "edge_emf", "ct"};
+
+struct Profiler
+{
+    bool on = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KP_COUNT];
+    size_t used[KP_COUNT] = {};
+    ~Profiler()
+    {
+        for (auto &v : ev)
+            for (auto &p : v)
+            {
+                cudaEventDestroy(p.first);
+                cudaEventDestroy(p.second);
+            }
+    }
+    void begin(int k, cudaStream_t s)
+    {
+        if (!on) return;
+        if (used[k] == ev[k].size())
+        {
+            cudaEvent_t a, b;
+            MHD_CUDA(cudaEventCreate(&a));
+            MHD_CUDA(cudaEventCreate(&b));
+            ev[k].emplace_back(a, b);
+        }
+        MHD_CUDA(cudaEventRecord(ev[k][used[k]].first, s));
+    }
+    void end(int k, cudaStream_t s)
+    {
+        if (!on) return;
+        MHD_CUDA(cudaEventRecord(ev[k][used[k]].second, s));
+        ++used[k];
+    }
+};
+} // namespace mhd
+
+struct MhdState
+{
+    MhdMesh *mesh = nullptr;
+    MhdStepParams prm{};
+    mhd::FluidParams fp{};
+    int nsp = 0, group = 0;
+    mhd::DBuf<double> U0, U1, W, grad, F, phi0, phi1, phi_add, badd, bind, btot, up, Ef, E, mass, stage;
+    mhd::DBuf<double> scal; // [0] dt
+    mhd::DBuf<unsigned long long> dt_bits;
+    mhd::DBuf<int> flag;
+    double *pinned = nullptr;
+    int64_t launches = 0; // kernels launched by the step since creation
+    mhd::Profiler prof;
+    ~MhdState()
+    {
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
+namespace mhd
+{
+namespace
+{
+SField<double> soa_state(double *p, int64_t nc) { return {p, 5 * nc, 1, nc}; }
+SField<const double> soa_cstate(const double *p, int64_t nc) { return {p, 5 * nc, 1, nc}; }
+
+void stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max)
+{
+    MhdMesh *mesh = st->mesh;
+    const MeshView &m = mesh->v;
+    cudaStream_t s = mesh->stream;
+    const int64_t nc = m.nc;
+    const int nsp = st->nsp;
+    Profiler &P = st->prof;
+    if (m.nc)
+    {
+        P.begin(KP_PREPARE, s);
+        k_prepare<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->fp, st->mass.p, st->prm.M_ref, soa_cstate(Us, nc), soa_state(st->W.p, nc),
+                                                      phis, st->badd.p, st->bind.p, st->btot.p, st->up.p);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_PREPARE, s);
+        ++st->launches;
+    }
+    if (cfl)
+    {
+        P.begin(KP_CFL, s);
+        k_cfl_init<<<1, 1, 0, s>>>(st->dt_bits.p, st->flag.p);
+        if (m.no_cells)
+            k_cfl_cells<<<grid_for(m.no_cells, 128), 128, 0, s>>>(m, st->fp, st->prm.cfl, st->prm.inver_MA2, st->prm.rho_floor_dt,
+                                                                   soa_cstate(st->W.p, nc), st->btot.p, st->dt_bits.p, st->flag.p);
+        k_cfl_final<<<1, 1, 0, s>>>(st->dt_bits.p, dt_max, st->scal.p, st->flag.p);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_CFL, s);
+        st->launches += m.no_cells ? 3 : 2;
+    }
+    for (int s0 = 0; s0 < nsp; s0 += st->group)
+    {
+        const int ng = std::min(st->group, nsp - s0);
+        FluidParams gp = st->fp;
+        gp.nsp = ng;
+        for (int g = 0; g < ng; ++g)
+        {
+            gp.fs[g] = st->fp.fs[s0 + g];
+            gp.absorb[g] = st->fp.absorb[s0 + g];
+        }
+        const SField<const double> Wg{st->W.p + (int64_t)s0 * 5 * nc, 5 * nc, 1, nc};
+        const SField<double> Gg{st->grad.p, 15 * nc, 1, nc};
+        P.begin(KP_GRAD, s);
+        if (st->prm.second_order) launch_limited_gradients(m, gp, Wg, Gg, s);
+        else MHD_CUDA(cudaMemsetAsync(st->grad.p, 0, (size_t)15 * ng * nc * sizeof(double), s));
+        P.end(KP_GRAD, s);
+        P.begin(KP_FLUX, s);
+        launch_face_flux(m, gp, Wg, SField<const double>{st->grad.p, 15 * nc, 1, nc}, st->F.p, s);
+        P.end(KP_FLUX, s);
+        if (m.nc)
+        {
+            P.begin(KP_UPDATE, s);
+            k_update<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
+                                                         stage2 ? 1 : 0);
+            MHD_LAUNCH_CHECK();
+            P.end(KP_UPDATE, s);
+        }
+        st->launches += (st->prm.second_order && m.nc ? 1 : 0) + (m.nf ? 1 : 0) + (m.nc ? 1 : 0);
+    }
+    const V3 ui = mk(st->prm.u_inf[0], st->prm.u_inf[1], st->prm.u_inf[2]), bi = mk(st->prm.B_imf[0], st->prm.B_imf[1], st->prm.B_imf[2]);
+    const V3 Einf = -1.0 * cross(ui, bi);
+    P.begin(KP_FACE_CAND, s);
+    launch_face_candidate(m, st->up.p, st->btot.p, st->bind.p, phis, st->phi_add.p, st->Ef.p, s);
+    P.end(KP_FACE_CAND, s);
+    P.begin(KP_EDGE_EMF, s);
+    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s);
+    P.end(KP_EDGE_EMF, s);
+    st->launches += (m.nf ? 1 : 0) + (m.ne ? 1 : 0);
+    if (m.nf)
+    {
+        P.begin(KP_CT, s);
+        k_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m, st->E.p, phis, phio, st->scal.p, stage2 ? 1 : 0);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_CT, s);
+        ++st->launches;
+    }
+}
+
+void read_dt(MhdState *st, double *dt_host)
+{
+    cudaStream_t s = st->mesh->stream;
+    MHD_CUDA(cudaMemcpyAsync(st->pinned, st->scal.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaMemcpyAsync(st->pinned + 1, st->flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaStreamSynchronize(s));
+    int flag;
+    std::memcpy(&flag, st->pinned + 1, sizeof(int));
+    if (flag) throw ApiError(MHD_ESTATE, "invalid time step");
+    *dt_host = st->pinned[0];
+}
+} // namespace
+} // namespace mhd
+
+using namespace mhd;
+
+extern "C" {
+
+int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
+{
+    MhdState *st = nullptr;
+    int rc = guarded([&] {
+        MHD_REQUIRE(mesh && p && out, "null argument");
+        MHD_REQUIRE(p->n_species >= 1 && p->n_species <= kMaxSpecies, "n_species must be 1..16");
+        MHD_REQUIRE(p->gamma > 1.0, "gamma must exceed 1");
+        for (int s = 0; s < p->n_species; ++s) MHD_REQUIRE(p->mass[s] > 0, "species masses must be positive");
+        st = new MhdState;
+        st->mesh = mesh;
+        st->prm = *p;
+        st->nsp = p->n_species;
+        st->group = std::min(kGroup, st->nsp);
+        FluidParams &fp = st->fp;
+        fp.nsp = st->nsp;
+        fp.limit = 1;
+        fp.gamma = p->gamma;
+        fp.rel_limit = p->rel_limit;
+        fp.rho_floor = p->rho_floor;
+        fp.p_floor = p->p_floor;
+        for (int s = 0; s < st->nsp; ++s)
+        {
+            fp.fs[s] = Prim5{p->fs[s].rho, p->fs[s].u, p->fs[s].v, p->fs[s].w, p->fs[s].p};
+            fp.absorb[s] = p->absorb[s];
+        }
+        const MeshView &m = mesh->v;
+        const size_t nc = m.nc, nf = m.nf, ne = m.ne;
+        st->U0.alloc(5 * nc * st->nsp);
+        st->U1.alloc(5 * nc * st->nsp);
+        st->W.alloc(5 * nc * st->nsp);
+        st->grad.alloc(15 * nc * st->group);
+        st->F.alloc(5 * nf * st->group);
+        st->phi0.alloc(nf);
+        st->phi1.alloc(nf);
+        st->phi_add.alloc(nf);
+        st->badd.alloc(3 * nc);
+        st->bind.alloc(3 * nc);
+        st->btot.alloc(3 * nc);
+        st->up.alloc(3 * nc);
+        st->Ef.alloc(3 * nf);
+        st->E.alloc(ne);
+        st->stage.alloc(std::max<size_t>(5 * nc, 3 * nc));
+        st->scal.alloc(4);
+        st->dt_bits.alloc(1);
+        st->flag.alloc(1);
+        st->mass.upload(p->mass, st->nsp);
+        MHD_CUDA(cudaMallocHost(&st->pinned, 8 * sizeof(double)));
+        cudaStream_t s = mesh->stream;
+        if (nc) MHD_CUDA(cudaMemsetAsync(st->U0.p, 0, 5 * nc * st->nsp * sizeof(double), s));
+        if (nf)
+        {
+            MHD_CUDA(cudaMemsetAsync(st->phi0.p, 0, nf * sizeof(double), s));
+            MHD_CUDA(cudaMemsetAsync(st->phi_add.p, 0, nf * sizeof(double), s));
+        }
+        if (nc) MHD_CUDA(cudaMemsetAsync(st->badd.p, 0, 3 * nc * sizeof(double), s));
+        MHD_CUDA(cudaMemsetAsync(st->flag.p, 0, sizeof(int), s));
+        MHD_CUDA(cudaStreamSynchronize(s));
+        *out = st;
+    });
+    if (rc != MHD_OK) delete st;
+    return rc;
+}
+
+int mhd_gpu_state_destroy(MhdState *st)
+{
+    return guarded([&] {
+        if (!st) return;
+        cudaStreamSynchronize(st->mesh->stream);
+        delete st;
+    });
+}
+
+int mhd_gpu_state_upload(MhdState *st, int32_t field, int32_t species, const double *host)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st && host, "null argument");
+        const MeshView &m = st->mesh->v;
+        cudaStream_t s = st->mesh->stream;
+        if (field == MHD_FIELD_U)
+        {
+            MHD_REQUIRE(species >= 0 && species < st->nsp, "species out of range");
+            if (!m.nc) return;
+            MHD_CUDA(cudaMemcpyAsync(st->stage.p, host, 5 * (size_t)m.nc * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_aos_to_soa<<<grid_for(5 * (int64_t)m.nc, 256), 256, 0, s>>>(st->stage.p, st->U0.p + (size_t)species * 5 * m.nc, m.nc, 5);
+            MHD_LAUNCH_CHECK();
+        }
+        else if (field == MHD_FIELD_PHI)
+            MHD_CUDA(cudaMemcpyAsync(st->phi0.p, host, (size_t)m.nf * sizeof(double), cudaMemcpyHostToDevice, s));
+        else if (field == MHD_FIELD_PHIADD)
+        {
+            MHD_CUDA(cudaMemcpyAsync(st->phi_add.p, host, (size_t)m.nf * sizeof(double), cudaMemcpyHostToDevice, s));
+            // BaddCell = reconstruct_cell_vector(PhiAdd) (MercuryUns/initial/Initial.cpp:82-83)
+            if (m.nc) k_cell_vector_all<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->phi_add.p, st->badd.p);
+            MHD_LAUNCH_CHECK();
+        }
+        else
+            MHD_REQUIRE(false, "unknown field");
+        MHD_CUDA(cudaStreamSynchronize(s)); // the host buffer may be reused on return
+    });
+}
+
+int mhd_gpu_state_download(MhdState *st, int32_t field, int32_t species, double *host)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st && host, "null argument");
+        const MeshView &m = st->mesh->v;
+        cudaStream_t s = st->mesh->stream;
+        if (field == MHD_FIELD_U)
+        {
+            MHD_REQUIRE(species >= 0 && species < st->nsp, "species out of range");
+            if (!m.nc) return;
+            k_soa_to_aos<<<grid_for(5 * (int64_t)m.nc, 256), 256, 0, s>>>(st->U0.p + (size_t)species * 5 * m.nc, st->stage.p, m.nc, 5);
+            MHD_LAUNCH_CHECK();
+            MHD_CUDA(cudaMemcpyAsync(host, st->stage.p, 5 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        else if (field == MHD_FIELD_PHI)
+            MHD_CUDA(cudaMemcpyAsync(host, st->phi0.p, (size_t)m.nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        else if (field == MHD_FIELD_PHIADD)
+            MHD_CUDA(cudaMemcpyAsync(host, st->phi_add.p, (size_t)m.nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        else if (field == MHD_FIELD_BADD)
+            MHD_CUDA(cudaMemcpyAsync(host, st->badd.p, 3 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+        else
+            MHD_REQUIRE(false, "unknown field");
+        MHD_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mhd_gpu_state_device_ptr(MhdState *st, int32_t field, double **out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st && out, "null argument");
+        if (field == MHD_FIELD_U) *out = st->U0.p;
+        else if (field == MHD_FIELD_PHI) *out = st->phi0.p;
+        else if (field == MHD_FIELD_PHIADD) *out = st->phi_add.p;
+        else if (field == MHD_FIELD_BADD) *out = st->badd.p;
+        else MHD_REQUIRE(false, "unknown field");
+    });
+}
+
+int mhd_gpu_cfl_dt(MhdState *st, double dt_max, double *host_dt)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st && host_dt, "null argument");
+        MhdMesh *mesh = st->mesh;
+        const MeshView &m = mesh->v;
+        cudaStream_t s = mesh->stream;
+        const int64_t nc = m.nc;
+        if (nc)
+            k_prepare<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->fp, st->mass.p, st->prm.M_ref, soa_cstate(st->U0.p, nc),
+                                                          soa_state(st->W.p, nc), st->phi0.p, st->badd.p, st->bind.p, st->btot.p,
+                                                          st->up.p);
+        k_cfl_init<<<1, 1, 0, s>>>(st->dt_bits.p, st->flag.p);
+        if (m.no_cells)
+            k_cfl_cells<<<grid_for(m.no_cells, 128), 128, 0, s>>>(m, st->fp, st->prm.cfl, st->prm.inver_MA2, st->prm.rho_floor_dt,
+                                                                   soa_cstate(st->W.p, nc), st->btot.p, st->dt_bits.p, st->flag.p);
+        k_cfl_final<<<1, 1, 0, s>>>(st->dt_bits.p, dt_max, st->scal.p, st->flag.p);
+        MHD_LAUNCH_CHECK();
+        read_dt(st, host_dt);
+    });
+}
+
+int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_used)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st, "null state");
+        MHD_REQUIRE(dt_fixed > 0 || dt_max > 0, "need dt_fixed > 0 or dt_max > 0");
+        cudaStream_t s = st->mesh->stream;
+        const bool cfl = !(dt_fixed > 0);
+        if (!cfl)
+        {
+            k_set_dt<<<1, 1, 0, s>>>(st->scal.p, dt_fixed, st->flag.p);
+            MHD_LAUNCH_CHECK();
+            ++st->launches;
+        }
+        stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl, dt_max);
+        stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
+        if (dt_used) read_dt(st, dt_used);
+    });
+}
+
+int mhd_gpu_state_profile(MhdState *st, int32_t enable)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st, "null state");
+        MHD_CUDA(cudaStreamSynchronize(st->mesh->stream));
+        st->prof.on = enable != 0;
+        for (auto &u : st->prof.used) u = 0;
+    });
+}
+
+int mhd_gpu_state_profile_read(MhdState *st, int32_t max_kernels, char *names, double *ms_total, int64_t *count, int32_t *n_out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st && names && ms_total && count && n_out, "null argument");
+        MHD_CUDA(cudaStreamSynchronize(st->mesh->stream));
+        int n = 0;
+        for (int k = 0; k < KP_COUNT && n < max_kernels; ++k, ++n)
+        {
+            std::strncpy(names + 32 * n, kStepKernelNames[k], 31);
+            names[32 * n + 31] = 0;
+            double tot = 0;
+            for (size_t i = 0; i < st->prof.used[k]; ++i)
+            {
+                float ms = 0;
+                MHD_CUDA(cudaEventElapsedTime(&ms, st->prof.ev[k][i].first, st->prof.ev[k][i].second));
+                tot += ms;
+            }
+            ms_total[n] = tot;
+            count[n] = static_cast<int64_t>(st->prof.used[k]);
+            st->prof.used[k] = 0;
+        }
+        *n_out = n;
+    });
+}
+
+int mhd_gpu_state_launches(MhdState *st, int64_t *out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st && out, "null argument");
+        *out = st->launches;
+    });
+}
+
+} // extern "C"

@@ -41,8 +41,28 @@ class Prim(ctypes.Structure):
     _fields_ = [("rho", dbl), ("u", dbl), ("v", dbl), ("w", dbl), ("p", dbl)]
 
 
+class StepParams(ctypes.Structure):
+    """MhdStepParams of include/mhd_gpu.h (the Config / Scales fields the explicit step reads)."""
+    _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
+                ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("cfl", dbl), ("inver_MA2", dbl),
+                ("rho_floor_dt", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", Prim * 16),
+                ("absorb", ctypes.c_int8 * 16)]
+
+
+FIELD_U, FIELD_PHI, FIELD_PHIADD, FIELD_BADD = 0, 1, 2, 3
+
 _SIGS = {
     "mhd_gpu_last_error": ([], ctypes.c_char_p),
+    "mhd_gpu_state_create": ([vp, ctypes.POINTER(StepParams), ctypes.POINTER(vp)], ctypes.c_int),
+    "mhd_gpu_state_destroy": ([vp], ctypes.c_int),
+    "mhd_gpu_state_upload": ([vp, i32, i32, vp], ctypes.c_int),
+    "mhd_gpu_state_download": ([vp, i32, i32, vp], ctypes.c_int),
+    "mhd_gpu_state_device_ptr": ([vp, i32, ctypes.POINTER(vp)], ctypes.c_int),
+    "mhd_gpu_cfl_dt": ([vp, dbl, ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_step_rk2": ([vp, dbl, dbl, ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_state_profile": ([vp, i32], ctypes.c_int),
+    "mhd_gpu_state_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
+    "mhd_gpu_state_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
     "mhd_gpu_device_info": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
     "mhd_gpu_mesh_create": ([ctypes.POINTER(MeshDesc), ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_mesh_destroy": ([vp], ctypes.c_int),
@@ -279,3 +299,103 @@ class DeviceMesh:
         check(lib().mhd_gpu_cell_current(self._h, ptr(B), ptr(J)))
         self._leave()
         return J
+
+
+def step_params(n_species, gamma=5.0 / 3.0, fs=None, mass=None, u_inf=(0.0, 0.0, 0.0), B_imf=(0.0, 0.0, 0.0), cuct=0.5,
+                second_order=True, rho_floor=1e-10, p_floor=1e-12, rel_limit=0.0, cfl=0.4, inver_MA2=1.0, rho_floor_dt=1e-2,
+                M_ref=1.0, ne_floor=0.01, absorb=None):
+    """MhdStepParams with the reference's Config / Scales defaults (Common/config/Config.h:19-96)."""
+    p = StepParams()
+    p.n_species, p.second_order = int(n_species), int(bool(second_order))
+    p.gamma, p.rho_floor, p.p_floor, p.cuct = gamma, rho_floor, p_floor, cuct
+    p.M_ref, p.ne_floor, p.rel_limit = M_ref, ne_floor, rel_limit
+    p.cfl, p.inver_MA2, p.rho_floor_dt = cfl, inver_MA2, rho_floor_dt
+    p.u_inf[:] = [float(v) for v in u_inf]
+    p.B_imf[:] = [float(v) for v in B_imf]
+    mass = mass or [1.0] * n_species
+    fs = fs or [(1.0, 0.0, 0.0, 0.0, 1.0)] * n_species
+    for s in range(n_species):
+        p.mass[s] = float(mass[s])
+        p.fs[s] = Prim(*[float(v) for v in fs[s]])
+        # reference ghost_state: species 1 is absorbed at walls (Common/fluid/Reconstruction.cpp:15)
+        p.absorb[s] = int(s == 1) if absorb is None else int(bool(absorb[s]))
+    return p
+
+
+class ResidentState:
+    """Device-resident state of the fused explicit step (MhdState of include/mhd_gpu.h)."""
+
+    def __init__(self, dmesh: DeviceMesh, params: StepParams):
+        self.mesh = dmesh
+        self.params = params
+        self.n_species = params.n_species
+        h = vp()
+        check(lib().mhd_gpu_state_create(dmesh.handle, ctypes.byref(params), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mhd_gpu_state_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def upload(self, field, data, species=0):
+        a = np.ascontiguousarray(data, np.float64)
+        check(lib().mhd_gpu_state_upload(self._h, field, species, a.ctypes.data_as(vp)))
+
+    def download(self, field, species=0):
+        n = {FIELD_U: 5 * self.mesh.n_cells, FIELD_PHI: self.mesh.n_faces, FIELD_PHIADD: self.mesh.n_faces,
+             FIELD_BADD: 3 * self.mesh.n_cells}[field]
+        a = np.empty(n)
+        check(lib().mhd_gpu_state_download(self._h, field, species, a.ctypes.data_as(vp)))
+        return a
+
+    def set(self, U_list, Phi, PhiAdd=None):
+        for s, U in enumerate(U_list):
+            self.upload(FIELD_U, U, s)
+        self.upload(FIELD_PHI, Phi)
+        if PhiAdd is not None:
+            self.upload(FIELD_PHIADD, PhiAdd)
+
+    def U(self, species):
+        return self.download(FIELD_U, species)
+
+    def Phi(self):
+        return self.download(FIELD_PHI)
+
+    def device_ptr(self, field):
+        p = vp()
+        check(lib().mhd_gpu_state_device_ptr(self._h, field, ctypes.byref(p)))
+        return p.value
+
+    def cfl_dt(self, dt_max=1e300):
+        d = dbl()
+        check(lib().mhd_gpu_cfl_dt(self._h, float(dt_max), ctypes.byref(d)))
+        return d.value
+
+    def step(self, dt=0.0, dt_max=1e300, sync=True):
+        """One SSP-RK2 step (Solver::step of the hot path); returns the dt used when sync."""
+        d = dbl()
+        check(lib().mhd_gpu_step_rk2(self._h, float(dt), float(dt_max), ctypes.byref(d) if sync else None))
+        return d.value if sync else None
+
+    def profile(self, enable=True):
+        check(lib().mhd_gpu_state_profile(self._h, int(bool(enable))))
+
+    def profile_read(self):
+        """{kernel class: (summed ms, launches)} since the last read (synchronises)."""
+        names = ctypes.create_string_buffer(32 * 16)
+        ms = np.zeros(16)
+        cnt = np.zeros(16, np.int64)
+        n = i32()
+        check(lib().mhd_gpu_state_profile_read(self._h, 16, names, ms.ctypes.data_as(vp), cnt.ctypes.data_as(vp), ctypes.byref(n)))
+        raw = names.raw
+        return {raw[32 * k:32 * k + 32].split(b"\0")[0].decode(): (float(ms[k]), int(cnt[k])) for k in range(n.value)}
+
+    def launches(self):
+        v = i64()
+        check(lib().mhd_gpu_state_launches(self._h, ctypes.byref(v)))
+        return v.value

@@ -166,6 +166,24 @@ class HostMesh:
         self._cache[name] = a
         return a
 
+    def cell_loops_flat(self):
+        """Builder input of this complex as flat arrays (cell_ptr, loop_ptr, loop_nodes): per cell its
+        face loops oriented outward, in c2f order."""
+        e2n = np.asarray(self["e2n_idx"]).reshape(-1, 2)
+        f2e_ptr, f2e_idx, f2e_sgn = (np.asarray(self[k]) for k in ("f2e_ptr", "f2e_idx", "f2e_sgn"))
+        c2f_ptr, c2f_idx, c2f_sgn = (np.asarray(self[k]) for k in ("c2f_ptr", "c2f_idx", "c2f_sgn"))
+        # node at which each f2e entry enters its edge: start if traversed forward, else end
+        enter = np.where(f2e_sgn > 0, e2n[f2e_idx, 0], e2n[f2e_idx, 1]).astype(np.int32)
+        lens = (f2e_ptr[c2f_idx + 1] - f2e_ptr[c2f_idx]).astype(np.int64)
+        loop_ptr = np.zeros(len(c2f_idx) + 1, np.int64)
+        np.cumsum(lens, out=loop_ptr[1:])
+        pos = np.arange(loop_ptr[-1], dtype=np.int64) - np.repeat(loop_ptr[:-1], lens)   # position inside the loop
+        start = np.repeat(f2e_ptr[c2f_idx], lens)
+        L = np.repeat(lens, lens)
+        rev = np.repeat(c2f_sgn < 0, lens)
+        src = np.where(rev, start + (L - 1 - pos), start + pos)
+        return np.asarray(c2f_ptr, np.int64), loop_ptr, enter[src]
+
     def outward_loops(self):
         """Per cell, its face loops oriented outward (c2f order): the builder input that reproduces this complex."""
         e2n_idx = self["e2n_idx"].reshape(-1, 2)

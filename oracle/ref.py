@@ -151,6 +151,27 @@ class RefMesh:
                                              len(tid), _p(tptr), _p(tnodes), _p(tid), len(tag_names),
                                              ctypes.cast(names, ctypes.c_void_p)))
 
+    @classmethod
+    def from_flat(cls, x, cell_ptr, loop_ptr, loop_nodes, material, tagged=(), tag_names=("",)):
+        """Generic polyhedra from flat builder arrays (see HostMesh.cell_loops_flat)."""
+        x = np.ascontiguousarray(x, np.float64).reshape(-1, 3)
+        cell_ptr = np.ascontiguousarray(cell_ptr, np.int64)
+        loop_ptr = np.ascontiguousarray(loop_ptr, np.int64)
+        loop_nodes = np.ascontiguousarray(loop_nodes, np.int32)
+        mat = np.ascontiguousarray(material, np.int32)
+        tptr, tnodes, tid = [0], [], []
+        for t_nodes, t in tagged:
+            tnodes.extend(int(v) for v in t_nodes)
+            tptr.append(len(tnodes))
+            tid.append(int(t))
+        tptr = np.asarray(tptr, np.int64)
+        tnodes = np.asarray(tnodes, np.int32)
+        tid = np.asarray(tid, np.int32)
+        names = (ctypes.c_char_p * len(tag_names))(*[n.encode() for n in tag_names])
+        return cls(lib().ref_mesh_from_cells(len(x), _p(x), len(cell_ptr) - 1, _p(cell_ptr), _p(loop_ptr), _p(loop_nodes),
+                                             _p(mat), len(tid), _p(tptr), _p(tnodes), _p(tid), len(tag_names),
+                                             ctypes.cast(names, ctypes.c_void_p)))
+
     def topology_hash(self):
         return int(lib().ref_topology_hash(self._h))
 

@@ -29,8 +29,8 @@ def tagged_faces(m: HostMesh):
 def ref_twin(m: HostMesh, tag_names):
     """The same complex built by the reference's ComplexBuilder from this mesh's cells."""
     from oracle.ref import RefMesh
-    return RefMesh.from_cells(np.asarray(m["x"]), m.outward_loops(), np.asarray(m["cell_material"]), tagged_faces(m),
-                              tag_names)
+    cp, lp, ln = m.cell_loops_flat()
+    return RefMesh.from_flat(np.asarray(m["x"]), cp, lp, ln, np.asarray(m["cell_material"]), tagged_faces(m), tag_names)
 
 
 def host_from_ref(r, tag_names):
