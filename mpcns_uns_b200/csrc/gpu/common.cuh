@@ -134,6 +134,7 @@ struct Prim5
 struct MeshView
 {
     int32_t nn, ne, nf, nc, no_cells, no_edges;
+    int32_t max_valence; // largest number of faces at an edge
     const int32_t *c2f_ptr, *c2f_idx;
     const int8_t *c2f_sgn;
     const int32_t *f2e_ptr, *f2e_idx;

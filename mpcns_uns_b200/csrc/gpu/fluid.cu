@@ -19,18 +19,39 @@ __global__ void k_to_prim(SField<const double> U, SField<double> W, int32_t n, i
     }
 }
 
-// mhd::Stencil::limited_gradients (Common/fluid/Reconstruction.cpp:80-142), one thread per cell,
-// all species of the launch: least-squares gradient of the 5 primitives from the precomputed
-// w*d and the symmetric inverse, Barth-Jespersen psi over all faces of the cell, optional relative
-// limiter on rho and p, clamp to [0, 1].  Cells without a valid stencil get zero.
-__global__ void __launch_bounds__(128) k_limited_gradients(MeshView m, FluidParams p, SField<const double> W, SField<double> G)
+// One component of mhd::ghost_state (Common/fluid/Reconstruction.cpp:9-24); (cu, cv, cw) the velocity
+// of the inside state, wc its component q.
+__device__ __forceinline__ double ghost_component(int kind, bool absorb, int q, double wc, double cu, double cv, double cw, V3 n,
+                                                  const Prim5 &fs)
 {
-    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kind == 1)
+    {
+        if (absorb) return (q == 0 || q == 4) ? 1e-12 : 0.0;
+        if (q == 0 || q == 4) return wc;
+        const double un = cu * n.x + cv * n.y + cw * n.z;
+        const double nq = q == 1 ? n.x : (q == 2 ? n.y : n.z);
+        return wc - 2 * un * nq;
+    }
+    if (kind == 2) return q == 0 ? fs.rho : q == 1 ? fs.u : q == 2 ? fs.v : q == 3 ? fs.w : fs.p;
+    return wc;
+}
+
+// mhd::Stencil::limited_gradients (Common/fluid/Reconstruction.cpp:80-142): least-squares gradient
+// from the precomputed w*d and the symmetric inverse, Barth-Jespersen psi over all faces of the cell,
+// optional relative limiter on rho and p, clamp to [0, 1]; zero for cells without a valid stencil.
+// One thread per (cell, primitive variable): blockDim = (32, 5), warp q of a block handles variable
+// q of 32 consecutive cells.  Each variable's fit and limiter are independent of the others (wall
+// ghosts only read the velocity), so the per-thread state is small, occupancy high, and the five
+// warps share the cell's geometry through L1.  The reference's arithmetic order is kept per variable.
+__global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidParams p, SField<const double> W, SField<double> G)
+{
+    const int32_t c = blockIdx.x * 32 + threadIdx.x;
+    const int q = threadIdx.y;
     if (c >= m.nc) return;
     if (c >= m.no_cells || !m.st_valid[c])
     {
         for (int s = 0; s < p.nsp; ++s)
-            for (int q = 0; q < 15; ++q) G(s, c, q) = 0.0;
+            for (int a = 0; a < 3; ++a) G(s, c, 3 * q + a) = 0.0;
         return;
     }
     const int32_t k0 = m.c2f_ptr[c], k1 = m.c2f_ptr[c + 1];
@@ -39,79 +60,55 @@ __global__ void __launch_bounds__(128) k_limited_gradients(MeshView m, FluidPara
     const double I00 = Ip[0], I01 = Ip[1], I02 = Ip[2], I11 = Ip[3], I12 = Ip[4], I22 = Ip[5];
     for (int s = 0; s < p.nsp; ++s)
     {
-        double wc[5], lo[5], hi[5], g[5][3];
-        for (int q = 0; q < 5; ++q)
-        {
-            wc[q] = W(s, c, q);
-            lo[q] = hi[q] = wc[q];
-            g[q][0] = g[q][1] = g[q][2] = 0.0;
-        }
-        const Prim5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
+        const double wc = W(s, c, q);
+        double lo = wc, hi = wc, r0 = 0, r1 = 0, r2 = 0;
         for (int32_t k = k0; k < k1; ++k)
         {
             const int32_t nb = m.st_nb[k];
             if (nb == INT32_MIN) continue;
-            double wn[5];
-            if (nb >= 0)
-            {
-                for (int q = 0; q < 5; ++q) wn[q] = W(s, nb, q);
-            }
+            double wn;
+            if (nb >= 0) wn = W(s, nb, q);
             else
             {
                 const int32_t f = -(nb + 1);
+                const int kind = m.face_kind[f];
                 const V3 n = (double(m.c2f_sgn[k]) / m.face_area_mag[f]) * ld3(m.face_area, f);
-                prim_arr(ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, n, p.fs[s]), wn);
+                const bool vel = kind == 1 && !p.absorb[s] && q >= 1 && q <= 3;
+                wn = ghost_component(kind, p.absorb[s] != 0, q, wc, vel ? W(s, c, 1) : 0.0, vel ? W(s, c, 2) : 0.0,
+                                     vel ? W(s, c, 3) : 0.0, n, p.fs[s]);
             }
-            const double wx = m.st_wd[3 * (int64_t)k], wy = m.st_wd[3 * (int64_t)k + 1], wz = m.st_wd[3 * (int64_t)k + 2];
-            for (int q = 0; q < 5; ++q)
-            {
-                const double dq = wn[q] - wc[q];
-                g[q][0] += wx * dq;
-                g[q][1] += wy * dq;
-                g[q][2] += wz * dq;
-                lo[q] = dmin(lo[q], wn[q]);
-                hi[q] = dmax(hi[q], wn[q]);
-            }
+            const double dq = wn - wc;
+            r0 += m.st_wd[3 * (int64_t)k] * dq;
+            r1 += m.st_wd[3 * (int64_t)k + 1] * dq;
+            r2 += m.st_wd[3 * (int64_t)k + 2] * dq;
+            lo = dmin(lo, wn);
+            hi = dmax(hi, wn);
         }
-        double psi[5];
-        for (int q = 0; q < 5; ++q)
-        {
-            const double r0 = g[q][0], r1 = g[q][1], r2 = g[q][2];
-            g[q][0] = I00 * r0 + I01 * r1 + I02 * r2;
-            g[q][1] = I01 * r0 + I11 * r1 + I12 * r2;
-            g[q][2] = I02 * r0 + I12 * r1 + I22 * r2;
-            psi[q] = 1.0;
-        }
+        const double g0 = I00 * r0 + I01 * r1 + I02 * r2;
+        const double g1 = I01 * r0 + I11 * r1 + I12 * r2;
+        const double g2 = I02 * r0 + I12 * r1 + I22 * r2;
+        double psi = 1.0;
         if (p.limit)
         {
             for (int32_t k = k0; k < k1; ++k)
             {
                 const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
-                for (int q = 0; q < 5; ++q)
-                {
-                    const double dl = g[q][0] * dx.x + g[q][1] * dx.y + g[q][2] * dx.z;
-                    if (dl > 1e-300) psi[q] = dmin(psi[q], (hi[q] - wc[q]) / dl);
-                    else if (dl < -1e-300) psi[q] = dmin(psi[q], (lo[q] - wc[q]) / dl);
-                }
+                const double dl = g0 * dx.x + g1 * dx.y + g2 * dx.z;
+                if (dl > 1e-300) psi = dmin(psi, (hi - wc) / dl);
+                else if (dl < -1e-300) psi = dmin(psi, (lo - wc) / dl);
             }
-            if (p.rel_limit > 0)
+            if (p.rel_limit > 0 && (q == 0 || q == 4))
                 for (int32_t k = k0; k < k1; ++k)
                 {
                     const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
-                    for (int q = 0; q < 5; q += 4)
-                    {
-                        const double dl = fabs(g[q][0] * dx.x + g[q][1] * dx.y + g[q][2] * dx.z);
-                        if (dl > 1e-300) psi[q] = dmin(psi[q], p.rel_limit * wc[q] / dl);
-                    }
+                    const double dl = fabs(g0 * dx.x + g1 * dx.y + g2 * dx.z);
+                    if (dl > 1e-300) psi = dmin(psi, p.rel_limit * wc / dl);
                 }
         }
-        for (int q = 0; q < 5; ++q)
-        {
-            const double ps = dmax(0.0, dmin(1.0, psi[q]));
-            G(s, c, 3 * q) = ps * g[q][0];
-            G(s, c, 3 * q + 1) = ps * g[q][1];
-            G(s, c, 3 * q + 2) = ps * g[q][2];
-        }
+        const double ps = dmax(0.0, dmin(1.0, psi));
+        G(s, c, 3 * q) = ps * g0;
+        G(s, c, 3 * q + 1) = ps * g1;
+        G(s, c, 3 * q + 2) = ps * g2;
     }
 }
 
@@ -121,8 +118,10 @@ __global__ void __launch_bounds__(128) k_limited_gradients(MeshView m, FluidPara
 __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SField<const double> W, SField<const double> G,
                                                    double *__restrict__ F)
 {
+    // one species per grid row (blockIdx.y)
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= m.nf) return;
+    const int s = blockIdx.y;
+    if (f >= m.nf || s >= p.nsp) return;
     const int64_t nf = m.nf;
     const int kind = m.face_kind[f];
     const int32_t p0 = m.f2c_ptr[f], cnt = m.f2c_ptr[f + 1] - p0;
@@ -134,8 +133,7 @@ __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SF
     }
     if (kind == 4 || !any_owned)
     {
-        for (int s = 0; s < p.nsp; ++s)
-            for (int q = 0; q < 5; ++q) F[(s * 5 + q) * nf + f] = 0.0;
+        for (int q = 0; q < 5; ++q) F[(s * 5 + q) * nf + f] = 0.0;
         return;
     }
     const double A = m.face_area_mag[f];
@@ -159,7 +157,6 @@ __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SF
             sgn = m.f2c_sgn[p0 + 1];
         }
     }
-    for (int s = 0; s < p.nsp; ++s)
     {
         Prim5 L, R;
         double g[15];
@@ -222,14 +219,14 @@ __global__ void k_gather_rhs(MeshView m, int nsp, const double *__restrict__ F, 
 void launch_limited_gradients(const MeshView &m, const FluidParams &p, SField<const double> W, SField<double> G, cudaStream_t s)
 {
     if (!m.nc) return;
-    k_limited_gradients<<<grid_for(m.nc, 128), 128, 0, s>>>(m, p, W, G);
+    k_limited_gradients_v<<<grid_for(m.nc, 32), dim3(32, 5), 0, s>>>(m, p, W, G);
     MHD_LAUNCH_CHECK();
 }
 
 void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const double> W, SField<const double> G, double *F, cudaStream_t s)
 {
     if (!m.nf) return;
-    k_face_flux<<<grid_for(m.nf, 128), 128, 0, s>>>(m, p, W, G, F);
+    k_face_flux<<<dim3(grid_for(m.nf, 128), p.nsp), 128, 0, s>>>(m, p, W, G, F);
     MHD_LAUNCH_CHECK();
 }
 
@@ -270,9 +267,7 @@ int mhd_gpu_limited_gradients(MhdMesh *mesh, const double *W, int32_t species, c
         const MeshView &m = mesh->v;
         if (!m.nc) return;
         const FluidParams p = single_species(species, fs, 0.0, limit, rel_limit);
-        k_limited_gradients<<<grid_for(m.nc, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
-                                                                           SField<double>{grad, 0, 15, 1});
-        MHD_LAUNCH_CHECK();
+        launch_limited_gradients(m, p, SField<const double>{W, 0, 5, 1}, SField<double>{grad, 0, 15, 1}, mesh->stream);
     });
 }
 

@@ -49,6 +49,9 @@ __global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const
 // edge: central part sum_f w_ef E_f . t, transverse upwind part with the weights omega corrected
 // by the 2x2 solve in the plane normal to the edge.
 // Returns false for the edges the reference skips (no faces, zero length, no fluid cell).
+// MAXV bounds the faces per edge: the per-face values live in registers when the loops over
+// [0, MAXV) unroll (MAXV = 8 covers every tetrahedral split mesh), in local memory for MAXV = 32.
+template <int MAXV>
 __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const double *__restrict__ Ef, const double *__restrict__ u,
                                          const double *__restrict__ phi_ind, double cuct, double &out)
 {
@@ -67,10 +70,12 @@ __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const dou
     V3 e1 = cross(th, ax);
     e1 = (1.0 / sqrt(dot(e1, e1))) * e1;
     const V3 e2 = cross(th, e1);
-    double w[kMaxValence], aef[kMaxValence], sg[kMaxValence], qa[kMaxValence], qb[kMaxValence];
+    double w[MAXV], aef[MAXV], sg[MAXV], qa[MAXV], qb[MAXV];
     double Ec = 0, M11 = 0, M12 = 0, M22 = 0, g1 = 0, g2 = 0;
-    for (int i = 0; i < nf; ++i)
+#pragma unroll
+    for (int i = 0; i < MAXV; ++i)
     {
+        if (i >= nf) break;
         const int32_t f = m.e2f_idx[f0 + i];
         w[i] = m.ef_weight[f0 + i];
         Ec += w[i] * dot(ld3(Ef, f), t);
@@ -102,8 +107,10 @@ __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const dou
         l2 = ((M11 + eps) * g2 - M12 * g1) / det;
     }
     double Eu = 0;
-    for (int i = 0; i < nf; ++i)
+#pragma unroll
+    for (int i = 0; i < MAXV; ++i)
     {
+        if (i >= nf) break;
         const int32_t f = m.e2f_idx[f0 + i];
         const double omega = w[i] * (1.0 - (qa[i] * l1 + qb[i] * l2));
         Eu += omega * aef[i] * sg[i] * (phi_ind[f] / m.face_area_mag[f]);
@@ -112,16 +119,19 @@ __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const dou
     return true;
 }
 
+template <int MAXV>
 __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                    const double *__restrict__ phi_ind, double cuct, double *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.no_edges) return;
     double v;
-    if (edge_uct(m, e, Ef, u, phi_ind, cuct, v)) E[e] += v;
+    if (edge_uct<MAXV>(m, e, Ef, u, phi_ind, cuct, v)) E[e] += v;
 }
 
-// EdgeEMF::begin (zero) + add_ideal_emf + the boundary edge values of Solver::rhs (Solver.cpp:150-167)
+// EdgeEMF::begin (zero) + add_ideal_emf + the boundary edge values of Solver::rhs (Solver.cpp:150-167).
+// Wall and inflow edges are overwritten by the reference, so their UCT value is not evaluated.
+template <int MAXV>
 __global__ void __launch_bounds__(128) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                           const double *__restrict__ phi_ind, double cuct, V3 E_inf,
                                                           double *__restrict__ E)
@@ -131,11 +141,14 @@ __global__ void __launch_bounds__(128) k_edge_emf_assign(MeshView m, const doubl
     double val = 0.0;
     if (e < m.no_edges)
     {
-        double v;
-        if (edge_uct(m, e, Ef, u, phi_ind, cuct, v)) val += v;
         const int mode = m.edge_mode[e];
         if (mode == 1) val = 0.0;
         else if (mode == 2) val = dot(E_inf, ld3(m.edge_vec, e));
+        else
+        {
+            double v;
+            if (edge_uct<MAXV>(m, e, Ef, u, phi_ind, cuct, v)) val += v;
+        }
     }
     E[e] = val;
 }
@@ -152,7 +165,8 @@ void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u
                             double *E, cudaStream_t s)
 {
     if (!m.ne) return;
-    k_edge_emf_assign<<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, E);
+    if (m.max_valence <= 8) k_edge_emf_assign<8><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, E);
+    else k_edge_emf_assign<kMaxValence><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, E);
     MHD_LAUNCH_CHECK();
 }
 
@@ -322,7 +336,10 @@ int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const do
         MHD_LAUNCH_CHECK();
         if (m.no_edges)
         {
-            k_edge_uct<<<grid_for(m.no_edges, 128), 128, 0, mesh->stream>>>(m, mesh->scratch_face3.p, u, phi_ind, cuct, E);
+            if (m.max_valence <= 8)
+                k_edge_uct<8><<<grid_for(m.no_edges, 128), 128, 0, mesh->stream>>>(m, mesh->scratch_face3.p, u, phi_ind, cuct, E);
+            else
+                k_edge_uct<kMaxValence><<<grid_for(m.no_edges, 128), 128, 0, mesh->stream>>>(m, mesh->scratch_face3.p, u, phi_ind, cuct, E);
             MHD_LAUNCH_CHECK();
         }
     });

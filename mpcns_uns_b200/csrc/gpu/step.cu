@@ -41,43 +41,60 @@ __global__ void __launch_bounds__(128) k_prepare(MeshView m, FluidParams p, cons
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
-    double rho[kMaxSpecies];
+    // charge-weighted ion velocity: mhd::Scales::numinfo (Common/physics/Scales.cpp:50-62) generalised to n
+    // species; the number densities are recomputed from the primitives this thread has just written
+    double ne = 0;
     for (int s = 0; s < p.nsp; ++s)
     {
         const Prim5 w = to_prim(U(s, c, 0), U(s, c, 1), U(s, c, 2), U(s, c, 3), U(s, c, 4), p.gamma, p.rho_floor, p.p_floor);
         W(s, c, 0) = w.rho; W(s, c, 1) = w.u; W(s, c, 2) = w.v; W(s, c, 3) = w.w; W(s, c, 4) = w.p;
-        rho[s] = w.rho;
+        ne += dmax(w.rho, 0.0) / mass[s] * M_ref;
     }
     const V3 b = cell_vector(m, phi, c);
     st3(Bind, c, b);
     st3(Btot, c, mk(b.x + Badd[3 * (int64_t)c], b.y + Badd[3 * (int64_t)c + 1], b.z + Badd[3 * (int64_t)c + 2]));
-    // charge-weighted ion velocity: mhd::Scales::numinfo (Common/physics/Scales.cpp:50-62) generalised to n species
     double u[3] = {0, 0, 0};
     if (m.material[c] == 0)
-    {
-        double n[kMaxSpecies], ne = 0;
         for (int s = 0; s < p.nsp; ++s)
         {
-            n[s] = dmax(rho[s], 0.0) / mass[s] * M_ref;
-            ne += n[s];
-        }
-        for (int s = 0; s < p.nsp; ++s)
-        {
-            const double chi = ne > 1e-300 ? n[s] / ne : (s == 0 ? 1.0 : 0.0);
+            const double ns = dmax(W(s, c, 0), 0.0) / mass[s] * M_ref;
+            const double chi = ne > 1e-300 ? ns / ne : (s == 0 ? 1.0 : 0.0);
             for (int a = 0; a < 3; ++a) u[a] += chi * W(s, c, 1 + a);
         }
-    }
     st3(up, c, mk(u[0], u[1], u[2]));
 }
 
+__device__ __forceinline__ double cell_dt(const MeshView &m, const FluidParams &p, double cfl, double inver_MA2, double rho_floor_dt,
+                                          const SField<const double> &W, const double *__restrict__ Btot, int32_t c);
+
 // mercury::cell_time_steps (MercuryUns/fluid/MercurySources.cpp:65-106) without the optional gyration
-// limit, n species (the wave speeds use the summed density, as the reference does for its two ions).
+// limit, n species (the wave speeds use the summed density, as the reference does for its two ions);
+// the device-wide minimum of mercury::local_time_step (:108-116) is reduced per block first.
 __global__ void __launch_bounds__(128) k_cfl_cells(MeshView m, FluidParams p, double cfl, double inver_MA2, double rho_floor_dt,
                                                     SField<const double> W, const double *__restrict__ Btot,
                                                     unsigned long long *__restrict__ dt_bits, int *__restrict__ flag)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.no_cells || m.material[c] != 0) return;
+    double dt = CUDART_INF;
+    if (c < m.no_cells && m.material[c] == 0) dt = cell_dt(m, p, cfl, inver_MA2, rho_floor_dt, W, Btot, c);
+    if (!(dt > 0)) atomicOr(flag, 1); // zero, negative or NaN: the reference's "invalid time step"
+    // block minimum (min is exact, so the order of the reduction does not matter), one atomic per block
+    __shared__ double sh[32];
+    double v = dt > 0 ? dt : CUDART_INF;
+    for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : CUDART_INF;
+        for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v < CUDART_INF) atomicMin(dt_bits, static_cast<unsigned long long>(__double_as_longlong(v)));
+    }
+}
+
+__device__ __forceinline__ double cell_dt(const MeshView &m, const FluidParams &p, double cfl, double inver_MA2, double rho_floor_dt,
+                                          const SField<const double> &W, const double *__restrict__ Btot, int32_t c)
+{
     double dt = CUDART_INF;
     const V3 b = ld3(Btot, c);
     const double B2 = dot(b, b);
@@ -102,8 +119,7 @@ __global__ void __launch_bounds__(128) k_cfl_cells(MeshView m, FluidParams p, do
         }
         if (denom > 0) dt = dmin(dt, cfl * m.cell_volume[c] / denom);
     }
-    if (!(dt > 0)) atomicOr(flag, 1); // zero, negative or NaN: the reference's "invalid time step"
-    else atomicMin(dt_bits, static_cast<unsigned long long>(__double_as_longlong(dt)));
+    return dt;
 }
 
 __global__ void k_cfl_init(unsigned long long *dt_bits, int *flag)
