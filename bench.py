@@ -53,10 +53,24 @@ def mesh_counts(h):
                 e2f=len(h["e2f_idx"]), ec=len(h["ec_cell"]), f2c=len(h["f2c_idx"]))
 
 
-def algorithmic_bytes(k, c, nsp, group, p=8):
+def algorithmic_bytes(k, c, nsp, group, precision="fp64"):
     """Compulsory bytes of one launch of kernel class k: every array the pass needs, counted once
-    (perfect reuse within the pass); FP64 values p bytes, indices 4, signs / flags 1."""
+    (perfect reuse within the pass); values 8 bytes (FP64) or 4 (FP32 bulk of the mixed path; the
+    state U and the face fluxes Phi stay 8), indices 4, signs / flags 1."""
     nc, nf, ne = c["nc"], c["nf"], c["ne"]
+    if precision == "mixed":
+        g, e2f, f2e, ec = group, c["e2f"], c["f2e"], c["ec"]
+        return {
+            "prepare": 40 * nsp * nc + 20 * nsp * nc + 16 * nc + 48 * nc + 8 * nf + 16 * nc + 48 * nc + nc,
+            "cfl": 20 * nsp * nc + 16 * nc + 16 * nc + 16 * nf + 4 * nc + nc,
+            "limited_gradients": 20 * g * nc + 16 * nc + 120 * nc + nc + 60 * g * nc + 4 * nc,
+            "face_flux": 20 * g * nc + 60 * g * nc + 16 * nf + 24 * nf + 8 * nf + 14 * nf + nf + nc + 20 * g * nf,
+            "update": 20 * g * nf + 20 * nc + 40 * g * nc + 60 * g * nc + 4 * nc + nc,
+            "face_candidate": 48 * nc + 16 * nf + 16 * nf + 8 * nf + 12 * nf,
+            "edge_emf": 48 * ne + 4 * ne + 24 * e2f + 4 * ne + 4 * ec + nc + 12 * nf + 16 * nf + 8 * nf + 16 * nc + ne + 4 * ne,
+            "ct": 4 * ne + 20 * nf + 4 * nf + 5 * f2e + 12 * nf,
+        }.get(k, 0.0)
+    p = 8
     csr_c2f = c["c2f"] * 5 + nc * 4          # idx + sgn + ptr
     if k == "prepare":
         return (10 * nsp * nc + nf * 5 + 3 * nc + 9 * nc) * p + csr_c2f + nc
@@ -197,6 +211,7 @@ def main():
     ap.add_argument("--nr", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--accuracy-steps", type=int, default=100)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -236,59 +251,98 @@ def main():
     wl = make_workload(args)
     h = wl.mesh
     dm = gpu.DeviceMesh(h)
-    p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl)
-    st = gpu.ResidentState(dm, p)
-    st.set(wl.U, wl.Phi, wl.PhiAdd)
     stream = dm.stream
-
-    for _ in range(args.warmup):
-        st.step(0.0, sync=True)
-    torch.cuda.synchronize()
-
-    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = st.launches()
-    st.profile(True)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for _ in range(args.steps):
-        st.step(0.0, sync=False)
-    ev1.record(stream)
-    ev1.synchronize()
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    prof = st.profile_read()
-    st.profile(False)
-    launches = st.launches() - l0
-    if dist:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    clocks = sampler.stop() if sampler else None
-    dt_last = st.cfl_dt()
-    if not np.isfinite(dt_last):
-        raise RuntimeError("state became invalid")
-
-    cu_per_step = h.n_cells * wl.n_species * 2
-    value = cu_per_step * args.steps * world / (ms / 1e3)
-
-    # roofline of the dominant kernel (live CUDA-event timing on the handle's stream)
     counts = mesh_counts(h)
-    peak, peak_kind = peaks()
-    kern = max(prof, key=lambda k: prof[k][0])
-    k_ms, k_n = prof[kern]
     group = min(2, wl.n_species)
-    bytes_launch = algorithmic_bytes(kern, counts, wl.n_species, group)
-    achieved = bytes_launch / (k_ms / k_n / 1e3) / 1e9
-    breakdown = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
-                     "GBps": (algorithmic_bytes(k, counts, wl.n_species, group) / (v[0] / v[1] / 1e3) / 1e9) if v[1] else None}
-                 for k, v in prof.items() if v[1]}
+    cu_per_step = h.n_cells * wl.n_species * 2
+
+    def new_state(precision):
+        p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl,
+                            precision=precision)
+        st = gpu.ResidentState(dm, p)
+        st.set(wl.U, wl.Phi, wl.PhiAdd)
+        return st
+
+    def timed(st, precision, sampler=None):
+        """K device-timed steps (CUDA events on the handle's stream) with live per-kernel events."""
+        for _ in range(args.warmup):
+            st.step(0.0, sync=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        l0 = st.launches()
+        st.profile(True)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(args.steps):
+            st.step(0.0, sync=False)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        prof = st.profile_read()
+        st.profile(False)
+        launches = st.launches() - l0
+        if dist:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        if not np.isfinite(st.cfl_dt()):
+            raise RuntimeError("state became invalid")
+        kern = max(prof, key=lambda k: prof[k][0])
+        k_ms, k_n = prof[kern]
+        bl = algorithmic_bytes(kern, counts, wl.n_species, group, precision)
+        breakdown = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
+                         "GBps": algorithmic_bytes(k, counts, wl.n_species, group, precision) / (v[0] / v[1] / 1e3) / 1e9}
+                     for k, v in prof.items() if v[1]}
+        return dict(ms=ms, value=cu_per_step * args.steps * world / (ms / 1e3), launches=launches, kernel=kern,
+                    bytes_launch=bl, achieved=bl / (k_ms / k_n / 1e3) / 1e9, kernels=breakdown)
+
+    st64 = new_state("fp64")
+    r64 = timed(st64, "fp64")
+    st32 = new_state("mixed")
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
+    rmx = timed(st32, "mixed")
+    clocks = sampler.stop() if sampler else None
+
+    # accuracy of the mixed step against the FP64 step (itself bit-identical to the reference)
+    acc = None
+    if args.accuracy_steps > 0:
+        for st in (st64, st32):
+            st.set(wl.U, wl.Phi, wl.PhiAdd)
+            for _ in range(args.accuracy_steps):
+                st.step(0.0, sync=False)
+        err = {}
+        num = den = 0.0
+        U64 = [st64.U(s) for s in range(wl.n_species)]
+        P32, P64 = st32.Phi(), st64.Phi()
+        for s in range(wl.n_species):
+            a, b = st32.U(s), U64[s]
+            err[f"U{s}_rel_l2"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+            num += float(np.sum((a - b) ** 2))
+            den += float(np.sum(b ** 2))
+        err["U_all_rel_l2"] = float(np.sqrt(num / den))
+        # conditioning of the problem itself: the FP64 step from a state perturbed by 1e-7 (relative,
+        # seeded uniform), the size of single-precision input rounding
+        rng = np.random.default_rng(7)
+        st64.set([u * (1 + 1e-7 * rng.uniform(-1, 1, u.size)) for u in wl.U], wl.Phi, wl.PhiAdd)
+        for _ in range(args.accuracy_steps):
+            st64.step(0.0, sync=False)
+        for s in range(wl.n_species):
+            a = st64.U(s)
+            err[f"U{s}_rel_l2_fp64_perturbed_1e-7"] = float(np.linalg.norm(a - U64[s]) / np.linalg.norm(U64[s]))
+        err["Phi_rel_l2"] = float(np.linalg.norm(P32 - P64) / np.linalg.norm(P64 + wl.PhiAdd))
+        # d2 B relative to the total field the update works with (background flux in the normalisation,
+        # as the reference's diagnostics do: MercuryUns/driver/Solver.cpp:577)
+        acc = {"steps": args.accuracy_steps, **err, "div_b_max_rel_mixed": dm.div_b(P32, wl.PhiAdd)["max_rel"],
+               "div_b_max_rel_fp64": dm.div_b(P64, wl.PhiAdd)["max_rel"]}
+    peak, peak_kind = peaks()
 
     # end to end through the C-ABI with host buffers (pinned), copies inside the timed region
+    st = st32
     pin_U = [torch.empty(5 * h.n_cells, dtype=torch.float64).pin_memory() for _ in range(wl.n_species)]
     pin_P = torch.empty(h.n_faces, dtype=torch.float64).pin_memory()
     for s in range(wl.n_species):
@@ -306,8 +360,7 @@ def main():
             pin_U[s].numpy()[:] = st.U(s)
         pin_P.numpy()[:] = st.Phi()
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = float(np.median(e2e_times))
-    e2e_v = cu_per_step * world / e2e_s
+    e2e_v = cu_per_step * world / float(np.median(e2e_times))
     io_bytes = (5 * h.n_cells * wl.n_species + h.n_faces) * 8
 
     cpu = None
@@ -323,18 +376,23 @@ def main():
             log(f"[bench] cpu baseline failed: {e}")
 
     if rank == 0:
-        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-               "dtype": "f64", "data": "synthetic",
+        out = {"metric": METRIC, "value": rmx["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": rmx["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
                "config": {"workload": wl.name, "cells": h.n_cells, "faces": h.n_faces, "edges": h.n_edges,
                           "n_species": wl.n_species, "global_cells": h.n_cells * world,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                          "dt": "CFL 0.4 on device", "l2": "inputs > L2 (no flush needed)", "precision": "fp64 reference-exact"},
-               "gpu_launches": launches,
-               "roofline": {"bound": "hbm", "kernel": kern, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                            "algorithmic_bytes_per_launch": bytes_launch},
-               "kernels": breakdown,
+                          "dt": "CFL 0.4 on device", "l2": "inputs > L2 (no flush needed)",
+                          "precision": "mixed: FP32 reconstruction/limiter/flux/EMF, FP64 state/Phi/CT"},
+               "gpu_launches": rmx["launches"],
+               "roofline": {"bound": "hbm", "kernel": rmx["kernel"], "achieved": rmx["achieved"], "peak": peak, "unit": "GB/s",
+                            "frac": rmx["achieved"] / peak, "peak_kind": peak_kind, "traffic": None,
+                            "algorithmic_bytes_per_launch": rmx["bytes_launch"]},
+               "kernels": rmx["kernels"],
+               "fp64": {"value": r64["value"], "ms_per_step": r64["ms"] / args.steps, "speedup_mixed": rmx["value"] / r64["value"],
+                        "precision": "fp64 reference-exact", "kernels": r64["kernels"],
+                        "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
+               "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                "cpu_baseline": cpu, "clocks": clocks}
         print(json.dumps(out))

@@ -128,7 +128,14 @@ typedef struct MhdStepParams {
     double mass[16];                   /* molar mass per species (Scales::M_H, M_Na, ...) */
     MhdPrim fs[16];                    /* free-stream (inflow ghost) state per species */
     int8_t absorb[16];                 /* wall ghost absorbs the species (reference: species 1) */
+    int32_t precision;                 /* MHD_PREC_FP64 or MHD_PREC_MIXED */
 } MhdStepParams;
+
+/* FP64 reference-exact: every operation rounds as in the reference's host code.
+ * Mixed: reconstruction, limiters, Rusanov fluxes, CFL step and ideal EMF in FP32; the state U,
+ * the face fluxes Phi, the CT update and div B in FP64 (tetrahedral meshes). */
+#define MHD_PREC_FP64 0
+#define MHD_PREC_MIXED 1
 
 #define MHD_FIELD_U 0      /* conservative state of one species, 5 per cell */
 #define MHD_FIELD_PHI 1    /* induced face flux */

@@ -135,6 +135,13 @@ struct MeshView
 {
     int32_t nn, ne, nf, nc, no_cells, no_edges;
     int32_t max_valence; // largest number of faces at an edge
+    int32_t faces_per_cell; // 4 when every cell is a tetrahedron (c2f row k of cell c at 4c), else 0
+    const double *st_dx; // face_center - cell_center per c2f entry (3 each)
+    // tetrahedral meshes only: the stencil as structure of arrays over cells, slot j of cell c at
+    // [j*nc + c] (coalesced warp loads): neighbour code, c2f sign, w*d (3 per slot), dx (3 per slot), inverse (6)
+    const int32_t *t_nb;
+    const int8_t *t_sg;
+    const double *t_wd, *t_dx, *t_inv;
     const int32_t *c2f_ptr, *c2f_idx;
     const int8_t *c2f_sgn;
     const int32_t *f2e_ptr, *f2e_idx;
@@ -173,7 +180,9 @@ struct MhdMesh
         cfa_idx;
     mhd::DBuf<int8_t> c2f_sgn, f2e_sgn, e2f_sgn, f2c_sgn, material, face_kind, edge_mode, st_valid, cfa_sgn;
     mhd::DBuf<double> edge_vec, edge_mid, edge_len, face_area, face_center, face_area_mag, cell_center, cell_volume, ec_weight,
-        ef_weight, star1, star2, st_wd, st_inv;
+        ef_weight, star1, star2, st_wd, st_inv, st_dx, t_wd, t_dx, t_inv;
+    mhd::DBuf<int32_t> t_nb;
+    mhd::DBuf<int8_t> t_sg;
     // scratch reused across calls (stream ordered): face fluxes, face EMF candidates, reductions
     mhd::DBuf<double> scratch_face, scratch_face3, scratch_red;
     mhd::DBuf<double> host_red_dummy;

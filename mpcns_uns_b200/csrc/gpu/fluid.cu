@@ -112,6 +112,94 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
     }
 }
 
+// The same limited gradients on a tetrahedral mesh: one thread per (cell, species = blockIdx.y), the
+// four slots unrolled at compile time so that every stencil load (coalesced structure-of-arrays
+// tables) and the twenty neighbour gathers are in flight together.  Per variable the arithmetic and
+// its order are those of the reference (slots and faces in c2f order).
+__global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, FluidParams p, SField<const double> W, SField<double> G)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = blockIdx.y;
+    if (c >= m.nc || s >= p.nsp) return;
+    const int64_t n = m.nc;
+    if (c >= m.no_cells || !m.st_valid[c])
+    {
+        for (int q = 0; q < 15; ++q) G(s, c, q) = 0.0;
+        return;
+    }
+    int32_t nb[4];
+    double wd[12], dx[12], wc[5], wn[4][5];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) nb[j] = m.t_nb[j * n + c];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) wc[q] = W(s, c, q);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (nb[j] >= 0)
+        {
+#pragma unroll
+            for (int q = 0; q < 5; ++q) wn[j][q] = W(s, nb[j], q);
+        }
+#pragma unroll
+    for (int i = 0; i < 12; ++i)
+    {
+        wd[i] = m.t_wd[i * n + c];
+        dx[i] = m.t_dx[i * n + c];
+    }
+    const double I00 = m.t_inv[c], I01 = m.t_inv[n + c], I02 = m.t_inv[2 * n + c], I11 = m.t_inv[3 * n + c],
+                 I12 = m.t_inv[4 * n + c], I22 = m.t_inv[5 * n + c];
+    const Prim5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (nb[j] < 0 && nb[j] != INT32_MIN)
+        {
+            const int32_t f = -(nb[j] + 1);
+            const V3 nrm = (double(m.t_sg[j * n + c]) / m.face_area_mag[f]) * ld3(m.face_area, f);
+            prim_arr(ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, nrm, p.fs[s]), wn[j]);
+        }
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+    {
+        double r0 = 0, r1 = 0, r2 = 0, lo = wc[q], hi = wc[q];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            if (nb[j] == INT32_MIN) continue;
+            const double dq = wn[j][q] - wc[q];
+            r0 += wd[3 * j] * dq;
+            r1 += wd[3 * j + 1] * dq;
+            r2 += wd[3 * j + 2] * dq;
+            lo = dmin(lo, wn[j][q]);
+            hi = dmax(hi, wn[j][q]);
+        }
+        const double g0 = I00 * r0 + I01 * r1 + I02 * r2;
+        const double g1 = I01 * r0 + I11 * r1 + I12 * r2;
+        const double g2 = I02 * r0 + I12 * r1 + I22 * r2;
+        double psi = 1.0;
+        if (p.limit)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const double dl = g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2];
+                if (dl > 1e-300) psi = dmin(psi, (hi - wc[q]) / dl);
+                else if (dl < -1e-300) psi = dmin(psi, (lo - wc[q]) / dl);
+            }
+            if (p.rel_limit > 0 && (q == 0 || q == 4))
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const double dl = fabs(g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2]);
+                    if (dl > 1e-300) psi = dmin(psi, p.rel_limit * wc[q] / dl);
+                }
+        }
+        const double ps = dmax(0.0, dmin(1.0, psi));
+        G(s, c, 3 * q) = ps * g0;
+        G(s, c, 3 * q + 1) = ps * g1;
+        G(s, c, 3 * q + 2) = ps * g2;
+    }
+}
+
 // Face loop of mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:36-69): Rusanov flux of the
 // reconstructed face states times |A|, per face and species (SoA: F[(s*5 + m)*nf + f]).
 // Faces that the reference skips (Skip kind, no owned fluid cell) get zero.
@@ -219,7 +307,8 @@ __global__ void k_gather_rhs(MeshView m, int nsp, const double *__restrict__ F, 
 void launch_limited_gradients(const MeshView &m, const FluidParams &p, SField<const double> W, SField<double> G, cudaStream_t s)
 {
     if (!m.nc) return;
-    k_limited_gradients_v<<<grid_for(m.nc, 32), dim3(32, 5), 0, s>>>(m, p, W, G);
+    if (m.faces_per_cell == 4) k_limited_gradients_tet<<<dim3(grid_for(m.nc, 128), p.nsp), 128, 0, s>>>(m, p, W, G);
+    else k_limited_gradients_v<<<grid_for(m.nc, 32), dim3(32, 5), 0, s>>>(m, p, W, G);
     MHD_LAUNCH_CHECK();
 }
 

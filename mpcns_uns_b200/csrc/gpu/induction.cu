@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__re
 // EdgeEMF::begin (zero) + add_ideal_emf + the boundary edge values of Solver::rhs (Solver.cpp:150-167).
 // Wall and inflow edges are overwritten by the reference, so their UCT value is not evaluated.
 template <int MAXV>
-__global__ void __launch_bounds__(128) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
+__global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                           const double *__restrict__ phi_ind, double cuct, V3 E_inf,
                                                           double *__restrict__ E)
 {

@@ -74,6 +74,36 @@ __global__ void k_stencil(MeshView m, int32_t *nb_out, double *wd_out, double *i
     valid_out[c] = 1;
 }
 
+// face_center - cell_center per c2f entry: the offset the limiter and the face reconstruction use
+// (Reconstruction.cpp:121, FluxRHS.cpp:54), one exact subtraction precomputed.
+__global__ void k_slot_dx(MeshView m, double *dx)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const V3 xc = ld3(m.cell_center, c);
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k) st3(dx, k, ld3(m.face_center, m.c2f_idx[k]) - xc);
+}
+
+// structure-of-arrays copy of the stencil of a tetrahedral mesh (4 slots per cell)
+__global__ void k_tet_tables(MeshView m, int32_t *nb, int8_t *sg, double *wd, double *dx, double *inv)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int64_t n = m.nc;
+    for (int j = 0; j < 4; ++j)
+    {
+        const int64_t k = 4 * (int64_t)c + j;
+        nb[j * n + c] = c < m.no_cells ? m.st_nb[k] : INT32_MIN;
+        sg[j * n + c] = m.c2f_sgn[k];
+        for (int a = 0; a < 3; ++a)
+        {
+            wd[(3 * j + a) * n + c] = m.st_wd[3 * k + a];
+            dx[(3 * j + a) * n + c] = m.st_dx[3 * k + a];
+        }
+    }
+    for (int q = 0; q < 6; ++q) inv[q * n + c] = m.st_inv[6 * (int64_t)c + q];
+}
+
 std::vector<int32_t> ptr32(const int64_t *p, int64_t rows, const char *what)
 {
     MHD_REQUIRE(p != nullptr, std::string("missing ") + what);
@@ -236,6 +266,27 @@ int mhd_gpu_mesh_create(const MhdMeshDesc *d, MhdMesh **out)
             MHD_LAUNCH_CHECK();
         }
         v.st_nb = m->st_nb.p; v.st_wd = m->st_wd.p; v.st_inv = m->st_inv.p; v.st_valid = m->st_valid.p;
+        bool tets = nc > 0;
+        for (int64_t c = 0; c < nc && tets; ++c) tets = c2fp[c + 1] - c2fp[c] == 4;
+        v.faces_per_cell = tets ? 4 : 0;
+        m->st_dx.alloc(3 * static_cast<size_t>(c2fp[nc]));
+        if (nc)
+        {
+            k_slot_dx<<<grid_for(nc, 256), 256, 0, m->stream>>>(v, m->st_dx.p);
+            MHD_LAUNCH_CHECK();
+        }
+        v.st_dx = m->st_dx.p;
+        if (tets)
+        {
+            m->t_nb.alloc(4 * static_cast<size_t>(nc));
+            m->t_sg.alloc(4 * static_cast<size_t>(nc));
+            m->t_wd.alloc(12 * static_cast<size_t>(nc));
+            m->t_dx.alloc(12 * static_cast<size_t>(nc));
+            m->t_inv.alloc(6 * static_cast<size_t>(nc));
+            k_tet_tables<<<grid_for(nc, 256), 256, 0, m->stream>>>(v, m->t_nb.p, m->t_sg.p, m->t_wd.p, m->t_dx.p, m->t_inv.p);
+            MHD_LAUNCH_CHECK();
+            v.t_nb = m->t_nb.p; v.t_sg = m->t_sg.p; v.t_wd = m->t_wd.p; v.t_dx = m->t_dx.p; v.t_inv = m->t_inv.p;
+        }
         MHD_CUDA(cudaStreamSynchronize(m->stream));
         *out = m;
     });

@@ -1,0 +1,799 @@
+// nvcc-flags: -prec-div=false -prec-sqrt=false
+// Mixed-precision stage of the explicit step (tetrahedral meshes).
+//
+// FP32: primitives, least-squares gradients with the Barth-Jespersen limiter, Rusanov face fluxes,
+//       cell field fit, charge-weighted velocity, CFL step, face EMF candidates and the UCT edge EMF.
+// FP64: the conservative state U (U += dt rhs and the floors), the face fluxes Phi, the CT update
+//       Phi -= dt d1 E (the edge values are summed in FP64, so d2 Phi stays at FP64 round-off for any
+//       E) and the SSP-RK2 averages.
+// The algorithm is the reference's (see step.cu for the per-kernel citations); the geometry enters
+// through single-precision tables derived once from the FP64 mesh, laid out as structures of arrays
+// over cells, faces and edges so that every warp load is coalesced and every gather is independent.
+#include <math_constants.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "state.cuh"
+
+namespace mhd
+{
+namespace
+{
+struct F5
+{
+    float rho, u, v, w, p;
+};
+
+struct MV
+{
+    int32_t nc, nf, ne, no_cells, no_edges;
+    const int32_t *c2f_idx, *cfa_idx, *t_nb, *face_L, *face_R, *f2c_ptr, *f2c_idx, *f2e_ptr, *f2e_idx, *e2f_ptr, *e2f_idx, *ec_ptr,
+        *ec_cell;
+    const int8_t *c2f_sgn, *cfa_sgn, *t_sg, *material, *face_kind, *edge_mode, *st_valid, *f2c_sgn, *f2e_sgn;
+    const float *wd, *dx, *inv, *recon, *fdx, *ew, *vol_inv;
+    const float4 *fn, *eth, *ee1, *ee2, *em;
+    const char2 *fslot;
+    const double *cell_volume; // FP64: the update divides the FP64-summed fluxes by it
+};
+
+MV make_view(const MeshView &m, const MixedTables &t)
+{
+    MV v;
+    v.nc = m.nc; v.nf = m.nf; v.ne = m.ne; v.no_cells = m.no_cells; v.no_edges = m.no_edges;
+    v.c2f_idx = m.c2f_idx; v.cfa_idx = m.cfa_idx; v.t_nb = m.t_nb; v.face_L = m.face_L; v.face_R = m.face_R;
+    v.f2c_ptr = m.f2c_ptr; v.f2c_idx = m.f2c_idx; v.f2e_ptr = m.f2e_ptr; v.f2e_idx = m.f2e_idx; v.e2f_ptr = m.e2f_ptr;
+    v.e2f_idx = m.e2f_idx; v.ec_ptr = m.ec_ptr; v.ec_cell = m.ec_cell;
+    v.c2f_sgn = m.c2f_sgn; v.cfa_sgn = m.cfa_sgn; v.t_sg = m.t_sg; v.material = m.material; v.face_kind = m.face_kind;
+    v.edge_mode = m.edge_mode; v.st_valid = m.st_valid; v.f2c_sgn = m.f2c_sgn; v.f2e_sgn = m.f2e_sgn;
+    v.wd = t.wd.p; v.dx = t.dx.p; v.inv = t.inv.p; v.recon = t.recon.p; v.fdx = t.fdx.p; v.ew = t.ew.p; v.vol_inv = t.vol_inv.p;
+    v.fn = t.fn.p; v.eth = t.eth.p; v.ee1 = t.ee1.p; v.ee2 = t.ee2.p; v.em = t.em.p;
+    v.fslot = t.fslot.p;
+    v.cell_volume = m.cell_volume;
+    return v;
+}
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float fdot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 fcross(float3 a, float3 b)
+{
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+// ------------------------------------------------------------------ one-time tables (FP64 in, FP32 out)
+__global__ void k_mx_cells(MeshView m, float *wd, float *dx, float *inv, float *recon, float *vol_inv)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int64_t n = m.nc;
+    for (int i = 0; i < 12; ++i)
+    {
+        wd[i * n + c] = static_cast<float>(m.t_wd[i * n + c]);
+        dx[i * n + c] = static_cast<float>(m.t_dx[i * n + c]);
+    }
+    for (int i = 0; i < 6; ++i) inv[i * n + c] = static_cast<float>(m.t_inv[i * n + c]);
+    vol_inv[c] = static_cast<float>(1.0 / m.cell_volume[c]);
+    // cell-field coefficients B_c = sum_j recon_j Phi_j of ImplicitInduction's constructor
+    // (Common/induction/ImplicitInduction.cpp:34-62): recon_j = M^-1 n_j, M = sum A n n^T
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    V3 nn[4];
+    double A[4];
+    for (int j = 0; j < 4; ++j)
+    {
+        const int32_t f = m.c2f_idx[4 * (int64_t)c + j];
+        A[j] = m.face_area_mag[f];
+        nn[j] = A[j] > 0 ? (1.0 / A[j]) * ld3(m.face_area, f) : mk(0, 0, 0);
+        const double nv[3] = {nn[j].x, nn[j].y, nn[j].z};
+        if (A[j] > 0)
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) M[a][b] += A[j] * nv[a] * nv[b];
+    }
+    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    const double sc = fmax(fmax(M[0][0], M[1][1]), fmax(M[2][2], 1e-300));
+    double I[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (fabs(det) >= 1e-12 * sc * sc * sc)
+    {
+        I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det; I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det; I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+        I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det; I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det; I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+        I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+    }
+    for (int j = 0; j < 4; ++j)
+        for (int a = 0; a < 3; ++a)
+            recon[(3 * j + a) * n + c] = A[j] > 0 ? static_cast<float>(I[a][0] * nn[j].x + I[a][1] * nn[j].y + I[a][2] * nn[j].z) : 0.f;
+}
+
+__global__ void k_mx_faces(MeshView m, float4 *fn, float *fdx, char2 *fslot)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    // position of f in the c2f rows of its L and R cells (the face-value slot of k_mx_grad)
+    {
+        const int32_t L = m.face_L[f], R = m.face_R[f];
+        signed char jl = 0, jr = 0;
+        for (int j = 0; j < 4; ++j)
+        {
+            if (L >= 0 && m.c2f_idx[4 * (int64_t)L + j] == f) jl = static_cast<signed char>(j);
+            if (R >= 0 && m.c2f_idx[4 * (int64_t)R + j] == f) jr = static_cast<signed char>(j);
+        }
+        fslot[f] = make_char2(jl, jr);
+    }
+    const int64_t n = m.nf;
+    const double A = m.face_area_mag[f];
+    const V3 nr = (1.0 / A) * ld3(m.face_area, f);
+    fn[f] = make_float4(static_cast<float>(nr.x), static_cast<float>(nr.y), static_cast<float>(nr.z), static_cast<float>(A));
+    const V3 xf = ld3(m.face_center, f);
+    const int32_t L = m.face_L[f], R = m.face_R[f];
+    const V3 dL = L >= 0 ? xf - ld3(m.cell_center, L) : mk(0, 0, 0);
+    const V3 dR = R >= 0 ? xf - ld3(m.cell_center, R) : mk(0, 0, 0);
+    fdx[0 * n + f] = static_cast<float>(dL.x); fdx[1 * n + f] = static_cast<float>(dL.y); fdx[2 * n + f] = static_cast<float>(dL.z);
+    fdx[3 * n + f] = static_cast<float>(dR.x); fdx[4 * n + f] = static_cast<float>(dR.y); fdx[5 * n + f] = static_cast<float>(dR.z);
+}
+
+__global__ void k_mx_edges(MeshView m, float4 *eth, float4 *ee1, float4 *ee2, float4 *em, float *ew)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    const double L = m.edge_len[e];
+    const V3 th = L > 0 ? (1.0 / L) * ld3(m.edge_vec, e) : mk(0, 0, 0);
+    const V3 ax = fabs(th.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
+    V3 e1 = cross(th, ax);
+    const double n1 = sqrt(dot(e1, e1));
+    e1 = n1 > 0 ? (1.0 / n1) * e1 : mk(0, 0, 0);
+    const V3 e2 = cross(th, e1);
+    eth[e] = make_float4(static_cast<float>(th.x), static_cast<float>(th.y), static_cast<float>(th.z), static_cast<float>(L));
+    ee1[e] = make_float4(static_cast<float>(e1.x), static_cast<float>(e1.y), static_cast<float>(e1.z), 0.f);
+    ee2[e] = make_float4(static_cast<float>(e2.x), static_cast<float>(e2.y), static_cast<float>(e2.z), 0.f);
+    const V3 mid = ld3(m.edge_mid, e);
+    for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k)
+    {
+        const int32_t f = m.e2f_idx[k];
+        V3 v = ld3(m.face_center, f) - mid;
+        v = v - dot(v, th) * th;
+        const double nv = sqrt(dot(v, v));
+        const V3 mi = nv > 0 ? (1.0 / nv) * v : mk(0, 0, 0);
+        const V3 nrm = (1.0 / m.face_area_mag[f]) * ld3(m.face_area, f);
+        const double sig = dot(th, cross(mi, nrm));
+        em[k] = make_float4(static_cast<float>(mi.x), static_cast<float>(mi.y), static_cast<float>(mi.z), static_cast<float>(sig));
+        ew[k] = static_cast<float>(m.ef_weight[k]);
+    }
+}
+
+__global__ void k_mx_badd(const double *badd, float4 *b32, int32_t nc)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    b32[c] = make_float4(static_cast<float>(badd[3 * (int64_t)c]), static_cast<float>(badd[3 * (int64_t)c + 1]),
+                         static_cast<float>(badd[3 * (int64_t)c + 2]), 0.f);
+}
+
+// ------------------------------------------------------------------ stage kernels
+struct MxParams
+{
+    int nsp, limit;
+    float gamma, rel_limit, rho_floor, p_floor;
+    double rho_floor_d, p_floor_d, gamma_d;
+    F5 fs[kMaxSpecies];
+    int8_t absorb[kMaxSpecies];
+    float mass[kMaxSpecies];
+    float M_ref;
+};
+
+__device__ __forceinline__ F5 ghost32(int kind, bool absorb, const F5 &in, float3 n, const F5 &fs)
+{
+    if (kind == 1)
+    {
+        if (absorb) return F5{1e-12f, 0.f, 0.f, 0.f, 1e-12f};
+        const float un = in.u * n.x + in.v * n.y + in.w * n.z;
+        F5 g = in;
+        g.u -= 2.f * un * n.x;
+        g.v -= 2.f * un * n.y;
+        g.w -= 2.f * un * n.z;
+        return g;
+    }
+    if (kind == 2) return fs;
+    return in;
+}
+
+__device__ __forceinline__ void rusanov32(const F5 &L, const F5 &R, float3 n, float gamma, float *F)
+{
+    const float gm1 = 1.f / (gamma - 1.f);
+    const float EL = L.p * gm1 + 0.5f * L.rho * (L.u * L.u + L.v * L.v + L.w * L.w);
+    const float ER = R.p * gm1 + 0.5f * R.rho * (R.u * R.u + R.v * R.v + R.w * R.w);
+    const float unL = L.u * n.x + L.v * n.y + L.w * n.z, unR = R.u * n.x + R.v * n.y + R.w * n.z;
+    const float mL = L.rho * unL, mR = R.rho * unR;
+    const float sL = fabsf(unL) + sqrtf(gamma * L.p / L.rho), sR = fabsf(unR) + sqrtf(gamma * R.p / R.rho);
+    const float s = fmaxf(sL, sR);
+    F[0] = 0.5f * (mL + mR) - 0.5f * s * (R.rho - L.rho);
+    F[1] = 0.5f * (mL * L.u + L.p * n.x + mR * R.u + R.p * n.x) - 0.5f * s * (R.rho * R.u - L.rho * L.u);
+    F[2] = 0.5f * (mL * L.v + L.p * n.y + mR * R.v + R.p * n.y) - 0.5f * s * (R.rho * R.v - L.rho * L.v);
+    F[3] = 0.5f * (mL * L.w + L.p * n.z + mR * R.w + R.p * n.z) - 0.5f * s * (R.rho * R.w - L.rho * L.w);
+    F[4] = 0.5f * (unL * (EL + L.p) + unR * (ER + R.p)) - 0.5f * s * (ER - EL);
+}
+
+// primitives (FP32), cell field fit, total field, charge-weighted velocity
+__global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const double *__restrict__ U, const double *__restrict__ phi,
+                                                     const float4 *__restrict__ badd, float *__restrict__ W, float4 *__restrict__ up,
+                                                     float4 *__restrict__ bt, float4 *__restrict__ bi)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int64_t n = m.nc;
+    float ne = 0.f;
+    for (int s = 0; s < p.nsp; ++s)
+    {
+        const double *Us = U + (int64_t)s * 5 * n;
+        const double r = fmax(Us[c], p.rho_floor_d);
+        const double ir = 1.0 / r;
+        const double u = Us[n + c] * ir, v = Us[2 * n + c] * ir, w = Us[3 * n + c] * ir;
+        const double pr = fmax((p.gamma_d - 1.0) * (Us[4 * n + c] - 0.5 * r * (u * u + v * v + w * w)), p.p_floor_d);
+        float *Ws = W + (int64_t)s * 5 * n;
+        Ws[c] = static_cast<float>(r);
+        Ws[n + c] = static_cast<float>(u);
+        Ws[2 * n + c] = static_cast<float>(v);
+        Ws[3 * n + c] = static_cast<float>(w);
+        Ws[4 * n + c] = static_cast<float>(pr);
+        ne += static_cast<float>(r) / p.mass[s] * p.M_ref;
+    }
+    const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
+    const float ph[4] = {static_cast<float>(phi[fi.x]), static_cast<float>(phi[fi.y]), static_cast<float>(phi[fi.z]),
+                         static_cast<float>(phi[fi.w])};
+    float b[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) b[a] += m.recon[(3 * j + a) * n + c] * ph[j];
+    const float4 ba = badd[c];
+    bi[c] = make_float4(b[0], b[1], b[2], 0.f);
+    bt[c] = make_float4(b[0] + ba.x, b[1] + ba.y, b[2] + ba.z, 0.f);
+    float u3[3] = {0.f, 0.f, 0.f};
+    if (m.material[c] == 0)
+        for (int s = 0; s < p.nsp; ++s)
+        {
+            // number density and velocity re-read from the primitives this thread has just written
+            const float *Ws = W + (int64_t)s * 5 * n;
+            const float chi = ne > 1e-30f ? (Ws[c] / p.mass[s] * p.M_ref) / ne : (s == 0 ? 1.f : 0.f);
+            for (int a = 0; a < 3; ++a) u3[a] += chi * Ws[(1 + a) * n + c];
+        }
+    up[c] = make_float4(u3[0], u3[1], u3[2], 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_mx_cfl(MV m, MxParams p, float cfl, float inver_MA2, float rho_floor_dt,
+                                                 const float *__restrict__ W, const float4 *__restrict__ bt,
+                                                 unsigned long long *__restrict__ dt_bits, int *__restrict__ flag)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = m.nc;
+    float dt = CUDART_INF_F;
+    if (c < m.no_cells && m.material[c] == 0)
+    {
+        const float3 b = f3(bt[c]);
+        const float B2 = fdot(b, b);
+        float rs = 0.f;
+        for (int s = 0; s < p.nsp; ++s) rs += W[(int64_t)s * 5 * n + c];
+        const float rho_tot = fmaxf(rs, rho_floor_dt);
+        const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
+        const float4 fn4[4] = {m.fn[fi.x], m.fn[fi.y], m.fn[fi.z], m.fn[fi.w]};
+        const float vol = 1.f / m.vol_inv[c];
+        for (int s = 0; s < p.nsp; ++s)
+        {
+            const float *Ws = W + (int64_t)s * 5 * n;
+            const float rho = Ws[c], u = Ws[n + c], v = Ws[2 * n + c], w = Ws[3 * n + c], pr = Ws[4 * n + c];
+            const float cs2 = p.gamma * pr / fmaxf(rho, 1e-30f);
+            const float vA2 = inver_MA2 * B2 / rho_tot;
+            float denom = 0.f;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const float3 nr = f3(fn4[j]);
+                const float bn = fdot(b, nr);
+                const float vAn2 = inver_MA2 * bn * bn / rho_tot;
+                const float term = cs2 + vA2;
+                const float cf = sqrtf(0.5f * (term + sqrtf(fmaxf(0.f, term * term - 4.f * cs2 * vAn2))));
+                denom += (fabsf(u * nr.x + v * nr.y + w * nr.z) + cf) * fn4[j].w;
+            }
+            if (denom > 0.f) dt = fminf(dt, cfl * vol / denom);
+        }
+        if (!(dt > 0.f)) atomicOr(flag, 1);
+    }
+    __shared__ float sh[32];
+    float v = dt > 0.f ? dt : CUDART_INF_F;
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : CUDART_INF_F;
+        for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (threadIdx.x == 0 && v < CUDART_INF_F)
+            atomicMin(dt_bits, static_cast<unsigned long long>(__double_as_longlong(static_cast<double>(v))));
+    }
+}
+
+// limited face values (see below), one thread per (cell, species = blockIdx.y)
+__global__ void __launch_bounds__(128) k_mx_grad(MV m, MxParams p, int s0, const float *__restrict__ W, const double *__restrict__ U,
+                                                 float *__restrict__ G)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y, s = s0 + g;
+    if (c >= m.nc) return;
+    const int64_t n = m.nc;
+    float *Gs = G + (int64_t)g * 20 * n;
+    const float *Ws = W + (int64_t)s * 5 * n;
+    if (c >= m.no_cells || !m.st_valid[c])
+    {
+        // zero gradient: every face value is the cell value
+        for (int q = 0; q < 5; ++q)
+        {
+            const float w = Ws[q * n + c];
+            for (int j = 0; j < 4; ++j) Gs[(4 * q + j) * n + c] = w;
+        }
+        return;
+    }
+    int32_t nb[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) nb[j] = m.t_nb[j * n + c];
+    float wc[5], wn[4][5], wd[12], dx[12];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) wc[q] = Ws[q * n + c];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (nb[j] >= 0)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) wn[j][q] = Ws[q * n + nb[j]];
+#pragma unroll
+    for (int i = 0; i < 12; ++i)
+    {
+        wd[i] = m.wd[i * n + c];
+        dx[i] = m.dx[i * n + c];
+    }
+    const float I00 = m.inv[c], I01 = m.inv[n + c], I02 = m.inv[2 * n + c], I11 = m.inv[3 * n + c], I12 = m.inv[4 * n + c],
+                I22 = m.inv[5 * n + c];
+    const F5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (nb[j] < 0 && nb[j] != INT32_MIN)
+        {
+            const int32_t f = -(nb[j] + 1);
+            const float4 nf = m.fn[f];
+            const float sg = m.t_sg[j * n + c];
+            const F5 gh = ghost32(m.face_kind[f], p.absorb[s] != 0, wcp, make_float3(sg * nf.x, sg * nf.y, sg * nf.z), p.fs[s]);
+            wn[j][0] = gh.rho; wn[j][1] = gh.u; wn[j][2] = gh.v; wn[j][3] = gh.w; wn[j][4] = gh.p;
+        }
+    (void)U;
+    // Limited face values v_j = w + psi g.dx_j (the face_state of FluxRHS.cpp:16-27 before its positivity
+    // test) instead of the gradient.  The face that sets the Barth-Jespersen psi is snapped to its bound,
+    // which exact arithmetic gives (w + (b - w)/dl * dl = b): near an absorbing wall the bound is the
+    // 1e-12 floor state and the single-precision sum w + psi dl, with w ~ 1e-3, could not resolve it.
+    float fv[5][4];
+#pragma unroll
+    for (int q = 0; q < 5; ++q)
+    {
+        float r0 = 0.f, r1 = 0.f, r2 = 0.f, lo = wc[q], hi = wc[q];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            if (nb[j] == INT32_MIN) continue;
+            const float dq = wn[j][q] - wc[q];
+            r0 += wd[3 * j] * dq;
+            r1 += wd[3 * j + 1] * dq;
+            r2 += wd[3 * j + 2] * dq;
+            lo = fminf(lo, wn[j][q]);
+            hi = fmaxf(hi, wn[j][q]);
+        }
+        const float g0 = I00 * r0 + I01 * r1 + I02 * r2;
+        const float g1 = I01 * r0 + I11 * r1 + I12 * r2;
+        const float g2 = I02 * r0 + I12 * r1 + I22 * r2;
+        float dl[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dl[j] = g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2];
+        float psi = 1.f, bound = 0.f;
+        int jb = -1;
+        if (p.limit)
+        {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                if (dl[j] > 1e-30f)
+                {
+                    const float r = (hi - wc[q]) / dl[j];
+                    if (r < psi) { psi = r; jb = j; bound = hi; }
+                }
+                else if (dl[j] < -1e-30f)
+                {
+                    const float r = (lo - wc[q]) / dl[j];
+                    if (r < psi) { psi = r; jb = j; bound = lo; }
+                }
+            }
+            if (p.rel_limit > 0.f && (q == 0 || q == 4))
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const float a = fabsf(dl[j]);
+                    if (a > 1e-30f)
+                    {
+                        const float r = p.rel_limit * wc[q] / a;
+                        if (r < psi) { psi = r; jb = -1; }
+                    }
+                }
+        }
+        if (psi < 0.f) { psi = 0.f; jb = -1; }
+        psi = fminf(1.f, psi);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) fv[q][j] = j == jb ? bound : wc[q] + psi * dl[j];
+    }
+    // positivity fallback of face_state: a face with rho <= 0 or p <= 0 takes the cell state
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        const bool ok = fv[0][j] > 0.f && fv[4][j] > 0.f;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) Gs[(4 * q + j) * n + c] = ok ? fv[q][j] : wc[q];
+    }
+}
+
+// Rusanov face flux times |A|, one thread per (face, species = blockIdx.y)
+__global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, const float *__restrict__ W, const float *__restrict__ G,
+                                                 float *__restrict__ F)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y, s = s0 + g;
+    if (f >= m.nf) return;
+    const int64_t nf = m.nf, n = m.nc;
+    float *Fs = F + (int64_t)g * 5 * nf;
+    const int kind = m.face_kind[f];
+    const int32_t p0 = m.f2c_ptr[f], cnt = m.f2c_ptr[f + 1] - p0;
+    const int32_t L = m.face_L[f], R = m.face_R[f];
+    bool any = false;
+    if (L >= 0) any |= L < m.no_cells && m.material[L] == 0;
+    if (R >= 0) any |= R < m.no_cells && m.material[R] == 0;
+    if (kind == 4 || !any)
+    {
+        for (int q = 0; q < 5; ++q) Fs[q * nf + f] = 0.f;
+        return;
+    }
+    const float *Ws = W + (int64_t)s * 5 * n;
+    const float *Gs = G + (int64_t)g * 20 * n;
+    const float4 nf4 = m.fn[f];
+    const float3 nr = f3(nf4);
+    const char2 sl = m.fslot[f];
+    (void)Ws;
+    // reconstructed face state of cell c (positivity fallback already applied by k_mx_grad)
+    auto state = [&](int32_t c, int side) {
+        const int j = side == 0 ? sl.x : sl.y;
+        return F5{Gs[(0 + j) * n + c], Gs[(4 + j) * n + c], Gs[(8 + j) * n + c], Gs[(12 + j) * n + c], Gs[(16 + j) * n + c]};
+    };
+    F5 Ls, Rs;
+    if (cnt == 2 && kind == 0)
+    {
+        Ls = state(L, 0);
+        Rs = state(R, 1);
+    }
+    else
+    {
+        // the one fluid cell of a boundary / interface face (FluxRHS.cpp:58-66)
+        int32_t c = m.f2c_idx[p0];
+        int sgn = m.f2c_sgn[p0];
+        if (cnt == 2 && m.material[c] != 0)
+        {
+            c = m.f2c_idx[p0 + 1];
+            sgn = m.f2c_sgn[p0 + 1];
+        }
+        const F5 in = state(c, sgn > 0 ? 0 : 1);
+        const float sf = static_cast<float>(sgn);
+        const F5 gh = ghost32(kind, p.absorb[s] != 0, in, make_float3(sf * nr.x, sf * nr.y, sf * nr.z), p.fs[s]);
+        if (sgn > 0) { Ls = in; Rs = gh; }
+        else { Rs = in; Ls = gh; }
+    }
+    float Fl[5];
+    rusanov32(Ls, Rs, nr, p.gamma, Fl);
+#pragma unroll
+    for (int q = 0; q < 5; ++q) Fs[q * nf + f] = Fl[q] * nf4.w;
+}
+
+// rhs gathered from the face fluxes, U (FP64) += dt rhs, floors, SSP-RK2 average in stage 2
+__global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, const float *__restrict__ F, const double *__restrict__ Ub,
+                                                   double *__restrict__ Uo, const double *__restrict__ dtp, int stage2)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int g = blockIdx.y, s = s0 + g;
+    if (c >= m.nc) return;
+    const int64_t n = m.nc, nf = m.nf;
+    const double *ub = Ub + (int64_t)s * 5 * n;
+    double *uo = Uo + (int64_t)s * 5 * n;
+    const float *Fs = F + (int64_t)g * 5 * nf;
+    double u[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) u[q] = ub[q * n + c];
+    if (c < m.no_cells && m.material[c] == 0)
+    {
+        const int4 fi = *reinterpret_cast<const int4 *>(m.cfa_idx + 4 * (int64_t)c);
+        const char4 sg = *reinterpret_cast<const char4 *>(m.cfa_sgn + 4 * (int64_t)c);
+        const int32_t ff[4] = {fi.x, fi.y, fi.z, fi.w};
+        const double sv[4] = {sg.x > 0 ? -1.0 : 1.0, sg.y > 0 ? -1.0 : 1.0, sg.z > 0 ? -1.0 : 1.0, sg.w > 0 ? -1.0 : 1.0};
+        // the face fluxes are summed in FP64: the rhs is a difference of fluxes that can nearly cancel
+        double r[5] = {0, 0, 0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) r[q] += sv[j] * static_cast<double>(Fs[q * nf + ff[j]]);
+        const double dtv = *dtp / m.cell_volume[c];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) u[q] += dtv * r[q];
+        const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
+        const double gm = p.gamma_d;
+        if (!(u[0] >= p.rho_floor_d))
+        {
+            u[0] = p.rho_floor_d; u[1] = u[2] = u[3] = 0.0;
+            u[4] = p.p_floor_d / (gm - 1.0);
+        }
+        else if ((gm - 1.0) * (u[4] - ke) < p.p_floor_d)
+            u[4] = p.p_floor_d / (gm - 1.0) + ke;
+    }
+    if (stage2)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) uo[q * n + c] = 0.5 * (uo[q * n + c] + u[q]);
+    else
+#pragma unroll
+        for (int q = 0; q < 5; ++q) uo[q * n + c] = u[q];
+}
+
+// face EMF candidates E_f = -n x F_f (IdealEMF.cpp:32-55), 3 per face (structure of arrays)
+__global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__restrict__ up, const float4 *__restrict__ bt,
+                                                      const float4 *__restrict__ bi, const double *__restrict__ phi,
+                                                      const double *__restrict__ phi_add, float *__restrict__ Ef)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    const int64_t nf = m.nf;
+    const float4 nf4 = m.fn[f];
+    const float3 n = f3(nf4);
+    const float Bn = static_cast<float>((phi[f] + phi_add[f]) / static_cast<double>(nf4.w));
+    const int32_t L = m.face_L[f], R = m.face_R[f];
+    float3 F;
+    auto flux = [&](int32_t c) {
+        const float3 uc = f3(up[c]), bc = f3(bt[c]);
+        const float un = fdot(uc, n);
+        return make_float3(un * bc.x - Bn * uc.x, un * bc.y - Bn * uc.y, un * bc.z - Bn * uc.z);
+    };
+    if (L >= 0 && R >= 0)
+    {
+        const float a = fmaxf(fabsf(fdot(f3(up[L]), n)), fabsf(fdot(f3(up[R]), n)));
+        const float3 FL = flux(L), FR = flux(R);
+        const float3 bL = f3(bi[L]), bR = f3(bi[R]);
+        F = make_float3(0.5f * (FL.x + FR.x) - 0.5f * a * (bR.x - bL.x), 0.5f * (FL.y + FR.y) - 0.5f * a * (bR.y - bL.y),
+                        0.5f * (FL.z + FR.z) - 0.5f * a * (bR.z - bL.z));
+    }
+    else
+        F = flux(L >= 0 ? L : R);
+    const float3 E = fcross(n, F);
+    Ef[f] = -E.x;
+    Ef[nf + f] = -E.y;
+    Ef[2 * nf + f] = -E.z;
+}
+
+// UCT edge EMF (IdealEMF.cpp:59-128) with the boundary edge values (Solver.cpp:162-167)
+__global__ void __launch_bounds__(128) k_mx_edge(MV m, const float *__restrict__ Ef, const float4 *__restrict__ up,
+                                                 const double *__restrict__ phi, float cuct, float3 E_inf, float *__restrict__ E)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    const int64_t nf = m.nf;
+    float val = 0.f;
+    const float4 t4 = m.eth[e];
+    const float Lg = t4.w;
+    const float3 th = f3(t4);
+    const int mode = e < m.no_edges ? m.edge_mode[e] : -1;
+    if (mode == 1) val = 0.f;
+    else if (mode == 2) val = Lg * fdot(E_inf, th);
+    else if (mode == 0)
+    {
+        const int32_t f0 = m.e2f_ptr[e], nfe = m.e2f_ptr[e + 1] - f0;
+        const int32_t q0 = m.ec_ptr[e], q1 = m.ec_ptr[e + 1];
+        bool any_fluid = false;
+        for (int32_t k = q0; k < q1 && !any_fluid; ++k) any_fluid = m.material[m.ec_cell[k]] == 0;
+        if (nfe > 0 && Lg > 0.f && any_fluid)
+        {
+            const float3 e1 = f3(m.ee1[e]), e2 = f3(m.ee2[e]);
+            float w[8], aef[8], sg[8], qa[8], qb[8], pA[8];
+            float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+                if (i >= nfe) break;
+                const int32_t f = m.e2f_idx[f0 + i];
+                const float4 mi4 = m.em[f0 + i];
+                const float3 mi = f3(mi4);
+                const float4 nf4 = m.fn[f];
+                w[i] = m.ew[f0 + i];
+                Ec += w[i] * (Ef[f] * th.x + Ef[nf + f] * th.y + Ef[2 * nf + f] * th.z);
+                float a = 0.f;
+                for (int32_t k = q0; k < q1; ++k) a = fmaxf(a, fabsf(fdot(f3(up[m.ec_cell[k]]), mi)));
+                aef[i] = a;
+                sg[i] = mi4.w;
+                const float as = a * sg[i];
+                qa[i] = as * (nf4.x * e1.x + nf4.y * e1.y + nf4.z * e1.z);
+                qb[i] = as * (nf4.x * e2.x + nf4.y * e2.y + nf4.z * e2.z);
+                pA[i] = static_cast<float>(phi[f] / static_cast<double>(nf4.w));
+                M11 += w[i] * qa[i] * qa[i];
+                M12 += w[i] * qa[i] * qb[i];
+                M22 += w[i] * qb[i] * qb[i];
+                g1 += w[i] * qa[i];
+                g2 += w[i] * qb[i];
+            }
+            const float tr = M11 + M22;
+            const float eps = 1e-14f * tr;
+            const float det = (M11 + eps) * (M22 + eps) - M12 * M12;
+            float l1 = 0.f, l2 = 0.f;
+            if (tr > 0.f && det > 0.f)
+            {
+                l1 = ((M22 + eps) * g1 - M12 * g2) / det;
+                l2 = ((M11 + eps) * g2 - M12 * g1) / det;
+            }
+            float Eu = 0.f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+            {
+                if (i >= nfe) break;
+                Eu += w[i] * (1.f - (qa[i] * l1 + qb[i] * l2)) * aef[i] * sg[i] * pA[i];
+            }
+            val = Lg * Ec + 2.f * cuct * Lg * Eu;
+        }
+    }
+    E[e] = val;
+}
+
+// Phi -= dt d1 E on the active faces, E summed in FP64; stage 2 averages with Phi0
+__global__ void __launch_bounds__(256) k_mx_ct(MV m, const float *__restrict__ E, const double *__restrict__ phis,
+                                               double *__restrict__ phio, const double *__restrict__ dtp, int stage2)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    bool active = false;
+    for (int32_t k = m.f2c_ptr[f]; k < m.f2c_ptr[f + 1]; ++k) active |= m.f2c_idx[k] < m.no_cells;
+    double v = phis[f];
+    if (active)
+    {
+        double circ = 0.0;
+        for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) circ += m.f2e_sgn[k] * static_cast<double>(E[m.f2e_idx[k]]);
+        v -= *dtp * circ;
+    }
+    phio[f] = stage2 ? 0.5 * (phio[f] + v) : v;
+}
+
+__global__ void k_mx_cfl_init(unsigned long long *dt_bits, int *flag)
+{
+    *dt_bits = static_cast<unsigned long long>(__double_as_longlong(CUDART_INF));
+    *flag = 0;
+}
+
+__global__ void k_mx_cfl_final(const unsigned long long *dt_bits, double dt_max, double *dt, int *flag)
+{
+    double g = __longlong_as_double(static_cast<long long>(*dt_bits));
+    g = fmin(g, dt_max);
+    if (!isfinite(g) || g <= 0) atomicOr(flag, 1);
+    *dt = g;
+}
+
+MxParams mx_params(const MhdState *st)
+{
+    MxParams p{};
+    const MhdStepParams &q = st->prm;
+    p.nsp = st->nsp;
+    p.limit = 1;
+    p.gamma = static_cast<float>(q.gamma);
+    p.gamma_d = q.gamma;
+    p.rel_limit = static_cast<float>(q.rel_limit);
+    p.rho_floor = static_cast<float>(q.rho_floor);
+    p.p_floor = static_cast<float>(q.p_floor);
+    p.rho_floor_d = q.rho_floor;
+    p.p_floor_d = q.p_floor;
+    p.M_ref = static_cast<float>(q.M_ref);
+    for (int s = 0; s < st->nsp; ++s)
+    {
+        p.fs[s] = F5{static_cast<float>(q.fs[s].rho), static_cast<float>(q.fs[s].u), static_cast<float>(q.fs[s].v),
+                     static_cast<float>(q.fs[s].w), static_cast<float>(q.fs[s].p)};
+        p.absorb[s] = q.absorb[s];
+        p.mass[s] = static_cast<float>(q.mass[s]);
+    }
+    return p;
+}
+} // namespace
+
+void mixed_setup(MhdState *st)
+{
+    MhdMesh *mesh = st->mesh;
+    const MeshView &m = mesh->v;
+    cudaStream_t s = mesh->stream;
+    MixedTables &t = st->mt;
+    const size_t nc = m.nc, nf = m.nf, ne = m.ne;
+    int32_t nnz_e2f = 0;
+    MHD_CUDA(cudaMemcpy(&nnz_e2f, m.e2f_ptr + m.ne, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    t.wd.alloc(12 * nc); t.dx.alloc(12 * nc); t.inv.alloc(6 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
+    t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
+    t.eth.alloc(ne); t.ee1.alloc(ne); t.ee2.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
+    if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.wd.p, t.dx.p, t.inv.p, t.recon.p, t.vol_inv.p);
+    if (nf) k_mx_faces<<<grid_for(nf, 256), 256, 0, s>>>(m, t.fn.p, t.fdx.p, t.fslot.p);
+    if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.ee1.p, t.ee2.p, t.em.p, t.ew.p);
+    MHD_LAUNCH_CHECK();
+    st->W32.alloc(5 * nc * st->nsp);
+    st->grad32.alloc(20 * nc * st->group); // limited face values, 5 variables x 4 faces per cell
+    st->F32.alloc(5 * nf * st->group);
+    st->Ef32.alloc(3 * nf);
+    st->E32.alloc(ne);
+    st->up32.alloc(nc); st->bt32.alloc(nc); st->bi32.alloc(nc); st->badd32.alloc(nc);
+    if (nc) MHD_CUDA(cudaMemsetAsync(st->badd32.p, 0, nc * sizeof(float4), s));
+    MHD_CUDA(cudaStreamSynchronize(s));
+}
+
+void mixed_badd(MhdState *st)
+{
+    const MeshView &m = st->mesh->v;
+    if (!m.nc) return;
+    k_mx_badd<<<grid_for(m.nc, 256), 256, 0, st->mesh->stream>>>(st->badd.p, st->badd32.p, m.nc);
+    MHD_LAUNCH_CHECK();
+}
+
+void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max)
+{
+    MhdMesh *mesh = st->mesh;
+    const MeshView &mv = mesh->v;
+    const MV m = make_view(mv, st->mt);
+    cudaStream_t s = mesh->stream;
+    Profiler &P = st->prof;
+    const MxParams p = mx_params(st);
+    const int gc = grid_for(m.nc, 128), gf = grid_for(m.nf, 128), ge = grid_for(m.ne, 128);
+    if (!m.nc) return;
+    P.begin(KP_PREPARE, s);
+    k_mx_prepare<<<gc, 128, 0, s>>>(m, p, Us, phis, st->badd32.p, st->W32.p, st->up32.p, st->bt32.p, st->bi32.p);
+    MHD_LAUNCH_CHECK();
+    P.end(KP_PREPARE, s);
+    ++st->launches;
+    if (cfl)
+    {
+        P.begin(KP_CFL, s);
+        k_mx_cfl_init<<<1, 1, 0, s>>>(st->dt_bits.p, st->flag.p);
+        k_mx_cfl<<<gc, 128, 0, s>>>(m, p, static_cast<float>(st->prm.cfl), static_cast<float>(st->prm.inver_MA2),
+                                    static_cast<float>(st->prm.rho_floor_dt), st->W32.p, st->bt32.p, st->dt_bits.p, st->flag.p);
+        k_mx_cfl_final<<<1, 1, 0, s>>>(st->dt_bits.p, dt_max, st->scal.p, st->flag.p);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_CFL, s);
+        st->launches += 3;
+    }
+    for (int s0 = 0; s0 < st->nsp; s0 += st->group)
+    {
+        const int ng = std::min(st->group, st->nsp - s0);
+        P.begin(KP_GRAD, s);
+        k_mx_grad<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->W32.p, Us, st->grad32.p);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_GRAD, s);
+        P.begin(KP_FLUX, s);
+        k_mx_flux<<<dim3(gf, ng), 128, 0, s>>>(m, p, s0, st->W32.p, st->grad32.p, st->F32.p);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_FLUX, s);
+        P.begin(KP_UPDATE, s);
+        k_mx_update<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0);
+        MHD_LAUNCH_CHECK();
+        P.end(KP_UPDATE, s);
+        st->launches += 3;
+    }
+    const float3 Einf = make_float3(static_cast<float>(-(st->prm.u_inf[1] * st->prm.B_imf[2] - st->prm.u_inf[2] * st->prm.B_imf[1])),
+                                    static_cast<float>(-(st->prm.u_inf[2] * st->prm.B_imf[0] - st->prm.u_inf[0] * st->prm.B_imf[2])),
+                                    static_cast<float>(-(st->prm.u_inf[0] * st->prm.B_imf[1] - st->prm.u_inf[1] * st->prm.B_imf[0])));
+    P.begin(KP_FACE_CAND, s);
+    k_mx_face_cand<<<gf, 128, 0, s>>>(m, st->up32.p, st->bt32.p, st->bi32.p, phis, st->phi_add.p, st->Ef32.p);
+    MHD_LAUNCH_CHECK();
+    P.end(KP_FACE_CAND, s);
+    P.begin(KP_EDGE_EMF, s);
+    k_mx_edge<<<ge, 128, 0, s>>>(m, st->Ef32.p, st->up32.p, phis, static_cast<float>(st->prm.cuct), Einf, st->E32.p);
+    MHD_LAUNCH_CHECK();
+    P.end(KP_EDGE_EMF, s);
+    P.begin(KP_CT, s);
+    k_mx_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m, st->E32.p, phis, phio, st->scal.p, stage2 ? 1 : 0);
+    MHD_LAUNCH_CHECK();
+    P.end(KP_CT, s);
+    st->launches += 3;
+}
+} // namespace mhd

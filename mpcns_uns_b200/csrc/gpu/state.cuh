@@ -1,0 +1,95 @@
+// Resident state of the fused step, shared by the FP64 (step.cu) and the mixed-precision (mixed.cu)
+// translation units.
+#pragma once
+#include <vector>
+
+#include "fluid.cuh"
+
+namespace mhd
+{
+// Kernel classes of the step, timed with CUDA events on the handle's stream when profiling is on.
+enum StepKernel { KP_PREPARE = 0, KP_CFL, KP_GRAD, KP_FLUX, KP_UPDATE, KP_FACE_CAND, KP_EDGE_EMF, KP_CT, KP_COUNT };
+static const char *const kStepKernelNames[KP_COUNT] = {"prepare", "cfl", "limited_gradients", "face_flux",
+                                                        "update",  "face_candidate", "edge_emf", "ct"};
+
+struct Profiler
+{
+    bool on = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KP_COUNT];
+    size_t used[KP_COUNT] = {};
+    ~Profiler()
+    {
+        for (auto &v : ev)
+            for (auto &p : v)
+            {
+                cudaEventDestroy(p.first);
+                cudaEventDestroy(p.second);
+            }
+    }
+    void begin(int k, cudaStream_t s)
+    {
+        if (!on) return;
+        if (used[k] == ev[k].size())
+        {
+            cudaEvent_t a, b;
+            MHD_CUDA(cudaEventCreate(&a));
+            MHD_CUDA(cudaEventCreate(&b));
+            ev[k].emplace_back(a, b);
+        }
+        MHD_CUDA(cudaEventRecord(ev[k][used[k]].first, s));
+    }
+    void end(int k, cudaStream_t s)
+    {
+        if (!on) return;
+        MHD_CUDA(cudaEventRecord(ev[k][used[k]].second, s));
+        ++used[k];
+    }
+};
+
+// Single-precision tables of the mixed path, derived once from the FP64 mesh (tetrahedral meshes):
+// structure of arrays over cells / faces / edges so that every warp load is coalesced.
+struct MixedTables
+{
+    DBuf<float> wd, dx, inv;    // stencil: [12][nc], [12][nc], [6][nc]
+    DBuf<float> recon;          // cell field from face fluxes: B_c = sum_j recon[j] Phi_{f_j}, [12][nc]
+    DBuf<float4> fn;            // per face: canonical unit normal, |A|
+    DBuf<float> fdx;            // per face: x_f - x_L (3), x_f - x_R (3): [6][nf]
+    DBuf<char2> fslot;          // per face: its position in the c2f rows of L and R
+    DBuf<float4> eth;           // per edge: unit tangent, length
+    DBuf<float4> ee1, ee2;      // per edge: orthonormal basis of the plane normal to the edge
+    DBuf<float4> em;            // per e2f entry: in-face unit direction away from the edge, sigma = t.(m x n)
+    DBuf<float> ew;             // per e2f entry: w_ef
+    DBuf<float> vol_inv;        // per cell: 1 / V
+};
+} // namespace mhd
+
+struct MhdState
+{
+    MhdMesh *mesh = nullptr;
+    MhdStepParams prm{};
+    mhd::FluidParams fp{};
+    int nsp = 0, group = 0;
+    bool mixed = false;
+    mhd::DBuf<double> U0, U1, W, grad, F, phi0, phi1, phi_add, badd, bind, btot, up, Ef, E, mass, stage;
+    mhd::DBuf<double> scal; // [0] dt
+    mhd::DBuf<unsigned long long> dt_bits;
+    mhd::DBuf<int> flag;
+    // mixed precision: FP32 bulk arrays (the state U and the face fluxes Phi stay FP64)
+    mhd::MixedTables mt;
+    mhd::DBuf<float> W32, grad32, F32, Ef32, E32;
+    mhd::DBuf<float4> up32, bt32, bi32, badd32;
+    double *pinned = nullptr;
+    int64_t launches = 0; // kernels launched by the step since creation
+    mhd::Profiler prof;
+    ~MhdState()
+    {
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
+namespace mhd
+{
+void mixed_setup(MhdState *st);
+void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max);
+void mixed_badd(MhdState *st);
+} // namespace mhd

@@ -17,6 +17,7 @@
 
 #include "induction.cuh"
 #include "kernels.cuh"
+#include "state.cuh"
 
 namespace mhd
 {
@@ -146,17 +147,20 @@ __global__ void k_set_dt(double *dt, double v, int *flag)
 // Solver::advance (Solver.cpp:194-206) for one species group: rhs gathered from the face fluxes in the
 // reference's scatter order, U = U_base + dt rhs on the owned fluid cells, Solver::enforce_floors
 // (:171-191); stage 2 averages with U0 in place (Solver.cpp:505-506).
+// NF = 4: tetrahedral mesh, the four faces of the cell unrolled (all flux gathers in flight together);
+// NF = 0: any polyhedra.  One thread per (cell, species of the group = blockIdx.y).
+template <int NF>
 __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s0, int ng, const double *__restrict__ F,
                                                  SField<const double> Ub, SField<double> Uo, const double *__restrict__ dtp, int stage2)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
+    const int g = blockIdx.y;
+    if (c >= m.nc || g >= ng) return;
     const int64_t nf = m.nf;
     const double dt = *dtp;
     const bool live = c < m.no_cells && m.material[c] == 0;
-    const int32_t k0 = m.c2f_ptr[c], k1 = m.c2f_ptr[c + 1];
+    const int32_t k0 = NF ? NF * c : m.c2f_ptr[c], k1 = NF ? NF * c + NF : m.c2f_ptr[c + 1];
     const double V = m.cell_volume[c];
-    for (int g = 0; g < ng; ++g)
     {
         const int s = s0 + g;
         double u[5];
@@ -164,16 +168,37 @@ __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s
         if (live)
         {
             double r[5] = {0, 0, 0, 0, 0};
-            for (int32_t k = k0; k < k1; ++k)
+            if constexpr (NF == 4)
             {
-                const int32_t f = m.cfa_idx[k];
-                const bool out = m.cfa_sgn[k] > 0;
-                for (int q = 0; q < 5; ++q)
-                {
-                    const double v = F[(g * 5 + q) * nf + f] / V;
-                    r[q] = out ? r[q] - v : r[q] + v;
-                }
+                const int4 fi = *reinterpret_cast<const int4 *>(m.cfa_idx + k0);
+                const char4 sg = *reinterpret_cast<const char4 *>(m.cfa_sgn + k0);
+                const int32_t ff[4] = {fi.x, fi.y, fi.z, fi.w};
+                const bool out[4] = {sg.x > 0, sg.y > 0, sg.z > 0, sg.w > 0};
+                double Fv[4][5];
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int q = 0; q < 5; ++q) Fv[j][q] = F[(g * 5 + q) * nf + ff[j]];
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int q = 0; q < 5; ++q)
+                    {
+                        const double v = Fv[j][q] / V;
+                        r[q] = out[j] ? r[q] - v : r[q] + v;
+                    }
             }
+            else
+                for (int32_t k = k0; k < k1; ++k)
+                {
+                    const int32_t f = m.cfa_idx[k];
+                    const bool out = m.cfa_sgn[k] > 0;
+                    for (int q = 0; q < 5; ++q)
+                    {
+                        const double v = F[(g * 5 + q) * nf + f] / V;
+                        r[q] = out ? r[q] - v : r[q] + v;
+                    }
+                }
             for (int q = 0; q < 5; ++q) u[q] += dt * r[q];
             const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
             if (!(u[0] >= p.rho_floor)) to_cons5(Prim5{p.rho_floor, 0, 0, 0, p.p_floor}, p.gamma, u);
@@ -229,67 +254,6 @@ __global__ void k_cell_vector_all(MeshView m, const double *__restrict__ flux, d
 }
 } // namespace
 } // namespace mhd
-
-namespace mhd
-{
-// Kernel classes of the step, timed with CUDA events on the handle's stream when profiling is on.
-enum StepKernel { KP_PREPARE = 0, KP_CFL, KP_GRAD, KP_FLUX, KP_UPDATE, KP_FACE_CAND, KP_EDGE_EMF, KP_CT, KP_COUNT };
-static const char *const kStepKernelNames[KP_COUNT] = {"prepare", "cfl", "limited_gradients", "face_flux",
-                                                        "update",  "face_candidate", "edge_emf", "ct"};
-
-struct Profiler
-{
-    bool on = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KP_COUNT];
-    size_t used[KP_COUNT] = {};
-    ~Profiler()
-    {
-        for (auto &v : ev)
-            for (auto &p : v)
-            {
-                cudaEventDestroy(p.first);
-                cudaEventDestroy(p.second);
-            }
-    }
-    void begin(int k, cudaStream_t s)
-    {
-        if (!on) return;
-        if (used[k] == ev[k].size())
-        {
-            cudaEvent_t a, b;
-            MHD_CUDA(cudaEventCreate(&a));
-            MHD_CUDA(cudaEventCreate(&b));
-            ev[k].emplace_back(a, b);
-        }
-        MHD_CUDA(cudaEventRecord(ev[k][used[k]].first, s));
-    }
-    void end(int k, cudaStream_t s)
-    {
-        if (!on) return;
-        MHD_CUDA(cudaEventRecord(ev[k][used[k]].second, s));
-        ++used[k];
-    }
-};
-} // namespace mhd
-
-struct MhdState
-{
-    MhdMesh *mesh = nullptr;
-    MhdStepParams prm{};
-    mhd::FluidParams fp{};
-    int nsp = 0, group = 0;
-    mhd::DBuf<double> U0, U1, W, grad, F, phi0, phi1, phi_add, badd, bind, btot, up, Ef, E, mass, stage;
-    mhd::DBuf<double> scal; // [0] dt
-    mhd::DBuf<unsigned long long> dt_bits;
-    mhd::DBuf<int> flag;
-    double *pinned = nullptr;
-    int64_t launches = 0; // kernels launched by the step since creation
-    mhd::Profiler prof;
-    ~MhdState()
-    {
-        if (pinned) cudaFreeHost(pinned);
-    }
-};
 
 namespace mhd
 {
@@ -349,8 +313,13 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
         if (m.nc)
         {
             P.begin(KP_UPDATE, s);
-            k_update<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
-                                                         stage2 ? 1 : 0);
+            const dim3 grid(grid_for(m.nc, 128), ng);
+            if (m.faces_per_cell == 4)
+                k_update<4><<<grid, 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
+                                                 stage2 ? 1 : 0);
+            else
+                k_update<0><<<grid, 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
+                                                 stage2 ? 1 : 0);
             MHD_LAUNCH_CHECK();
             P.end(KP_UPDATE, s);
         }
@@ -440,6 +409,14 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         st->flag.alloc(1);
         st->mass.upload(p->mass, st->nsp);
         MHD_CUDA(cudaMallocHost(&st->pinned, 8 * sizeof(double)));
+        MHD_REQUIRE(p->precision == MHD_PREC_FP64 || p->precision == MHD_PREC_MIXED, "unknown precision");
+        st->mixed = p->precision == MHD_PREC_MIXED;
+        if (st->mixed)
+        {
+            MHD_REQUIRE(m.faces_per_cell == 4, "mixed precision needs a tetrahedral mesh");
+            MHD_REQUIRE(m.max_valence <= 8, "mixed precision needs edge valence <= 8");
+            mixed_setup(st);
+        }
         cudaStream_t s = mesh->stream;
         if (nc) MHD_CUDA(cudaMemsetAsync(st->U0.p, 0, 5 * nc * st->nsp * sizeof(double), s));
         if (nf)
@@ -487,6 +464,7 @@ int mhd_gpu_state_upload(MhdState *st, int32_t field, int32_t species, const dou
             // BaddCell = reconstruct_cell_vector(PhiAdd) (MercuryUns/initial/Initial.cpp:82-83)
             if (m.nc) k_cell_vector_all<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->phi_add.p, st->badd.p);
             MHD_LAUNCH_CHECK();
+            if (st->mixed) mixed_badd(st);
         }
         else
             MHD_REQUIRE(false, "unknown field");
@@ -567,8 +545,16 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
             MHD_LAUNCH_CHECK();
             ++st->launches;
         }
-        stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl, dt_max);
-        stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
+        if (st->mixed)
+        {
+            mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl, dt_max);
+            mixed_stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
+        }
+        else
+        {
+            stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl, dt_max);
+            stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
+        }
         if (dt_used) read_dt(st, dt_used);
     });
 }

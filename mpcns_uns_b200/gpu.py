@@ -46,10 +46,11 @@ class StepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
                 ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("cfl", dbl), ("inver_MA2", dbl),
                 ("rho_floor_dt", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", Prim * 16),
-                ("absorb", ctypes.c_int8 * 16)]
+                ("absorb", ctypes.c_int8 * 16), ("precision", i32)]
 
 
 FIELD_U, FIELD_PHI, FIELD_PHIADD, FIELD_BADD = 0, 1, 2, 3
+PREC_FP64, PREC_MIXED = 0, 1
 
 _SIGS = {
     "mhd_gpu_last_error": ([], ctypes.c_char_p),
@@ -303,9 +304,10 @@ class DeviceMesh:
 
 def step_params(n_species, gamma=5.0 / 3.0, fs=None, mass=None, u_inf=(0.0, 0.0, 0.0), B_imf=(0.0, 0.0, 0.0), cuct=0.5,
                 second_order=True, rho_floor=1e-10, p_floor=1e-12, rel_limit=0.0, cfl=0.4, inver_MA2=1.0, rho_floor_dt=1e-2,
-                M_ref=1.0, ne_floor=0.01, absorb=None):
+                M_ref=1.0, ne_floor=0.01, absorb=None, precision="fp64"):
     """MhdStepParams with the reference's Config / Scales defaults (Common/config/Config.h:19-96)."""
     p = StepParams()
+    p.precision = PREC_MIXED if precision == "mixed" else PREC_FP64
     p.n_species, p.second_order = int(n_species), int(bool(second_order))
     p.gamma, p.rho_floor, p.p_floor, p.cuct = gamma, rho_floor, p_floor, cuct
     p.M_ref, p.ne_floor, p.rel_limit = M_ref, ne_floor, rel_limit

@@ -1,0 +1,42 @@
+"""Mixed-precision step (FP32 bulk, FP64 state / face fluxes / CT) against the FP64 GPU oracle.
+
+The FP64 path is itself pinned to the reference (test_gpu_step.py).  Tolerances, stated per
+quantity: relative L2 state error <= 1e-5 after the steps run here, div B at FP64 round-off
+(max relative |d2 Phi| <= 1e-12), which the FP64 CT update guarantees for any edge EMF.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+L2_TOL = 1e-5
+DIVB_TOL = 1e-12
+
+
+def _run(wl, precision, nsteps):
+    from mpcns_uns_b200 import gpu
+    dm = gpu.DeviceMesh(wl.mesh)
+    p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, precision=precision)
+    st = gpu.ResidentState(dm, p)
+    st.set(wl.U, wl.Phi, wl.PhiAdd)
+    dts = [st.step(0.0) for _ in range(nsteps)]
+    return [st.U(s) for s in range(wl.n_species)], st.Phi(), dts, dm
+
+
+def _l2(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("case", ["shell", "box"])
+def test_mixed_vs_fp64(case):
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(6, 8) if case == "shell" else workloads.box(8)
+    n = 20
+    U64, P64, dt64, dm = _run(wl, "fp64", n)
+    U32, P32, dt32, _ = _run(wl, "mixed", n)
+    assert np.allclose(dt32, dt64, rtol=1e-5)
+    for s in range(wl.n_species):
+        e = _l2(U32[s], U64[s])
+        assert e < L2_TOL, (s, e)
+    dP = np.linalg.norm(P32 - P64) / max(np.linalg.norm(P64 + wl.PhiAdd), 1e-300)
+    assert dP < L2_TOL
+    assert dm.div_b(P32)["max_rel"] < DIVB_TOL
