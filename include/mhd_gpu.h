@@ -107,6 +107,21 @@ int mhd_gpu_faraday_edge_dt(MhdMesh *mesh, const double *E, const double *dt_edg
  * host_out[0] = max |d2 B|, host_out[1] = max relative, host_out[2] = id of the worst cell. */
 int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *host_out);
 
+/* The div B diagnostic of mhd_gpu_div_b for callers that cannot allocate device memory: code
+ * running inside a CUDA stream capture, under an external memory budget or pool that forbids
+ * cudaMalloc, or in a host that must not grow its footprint after start-up.  This entry point
+ * has no counterpart in the reference.  It calls no cudaMalloc / cudaFree and no allocating
+ * library routine: its block partials and result live in one static device array of
+ * MHD_NOALLOC_DIVB_MAX_BLOCKS partials (1.5 MiB), which every GPU that loads this library holds
+ * until the process exits.  One block reduces 1024 cells, so a mesh may have at most
+ * MHD_NOALLOC_DIVB_MAX_BLOCKS * 1024 owned cells; larger meshes are rejected with MHD_EINVAL.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current; make that first call before any stream capture.  Every call overwrites
+ * the partials it reads, so nothing has to start at zero; calls that overlap on the GPU (other
+ * streams, other threads) share the array and race.  Results equal mhd_gpu_div_b's. */
+#define MHD_NOALLOC_DIVB_MAX_BLOCKS 65536
+int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, double *host_out);
+
 /* mhd::cell_current (Common/induction/Current.cpp:9-31): B 3 per cell -> J 3 per cell. */
 int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);
 

@@ -3,6 +3,8 @@
 // UCT edge EMF, boundary edge values, constrained transport (FP64) and the div B diagnostic.
 // FP64, reference-exact (see fluid.cu): no multiply-add contraction, reference operation order.
 #include <cfloat>
+#include <mutex>
+#include <vector>
 
 #include "induction.cuh"
 #include "kernels.cuh"
@@ -307,6 +309,57 @@ __global__ void k_cell_current(MeshView m, const double *__restrict__ B, double 
 }
 
 int div_b_blocks(const MeshView &m) { return static_cast<int>(std::min<int64_t>(grid_for(m.no_cells, 256), 4 * 148)); }
+
+// ---------------------------------------------------------------- div B without allocation
+// Static scratch of mhd_gpu_div_b_noalloc: MHD_NOALLOC_DIVB_MAX_BLOCKS block partials, then the
+// 3-value result.  Host code must not take this name as a device address: the address comes from
+// cudaGetSymbolAddress (noalloc_scratch below), per device.
+constexpr int kNoAllocCellsPerBlock = 1024; // 256 threads x 4 cells
+static __device__ __align__(256) double g_divb_scratch[3 * MHD_NOALLOC_DIVB_MAX_BLOCKS + 4];
+
+// one partial per block of 1024 consecutive owned cells (no grid-stride: the block count is the
+// scratch index, bounded by the mesh-size check of the entry point)
+__global__ void __launch_bounds__(256) k_div_b_block(MeshView m, const double *__restrict__ B, const double *__restrict__ extra,
+                                                      DivPart *__restrict__ part)
+{
+    DivPart v{0.0, -1.0, 0.0};
+    const int64_t base = (int64_t)blockIdx.x * kNoAllocCellsPerBlock;
+    for (int i = 0; i < kNoAllocCellsPerBlock / 256; ++i)
+    {
+        const int64_t cc = base + i * 256 + threadIdx.x;
+        if (cc >= m.no_cells) break;
+        const int32_t c = static_cast<int32_t>(cc);
+        double s = 0, a = 0;
+        for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m.c2f_idx[k];
+            s += m.c2f_sgn[k] * B[f];
+            a += fabs(B[f]) + (extra ? fabs(extra[f]) : 0.0);
+        }
+        const double rel = a > 0 ? fabs(s) / a : 0.0;
+        div_combine(v, DivPart{fabs(s), fabs(s) > 0 ? double(c) : -1.0, rel});
+    }
+    v = div_block_reduce(v);
+    if (threadIdx.x == 0) part[blockIdx.x] = v;
+}
+
+// Device address of g_divb_scratch on the current device, looked up once per device.
+double *noalloc_scratch()
+{
+    static std::mutex mu;
+    static std::vector<double *> addr;
+    int dev = 0;
+    MHD_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    if (static_cast<int>(addr.size()) <= dev) addr.resize(dev + 1, nullptr);
+    if (!addr[dev])
+    {
+        void *p = nullptr;
+        MHD_CUDA(cudaGetSymbolAddress(&p, g_divb_scratch));
+        addr[dev] = static_cast<double *>(p);
+    }
+    return addr[dev];
+}
 } // namespace mhd
 
 using namespace mhd;
@@ -396,6 +449,39 @@ int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *h
         MHD_LAUNCH_CHECK();
         k_div_b_final<<<1, 1024, 0, mesh->stream>>>(part, nb, res);
         MHD_LAUNCH_CHECK();
+        MHD_CUDA(cudaMemcpyAsync(mesh->pinned, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, mesh->stream));
+        MHD_CUDA(cudaStreamSynchronize(mesh->stream));
+        host_out[0] = mesh->pinned[0];
+        host_out[1] = mesh->pinned[1];
+        host_out[2] = mesh->pinned[2];
+    });
+}
+
+int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, double *host_out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && B && host_out, "bad argument");
+        const MeshView &m = mesh->v;
+        if (!m.no_cells)
+        {
+            host_out[0] = host_out[1] = 0.0;
+            host_out[2] = -1.0;
+            return;
+        }
+        const int64_t nb = (static_cast<int64_t>(m.no_cells) + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock;
+        MHD_REQUIRE(nb <= MHD_NOALLOC_DIVB_MAX_BLOCKS,
+                    "div_b_noalloc: the static scratch holds " + std::to_string(MHD_NOALLOC_DIVB_MAX_BLOCKS) +
+                        " block partials, i.e. at most " +
+                        std::to_string(static_cast<int64_t>(MHD_NOALLOC_DIVB_MAX_BLOCKS) * kNoAllocCellsPerBlock) +
+                        " owned cells; this mesh has " + std::to_string(m.no_cells));
+        double *scratch = noalloc_scratch();
+        DivPart *part = reinterpret_cast<DivPart *>(scratch);
+        double *res = scratch + 3 * MHD_NOALLOC_DIVB_MAX_BLOCKS;
+        k_div_b_block<<<static_cast<int>(nb), 256, 0, mesh->stream>>>(m, B, extra, part);
+        MHD_LAUNCH_CHECK();
+        k_div_b_final<<<1, 1024, 0, mesh->stream>>>(part, static_cast<int>(nb), res);
+        MHD_LAUNCH_CHECK();
+        // into the handle's pinned buffer, allocated when the mesh was created
         MHD_CUDA(cudaMemcpyAsync(mesh->pinned, res, 3 * sizeof(double), cudaMemcpyDeviceToHost, mesh->stream));
         MHD_CUDA(cudaStreamSynchronize(mesh->stream));
         host_out[0] = mesh->pinned[0];
