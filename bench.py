@@ -199,6 +199,16 @@ def time_reference(wl, steps, warmup):
     return wl.mesh.n_cells * wl.n_species * 2 / per_step, per_step
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's device time: every rank's K steps count once, the job ends with the last."""
+    if dist is None:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 # ------------------------------------------------------------------ main
 def main():
     ap = argparse.ArgumentParser()
@@ -285,10 +295,8 @@ def main():
         prof = st.profile_read()
         st.profile(False)
         launches = st.launches() - l0
+        ms = max_over_ranks(ms, dist, "cuda")
         if dist:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
             dist.barrier()
         if not np.isfinite(st.cfl_dt()):
             raise RuntimeError("state became invalid")

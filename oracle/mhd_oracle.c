@@ -1,0 +1,891 @@
+/* CPU restatement of the reference's hot path (TEST INFRASTRUCTURE ONLY; see mhd_oracle.h).
+ * Plain C11, the reference's operation order, no fused multiply-add (x86-64 baseline): on the same
+ * inputs the results equal the compiled reference's bit for bit, which tests/test_oracle.py checks. */
+#include "mhd_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct { double x, y, z; } v3;
+static inline v3 mk3(double x, double y, double z) { v3 r = {x, y, z}; return r; }
+static inline v3 ld(const double *a, int64_t i) { return mk3(a[3 * i], a[3 * i + 1], a[3 * i + 2]); }
+static inline v3 add3(v3 a, v3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub3(v3 a, v3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 scl(double s, v3 a) { return mk3(a.x * s, a.y * s, a.z * s); }
+static inline double dot3(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 cross3(v3 a, v3 b) { return mk3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline double dmax(double a, double b) { return (a < b) ? b : a; } /* std::max */
+static inline double dmin(double a, double b) { return (b < a) ? b : a; } /* std::min */
+
+/* mhd::to_prim (Common/physics/Euler.h:13-21) */
+static OrPrim to_prim1(const double *U, double gamma, double rho_floor, double p_floor)
+{
+    OrPrim W;
+    W.rho = dmax(U[0], rho_floor);
+    W.u = U[1] / W.rho; W.v = U[2] / W.rho; W.w = U[3] / W.rho;
+    const double ke = 0.5 * W.rho * (W.u * W.u + W.v * W.v + W.w * W.w);
+    W.p = dmax((gamma - 1.0) * (U[4] - ke), p_floor);
+    return W;
+}
+
+/* mhd::to_cons (Euler.h:22-26) */
+static void to_cons1(OrPrim W, double gamma, double *U)
+{
+    U[0] = W.rho; U[1] = W.rho * W.u; U[2] = W.rho * W.v; U[3] = W.rho * W.w;
+    U[4] = W.p / (gamma - 1.0) + 0.5 * W.rho * (W.u * W.u + W.v * W.v + W.w * W.w);
+}
+
+void or_to_prim(const double *U, int64_t n, double gamma, double rho_floor, double p_floor, double *W)
+{
+    for (int64_t c = 0; c < n; ++c)
+    {
+        const OrPrim w = to_prim1(U + 5 * c, gamma, rho_floor, p_floor);
+        W[5 * c] = w.rho; W[5 * c + 1] = w.u; W[5 * c + 2] = w.v; W[5 * c + 3] = w.w; W[5 * c + 4] = w.p;
+    }
+}
+
+/* mhd::ghost_state (Common/fluid/Reconstruction.cpp:9-24); kind 1 wall, 2 inflow */
+static OrPrim ghost(int kind, int absorb, OrPrim in, v3 n, OrPrim fs)
+{
+    if (kind == 1)
+    {
+        if (absorb) { OrPrim g = {1e-12, 0, 0, 0, 1e-12}; return g; }
+        const double un = in.u * n.x + in.v * n.y + in.w * n.z;
+        OrPrim g = in;
+        g.u -= 2 * un * n.x; g.v -= 2 * un * n.y; g.w -= 2 * un * n.z;
+        return g;
+    }
+    if (kind == 2) return fs;
+    return in;
+}
+
+static int f2c_count(const OrMesh *m, int32_t f) { return (int)(m->f2c_ptr[f + 1] - m->f2c_ptr[f]); }
+
+/* mhd::Stencil::Stencil + limited_gradients (Common/fluid/Reconstruction.cpp:26-78, :80-142).  The
+ * stencil of each cell is rebuilt here with the constructor's arithmetic (the reference keeps it). */
+void or_limited_gradients(const OrMesh *m, const double *W, int32_t absorb, const OrPrim *fs, int32_t limit, double rel_limit, double *grad)
+{
+    memset(grad, 0, sizeof(double) * 15 * (size_t)m->n_cells);
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        if (m->cell_material[c] == 1) continue;
+        const int64_t k0 = m->c2f_ptr[c], k1 = m->c2f_ptr[c + 1];
+        double M[3][3] = {{0}}, wk[64], dk[64][3];
+        int32_t nbk[64];
+        int64_t kk_of[64];
+        int ns = 0;
+        const v3 xc = ld(m->cell_center, c);
+        for (int64_t k = k0; k < k1; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            const int kind = m->face_kind[f];
+            if (kind == 4) continue;
+            v3 d;
+            int32_t nb;
+            if (f2c_count(m, f) == 2 && kind == 0)
+            {
+                const int64_t p0 = m->f2c_ptr[f];
+                nb = m->f2c_idx[p0] == c ? m->f2c_idx[p0 + 1] : m->f2c_idx[p0];
+                d = sub3(ld(m->cell_center, nb), xc);
+            }
+            else
+            {
+                const v3 n = scl(m->c2f_sgn[k] / m->face_area_mag[f], ld(m->face_area, f));
+                d = scl(2.0 * dot3(sub3(ld(m->face_center, f), xc), n), n);
+                nb = -(f + 1);
+            }
+            const double w = 1.0 / dot3(d, d);
+            nbk[ns] = nb; wk[ns] = w; dk[ns][0] = d.x; dk[ns][1] = d.y; dk[ns][2] = d.z; kk_of[ns] = k;
+            ++ns;
+            for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) M[a][b] += w * dk[ns - 1][a] * dk[ns - 1][b];
+        }
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        const double sc = dmax(dmax(dmax(M[0][0], M[1][1]), M[2][2]), 1e-300);
+        if (fabs(det) < 1e-9 * sc * sc * sc) continue;
+        double I[9];
+        I[0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
+        I[1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        I[2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
+        I[3] = I[1];
+        I[4] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
+        I[5] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        I[6] = I[2];
+        I[7] = I[5];
+        I[8] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+        const double *wp = W + 5 * (int64_t)c;
+        const OrPrim wc = {wp[0], wp[1], wp[2], wp[3], wp[4]};
+        const double wcv[5] = {wc.rho, wc.u, wc.v, wc.w, wc.p};
+        double r[5][3] = {{0}}, lo[5], hi[5];
+        for (int q = 0; q < 5; ++q) lo[q] = hi[q] = wcv[q];
+        for (int i = 0; i < ns; ++i)
+        {
+            OrPrim wn;
+            if (nbk[i] >= 0)
+            {
+                const double *np = W + 5 * (int64_t)nbk[i];
+                wn.rho = np[0]; wn.u = np[1]; wn.v = np[2]; wn.w = np[3]; wn.p = np[4];
+            }
+            else
+            {
+                const int32_t f = -(nbk[i] + 1);
+                const v3 n = scl(m->c2f_sgn[kk_of[i]] / m->face_area_mag[f], ld(m->face_area, f));
+                wn = ghost(m->face_kind[f], absorb, wc, n, *fs);
+            }
+            const double wnv[5] = {wn.rho, wn.u, wn.v, wn.w, wn.p};
+            for (int q = 0; q < 5; ++q)
+            {
+                const double dq = wnv[q] - wcv[q];
+                r[q][0] += wk[i] * dk[i][0] * dq; r[q][1] += wk[i] * dk[i][1] * dq; r[q][2] += wk[i] * dk[i][2] * dq;
+                lo[q] = dmin(lo[q], wnv[q]);
+                hi[q] = dmax(hi[q], wnv[q]);
+            }
+        }
+        for (int q = 0; q < 5; ++q)
+        {
+            const double g[3] = {I[0] * r[q][0] + I[1] * r[q][1] + I[2] * r[q][2], I[3] * r[q][0] + I[4] * r[q][1] + I[5] * r[q][2],
+                                 I[6] * r[q][0] + I[7] * r[q][1] + I[8] * r[q][2]};
+            double psi = 1.0;
+            if (limit)
+                for (int64_t kf = k0; kf < k1; ++kf)
+                {
+                    const v3 dx = sub3(ld(m->face_center, m->c2f_idx[kf]), xc);
+                    const double dl = g[0] * dx.x + g[1] * dx.y + g[2] * dx.z;
+                    if (dl > 1e-300) psi = dmin(psi, (hi[q] - wcv[q]) / dl);
+                    else if (dl < -1e-300) psi = dmin(psi, (lo[q] - wcv[q]) / dl);
+                }
+            if (limit && rel_limit > 0 && (q == 0 || q == 4))
+                for (int64_t kf = k0; kf < k1; ++kf)
+                {
+                    const v3 dx = sub3(ld(m->face_center, m->c2f_idx[kf]), xc);
+                    const double dl = fabs(g[0] * dx.x + g[1] * dx.y + g[2] * dx.z);
+                    if (dl > 1e-300) psi = dmin(psi, rel_limit * wcv[q] / dl);
+                }
+            psi = dmax(0.0, dmin(1.0, psi));
+            double *out = grad + 15 * (int64_t)c + 3 * q;
+            out[0] = psi * g[0]; out[1] = psi * g[1]; out[2] = psi * g[2];
+        }
+    }
+}
+
+/* face_state of Common/fluid/FluxRHS.cpp:16-27 */
+static OrPrim face_state(const double *W, const double *grad, int32_t c, v3 dx)
+{
+    const double *w = W + 5 * (int64_t)c, *g = grad + 15 * (int64_t)c;
+    OrPrim wc = {w[0], w[1], w[2], w[3], w[4]}, r;
+    r.rho = wc.rho + g[0] * dx.x + g[1] * dx.y + g[2] * dx.z;
+    r.u = wc.u + g[3] * dx.x + g[4] * dx.y + g[5] * dx.z;
+    r.v = wc.v + g[6] * dx.x + g[7] * dx.y + g[8] * dx.z;
+    r.w = wc.w + g[9] * dx.x + g[10] * dx.y + g[11] * dx.z;
+    r.p = wc.p + g[12] * dx.x + g[13] * dx.y + g[14] * dx.z;
+    return (r.rho > 0 && r.p > 0) ? r : wc;
+}
+
+/* mhd::rusanov (Common/physics/Euler.h:30-49) */
+static void rusanov(OrPrim L, OrPrim R, const double n[3], double gamma, double *F)
+{
+    double UL[5], UR[5], FL[5], FR[5];
+    to_cons1(L, gamma, UL);
+    to_cons1(R, gamma, UR);
+    const OrPrim *Ws[2] = {&L, &R};
+    double *Us[2] = {UL, UR}, *Fs[2] = {FL, FR};
+    for (int i = 0; i < 2; ++i)
+    {
+        const OrPrim W = *Ws[i];
+        const double un = W.u * n[0] + W.v * n[1] + W.w * n[2];
+        Fs[i][0] = W.rho * un;
+        Fs[i][1] = W.rho * un * W.u + W.p * n[0];
+        Fs[i][2] = W.rho * un * W.v + W.p * n[1];
+        Fs[i][3] = W.rho * un * W.w + W.p * n[2];
+        Fs[i][4] = un * (Us[i][4] + W.p);
+    }
+    const double sL = fabs(L.u * n[0] + L.v * n[1] + L.w * n[2]) + sqrt(gamma * L.p / L.rho);
+    const double sR = fabs(R.u * n[0] + R.v * n[1] + R.w * n[2]) + sqrt(gamma * R.p / R.rho);
+    const double s = dmax(sL, sR);
+    for (int q = 0; q < 5; ++q) F[q] = 0.5 * (FL[q] + FR[q]) - 0.5 * s * (UR[q] - UL[q]);
+}
+
+/* mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:30-74) */
+void or_flux_rhs(const OrMesh *m, double gamma, int32_t absorb, const OrPrim *fs, const double *W, const double *grad, double *rhs)
+{
+    const int32_t no = m->n_owned_cells;
+    memset(rhs, 0, sizeof(double) * 5 * (size_t)m->n_cells);
+    for (int32_t f = 0; f < m->n_faces; ++f)
+    {
+        const int kind = m->face_kind[f];
+        if (kind == 4) continue;
+        const int64_t k0 = m->f2c_ptr[f];
+        const int nc = f2c_count(m, f);
+        int any = 0;
+        for (int q = 0; q < nc; ++q) any |= m->f2c_idx[k0 + q] < no && m->cell_material[m->f2c_idx[k0 + q]] == 0;
+        if (!any) continue;
+        const double A = m->face_area_mag[f];
+        const v3 n = scl(1.0 / A, ld(m->face_area, f));
+        const double nv[3] = {n.x, n.y, n.z};
+        const v3 xf = ld(m->face_center, f);
+        OrPrim L, R;
+        int32_t cL = -1, cR = -1;
+        if (nc == 2 && kind == 0)
+        {
+            cL = m->f2c_idx[k0]; cR = m->f2c_idx[k0 + 1];
+            if (m->f2c_sgn[k0] < 0) { const int32_t t = cL; cL = cR; cR = t; }
+            L = face_state(W, grad, cL, sub3(xf, ld(m->cell_center, cL)));
+            R = face_state(W, grad, cR, sub3(xf, ld(m->cell_center, cR)));
+        }
+        else
+        {
+            int32_t c = m->f2c_idx[k0];
+            int sgn = m->f2c_sgn[k0];
+            if (nc == 2 && m->cell_material[c] == 1) { c = m->f2c_idx[k0 + 1]; sgn = m->f2c_sgn[k0 + 1]; }
+            const OrPrim in = face_state(W, grad, c, sub3(xf, ld(m->cell_center, c)));
+            const OrPrim gh = ghost(kind, absorb, in, scl((double)sgn, n), *fs);
+            if (sgn > 0) { cL = c; L = in; R = gh; }
+            else { cR = c; R = in; L = gh; }
+        }
+        double F[5];
+        rusanov(L, R, nv, gamma, F);
+        for (int q = 0; q < 5; ++q) F[q] *= A;
+        if (cL >= 0 && cL < no)
+            for (int q = 0; q < 5; ++q) rhs[5 * (int64_t)cL + q] -= F[q] / m->cell_volume[cL];
+        if (cR >= 0 && cR < no)
+            for (int q = 0; q < 5; ++q) rhs[5 * (int64_t)cR + q] += F[q] / m->cell_volume[cR];
+    }
+}
+
+/* uns::reconstruct_cell_vector (src/uns/geometry/Reconstruct.cpp:8-46) */
+void or_cell_vector(const OrMesh *m, const double *flux, int32_t ncells, double *out)
+{
+    for (int32_t c = 0; c < ncells; ++c)
+    {
+        double M[3][3] = {{0}}, r[3] = {0, 0, 0};
+        out[3 * (int64_t)c] = out[3 * (int64_t)c + 1] = out[3 * (int64_t)c + 2] = 0.0;
+        for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            const double A = m->face_area_mag[f];
+            if (A <= 0) continue;
+            const v3 n = scl(m->c2f_sgn[k] / A, ld(m->face_area, f));
+            const double nv[3] = {n.x, n.y, n.z};
+            const double phi = m->c2f_sgn[k] * flux[f];
+            for (int i = 0; i < 3; ++i)
+            {
+                r[i] += nv[i] * phi;
+                for (int j = 0; j < 3; ++j) M[i][j] += A * nv[i] * nv[j];
+            }
+        }
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        const double sc = dmax(dmax(dmax(M[0][0], M[1][1]), M[2][2]), 1e-300);
+        if (fabs(det) < 1e-12 * sc * sc * sc) continue;
+        double I[3][3];
+        I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det;
+        I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det;
+        I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+        I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det;
+        I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det;
+        I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+        I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+        for (int a = 0; a < 3; ++a) out[3 * (int64_t)c + a] = I[a][0] * r[0] + I[a][1] * r[1] + I[a][2] * r[2];
+    }
+}
+
+/* mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:25-129), adds into E */
+void or_ideal_emf(const OrMesh *m, const double *u, const double *Bt, const double *Bi, const double *phi_tot, const double *phi_ind,
+                  double cuct, double *E)
+{
+    double *Ef = (double *)malloc(sizeof(double) * 3 * (size_t)(m->n_faces > 0 ? m->n_faces : 1));
+    char *have = (char *)calloc((size_t)(m->n_faces > 0 ? m->n_faces : 1), 1);
+    for (int32_t e = 0; e < m->n_owned_edges; ++e)
+    {
+        const int64_t f0 = m->e2f_ptr[e], f1 = m->e2f_ptr[e + 1];
+        const int nf = (int)(f1 - f0);
+        if (nf == 0 || m->edge_len[e] <= 0) continue;
+        int any = 0;
+        for (int64_t k = m->ec_ptr[e]; k < m->ec_ptr[e + 1] && !any; ++k) any = m->cell_material[m->ec_cell[k]] == 0;
+        if (!any) continue;
+        const v3 t = ld(m->edge_vec, e);
+        const double L = m->edge_len[e];
+        const v3 th = scl(1.0 / L, t);
+        double Ec = 0, w[64], aef[64];
+        v3 mm[64], nrm[64];
+        for (int i = 0; i < nf; ++i)
+        {
+            const int32_t f = m->e2f_idx[f0 + i];
+            if (!have[f])
+            {
+                /* face candidate (:32-55) */
+                have[f] = 1;
+                const double A = m->face_area_mag[f];
+                const v3 n = scl(1.0 / A, ld(m->face_area, f));
+                const double Bn = phi_tot[f] / A;
+                const int64_t p0 = m->f2c_ptr[f];
+                v3 F;
+                if (f2c_count(m, f) == 2)
+                {
+                    int32_t cl = m->f2c_idx[p0], cr = m->f2c_idx[p0 + 1];
+                    if (m->f2c_sgn[p0] < 0) { const int32_t tt = cl; cl = cr; cr = tt; }
+                    const v3 uL = ld(u, cl), uR = ld(u, cr);
+                    const double a = dmax(fabs(dot3(uL, n)), fabs(dot3(uR, n)));
+                    const v3 FL = sub3(scl(dot3(uL, n), ld(Bt, cl)), scl(Bn, uL));
+                    const v3 FR = sub3(scl(dot3(uR, n), ld(Bt, cr)), scl(Bn, uR));
+                    F = sub3(scl(0.5, add3(FL, FR)), scl(0.5 * a, sub3(ld(Bi, cr), ld(Bi, cl))));
+                }
+                else
+                {
+                    const int32_t c = m->f2c_idx[p0];
+                    const v3 uc = ld(u, c);
+                    F = sub3(scl(dot3(uc, n), ld(Bt, c)), scl(Bn, uc));
+                }
+                const v3 Ev = scl(-1.0, cross3(n, F));
+                Ef[3 * (int64_t)f] = Ev.x; Ef[3 * (int64_t)f + 1] = Ev.y; Ef[3 * (int64_t)f + 2] = Ev.z;
+            }
+            w[i] = m->ef_weight[f0 + i];
+            Ec += w[i] * dot3(ld(Ef, f), t);
+            v3 v = sub3(ld(m->face_center, f), ld(m->edge_mid, e));
+            v = sub3(v, scl(dot3(v, th), th));
+            const double nv = sqrt(dot3(v, v));
+            mm[i] = nv > 0 ? scl(1.0 / nv, v) : mk3(0, 0, 0);
+            nrm[i] = scl(1.0 / m->face_area_mag[f], ld(m->face_area, f));
+            aef[i] = 0.0;
+        }
+        for (int64_t k = m->ec_ptr[e]; k < m->ec_ptr[e + 1]; ++k)
+        {
+            const v3 uc = ld(u, m->ec_cell[k]);
+            for (int i = 0; i < nf; ++i) aef[i] = dmax(aef[i], fabs(dot3(uc, mm[i])));
+        }
+        const v3 ax = fabs(th.x) < 0.9 ? mk3(1, 0, 0) : mk3(0, 1, 0);
+        v3 e1 = cross3(th, ax);
+        e1 = scl(1.0 / sqrt(dot3(e1, e1)), e1);
+        const v3 e2 = cross3(th, e1);
+        double M11 = 0, M12 = 0, M22 = 0, g1 = 0, g2 = 0, qa[64], qb[64];
+        for (int i = 0; i < nf; ++i)
+        {
+            const v3 qv = scl(aef[i] * dot3(th, cross3(mm[i], nrm[i])), nrm[i]);
+            qa[i] = dot3(qv, e1);
+            qb[i] = dot3(qv, e2);
+            M11 += w[i] * qa[i] * qa[i];
+            M12 += w[i] * qa[i] * qb[i];
+            M22 += w[i] * qb[i] * qb[i];
+            g1 += w[i] * qa[i];
+            g2 += w[i] * qb[i];
+        }
+        const double tr = M11 + M22, eps = 1e-14 * tr, det = (M11 + eps) * (M22 + eps) - M12 * M12;
+        double l1 = 0, l2 = 0;
+        if (tr > 0 && det > 0)
+        {
+            l1 = ((M22 + eps) * g1 - M12 * g2) / det;
+            l2 = ((M11 + eps) * g2 - M12 * g1) / det;
+        }
+        double Eu = 0;
+        for (int i = 0; i < nf; ++i)
+        {
+            const int32_t f = m->e2f_idx[f0 + i];
+            const double omega = w[i] * (1.0 - (qa[i] * l1 + qb[i] * l2));
+            const double sig = dot3(th, cross3(mm[i], nrm[i]));
+            Eu += omega * aef[i] * sig * (phi_ind[f] / m->face_area_mag[f]);
+        }
+        E[e] += Ec + 2.0 * cuct * L * Eu;
+    }
+    free(Ef);
+    free(have);
+}
+
+/* boundary edge values of mercury::Solver::rhs (MercuryUns/driver/Solver.cpp:162-167) */
+void or_edge_modes(const OrMesh *m, const double *u_inf, const double *B_imf, double *E)
+{
+    const v3 Einf = scl(-1.0, cross3(mk3(u_inf[0], u_inf[1], u_inf[2]), mk3(B_imf[0], B_imf[1], B_imf[2])));
+    for (int32_t e = 0; e < m->n_owned_edges; ++e)
+    {
+        if (m->edge_mode[e] == 1) E[e] = 0.0;
+        else if (m->edge_mode[e] == 2) E[e] = dot3(Einf, ld(m->edge_vec, e));
+    }
+}
+
+/* mhd::faraday_update / faraday_update_edge_dt (Common/induction/Faraday.cpp:15-36) over active_faces (:7-13) */
+void or_faraday(const OrMesh *m, const double *E, const double *dt_edge, double dt, double *B)
+{
+    for (int32_t f = 0; f < m->n_faces; ++f)
+    {
+        int active = 0;
+        for (int64_t k = m->f2c_ptr[f]; k < m->f2c_ptr[f + 1]; ++k) active |= m->f2c_idx[k] < m->n_owned_cells;
+        if (!active) continue;
+        double circ = 0.0;
+        if (dt_edge)
+        {
+            for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) circ += m->f2e_sgn[k] * dt_edge[m->f2e_idx[k]] * E[m->f2e_idx[k]];
+            B[f] -= circ;
+        }
+        else
+        {
+            for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) circ += m->f2e_sgn[k] * E[m->f2e_idx[k]];
+            B[f] -= dt * circ;
+        }
+    }
+}
+
+/* mhd::div_b (Common/diagnostics/DivB.cpp:8-24): max_abs, max_rel, worst cell */
+void or_div_b(const OrMesh *m, const double *B, const double *extra, double *out3)
+{
+    double max_abs = 0, max_rel = 0, worst = -1;
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        double s = 0, a = 0;
+        for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            s += m->c2f_sgn[k] * B[f];
+            a += fabs(B[f]) + (extra ? fabs(extra[f]) : 0.0);
+        }
+        const double rel = a > 0 ? fabs(s) / a : 0.0;
+        if (fabs(s) > max_abs) { max_abs = fabs(s); worst = c; }
+        max_rel = dmax(max_rel, rel);
+    }
+    out3[0] = max_abs; out3[1] = max_rel; out3[2] = worst;
+}
+
+/* mhd::cell_current (Common/induction/Current.cpp:9-31) */
+void or_cell_current(const OrMesh *m, const double *B, double *J)
+{
+    memset(J, 0, sizeof(double) * 3 * (size_t)m->n_cells);
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        v3 sum = mk3(0, 0, 0);
+        const v3 bc = ld(B, c);
+        for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            v3 bf = bc;
+            const int64_t p0 = m->f2c_ptr[f];
+            if (f2c_count(m, f) == 2)
+            {
+                const int32_t o = m->f2c_idx[p0] == c ? m->f2c_idx[p0 + 1] : m->f2c_idx[p0];
+                bf = scl(0.5, add3(bc, ld(B, o)));
+            }
+            sum = add3(sum, cross3(scl((double)m->c2f_sgn[k], ld(m->face_area, f)), bf));
+        }
+        const double invV = 1.0 / m->cell_volume[c];
+        J[3 * (int64_t)c] = sum.x * invV; J[3 * (int64_t)c + 1] = sum.y * invV; J[3 * (int64_t)c + 2] = sum.z * invV;
+    }
+}
+
+/* mercury::cell_time_steps + local_time_step (MercuryUns/fluid/MercurySources.cpp:65-116) for n species
+ * (no gyration limit); the wave speeds use the summed density as the reference does for its two ions */
+double or_local_time_step(const OrMesh *m, int32_t ns, const double *const *W, const double *B, double gamma, double cfl, double inver_MA2,
+                          double rho_floor_dt)
+{
+    double gdt = INFINITY;
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        if (m->cell_material[c] == 1) continue;
+        double dt = INFINITY;
+        const v3 b = ld(B, c);
+        const double B2 = dot3(b, b);
+        double rs = W[0][5 * (int64_t)c];
+        for (int s = 1; s < ns; ++s) rs = rs + W[s][5 * (int64_t)c];
+        const double rho_tot = dmax(rs, rho_floor_dt);
+        for (int s = 0; s < ns; ++s)
+        {
+            const double *w = W[s] + 5 * (int64_t)c;
+            const double cs2 = gamma * w[4] / dmax(w[0], 1e-30);
+            double denom = 0;
+            for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+            {
+                const int32_t f = m->c2f_idx[k];
+                const double A = m->face_area_mag[f];
+                const v3 n = scl(1.0 / A, ld(m->face_area, f));
+                const double vA2 = inver_MA2 * B2 / rho_tot;
+                const double vAn2 = inver_MA2 * dot3(b, n) * dot3(b, n) / rho_tot;
+                const double term = cs2 + vA2;
+                const double cf = sqrt(0.5 * (term + sqrt(dmax(0.0, term * term - 4 * cs2 * vAn2))));
+                denom += (fabs(w[1] * n.x + w[2] * n.y + w[3] * n.z) + cf) * A;
+            }
+            if (denom > 0) dt = dmin(dt, cfl * m->cell_volume[c] / denom);
+        }
+        gdt = dmin(gdt, dt);
+    }
+    return gdt;
+}
+
+/* one SSP-RK2 step of the hot path: mercury::Solver::step (MercuryUns/driver/Solver.cpp:481-516) with
+ * prepare (:94-125, no current), rhs (:132-169, no model sources), advance (:194-206) and floors (:171-191) */
+static void floors(const OrMesh *m, const OrStepParams *p, double *const *U)
+{
+    for (int k = 0; k < p->n_species; ++k)
+        for (int32_t c = 0; c < m->n_owned_cells; ++c)
+        {
+            if (m->cell_material[c] == 1) continue;
+            double *u = U[k] + 5 * (int64_t)c;
+            const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
+            if (!(u[0] >= p->rho_floor)) { const OrPrim f = {p->rho_floor, 0, 0, 0, p->p_floor}; to_cons1(f, p->gamma, u); }
+            else if ((p->gamma - 1.0) * (u[4] - ke) < p->p_floor) to_cons1(to_prim1(u, p->gamma, p->rho_floor, p->p_floor), p->gamma, u);
+        }
+}
+
+int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
+{
+    const int32_t nc = m->n_cells, nf = m->n_faces, ne = m->n_edges, ns = p->n_species;
+    const size_t c5 = 5 * (size_t)nc;
+    double *mem = (double *)malloc(sizeof(double) * (ns * (5 + 15 + 5 + 5 + 5) * (size_t)nc + 9 * (size_t)nc + 3 * (size_t)nf + ne));
+    if (!mem) return -1;
+    double *W = mem, *G = W + ns * c5, *R = G + 3 * ns * c5, *U1 = R + ns * c5, *U2 = U1 + ns * c5;
+    double *Bi = U2 + ns * c5, *Bt = Bi + 3 * (size_t)nc, *up = Bt + 3 * (size_t)nc, *Pt = up + 3 * (size_t)nc, *P1 = Pt + nf, *P2 = P1 + nf;
+    double *E = P2 + nf;
+    double *Us[16], *U1s[16], *U2s[16];
+    for (int s = 0; s < ns; ++s) { Us[s] = U[s]; U1s[s] = U1 + s * c5; U2s[s] = U2 + s * c5; }
+    for (int st = 0; st < 2; ++st)
+    {
+        double *const *Ui = st == 0 ? Us : U1s;
+        double *const *Uo = st == 0 ? U1s : U2s;
+        const double *phis = st == 0 ? Phi : P1;
+        double *phio = st == 0 ? P1 : P2;
+        for (int s = 0; s < ns; ++s) or_to_prim(Ui[s], nc, p->gamma, p->rho_floor, p->p_floor, W + s * c5);
+        or_cell_vector(m, phis, nc, Bi);
+        for (int32_t c = 0; c < nc; ++c)
+        {
+            for (int a = 0; a < 3; ++a) Bt[3 * (int64_t)c + a] = Bi[3 * (int64_t)c + a] + BaddCell[3 * (int64_t)c + a];
+            double u3[3] = {0, 0, 0};
+            if (m->cell_material[c] == 0)
+            {
+                double nsv[16], ne_ = 0;
+                for (int s = 0; s < ns; ++s) { nsv[s] = dmax(W[s * c5 + 5 * (size_t)c], 0.0) / p->mass[s] * p->M_ref; ne_ += nsv[s]; }
+                for (int s = 0; s < ns; ++s)
+                {
+                    const double chi = ne_ > 1e-300 ? nsv[s] / ne_ : (s == 0 ? 1.0 : 0.0);
+                    for (int a = 0; a < 3; ++a) u3[a] += chi * W[s * c5 + 5 * (size_t)c + 1 + a];
+                }
+            }
+            for (int a = 0; a < 3; ++a) up[3 * (int64_t)c + a] = u3[a];
+        }
+        for (int32_t f = 0; f < nf; ++f) Pt[f] = phis[f] + PhiAdd[f];
+        for (int s = 0; s < ns; ++s)
+        {
+            if (p->second_order) or_limited_gradients(m, W + s * c5, p->absorb[s], &p->fs[s], 1, p->rel_limit, G + 3 * s * c5);
+            else memset(G + 3 * s * c5, 0, sizeof(double) * 3 * c5);
+            or_flux_rhs(m, p->gamma, p->absorb[s], &p->fs[s], W + s * c5, G + 3 * s * c5, R + s * c5);
+        }
+        memset(E, 0, sizeof(double) * (size_t)ne);
+        or_ideal_emf(m, up, Bt, Bi, Pt, phis, p->cuct, E);
+        or_edge_modes(m, p->u_inf, p->B_imf, E);
+        for (int s = 0; s < ns; ++s)
+        {
+            memcpy(Uo[s], Ui[s], sizeof(double) * c5);
+            for (int32_t c = 0; c < m->n_owned_cells; ++c)
+            {
+                if (m->cell_material[c] == 1) continue;
+                for (int q = 0; q < 5; ++q) Uo[s][5 * (size_t)c + q] += dt * R[s * c5 + 5 * (size_t)c + q];
+            }
+        }
+        memcpy(phio, phis, sizeof(double) * (size_t)nf);
+        or_faraday(m, E, NULL, dt, phio);
+        floors(m, p, Uo);
+    }
+    for (int s = 0; s < ns; ++s)
+        for (size_t i = 0; i < c5; ++i) U[s][i] = 0.5 * (U[s][i] + U2s[s][i]);
+    for (int32_t f = 0; f < nf; ++f) Phi[f] = 0.5 * (Phi[f] + P2[f]);
+    free(mem);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ semi-implicit induction
+ * mhd::ImplicitInduction (Common/induction/ImplicitInduction.cpp): constructor tables (:10-103),
+ * set_frozen_state (:105-111), apply_F (:127-183), apply_A (:185-198), dot_owned (:200-207) and the
+ * restarted GMRES(m) with modified Gram-Schmidt, Givens rotations and the Jacobi right
+ * preconditioner (:299-390).  The resistive coefficient m_e = eta_e / star1_e is an input (the
+ * reference fills it from its tanh window). */
+struct OrInduction
+{
+    const OrMesh *m;
+    OrIndParams p;
+    int resistive, hall;
+    double *m_edge, *taper, *alpha, *B0, *recon, *d2, *ce_wt, *corr;
+    int64_t *ce_ptr;
+    int32_t *ce_edge;
+    double *phi, *bcell, *part, *tmp;
+};
+
+static int cmp_i32(const void *a, const void *b)
+{
+    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+OrInduction *or_ind_create(const OrMesh *m, const OrIndParams *p, const double *m_edge)
+{
+    OrInduction *s = (OrInduction *)calloc(1, sizeof(OrInduction));
+    const int32_t ne = m->n_edges, nc = m->n_cells, no = m->n_owned_cells;
+    s->m = m;
+    s->p = *p;
+    s->hall = p->hall && p->hall_coef > 0;
+    s->m_edge = (double *)calloc((size_t)ne + 1, sizeof(double));
+    if (m_edge)
+        for (int32_t e = 0; e < ne; ++e) { s->m_edge[e] = m_edge[e]; s->resistive |= m_edge[e] != 0.0; }
+    s->taper = (double *)calloc((size_t)nc + 1, sizeof(double));
+    s->alpha = (double *)calloc((size_t)nc + 1, sizeof(double));
+    s->B0 = (double *)calloc(3 * (size_t)nc + 1, sizeof(double));
+    const double mid = 0.5 * (p->hall_r_min + p->hall_r_max), width = p->hall_r_max - p->hall_r_min;
+    for (int32_t c = 0; c < nc; ++c)
+    {
+        if (m->cell_material[c] == 1) continue;
+        const double r = sqrt(dot3(ld(m->cell_center, c), ld(m->cell_center, c)));
+        s->taper[c] = width <= 0 ? (r >= p->hall_r_min ? 1.0 : 0.0) : 0.5 * (1.0 + tanh(2.0 * (r - mid) / width));
+    }
+    const int64_t nnz = m->c2f_ptr[nc];
+    s->recon = (double *)calloc(3 * (size_t)nnz + 1, sizeof(double));
+    for (int32_t c = 0; c < nc; ++c)
+    {
+        double M[3][3] = {{0}};
+        for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            const double A = m->face_area_mag[f];
+            if (A <= 0) continue;
+            const v3 n = scl(1.0 / A, ld(m->face_area, f));
+            const double nv[3] = {n.x, n.y, n.z};
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) M[i][j] += A * nv[i] * nv[j];
+        }
+        const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                           M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+        const double sc = dmax(dmax(dmax(M[0][0], M[1][1]), M[2][2]), 1e-300);
+        if (fabs(det) < 1e-12 * sc * sc * sc) continue;
+        double I[3][3];
+        I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det; I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+        I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det; I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+        I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det; I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+        I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det; I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+        I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+        for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            const double A = m->face_area_mag[f];
+            if (A <= 0) continue;
+            const v3 n = scl(1.0 / A, ld(m->face_area, f));
+            for (int i = 0; i < 3; ++i) s->recon[3 * k + i] = I[i][0] * n.x + I[i][1] * n.y + I[i][2] * n.z;
+        }
+    }
+    /* owned fluid cell -> (edge, w_ec t_e) */
+    s->ce_ptr = (int64_t *)calloc((size_t)no + 1, sizeof(int64_t));
+    size_t cap = 1024, cnt = 0;
+    s->ce_edge = (int32_t *)malloc(cap * sizeof(int32_t));
+    s->ce_wt = (double *)malloc(3 * cap * sizeof(double));
+    int32_t es[256];
+    for (int32_t c = 0; c < no; ++c)
+    {
+        int nes = 0;
+        if (m->cell_material[c] == 0)
+            for (int64_t kf = m->c2f_ptr[c]; kf < m->c2f_ptr[c + 1]; ++kf)
+                for (int64_t ke = m->f2e_ptr[m->c2f_idx[kf]]; ke < m->f2e_ptr[m->c2f_idx[kf] + 1]; ++ke)
+                    if (nes < 256) es[nes++] = m->f2e_idx[ke];
+        qsort(es, (size_t)nes, sizeof(int32_t), cmp_i32);
+        int u = 0;
+        for (int i = 0; i < nes; ++i)
+            if (i == 0 || es[i] != es[i - 1]) es[u++] = es[i];
+        for (int i = 0; i < u; ++i)
+        {
+            const int32_t e = es[i];
+            int64_t lo = m->ec_ptr[e], hi = m->ec_ptr[e + 1];
+            while (lo < hi) { const int64_t mid2 = (lo + hi) / 2; if (m->ec_cell[mid2] < c) lo = mid2 + 1; else hi = mid2; }
+            if (lo == m->ec_ptr[e + 1] || m->ec_cell[lo] != c) continue;
+            if (cnt == cap)
+            {
+                cap *= 2;
+                s->ce_edge = (int32_t *)realloc(s->ce_edge, cap * sizeof(int32_t));
+                s->ce_wt = (double *)realloc(s->ce_wt, 3 * cap * sizeof(double));
+            }
+            const v3 wt = scl(m->ec_weight[lo], ld(m->edge_vec, e));
+            s->ce_edge[cnt] = e;
+            s->ce_wt[3 * cnt] = wt.x; s->ce_wt[3 * cnt + 1] = wt.y; s->ce_wt[3 * cnt + 2] = wt.z;
+            ++cnt;
+        }
+        s->ce_ptr[c + 1] = (int64_t)cnt;
+    }
+    s->d2 = (double *)calloc((size_t)ne + 1, sizeof(double));
+    for (int32_t f = 0; f < m->n_faces; ++f) /* every face is owned on one rank */
+        for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) s->d2[m->f2e_idx[k]] += m->star2[f];
+    s->phi = (double *)calloc((size_t)m->n_faces + 1, sizeof(double));
+    s->bcell = (double *)calloc(3 * (size_t)nc + 1, sizeof(double));
+    s->part = (double *)calloc(3 * (size_t)ne + 1, sizeof(double));
+    s->tmp = (double *)calloc((size_t)ne + 1, sizeof(double));
+    return s;
+}
+
+void or_ind_free(OrInduction *s)
+{
+    if (!s) return;
+    free(s->m_edge); free(s->taper); free(s->alpha); free(s->B0); free(s->recon); free(s->d2); free(s->ce_wt); free(s->corr);
+    free(s->ce_ptr); free(s->ce_edge); free(s->phi); free(s->bcell); free(s->part); free(s->tmp);
+    free(s);
+}
+
+void or_ind_set_frozen(OrInduction *s, const double *B0, const double *ne)
+{
+    const int32_t nc = s->m->n_cells;
+    memcpy(s->B0, B0, 3 * (size_t)nc * sizeof(double));
+    for (int32_t c = 0; c < nc; ++c) s->alpha[c] = (s->hall && ne[c] > 0) ? s->taper[c] * s->p.hall_coef / ne[c] : 0.0;
+}
+
+void or_ind_apply_F(OrInduction *s, const double *phi, double *out)
+{
+    const OrMesh *m = s->m;
+    const int32_t ne = m->n_edges, nc = m->n_cells;
+    memset(s->part, 0, 3 * (size_t)ne * sizeof(double));
+    if (s->resistive)
+        for (int32_t f = 0; f < m->n_faces; ++f)
+        {
+            const double v = m->star2[f] * phi[f];
+            for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) s->part[3 * (int64_t)m->f2e_idx[k]] += m->f2e_sgn[k] * v;
+        }
+    if (s->hall)
+    {
+        for (int32_t c = 0; c < nc; ++c)
+        {
+            double b[3] = {0, 0, 0};
+            for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+            {
+                const double v = phi[m->c2f_idx[k]];
+                b[0] += s->recon[3 * k] * v; b[1] += s->recon[3 * k + 1] * v; b[2] += s->recon[3 * k + 2] * v;
+            }
+            s->bcell[3 * (int64_t)c] = b[0]; s->bcell[3 * (int64_t)c + 1] = b[1]; s->bcell[3 * (int64_t)c + 2] = b[2];
+        }
+        for (int32_t c = 0; c < m->n_owned_cells; ++c)
+        {
+            if (s->alpha[c] == 0.0) continue;
+            v3 sum = mk3(0, 0, 0);
+            const v3 bc = ld(s->bcell, c);
+            for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+            {
+                const int32_t f = m->c2f_idx[k];
+                v3 bf = bc;
+                const int64_t p0 = m->f2c_ptr[f];
+                if (f2c_count(m, f) == 2)
+                {
+                    const int32_t o = m->f2c_idx[p0] == c ? m->f2c_idx[p0 + 1] : m->f2c_idx[p0];
+                    bf = scl(0.5, add3(bc, ld(s->bcell, o)));
+                }
+                sum = add3(sum, cross3(scl((double)m->c2f_sgn[k], ld(m->face_area, f)), bf));
+            }
+            const v3 J = scl(1.0 / m->cell_volume[c], sum);
+            const v3 g = scl(s->alpha[c], cross3(J, ld(s->B0, c)));
+            for (int64_t q = s->ce_ptr[c]; q < s->ce_ptr[c + 1]; ++q) s->part[3 * (int64_t)s->ce_edge[q] + 1] += dot3(g, ld(s->ce_wt, q));
+        }
+    }
+    for (int32_t e = 0; e < ne; ++e) out[e] = s->m_edge[e] * s->part[3 * (int64_t)e] + s->part[3 * (int64_t)e + 1] + s->part[3 * (int64_t)e + 2];
+}
+
+void or_ind_apply_A(OrInduction *s, const double *x, double dt, double *y)
+{
+    const OrMesh *m = s->m;
+    for (int32_t f = 0; f < m->n_faces; ++f)
+    {
+        double v = 0;
+        for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) v += m->f2e_sgn[k] * x[m->f2e_idx[k]];
+        s->phi[f] = v;
+    }
+    or_ind_apply_F(s, s->phi, s->tmp);
+    for (int32_t e = 0; e < m->n_edges; ++e) y[e] = x[e] + dt * s->tmp[e];
+}
+
+static double dot_owned(const OrMesh *m, const double *a, const double *b)
+{
+    double s = 0;
+    for (int32_t e = 0; e < m->n_owned_edges; ++e) s += a[e] * b[e];
+    return s;
+}
+
+int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, const int8_t *dir, double dt, int32_t warm, double *E, double *rel_res)
+{
+    const OrMesh *m = s->m;
+    const int32_t ne = m->n_edges, mr = s->p.restart < 2 ? 2 : s->p.restart;
+    const size_t nb = sizeof(double) * (size_t)(ne > 0 ? ne : 1);
+    double *x0 = (double *)malloc(nb), *b = (double *)malloc(nb), *r = (double *)malloc(nb), *Ax = (double *)malloc(nb);
+    double *Fn = (double *)malloc(nb), *idg = (double *)malloc(nb), *delta = (double *)calloc((size_t)ne + 1, sizeof(double));
+    double *w = (double *)malloc(nb), *z = (double *)malloc(nb), *comb = (double *)malloc(nb);
+    double *V = (double *)malloc(nb * (size_t)(mr + 1));
+    double *H = (double *)calloc((size_t)(mr + 1) * (size_t)mr, sizeof(double));
+    double *cs = (double *)calloc((size_t)mr, sizeof(double)), *sn = (double *)calloc((size_t)mr, sizeof(double));
+    double *g = (double *)calloc((size_t)mr + 1, sizeof(double)), *yv = (double *)calloc((size_t)mr, sizeof(double));
+#define HH(i, j) H[(size_t)(i) * (size_t)mr + (size_t)(j)]
+    memcpy(x0, Eexp, nb);
+    if (!warm && s->corr) { free(s->corr); s->corr = NULL; }
+    if (s->corr)
+        for (int32_t e = 0; e < ne; ++e)
+            if (!dir[e]) x0[e] += s->corr[e];
+    or_ind_apply_F(s, Phi, Fn);
+    for (int32_t e = 0; e < ne; ++e) b[e] = Eexp[e] + Fn[e];
+    or_ind_apply_A(s, x0, dt, Ax);
+    for (int32_t e = 0; e < ne; ++e) r[e] = dir[e] ? 0.0 : b[e] - Ax[e];
+    for (int32_t e = 0; e < ne; ++e) idg[e] = 1.0 / (1.0 + dt * s->m_edge[e] * s->d2[e]);
+    const double bnorm = sqrt(dmax(dot_owned(m, b, b), 1e-300));
+    double beta = sqrt(dot_owned(m, r, r));
+    int total = 0;
+    while (beta > s->p.rtol * bnorm && total < s->p.max_it)
+    {
+        for (int32_t e = 0; e < ne; ++e) V[e] = r[e] / beta;
+        memset(g, 0, sizeof(double) * ((size_t)mr + 1));
+        g[0] = beta;
+        int j = 0;
+        for (; j < mr && total < s->p.max_it; ++j, ++total)
+        {
+            const double *Vj = V + (size_t)j * (size_t)ne;
+            for (int32_t e = 0; e < ne; ++e) z[e] = dir[e] ? 0.0 : Vj[e] * idg[e];
+            or_ind_apply_A(s, z, dt, w);
+            for (int32_t e = 0; e < ne; ++e)
+                if (dir[e]) w[e] = 0.0;
+            for (int i = 0; i <= j; ++i)
+            {
+                const double *Vi = V + (size_t)i * (size_t)ne;
+                HH(i, j) = dot_owned(m, w, Vi);
+                for (int32_t e = 0; e < ne; ++e) w[e] -= HH(i, j) * Vi[e];
+            }
+            HH(j + 1, j) = sqrt(dot_owned(m, w, w));
+            if (HH(j + 1, j) > 1e-300)
+            {
+                double *Vn = V + (size_t)(j + 1) * (size_t)ne;
+                for (int32_t e = 0; e < ne; ++e) Vn[e] = w[e] / HH(j + 1, j);
+            }
+            for (int i = 0; i < j; ++i)
+            {
+                const double t = cs[i] * HH(i, j) + sn[i] * HH(i + 1, j);
+                HH(i + 1, j) = -sn[i] * HH(i, j) + cs[i] * HH(i + 1, j);
+                HH(i, j) = t;
+            }
+            const double den = hypot(HH(j, j), HH(j + 1, j));
+            cs[j] = den > 0 ? HH(j, j) / den : 1.0;
+            sn[j] = den > 0 ? HH(j + 1, j) / den : 0.0;
+            HH(j, j) = den;
+            HH(j + 1, j) = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            if (fabs(g[j + 1]) <= s->p.rtol * bnorm) { ++j; ++total; break; }
+        }
+        for (int i = j - 1; i >= 0; --i)
+        {
+            double t = g[i];
+            for (int k = i + 1; k < j; ++k) t -= HH(i, k) * yv[k];
+            yv[i] = t / HH(i, i);
+        }
+        for (int32_t e = 0; e < ne; ++e)
+        {
+            double t = 0;
+            for (int i = 0; i < j; ++i) t += yv[i] * V[(size_t)i * (size_t)ne + e];
+            comb[e] = t;
+        }
+        for (int32_t e = 0; e < ne; ++e) delta[e] += dir[e] ? 0.0 : comb[e] * idg[e];
+        for (int32_t e = 0; e < ne; ++e) z[e] = x0[e] + delta[e];
+        or_ind_apply_A(s, z, dt, Ax);
+        for (int32_t e = 0; e < ne; ++e) r[e] = dir[e] ? 0.0 : b[e] - Ax[e];
+        beta = sqrt(dot_owned(m, r, r));
+    }
+#undef HH
+    for (int32_t e = 0; e < ne; ++e) E[e] = x0[e] + delta[e];
+    if (!s->corr) s->corr = (double *)malloc(nb);
+    for (int32_t e = 0; e < ne; ++e) s->corr[e] = dir[e] ? 0.0 : E[e] - Eexp[e];
+    if (rel_res) *rel_res = beta / bnorm;
+    free(x0); free(b); free(r); free(Ax); free(Fn); free(idg); free(delta); free(w); free(z); free(comb); free(V); free(H);
+    free(cs); free(sn); free(g); free(yv);
+    return total;
+}

@@ -1,0 +1,64 @@
+"""Native mesh services against the reference's own builder, generators and geometry (CPU).
+
+Topology hash (uns::topology_hash), every CSR table and every geometry array must be identical,
+for the reference's hexahedral generators and for the tetrahedral split fed to its builder.
+"""
+import numpy as np
+import pytest
+
+from helpers import BOX_TAGS, SHELL_TAGS, ref_twin
+from mpcns_uns_b200.mesh import HostMesh
+
+ref = pytest.importorskip("oracle.ref")
+if not ref.available():
+    pytest.skip("reference checker not built (make -C oracle ref)", allow_module_level=True)
+
+TOP = ["e2n_ptr", "e2n_idx", "e2n_sgn", "f2e_ptr", "f2e_idx", "f2e_sgn", "c2f_ptr", "c2f_idx", "c2f_sgn", "e2f_ptr", "e2f_idx",
+       "e2f_sgn", "f2c_ptr", "f2c_idx", "f2c_sgn", "cell_material", "face_tag", "x"]
+GEO = ["edge_vec", "edge_mid", "edge_len", "face_area", "face_center", "face_area_mag", "cell_center", "cell_volume",
+       "cell_min_tet_volume", "edge_dual_area", "ec_ptr", "ec_cell", "ec_weight", "ef_weight", "ec_misoriented", "star0", "star1",
+       "star2", "star3"]
+
+
+def identical(h, r):
+    h.compute_geometry()
+    assert h.topology_hash() == r.topology_hash()
+    for k in TOP + GEO:
+        a, b = np.asarray(h[k]), np.asarray(r[k])
+        assert a.shape == b.shape and np.array_equal(a, b), k
+
+
+def test_box_hex():
+    identical(HostMesh.box(5, 4, 3, hi=(5, 4, 3)), ref.RefMesh.box(5, 4, 3, hi=(5, 4, 3)))
+
+
+@pytest.mark.parametrize("n_solid", [0, 1])
+def test_shell_hex(n_solid):
+    identical(HostMesh.shell(4, 4, 1.0, 5.0, 1.2, n_solid=n_solid), ref.RefMesh.shell(4, 4, 1.0, 5.0, 1.2, n_solid=n_solid))
+
+
+def test_box_tets_jittered():
+    h = HostMesh.box(4, 4, 4, tets=True, jitter=0.15, seed=0)
+    r = ref_twin(h, BOX_TAGS)
+    identical(h, r)
+    v = r.validate()
+    g = r.check_geometry()
+    assert v["ok"] and v["euler"] == 1 and v["d1d0"] == 0 and v["d2d1"] == 0
+    assert g["ok"] and g["nonpositive_volume"] == 0 and g["misoriented_dual"] == 0
+
+
+def test_shell_tets():
+    h = HostMesh.shell(3, 3, 1.0, 6.0, 1.3, tets=True)
+    r = ref_twin(h, SHELL_TAGS)
+    identical(h, r)
+    v = r.validate()
+    assert v["ok"] and v["euler"] == 2 and v["d2d1"] == 0
+    assert r.check_geometry()["ok"]
+
+
+def test_counts_of_the_benchmark_meshes():
+    """Entity counts of the 6-tet split: the first configuration exactly."""
+    h = HostMesh.box(16, 16, 16, tets=True, jitter=0.15, seed=0)
+    assert (h.n_nodes, h.n_edges, h.n_faces, h.n_cells) == (4913, 31024, 50688, 24576)
+    s = HostMesh.shell(8, 4, 1.0, 6.0, 1.0, tets=True)
+    assert s.n_cells == 6 * 8 * 8 * 4 * 6

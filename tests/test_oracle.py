@@ -1,0 +1,136 @@
+"""The oracle's C restatement against the reference's own compiled code (CPU, no GPU needed).
+
+Both run on the same seeded inputs and meshes; the restatement keeps the reference's operation
+order, so the results must be identical bit for bit.  Skipped where the compiled reference
+(oracle/_ref) is absent; tests/test_golden.py pins the restatement to committed vectors instead.
+"""
+import numpy as np
+import pytest
+
+from helpers import BOX_TAGS, MIXED_BOX_BC, SHELL_BC, SHELL_TAGS, host_from_ref, random_prims, ref_twin
+from mpcns_uns_b200.mesh import HostMesh
+from oracle import port
+
+ref = pytest.importorskip("oracle.ref")
+if not ref.available():
+    pytest.skip("reference checker not built (make -C oracle ref)", allow_module_level=True)
+
+CASES = ["box_tets_mixed", "shell_solid", "hanging"]
+
+
+def _mk(name):
+    if name == "box_tets_mixed":
+        h, bc, tags = HostMesh.box(5, 4, 3, tets=True, jitter=0.1, seed=3), MIXED_BOX_BC, BOX_TAGS
+    elif name == "shell_solid":
+        h, bc, tags = HostMesh.shell(4, 4, 0.8, 5.0, 1.2, n_solid=1, tets=True), SHELL_BC, SHELL_TAGS
+    else:
+        h, bc, tags = host_from_ref(ref.RefMesh.hanging_box(), BOX_TAGS), MIXED_BOX_BC, BOX_TAGS
+    h.compute_geometry().boundary(*bc)
+    return h, ref_twin(h, tags).boundary(*bc), port.PortMesh(h)
+
+
+_cache = {}
+
+
+@pytest.fixture(params=CASES)
+def trio(request):
+    if request.param not in _cache:
+        _cache[request.param] = _mk(request.param)
+    return _cache[request.param]
+
+
+def same(a, b):
+    assert np.array_equal(np.asarray(a), np.asarray(b)), float(np.max(np.abs(np.asarray(a) - np.asarray(b))))
+
+
+def test_fluid(trio):
+    h, r, o = trio
+    rng = np.random.default_rng(5)
+    W = random_prims(h.n_cells, rng)
+    fs = (1.1, 0.3, -0.2, 0.1, 0.12)
+    for sp in (0, 1):
+        for limit, rel in ((True, 0.0), (False, 0.0), (True, 0.5)):
+            g = o.limited_gradients(W, sp == 1, fs, limit, rel)
+            same(g, r.limited_gradients(W, sp, fs, limit, rel))
+        same(o.flux_rhs(W, g, sp == 1, fs, 5 / 3), r.flux_rhs(W, g, sp, fs, 5 / 3))
+    U = rng.uniform(-1, 1, 5 * h.n_cells)
+    same(o.to_prim(U, 5 / 3), r.to_prim(U, 5 / 3))
+
+
+def test_induction_pieces(trio):
+    h, r, o = trio
+    rng = np.random.default_rng(6)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    same(o.cell_vector(phi), r.cell_vector(phi))
+    args = [rng.uniform(-1, 1, 3 * h.n_cells) for _ in range(3)] + [rng.uniform(-1, 1, h.n_faces) for _ in range(2)]
+    E0 = rng.uniform(-1, 1, h.n_edges)
+    same(o.ideal_emf(*args, 0.5, E0), r.ideal_emf(*args, 0.5, E0))
+    E = rng.uniform(-1, 1, h.n_edges)
+    same(o.faraday(E, phi, 0.3), r.faraday(E, phi, 0.3))
+    dte = rng.uniform(0.1, 1, h.n_edges)
+    same(o.faraday(E, phi, 0.0, dte), r.faraday_edge_dt(E, dte, phi))
+    for ex in (None, rng.uniform(-1, 1, h.n_faces)):
+        a, b = o.div_b(phi, ex), r.div_b(phi, ex)
+        assert a == b
+    B = rng.uniform(-1, 1, 3 * h.n_cells)
+    same(o.cell_current(B), r.cell_current(B))
+
+
+def test_cfl_and_step():
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5)
+    h = wl.mesh
+    r = ref_twin(h, SHELL_TAGS).boundary(*SHELL_BC)
+    o = port.PortMesh(h)
+    Badd = r.cell_vector(wl.PhiAdd)
+    same(o.cell_vector(wl.PhiAdd), Badd)
+    Uo = [np.array(u) for u in wl.U]
+    Ur = [np.array(u) for u in wl.U]
+    Po, Pr = np.array(wl.Phi), np.array(wl.Phi)
+    rp = ref.StepParams()
+    rp.n_species, rp.second_order, rp.gamma, rp.rho_floor, rp.p_floor, rp.cuct = 2, 1, wl.gamma, 1e-10, 1e-12, 0.5
+    rp.M_ref, rp.ne_floor = 1.0, 0.01
+    rp.u_inf[:] = list(wl.u_inf)
+    rp.B_imf[:] = list(wl.B_imf)
+    for s in range(2):
+        rp.mass[s] = wl.mass[s]
+        rp.fs[s][:] = list(wl.fs[s])
+    for _ in range(3):
+        W = [r.to_prim(u, wl.gamma) for u in Ur]
+        Bt = r.cell_vector(Pr) + Badd
+        dt = r.local_time_step(wl.gamma, 0.4, 1.0, 1e-2, W[0], W[1], Bt)
+        assert o.local_time_step([o.to_prim(u, wl.gamma) for u in Uo], o.cell_vector(Po) + Badd, wl.gamma, 0.4) == dt
+        o.rk2_step(wl, Uo, Po, Badd, dt)
+        r.rk2_step(rp, Ur, Pr, wl.PhiAdd, Badd, dt)
+        for a, b in zip(Uo, Ur):
+            same(a, b)
+        same(Po, Pr)
+
+
+@pytest.mark.parametrize("hall,resistive", [(True, False), (False, True), (True, True)])
+def test_implicit_induction(hall, resistive):
+    h = HostMesh.box(6, 5, 4, tets=True, jitter=0.1, seed=8).compute_geometry().boundary(*MIXED_BOX_BC)
+    r = ref_twin(h, BOX_TAGS).boundary(*MIXED_BOX_BC)
+    o = port.PortMesh(h)
+    rng = np.random.default_rng(12)
+    m_edge = rng.uniform(0.5, 2.0, h.n_edges) / np.asarray(h["star1"]) if resistive else None
+    kw = dict(hall=hall, hall_coef=0.5, hall_r_min=-100.0, hall_r_max=-99.0, rtol=1e-10, max_it=200, restart=15)
+    ri = ref.RefInduction(r, **kw)
+    if resistive:
+        ri.set_m(m_edge)
+    oi = port.PortInduction(o, m_edge, **kw)
+    B0 = rng.uniform(-1, 1, 3 * h.n_cells)
+    ne = rng.uniform(0.5, 2.0, h.n_cells)
+    ri.set_frozen_state(B0, ne)
+    oi.set_frozen_state(B0, ne)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    same(oi.apply_F(phi), ri.apply_F(phi))
+    x = rng.uniform(-1, 1, h.n_edges)
+    same(oi.apply_A(x, 0.05), ri.apply_A(x, 0.05))
+    dirichlet = (np.asarray(h["edge_mode"]) == 2).astype(np.int8)
+    Ee = rng.uniform(-1, 1, h.n_edges)
+    for warm in (False, True):
+        Eo, ito, rro = oi.solve(phi, Ee, dirichlet, 0.05, warm)
+        Er, itr, rrr = ri.solve(phi, Ee, dirichlet, 0.05, warm)
+        assert ito == itr and rro == rrr
+        same(Eo, Er)
