@@ -125,6 +125,35 @@ int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, d
 /* mhd::cell_current (Common/induction/Current.cpp:9-31): B 3 per cell -> J 3 per cell. */
 int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);
 
+/* ------------------------------------------------------------------ semi-implicit induction
+ * mhd::ImplicitInduction (Common/induction/ImplicitInduction.h:27-94): the operator
+ *   F(Phi) = M d1^T S2 Phi + H(Phi),  A x = x + dt F(d1 x)
+ * and the restarted GMRES(m) with modified Gram-Schmidt, Givens rotations, Jacobi right
+ * preconditioner, true residual at every restart and warm start (.cpp:299-390).  The resistive
+ * coefficient m_e = eta_e / star1_e is given per edge (host array, may be NULL), which covers the
+ * reference's tanh window and any other profile.  Mixed precision: the operator and the
+ * preconditioner inside the Arnoldi cycles in FP32; Krylov basis, Gram-Schmidt, Hessenberg,
+ * least squares and the true residual of every restart (an FP64 iterative refinement) in FP64. */
+typedef struct MhdInductionParams {
+    int32_t hall;                  /* Config::hall (Hall term on) */
+    int32_t max_it, restart;       /* Config::ind_max_it, ind_restart */
+    int32_t precision;             /* MHD_PREC_FP64 or MHD_PREC_MIXED */
+    double hall_coef, hall_r_min, hall_r_max, rtol; /* Scales::hall_coef, Config::hall_r_min/max, ind_rtol */
+} MhdInductionParams;
+
+int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *params, const double *m_edge_host, MhdInduction **out);
+int mhd_gpu_induction_destroy(MhdInduction *ind);
+/* ImplicitInduction::set_frozen_state (:105-111): B0 3 per cell, n_e,eff 1 per cell (device). */
+int mhd_gpu_induction_set_frozen(MhdInduction *ind, const double *B0, const double *ne_eff);
+/* ImplicitInduction::apply_F (:127-183) and apply_A (:185-198) in FP64 (device arrays). */
+int mhd_gpu_induction_apply_F(MhdInduction *ind, const double *phi, double *out);
+int mhd_gpu_induction_apply_A(MhdInduction *ind, const double *x, double dt, double *y);
+/* ImplicitInduction::solve (:299-390).  dirichlet[e] != 0 imposes E = E_expl (device int8 array);
+ * warm = 0 drops the previous step's correction.  Returns MHD_ENOCONV (with E, iterations and
+ * rel_res set) when max_it is reached above rtol, which the reference reports without throwing. */
+int mhd_gpu_induction_solve(MhdInduction *ind, const double *Phi, const double *E_expl, const int8_t *dirichlet, double dt,
+                            int32_t warm, double *E, int32_t *iterations, double *rel_res);
+
 /* ------------------------------------------------------------------ resident state, fused step
  * The explicit step of mercury::Solver::step (MercuryUns/driver/Solver.cpp:481-516) restricted to
  * the hot path (prepare :94-125 without the current, rhs :132-169 without model sources, advance

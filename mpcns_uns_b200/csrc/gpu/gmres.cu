@@ -1,0 +1,786 @@
+// nvcc-flags: -fmad=false
+// Semi-implicit Hall / resistive induction on the device: the operator of mhd::ImplicitInduction
+// and its restarted GMRES (Common/induction/ImplicitInduction.cpp).
+//
+// The operator's scatters become gathers whose summation order equals the reference's: the
+// resistive current flux reaches an edge from its faces in ascending face order (e2f rows), the Hall
+// EMF from its cells in ascending cell order (ec rows, the reference's ce lists); the FP64 operator
+// is therefore reference-exact.  The Krylov part keeps H, g and the Givens rotations on the device;
+// the host reads one value per Arnoldi step (the early-exit test) and one per restart (the true
+// residual).  Its dot products are deterministic block reductions, whose rounding differs from the
+// reference's sequential sums, so GMRES iterates agree to the solver tolerance, not bit for bit.
+//
+// Fusions of the Arnoldi step (each keeps the reference's arithmetic per element):
+//   * the Jacobi preconditioner z = dir ? 0 : V_j / (1 + dt m d2) is applied while gathering z in d1;
+//   * V_j = w / H(j, j-1) is formed lazily in the next matvec (the face pass gathers w / h, the edge
+//     pass stores V_j), so w is not re-read to normalise it;
+//   * the edge pass zeroes the Dirichlet rows of w and produces the block partials of w . V_0;
+//   * each modified Gram-Schmidt subtraction w -= H(i-1, j) V_{i-1} is fused with the next dot w . V_i,
+//     and consecutive passes sweep the edges in opposite directions so that the tail of w and V_{i-1}
+//     that the previous pass left in L2 is reused first.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace mhd
+{
+namespace
+{
+constexpr int kRedBlocks = 8 * 148; // streaming reductions: 8 resident 256-thread blocks per SM
+
+__device__ __forceinline__ double block_sum(double v)
+{
+    __shared__ double sh[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    if (wid == 0)
+    {
+        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------- one-time tables
+// cell-field coefficients of the constructor (:34-62): B_c = sum_k recon_k Phi_{f_k}
+__global__ void k_ind_recon(MeshView m, double *recon)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    double M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        const double A = m.face_area_mag[f];
+        for (int i = 0; i < 3; ++i) recon[3 * (int64_t)k + i] = 0.0;
+        if (A <= 0) continue;
+        const V3 n = (1.0 / A) * ld3(m.face_area, f);
+        const double nv[3] = {n.x, n.y, n.z};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) M[i][j] += A * nv[i] * nv[j];
+    }
+    const double det = M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0]) +
+                       M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+    const double sc = dmax(dmax(dmax(M[0][0], M[1][1]), M[2][2]), 1e-300);
+    if (fabs(det) < 1e-12 * sc * sc * sc) return;
+    double I[3][3];
+    I[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) / det; I[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) / det;
+    I[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) / det; I[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) / det;
+    I[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) / det; I[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) / det;
+    I[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) / det; I[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) / det;
+    I[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) / det;
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        const double A = m.face_area_mag[f];
+        if (A <= 0) continue;
+        const V3 n = (1.0 / A) * ld3(m.face_area, f);
+        for (int i = 0; i < 3; ++i) recon[3 * (int64_t)k + i] = I[i][0] * n.x + I[i][1] * n.y + I[i][2] * n.z;
+    }
+}
+
+// d2_e = sum of star2 over the faces of e, ascending face order (:87-89)
+__global__ void k_ind_d2(MeshView m, double *d2)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    double s = 0.0;
+    for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k) s += m.star2[m.e2f_idx[k]];
+    d2[e] = s;
+}
+
+// set_frozen_state (:105-111)
+__global__ void k_ind_alpha(int32_t nc, const double *taper, const double *ne_eff, int hall, double hall_coef, double *alpha)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    alpha[c] = (hall && ne_eff[c] > 0) ? taper[c] * hall_coef / ne_eff[c] : 0.0;
+}
+
+// FP32 copies of the operator's tables (mixed precision)
+__global__ void k_ind_tables32(MeshView m, const double *recon, const double *mcoef, float *recon32, float *m32, float *ecw32,
+                               float *tv32, float *fa32, float *vinv32)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < 3 * (int64_t)m.c2f_ptr[m.nc]) recon32[i] = static_cast<float>(recon[i]);
+    if (i < m.ec_ptr[m.ne]) ecw32[i] = static_cast<float>(m.ec_weight[i]);
+    if (i < m.ne)
+    {
+        m32[i] = static_cast<float>(mcoef[i]);
+        for (int a = 0; a < 3; ++a) tv32[3 * i + a] = static_cast<float>(m.edge_vec[3 * i + a]);
+    }
+    if (i < m.nf)
+        for (int a = 0; a < 3; ++a) fa32[3 * i + a] = static_cast<float>(m.face_area[3 * i + a]);
+    if (i < m.nc) vinv32[i] = static_cast<float>(1.0 / m.cell_volume[i]);
+}
+
+__global__ void k_to_float(const double *a, float *b, int64_t n)
+{
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) b[i] = static_cast<float>(a[i]);
+}
+
+// ---------------------------------------------------------------- operator
+// Input of a matvec: x_e directly (apply_A), or the preconditioned Krylov vector
+// x_e = (src_e / *hs) * pd_e with pd_e = dir_e ? 0 : 1 / (1 + dt m_e d2_e)  (:338)
+struct MatIn
+{
+    const double *x = nullptr;
+    const double *src = nullptr, *hs = nullptr, *pd = nullptr;
+};
+
+__device__ __forceinline__ double mat_in(const MatIn &in, int32_t e)
+{
+    if (!in.src) return in.x[e];
+    double v = in.src[e];
+    if (in.hs) v = v / *in.hs;
+    return v * in.pd[e];
+}
+
+// Phi' = d1 x on every face (:185-190), with star2 Phi' for the resistive current flux (:131-136).
+// FP64 sums in both precisions; the FP32 operator stores the rounded results.
+template <class T>
+__global__ void k_ind_face(MeshView m, MatIn in, int hall, int resistive, T *__restrict__ phi, T *__restrict__ s2phi)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= m.nf) return;
+    double s = 0;
+    for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) s += m.f2e_sgn[k] * mat_in(in, m.f2e_idx[k]);
+    if (hall) phi[f] = static_cast<T>(s);
+    if (resistive) s2phi[f] = static_cast<T>(m.star2[f] * s);
+}
+
+__global__ void k_ind_s2phi(MeshView m, const double *__restrict__ phi, double *__restrict__ s2phi)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f < m.nf) s2phi[f] = m.star2[f] * phi[f];
+}
+
+// cell field from the face fluxes (:139-149)
+template <class T>
+__global__ void k_ind_bcell(MeshView m, const T *__restrict__ recon, const T *__restrict__ phi, T *__restrict__ b)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    T bx = 0, by = 0, bz = 0;
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const T v = phi[m.c2f_idx[k]];
+        bx += recon[3 * (int64_t)k] * v;
+        by += recon[3 * (int64_t)k + 1] * v;
+        bz += recon[3 * (int64_t)k + 2] * v;
+    }
+    b[3 * (int64_t)c] = bx; b[3 * (int64_t)c + 1] = by; b[3 * (int64_t)c + 2] = bz;
+}
+
+// Hall EMF per owned cell (:159-178): J_c = (1/V) sum s A x 1/2 (b_c + b_nb), g_c = alpha_c J_c x B0_c.
+// g_c = 0 where the reference skips the cell (alpha = 0, or not fluid: its ce list is empty), so that
+// the edge gather may add every owned cell: adding the zero product leaves each sum unchanged.
+__global__ void k_ind_hall(MeshView m, const double *__restrict__ b, const double *__restrict__ alpha, const double *__restrict__ B0,
+                           double *__restrict__ g)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.no_cells) return;
+    if (alpha[c] == 0.0 || m.material[c] != 0)
+    {
+        st3(g, c, mk(0, 0, 0));
+        return;
+    }
+    V3 sum = mk(0, 0, 0);
+    const V3 bc = ld3(b, c);
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        V3 bf = bc;
+        const int32_t p0 = m.f2c_ptr[f];
+        if (m.f2c_ptr[f + 1] - p0 == 2)
+        {
+            const int32_t o = m.f2c_idx[p0] == c ? m.f2c_idx[p0 + 1] : m.f2c_idx[p0];
+            bf = 0.5 * (bc + ld3(b, o));
+        }
+        sum = sum + cross(double(m.c2f_sgn[k]) * ld3(m.face_area, f), bf);
+    }
+    const V3 J = (1.0 / m.cell_volume[c]) * sum;
+    st3(g, c, alpha[c] * cross(J, ld3(B0, c)));
+}
+
+__global__ void k_ind_hall32(MeshView m, const float *__restrict__ b, const float *__restrict__ alpha, const float *__restrict__ B0,
+                             const float *__restrict__ fa, const float *__restrict__ vinv, float *__restrict__ g)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.no_cells) return;
+    const float a = alpha[c];
+    if (a == 0.f || m.material[c] != 0)
+    {
+        g[3 * (int64_t)c] = g[3 * (int64_t)c + 1] = g[3 * (int64_t)c + 2] = 0.f;
+        return;
+    }
+    float sx = 0.f, sy = 0.f, sz = 0.f;
+    const float bcx = b[3 * (int64_t)c], bcy = b[3 * (int64_t)c + 1], bcz = b[3 * (int64_t)c + 2];
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        float bx = bcx, by = bcy, bz = bcz;
+        const int32_t p0 = m.f2c_ptr[f];
+        if (m.f2c_ptr[f + 1] - p0 == 2)
+        {
+            const int32_t o = m.f2c_idx[p0] == c ? m.f2c_idx[p0 + 1] : m.f2c_idx[p0];
+            bx = 0.5f * (bcx + b[3 * (int64_t)o]);
+            by = 0.5f * (bcy + b[3 * (int64_t)o + 1]);
+            bz = 0.5f * (bcz + b[3 * (int64_t)o + 2]);
+        }
+        const float s = m.c2f_sgn[k];
+        const float ax = s * fa[3 * (int64_t)f], ay = s * fa[3 * (int64_t)f + 1], az = s * fa[3 * (int64_t)f + 2];
+        sx += ay * bz - az * by;
+        sy += az * bx - ax * bz;
+        sz += ax * by - ay * bx;
+    }
+    const float iv = vinv[c];
+    const float Jx = iv * sx, Jy = iv * sy, Jz = iv * sz;
+    const float Bx = B0[3 * (int64_t)c], By = B0[3 * (int64_t)c + 1], Bz = B0[3 * (int64_t)c + 2];
+    g[3 * (int64_t)c] = a * (Jy * Bz - Jz * By);
+    g[3 * (int64_t)c + 1] = a * (Jz * Bx - Jx * Bz);
+    g[3 * (int64_t)c + 2] = a * (Jx * By - Jy * Bx);
+}
+
+template <class T> struct EdgeArgs
+{
+    int resistive = 0, hall = 0;
+    const T *s2phi = nullptr, *g = nullptr, *mcoef = nullptr, *ecw = nullptr, *tvec = nullptr;
+    MatIn in;                    // x of y = x + dt F; no input: y = F (apply_F)
+    double dt = 0;
+    double *vout = nullptr;      // stores src / *hs (the lazily normalised Krylov vector V_j)
+    const int8_t *dir = nullptr; // zero y on Dirichlet edges (:339)
+    const double *v0 = nullptr;  // block partials of y . v0 over the owned edges
+    double *part = nullptr;
+    double *out = nullptr;
+};
+
+// Per edge: part0 = sum_f s star2 Phi' (resistive, ascending faces), part1 = sum_c g_c . (w_ec t_e)
+// (Hall, ascending cells), F = m part0 + part1 + part2 (:176-182); y = F, or y = x + dt F (:191-197).
+template <class T>
+__global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    double contrib = 0.0;
+    if (e < m.ne)
+    {
+        T p0 = 0, p1 = 0;
+        if (a.resistive)
+            for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k) p0 += static_cast<T>(m.e2f_sgn[k]) * a.s2phi[m.e2f_idx[k]];
+        if (a.hall)
+        {
+            const T tx = a.tvec[3 * (int64_t)e], ty = a.tvec[3 * (int64_t)e + 1], tz = a.tvec[3 * (int64_t)e + 2];
+            for (int32_t k = m.ec_ptr[e]; k < m.ec_ptr[e + 1]; ++k)
+            {
+                const int32_t c = m.ec_cell[k];
+                if (c >= m.no_cells) continue;
+                const T w = a.ecw[k];
+                const T wx = w * tx, wy = w * ty, wz = w * tz;
+                p1 += a.g[3 * (int64_t)c] * wx + a.g[3 * (int64_t)c + 1] * wy + a.g[3 * (int64_t)c + 2] * wz;
+            }
+        }
+        const T F = a.mcoef[e] * p0 + p1 + static_cast<T>(0);
+        double y = static_cast<double>(F);
+        if (a.in.src || a.in.x)
+        {
+            double xe;
+            if (a.in.src)
+            {
+                double v = a.in.src[e];
+                if (a.in.hs) v = v / *a.in.hs;
+                if (a.vout) a.vout[e] = v;
+                xe = v * a.in.pd[e];
+            }
+            else
+                xe = a.in.x[e];
+            y = xe + a.dt * static_cast<double>(F);
+        }
+        if (a.dir && a.dir[e]) y = 0.0;
+        a.out[e] = y;
+        if (a.v0 && e < m.no_edges) contrib = y * a.v0[e];
+    }
+    if (a.v0)
+    {
+        contrib = block_sum(contrib);
+        if (threadIdx.x == 0) a.part[blockIdx.x] = contrib;
+    }
+}
+
+// ---------------------------------------------------------------- Krylov vectors (FP64)
+// a . b over the owned edges, block partials (deterministic order)
+__global__ void __launch_bounds__(256) k_dot_part(const double *__restrict__ a, const double *__restrict__ b, int32_t n,
+                                                   double *__restrict__ part)
+{
+    double s = 0.0;
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// Modified Gram-Schmidt step fused with the next dot: w -= (*h) Vprev on all edges (if Vprev), then
+// block partials of w . Vi over the owned edges (Vi null: w . w).  `reverse` sweeps from the last edge.
+__global__ void __launch_bounds__(256) k_mgs(double *__restrict__ w, const double *__restrict__ Vprev, const double *__restrict__ h,
+                                              const double *__restrict__ Vi, int32_t n_all, int32_t n_owned, int reverse,
+                                              double *__restrict__ part)
+{
+    constexpr int U = 4;
+    const double hv = Vprev ? *h : 0.0;
+    const int32_t stride = gridDim.x * blockDim.x;
+    double s = 0.0;
+    for (int32_t t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < n_all; t0 += U * stride)
+    {
+        int32_t idx[U];
+        double wv[U], pv[U], iv[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            const int32_t t = t0 + u * stride;
+            idx[u] = t < n_all ? (reverse ? n_all - 1 - t : t) : -1;
+            if (idx[u] >= 0)
+            {
+                wv[u] = w[idx[u]];
+                pv[u] = Vprev ? Vprev[idx[u]] : 0.0;
+                iv[u] = Vi ? Vi[idx[u]] : 0.0;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+        {
+            if (idx[u] < 0) continue;
+            double wi = wv[u];
+            if (Vprev)
+            {
+                wi -= hv * pv[u];
+                w[idx[u]] = wi;
+            }
+            if (idx[u] < n_owned) s += wi * (Vi ? iv[u] : wi);
+        }
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+// *out = sum of the partials (op 1: its square root, op 2: sqrt(max(sum, 1e-300)))
+__global__ void __launch_bounds__(1024) k_dot_final(const double *__restrict__ part, int n, int op, double *__restrict__ out)
+{
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) *out = op == 0 ? s : (op == 1 ? sqrt(s) : sqrt(dmax(s, 1e-300)));
+}
+
+__global__ void k_vec_x0(int32_t n, const double *Ee, const double *corr, const int8_t *dir, double *x0, double *delta)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    x0[i] = (corr && !dir[i]) ? Ee[i] + corr[i] : Ee[i];
+    delta[i] = 0.0;
+}
+__global__ void k_vec_add(int32_t n, const double *a, const double *b, double *c)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) c[i] = a[i] + b[i];
+}
+// r = dir ? 0 : b - Ax
+__global__ void k_vec_resid(int32_t n, const double *b, const double *Ax, const int8_t *dir, double *r)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = dir[i] ? 0.0 : b[i] - Ax[i];
+}
+// pd = dir ? 0 : 1 / (1 + dt m d2)  (Jacobi, :315-316)
+__global__ void k_vec_pd(int32_t n, double dt, const double *mc, const double *d2, const int8_t *dir, double *pd)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pd[i] = dir[i] ? 0.0 : 1.0 / (1.0 + dt * mc[i] * d2[i]);
+}
+// V0 = r / beta
+__global__ void k_vec_v0(int32_t n, const double *r, const double *beta, double *V0)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) V0[i] = r[i] / *beta;
+}
+
+// Givens rotations of column j and the residual estimate (:337-347); single thread.
+// H is (m+1) x m row-major; nrm[j+1] keeps H(j+1, j) before the rotation (the divisor of V_{j+1}).
+__global__ void k_givens(double *H, int mcols, int j, double *cs, double *sn, double *g, double *nrm, double *est)
+{
+    auto h = [&](int r, int c) -> double & { return H[r * mcols + c]; };
+    nrm[j + 1] = h(j + 1, j);
+    for (int i = 0; i < j; ++i)
+    {
+        const double t = cs[i] * h(i, j) + sn[i] * h(i + 1, j);
+        h(i + 1, j) = -sn[i] * h(i, j) + cs[i] * h(i + 1, j);
+        h(i, j) = t;
+    }
+    const double den = hypot(h(j, j), h(j + 1, j));
+    cs[j] = den > 0 ? h(j, j) / den : 1.0;
+    sn[j] = den > 0 ? h(j + 1, j) / den : 0.0;
+    h(j, j) = den;
+    h(j + 1, j) = 0.0;
+    g[j + 1] = -sn[j] * g[j];
+    g[j] = cs[j] * g[j];
+    est[0] = fabs(g[j + 1]);
+}
+
+__global__ void k_g_init(double *g, int n, const double *beta)
+{
+    for (int i = 0; i < n; ++i) g[i] = 0.0;
+    g[0] = *beta;
+}
+
+// back substitution of the least-squares problem (:349-354); single thread
+__global__ void k_backsub(const double *H, int mcols, int j, const double *g, double *y)
+{
+    for (int i = j - 1; i >= 0; --i)
+    {
+        double s = g[i];
+        for (int k = i + 1; k < j; ++k) s -= H[i * mcols + k] * y[k];
+        y[i] = s / H[i * mcols + i];
+    }
+}
+
+// delta += dir ? 0 : (sum_i y_i V_i) / (1 + dt m d2)  (:355-364); z = x0 + delta for the true residual
+__global__ void k_vec_update(int32_t n, const double *V, int j, const double *y, const double *pd, const int8_t *dir,
+                             const double *x0, double *delta, double *z)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    double s = 0.0;
+    for (int i = 0; i < j; ++i) s += y[i] * V[(int64_t)i * n + e];
+    const double d = delta[e] + (dir[e] ? 0.0 : s * pd[e]);
+    delta[e] = d;
+    z[e] = x0[e] + d;
+}
+
+// E = x0 + delta, corr = dir ? 0 : E - E_expl (:379-381)
+__global__ void k_vec_final(int32_t n, const double *x0, const double *delta, const double *Ee, const int8_t *dir, double *E, double *corr)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double v = x0[i] + delta[i];
+    E[i] = v;
+    corr[i] = dir[i] ? 0.0 : v - Ee[i];
+}
+} // namespace
+} // namespace mhd
+
+using namespace mhd;
+
+struct MhdInduction
+{
+    MhdMesh *mesh = nullptr;
+    MhdInductionParams p{};
+    bool resistive = false, hall = false, mixed = false, have_corr = false;
+    int edge_blocks = 0;
+    DBuf<double> mcoef, taper, alpha, B0, recon, d2, corr, phi, s2phi, bcell, g;
+    DBuf<double> V, w, z, r, b, x0, delta, Ax, pd, Fn, part, H, cs, sn, gv, yv, nrm, scal;
+    DBuf<float> recon32, m32, ecw32, tv32, fa32, vinv32, alpha32, B0_32, phi32, s2phi32, b32, g32;
+    double *pinned = nullptr;
+    ~MhdInduction()
+    {
+        if (pinned) cudaFreeHost(pinned);
+    }
+};
+
+namespace mhd
+{
+namespace
+{
+int g1(int64_t n) { return grid_for(n, 256); }
+
+// y = F(phi) (in.x and in.src null, phi given) or y = A x; optional fused outputs as in EdgeArgs.
+void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, double *y, double *vout = nullptr,
+          const int8_t *dir = nullptr, const double *v0 = nullptr)
+{
+    const MeshView &m = I->mesh->v;
+    cudaStream_t s = I->mesh->stream;
+    const double *phi = phi_in;
+    if (in.x || in.src)
+    {
+        if (m.nf) k_ind_face<double><<<g1(m.nf), 256, 0, s>>>(m, in, I->hall, I->resistive, I->phi.p, I->s2phi.p);
+        phi = I->phi.p;
+    }
+    else if (I->resistive && m.nf)
+        k_ind_s2phi<<<g1(m.nf), 256, 0, s>>>(m, phi, I->s2phi.p);
+    if (I->hall && m.nc)
+    {
+        k_ind_bcell<double><<<g1(m.nc), 256, 0, s>>>(m, I->recon.p, phi, I->bcell.p);
+        if (m.no_cells) k_ind_hall<<<g1(m.no_cells), 256, 0, s>>>(m, I->bcell.p, I->alpha.p, I->B0.p, I->g.p);
+    }
+    EdgeArgs<double> a;
+    a.resistive = I->resistive; a.hall = I->hall;
+    a.s2phi = I->s2phi.p; a.g = I->g.p; a.mcoef = I->mcoef.p; a.ecw = m.ec_weight; a.tvec = m.edge_vec;
+    a.in = in; a.dt = dt; a.vout = vout; a.dir = dir; a.v0 = v0; a.part = I->part.p; a.out = y;
+    if (m.ne) k_ind_edge<double><<<I->edge_blocks, 256, 0, s>>>(m, a);
+    MHD_LAUNCH_CHECK();
+}
+
+// the same Arnoldi matvec with the FP32 operator (mixed precision inner iterations)
+void op32(MhdInduction *I, const MatIn &in, double dt, double *y, double *vout, const int8_t *dir, const double *v0)
+{
+    const MeshView &m = I->mesh->v;
+    cudaStream_t s = I->mesh->stream;
+    if (m.nf) k_ind_face<float><<<g1(m.nf), 256, 0, s>>>(m, in, I->hall, I->resistive, I->phi32.p, I->s2phi32.p);
+    if (I->hall && m.nc)
+    {
+        k_ind_bcell<float><<<g1(m.nc), 256, 0, s>>>(m, I->recon32.p, I->phi32.p, I->b32.p);
+        if (m.no_cells)
+            k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, I->b32.p, I->alpha32.p, I->B0_32.p, I->fa32.p, I->vinv32.p, I->g32.p);
+    }
+    EdgeArgs<float> a;
+    a.resistive = I->resistive; a.hall = I->hall;
+    a.s2phi = I->s2phi32.p; a.g = I->g32.p; a.mcoef = I->m32.p; a.ecw = I->ecw32.p; a.tvec = I->tv32.p;
+    a.in = in; a.dt = dt; a.vout = vout; a.dir = dir; a.v0 = v0; a.part = I->part.p; a.out = y;
+    if (m.ne) k_ind_edge<float><<<I->edge_blocks, 256, 0, s>>>(m, a);
+    MHD_LAUNCH_CHECK();
+}
+
+void apply_plain(MhdInduction *I, const double *x, double dt, double *y)
+{
+    MatIn in;
+    in.x = x;
+    op64(I, in, nullptr, dt, y);
+}
+
+// dot over the owned edges into *out (op as k_dot_final)
+void dev_dot(MhdInduction *I, const double *a, const double *b, int op, double *out)
+{
+    cudaStream_t s = I->mesh->stream;
+    k_dot_part<<<kRedBlocks, 256, 0, s>>>(a, b, I->mesh->v.no_edges, I->part.p);
+    k_dot_final<<<1, 1024, 0, s>>>(I->part.p, kRedBlocks, op, out);
+    MHD_LAUNCH_CHECK();
+}
+
+double host_read(MhdInduction *I, const double *dev)
+{
+    cudaStream_t s = I->mesh->stream;
+    MHD_CUDA(cudaMemcpyAsync(I->pinned, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaStreamSynchronize(s));
+    return I->pinned[0];
+}
+} // namespace
+} // namespace mhd
+
+extern "C" {
+
+int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const double *m_edge_host, MhdInduction **out)
+{
+    MhdInduction *I = nullptr;
+    int rc = guarded([&] {
+        MHD_REQUIRE(mesh && p && out, "null argument");
+        MHD_REQUIRE(p->precision == MHD_PREC_FP64 || p->precision == MHD_PREC_MIXED, "unknown precision");
+        MHD_REQUIRE(p->restart >= 1 && p->max_it >= 0, "bad restart / max_it");
+        const MeshView &m = mesh->v;
+        cudaStream_t s = mesh->stream;
+        I = new MhdInduction;
+        I->mesh = mesh;
+        I->p = *p;
+        I->p.restart = std::max(2, p->restart); // restart_(std::max(2, cfg.ind_restart)) of the constructor
+        I->hall = p->hall && p->hall_coef > 0;
+        I->mixed = p->precision == MHD_PREC_MIXED;
+        I->edge_blocks = g1(m.ne);
+        const size_t ne = m.ne, nf = m.nf, nc = m.nc;
+        std::vector<double> mc(ne, 0.0);
+        if (m_edge_host)
+            for (size_t e = 0; e < ne; ++e)
+            {
+                mc[e] = m_edge_host[e];
+                I->resistive |= mc[e] != 0.0;
+            }
+        I->mcoef.upload(mc);
+        // Hall radial taper with the host's tanh, as the reference computes it (:23-30)
+        std::vector<double> xc(3 * nc);
+        std::vector<int8_t> mat(nc);
+        if (nc)
+        {
+            MHD_CUDA(cudaMemcpy(xc.data(), m.cell_center, 3 * nc * sizeof(double), cudaMemcpyDeviceToHost));
+            MHD_CUDA(cudaMemcpy(mat.data(), m.material, nc, cudaMemcpyDeviceToHost));
+        }
+        std::vector<double> taper(nc, 0.0);
+        const double mid = 0.5 * (p->hall_r_min + p->hall_r_max), width = p->hall_r_max - p->hall_r_min;
+        for (size_t c = 0; c < nc; ++c)
+        {
+            if (mat[c] == 1) continue;
+            const double x = xc[3 * c], y = xc[3 * c + 1], z = xc[3 * c + 2];
+            const double r = std::sqrt(x * x + y * y + z * z);
+            taper[c] = width <= 0 ? (r >= p->hall_r_min ? 1.0 : 0.0) : 0.5 * (1.0 + std::tanh(2.0 * (r - mid) / width));
+        }
+        I->taper.upload(taper);
+        int32_t nnz_c = 0, nnz_ec = 0;
+        MHD_CUDA(cudaMemcpy(&nnz_c, m.c2f_ptr + m.nc, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        MHD_CUDA(cudaMemcpy(&nnz_ec, m.ec_ptr + m.ne, sizeof(int32_t), cudaMemcpyDeviceToHost));
+        I->alpha.alloc(nc); I->B0.alloc(3 * nc); I->recon.alloc(3 * (size_t)nnz_c); I->d2.alloc(ne); I->corr.alloc(ne);
+        I->phi.alloc(nf); I->s2phi.alloc(nf); I->bcell.alloc(3 * nc); I->g.alloc(3 * nc);
+        const int mr = I->p.restart;
+        I->V.alloc((size_t)(mr + 1) * ne); I->w.alloc(ne); I->z.alloc(ne); I->r.alloc(ne); I->b.alloc(ne); I->x0.alloc(ne);
+        I->delta.alloc(ne); I->Ax.alloc(ne); I->pd.alloc(ne); I->Fn.alloc(ne);
+        I->part.alloc((size_t)std::max(kRedBlocks, I->edge_blocks));
+        I->H.alloc((size_t)(mr + 1) * mr); I->cs.alloc(mr); I->sn.alloc(mr); I->gv.alloc(mr + 1); I->yv.alloc(mr);
+        I->nrm.alloc(mr + 1); I->scal.alloc(8);
+        MHD_CUDA(cudaMallocHost(&I->pinned, 8 * sizeof(double)));
+        if (nc)
+        {
+            MHD_CUDA(cudaMemsetAsync(I->alpha.p, 0, nc * sizeof(double), s));
+            MHD_CUDA(cudaMemsetAsync(I->B0.p, 0, 3 * nc * sizeof(double), s));
+            MHD_CUDA(cudaMemsetAsync(I->g.p, 0, 3 * nc * sizeof(double), s));
+            k_ind_recon<<<g1(nc), 256, 0, s>>>(m, I->recon.p);
+        }
+        if (ne) k_ind_d2<<<g1(ne), 256, 0, s>>>(m, I->d2.p);
+        MHD_CUDA(cudaMemsetAsync(I->H.p, 0, (size_t)(mr + 1) * mr * sizeof(double), s));
+        MHD_LAUNCH_CHECK();
+        if (I->mixed)
+        {
+            I->recon32.alloc(3 * (size_t)nnz_c); I->m32.alloc(ne); I->ecw32.alloc(nnz_ec); I->tv32.alloc(3 * ne); I->fa32.alloc(3 * nf);
+            I->vinv32.alloc(nc); I->alpha32.alloc(nc); I->B0_32.alloc(3 * nc); I->phi32.alloc(nf); I->s2phi32.alloc(nf);
+            I->b32.alloc(3 * nc); I->g32.alloc(3 * nc);
+            const int64_t nmax = std::max<int64_t>({3 * (int64_t)nnz_c, (int64_t)nnz_ec, (int64_t)ne, (int64_t)nf, (int64_t)nc});
+            if (nmax)
+                k_ind_tables32<<<grid_for(nmax, 256), 256, 0, s>>>(m, I->recon.p, I->mcoef.p, I->recon32.p, I->m32.p, I->ecw32.p,
+                                                                 I->tv32.p, I->fa32.p, I->vinv32.p);
+            if (nc)
+            {
+                MHD_CUDA(cudaMemsetAsync(I->alpha32.p, 0, nc * sizeof(float), s));
+                MHD_CUDA(cudaMemsetAsync(I->g32.p, 0, 3 * nc * sizeof(float), s));
+            }
+            MHD_LAUNCH_CHECK();
+        }
+        MHD_CUDA(cudaStreamSynchronize(s));
+        *out = I;
+    });
+    if (rc != MHD_OK) delete I;
+    return rc;
+}
+
+int mhd_gpu_induction_destroy(MhdInduction *I)
+{
+    return guarded([&] {
+        if (!I) return;
+        cudaStreamSynchronize(I->mesh->stream);
+        delete I;
+    });
+}
+
+int mhd_gpu_induction_set_frozen(MhdInduction *I, const double *B0, const double *ne_eff)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && B0 && ne_eff, "null argument");
+        const MeshView &m = I->mesh->v;
+        cudaStream_t s = I->mesh->stream;
+        if (!m.nc) return;
+        MHD_CUDA(cudaMemcpyAsync(I->B0.p, B0, 3 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        k_ind_alpha<<<g1(m.nc), 256, 0, s>>>(m.nc, I->taper.p, ne_eff, I->hall ? 1 : 0, I->p.hall_coef, I->alpha.p);
+        if (I->mixed)
+        {
+            k_to_float<<<g1(3 * (int64_t)m.nc), 256, 0, s>>>(I->B0.p, I->B0_32.p, 3 * (int64_t)m.nc);
+            k_to_float<<<g1(m.nc), 256, 0, s>>>(I->alpha.p, I->alpha32.p, m.nc);
+        }
+        MHD_LAUNCH_CHECK();
+    });
+}
+
+int mhd_gpu_induction_apply_F(MhdInduction *I, const double *phi, double *out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && phi && out, "null argument");
+        op64(I, MatIn{}, phi, 0.0, out);
+    });
+}
+
+int mhd_gpu_induction_apply_A(MhdInduction *I, const double *x, double dt, double *y)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && x && y, "null argument");
+        apply_plain(I, x, dt, y);
+    });
+}
+
+int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee, const int8_t *dir, double dt, int32_t warm, double *E,
+                            int32_t *iterations, double *rel_res)
+{
+    int status = MHD_OK;
+    int rc = guarded([&] {
+        MHD_REQUIRE(I && Phi && Ee && dir && E, "null argument");
+        const MeshView &m = I->mesh->v;
+        cudaStream_t s = I->mesh->stream;
+        const int32_t ne = m.ne;
+        if (iterations) *iterations = 0;
+        if (rel_res) *rel_res = 0.0;
+        if (ne == 0) return;
+        const int mr = I->p.restart;
+        const int ge = g1(ne);
+        if (!warm) I->have_corr = false;
+        double *sc = I->scal.p; // [0] |b|  [1] beta  [2] |g_{j+1}|
+        k_vec_x0<<<ge, 256, 0, s>>>(ne, Ee, I->have_corr ? I->corr.p : nullptr, dir, I->x0.p, I->delta.p);
+        op64(I, MatIn{}, Phi, 0.0, I->Fn.p);                          // F(Phi^n)
+        k_vec_add<<<ge, 256, 0, s>>>(ne, Ee, I->Fn.p, I->b.p);          // b = E_expl + F(Phi^n)
+        apply_plain(I, I->x0.p, dt, I->Ax.p);                         // A x0
+        k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p);
+        k_vec_pd<<<ge, 256, 0, s>>>(ne, dt, I->mcoef.p, I->d2.p, dir, I->pd.p);
+        MHD_LAUNCH_CHECK();
+        dev_dot(I, I->b.p, I->b.p, 2, sc + 0);
+        dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
+        const double bnorm = host_read(I, sc + 0);
+        double beta = host_read(I, sc + 1);
+        const double tol = I->p.rtol * bnorm;
+        int total = 0;
+        double *V = I->V.p, *H = I->H.p;
+        while (beta > tol && total < I->p.max_it)
+        {
+            k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, V);
+            k_g_init<<<1, 1, 0, s>>>(I->gv.p, mr + 1, sc + 1);
+            int j = 0;
+            for (; j < mr && total < I->p.max_it; ++j, ++total)
+            {
+                // w = A P^-1 V_j with V_j = w_prev / H(j, j-1) formed on the fly, Dirichlet rows zeroed,
+                // and the block partials of w . V_0
+                MatIn in;
+                in.src = j == 0 ? V : I->w.p;
+                in.hs = j == 0 ? nullptr : I->nrm.p + j;
+                in.pd = I->pd.p;
+                double *vout = j == 0 ? nullptr : V + (int64_t)j * ne;
+                if (I->mixed) op32(I, in, dt, I->w.p, vout, dir, V);
+                else op64(I, in, nullptr, dt, I->w.p, vout, dir, V);
+                k_dot_final<<<1, 1024, 0, s>>>(I->part.p, I->edge_blocks, 0, H + j);
+                // modified Gram-Schmidt (:340-345): w -= H(i-1, j) V_{i-1}, fused with H(i, j) = w . V_i
+                for (int i = 1; i <= j + 1; ++i)
+                {
+                    const double *Vi = i <= j ? V + (int64_t)i * ne : nullptr; // i = j+1: the norm of w
+                    k_mgs<<<kRedBlocks, 256, 0, s>>>(I->w.p, V + (int64_t)(i - 1) * ne, H + (int64_t)(i - 1) * mr + j, Vi, ne,
+                                                     m.no_edges, i & 1, I->part.p);
+                    k_dot_final<<<1, 1024, 0, s>>>(I->part.p, kRedBlocks, i <= j ? 0 : 1, H + (int64_t)i * mr + j);
+                }
+                k_givens<<<1, 1, 0, s>>>(H, mr, j, I->cs.p, I->sn.p, I->gv.p, I->nrm.p, sc + 2);
+                MHD_LAUNCH_CHECK();
+                if (host_read(I, sc + 2) <= tol)
+                {
+                    ++j;
+                    ++total;
+                    break;
+                }
+            }
+            k_backsub<<<1, 1, 0, s>>>(H, mr, j, I->gv.p, I->yv.p);
+            k_vec_update<<<ge, 256, 0, s>>>(ne, V, j, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p);
+            // true residual in FP64 (the outer iterative refinement of the mixed-precision solve)
+            apply_plain(I, I->z.p, dt, I->Ax.p);
+            k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p);
+            dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
+            beta = host_read(I, sc + 1);
+        }
+        k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p);
+        MHD_LAUNCH_CHECK();
+        MHD_CUDA(cudaStreamSynchronize(s));
+        I->have_corr = true;
+        if (iterations) *iterations = total;
+        if (rel_res) *rel_res = beta / bnorm;
+        if (beta > tol) status = MHD_ENOCONV;
+    });
+    return rc != MHD_OK ? rc : status;
+}
+
+} // extern "C"

@@ -49,6 +49,12 @@ class StepParams(ctypes.Structure):
                 ("absorb", ctypes.c_int8 * 16), ("precision", i32)]
 
 
+class InductionParams(ctypes.Structure):
+    """MhdInductionParams of include/mhd_gpu.h (the Config fields mhd::ImplicitInduction reads)."""
+    _fields_ = [("hall", i32), ("max_it", i32), ("restart", i32), ("precision", i32), ("hall_coef", dbl),
+                ("hall_r_min", dbl), ("hall_r_max", dbl), ("rtol", dbl)]
+
+
 FIELD_U, FIELD_PHI, FIELD_PHIADD, FIELD_BADD = 0, 1, 2, 3
 PREC_FP64, PREC_MIXED = 0, 1
 
@@ -80,6 +86,12 @@ _SIGS = {
     "mhd_gpu_faraday_edge_dt": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_div_b": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_cell_current": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_induction_create": ([vp, ctypes.POINTER(InductionParams), vp, ctypes.POINTER(vp)], ctypes.c_int),
+    "mhd_gpu_induction_destroy": ([vp], ctypes.c_int),
+    "mhd_gpu_induction_set_frozen": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_induction_apply_F": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_induction_apply_A": ([vp, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_induction_solve": ([vp, vp, vp, vp, dbl, i32, vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)], ctypes.c_int),
 }
 
 
@@ -401,3 +413,72 @@ class ResidentState:
         v = i64()
         check(lib().mhd_gpu_state_launches(self._h, ctypes.byref(v)))
         return v.value
+
+
+class DeviceInduction:
+    """mhd::ImplicitInduction on the device (Common/induction/ImplicitInduction.cpp; MhdInduction of include/mhd_gpu.h).
+
+    ``m_edge`` is the per-edge resistive coefficient m_e (the reference's ``m_``, ctor :16-22), ``None`` for
+    a Hall-only solve.  ``precision="mixed"`` runs the Arnoldi matvecs with the FP32 operator and keeps the
+    Krylov basis, Hessenberg, Givens and the true residual of every restart in FP64.  Vectors may be numpy
+    arrays or CUDA tensors; results are CUDA float64 tensors.  Like the reference, ``solve`` does not raise
+    when GMRES stops at ``max_it`` above ``rtol``: it returns the iterations and the relative residual.
+    """
+
+    def __init__(self, dmesh: DeviceMesh, m_edge=None, hall=False, hall_coef=0.0, hall_r_min=1.0, hall_r_max=1.012,
+                 rtol=1e-4, max_it=100, restart=20, precision="fp64"):
+        self.mesh = dmesh
+        p = InductionParams(int(bool(hall)), int(max_it), int(restart), PREC_MIXED if precision == "mixed" else PREC_FP64,
+                            float(hall_coef), float(hall_r_min), float(hall_r_max), float(rtol))
+        self.params = p
+        m = None if m_edge is None else np.ascontiguousarray(m_edge, np.float64)
+        h = vp()
+        check(lib().mhd_gpu_induction_create(dmesh.handle, ctypes.byref(p), None if m is None else m.ctypes.data_as(vp),
+                                             ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mhd_gpu_induction_destroy(self._h)
+            self._h = None
+
+    def set_frozen_state(self, B0, ne_eff):
+        B0, ne = dev(B0), dev(ne_eff)
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_set_frozen(self._h, ptr(B0), ptr(ne)))
+        self.mesh._leave()
+
+    def apply_F(self, phi):
+        torch = _torch()
+        phi = dev(phi)
+        out = torch.empty(self.mesh.n_edges, dtype=torch.float64, device="cuda")
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_apply_F(self._h, ptr(phi), ptr(out)))
+        self.mesh._leave()
+        return out
+
+    def apply_A(self, x, dt):
+        torch = _torch()
+        x = dev(x)
+        y = torch.empty(self.mesh.n_edges, dtype=torch.float64, device="cuda")
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_apply_A(self._h, ptr(x), float(dt), ptr(y)))
+        self.mesh._leave()
+        return y
+
+    def solve(self, Phi, E_expl, dirichlet, dt, warm=True, E=None):
+        """ImplicitInduction::solve (:299-390) -> (E, iterations, rel_res)."""
+        torch = _torch()
+        Phi, Ee = dev(Phi), dev(E_expl)
+        d = dev(np.ascontiguousarray(dirichlet, np.int8)) if not isinstance(dirichlet, torch.Tensor) else dirichlet.to(
+            torch.int8).contiguous().cuda()
+        if E is None:
+            E = torch.empty(self.mesh.n_edges, dtype=torch.float64, device="cuda")
+        it, rr = i32(), dbl()
+        self.mesh._enter()
+        rc = lib().mhd_gpu_induction_solve(self._h, ptr(Phi), ptr(Ee), ptr(d), float(dt), int(bool(warm)), ptr(E),
+                                           ctypes.byref(it), ctypes.byref(rr))
+        self.mesh._leave()
+        if rc != MHD_ENOCONV:
+            check(rc)
+        return E, it.value, rr.value

@@ -149,3 +149,67 @@ def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, mas
     return Workload(name=f"shell6x{ncube}x{ncube}x{nr}x6", mesh=m, n_species=n_species, gamma=GAMMA, U=U,
                     Phi=np.zeros(m.n_faces), PhiAdd=PhiAdd, fs=fs, mass=masses, u_inf=tuple(u_inf), B_imf=B_imf,
                     cfl=0.4, steps=100, extra=dict(stretch=stretch))
+
+
+def dipole_field(x, m=(0.0, 0.0, 1.0), c=(0.0, 0.0, 0.2), B_imf=(0.0, 0.0, -0.5)):
+    """Point-dipole field (3 (m.r^) r^ - m) / |r|^3 about c plus a uniform IMF, at the points x (n, 3)."""
+    r = np.asarray(x, np.float64) - np.asarray(c, np.float64)
+    d = np.linalg.norm(r, axis=1)
+    rh = r / d[:, None]
+    mv = np.asarray(m, np.float64)
+    return (3.0 * (rh @ mv)[:, None] * rh - mv) / (d ** 3)[:, None] + np.asarray(B_imf, np.float64)
+
+
+def whistler_dt(mesh: HostMesh, B0, ne, hall_coef, hall_r_min):
+    """Explicit Hall (whistler) time-step limit of mercury::Solver::collect (MercuryUns/driver/Solver.cpp:588-601):
+    min over fluid cells with r >= hall_r_min of h^2 n_e / (9.8696 hall_coef |B|), h = 6 V / sum_f |A_f|."""
+    ptr = np.asarray(mesh["c2f_ptr"])
+    area = np.add.reduceat(np.asarray(mesh["face_area_mag"])[np.asarray(mesh["c2f_idx"])], ptr[:-1])
+    h = 6.0 * np.asarray(mesh["cell_volume"]) / area
+    r = np.linalg.norm(np.asarray(mesh["cell_center"]), axis=1)
+    B = np.linalg.norm(np.asarray(B0).reshape(-1, 3), axis=1)
+    ok = (np.asarray(mesh["cell_material"]) != 1) & (r >= hall_r_min)
+    return float(np.min(h[ok] ** 2 * np.asarray(ne)[ok] / (9.8696 * hall_coef * np.maximum(B[ok], 1e-30))))
+
+
+@dataclass
+class InductionCase:
+    """Inputs of one semi-implicit induction solve (mhd::ImplicitInduction::solve)."""
+    name: str
+    mesh: HostMesh
+    m_edge: np.ndarray      # per-edge resistive coefficient m_e = eta(r_e) / star1_e
+    B0: np.ndarray          # frozen total field per cell (3 per cell)
+    ne: np.ndarray          # frozen effective electron density per cell
+    Phi: np.ndarray         # induced face flux Phi^n
+    E_expl: np.ndarray      # explicit EMF per edge
+    dirichlet: np.ndarray   # int8 per edge: edge_mode == 2 (far-field inflow edges keep E_expl)
+    dt: float
+    dt_whistler: float
+    hall_coef: float
+    hall_r_min: float
+    hall_r_max: float
+
+
+def induction_case(ncube=48, nr=96, r_in=0.8, r_out=6.0, eta_inner=1.0, eta_outer=1e-3, r_eta=1.0, hall_coef=1.0,
+                   hall_r_min=1.0, hall_r_max=1.012, dt_factor=20.0, seed=0, u_inf=(-8.0, 0.0, 0.0)):
+    """The semi-implicit Hall + resistive solve on a cubed-sphere shell r in [r_in, r_out] (6 tetrahedra per hexahedron,
+    nr geometric layers): eta = eta_inner below r_eta and eta_outer above it, set per edge as m_e = eta / star1_e; Hall
+    on with the reference's radial taper; B0 = dipole of moment 1 at (0, 0, 0.2) plus the IMF (0, 0, -0.5) at the cell
+    centres; n_e = 1 + U(0, 0.5) (seeded); Phi^n = d1 of 8 seeded Fourier modes of amplitude 0.05; E_expl = (-u x B0) . t
+    at the edge midpoints; dt = dt_factor x the explicit whistler limit.  ncube = 48, nr = 96 is the 7.96M-cell case."""
+    stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
+    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry()
+    m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
+    rng = np.random.default_rng(seed)
+    r_e = np.linalg.norm(np.asarray(m["edge_mid"]), axis=1)
+    m_edge = np.where(r_e < r_eta, eta_inner, eta_outer) / np.asarray(m["star1"])
+    B0 = dipole_field(np.asarray(m["cell_center"])).ravel()
+    ne = 1.0 + 0.5 * rng.uniform(0.0, 1.0, m.n_cells)
+    Phi = d1(m, fourier_potential(m, seed + 2, B0=(0.0, 0.0, 0.0)))
+    Bm = dipole_field(np.asarray(m["edge_mid"]))
+    E_expl = (-np.cross(np.asarray(u_inf, np.float64), Bm) * np.asarray(m["edge_vec"])).sum(1)
+    dirichlet = (np.asarray(m["edge_mode"]) == 2).astype(np.int8)
+    dtw = whistler_dt(m, B0, ne, hall_coef, hall_r_min)
+    return InductionCase(name=f"shell6x{ncube}x{ncube}x{nr}x6_r{r_in:g}-{r_out:g}", mesh=m, m_edge=m_edge, B0=B0, ne=ne, Phi=Phi,
+                         E_expl=E_expl, dirichlet=dirichlet, dt=dt_factor * dtw, dt_whistler=dtw, hall_coef=hall_coef,
+                         hall_r_min=hall_r_min, hall_r_max=hall_r_max)

@@ -1,0 +1,181 @@
+"""Semi-implicit Hall / resistive induction on the device against the oracle and the reference's golden vectors.
+
+The operator (apply_F, apply_A) mirrors the reference's summation order and must agree to 1e-13
+relative (FP64).  GMRES's dot products are block reductions whose rounding differs from the
+reference's sequential sums, so solves are compared through what GMRES guarantees: the true
+relative residual is at most rtol, E agrees with the oracle's E to within a small multiple of
+rtol, the iteration counts agree to within two, and Dirichlet edges keep E_expl exactly.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import MIXED_BOX_BC, SHELL_BC, rel_err
+from mpcns_uns_b200.mesh import HostMesh
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+OP_TOL = 1e-13
+
+port = pytest.importorskip("oracle.port")
+
+
+def _np(t):
+    return t.detach().cpu().numpy()
+
+
+def _box():
+    return HostMesh.box(6, 5, 4, tets=True, jitter=0.1, seed=8).compute_geometry().boundary(*MIXED_BOX_BC)
+
+
+def _shell():
+    return HostMesh.shell(5, 6, 0.8, 4.0, 1.3, n_solid=1, tets=True).compute_geometry().boundary(*SHELL_BC)
+
+
+_cache = {}
+
+
+def _mesh(name):
+    if name not in _cache:
+        from mpcns_uns_b200.gpu import DeviceMesh
+        h = _box() if name == "box" else _shell()
+        _cache[name] = (h, DeviceMesh(h), port.PortMesh(h))
+    return _cache[name]
+
+
+def _setup(name, hall, resistive, seed=12, **kw):
+    from mpcns_uns_b200.gpu import DeviceInduction
+    h, dm, pm = _mesh(name)
+    rng = np.random.default_rng(seed)
+    m_edge = rng.uniform(0.5, 2.0, h.n_edges) / np.asarray(h["star1"]) if resistive else None
+    taper = dict(hall_r_min=-100.0, hall_r_max=-99.0) if name == "box" else dict(hall_r_min=1.0, hall_r_max=1.6)
+    args = dict(hall=hall, hall_coef=0.5, rtol=1e-10, max_it=200, restart=15, **taper)
+    args.update(kw)
+    prec = args.pop("precision", "fp64")
+    di = DeviceInduction(dm, m_edge, precision=prec, **args)
+    oi = port.PortInduction(pm, m_edge, **args)
+    B0 = rng.uniform(-1, 1, 3 * h.n_cells)
+    ne = rng.uniform(0.5, 2.0, h.n_cells)
+    di.set_frozen_state(B0, ne)
+    oi.set_frozen_state(B0, ne)
+    return h, di, oi, rng
+
+
+CASES = [("box", True, False), ("box", False, True), ("box", True, True), ("shell", True, True), ("shell", True, False)]
+
+
+@pytest.mark.parametrize("name,hall,resistive", CASES)
+def test_operator_matches_oracle(name, hall, resistive):
+    h, di, oi, rng = _setup(name, hall, resistive)
+    for _ in range(2):
+        phi = rng.uniform(-1, 1, h.n_faces)
+        assert rel_err(_np(di.apply_F(phi)), oi.apply_F(phi)) <= OP_TOL
+        x = rng.uniform(-1, 1, h.n_edges)
+        for dt in (0.05, 3.0):
+            assert rel_err(_np(di.apply_A(x, dt)), oi.apply_A(x, dt)) <= OP_TOL
+
+
+def _true_rel_res(di, phi, Ee, E, dirichlet, dt):
+    b = Ee + _np(di.apply_F(phi))
+    r = b - _np(di.apply_A(E, dt))
+    r[dirichlet != 0] = 0.0
+    return np.linalg.norm(r) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("name,hall,resistive", CASES)
+def test_solve_matches_oracle(name, hall, resistive):
+    h, di, oi, rng = _setup(name, hall, resistive)
+    dirichlet = (np.asarray(h["edge_mode"]) == 2).astype(np.int8)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    Ee = rng.uniform(-1, 1, h.n_edges)
+    dt = 0.01
+    for warm in (False, True):
+        Ed, itd, rrd = di.solve(phi, Ee, dirichlet, dt, warm)
+        Eo, ito, rro = oi.solve(phi, Ee, dirichlet, dt, warm)
+        Ed = _np(Ed)
+        assert rrd <= 1e-10 and rro <= 1e-10
+        assert abs(itd - ito) <= 2, (itd, ito)
+        assert rel_err(Ed, Eo) <= 1e-8
+        assert _true_rel_res(di, phi, Ee, Ed, dirichlet, dt) <= 2e-10
+        assert np.array_equal(Ed[dirichlet != 0], Ee[dirichlet != 0])
+
+
+def test_golden_vectors():
+    """The reference's own apply_F / apply_A / solve outputs (tests/golden/induction_box.npz)."""
+    from mpcns_uns_b200.gpu import DeviceInduction
+    g = np.load(os.path.join(HERE, "golden", "induction_box.npz"))
+    h, dm, _ = _mesh("box")
+    assert int(h.topology_hash()) == int(g["topology_hash"])
+    di = DeviceInduction(dm, g["in_m"], hall=True, hall_coef=0.5, hall_r_min=-100.0, hall_r_max=-99.0, rtol=1e-10, max_it=200,
+                         restart=15)
+    di.set_frozen_state(g["in_B0"], g["in_ne"])
+    assert rel_err(_np(di.apply_F(g["in_phi"])), g["apply_F"]) <= OP_TOL
+    assert rel_err(_np(di.apply_A(g["in_x"], 0.05)), g["apply_A"]) <= OP_TOL
+    dirichlet = (np.asarray(h["edge_mode"]) == 2).astype(np.int8)
+    for warm in (0, 1):
+        E, it, rr = di.solve(g["in_phi"], g["in_Ee"], dirichlet, 0.05, bool(warm))
+        assert rel_err(_np(E), g[f"solve{warm}_E"]) <= 1e-8
+        assert abs(it - int(g[f"solve{warm}_it"])) <= 2
+        assert rr <= 1e-10
+
+
+@pytest.mark.parametrize("name", ["box", "shell"])
+def test_mixed_precision_refines_to_fp64(name):
+    """FP32 operator inside the Arnoldi, FP64 true residual at every restart: the FP64 tolerance is met."""
+    h, di, oi, rng = _setup(name, True, True, precision="mixed")
+    dirichlet = (np.asarray(h["edge_mode"]) == 2).astype(np.int8)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    Ee = rng.uniform(-1, 1, h.n_edges)
+    Ed, itd, rrd = di.solve(phi, Ee, dirichlet, 0.05, False)
+    Eo, ito, _ = oi.solve(phi, Ee, dirichlet, 0.05, False)
+    Ed = _np(Ed)
+    assert rrd <= 1e-10
+    assert _true_rel_res(di, phi, Ee, Ed, dirichlet, 0.05) <= 2e-10
+    assert rel_err(Ed, Eo) <= 1e-8
+    assert itd <= 2 * ito + 15
+    assert np.array_equal(Ed[dirichlet != 0], Ee[dirichlet != 0])
+
+
+def test_no_convergence_is_reported_not_raised():
+    """max_it reached above rtol: the reference returns iterations and rel_res without throwing."""
+    h, di, oi, rng = _setup("box", True, True, rtol=1e-15, max_it=4)
+    dirichlet = np.zeros(h.n_edges, np.int8)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    Ee = rng.uniform(-1, 1, h.n_edges)
+    E, it, rr = di.solve(phi, Ee, dirichlet, 0.05, False)
+    Eo, ito, rro = oi.solve(phi, Ee, dirichlet, 0.05, False)
+    assert it == ito == 4
+    assert rr > 1e-15 and rr == pytest.approx(rro, rel=1e-6)
+    assert rel_err(_np(E), Eo) <= 1e-10
+
+
+def test_cold_start_resets_warm_correction():
+    h, di, oi, rng = _setup("box", True, True)
+    dirichlet = np.zeros(h.n_edges, np.int8)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    Ee = rng.uniform(-1, 1, h.n_edges)
+    E1, it1, _ = di.solve(phi, Ee, dirichlet, 0.05, False)
+    E2, it2, _ = di.solve(phi, Ee, dirichlet, 0.05, True)
+    E3, it3, _ = di.solve(phi, Ee, dirichlet, 0.05, False)
+    assert it2 <= 2 < it1 and it3 == it1
+    assert rel_err(_np(E3), _np(E1)) <= 1e-13
+
+
+def test_large_shell_residual_property():
+    """A 262k-edge shell: the solve meets rtol in the true FP64 residual (size-independent check), both precisions."""
+    from mpcns_uns_b200 import workloads
+    from mpcns_uns_b200.gpu import DeviceInduction, DeviceMesh
+    case = workloads.induction_case(ncube=16, nr=24)
+    dm = DeviceMesh(case.mesh)
+    res = {}
+    for prec in ("fp64", "mixed"):
+        di = DeviceInduction(dm, case.m_edge, hall=True, hall_coef=case.hall_coef, hall_r_min=case.hall_r_min,
+                             hall_r_max=case.hall_r_max, rtol=1e-8, max_it=400, restart=30, precision=prec)
+        di.set_frozen_state(case.B0, case.ne)
+        E, it, rr = di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)
+        E = _np(E)
+        assert rr <= 1e-8, (prec, it, rr)
+        assert _true_rel_res(di, case.Phi, case.E_expl, E, case.dirichlet, case.dt) <= 1.5e-8
+        res[prec] = (E, it)
+    assert rel_err(res["mixed"][0], res["fp64"][0]) <= 1e-6
