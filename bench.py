@@ -12,6 +12,13 @@ UCT EMF + CT, floors, SSP-RK2 average, all on the device.  Metric: cell-updates/
 (cells x species x 2 stages per step).  Inputs exceed L2 (126 MB) many times over, so no
 flush is needed between steps.
 
+The line's "gmres" object is the second half of the metric: the semi-implicit Hall + resistive
+induction solve (ImplicitInduction::solve) on the cubed-sphere shell r in [0.8, 6], 6 x 48 x 48 x 96
+x 6 tetrahedra (7,962,624 cells, 9,331,392 edge unknowns), eta = 1 below r = 1 and 1e-3 above, Hall
+on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, cold start, capped at
+--gmres-max-it iterations: seconds per solve in FP64 and mixed precision, per-kernel GB/s, and the
+reference's own solve on a bounded sample beside it.
+
 Under torchrun (N > 1) every rank runs an independent replica on its own GPU (the hot path
 has no data-path exchange on one mesh per GPU); value = all ranks' cell-updates / max time.
 """
@@ -199,6 +206,104 @@ def time_reference(wl, steps, warmup):
     return wl.mesh.n_cells * wl.n_species * 2 / per_step, per_step
 
 
+def gmres_bytes(k, c, precision, steps, mgs_launches):
+    """Compulsory bytes of one launch of kernel class k of the induction solve, in the form the
+    Arnoldi step runs it (preconditioned input, lazily normalised basis vector, Dirichlet mask, dot
+    with V_0).  q = bytes of the operator's arrays (8 FP64, 4 for the FP32 operator of the mixed solve);
+    Krylov vectors are FP64.  mgs: one launch reads w, V_{i-1}, V_i and writes w (the last of a step
+    reads w and V_j only), so a solve of `steps` Arnoldi steps and L launches moves (4L - steps) vectors."""
+    q = 4 if precision == "mixed" else 8
+    nc, nf, ne = c["nc"], c["nf"], c["ne"]
+    if k == "face_d1":
+        return 4 * (nf + 1) + 5 * c["f2e"] + 16 * ne + 8 * nf + 2 * q * nf
+    if k == "cell_field":
+        return 4 * (nc + 1) + 4 * c["c2f"] + 3 * q * c["c2f"] + q * nf + 3 * q * nc
+    if k == "hall_emf":
+        return 4 * nc + 5 * c["c2f"] + 4 * nf + 4 * c["f2c"] + 3 * q * nf + 11 * q * nc + nc
+    if k == "edge_gather":
+        return 8 * ne + 5 * c["e2f"] + q * nf + (4 + q) * c["ec"] + 4 * q * ne + 3 * q * nc + 41 * ne
+    if k == "mgs":
+        return (4 * mgs_launches - steps) * 8 * ne / max(mgs_launches, 1)
+    return 0
+
+
+def bench_gmres(args, peak):
+    """Semi-implicit Hall + resistive induction solve (ImplicitInduction::solve) on the r in [0.8, 6]
+    shell: GMRES(30), Jacobi, rtol 1e-8, dt = 20 x the explicit whistler limit, cold start; FP64 and
+    mixed (FP32 operator in the Arnoldi, FP64 basis / Hessenberg / true residual)."""
+    import torch
+    from mpcns_uns_b200 import gpu, workloads
+    t = time.time()
+    case = workloads.induction_case(args.gmres_ncube, args.gmres_nr)
+    h = case.mesh
+    log(f"[bench] induction workload {case.name}: {h.n_cells} cells, {h.n_edges} edges (setup {time.time() - t:.1f}s)")
+    dm = gpu.DeviceMesh(h)
+    counts = mesh_counts(h)
+    out = {"workload": case.name, "cells": h.n_cells, "faces": h.n_faces, "edges": h.n_edges, "restart": 30, "rtol": 1e-8,
+           "max_it": args.gmres_max_it, "dt": case.dt, "dt_over_whistler_limit": case.dt / case.dt_whistler,
+           "solves_timed": args.gmres_solves}
+    E = {}
+    for prec in ("fp64", "mixed"):
+        di = gpu.DeviceInduction(dm, case.m_edge, hall=True, hall_coef=case.hall_coef, hall_r_min=case.hall_r_min,
+                                 hall_r_max=case.hall_r_max, rtol=1e-8, max_it=args.gmres_max_it, restart=30, precision=prec)
+        di.set_frozen_state(case.B0, case.ne)
+        di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)  # warm-up (captures the cycle graph)
+        torch.cuda.synchronize()
+        l0 = di.launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(dm.stream)
+        for _ in range(args.gmres_solves):
+            Ed, it, rr = di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)
+        ev1.record(dm.stream)
+        ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.gmres_solves
+        launches = (di.launches() - l0) // args.gmres_solves
+        # one more solve with per-kernel events (direct launches instead of the graph)
+        di.profile(True)
+        di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)
+        prof = di.profile_read()
+        di.profile(False)
+        mgs_l = prof.get("mgs", (0, 0))[1]
+        kern = {}
+        for k, (kms, n) in prof.items():
+            if not n:
+                continue
+            b = gmres_bytes(k, counts, prec, it, mgs_l)
+            kern[k] = {"ms_per_solve": kms, "launches_per_solve": n, "GBps": b / (kms / n / 1e3) / 1e9 if b else None}
+        top = max((k for k in kern if kern[k]["GBps"]), key=lambda k: kern[k]["ms_per_solve"])
+        E[prec] = Ed.double().cpu().numpy()
+        out[prec] = {"s_per_solve": ms / 1e3, "iterations": it, "rel_res": rr, "converged": rr <= 1e-8,
+                     "ms_per_iteration": ms / max(it, 1), "gpu_launches_per_solve": launches, "kernels": kern,
+                     "roofline": {"bound": "hbm", "kernel": top, "achieved": kern[top]["GBps"], "peak": peak, "unit": "GB/s",
+                                  "frac": kern[top]["GBps"] / peak}}
+        del di
+    out["speedup_mixed"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
+    out["E_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(E["mixed"] - E["fp64"]) / np.linalg.norm(E["fp64"]))
+    out["rel_res_ratio_mixed_vs_fp64"] = out["mixed"]["rel_res"] / out["fp64"]["rel_res"]
+    return out
+
+
+def gmres_cpu_baseline(max_it=60):
+    """ImplicitInduction::solve of the reference (oracle/_ref, np = 1, one core) on the same construction at
+    6 x 16 x 16 x 24 (262,704 edges), cold start, `max_it` iterations: seconds per GMRES iteration."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle import ref
+    from helpers import SHELL_TAGS, ref_twin
+    from mpcns_uns_b200 import workloads
+    case = workloads.induction_case(16, 24)
+    r = ref_twin(case.mesh, SHELL_TAGS).boundary("outflow", {"inner": "wall", "outer": "farfield"}, (-8.0, 0.0, 0.0))
+    ri = ref.RefInduction(r, hall=True, hall_coef=case.hall_coef, hall_r_min=case.hall_r_min, hall_r_max=case.hall_r_max,
+                          rtol=1e-8, max_it=max_it, restart=30)
+    ri.set_m(case.m_edge)
+    ri.set_frozen_state(case.B0, case.ne)
+    t0 = time.perf_counter()
+    _, it, rr = ri.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)
+    el = time.perf_counter() - t0
+    return {"ms_per_iteration": 1e3 * el / max(it, 1), "iterations": it, "rel_res": rr, "cores": 1, "kind": "reference",
+            "sample": f"{case.name} ({case.mesh.n_edges} edges), one cold solve capped at {max_it} iterations, np=1",
+            "edges": case.mesh.n_edges}
+
+
 def max_over_ranks(ms, dist, device):
     """The slowest rank's device time: every rank's K steps count once, the job ends with the last."""
     if dist is None:
@@ -222,6 +327,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--accuracy-steps", type=int, default=100)
+    ap.add_argument("--no-gmres", action="store_true")
+    ap.add_argument("--gmres-ncube", type=int, default=48)
+    ap.add_argument("--gmres-nr", type=int, default=96)
+    ap.add_argument("--gmres-max-it", type=int, default=300)
+    ap.add_argument("--gmres-solves", type=int, default=2)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -383,6 +493,19 @@ def main():
         except Exception as e:  # the baseline is reported, never required
             log(f"[bench] cpu baseline failed: {e}")
 
+    gm = None
+    if rank == 0 and not args.no_gmres:
+        del st64, st32, st
+        torch.cuda.empty_cache()
+        gm = bench_gmres(args, peak)
+        if not args.no_cpu_baseline:
+            try:
+                from oracle import ref
+                if ref.available():
+                    gm["cpu_baseline"] = gmres_cpu_baseline()
+            except Exception as e:
+                log(f"[bench] gmres cpu baseline failed: {e}")
+
     if rank == 0:
         out = {"metric": METRIC, "value": rmx["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": rmx["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -402,7 +525,7 @@ def main():
                         "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
                "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-               "cpu_baseline": cpu, "clocks": clocks}
+               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm}
         print(json.dumps(out))
     if dist:
         dist.barrier()

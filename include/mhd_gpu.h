@@ -153,6 +153,14 @@ int mhd_gpu_induction_apply_A(MhdInduction *ind, const double *x, double dt, dou
  * rel_res set) when max_it is reached above rtol, which the reference reports without throwing. */
 int mhd_gpu_induction_solve(MhdInduction *ind, const double *Phi, const double *E_expl, const int8_t *dirichlet, double dt,
                             int32_t warm, double *E, int32_t *iterations, double *rel_res);
+/* Per-kernel-class device time of the solve (CUDA events on the mesh stream while enabled; classes:
+ * face_d1, cell_field, hall_emf, edge_gather, mgs, krylov_scalar, krylov_vector; a profiled solve
+ * launches its kernels one by one instead of replaying the restart-cycle graph), read as
+ * in mhd_gpu_state_profile_read; and the number of kernels the handle has launched. */
+int mhd_gpu_induction_profile(MhdInduction *ind, int32_t enable);
+int mhd_gpu_induction_profile_read(MhdInduction *ind, int32_t max_kernels, char *names, double *ms_total, int64_t *count,
+                                   int32_t *n_out);
+int mhd_gpu_induction_launches(MhdInduction *ind, int64_t *out);
 
 /* ------------------------------------------------------------------ resident state, fused step
  * The explicit step of mercury::Solver::step (MercuryUns/driver/Solver.cpp:481-516) restricted to

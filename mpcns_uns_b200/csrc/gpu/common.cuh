@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "mhd_gpu.h"
@@ -169,6 +170,56 @@ struct MeshView
 constexpr int kMaxValence = 32; // faces per edge handled by the UCT edge kernel (checked at mesh creation)
 
 inline int grid_for(int64_t n, int block) { return static_cast<int>((n + block - 1) / block); }
+
+// Per-kernel-class device time: CUDA event pairs recorded on the launching stream while `on`;
+// events are created on first use and reused after each read.
+template <int N> struct EventProfiler
+{
+    bool on = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[N];
+    size_t used[N] = {};
+    ~EventProfiler()
+    {
+        for (auto &v : ev)
+            for (auto &p : v)
+            {
+                cudaEventDestroy(p.first);
+                cudaEventDestroy(p.second);
+            }
+    }
+    void begin(int k, cudaStream_t s)
+    {
+        if (!on) return;
+        if (used[k] == ev[k].size())
+        {
+            cudaEvent_t a, b;
+            MHD_CUDA(cudaEventCreate(&a));
+            MHD_CUDA(cudaEventCreate(&b));
+            ev[k].emplace_back(a, b);
+        }
+        MHD_CUDA(cudaEventRecord(ev[k][used[k]].first, s));
+    }
+    void end(int k, cudaStream_t s)
+    {
+        if (!on) return;
+        MHD_CUDA(cudaEventRecord(ev[k][used[k]].second, s));
+        ++used[k];
+    }
+    // summed milliseconds and launch count of class k since the last read (the stream must be idle)
+    void read(int k, double &ms_total, int64_t &count)
+    {
+        double tot = 0;
+        for (size_t i = 0; i < used[k]; ++i)
+        {
+            float ms = 0;
+            MHD_CUDA(cudaEventElapsedTime(&ms, ev[k][i].first, ev[k][i].second));
+            tot += ms;
+        }
+        ms_total = tot;
+        count = static_cast<int64_t>(used[k]);
+        used[k] = 0;
+    }
+};
 } // namespace mhd
 
 struct MhdMesh

@@ -14,10 +14,13 @@
 //   * the Jacobi preconditioner z = dir ? 0 : V_j / (1 + dt m d2) is applied while gathering z in d1;
 //   * V_j = w / H(j, j-1) is formed lazily in the next matvec (the face pass gathers w / h, the edge
 //     pass stores V_j), so w is not re-read to normalise it;
-//   * the edge pass zeroes the Dirichlet rows of w and produces the block partials of w . V_0;
+//   * the edge pass zeroes the Dirichlet rows of w and produces H(0, j) = w . V_0;
 //   * each modified Gram-Schmidt subtraction w -= H(i-1, j) V_{i-1} is fused with the next dot w . V_i,
 //     and consecutive passes sweep the edges in opposite directions so that the tail of w and V_{i-1}
-//     that the previous pass left in L2 is reused first.
+//     that the previous pass left in L2 is reused first;
+//   * every dot finishes in the kernel that produces it (the last block adds the block partials), and
+//     a restart cycle runs as one CUDA graph whose steps test a device-side flag, so the host waits
+//     once per restart instead of once per Arnoldi step.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -30,6 +33,11 @@ namespace mhd
 namespace
 {
 constexpr int kRedBlocks = 8 * 148; // streaming reductions: 8 resident 256-thread blocks per SM
+
+// kernel classes of the solve, timed with CUDA events on the handle's stream when profiling is on
+enum IndKernel { KI_FACE = 0, KI_BCELL, KI_HALL, KI_EDGE, KI_MGS, KI_SCALAR, KI_VECTOR, KI_COUNT };
+const char *const kIndKernelNames[KI_COUNT] = {"face_d1", "cell_field", "hall_emf",     "edge_gather",
+                                               "mgs",     "krylov_scalar", "krylov_vector"};
 
 __device__ __forceinline__ double block_sum(double v)
 {
@@ -44,6 +52,47 @@ __device__ __forceinline__ double block_sum(double v)
         for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     }
     return v;
+}
+
+// Device-side control of one restart cycle: the Arnoldi steps of a cycle are enqueued (or replayed as
+// one CUDA graph) without host round trips; a step whose predecessor met the tolerance, or that lies
+// beyond the iteration limit, returns at once.
+struct Ctl
+{
+    int done, jend, limit, pad;
+    double tol, dt;
+};
+struct Gate
+{
+    const Ctl *ctl = nullptr;
+    int j = 0;
+    __device__ __forceinline__ bool off() const { return ctl && (ctl->done || j >= ctl->limit); }
+};
+
+// Block partials of a grid-wide sum; the last block to finish adds them in block order (deterministic)
+// and stores op(sum) to *out (op 0: the sum, 1: its square root, 2: sqrt(max(sum, 1e-300))), then
+// re-arms the counter.  No block waits for another.
+__device__ __forceinline__ void grid_sum_tail(double v, double *part, unsigned *counter, int op, double *out)
+{
+    __shared__ bool last;
+    v = block_sum(v);
+    if (threadIdx.x == 0)
+    {
+        part[blockIdx.x] = v;
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double s = 0.0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) s += __ldcg(part + i);
+    s = block_sum(s);
+    if (threadIdx.x == 0)
+    {
+        *out = op == 0 ? s : (op == 1 ? sqrt(s) : sqrt(dmax(s, 1e-300)));
+        *counter = 0;
+    }
 }
 
 // ---------------------------------------------------------------- one-time tables
@@ -145,10 +194,10 @@ __device__ __forceinline__ double mat_in(const MatIn &in, int32_t e)
 // Phi' = d1 x on every face (:185-190), with star2 Phi' for the resistive current flux (:131-136).
 // FP64 sums in both precisions; the FP32 operator stores the rounded results.
 template <class T>
-__global__ void k_ind_face(MeshView m, MatIn in, int hall, int resistive, T *__restrict__ phi, T *__restrict__ s2phi)
+__global__ void k_ind_face(MeshView m, Gate gt, MatIn in, int hall, int resistive, T *__restrict__ phi, T *__restrict__ s2phi)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= m.nf) return;
+    if (f >= m.nf || gt.off()) return;
     double s = 0;
     for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) s += m.f2e_sgn[k] * mat_in(in, m.f2e_idx[k]);
     if (hall) phi[f] = static_cast<T>(s);
@@ -163,10 +212,10 @@ __global__ void k_ind_s2phi(MeshView m, const double *__restrict__ phi, double *
 
 // cell field from the face fluxes (:139-149)
 template <class T>
-__global__ void k_ind_bcell(MeshView m, const T *__restrict__ recon, const T *__restrict__ phi, T *__restrict__ b)
+__global__ void k_ind_bcell(MeshView m, Gate gt, const T *__restrict__ recon, const T *__restrict__ phi, T *__restrict__ b)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
+    if (c >= m.nc || gt.off()) return;
     T bx = 0, by = 0, bz = 0;
     for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
     {
@@ -181,11 +230,11 @@ __global__ void k_ind_bcell(MeshView m, const T *__restrict__ recon, const T *__
 // Hall EMF per owned cell (:159-178): J_c = (1/V) sum s A x 1/2 (b_c + b_nb), g_c = alpha_c J_c x B0_c.
 // g_c = 0 where the reference skips the cell (alpha = 0, or not fluid: its ce list is empty), so that
 // the edge gather may add every owned cell: adding the zero product leaves each sum unchanged.
-__global__ void k_ind_hall(MeshView m, const double *__restrict__ b, const double *__restrict__ alpha, const double *__restrict__ B0,
-                           double *__restrict__ g)
+__global__ void k_ind_hall(MeshView m, Gate gt, const double *__restrict__ b, const double *__restrict__ alpha,
+                           const double *__restrict__ B0, double *__restrict__ g)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.no_cells) return;
+    if (c >= m.no_cells || gt.off()) return;
     if (alpha[c] == 0.0 || m.material[c] != 0)
     {
         st3(g, c, mk(0, 0, 0));
@@ -209,11 +258,12 @@ __global__ void k_ind_hall(MeshView m, const double *__restrict__ b, const doubl
     st3(g, c, alpha[c] * cross(J, ld3(B0, c)));
 }
 
-__global__ void k_ind_hall32(MeshView m, const float *__restrict__ b, const float *__restrict__ alpha, const float *__restrict__ B0,
-                             const float *__restrict__ fa, const float *__restrict__ vinv, float *__restrict__ g)
+__global__ void k_ind_hall32(MeshView m, Gate gt, const float *__restrict__ b, const float *__restrict__ alpha,
+                             const float *__restrict__ B0, const float *__restrict__ fa, const float *__restrict__ vinv,
+                             float *__restrict__ g)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.no_cells) return;
+    if (c >= m.no_cells || gt.off()) return;
     const float a = alpha[c];
     if (a == 0.f || m.material[c] != 0)
     {
@@ -254,11 +304,14 @@ template <class T> struct EdgeArgs
     const T *s2phi = nullptr, *g = nullptr, *mcoef = nullptr, *ecw = nullptr, *tvec = nullptr;
     MatIn in;                    // x of y = x + dt F; no input: y = F (apply_F)
     double dt = 0;
+    const double *dtp = nullptr; // dt read from the cycle control instead
     double *vout = nullptr;      // stores src / *hs (the lazily normalised Krylov vector V_j)
     const int8_t *dir = nullptr; // zero y on Dirichlet edges (:339)
-    const double *v0 = nullptr;  // block partials of y . v0 over the owned edges
-    double *part = nullptr;
+    const double *v0 = nullptr;  // y . v0 over the owned edges, stored to *dot
+    double *part = nullptr, *dot = nullptr;
+    unsigned *counter = nullptr;
     double *out = nullptr;
+    Gate gt;
 };
 
 // Per edge: part0 = sum_f s star2 Phi' (resistive, ascending faces), part1 = sum_c g_c . (w_ec t_e)
@@ -266,6 +319,7 @@ template <class T> struct EdgeArgs
 template <class T>
 __global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
 {
+    if (a.gt.off()) return;
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     double contrib = 0.0;
     if (e < m.ne)
@@ -299,38 +353,35 @@ __global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
             }
             else
                 xe = a.in.x[e];
-            y = xe + a.dt * static_cast<double>(F);
+            y = xe + (a.dtp ? *a.dtp : a.dt) * static_cast<double>(F);
         }
         if (a.dir && a.dir[e]) y = 0.0;
         a.out[e] = y;
         if (a.v0 && e < m.no_edges) contrib = y * a.v0[e];
     }
-    if (a.v0)
-    {
-        contrib = block_sum(contrib);
-        if (threadIdx.x == 0) a.part[blockIdx.x] = contrib;
-    }
+    if (a.v0) grid_sum_tail(contrib, a.part, a.counter, 0, a.dot);
 }
 
 // ---------------------------------------------------------------- Krylov vectors (FP64)
-// a . b over the owned edges, block partials (deterministic order)
-__global__ void __launch_bounds__(256) k_dot_part(const double *__restrict__ a, const double *__restrict__ b, int32_t n,
-                                                   double *__restrict__ part)
+// a . b over the owned edges -> op(sum) in *out
+__global__ void __launch_bounds__(256) k_dot(const double *__restrict__ a, const double *__restrict__ b, int32_t n, double *part,
+                                             unsigned *counter, int op, double *out)
 {
     double s = 0.0;
     for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) s += a[i] * b[i];
-    s = block_sum(s);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    grid_sum_tail(s, part, counter, op, out);
 }
 
-// Modified Gram-Schmidt step fused with the next dot: w -= (*h) Vprev on all edges (if Vprev), then
-// block partials of w . Vi over the owned edges (Vi null: w . w).  `reverse` sweeps from the last edge.
-__global__ void __launch_bounds__(256) k_mgs(double *__restrict__ w, const double *__restrict__ Vprev, const double *__restrict__ h,
-                                              const double *__restrict__ Vi, int32_t n_all, int32_t n_owned, int reverse,
-                                              double *__restrict__ part)
+// Modified Gram-Schmidt step fused with the next dot (:340-345): w -= (*h) Vprev on all edges, then
+// *out = w . Vi over the owned edges (Vi null: |w|).  `reverse` sweeps from the last edge so that what
+// the previous pass left in L2 is read first.
+__global__ void __launch_bounds__(256) k_mgs(Gate gt, double *__restrict__ w, const double *__restrict__ Vprev,
+                                              const double *__restrict__ h, const double *__restrict__ Vi, int32_t n_all,
+                                              int32_t n_owned, int reverse, double *part, unsigned *counter, double *out)
 {
+    if (gt.off()) return;
     constexpr int U = 4;
-    const double hv = Vprev ? *h : 0.0;
+    const double hv = *h;
     const int32_t stride = gridDim.x * blockDim.x;
     double s = 0.0;
     for (int32_t t0 = blockIdx.x * blockDim.x + threadIdx.x; t0 < n_all; t0 += U * stride)
@@ -345,7 +396,7 @@ __global__ void __launch_bounds__(256) k_mgs(double *__restrict__ w, const doubl
             if (idx[u] >= 0)
             {
                 wv[u] = w[idx[u]];
-                pv[u] = Vprev ? Vprev[idx[u]] : 0.0;
+                pv[u] = Vprev[idx[u]];
                 iv[u] = Vi ? Vi[idx[u]] : 0.0;
             }
         }
@@ -353,26 +404,12 @@ __global__ void __launch_bounds__(256) k_mgs(double *__restrict__ w, const doubl
         for (int u = 0; u < U; ++u)
         {
             if (idx[u] < 0) continue;
-            double wi = wv[u];
-            if (Vprev)
-            {
-                wi -= hv * pv[u];
-                w[idx[u]] = wi;
-            }
+            const double wi = wv[u] - hv * pv[u];
+            w[idx[u]] = wi;
             if (idx[u] < n_owned) s += wi * (Vi ? iv[u] : wi);
         }
     }
-    s = block_sum(s);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
-}
-
-// *out = sum of the partials (op 1: its square root, op 2: sqrt(max(sum, 1e-300)))
-__global__ void __launch_bounds__(1024) k_dot_final(const double *__restrict__ part, int n, int op, double *__restrict__ out)
-{
-    double s = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s += part[i];
-    s = block_sum(s);
-    if (threadIdx.x == 0) *out = op == 0 ? s : (op == 1 ? sqrt(s) : sqrt(dmax(s, 1e-300)));
+    grid_sum_tail(s, part, counter, Vi ? 0 : 1, out);
 }
 
 __global__ void k_vec_x0(int32_t n, const double *Ee, const double *corr, const int8_t *dir, double *x0, double *delta)
@@ -393,11 +430,13 @@ __global__ void k_vec_resid(int32_t n, const double *b, const double *Ax, const 
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) r[i] = dir[i] ? 0.0 : b[i] - Ax[i];
 }
-// pd = dir ? 0 : 1 / (1 + dt m d2)  (Jacobi, :315-316)
-__global__ void k_vec_pd(int32_t n, double dt, const double *mc, const double *d2, const int8_t *dir, double *pd)
+// pd = dir ? 0 : 1 / (1 + dt m d2)  (Jacobi, :315-316); dirc = the caller's Dirichlet flags, kept for the cycle
+__global__ void k_vec_pd(int32_t n, double dt, const double *mc, const double *d2, const int8_t *dir, double *pd, int8_t *dirc)
 {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) pd[i] = dir[i] ? 0.0 : 1.0 / (1.0 + dt * mc[i] * d2[i]);
+    if (i >= n) return;
+    pd[i] = dir[i] ? 0.0 : 1.0 / (1.0 + dt * mc[i] * d2[i]);
+    dirc[i] = dir[i];
 }
 // V0 = r / beta
 __global__ void k_vec_v0(int32_t n, const double *r, const double *beta, double *V0)
@@ -406,10 +445,23 @@ __global__ void k_vec_v0(int32_t n, const double *r, const double *beta, double 
     if (i < n) V0[i] = r[i] / *beta;
 }
 
+// start of a restart cycle: g = (beta, 0, ...), at most `limit` Arnoldi steps, early exit at |g_{j+1}| <= tol
+__global__ void k_cycle_init(Ctl *ctl, int limit, double tol, double dt, double *g, int n, const double *beta)
+{
+    ctl->done = 0;
+    ctl->jend = 0;
+    ctl->limit = limit;
+    ctl->tol = tol;
+    ctl->dt = dt;
+    for (int i = 0; i < n; ++i) g[i] = 0.0;
+    g[0] = *beta;
+}
+
 // Givens rotations of column j and the residual estimate (:337-347); single thread.
 // H is (m+1) x m row-major; nrm[j+1] keeps H(j+1, j) before the rotation (the divisor of V_{j+1}).
-__global__ void k_givens(double *H, int mcols, int j, double *cs, double *sn, double *g, double *nrm, double *est)
+__global__ void k_givens(Ctl *ctl, double *H, int mcols, int j, double *cs, double *sn, double *g, double *nrm)
 {
+    if (ctl->done || j >= ctl->limit) return;
     auto h = [&](int r, int c) -> double & { return H[r * mcols + c]; };
     nrm[j + 1] = h(j + 1, j);
     for (int i = 0; i < j; ++i)
@@ -425,32 +477,30 @@ __global__ void k_givens(double *H, int mcols, int j, double *cs, double *sn, do
     h(j + 1, j) = 0.0;
     g[j + 1] = -sn[j] * g[j];
     g[j] = cs[j] * g[j];
-    est[0] = fabs(g[j + 1]);
+    ctl->jend = j + 1;
+    if (fabs(g[j + 1]) <= ctl->tol) ctl->done = 1;
 }
 
-__global__ void k_g_init(double *g, int n, const double *beta)
+// back substitution of the least-squares problem (:349-354) over the jend steps of the cycle; single thread
+__global__ void k_backsub(const Ctl *ctl, const double *H, int mcols, const double *g, double *y, double *jend_out)
 {
-    for (int i = 0; i < n; ++i) g[i] = 0.0;
-    g[0] = *beta;
-}
-
-// back substitution of the least-squares problem (:349-354); single thread
-__global__ void k_backsub(const double *H, int mcols, int j, const double *g, double *y)
-{
+    const int j = ctl->jend;
     for (int i = j - 1; i >= 0; --i)
     {
         double s = g[i];
         for (int k = i + 1; k < j; ++k) s -= H[i * mcols + k] * y[k];
         y[i] = s / H[i * mcols + i];
     }
+    *jend_out = j;
 }
 
 // delta += dir ? 0 : (sum_i y_i V_i) / (1 + dt m d2)  (:355-364); z = x0 + delta for the true residual
-__global__ void k_vec_update(int32_t n, const double *V, int j, const double *y, const double *pd, const int8_t *dir,
+__global__ void k_vec_update(const Ctl *ctl, int32_t n, const double *V, const double *y, const double *pd, const int8_t *dir,
                              const double *x0, double *delta, double *z)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
+    const int j = ctl->jend;
     double s = 0.0;
     for (int i = 0; i < j; ++i) s += y[i] * V[(int64_t)i * n + e];
     const double d = delta[e] + (dir[e] ? 0.0 : s * pd[e]);
@@ -481,9 +531,20 @@ struct MhdInduction
     DBuf<double> mcoef, taper, alpha, B0, recon, d2, corr, phi, s2phi, bcell, g;
     DBuf<double> V, w, z, r, b, x0, delta, Ax, pd, Fn, part, H, cs, sn, gv, yv, nrm, scal;
     DBuf<float> recon32, m32, ecw32, tv32, fa32, vinv32, alpha32, B0_32, phi32, s2phi32, b32, g32;
+    DBuf<int8_t> dirc;
+    DBuf<unsigned> counter;
+    DBuf<Ctl> ctl;
     double *pinned = nullptr;
+    EventProfiler<KI_COUNT> prof;
+    int64_t launches = 0;
+    // one restart cycle (mr Arnoldi steps) captured as a CUDA graph on the first unprofiled solve
+    cudaGraphExec_t cycle = nullptr;
+    bool cycle_tried = false;
+    int64_t cycle_kernels = 0;
+    bool capturing = false;
     ~MhdInduction()
     {
+        if (cycle) cudaGraphExecDestroy(cycle);
         if (pinned) cudaFreeHost(pinned);
     }
 };
@@ -494,51 +555,76 @@ namespace
 {
 int g1(int64_t n) { return grid_for(n, 256); }
 
-// y = F(phi) (in.x and in.src null, phi given) or y = A x; optional fused outputs as in EdgeArgs.
-void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, double *y, double *vout = nullptr,
-          const int8_t *dir = nullptr, const double *v0 = nullptr)
+// one launch of kernel class k on the handle's stream, counted and (when profiling, outside a graph
+// capture) timed
+#define IND_LAUNCH(I, k, s, ...)                                                                                         \
+    do                                                                                                                   \
+    {                                                                                                                    \
+        if (!(I)->capturing) (I)->prof.begin(k, s);                                                                      \
+        __VA_ARGS__;                                                                                                     \
+        if (!(I)->capturing) (I)->prof.end(k, s);                                                                        \
+        ++(I)->launches;                                                                                                 \
+    } while (0)
+
+struct Fused
+{
+    double *vout = nullptr;
+    const int8_t *dir = nullptr;
+    const double *v0 = nullptr;
+    double *dot = nullptr;
+    const double *dtp = nullptr;
+    Gate gt;
+};
+
+// y = F(phi) (no input in `in`, phi given) or y = A x; optional fused outputs as in EdgeArgs.
+void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, double *y, const Fused &fz = Fused{})
 {
     const MeshView &m = I->mesh->v;
     cudaStream_t s = I->mesh->stream;
     const double *phi = phi_in;
     if (in.x || in.src)
     {
-        if (m.nf) k_ind_face<double><<<g1(m.nf), 256, 0, s>>>(m, in, I->hall, I->resistive, I->phi.p, I->s2phi.p);
+        if (m.nf)
+            IND_LAUNCH(I, KI_FACE, s, k_ind_face<double><<<g1(m.nf), 256, 0, s>>>(m, fz.gt, in, I->hall, I->resistive, I->phi.p, I->s2phi.p));
         phi = I->phi.p;
     }
     else if (I->resistive && m.nf)
-        k_ind_s2phi<<<g1(m.nf), 256, 0, s>>>(m, phi, I->s2phi.p);
+        IND_LAUNCH(I, KI_FACE, s, k_ind_s2phi<<<g1(m.nf), 256, 0, s>>>(m, phi, I->s2phi.p));
     if (I->hall && m.nc)
     {
-        k_ind_bcell<double><<<g1(m.nc), 256, 0, s>>>(m, I->recon.p, phi, I->bcell.p);
-        if (m.no_cells) k_ind_hall<<<g1(m.no_cells), 256, 0, s>>>(m, I->bcell.p, I->alpha.p, I->B0.p, I->g.p);
+        IND_LAUNCH(I, KI_BCELL, s, k_ind_bcell<double><<<g1(m.nc), 256, 0, s>>>(m, fz.gt, I->recon.p, phi, I->bcell.p));
+        if (m.no_cells)
+            IND_LAUNCH(I, KI_HALL, s, k_ind_hall<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->bcell.p, I->alpha.p, I->B0.p, I->g.p));
     }
     EdgeArgs<double> a;
     a.resistive = I->resistive; a.hall = I->hall;
     a.s2phi = I->s2phi.p; a.g = I->g.p; a.mcoef = I->mcoef.p; a.ecw = m.ec_weight; a.tvec = m.edge_vec;
-    a.in = in; a.dt = dt; a.vout = vout; a.dir = dir; a.v0 = v0; a.part = I->part.p; a.out = y;
-    if (m.ne) k_ind_edge<double><<<I->edge_blocks, 256, 0, s>>>(m, a);
-    MHD_LAUNCH_CHECK();
+    a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
+    a.part = I->part.p; a.counter = I->counter.p; a.out = y;
+    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, k_ind_edge<double><<<I->edge_blocks, 256, 0, s>>>(m, a));
 }
 
 // the same Arnoldi matvec with the FP32 operator (mixed precision inner iterations)
-void op32(MhdInduction *I, const MatIn &in, double dt, double *y, double *vout, const int8_t *dir, const double *v0)
+void op32(MhdInduction *I, const MatIn &in, double dt, double *y, const Fused &fz)
 {
     const MeshView &m = I->mesh->v;
     cudaStream_t s = I->mesh->stream;
-    if (m.nf) k_ind_face<float><<<g1(m.nf), 256, 0, s>>>(m, in, I->hall, I->resistive, I->phi32.p, I->s2phi32.p);
+    if (m.nf)
+        IND_LAUNCH(I, KI_FACE, s, k_ind_face<float><<<g1(m.nf), 256, 0, s>>>(m, fz.gt, in, I->hall, I->resistive, I->phi32.p, I->s2phi32.p));
     if (I->hall && m.nc)
     {
-        k_ind_bcell<float><<<g1(m.nc), 256, 0, s>>>(m, I->recon32.p, I->phi32.p, I->b32.p);
+        IND_LAUNCH(I, KI_BCELL, s, k_ind_bcell<float><<<g1(m.nc), 256, 0, s>>>(m, fz.gt, I->recon32.p, I->phi32.p, I->b32.p));
         if (m.no_cells)
-            k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, I->b32.p, I->alpha32.p, I->B0_32.p, I->fa32.p, I->vinv32.p, I->g32.p);
+            IND_LAUNCH(I, KI_HALL, s,
+                       k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->b32.p, I->alpha32.p, I->B0_32.p, I->fa32.p, I->vinv32.p,
+                                                                   I->g32.p));
     }
     EdgeArgs<float> a;
     a.resistive = I->resistive; a.hall = I->hall;
     a.s2phi = I->s2phi32.p; a.g = I->g32.p; a.mcoef = I->m32.p; a.ecw = I->ecw32.p; a.tvec = I->tv32.p;
-    a.in = in; a.dt = dt; a.vout = vout; a.dir = dir; a.v0 = v0; a.part = I->part.p; a.out = y;
-    if (m.ne) k_ind_edge<float><<<I->edge_blocks, 256, 0, s>>>(m, a);
-    MHD_LAUNCH_CHECK();
+    a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
+    a.part = I->part.p; a.counter = I->counter.p; a.out = y;
+    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, k_ind_edge<float><<<I->edge_blocks, 256, 0, s>>>(m, a));
 }
 
 void apply_plain(MhdInduction *I, const double *x, double dt, double *y)
@@ -548,21 +634,92 @@ void apply_plain(MhdInduction *I, const double *x, double dt, double *y)
     op64(I, in, nullptr, dt, y);
 }
 
-// dot over the owned edges into *out (op as k_dot_final)
+// dot over the owned edges into *out (op as grid_sum_tail)
 void dev_dot(MhdInduction *I, const double *a, const double *b, int op, double *out)
 {
     cudaStream_t s = I->mesh->stream;
-    k_dot_part<<<kRedBlocks, 256, 0, s>>>(a, b, I->mesh->v.no_edges, I->part.p);
-    k_dot_final<<<1, 1024, 0, s>>>(I->part.p, kRedBlocks, op, out);
-    MHD_LAUNCH_CHECK();
+    IND_LAUNCH(I, KI_VECTOR, s, k_dot<<<kRedBlocks, 256, 0, s>>>(a, b, I->mesh->v.no_edges, I->part.p, I->counter.p, op, out));
 }
 
-double host_read(MhdInduction *I, const double *dev)
+// The mr Arnoldi steps of one restart cycle (:333-348), each gated by the cycle control:
+// w = A P^-1 V_j with V_j = w_prev / H(j, j-1) formed on the fly, Dirichlet rows zeroed and H(0, j) = w . V_0;
+// modified Gram-Schmidt w -= H(i-1, j) V_{i-1} fused with H(i, j) = w . V_i; Givens and the early-exit test.
+void enqueue_cycle(MhdInduction *I)
+{
+    const MeshView &m = I->mesh->v;
+    cudaStream_t s = I->mesh->stream;
+    const int32_t ne = m.ne;
+    const int mr = I->p.restart;
+    double *V = I->V.p, *H = I->H.p;
+    for (int j = 0; j < mr; ++j)
+    {
+        Gate gt;
+        gt.ctl = I->ctl.p;
+        gt.j = j;
+        MatIn in;
+        in.src = j == 0 ? V : I->w.p;
+        in.hs = j == 0 ? nullptr : I->nrm.p + j;
+        in.pd = I->pd.p;
+        Fused fz;
+        fz.vout = j == 0 ? nullptr : V + (int64_t)j * ne;
+        fz.dir = I->dirc.p;
+        fz.v0 = V;
+        fz.dot = H + j;
+        fz.dtp = &I->ctl.p->dt;
+        fz.gt = gt;
+        if (I->mixed) op32(I, in, 0.0, I->w.p, fz);
+        else op64(I, in, nullptr, 0.0, I->w.p, fz);
+        for (int i = 1; i <= j + 1; ++i)
+        {
+            const double *Vi = i <= j ? V + (int64_t)i * ne : nullptr; // i = j+1: the norm of w
+            IND_LAUNCH(I, KI_MGS, s,
+                       k_mgs<<<kRedBlocks, 256, 0, s>>>(gt, I->w.p, V + (int64_t)(i - 1) * ne, H + (int64_t)(i - 1) * mr + j, Vi, ne,
+                                                        m.no_edges, i & 1, I->part.p, I->counter.p, H + (int64_t)i * mr + j));
+        }
+        IND_LAUNCH(I, KI_SCALAR, s, k_givens<<<1, 1, 0, s>>>(I->ctl.p, H, mr, j, I->cs.p, I->sn.p, I->gv.p, I->nrm.p));
+    }
+}
+
+// Capture the cycle once as a CUDA graph; a stream that cannot be captured keeps direct launches.
+void build_cycle_graph(MhdInduction *I)
+{
+    I->cycle_tried = true;
+    cudaStream_t s = I->mesh->stream;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return;
+    }
+    const int64_t l0 = I->launches;
+    I->capturing = true;
+    enqueue_cycle(I);
+    I->capturing = false;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+    I->cycle_kernels = I->launches - l0;
+    I->launches = l0;
+    if (ce != cudaSuccess || !graph)
+    {
+        cudaGetLastError();
+        if (graph) cudaGraphDestroy(graph);
+        return;
+    }
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess)
+    {
+        cudaGetLastError();
+        return;
+    }
+    I->cycle = exec;
+}
+
+void host_read2(MhdInduction *I, const double *dev)
 {
     cudaStream_t s = I->mesh->stream;
-    MHD_CUDA(cudaMemcpyAsync(I->pinned, dev, sizeof(double), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaMemcpyAsync(I->pinned, dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     MHD_CUDA(cudaStreamSynchronize(s));
-    return I->pinned[0];
 }
 } // namespace
 } // namespace mhd
@@ -619,11 +776,14 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
         I->phi.alloc(nf); I->s2phi.alloc(nf); I->bcell.alloc(3 * nc); I->g.alloc(3 * nc);
         const int mr = I->p.restart;
         I->V.alloc((size_t)(mr + 1) * ne); I->w.alloc(ne); I->z.alloc(ne); I->r.alloc(ne); I->b.alloc(ne); I->x0.alloc(ne);
-        I->delta.alloc(ne); I->Ax.alloc(ne); I->pd.alloc(ne); I->Fn.alloc(ne);
+        I->delta.alloc(ne); I->Ax.alloc(ne); I->pd.alloc(ne); I->Fn.alloc(ne); I->dirc.alloc(ne);
         I->part.alloc((size_t)std::max(kRedBlocks, I->edge_blocks));
         I->H.alloc((size_t)(mr + 1) * mr); I->cs.alloc(mr); I->sn.alloc(mr); I->gv.alloc(mr + 1); I->yv.alloc(mr);
-        I->nrm.alloc(mr + 1); I->scal.alloc(8);
+        I->nrm.alloc(mr + 1); I->scal.alloc(8); I->counter.alloc(1); I->ctl.alloc(1);
         MHD_CUDA(cudaMallocHost(&I->pinned, 8 * sizeof(double)));
+        MHD_CUDA(cudaMemsetAsync(I->counter.p, 0, sizeof(unsigned), s));
+        MHD_CUDA(cudaMemsetAsync(I->ctl.p, 0, sizeof(Ctl), s));
+        MHD_CUDA(cudaMemsetAsync(I->scal.p, 0, 8 * sizeof(double), s));
         if (nc)
         {
             MHD_CUDA(cudaMemsetAsync(I->alpha.p, 0, nc * sizeof(double), s));
@@ -689,6 +849,7 @@ int mhd_gpu_induction_apply_F(MhdInduction *I, const double *phi, double *out)
     return guarded([&] {
         MHD_REQUIRE(I && phi && out, "null argument");
         op64(I, MatIn{}, phi, 0.0, out);
+        MHD_LAUNCH_CHECK();
     });
 }
 
@@ -697,6 +858,7 @@ int mhd_gpu_induction_apply_A(MhdInduction *I, const double *x, double dt, doubl
     return guarded([&] {
         MHD_REQUIRE(I && x && y, "null argument");
         apply_plain(I, x, dt, y);
+        MHD_LAUNCH_CHECK();
     });
 }
 
@@ -715,64 +877,47 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         const int mr = I->p.restart;
         const int ge = g1(ne);
         if (!warm) I->have_corr = false;
-        double *sc = I->scal.p; // [0] |b|  [1] beta  [2] |g_{j+1}|
-        k_vec_x0<<<ge, 256, 0, s>>>(ne, Ee, I->have_corr ? I->corr.p : nullptr, dir, I->x0.p, I->delta.p);
-        op64(I, MatIn{}, Phi, 0.0, I->Fn.p);                          // F(Phi^n)
-        k_vec_add<<<ge, 256, 0, s>>>(ne, Ee, I->Fn.p, I->b.p);          // b = E_expl + F(Phi^n)
-        apply_plain(I, I->x0.p, dt, I->Ax.p);                         // A x0
-        k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p);
-        k_vec_pd<<<ge, 256, 0, s>>>(ne, dt, I->mcoef.p, I->d2.p, dir, I->pd.p);
-        MHD_LAUNCH_CHECK();
+        double *sc = I->scal.p; // [0] |b|  [1] beta  [2] steps of the last cycle
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_x0<<<ge, 256, 0, s>>>(ne, Ee, I->have_corr ? I->corr.p : nullptr, dir, I->x0.p, I->delta.p));
+        op64(I, MatIn{}, Phi, 0.0, I->Fn.p);                                                      // F(Phi^n)
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_add<<<ge, 256, 0, s>>>(ne, Ee, I->Fn.p, I->b.p));     // b = E_expl + F(Phi^n)
+        apply_plain(I, I->x0.p, dt, I->Ax.p);                                                     // A x0
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_pd<<<ge, 256, 0, s>>>(ne, dt, I->mcoef.p, I->d2.p, dir, I->pd.p, I->dirc.p));
         dev_dot(I, I->b.p, I->b.p, 2, sc + 0);
         dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
-        const double bnorm = host_read(I, sc + 0);
-        double beta = host_read(I, sc + 1);
+        MHD_LAUNCH_CHECK();
+        host_read2(I, sc + 0);
+        const double bnorm = I->pinned[0];
+        double beta = I->pinned[1];
         const double tol = I->p.rtol * bnorm;
         int total = 0;
-        double *V = I->V.p, *H = I->H.p;
         while (beta > tol && total < I->p.max_it)
         {
-            k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, V);
-            k_g_init<<<1, 1, 0, s>>>(I->gv.p, mr + 1, sc + 1);
-            int j = 0;
-            for (; j < mr && total < I->p.max_it; ++j, ++total)
+            IND_LAUNCH(I, KI_VECTOR, s, k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, I->V.p));
+            IND_LAUNCH(I, KI_SCALAR, s,
+                       k_cycle_init<<<1, 1, 0, s>>>(I->ctl.p, std::min(mr, I->p.max_it - total), tol, dt, I->gv.p, mr + 1, sc + 1));
+            if (!I->prof.on && !I->cycle_tried) build_cycle_graph(I);
+            if (!I->prof.on && I->cycle)
             {
-                // w = A P^-1 V_j with V_j = w_prev / H(j, j-1) formed on the fly, Dirichlet rows zeroed,
-                // and the block partials of w . V_0
-                MatIn in;
-                in.src = j == 0 ? V : I->w.p;
-                in.hs = j == 0 ? nullptr : I->nrm.p + j;
-                in.pd = I->pd.p;
-                double *vout = j == 0 ? nullptr : V + (int64_t)j * ne;
-                if (I->mixed) op32(I, in, dt, I->w.p, vout, dir, V);
-                else op64(I, in, nullptr, dt, I->w.p, vout, dir, V);
-                k_dot_final<<<1, 1024, 0, s>>>(I->part.p, I->edge_blocks, 0, H + j);
-                // modified Gram-Schmidt (:340-345): w -= H(i-1, j) V_{i-1}, fused with H(i, j) = w . V_i
-                for (int i = 1; i <= j + 1; ++i)
-                {
-                    const double *Vi = i <= j ? V + (int64_t)i * ne : nullptr; // i = j+1: the norm of w
-                    k_mgs<<<kRedBlocks, 256, 0, s>>>(I->w.p, V + (int64_t)(i - 1) * ne, H + (int64_t)(i - 1) * mr + j, Vi, ne,
-                                                     m.no_edges, i & 1, I->part.p);
-                    k_dot_final<<<1, 1024, 0, s>>>(I->part.p, kRedBlocks, i <= j ? 0 : 1, H + (int64_t)i * mr + j);
-                }
-                k_givens<<<1, 1, 0, s>>>(H, mr, j, I->cs.p, I->sn.p, I->gv.p, I->nrm.p, sc + 2);
-                MHD_LAUNCH_CHECK();
-                if (host_read(I, sc + 2) <= tol)
-                {
-                    ++j;
-                    ++total;
-                    break;
-                }
+                MHD_CUDA(cudaGraphLaunch(I->cycle, s));
+                I->launches += I->cycle_kernels;
             }
-            k_backsub<<<1, 1, 0, s>>>(H, mr, j, I->gv.p, I->yv.p);
-            k_vec_update<<<ge, 256, 0, s>>>(ne, V, j, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p);
+            else
+                enqueue_cycle(I);
+            IND_LAUNCH(I, KI_SCALAR, s, k_backsub<<<1, 1, 0, s>>>(I->ctl.p, I->H.p, mr, I->gv.p, I->yv.p, sc + 2));
+            IND_LAUNCH(I, KI_VECTOR, s,
+                       k_vec_update<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p));
             // true residual in FP64 (the outer iterative refinement of the mixed-precision solve)
             apply_plain(I, I->z.p, dt, I->Ax.p);
-            k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p);
+            IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
             dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
-            beta = host_read(I, sc + 1);
+            MHD_LAUNCH_CHECK();
+            host_read2(I, sc + 1);
+            beta = I->pinned[0];
+            total += static_cast<int>(I->pinned[1]);
         }
-        k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p);
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p));
         MHD_LAUNCH_CHECK();
         MHD_CUDA(cudaStreamSynchronize(s));
         I->have_corr = true;
@@ -781,6 +926,40 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         if (beta > tol) status = MHD_ENOCONV;
     });
     return rc != MHD_OK ? rc : status;
+}
+
+int mhd_gpu_induction_profile(MhdInduction *I, int32_t enable)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I, "null induction handle");
+        MHD_CUDA(cudaStreamSynchronize(I->mesh->stream));
+        I->prof.on = enable != 0;
+        for (auto &u : I->prof.used) u = 0;
+    });
+}
+
+int mhd_gpu_induction_profile_read(MhdInduction *I, int32_t max_kernels, char *names, double *ms_total, int64_t *count, int32_t *n_out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && names && ms_total && count && n_out, "null argument");
+        MHD_CUDA(cudaStreamSynchronize(I->mesh->stream));
+        int n = 0;
+        for (int k = 0; k < KI_COUNT && n < max_kernels; ++k, ++n)
+        {
+            std::strncpy(names + 32 * n, kIndKernelNames[k], 31);
+            names[32 * n + 31] = 0;
+            I->prof.read(k, ms_total[n], count[n]);
+        }
+        *n_out = n;
+    });
+}
+
+int mhd_gpu_induction_launches(MhdInduction *I, int64_t *out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && out, "null argument");
+        *out = I->launches;
+    });
 }
 
 } // extern "C"

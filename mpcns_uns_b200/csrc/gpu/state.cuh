@@ -12,39 +12,7 @@ enum StepKernel { KP_PREPARE = 0, KP_CFL, KP_GRAD, KP_FLUX, KP_UPDATE, KP_FACE_C
 static const char *const kStepKernelNames[KP_COUNT] = {"prepare", "cfl", "limited_gradients", "face_flux",
                                                         "update",  "face_candidate", "edge_emf", "ct"};
 
-struct Profiler
-{
-    bool on = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[KP_COUNT];
-    size_t used[KP_COUNT] = {};
-    ~Profiler()
-    {
-        for (auto &v : ev)
-            for (auto &p : v)
-            {
-                cudaEventDestroy(p.first);
-                cudaEventDestroy(p.second);
-            }
-    }
-    void begin(int k, cudaStream_t s)
-    {
-        if (!on) return;
-        if (used[k] == ev[k].size())
-        {
-            cudaEvent_t a, b;
-            MHD_CUDA(cudaEventCreate(&a));
-            MHD_CUDA(cudaEventCreate(&b));
-            ev[k].emplace_back(a, b);
-        }
-        MHD_CUDA(cudaEventRecord(ev[k][used[k]].first, s));
-    }
-    void end(int k, cudaStream_t s)
-    {
-        if (!on) return;
-        MHD_CUDA(cudaEventRecord(ev[k][used[k]].second, s));
-        ++used[k];
-    }
-};
+using Profiler = EventProfiler<KP_COUNT>;
 
 // Single-precision tables of the mixed path, derived once from the FP64 mesh (tetrahedral meshes):
 // structure of arrays over cells / faces / edges so that every warp load is coalesced.

@@ -579,16 +579,7 @@ int mhd_gpu_state_profile_read(MhdState *st, int32_t max_kernels, char *names, d
         {
             std::strncpy(names + 32 * n, kStepKernelNames[k], 31);
             names[32 * n + 31] = 0;
-            double tot = 0;
-            for (size_t i = 0; i < st->prof.used[k]; ++i)
-            {
-                float ms = 0;
-                MHD_CUDA(cudaEventElapsedTime(&ms, st->prof.ev[k][i].first, st->prof.ev[k][i].second));
-                tot += ms;
-            }
-            ms_total[n] = tot;
-            count[n] = static_cast<int64_t>(st->prof.used[k]);
-            st->prof.used[k] = 0;
+            st->prof.read(k, ms_total[n], count[n]);
         }
         *n_out = n;
     });

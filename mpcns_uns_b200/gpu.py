@@ -92,6 +92,9 @@ _SIGS = {
     "mhd_gpu_induction_apply_F": ([vp, vp, vp], ctypes.c_int),
     "mhd_gpu_induction_apply_A": ([vp, vp, dbl, vp], ctypes.c_int),
     "mhd_gpu_induction_solve": ([vp, vp, vp, vp, dbl, i32, vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_induction_profile": ([vp, i32], ctypes.c_int),
+    "mhd_gpu_induction_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
+    "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
 }
 
 
@@ -401,13 +404,7 @@ class ResidentState:
 
     def profile_read(self):
         """{kernel class: (summed ms, launches)} since the last read (synchronises)."""
-        names = ctypes.create_string_buffer(32 * 16)
-        ms = np.zeros(16)
-        cnt = np.zeros(16, np.int64)
-        n = i32()
-        check(lib().mhd_gpu_state_profile_read(self._h, 16, names, ms.ctypes.data_as(vp), cnt.ctypes.data_as(vp), ctypes.byref(n)))
-        raw = names.raw
-        return {raw[32 * k:32 * k + 32].split(b"\0")[0].decode(): (float(ms[k]), int(cnt[k])) for k in range(n.value)}
+        return _read_profile(lib().mhd_gpu_state_profile_read, self._h)
 
     def launches(self):
         v = i64()
@@ -482,3 +479,25 @@ class DeviceInduction:
         if rc != MHD_ENOCONV:
             check(rc)
         return E, it.value, rr.value
+
+    def profile(self, enable=True):
+        check(lib().mhd_gpu_induction_profile(self._h, int(bool(enable))))
+
+    def profile_read(self):
+        """{kernel class: (summed ms, launches)} since the last read (synchronises)."""
+        return _read_profile(lib().mhd_gpu_induction_profile_read, self._h)
+
+    def launches(self):
+        v = i64()
+        check(lib().mhd_gpu_induction_launches(self._h, ctypes.byref(v)))
+        return v.value
+
+
+def _read_profile(fn, h):
+    names = ctypes.create_string_buffer(32 * 16)
+    ms = np.zeros(16)
+    cnt = np.zeros(16, np.int64)
+    n = i32()
+    check(fn(h, 16, names, ms.ctypes.data_as(vp), cnt.ctypes.data_as(vp), ctypes.byref(n)))
+    raw = names.raw
+    return {raw[32 * k:32 * k + 32].split(b"\0")[0].decode(): (float(ms[k]), int(cnt[k])) for k in range(n.value)}
