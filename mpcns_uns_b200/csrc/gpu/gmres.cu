@@ -153,7 +153,7 @@ __global__ void k_ind_alpha(int32_t nc, const double *taper, const double *ne_ef
 
 // FP32 copies of the operator's tables (mixed precision)
 __global__ void k_ind_tables32(MeshView m, const double *recon, const double *mcoef, float *recon32, float *m32, float *ecw32,
-                               float *tv32, float *fa32, float *vinv32)
+                               float *tv32, float *vinv32)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < 3 * (int64_t)m.c2f_ptr[m.nc]) recon32[i] = static_cast<float>(recon[i]);
@@ -163,9 +163,27 @@ __global__ void k_ind_tables32(MeshView m, const double *recon, const double *mc
         m32[i] = static_cast<float>(mcoef[i]);
         for (int a = 0; a < 3; ++a) tv32[3 * i + a] = static_cast<float>(m.edge_vec[3 * i + a]);
     }
-    if (i < m.nf)
-        for (int a = 0; a < 3; ++a) fa32[3 * i + a] = static_cast<float>(m.face_area[3 * i + a]);
     if (i < m.nc) vinv32[i] = static_cast<float>(1.0 / m.cell_volume[i]);
+}
+
+// Per c2f slot of a cell: the cell across the face (-1 if the face has one cell) and the signed area
+// vector s A_f, so that the Hall pass reads its cell's slots contiguously instead of chasing f2c.
+__global__ void k_ind_slots(MeshView m, int32_t *slot_nb, double *slot_sa, float4 *slot32)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        const int32_t p0 = m.f2c_ptr[f];
+        int32_t o = -1;
+        if (m.f2c_ptr[f + 1] - p0 == 2) o = m.f2c_idx[p0] == c ? m.f2c_idx[p0 + 1] : m.f2c_idx[p0];
+        const V3 sa = double(m.c2f_sgn[k]) * ld3(m.face_area, f);
+        slot_nb[k] = o;
+        st3(slot_sa, k, sa);
+        if (slot32)
+            slot32[k] = make_float4(static_cast<float>(sa.x), static_cast<float>(sa.y), static_cast<float>(sa.z), __int_as_float(o));
+    }
 }
 
 __global__ void k_to_float(const double *a, float *b, int64_t n)
@@ -177,19 +195,15 @@ __global__ void k_to_float(const double *a, float *b, int64_t n)
 // ---------------------------------------------------------------- operator
 // Input of a matvec: x_e directly (apply_A), or the preconditioned Krylov vector
 // x_e = (src_e / *hs) * pd_e with pd_e = dir_e ? 0 : 1 / (1 + dt m_e d2_e)  (:338)
+// The face pass gathers one edge vector: x itself, or zs = w_prev * pd (stored by the last
+// Gram-Schmidt pass of the previous step, FP32 for the FP32 operator) whose d1 it divides by *hs.
 struct MatIn
 {
     const double *x = nullptr;
     const double *src = nullptr, *hs = nullptr, *pd = nullptr;
+    const double *zs = nullptr;
+    const float *zs32 = nullptr;
 };
-
-__device__ __forceinline__ double mat_in(const MatIn &in, int32_t e)
-{
-    if (!in.src) return in.x[e];
-    double v = in.src[e];
-    if (in.hs) v = v / *in.hs;
-    return v * in.pd[e];
-}
 
 // Phi' = d1 x on every face (:185-190), with star2 Phi' for the resistive current flux (:131-136).
 // FP64 sums in both precisions; the FP32 operator stores the rounded results.
@@ -199,7 +213,14 @@ __global__ void k_ind_face(MeshView m, Gate gt, MatIn in, int hall, int resistiv
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf || gt.off()) return;
     double s = 0;
-    for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) s += m.f2e_sgn[k] * mat_in(in, m.f2e_idx[k]);
+    const int32_t k0 = m.f2e_ptr[f], k1 = m.f2e_ptr[f + 1];
+    if (in.zs32)
+        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * static_cast<double>(in.zs32[m.f2e_idx[k]]);
+    else if (in.zs)
+        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.zs[m.f2e_idx[k]];
+    else
+        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.x[m.f2e_idx[k]];
+    if ((in.zs || in.zs32) && in.hs) s = s / *in.hs;
     if (hall) phi[f] = static_cast<T>(s);
     if (resistive) s2phi[f] = static_cast<T>(m.star2[f] * s);
 }
@@ -230,8 +251,9 @@ __global__ void k_ind_bcell(MeshView m, Gate gt, const T *__restrict__ recon, co
 // Hall EMF per owned cell (:159-178): J_c = (1/V) sum s A x 1/2 (b_c + b_nb), g_c = alpha_c J_c x B0_c.
 // g_c = 0 where the reference skips the cell (alpha = 0, or not fluid: its ce list is empty), so that
 // the edge gather may add every owned cell: adding the zero product leaves each sum unchanged.
-__global__ void k_ind_hall(MeshView m, Gate gt, const double *__restrict__ b, const double *__restrict__ alpha,
-                           const double *__restrict__ B0, double *__restrict__ g)
+__global__ void k_ind_hall(MeshView m, Gate gt, const int32_t *__restrict__ slot_nb, const double *__restrict__ slot_sa,
+                           const double *__restrict__ b, const double *__restrict__ alpha, const double *__restrict__ B0,
+                           double *__restrict__ g)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.no_cells || gt.off()) return;
@@ -244,22 +266,17 @@ __global__ void k_ind_hall(MeshView m, Gate gt, const double *__restrict__ b, co
     const V3 bc = ld3(b, c);
     for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
     {
-        const int32_t f = m.c2f_idx[k];
+        const int32_t o = slot_nb[k];
         V3 bf = bc;
-        const int32_t p0 = m.f2c_ptr[f];
-        if (m.f2c_ptr[f + 1] - p0 == 2)
-        {
-            const int32_t o = m.f2c_idx[p0] == c ? m.f2c_idx[p0 + 1] : m.f2c_idx[p0];
-            bf = 0.5 * (bc + ld3(b, o));
-        }
-        sum = sum + cross(double(m.c2f_sgn[k]) * ld3(m.face_area, f), bf);
+        if (o >= 0) bf = 0.5 * (bc + ld3(b, o));
+        sum = sum + cross(ld3(slot_sa, k), bf);
     }
     const V3 J = (1.0 / m.cell_volume[c]) * sum;
     st3(g, c, alpha[c] * cross(J, ld3(B0, c)));
 }
 
-__global__ void k_ind_hall32(MeshView m, Gate gt, const float *__restrict__ b, const float *__restrict__ alpha,
-                             const float *__restrict__ B0, const float *__restrict__ fa, const float *__restrict__ vinv,
+__global__ void k_ind_hall32(MeshView m, Gate gt, const float4 *__restrict__ slot32, const float *__restrict__ b,
+                             const float *__restrict__ alpha, const float *__restrict__ B0, const float *__restrict__ vinv,
                              float *__restrict__ g)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -274,18 +291,16 @@ __global__ void k_ind_hall32(MeshView m, Gate gt, const float *__restrict__ b, c
     const float bcx = b[3 * (int64_t)c], bcy = b[3 * (int64_t)c + 1], bcz = b[3 * (int64_t)c + 2];
     for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
     {
-        const int32_t f = m.c2f_idx[k];
+        const float4 sl = slot32[k];
+        const int32_t o = __float_as_int(sl.w);
         float bx = bcx, by = bcy, bz = bcz;
-        const int32_t p0 = m.f2c_ptr[f];
-        if (m.f2c_ptr[f + 1] - p0 == 2)
+        if (o >= 0)
         {
-            const int32_t o = m.f2c_idx[p0] == c ? m.f2c_idx[p0 + 1] : m.f2c_idx[p0];
             bx = 0.5f * (bcx + b[3 * (int64_t)o]);
             by = 0.5f * (bcy + b[3 * (int64_t)o + 1]);
             bz = 0.5f * (bcz + b[3 * (int64_t)o + 2]);
         }
-        const float s = m.c2f_sgn[k];
-        const float ax = s * fa[3 * (int64_t)f], ay = s * fa[3 * (int64_t)f + 1], az = s * fa[3 * (int64_t)f + 2];
+        const float ax = sl.x, ay = sl.y, az = sl.z;
         sx += ay * bz - az * by;
         sy += az * bx - ax * bz;
         sz += ax * by - ay * bx;
@@ -377,7 +392,8 @@ __global__ void __launch_bounds__(256) k_dot(const double *__restrict__ a, const
 // the previous pass left in L2 is read first.
 __global__ void __launch_bounds__(256) k_mgs(Gate gt, double *__restrict__ w, const double *__restrict__ Vprev,
                                               const double *__restrict__ h, const double *__restrict__ Vi, int32_t n_all,
-                                              int32_t n_owned, int reverse, double *part, unsigned *counter, double *out)
+                                              int32_t n_owned, int reverse, double *part, unsigned *counter, double *out,
+                                              const double *__restrict__ pd, double *__restrict__ zs, float *__restrict__ zs32)
 {
     if (gt.off()) return;
     constexpr int U = 4;
@@ -407,6 +423,8 @@ __global__ void __launch_bounds__(256) k_mgs(Gate gt, double *__restrict__ w, co
             const double wi = wv[u] - hv * pv[u];
             w[idx[u]] = wi;
             if (idx[u] < n_owned) s += wi * (Vi ? iv[u] : wi);
+            if (zs) zs[idx[u]] = wi * pd[idx[u]];
+            if (zs32) zs32[idx[u]] = static_cast<float>(wi * pd[idx[u]]);
         }
     }
     grid_sum_tail(s, part, counter, Vi ? 0 : 1, out);
@@ -438,11 +456,15 @@ __global__ void k_vec_pd(int32_t n, double dt, const double *mc, const double *d
     pd[i] = dir[i] ? 0.0 : 1.0 / (1.0 + dt * mc[i] * d2[i]);
     dirc[i] = dir[i];
 }
-// V0 = r / beta
-__global__ void k_vec_v0(int32_t n, const double *r, const double *beta, double *V0)
+// V0 = r / beta, and the face pass's input V0 * pd
+__global__ void k_vec_v0(int32_t n, const double *r, const double *beta, double *V0, const double *pd, double *zs, float *zs32)
 {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) V0[i] = r[i] / *beta;
+    if (i >= n) return;
+    const double v = r[i] / *beta;
+    V0[i] = v;
+    if (zs) zs[i] = v * pd[i];
+    if (zs32) zs32[i] = static_cast<float>(v * pd[i]);
 }
 
 // start of a restart cycle: g = (beta, 0, ...), at most `limit` Arnoldi steps, early exit at |g_{j+1}| <= tol
@@ -530,7 +552,10 @@ struct MhdInduction
     int edge_blocks = 0;
     DBuf<double> mcoef, taper, alpha, B0, recon, d2, corr, phi, s2phi, bcell, g;
     DBuf<double> V, w, z, r, b, x0, delta, Ax, pd, Fn, part, H, cs, sn, gv, yv, nrm, scal;
-    DBuf<float> recon32, m32, ecw32, tv32, fa32, vinv32, alpha32, B0_32, phi32, s2phi32, b32, g32;
+    DBuf<float> recon32, m32, ecw32, tv32, vinv32, alpha32, B0_32, phi32, s2phi32, b32, g32, zs32;
+    DBuf<double> slot_sa, zs;
+    DBuf<int32_t> slot_nb;
+    DBuf<float4> slot32;
     DBuf<int8_t> dirc;
     DBuf<unsigned> counter;
     DBuf<Ctl> ctl;
@@ -594,7 +619,9 @@ void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, dou
     {
         IND_LAUNCH(I, KI_BCELL, s, k_ind_bcell<double><<<g1(m.nc), 256, 0, s>>>(m, fz.gt, I->recon.p, phi, I->bcell.p));
         if (m.no_cells)
-            IND_LAUNCH(I, KI_HALL, s, k_ind_hall<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->bcell.p, I->alpha.p, I->B0.p, I->g.p));
+            IND_LAUNCH(I, KI_HALL, s,
+                       k_ind_hall<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot_nb.p, I->slot_sa.p, I->bcell.p, I->alpha.p, I->B0.p,
+                                                                 I->g.p));
     }
     EdgeArgs<double> a;
     a.resistive = I->resistive; a.hall = I->hall;
@@ -616,7 +643,7 @@ void op32(MhdInduction *I, const MatIn &in, double dt, double *y, const Fused &f
         IND_LAUNCH(I, KI_BCELL, s, k_ind_bcell<float><<<g1(m.nc), 256, 0, s>>>(m, fz.gt, I->recon32.p, I->phi32.p, I->b32.p));
         if (m.no_cells)
             IND_LAUNCH(I, KI_HALL, s,
-                       k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->b32.p, I->alpha32.p, I->B0_32.p, I->fa32.p, I->vinv32.p,
+                       k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot32.p, I->b32.p, I->alpha32.p, I->B0_32.p, I->vinv32.p,
                                                                    I->g32.p));
     }
     EdgeArgs<float> a;
@@ -660,6 +687,8 @@ void enqueue_cycle(MhdInduction *I)
         in.src = j == 0 ? V : I->w.p;
         in.hs = j == 0 ? nullptr : I->nrm.p + j;
         in.pd = I->pd.p;
+        if (I->mixed) in.zs32 = I->zs32.p;
+        else in.zs = I->zs.p;
         Fused fz;
         fz.vout = j == 0 ? nullptr : V + (int64_t)j * ne;
         fz.dir = I->dirc.p;
@@ -671,10 +700,12 @@ void enqueue_cycle(MhdInduction *I)
         else op64(I, in, nullptr, 0.0, I->w.p, fz);
         for (int i = 1; i <= j + 1; ++i)
         {
-            const double *Vi = i <= j ? V + (int64_t)i * ne : nullptr; // i = j+1: the norm of w
+            const bool last = i == j + 1; // the norm of w, and the next face pass's input w * pd
+            const double *Vi = last ? nullptr : V + (int64_t)i * ne;
             IND_LAUNCH(I, KI_MGS, s,
                        k_mgs<<<kRedBlocks, 256, 0, s>>>(gt, I->w.p, V + (int64_t)(i - 1) * ne, H + (int64_t)(i - 1) * mr + j, Vi, ne,
-                                                        m.no_edges, i & 1, I->part.p, I->counter.p, H + (int64_t)i * mr + j));
+                                                        m.no_edges, i & 1, I->part.p, I->counter.p, H + (int64_t)i * mr + j, I->pd.p,
+                                                        last && !I->mixed ? I->zs.p : nullptr, last && I->mixed ? I->zs32.p : nullptr));
         }
         IND_LAUNCH(I, KI_SCALAR, s, k_givens<<<1, 1, 0, s>>>(I->ctl.p, H, mr, j, I->cs.p, I->sn.p, I->gv.p, I->nrm.p));
     }
@@ -780,6 +811,8 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
         I->part.alloc((size_t)std::max(kRedBlocks, I->edge_blocks));
         I->H.alloc((size_t)(mr + 1) * mr); I->cs.alloc(mr); I->sn.alloc(mr); I->gv.alloc(mr + 1); I->yv.alloc(mr);
         I->nrm.alloc(mr + 1); I->scal.alloc(8); I->counter.alloc(1); I->ctl.alloc(1);
+        I->slot_nb.alloc(nnz_c); I->slot_sa.alloc(3 * (size_t)nnz_c);
+        if (!I->mixed) I->zs.alloc(ne);
         MHD_CUDA(cudaMallocHost(&I->pinned, 8 * sizeof(double)));
         MHD_CUDA(cudaMemsetAsync(I->counter.p, 0, sizeof(unsigned), s));
         MHD_CUDA(cudaMemsetAsync(I->ctl.p, 0, sizeof(Ctl), s));
@@ -796,13 +829,13 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
         MHD_LAUNCH_CHECK();
         if (I->mixed)
         {
-            I->recon32.alloc(3 * (size_t)nnz_c); I->m32.alloc(ne); I->ecw32.alloc(nnz_ec); I->tv32.alloc(3 * ne); I->fa32.alloc(3 * nf);
+            I->recon32.alloc(3 * (size_t)nnz_c); I->m32.alloc(ne); I->ecw32.alloc(nnz_ec); I->tv32.alloc(3 * ne); I->zs32.alloc(ne); I->slot32.alloc(nnz_c);
             I->vinv32.alloc(nc); I->alpha32.alloc(nc); I->B0_32.alloc(3 * nc); I->phi32.alloc(nf); I->s2phi32.alloc(nf);
             I->b32.alloc(3 * nc); I->g32.alloc(3 * nc);
             const int64_t nmax = std::max<int64_t>({3 * (int64_t)nnz_c, (int64_t)nnz_ec, (int64_t)ne, (int64_t)nf, (int64_t)nc});
             if (nmax)
                 k_ind_tables32<<<grid_for(nmax, 256), 256, 0, s>>>(m, I->recon.p, I->mcoef.p, I->recon32.p, I->m32.p, I->ecw32.p,
-                                                                 I->tv32.p, I->fa32.p, I->vinv32.p);
+                                                                 I->tv32.p, I->vinv32.p);
             if (nc)
             {
                 MHD_CUDA(cudaMemsetAsync(I->alpha32.p, 0, nc * sizeof(float), s));
@@ -810,6 +843,8 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
             }
             MHD_LAUNCH_CHECK();
         }
+        if (nc) k_ind_slots<<<g1(nc), 256, 0, s>>>(m, I->slot_nb.p, I->slot_sa.p, I->mixed ? I->slot32.p : nullptr);
+        MHD_LAUNCH_CHECK();
         MHD_CUDA(cudaStreamSynchronize(s));
         *out = I;
     });
@@ -894,7 +929,9 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         int total = 0;
         while (beta > tol && total < I->p.max_it)
         {
-            IND_LAUNCH(I, KI_VECTOR, s, k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, I->V.p));
+            IND_LAUNCH(I, KI_VECTOR, s,
+                       k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, I->V.p, I->pd.p, I->mixed ? nullptr : I->zs.p,
+                                                   I->mixed ? I->zs32.p : nullptr));
             IND_LAUNCH(I, KI_SCALAR, s,
                        k_cycle_init<<<1, 1, 0, s>>>(I->ctl.p, std::min(mr, I->p.max_it - total), tol, dt, I->gv.p, mr + 1, sc + 1));
             if (!I->prof.on && !I->cycle_tried) build_cycle_graph(I);

@@ -575,7 +575,7 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
 }
 
 // UCT edge EMF (IdealEMF.cpp:59-128) with the boundary edge values (Solver.cpp:162-167)
-__global__ void __launch_bounds__(128) k_mx_edge(MV m, const float *__restrict__ Ef, const float4 *__restrict__ up,
+__global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float *__restrict__ Ef, const float4 *__restrict__ up,
                                                  const double *__restrict__ phi, float cuct, float3 E_inf, float *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -597,7 +597,9 @@ __global__ void __launch_bounds__(128) k_mx_edge(MV m, const float *__restrict__
         if (nfe > 0 && Lg > 0.f && any_fluid)
         {
             const float3 e1 = f3(m.ee1[e]), e2 = f3(m.ee2[e]);
-            float w[8], aef[8], sg[8], qa[8], qb[8], pA[8];
+            // per face: q (2 components in the edge-normal plane) and w a sigma Phi/A; three arrays
+            // instead of six keep the kernel at 8 resident blocks of 128 threads
+            float qa[8], qb[8], wx[8];
             float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f;
 #pragma unroll
             for (int i = 0; i < 8; ++i)
@@ -607,21 +609,19 @@ __global__ void __launch_bounds__(128) k_mx_edge(MV m, const float *__restrict__
                 const float4 mi4 = m.em[f0 + i];
                 const float3 mi = f3(mi4);
                 const float4 nf4 = m.fn[f];
-                w[i] = m.ew[f0 + i];
-                Ec += w[i] * (Ef[f] * th.x + Ef[nf + f] * th.y + Ef[2 * nf + f] * th.z);
+                const float w = m.ew[f0 + i];
+                Ec += w * (Ef[f] * th.x + Ef[nf + f] * th.y + Ef[2 * nf + f] * th.z);
                 float a = 0.f;
                 for (int32_t k = q0; k < q1; ++k) a = fmaxf(a, fabsf(fdot(f3(up[m.ec_cell[k]]), mi)));
-                aef[i] = a;
-                sg[i] = mi4.w;
-                const float as = a * sg[i];
+                const float as = a * mi4.w;
                 qa[i] = as * (nf4.x * e1.x + nf4.y * e1.y + nf4.z * e1.z);
                 qb[i] = as * (nf4.x * e2.x + nf4.y * e2.y + nf4.z * e2.z);
-                pA[i] = static_cast<float>(phi[f] / static_cast<double>(nf4.w));
-                M11 += w[i] * qa[i] * qa[i];
-                M12 += w[i] * qa[i] * qb[i];
-                M22 += w[i] * qb[i] * qb[i];
-                g1 += w[i] * qa[i];
-                g2 += w[i] * qb[i];
+                wx[i] = w * as * static_cast<float>(phi[f] / static_cast<double>(nf4.w));
+                M11 += w * qa[i] * qa[i];
+                M12 += w * qa[i] * qb[i];
+                M22 += w * qb[i] * qb[i];
+                g1 += w * qa[i];
+                g2 += w * qb[i];
             }
             const float tr = M11 + M22;
             const float eps = 1e-14f * tr;
@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(128) k_mx_edge(MV m, const float *__restrict__
             for (int i = 0; i < 8; ++i)
             {
                 if (i >= nfe) break;
-                Eu += w[i] * (1.f - (qa[i] * l1 + qb[i] * l2)) * aef[i] * sg[i] * pA[i];
+                Eu += (1.f - (qa[i] * l1 + qb[i] * l2)) * wx[i];
             }
             val = Lg * Ec + 2.f * cuct * Lg * Eu;
         }
