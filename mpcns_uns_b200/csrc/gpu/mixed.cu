@@ -215,7 +215,7 @@ __device__ __forceinline__ void rusanov32(const F5 &L, const F5 &R, float3 n, fl
 
 // primitives (FP32), cell field fit, total field, charge-weighted velocity
 __global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const double *__restrict__ U, const double *__restrict__ phi,
-                                                     const float4 *__restrict__ badd, float *__restrict__ W, float4 *__restrict__ up,
+                                                     const float4 *__restrict__ badd, float4 *__restrict__ W, float4 *__restrict__ up,
                                                      float4 *__restrict__ bt, float4 *__restrict__ bi)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -229,12 +229,9 @@ __global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const doub
         const double ir = 1.0 / r;
         const double u = Us[n + c] * ir, v = Us[2 * n + c] * ir, w = Us[3 * n + c] * ir;
         const double pr = fmax((p.gamma_d - 1.0) * (Us[4 * n + c] - 0.5 * r * (u * u + v * v + w * w)), p.p_floor_d);
-        float *Ws = W + (int64_t)s * 5 * n;
-        Ws[c] = static_cast<float>(r);
-        Ws[n + c] = static_cast<float>(u);
-        Ws[2 * n + c] = static_cast<float>(v);
-        Ws[3 * n + c] = static_cast<float>(w);
-        Ws[4 * n + c] = static_cast<float>(pr);
+        float4 *Wc = W + 2 * ((int64_t)s * n + c);
+        Wc[0] = make_float4(static_cast<float>(r), static_cast<float>(u), static_cast<float>(v), static_cast<float>(w));
+        Wc[1] = make_float4(static_cast<float>(pr), 0.f, 0.f, 0.f);
         ne += static_cast<float>(r) / p.mass[s] * p.M_ref;
     }
     const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
@@ -253,15 +250,17 @@ __global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const doub
         for (int s = 0; s < p.nsp; ++s)
         {
             // number density and velocity re-read from the primitives this thread has just written
-            const float *Ws = W + (int64_t)s * 5 * n;
-            const float chi = ne > 1e-30f ? (Ws[c] / p.mass[s] * p.M_ref) / ne : (s == 0 ? 1.f : 0.f);
-            for (int a = 0; a < 3; ++a) u3[a] += chi * Ws[(1 + a) * n + c];
+            const float4 wv = W[2 * ((int64_t)s * n + c)];
+            const float chi = ne > 1e-30f ? (wv.x / p.mass[s] * p.M_ref) / ne : (s == 0 ? 1.f : 0.f);
+            u3[0] += chi * wv.y;
+            u3[1] += chi * wv.z;
+            u3[2] += chi * wv.w;
         }
     up[c] = make_float4(u3[0], u3[1], u3[2], 0.f);
 }
 
 __global__ void __launch_bounds__(128) k_mx_cfl(MV m, MxParams p, float cfl, float inver_MA2, float rho_floor_dt,
-                                                 const float *__restrict__ W, const float4 *__restrict__ bt,
+                                                 const float4 *__restrict__ W, const float4 *__restrict__ bt,
                                                  unsigned long long *__restrict__ dt_bits, int *__restrict__ flag)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -272,15 +271,15 @@ __global__ void __launch_bounds__(128) k_mx_cfl(MV m, MxParams p, float cfl, flo
         const float3 b = f3(bt[c]);
         const float B2 = fdot(b, b);
         float rs = 0.f;
-        for (int s = 0; s < p.nsp; ++s) rs += W[(int64_t)s * 5 * n + c];
+        for (int s = 0; s < p.nsp; ++s) rs += W[2 * ((int64_t)s * n + c)].x;
         const float rho_tot = fmaxf(rs, rho_floor_dt);
         const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
         const float4 fn4[4] = {m.fn[fi.x], m.fn[fi.y], m.fn[fi.z], m.fn[fi.w]};
         const float vol = 1.f / m.vol_inv[c];
         for (int s = 0; s < p.nsp; ++s)
         {
-            const float *Ws = W + (int64_t)s * 5 * n;
-            const float rho = Ws[c], u = Ws[n + c], v = Ws[2 * n + c], w = Ws[3 * n + c], pr = Ws[4 * n + c];
+            const float4 wa = W[2 * ((int64_t)s * n + c)];
+            const float rho = wa.x, u = wa.y, v = wa.z, w = wa.w, pr = W[2 * ((int64_t)s * n + c) + 1].x;
             const float cs2 = p.gamma * pr / fmaxf(rho, 1e-30f);
             const float vA2 = inver_MA2 * B2 / rho_tot;
             float denom = 0.f;
@@ -313,7 +312,7 @@ __global__ void __launch_bounds__(128) k_mx_cfl(MV m, MxParams p, float cfl, flo
 }
 
 // limited face values (see below), one thread per (cell, species = blockIdx.y)
-__global__ void __launch_bounds__(128) k_mx_grad(MV m, MxParams p, int s0, const float *__restrict__ W, const double *__restrict__ U,
+__global__ void __launch_bounds__(128) k_mx_grad(MV m, MxParams p, int s0, const float4 *__restrict__ W, const double *__restrict__ U,
                                                  float *__restrict__ G)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -321,28 +320,29 @@ __global__ void __launch_bounds__(128) k_mx_grad(MV m, MxParams p, int s0, const
     if (c >= m.nc) return;
     const int64_t n = m.nc;
     float *Gs = G + (int64_t)g * 20 * n;
-    const float *Ws = W + (int64_t)s * 5 * n;
+    // primitives of species s: 8 floats per cell (rho u v w | p - - -), one 32-byte sector per gather
+    const float4 *Ws = W + 2 * (int64_t)s * n;
+    auto prim = [&](int32_t cc, float *q5) {
+        const float4 a = Ws[2 * (int64_t)cc], b = Ws[2 * (int64_t)cc + 1];
+        q5[0] = a.x; q5[1] = a.y; q5[2] = a.z; q5[3] = a.w; q5[4] = b.x;
+    };
     if (c >= m.no_cells || !m.st_valid[c])
     {
         // zero gradient: every face value is the cell value
+        float w5[5];
+        prim(c, w5);
         for (int q = 0; q < 5; ++q)
-        {
-            const float w = Ws[q * n + c];
-            for (int j = 0; j < 4; ++j) Gs[(4 * q + j) * n + c] = w;
-        }
+            for (int j = 0; j < 4; ++j) Gs[(4 * q + j) * n + c] = w5[q];
         return;
     }
     int32_t nb[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) nb[j] = m.t_nb[j * n + c];
     float wc[5], wn[4][5], wd[12], dx[12];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) wc[q] = Ws[q * n + c];
+    prim(c, wc);
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-        if (nb[j] >= 0)
-#pragma unroll
-            for (int q = 0; q < 5; ++q) wn[j][q] = Ws[q * n + nb[j]];
+        if (nb[j] >= 0) prim(nb[j], wn[j]);
 #pragma unroll
     for (int i = 0; i < 12; ++i)
     {
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(128) k_mx_grad(MV m, MxParams p, int s0, const
 }
 
 // Rusanov face flux times |A|, one thread per (face, species = blockIdx.y)
-__global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, const float *__restrict__ W, const float *__restrict__ G,
+__global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, const float *__restrict__ G,
                                                  float *__restrict__ F)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
@@ -454,12 +454,10 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, const
         for (int q = 0; q < 5; ++q) Fs[q * nf + f] = 0.f;
         return;
     }
-    const float *Ws = W + (int64_t)s * 5 * n;
     const float *Gs = G + (int64_t)g * 20 * n;
     const float4 nf4 = m.fn[f];
     const float3 nr = f3(nf4);
     const char2 sl = m.fslot[f];
-    (void)Ws;
     // reconstructed face state of cell c (positivity fallback already applied by k_mx_grad)
     auto state = [&](int32_t c, int side) {
         const int j = side == 0 ? sl.x : sl.y;
@@ -718,7 +716,7 @@ void mixed_setup(MhdState *st)
     if (nf) k_mx_faces<<<grid_for(nf, 256), 256, 0, s>>>(m, t.fn.p, t.fdx.p, t.fslot.p);
     if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.ee1.p, t.ee2.p, t.em.p, t.ew.p);
     MHD_LAUNCH_CHECK();
-    st->W32.alloc(5 * nc * st->nsp);
+    st->W32.alloc(8 * nc * st->nsp); // 8 floats per (species, cell): rho u v w | p, padded to 32 bytes
     st->grad32.alloc(20 * nc * st->group); // limited face values, 5 variables x 4 faces per cell
     st->F32.alloc(5 * nf * st->group);
     st->Ef32.alloc(3 * nf);
@@ -746,8 +744,9 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     const MxParams p = mx_params(st);
     const int gc = grid_for(m.nc, 128), gf = grid_for(m.nf, 128), ge = grid_for(m.ne, 128);
     if (!m.nc) return;
+    float4 *W4 = reinterpret_cast<float4 *>(st->W32.p);
     P.begin(KP_PREPARE, s);
-    k_mx_prepare<<<gc, 128, 0, s>>>(m, p, Us, phis, st->badd32.p, st->W32.p, st->up32.p, st->bt32.p, st->bi32.p);
+    k_mx_prepare<<<gc, 128, 0, s>>>(m, p, Us, phis, st->badd32.p, W4, st->up32.p, st->bt32.p, st->bi32.p);
     MHD_LAUNCH_CHECK();
     P.end(KP_PREPARE, s);
     ++st->launches;
@@ -756,7 +755,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         P.begin(KP_CFL, s);
         k_mx_cfl_init<<<1, 1, 0, s>>>(st->dt_bits.p, st->flag.p);
         k_mx_cfl<<<gc, 128, 0, s>>>(m, p, static_cast<float>(st->prm.cfl), static_cast<float>(st->prm.inver_MA2),
-                                    static_cast<float>(st->prm.rho_floor_dt), st->W32.p, st->bt32.p, st->dt_bits.p, st->flag.p);
+                                    static_cast<float>(st->prm.rho_floor_dt), W4, st->bt32.p, st->dt_bits.p, st->flag.p);
         k_mx_cfl_final<<<1, 1, 0, s>>>(st->dt_bits.p, dt_max, st->scal.p, st->flag.p);
         MHD_LAUNCH_CHECK();
         P.end(KP_CFL, s);
@@ -766,11 +765,11 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     {
         const int ng = std::min(st->group, st->nsp - s0);
         P.begin(KP_GRAD, s);
-        k_mx_grad<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->W32.p, Us, st->grad32.p);
+        k_mx_grad<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, W4, Us, st->grad32.p);
         MHD_LAUNCH_CHECK();
         P.end(KP_GRAD, s);
         P.begin(KP_FLUX, s);
-        k_mx_flux<<<dim3(gf, ng), 128, 0, s>>>(m, p, s0, st->W32.p, st->grad32.p, st->F32.p);
+        k_mx_flux<<<dim3(gf, ng), 128, 0, s>>>(m, p, s0, st->grad32.p, st->F32.p);
         MHD_LAUNCH_CHECK();
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
