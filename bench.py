@@ -488,8 +488,8 @@ def main():
         st.upload(gpu.FIELD_PHI, pin_P.numpy())
         st.step(0.0, sync=True)
         for s in range(wl.n_species):
-            pin_U[s].numpy()[:] = st.U(s)
-        pin_P.numpy()[:] = st.Phi()
+            st.download(gpu.FIELD_U, s, out=pin_U[s].numpy())
+        st.download(gpu.FIELD_PHI, out=pin_P.numpy())
         e2e_times.append(time.perf_counter() - t0)
     e2e_v = cu_per_step * world / float(np.median(e2e_times))
     io_bytes = (5 * h.n_cells * wl.n_species + h.n_faces) * 8

@@ -590,13 +590,24 @@ __global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float *__restric
     {
         const int32_t f0 = m.e2f_ptr[e], nfe = m.e2f_ptr[e + 1] - f0;
         const int32_t q0 = m.ec_ptr[e], q1 = m.ec_ptr[e + 1];
+        // the velocities of the edge's cells, gathered once into this thread's column of shared
+        // memory (every face of the edge takes the maximum over them); edges with more cells than
+        // the column holds gather them per face
+        constexpr int kCells = 8;
+        __shared__ float4 s_up[kCells][128];
+        const bool cached = q1 - q0 <= kCells;
         bool any_fluid = false;
-        for (int32_t k = q0; k < q1 && !any_fluid; ++k) any_fluid = m.material[m.ec_cell[k]] == 0;
+        for (int32_t k = q0; k < q1; ++k)
+        {
+            const int32_t c = m.ec_cell[k];
+            any_fluid |= m.material[c] == 0;
+            if (cached) s_up[k - q0][threadIdx.x] = up[c];
+        }
         if (nfe > 0 && Lg > 0.f && any_fluid)
         {
             const float3 e1 = f3(m.ee1[e]), e2 = f3(m.ee2[e]);
             // per face: q (2 components in the edge-normal plane) and w a sigma Phi/A; three arrays
-            // instead of six keep the kernel at 8 resident blocks of 128 threads
+            // instead of six keep the kernel at 6 resident blocks of 128 threads
             float qa[8], qb[8], wx[8];
             float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f;
 #pragma unroll
@@ -610,7 +621,10 @@ __global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float *__restric
                 const float w = m.ew[f0 + i];
                 Ec += w * (Ef[f] * th.x + Ef[nf + f] * th.y + Ef[2 * nf + f] * th.z);
                 float a = 0.f;
-                for (int32_t k = q0; k < q1; ++k) a = fmaxf(a, fabsf(fdot(f3(up[m.ec_cell[k]]), mi)));
+                if (cached)
+                    for (int32_t k = 0; k < q1 - q0; ++k) a = fmaxf(a, fabsf(fdot(f3(s_up[k][threadIdx.x]), mi)));
+                else
+                    for (int32_t k = q0; k < q1; ++k) a = fmaxf(a, fabsf(fdot(f3(up[m.ec_cell[k]]), mi)));
                 const float as = a * mi4.w;
                 qa[i] = as * (nf4.x * e1.x + nf4.y * e1.y + nf4.z * e1.z);
                 qb[i] = as * (nf4.x * e2.x + nf4.y * e2.y + nf4.z * e2.z);

@@ -363,12 +363,17 @@ class ResidentState:
         a = np.ascontiguousarray(data, np.float64)
         check(lib().mhd_gpu_state_upload(self._h, field, species, a.ctypes.data_as(vp)))
 
-    def download(self, field, species=0):
+    def download(self, field, species=0, out=None):
+        """Copy a field to host memory: a new array, or `out` (contiguous float64 of the field's size,
+        e.g. a view of pinned memory, which the device then writes directly)."""
         n = {FIELD_U: 5 * self.mesh.n_cells, FIELD_PHI: self.mesh.n_faces, FIELD_PHIADD: self.mesh.n_faces,
              FIELD_BADD: 3 * self.mesh.n_cells}[field]
-        a = np.empty(n)
-        check(lib().mhd_gpu_state_download(self._h, field, species, a.ctypes.data_as(vp)))
-        return a
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"out must be a contiguous float64 array of {n} values")
+        check(lib().mhd_gpu_state_download(self._h, field, species, out.ctypes.data_as(vp)))
+        return out
 
     def set(self, U_list, Phi, PhiAdd=None):
         for s, U in enumerate(U_list):
