@@ -525,6 +525,79 @@ static void floors(const OrMesh *m, const OrStepParams *p, double *const *U)
         }
 }
 
+/* mhd::Scales::numinfo (Common/physics/Scales.cpp:50-62) */
+typedef struct { double nH, nNa, ne, ne_eff, chiH, chiNa, wH, wNa; } OrNumInfo;
+static OrNumInfo numinfo(const OrStepParams *p, double rhoH, double rhoNa)
+{
+    OrNumInfo n;
+    n.nH = dmax(rhoH, 0.0) / p->mass[0] * p->M_ref;
+    n.nNa = dmax(rhoNa, 0.0) / p->mass[1] * p->M_ref;
+    n.ne = n.nH + n.nNa;
+    n.ne_eff = sqrt(n.ne * n.ne + p->ne_floor * p->ne_floor);
+    if (n.ne > 1e-300) { n.chiH = n.nH / n.ne; n.chiNa = n.nNa / n.ne; }
+    else { n.chiH = 1.0; n.chiNa = 0.0; }
+    n.wH = n.nH / n.ne_eff;
+    n.wNa = n.nNa / n.ne_eff;
+    return n;
+}
+
+/* mercury::add_sources_n (MercuryUns/fluid/MercurySources.cpp:20-63) with the Lorentz force only:
+ * S = inver_MA2 w_s (J x B); rhs_m += S, rhs_E += u.S + dt |S|^2 / (2 rho) (mid-point velocity work) */
+void or_add_sources(const OrMesh *m, const OrStepParams *p, int32_t s, const double *WH, const double *WNa, const double *B,
+                    const double *J, double dt, double *rhs)
+{
+    const double *W = s == 0 ? WH : WNa;
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        if (m->cell_material[c] == 1) continue;
+        const size_t i = (size_t)c;
+        const OrNumInfo ni = numinfo(p, WH[5 * i], WNa[5 * i]);
+        const double ws = s == 0 ? ni.wH : ni.wNa;
+        const double rho = dmax(W[5 * i], 0.0);
+        const v3 u = mk3(W[5 * i + 1], W[5 * i + 2], W[5 * i + 3]);
+        double *r = rhs + 5 * i;
+        v3 S = mk3(0, 0, 0);
+        if (p->lorentz) S = add3(S, scl(p->inver_MA2 * ws, cross3(ld(J, c), ld(B, c))));
+        r[1] += S.x; r[2] += S.y; r[3] += S.z;
+        r[4] += dot3(u, S) + (rho > 1e-30 ? 0.5 * dt * dot3(S, S) / rho : 0.0);
+    }
+}
+
+/* mercury::gyrate_n (MercuryUns/physics/Gyration.cpp): w = u_H - u_Na rotated by
+ * th = (a_H chi_Na + a_Na chi_H) |B| dt about b = B/|B|, split f_H, -f_Na between the ions; the
+ * kinetic-energy change goes to the total energy */
+void or_gyrate(const OrMesh *m, const OrStepParams *p, const double *B, double dt, double *UH, double *UNa)
+{
+    if (p->induce_coeff <= 0 || !p->lorentz) return;
+    const double aH = p->induce_coeff * p->M_ref / p->mass[0], aN = p->induce_coeff * p->M_ref / p->mass[1];
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        if (m->cell_material[c] == 1) continue;
+        double *uh = UH + 5 * (size_t)c, *un = UNa + 5 * (size_t)c;
+        const OrPrim wh = to_prim1(uh, p->gamma, p->rho_floor, p->p_floor), wn = to_prim1(un, p->gamma, p->rho_floor, p->p_floor);
+        const OrNumInfo ni = numinfo(p, uh[0], un[0]);
+        const v3 b = ld(B, c);
+        const double bm = sqrt(dot3(b, b));
+        const double denom = aH * ni.chiNa + aN * ni.chiH;
+        if (bm <= 0 || denom <= 0) continue;
+        const v3 bh = scl(1.0 / bm, b);
+        const v3 uH = mk3(wh.u, wh.v, wh.w), uN = mk3(wn.u, wn.v, wn.w);
+        const v3 w = sub3(uH, uN);
+        const v3 wpar = scl(dot3(w, bh), bh), wperp = sub3(w, wpar);
+        const double th = denom * bm * dt;
+        const v3 dw = add3(scl(cos(th) - 1.0, wperp), scl(sin(th), cross3(wperp, bh)));
+        const double fH = aH * ni.chiNa / denom, fN = aN * ni.chiH / denom;
+        const v3 dH = scl(fH, dw), dN = scl(-fN, dw);
+        const v3 uH2 = add3(uH, dH), uN2 = add3(uN, dN);
+        double rho = uh[0];
+        uh[1] = rho * uH2.x; uh[2] = rho * uH2.y; uh[3] = rho * uH2.z;
+        uh[4] += 0.5 * rho * (dot3(uH2, uH2) - dot3(uH, uH));
+        rho = un[0];
+        un[1] = rho * uN2.x; un[2] = rho * uN2.y; un[3] = rho * uN2.z;
+        un[4] += 0.5 * rho * (dot3(uN2, uN2) - dot3(uN, uN));
+    }
+}
+
 int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
 {
     const int32_t nc = m->n_cells, nf = m->n_faces, ne = m->n_edges, ns = p->n_species;
@@ -535,7 +608,17 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
     double *Bi = U2 + ns * c5, *Bt = Bi + 3 * (size_t)nc, *up = Bt + 3 * (size_t)nc, *Pt = up + 3 * (size_t)nc, *P1 = Pt + nf, *P2 = P1 + nf;
     double *E = P2 + nf;
     double *Us[16], *U1s[16], *U2s[16];
+    const int lorentz = p->lorentz != 0, split = lorentz && p->induce_coeff > 0;
+    if (lorentz && ns != 2) { free(mem); return -1; }
+    double *Jc = lorentz ? (double *)malloc(sizeof(double) * 3 * (size_t)(nc > 0 ? nc : 1)) : NULL;
     for (int s = 0; s < ns; ++s) { Us[s] = U[s]; U1s[s] = U1 + s * c5; U2s[s] = U2 + s * c5; }
+    if (split)
+    {
+        /* the opening half-step gyration with Btot of prepare(U^n) (Solver.cpp:492-498) */
+        or_cell_vector(m, Phi, nc, Bi);
+        for (size_t i = 0; i < 3 * (size_t)nc; ++i) Bt[i] = Bi[i] + BaddCell[i];
+        or_gyrate(m, p, Bt, 0.5 * dt, Us[0], Us[1]);
+    }
     for (int st = 0; st < 2; ++st)
     {
         double *const *Ui = st == 0 ? Us : U1s;
@@ -567,6 +650,11 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
             else memset(G + 3 * s * c5, 0, sizeof(double) * 3 * c5);
             or_flux_rhs(m, p->gamma, p->absorb[s], &p->fs[s], W + s * c5, G + 3 * s * c5, R + s * c5);
         }
+        if (lorentz) /* Solver::rhs (Solver.cpp:146-149): J of the induced field, sources after both flux passes */
+        {
+            or_cell_current(m, Bi, Jc);
+            for (int s = 0; s < ns; ++s) or_add_sources(m, p, s, W, W + c5, Bt, Jc, dt, R + s * c5);
+        }
         memset(E, 0, sizeof(double) * (size_t)ne);
         or_ideal_emf(m, up, Bt, Bi, Pt, phis, p->cuct, E);
         or_edge_modes(m, p->u_inf, p->B_imf, E);
@@ -586,6 +674,9 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
     for (int s = 0; s < ns; ++s)
         for (size_t i = 0; i < c5; ++i) U[s][i] = 0.5 * (U[s][i] + U2s[s][i]);
     for (int32_t f = 0; f < nf; ++f) Phi[f] = 0.5 * (Phi[f] + P2[f]);
+    /* the closing half step with Btot of the stage-2 input (Solver.cpp:510) */
+    if (split) or_gyrate(m, p, Bt, 0.5 * dt, Us[0], Us[1]);
+    free(Jc);
     free(mem);
     return 0;
 }

@@ -50,7 +50,15 @@ typedef struct OrStepParams {
     double mass[16];
     OrPrim fs[16];
     int8_t absorb[16];
+    /* two-ion model sources: J x B force and the Strang-split exact gyration (needs n_species == 2) */
+    int32_t lorentz;
+    double induce_coeff, inver_MA2;
 } OrStepParams;
+/* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part, species s: rhs += S */
+void or_add_sources(const OrMesh *m, const OrStepParams *p, int32_t s, const double *WH, const double *WNa, const double *B,
+                    const double *J, double dt, double *rhs);
+/* mercury::gyrate (MercuryUns/physics/Gyration.cpp): exact rotation of the relative ion velocity about B */
+void or_gyrate(const OrMesh *m, const OrStepParams *p, const double *B, double dt, double *UH, double *UNa);
 int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell,
                 double dt);
 

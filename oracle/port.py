@@ -33,7 +33,8 @@ class OrPrim(ctypes.Structure):
 class OrStepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl), ("cuct", dbl),
                 ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3),
-                ("mass", dbl * 16), ("fs", OrPrim * 16), ("absorb", ctypes.c_int8 * 16)]
+                ("mass", dbl * 16), ("fs", OrPrim * 16), ("absorb", ctypes.c_int8 * 16), ("lorentz", i32),
+                ("induce_coeff", dbl), ("inver_MA2", dbl)]
 
 
 class OrIndParams(ctypes.Structure):
@@ -64,6 +65,8 @@ def lib():
             ("or_cell_current", [P(OrMesh), vp, vp], None),
             ("or_local_time_step", [P(OrMesh), i32, vp, vp, dbl, dbl, dbl, dbl], dbl),
             ("or_rk2_step", [P(OrMesh), P(OrStepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
+            ("or_add_sources", [P(OrMesh), P(OrStepParams), i32, vp, vp, vp, vp, dbl, vp], None),
+            ("or_gyrate", [P(OrMesh), P(OrStepParams), vp, dbl, vp, vp], None),
             ("or_ind_create", [P(OrMesh), P(OrIndParams), vp], vp),
             ("or_ind_free", [vp], None),
             ("or_ind_set_frozen", [vp, vp, vp], None),
@@ -176,8 +179,9 @@ class PortMesh:
         return lib().or_local_time_step(self.ref, len(Ws), ctypes.cast(arr, ctypes.c_void_p), _p(_f(B)), gamma, cfl, inver_MA2,
                                         rho_floor_dt)
 
-    def rk2_step(self, wl, U_list, Phi, Badd, dt, absorb=None):
-        """One SSP-RK2 step of the hot path for a Workload's parameters; U_list and Phi updated in place."""
+    @staticmethod
+    def step_params(wl, absorb=None, lorentz=False, induce_coeff=0.0, inver_MA2=1.0):
+        """OrStepParams of a Workload (the reference's Config defaults for the rest)."""
         p = OrStepParams()
         p.n_species, p.second_order = wl.n_species, 1
         p.gamma, p.rho_floor, p.p_floor, p.cuct, p.M_ref, p.ne_floor, p.rel_limit = wl.gamma, 1e-10, 1e-12, 0.5, 1.0, 0.01, 0.0
@@ -187,6 +191,21 @@ class PortMesh:
             p.mass[s] = wl.mass[s]
             p.fs[s] = OrPrim(*[float(v) for v in wl.fs[s]])
             p.absorb[s] = int(s == 1) if absorb is None else int(absorb[s])
+        p.lorentz, p.induce_coeff, p.inver_MA2 = int(bool(lorentz)), float(induce_coeff), float(inver_MA2)
+        return p
+
+    def add_sources(self, p, species, WH, WNa, B, J, dt, rhs):
+        """mercury::add_sources, J x B part (oracle restatement); rhs in place."""
+        lib().or_add_sources(self.ref, ctypes.byref(p), species, _p(_f(WH)), _p(_f(WNa)), _p(_f(B)), _p(_f(J)), dt, _p(rhs))
+
+    def gyrate(self, p, B, dt, UH, UNa):
+        """mercury::gyrate (oracle restatement); UH, UNa in place."""
+        lib().or_gyrate(self.ref, ctypes.byref(p), _p(_f(B)), dt, _p(UH), _p(UNa))
+
+    def rk2_step(self, wl, U_list, Phi, Badd, dt, absorb=None, lorentz=False, induce_coeff=0.0, inver_MA2=1.0):
+        """One SSP-RK2 step of the hot path for a Workload's parameters; U_list and Phi updated in place.
+        With lorentz: the J x B source and (induce_coeff > 0) the Strang-split gyration of the two-ion model."""
+        p = self.step_params(wl, absorb, lorentz, induce_coeff, inver_MA2)
         arr = (ctypes.c_void_p * len(U_list))(*[u.ctypes.data for u in U_list])
         rc = lib().or_rk2_step(self.ref, ctypes.byref(p), ctypes.cast(arr, ctypes.c_void_p), _p(Phi), _p(_f(wl.PhiAdd)), _p(_f(Badd)), dt)
         if rc != 0:

@@ -31,7 +31,8 @@ class IndParams(ctypes.Structure):
 class StepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
                 ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("u_inf", dbl * 3),
-                ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", (dbl * 5) * 16)]
+                ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", (dbl * 5) * 16), ("lorentz", i32), ("pad", i32),
+                ("induce_coeff", dbl), ("inver_MA2", dbl)]
 
 
 def lib():
@@ -72,6 +73,8 @@ def lib():
             ("ref_ind_apply_A", [vp, vp, dbl, vp], None),
             ("ref_ind_solve", [vp, vp, vp, vp, dbl, i32, vp, vp], i32),
             ("ref_rk2_step", [vp, ctypes.POINTER(StepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
+            ("ref_add_sources", [vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, dbl, vp], None),
+            ("ref_gyrate", [vp, ctypes.POINTER(StepParams), vp, dbl, vp, vp], None),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -275,8 +278,19 @@ class RefMesh:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (WH, WNa, B)]
         return lib().ref_local_time_step(self._h, gamma, cfl, inver_MA2, rho_floor_dt, *[_p(a) for a in arrs])
 
+    def add_sources(self, params: StepParams, species, WH, WNa, up, B, J, dt, rhs):
+        """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part; rhs in place."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (WH, WNa, up, B, J)]
+        lib().ref_add_sources(self._h, ctypes.byref(params), species, *[_p(x) for x in a], dt, _p(rhs))
+
+    def gyrate(self, params: StepParams, B, dt, UH, UNa):
+        """mercury::gyrate (MercuryUns/physics/Gyration.cpp); UH, UNa in place."""
+        B = np.ascontiguousarray(B, np.float64)
+        lib().ref_gyrate(self._h, ctypes.byref(params), _p(B), dt, _p(UH), _p(UNa))
+
     def rk2_step(self, params: StepParams, U_list, Phi, PhiAdd, BaddCell, dt):
-        """One SSP-RK2 step of the hot path (Solver::step without model sources); U_list and Phi in place."""
+        """One SSP-RK2 step of the hot path (Solver::step; with params.lorentz the J x B source and the
+        Strang-split gyration of the two-ion model); U_list and Phi in place."""
         arr = (ctypes.c_void_p * len(U_list))(*[a.ctypes.data for a in U_list])
         PhiAdd = np.ascontiguousarray(PhiAdd, np.float64)
         BaddCell = np.ascontiguousarray(BaddCell, np.float64)

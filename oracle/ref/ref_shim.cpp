@@ -23,6 +23,7 @@
 #include "fluid/FluxRHS.h"
 #include "fluid/MercurySources.h"
 #include "fluid/Reconstruction.h"
+#include "physics/Gyration.h"
 #include "induction/Current.h"
 #include "induction/EdgeEMF.h"
 #include "induction/Faraday.h"
@@ -481,14 +482,49 @@ struct RefStepParams
     double u_inf[3], B_imf[3];
     double mass[16];
     double fs[16][5];
+    // model sources of the two-ion step: J x B force (add_sources_n) and the exact gyration (gyrate)
+    int32_t lorentz, pad;
+    double induce_coeff, inver_MA2;
 };
+
+namespace
+{
+// Config / Scales of the two-ion source terms (MercurySources.cpp:20-63, Gyration.cpp)
+Config source_config(const RefMesh *r, const RefStepParams &p)
+{
+    Config c = r->cfg;
+    c.sc.gamma = p.gamma; c.sc.M_ref = p.M_ref; c.sc.M_H = p.mass[0]; c.sc.M_Na = p.mass[1];
+    c.sc.ne_floor = p.ne_floor; c.sc.inver_MA2 = p.inver_MA2; c.sc.induce_coeff = p.induce_coeff;
+    c.rho_floor = p.rho_floor; c.p_floor = p.p_floor;
+    c.lorentz_force = p.lorentz != 0; c.ambipolar = false; c.chemistry = false;
+    return c;
+}
+} // namespace
+
+// mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63) for species s, J x B part
+void ref_add_sources(void *h, const RefStepParams *p, int32_t s, const double *WH, const double *WNa, const double *up,
+                     const double *B, const double *J, double dt, double *rhs)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    const Config c = source_config(r, *p);
+    mercury::SourceFields sf;
+    mercury::add_sources(r->lm, c, s, WH, WNa, up, B, J, sf, dt, rhs, nullptr);
+}
+
+// mercury::gyrate (MercuryUns/physics/Gyration.cpp), in place on UH, UNa
+void ref_gyrate(void *h, const RefStepParams *p, const double *B, double dt, double *UH, double *UNa)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    const Config c = source_config(r, *p);
+    mercury::gyrate(r->lm, c, B, dt, UH, UNa);
+}
 
 namespace
 {
 struct StepWork
 {
     std::vector<std::vector<double>> W, grad, rhs, U1, U2;
-    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2;
+    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2, J;
 };
 
 // charge-weighted ion velocity of Solver::prepare (Solver.cpp:108-118) with mhd::Scales::numinfo (Scales.cpp:50-62)
@@ -554,6 +590,10 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
         r->stencil->set_rel_limit(p.rel_limit);
         const Vec3 uinf(p.u_inf[0], p.u_inf[1], p.u_inf[2]), bimf(p.B_imf[0], p.B_imf[1], p.B_imf[2]);
         const Vec3 E_inf = -1.0 * cross(uinf, bimf);
+        const bool lorentz = p.lorentz != 0;
+        if (lorentz && ns != 2) throw std::runtime_error("the source terms are those of the two-ion model");
+        const Config scfg = source_config(r, p);
+        const bool split = lorentz && p.induce_coeff > 0; // Strang splitting of the gyration (Solver.cpp:492-498)
 
         // prepare + rhs of one stage on (Us, phis); the stage result goes to (Uo, phio)
         auto stage = [&](std::vector<double *> &Us, const double *phis, std::vector<double *> &Uo, double *phio) {
@@ -568,12 +608,24 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
             }
             uplus_of(p, cx, w.W, w.uplus);
             for (Id f = 0; f < nf; ++f) w.PhiTot[f] = phis[f] + PhiAdd[f];
+            if (lorentz)
+            {
+                w.J.assign(3 * static_cast<size_t>(nc), 0.0);
+                cell_current(r->lm, r->geo, w.Bind.data(), w.J.data());
+            }
             for (int k = 0; k < ns; ++k)
             {
                 const Prim fs{p.fs[k][0], p.fs[k][1], p.fs[k][2], p.fs[k][3], p.fs[k][4]};
                 if (p.second_order) r->stencil->limited_gradients(r->lm, r->geo, r->bc, w.W[k].data(), k, fs, true, w.grad[k].data());
                 else std::fill(w.grad[k].begin(), w.grad[k].end(), 0.0);
                 fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, k, fs, w.W[k].data(), w.grad[k].data(), w.rhs[k].data());
+            }
+            if (lorentz) // Solver::rhs (Solver.cpp:146-149): sources of both species after both flux passes
+            {
+                mercury::SourceFields sf;
+                for (int k = 0; k < ns; ++k)
+                    mercury::add_sources(r->lm, scfg, k, w.W[0].data(), w.W[1].data(), w.uplus.data(), w.Btot.data(), w.J.data(), sf, dt,
+                                         w.rhs[k].data(), nullptr);
             }
             std::fill(w.E.begin(), w.E.end(), 0.0);
             IdealInputs in;
@@ -611,11 +663,24 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
         }
         w.Phi1.resize(nf);
         w.Phi2.resize(nf);
+        if (split)
+        {
+            // Btot of prepare(s_) (Solver.cpp:487): the cell fit of Phi plus the background
+            const auto bi = reconstruct_cell_vector(cx, r->geo, Phi, nc);
+            std::vector<double> bt(3 * static_cast<size_t>(nc));
+            for (Id c = 0; c < nc; ++c)
+            {
+                bt[3 * c] = bi[c].x + BaddCell[3 * c]; bt[3 * c + 1] = bi[c].y + BaddCell[3 * c + 1]; bt[3 * c + 2] = bi[c].z + BaddCell[3 * c + 2];
+            }
+            mercury::gyrate(r->lm, scfg, bt.data(), 0.5 * dt, U0[0], U0[1]);
+        }
         stage(U0, Phi, U1, w.Phi1.data());
         stage(U1, w.Phi1.data(), U2, w.Phi2.data());
         for (int k = 0; k < ns; ++k)
             for (size_t i = 0; i < 5 * static_cast<size_t>(nc); ++i) U0[k][i] = 0.5 * (U0[k][i] + U2[k][i]);
         for (Id f = 0; f < nf; ++f) Phi[f] = 0.5 * (Phi[f] + w.Phi2[f]);
+        // the closing half step uses Btot of the last prepare, that of the stage-2 input (Solver.cpp:510)
+        if (split) mercury::gyrate(r->lm, scfg, w.Btot.data(), 0.5 * dt, U0[0], U0[1]);
     });
 }
 

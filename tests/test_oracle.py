@@ -134,3 +134,62 @@ def test_implicit_induction(hall, resistive):
         Er, itr, rrr = ri.solve(phi, Ee, dirichlet, 0.05, warm)
         assert ito == itr and rro == rrr
         same(Eo, Er)
+
+
+def _ref_params(wl, lorentz, induce, inver_MA2):
+    rp = ref.StepParams()
+    rp.n_species, rp.second_order, rp.gamma, rp.rho_floor, rp.p_floor, rp.cuct = 2, 1, wl.gamma, 1e-10, 1e-12, 0.5
+    rp.M_ref, rp.ne_floor = 1.0, 0.01
+    rp.u_inf[:] = list(wl.u_inf)
+    rp.B_imf[:] = list(wl.B_imf)
+    for s in range(2):
+        rp.mass[s] = wl.mass[s]
+        rp.fs[s][:] = list(wl.fs[s])
+    rp.lorentz, rp.induce_coeff, rp.inver_MA2 = int(lorentz), induce, inver_MA2
+    return rp
+
+
+def test_lorentz_sources_gyration_and_step():
+    """The J x B source (add_sources), the exact gyration and the Strang-split two-ion step, bit for bit."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5)
+    h = wl.mesh
+    r = ref_twin(h, SHELL_TAGS).boundary(*SHELL_BC)
+    o = port.PortMesh(h)
+    rng = np.random.default_rng(21)
+    rp = _ref_params(wl, True, 0.7, 0.8)
+    op = o.step_params(wl, lorentz=True, induce_coeff=0.7, inver_MA2=0.8)
+    W = [r.to_prim(u, wl.gamma) for u in wl.U]
+    B = rng.uniform(-2, 2, 3 * h.n_cells)
+    J = rng.uniform(-1, 1, 3 * h.n_cells)
+    for s in range(2):
+        ro = rng.uniform(-1, 1, 5 * h.n_cells)
+        rr = ro.copy()
+        o.add_sources(op, s, W[0], W[1], B, J, 0.03, ro)
+        r.add_sources(rp, s, W[0], W[1], np.zeros(3 * h.n_cells), B, J, 0.03, rr)
+        same(ro, rr)
+    UH, UN = [np.array(u) for u in wl.U]
+    UH[1::5] += rng.uniform(-1, 1, h.n_cells)   # relative velocity to rotate
+    UHr, UNr = UH.copy(), UN.copy()
+    o.gyrate(op, B, 0.05, UH, UN)
+    r.gyrate(rp, B, 0.05, UHr, UNr)
+    same(UH, UHr)
+    same(UN, UNr)
+    Badd = r.cell_vector(wl.PhiAdd)
+    Uo = [np.array(u) for u in wl.U]
+    Ur = [np.array(u) for u in wl.U]
+    Po, Pr = np.array(wl.Phi), np.array(wl.Phi)
+    for _ in range(3):
+        W = [r.to_prim(u, wl.gamma) for u in Ur]
+        dt = r.local_time_step(wl.gamma, 0.4, 1.0, 1e-2, W[0], W[1], r.cell_vector(Pr) + Badd)
+        o.rk2_step(wl, Uo, Po, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8)
+        r.rk2_step(rp, Ur, Pr, wl.PhiAdd, Badd, dt)
+        for a, b in zip(Uo, Ur):
+            same(a, b)
+        same(Po, Pr)
+    # the source terms act: one step with them differs from one step without them
+    Ua, Ub = [np.array(u) for u in wl.U], [np.array(u) for u in wl.U]
+    Pa, Pb = np.array(wl.Phi), np.array(wl.Phi)
+    o.rk2_step(wl, Ua, Pa, Badd, dt)
+    o.rk2_step(wl, Ub, Pb, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8)
+    assert np.linalg.norm(Ua[0] - Ub[0]) > 1e-6 * np.linalg.norm(Ua[0])
