@@ -181,6 +181,13 @@ typedef struct MhdStepParams {
     MhdPrim fs[16];                    /* free-stream (inflow ghost) state per species */
     int8_t absorb[16];                 /* wall ghost absorbs the species (reference: species 1) */
     int32_t precision;                 /* MHD_PREC_FP64 or MHD_PREC_MIXED */
+    /* Sources of the two-ion model (n_species == 2: species 0 = H+, 1 = Na+; Config::lorentz_force,
+     * Scales::induce_coeff): with lorentz != 0 every stage adds the J x B force of
+     * mercury::add_sources_n (MercurySources.cpp:20-63), and with induce_coeff > 0 the step is
+     * wrapped in two half-step exact gyrations (mercury::gyrate, Strang splitting as in
+     * mercury::Solver::step, Solver.cpp:492-510).  Zero-initialised parameters leave them off. */
+    int32_t lorentz;
+    double induce_coeff;
 } MhdStepParams;
 
 /* FP64 reference-exact: every operation rounds as in the reference's host code.
@@ -207,6 +214,17 @@ int mhd_gpu_cfl_dt(MhdState *state, double dt_max, double *host_dt);
  * capped by dt_max is computed on the device.  dt_used (host, may be NULL) receives the step
  * and makes the call synchronous; with NULL the step is only enqueued (no host round trip). */
 int mhd_gpu_step_rk2(MhdState *state, double dt_fixed, double dt_max, double *dt_used);
+
+/* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part, for species 0 or 1 of
+ * the two-ion model (params: n_species 2, mass[0..1], M_ref, ne_floor, inver_MA2, lorentz): rhs += the
+ * source on the owned fluid cells.  WH, WNa: primitives (5 per cell); B total field, J current
+ * (3 per cell); FP64 in the reference's operation order. */
+int mhd_gpu_add_sources(MhdMesh *mesh, const MhdStepParams *params, int32_t species, const double *WH, const double *WNa,
+                        const double *B, const double *J, double dt, double *rhs);
+/* mercury::gyrate (MercuryUns/physics/Gyration.cpp): exact rotation of the ions' relative velocity
+ * about B over dt on the owned fluid cells, UH and UNa (5 per cell) in place; a no-op unless
+ * lorentz != 0 and induce_coeff > 0, as in the reference. */
+int mhd_gpu_gyrate(MhdMesh *mesh, const MhdStepParams *params, const double *B, double dt, double *UH, double *UNa);
 
 /* Live per-kernel timing of the fused step (CUDA events recorded on the handle's stream around
  * every launch while enabled).  _read synchronises, returns per kernel class its name (32 chars

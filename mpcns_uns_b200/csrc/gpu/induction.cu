@@ -360,6 +360,13 @@ double *noalloc_scratch()
     }
     return addr[dev];
 }
+
+void launch_cell_current(const MeshView &m, const double *B, double *J, cudaStream_t s)
+{
+    if (!m.nc) return;
+    k_cell_current<<<grid_for(m.nc, 128), 128, 0, s>>>(m, B, J);
+    MHD_LAUNCH_CHECK();
+}
 } // namespace mhd
 
 using namespace mhd;

@@ -179,6 +179,8 @@ struct MxParams
     int8_t absorb[kMaxSpecies];
     float mass[kMaxSpecies];
     float M_ref;
+    int src_on;                 // two-ion J x B force (species 0 = H+, 1 = Na+)
+    float inver_MA2, ne_floor;
 };
 
 __device__ __forceinline__ F5 ghost32(int kind, bool absorb, const F5 &in, float3 n, const F5 &fs)
@@ -491,9 +493,48 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, const
     for (int q = 0; q < 5; ++q) Fs[q * nf + f] = Fl[q] * nf4.w;
 }
 
+// mhd::cell_current (Common/induction/Current.cpp:9-31) of the induced cell field in FP32:
+// J_c = (1/V) sum_f s A_f x 1/2 (b_c + b_nb), b_c alone on faces with one cell
+__global__ void __launch_bounds__(128) k_mx_current(MV m, const float4 *__restrict__ bi, float4 *__restrict__ J)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    if (c >= m.no_cells)
+    {
+        J[c] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
+    const int32_t ff[4] = {fi.x, fi.y, fi.z, fi.w};
+    const float3 bc = f3(bi[c]);
+    float3 sum = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        const int32_t f = ff[j];
+        const int32_t L = m.face_L[f], R = m.face_R[f];
+        const int32_t o = L == c ? R : L;
+        float3 bf = bc;
+        if (o >= 0)
+        {
+            const float3 bo = f3(bi[o]);
+            bf = make_float3(0.5f * (bc.x + bo.x), 0.5f * (bc.y + bo.y), 0.5f * (bc.z + bo.z));
+        }
+        const float4 nf4 = m.fn[f];
+        const float sa = static_cast<float>(m.c2f_sgn[4 * (int64_t)c + j]) * nf4.w;
+        const float3 cr = fcross(make_float3(sa * nf4.x, sa * nf4.y, sa * nf4.z), bf);
+        sum.x += cr.x;
+        sum.y += cr.y;
+        sum.z += cr.z;
+    }
+    const float iv = m.vol_inv[c];
+    J[c] = make_float4(sum.x * iv, sum.y * iv, sum.z * iv, 0.f);
+}
+
 // rhs gathered from the face fluxes, U (FP64) += dt rhs, floors, SSP-RK2 average in stage 2
 __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, const float *__restrict__ F, const double *__restrict__ Ub,
-                                                   double *__restrict__ Uo, const double *__restrict__ dtp, int stage2)
+                                                   double *__restrict__ Uo, const double *__restrict__ dtp, int stage2,
+                                                   const float4 *__restrict__ W, const float4 *__restrict__ J, const float4 *__restrict__ bt)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y, s = s0 + g;
@@ -520,6 +561,25 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, con
         const double dtv = *dtp / m.cell_volume[c];
 #pragma unroll
         for (int q = 0; q < 5; ++q) u[q] += dtv * r[q];
+        if (p.src_on)
+        {
+            // J x B force of mercury::add_sources_n (MercurySources.cpp:29-47) in FP32, added to the FP64 update
+            const float4 wH = W[2 * (int64_t)c], wN = W[2 * ((int64_t)n + c)], ws4 = W[2 * ((int64_t)s * n + c)];
+            const float nH = fmaxf(wH.x, 0.f) / p.mass[0] * p.M_ref, nN = fmaxf(wN.x, 0.f) / p.mass[1] * p.M_ref;
+            const float ne = nH + nN, ne_eff = sqrtf(ne * ne + p.ne_floor * p.ne_floor);
+            const float wsp = (s == 0 ? nH : nN) / ne_eff;
+            const float3 Sv = fcross(f3(J[c]), f3(bt[c]));
+            const float k = p.inver_MA2 * wsp;
+            const float Sx = k * Sv.x, Sy = k * Sv.y, Sz = k * Sv.z;
+            const float rho = fmaxf(ws4.x, 0.f);
+            const double dt = *dtp;
+            const float work = ws4.y * Sx + ws4.z * Sy + ws4.w * Sz +
+                               (rho > 1e-30f ? 0.5f * static_cast<float>(dt) * (Sx * Sx + Sy * Sy + Sz * Sz) / rho : 0.f);
+            u[1] += dt * static_cast<double>(Sx);
+            u[2] += dt * static_cast<double>(Sy);
+            u[3] += dt * static_cast<double>(Sz);
+            u[4] += dt * static_cast<double>(work);
+        }
         const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
         const double gm = p.gamma_d;
         if (!(u[0] >= p.rho_floor_d))
@@ -703,6 +763,9 @@ MxParams mx_params(const MhdState *st)
     p.rho_floor_d = q.rho_floor;
     p.p_floor_d = q.p_floor;
     p.M_ref = static_cast<float>(q.M_ref);
+    p.src_on = st->src.on;
+    p.inver_MA2 = static_cast<float>(q.inver_MA2);
+    p.ne_floor = static_cast<float>(q.ne_floor);
     for (int s = 0; s < st->nsp; ++s)
     {
         p.fs[s] = F5{static_cast<float>(q.fs[s].rho), static_cast<float>(q.fs[s].u), static_cast<float>(q.fs[s].v),
@@ -724,6 +787,7 @@ void mixed_setup(MhdState *st)
     int32_t nnz_e2f = 0;
     MHD_CUDA(cudaMemcpy(&nnz_e2f, m.e2f_ptr + m.ne, sizeof(int32_t), cudaMemcpyDeviceToHost));
     t.wd.alloc(12 * nc); t.dx.alloc(12 * nc); t.inv.alloc(6 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
+    if (st->src.on) st->J32.alloc(nc);
     t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
     t.eth.alloc(ne); t.ee1.alloc(ne); t.ee2.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
     if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.wd.p, t.dx.p, t.inv.p, t.recon.p, t.vol_inv.p);
@@ -748,22 +812,27 @@ void mixed_badd(MhdState *st)
     MHD_LAUNCH_CHECK();
 }
 
-void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max)
+void mixed_prepare(MhdState *st, const double *Us, const double *phis, bool cfl, double dt_max)
 {
     MhdMesh *mesh = st->mesh;
-    const MeshView &mv = mesh->v;
-    const MV m = make_view(mv, st->mt);
+    const MV m = make_view(mesh->v, st->mt);
     cudaStream_t s = mesh->stream;
     Profiler &P = st->prof;
     const MxParams p = mx_params(st);
-    const int gc = grid_for(m.nc, 128), gf = grid_for(m.nf, 128), ge = grid_for(m.ne, 128);
+    const int gc = grid_for(m.nc, 128);
     if (!m.nc) return;
     float4 *W4 = reinterpret_cast<float4 *>(st->W32.p);
     P.begin(KP_PREPARE, s);
     k_mx_prepare<<<gc, 128, 0, s>>>(m, p, Us, phis, st->badd32.p, W4, st->up32.p, st->bt32.p, st->bi32.p);
     MHD_LAUNCH_CHECK();
-    P.end(KP_PREPARE, s);
     ++st->launches;
+    if (st->src.on) // J of the induced field (Solver.cpp:123)
+    {
+        k_mx_current<<<gc, 128, 0, s>>>(m, st->bi32.p, st->J32.p);
+        MHD_LAUNCH_CHECK();
+        ++st->launches;
+    }
+    P.end(KP_PREPARE, s);
     if (cfl)
     {
         P.begin(KP_CFL, s);
@@ -775,6 +844,20 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         P.end(KP_CFL, s);
         st->launches += 3;
     }
+}
+
+void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max)
+{
+    MhdMesh *mesh = st->mesh;
+    const MeshView &mv = mesh->v;
+    const MV m = make_view(mv, st->mt);
+    cudaStream_t s = mesh->stream;
+    Profiler &P = st->prof;
+    const MxParams p = mx_params(st);
+    const int gc = grid_for(m.nc, 128), gf = grid_for(m.nf, 128), ge = grid_for(m.ne, 128);
+    if (!m.nc) return;
+    float4 *W4 = reinterpret_cast<float4 *>(st->W32.p);
+    mixed_prepare(st, Us, phis, cfl, dt_max);
     for (int s0 = 0; s0 < st->nsp; s0 += st->group)
     {
         const int ng = std::min(st->group, st->nsp - s0);
@@ -787,7 +870,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         MHD_LAUNCH_CHECK();
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
-        k_mx_update<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0);
+        k_mx_update<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->J32.p, st->bt32.p);
         MHD_LAUNCH_CHECK();
         P.end(KP_UPDATE, s);
         st->launches += 3;

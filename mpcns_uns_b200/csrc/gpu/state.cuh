@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "fluid.cuh"
+#include "sources.cuh"
 
 namespace mhd
 {
@@ -39,6 +40,9 @@ struct MhdState
     int nsp = 0, group = 0;
     bool mixed = false;
     mhd::DBuf<double> U0, U1, W, grad, F, phi0, phi1, phi_add, badd, bind, btot, up, Ef, E, mass, stage;
+    mhd::SrcParams src;     // two-ion J x B force and gyration (off unless params.lorentz)
+    mhd::DBuf<double> J;    // cell current of the induced field (3 per cell) when the J x B force is on
+    mhd::DBuf<float4> J32;  // the same for the mixed-precision stage
     mhd::DBuf<double> scal; // [0] dt
     mhd::DBuf<unsigned long long> dt_bits;
     mhd::DBuf<int> flag;
@@ -60,4 +64,6 @@ namespace mhd
 void mixed_setup(MhdState *st);
 void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max);
 void mixed_badd(MhdState *st);
+// primitives, cell fields (and with cfl the device CFL step) of (Us, phis) in mixed precision
+void mixed_prepare(MhdState *st, const double *Us, const double *phis, bool cfl, double dt_max);
 } // namespace mhd

@@ -4,11 +4,13 @@
 //
 // One stage on (Us, Phi_s) -> (Uo, Phi_o):
 //   k_prepare      per cell: primitives of every species, B_ind = cell fit of Phi_s, B_tot, u+
+//   [k_cell_current] J of B_ind when the two-ion J x B force is on
 //   [k_cfl_*]      stage 1, CFL mode: per-cell step, device-wide minimum (no host round trip)
-//   per species group: k_limited_gradients, k_face_flux, k_update (gather + U += dt rhs + floors)
+//   per species group: k_limited_gradients, k_face_flux, k_update (gather [+ J x B] + U += dt rhs + floors)
 //   k_face_candidate, k_edge_emf_assign (begin + UCT + boundary edge values)
 //   k_ct           Phi_o = Phi_s - dt d1 E on the active faces
-// Stage 2 writes the SSP-RK2 averages U = (U0 + U2)/2, Phi = (Phi0 + Phi2)/2 in place.
+// Stage 2 writes the SSP-RK2 averages U = (U0 + U2)/2, Phi = (Phi0 + Phi2)/2 in place.  With the
+// gyration on, half-step exact gyrations (k_gyrate) wrap the two stages (Strang splitting).
 #include <math_constants.h>
 
 #include <algorithm>
@@ -144,14 +146,23 @@ __global__ void k_set_dt(double *dt, double v, int *flag)
     *flag = 0;
 }
 
+// Inputs of the two-ion J x B source added to the gathered rhs (mercury::Solver::rhs, Solver.cpp:146-149)
+struct SrcView
+{
+    SrcParams p;
+    SField<const double> W; // primitives of all species
+    const double *J, *Bt;   // cell current of the induced field, total cell field
+};
+
 // Solver::advance (Solver.cpp:194-206) for one species group: rhs gathered from the face fluxes in the
-// reference's scatter order, U = U_base + dt rhs on the owned fluid cells, Solver::enforce_floors
-// (:171-191); stage 2 averages with U0 in place (Solver.cpp:505-506).
+// reference's scatter order, plus the J x B source when it is on, U = U_base + dt rhs on the owned
+// fluid cells, Solver::enforce_floors (:171-191); stage 2 averages with U0 in place (Solver.cpp:505-506).
 // NF = 4: tetrahedral mesh, the four faces of the cell unrolled (all flux gathers in flight together);
 // NF = 0: any polyhedra.  One thread per (cell, species of the group = blockIdx.y).
 template <int NF>
 __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s0, int ng, const double *__restrict__ F,
-                                                 SField<const double> Ub, SField<double> Uo, const double *__restrict__ dtp, int stage2)
+                                                 SField<const double> Ub, SField<double> Uo, const double *__restrict__ dtp, int stage2,
+                                                 SrcView sv)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y;
@@ -199,6 +210,11 @@ __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s
                         r[q] = out ? r[q] - v : r[q] + v;
                     }
                 }
+            if (sv.p.on)
+            {
+                const double w[5] = {sv.W(s, c, 0), sv.W(s, c, 1), sv.W(s, c, 2), sv.W(s, c, 3), sv.W(s, c, 4)};
+                lorentz_source(sv.p, s, sv.W(0, c, 0), sv.W(1, c, 0), w, ld3(sv.J, c), ld3(sv.Bt, c), dt, r);
+            }
             for (int q = 0; q < 5; ++q) u[q] += dt * r[q];
             const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
             if (!(u[0] >= p.rho_floor)) to_cons5(Prim5{p.rho_floor, 0, 0, 0, p.p_floor}, p.gamma, u);
@@ -262,13 +278,14 @@ namespace
 SField<double> soa_state(double *p, int64_t nc) { return {p, 5 * nc, 1, nc}; }
 SField<const double> soa_cstate(const double *p, int64_t nc) { return {p, 5 * nc, 1, nc}; }
 
-void stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max)
+// Solver::prepare of (Us, phis) (with the cell current when the J x B force is on) and, with cfl,
+// the device CFL step (mercury::local_time_step) into scal[0]
+void prepare_cfl(MhdState *st, const double *Us, const double *phis, bool cfl, double dt_max)
 {
     MhdMesh *mesh = st->mesh;
     const MeshView &m = mesh->v;
     cudaStream_t s = mesh->stream;
     const int64_t nc = m.nc;
-    const int nsp = st->nsp;
     Profiler &P = st->prof;
     if (m.nc)
     {
@@ -276,8 +293,13 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
         k_prepare<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->fp, st->mass.p, st->prm.M_ref, soa_cstate(Us, nc), soa_state(st->W.p, nc),
                                                       phis, st->badd.p, st->bind.p, st->btot.p, st->up.p);
         MHD_LAUNCH_CHECK();
-        P.end(KP_PREPARE, s);
         ++st->launches;
+        if (st->src.on) // J of the induced field (Solver.cpp:123)
+        {
+            launch_cell_current(m, st->bind.p, st->J.p, s);
+            ++st->launches;
+        }
+        P.end(KP_PREPARE, s);
     }
     if (cfl)
     {
@@ -291,6 +313,19 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
         P.end(KP_CFL, s);
         st->launches += m.no_cells ? 3 : 2;
     }
+}
+
+void stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
+           bool prepared = false)
+{
+    MhdMesh *mesh = st->mesh;
+    const MeshView &m = mesh->v;
+    cudaStream_t s = mesh->stream;
+    const int64_t nc = m.nc;
+    const int nsp = st->nsp;
+    Profiler &P = st->prof;
+    if (!prepared) prepare_cfl(st, Us, phis, cfl, dt_max);
+    const SrcView sv{st->src, soa_cstate(st->W.p, nc), st->J.p, st->btot.p};
     for (int s0 = 0; s0 < nsp; s0 += st->group)
     {
         const int ng = std::min(st->group, nsp - s0);
@@ -316,10 +351,10 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
             const dim3 grid(grid_for(m.nc, 128), ng);
             if (m.faces_per_cell == 4)
                 k_update<4><<<grid, 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
-                                                 stage2 ? 1 : 0);
+                                                 stage2 ? 1 : 0, sv);
             else
                 k_update<0><<<grid, 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
-                                                 stage2 ? 1 : 0);
+                                                 stage2 ? 1 : 0, sv);
             MHD_LAUNCH_CHECK();
             P.end(KP_UPDATE, s);
         }
@@ -370,6 +405,7 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         MHD_REQUIRE(p->n_species >= 1 && p->n_species <= kMaxSpecies, "n_species must be 1..16");
         MHD_REQUIRE(p->gamma > 1.0, "gamma must exceed 1");
         for (int s = 0; s < p->n_species; ++s) MHD_REQUIRE(p->mass[s] > 0, "species masses must be positive");
+        MHD_REQUIRE(!p->lorentz || p->n_species == 2, "the J x B force and the gyration are those of the two-ion model (n_species == 2)");
         st = new MhdState;
         st->mesh = mesh;
         st->prm = *p;
@@ -408,6 +444,8 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         st->dt_bits.alloc(1);
         st->flag.alloc(1);
         st->mass.upload(p->mass, st->nsp);
+        st->src = src_params(*p);
+        if (st->src.on) st->J.alloc(3 * nc);
         MHD_CUDA(cudaMallocHost(&st->pinned, 8 * sizeof(double)));
         MHD_REQUIRE(p->precision == MHD_PREC_FP64 || p->precision == MHD_PREC_MIXED, "unknown precision");
         st->mixed = p->precision == MHD_PREC_MIXED;
@@ -545,16 +583,36 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
             MHD_LAUNCH_CHECK();
             ++st->launches;
         }
+        // Strang splitting of the gyration (Solver.cpp:487-510): prepare and CFL step of U^n, half-step
+        // gyration with its Btot, the two stages, then the closing half step with the Btot of the last
+        // prepare (that of the stage-2 input)
+        const bool split = st->src.on && st->src.induce > 0;
+        const MeshView &m = st->mesh->v;
         if (st->mixed)
         {
-            mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl, dt_max);
+            if (split)
+            {
+                mixed_prepare(st, st->U0.p, st->phi0.p, cfl, dt_max);
+                launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
+                st->launches += m.no_cells ? 1 : 0;
+            }
+            mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max);
             mixed_stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
+            if (split) launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
         }
         else
         {
-            stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl, dt_max);
+            if (split)
+            {
+                prepare_cfl(st, st->U0.p, st->phi0.p, cfl, dt_max);
+                launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
+                st->launches += m.no_cells ? 1 : 0;
+            }
+            stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max);
             stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
+            if (split) launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
         }
+        if (split && m.no_cells) ++st->launches;
         if (dt_used) read_dt(st, dt_used);
     });
 }

@@ -46,7 +46,7 @@ class StepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
                 ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("cfl", dbl), ("inver_MA2", dbl),
                 ("rho_floor_dt", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", Prim * 16),
-                ("absorb", ctypes.c_int8 * 16), ("precision", i32)]
+                ("absorb", ctypes.c_int8 * 16), ("precision", i32), ("lorentz", i32), ("induce_coeff", dbl)]
 
 
 class InductionParams(ctypes.Structure):
@@ -86,6 +86,8 @@ _SIGS = {
     "mhd_gpu_faraday_edge_dt": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_div_b": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_cell_current": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_add_sources": ([vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_gyrate": ([vp, ctypes.POINTER(StepParams), vp, dbl, vp, vp], ctypes.c_int),
     "mhd_gpu_induction_create": ([vp, ctypes.POINTER(InductionParams), vp, ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_induction_destroy": ([vp], ctypes.c_int),
     "mhd_gpu_induction_set_frozen": ([vp, vp, vp], ctypes.c_int),
@@ -306,6 +308,25 @@ class DeviceMesh:
         check(lib().mhd_gpu_div_b(self._h, ptr(B), ptr(ex), out.ctypes.data_as(vp)))
         return dict(max_abs=float(out[0]), max_rel=float(out[1]), worst_cell_gid=int(out[2]))
 
+    def add_sources(self, params, species, WH, WNa, B, J, dt, rhs):
+        """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part; returns rhs + source."""
+        WH, WNa, B, J = dev(WH), dev(WNa), dev(B), dev(J)
+        rhs = dev(rhs).clone()
+        self._enter()
+        check(lib().mhd_gpu_add_sources(self._h, ctypes.byref(params), int(species), ptr(WH), ptr(WNa), ptr(B), ptr(J), float(dt),
+                                         ptr(rhs)))
+        self._leave()
+        return rhs
+
+    def gyrate(self, params, B, dt, UH, UNa):
+        """mercury::gyrate (MercuryUns/physics/Gyration.cpp); returns the updated copies of UH, UNa."""
+        B = dev(B)
+        UH, UNa = dev(UH).clone(), dev(UNa).clone()
+        self._enter()
+        check(lib().mhd_gpu_gyrate(self._h, ctypes.byref(params), ptr(B), float(dt), ptr(UH), ptr(UNa)))
+        self._leave()
+        return UH, UNa
+
     def cell_current(self, B):
         """mhd::cell_current (Common/induction/Current.cpp:9-31): 3 per cell."""
         torch = _torch()
@@ -319,10 +340,11 @@ class DeviceMesh:
 
 def step_params(n_species, gamma=5.0 / 3.0, fs=None, mass=None, u_inf=(0.0, 0.0, 0.0), B_imf=(0.0, 0.0, 0.0), cuct=0.5,
                 second_order=True, rho_floor=1e-10, p_floor=1e-12, rel_limit=0.0, cfl=0.4, inver_MA2=1.0, rho_floor_dt=1e-2,
-                M_ref=1.0, ne_floor=0.01, absorb=None, precision="fp64"):
+                M_ref=1.0, ne_floor=0.01, absorb=None, precision="fp64", lorentz=False, induce_coeff=0.0):
     """MhdStepParams with the reference's Config / Scales defaults (Common/config/Config.h:19-96)."""
     p = StepParams()
     p.precision = PREC_MIXED if precision == "mixed" else PREC_FP64
+    p.lorentz, p.induce_coeff = int(bool(lorentz)), float(induce_coeff)
     p.n_species, p.second_order = int(n_species), int(bool(second_order))
     p.gamma, p.rho_floor, p.p_floor, p.cuct = gamma, rho_floor, p_floor, cuct
     p.M_ref, p.ne_floor, p.rel_limit = M_ref, ne_floor, rel_limit

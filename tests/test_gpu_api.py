@@ -174,3 +174,45 @@ def test_cell_current(meshes):
     rng = np.random.default_rng(700)
     B = rng.uniform(-1, 1, 3 * h.n_cells)
     assert rel_err(_np(d.cell_current(B)), r.cell_current(B)) < TOL
+
+
+def _two_ion_params(lorentz=True, induce=0.6):
+    from mpcns_uns_b200 import gpu
+    p = gpu.step_params(2, mass=[1.0, 23.0], lorentz=lorentz, induce_coeff=induce, inver_MA2=0.9, ne_floor=0.02)
+    rp = ref.StepParams()
+    rp.n_species, rp.second_order, rp.gamma, rp.rho_floor, rp.p_floor = 2, 1, p.gamma, p.rho_floor, p.p_floor
+    rp.M_ref, rp.ne_floor = p.M_ref, p.ne_floor
+    rp.mass[0], rp.mass[1] = 1.0, 23.0
+    rp.lorentz, rp.induce_coeff, rp.inver_MA2 = int(lorentz), induce, p.inver_MA2
+    return p, rp
+
+
+@pytest.mark.parametrize("lorentz", [True, False])
+def test_add_sources(meshes, lorentz):
+    """mercury::add_sources, J x B part, both ions (the source is zero with the force off)."""
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(701)
+    p, rp = _two_ion_params(lorentz)
+    WH, WN = random_prims(h.n_cells, rng), random_prims(h.n_cells, rng, rho=(1e-4, 1e-2))
+    B, J = rng.uniform(-2, 2, 3 * h.n_cells), rng.uniform(-1, 1, 3 * h.n_cells)
+    for s in (0, 1):
+        rhs = rng.uniform(-1, 1, 5 * h.n_cells)
+        want = rhs.copy()
+        r.add_sources(rp, s, WH, WN, np.zeros(3 * h.n_cells), B, J, 0.02, want)
+        assert rel_err(_np(d.add_sources(p, s, WH, WN, B, J, 0.02, rhs)), want) < TOL
+
+
+def test_gyrate(meshes):
+    """mercury::gyrate: exact rotation of the relative ion velocity about B."""
+    from mpcns_uns_b200 import workloads
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(702)
+    p, rp = _two_ion_params()
+    UH = workloads.to_cons(random_prims(h.n_cells, rng), p.gamma).ravel()
+    UN = workloads.to_cons(random_prims(h.n_cells, rng, rho=(1e-3, 1e-1)), p.gamma).ravel()
+    B = rng.uniform(-2, 2, 3 * h.n_cells)
+    UHr, UNr = UH.copy(), UN.copy()
+    r.gyrate(rp, B, 0.07, UHr, UNr)
+    gH, gN = d.gyrate(p, B, 0.07, UH, UN)
+    assert rel_err(_np(gH), UHr) < TOL and rel_err(_np(gN), UNr) < TOL
+    assert rel_err(UHr, UH) > 1e-6          # the rotation did something

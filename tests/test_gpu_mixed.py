@@ -12,10 +12,10 @@ L2_TOL = 1e-5
 DIVB_TOL = 1e-12
 
 
-def _run(wl, precision, nsteps):
+def _run(wl, precision, nsteps, **kw):
     from mpcns_uns_b200 import gpu
     dm = gpu.DeviceMesh(wl.mesh)
-    p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, precision=precision)
+    p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, precision=precision, **kw)
     st = gpu.ResidentState(dm, p)
     st.set(wl.U, wl.Phi, wl.PhiAdd)
     dts = [st.step(0.0) for _ in range(nsteps)]
@@ -40,3 +40,21 @@ def test_mixed_vs_fp64(case):
     dP = np.linalg.norm(P32 - P64) / max(np.linalg.norm(P64 + wl.PhiAdd), 1e-300)
     assert dP < L2_TOL
     assert dm.div_b(P32)["max_rel"] < DIVB_TOL
+
+
+def test_mixed_vs_fp64_lorentz_gyration():
+    """The two-ion step with the J x B force and the exact gyration: same tolerances."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(6, 8)
+    kw = dict(lorentz=True, induce_coeff=1.0)
+    n = 20
+    U64, P64, dt64, dm = _run(wl, "fp64", n, **kw)
+    U32, P32, dt32, _ = _run(wl, "mixed", n, **kw)
+    Un, _, _, _ = _run(wl, "fp64", n)
+    assert np.allclose(dt32, dt64, rtol=1e-5)
+    num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(U32, U64))
+    den = sum(float(np.sum(b ** 2)) for b in U64)
+    assert np.sqrt(num / den) < L2_TOL
+    assert _l2(U32[0], U64[0]) < L2_TOL
+    assert dm.div_b(P32)["max_rel"] < DIVB_TOL
+    assert _l2(Un[0], U64[0]) > 1e-6       # the sources act on this workload

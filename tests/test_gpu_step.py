@@ -29,6 +29,7 @@ def ref_params(p):
         rp.mass[s] = p.mass[s]
         f = p.fs[s]
         rp.fs[s][:] = [f.rho, f.u, f.v, f.w, f.p]
+    rp.lorentz, rp.induce_coeff, rp.inver_MA2 = p.lorentz, p.induce_coeff, p.inver_MA2
     return rp
 
 
@@ -101,4 +102,13 @@ def test_step_box_three_species_mixed_bc():
     wl.mass = [1.0, 16.0, 32.0]
     wl.u_inf, wl.B_imf = MIXED_BOX_BC[2], (0.05, -0.1, 0.2)
     div = run_pair(wl, BOX_TAGS, MIXED_BOX_BC, 3, use_cfl=False)
+    assert div < 1e-12
+
+
+@pytest.mark.parametrize("induce", [0.0, 0.8])
+def test_step_shell_two_ions_lorentz(induce):
+    """The two-ion step with the J x B force (and, induce > 0, the Strang-split exact gyration)."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5, r_in=1.0, r_out=6.0)
+    div = run_pair(wl, SHELL_TAGS, SHELL_BC, 4, params_kw=dict(lorentz=True, induce_coeff=induce, inver_MA2=0.7))
     assert div < 1e-12
