@@ -7,8 +7,10 @@ Workload (default): cubed-sphere shell r in [1, 6], 6 x 64 x 64 surface cells x 
 radial layers, every hexahedron cut into 6 tetrahedra (14,155,776 cells), two ions (H+, Na+),
 inflow u = (-8, 0, 0), IMF (0, 0, -0.5), dipole at (0, 0, 0.2), wall at r = 1; seeded synthetic
 state (mpcns_uns_b200/workloads.py).  One step = the reference's Solver::step hot path:
-CFL step, two stages of primitives + limited gradients + Rusanov fluxes for both ions + ideal
-UCT EMF + CT, floors, SSP-RK2 average, all on the device.  Metric: cell-updates/s
+CFL step, half-step exact gyration of the ions, two stages of primitives + cell current + limited
+gradients + Rusanov fluxes for both ions + J x B force + ideal UCT EMF + CT, floors, SSP-RK2
+average, closing half-step gyration, all on the device (--no-sources: without the J x B force
+and the gyration).  Metric: cell-updates/s
 (cells x species x 2 stages per step).  Inputs exceed L2 (126 MB) many times over, so no
 flush is needed between steps.
 
@@ -60,10 +62,24 @@ def mesh_counts(h):
                 e2f=len(h["e2f_idx"]), ec=len(h["ec_cell"]), f2c=len(h["f2c_idx"]))
 
 
-def algorithmic_bytes(k, c, nsp, group, precision="fp64"):
+def algorithmic_bytes(k, c, nsp, group, precision="fp64", sources=False):
     """Compulsory bytes of one launch of kernel class k: every array the pass needs, counted once
     (perfect reuse within the pass); values 8 bytes (FP64) or 4 (FP32 bulk of the mixed path; the
-    state U and the face fluxes Phi stay 8), indices 4, signs / flags 1."""
+    state U and the face fluxes Phi stay 8), indices 4, signs / flags 1.  With the two-ion sources,
+    `prepare` includes the cell-current pass and `update` reads the J x B inputs; `gyrate` reads and
+    rewrites both ions' state."""
+    base = _algorithmic_bytes(k, c, nsp, group, precision)
+    if not sources:
+        return base
+    nc, nf = c["nc"], c["nf"]
+    if precision == "mixed":
+        extra = {"prepare": 52 * nc + 24 * nf, "update": 64 * nc, "gyrate": 144 * nc + 16 * nc + nc}
+    else:
+        extra = {"prepare": 64 * nc + c["c2f"] * 5 + 36 * nf, "update": (2 + 3 + 3) * 8 * nc, "gyrate": 144 * nc + 24 * nc + nc}
+    return base + extra.get(k, 0.0)
+
+
+def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
     nc, nf, ne = c["nc"], c["nf"], c["ne"]
     if precision == "mixed":
         g, e2f, f2e, ec = group, c["e2f"], c["f2e"], c["ec"]
@@ -167,7 +183,7 @@ def make_workload(args):
     if args.config == "box":
         wl = workloads.box(args.ncube or 16)
     else:
-        wl = workloads.shell(args.ncube or 64, args.nr or 96, r_in=1.0, r_out=6.0)
+        wl = workloads.shell(args.ncube or 64, args.nr or 96, r_in=1.0, r_out=6.0, sources=not args.no_sources)
     log(f"[bench] workload {wl.name}: {wl.mesh.n_cells} cells, {wl.mesh.n_faces} faces, {wl.mesh.n_edges} edges "
         f"(setup {time.time() - t:.1f}s)")
     return wl
@@ -179,7 +195,7 @@ def cpu_sample(args):
     from mpcns_uns_b200 import workloads
     if args.config == "box":
         return workloads.box(12)
-    return workloads.shell(16, 24, r_in=1.0, r_out=6.0)
+    return workloads.shell(16, 24, r_in=1.0, r_out=6.0, sources=not args.no_sources)
 
 
 def time_reference(wl, steps, warmup):
@@ -199,6 +215,7 @@ def time_reference(wl, steps, warmup):
     for s in range(wl.n_species):
         p.mass[s] = wl.mass[s]
         p.fs[s][:] = list(wl.fs[s])
+    p.lorentz, p.induce_coeff, p.inver_MA2 = int(wl.lorentz), wl.induce_coeff, wl.inver_MA2
     U = [np.array(u) for u in wl.U]
     Phi = np.array(wl.Phi)
     Badd = r.cell_vector(wl.PhiAdd)
@@ -341,6 +358,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--no-gmres", action="store_true")
+    ap.add_argument("--no-sources", action="store_true", help="leave out the two-ion J x B force and gyration")
     ap.add_argument("--gmres-ncube", type=int, default=48)
     ap.add_argument("--gmres-nr", type=int, default=96)
     ap.add_argument("--gmres-max-it", type=int, default=300)
@@ -391,7 +409,7 @@ def main():
 
     def new_state(precision):
         p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl,
-                            precision=precision)
+                            precision=precision, lorentz=wl.lorentz, induce_coeff=wl.induce_coeff, inver_MA2=wl.inver_MA2)
         st = gpu.ResidentState(dm, p)
         st.set(wl.U, wl.Phi, wl.PhiAdd)
         return st
@@ -425,9 +443,9 @@ def main():
             raise RuntimeError("state became invalid")
         kern = max(prof, key=lambda k: prof[k][0])
         k_ms, k_n = prof[kern]
-        bl = algorithmic_bytes(kern, counts, wl.n_species, group, precision)
+        bl = algorithmic_bytes(kern, counts, wl.n_species, group, precision, wl.lorentz)
         breakdown = {k: {"ms_per_step": v[0] / args.steps, "launches": v[1],
-                         "GBps": algorithmic_bytes(k, counts, wl.n_species, group, precision) / (v[0] / v[1] / 1e3) / 1e9}
+                         "GBps": algorithmic_bytes(k, counts, wl.n_species, group, precision, wl.lorentz) / (v[0] / v[1] / 1e3) / 1e9}
                      for k, v in prof.items() if v[1]}
         return dict(ms=ms, value=cu_per_step * args.steps * world / (ms / 1e3), launches=launches, kernel=kern,
                     bytes_launch=bl, achieved=bl / (k_ms / k_n / 1e3) / 1e9, kernels=breakdown)
@@ -527,7 +545,8 @@ def main():
                           "n_species": wl.n_species, "global_cells": h.n_cells * world,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                           "dt": "CFL 0.4 on device", "l2": "inputs > L2 (no flush needed)",
-                          "precision": "mixed: FP32 reconstruction/limiter/flux/EMF, FP64 state/Phi/CT"},
+                          "precision": "mixed: FP32 reconstruction/limiter/flux/EMF, FP64 state/Phi/CT",
+                          "sources": "J x B force + Strang-split exact gyration" if wl.lorentz else "none"},
                "gpu_launches": rmx["launches"],
                "roofline": {"bound": "hbm", "kernel": rmx["kernel"], "achieved": rmx["achieved"], "peak": peak, "unit": "GB/s",
                             "frac": rmx["achieved"] / peak, "peak_kind": peak_kind,

@@ -493,48 +493,10 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, const
     for (int q = 0; q < 5; ++q) Fs[q * nf + f] = Fl[q] * nf4.w;
 }
 
-// mhd::cell_current (Common/induction/Current.cpp:9-31) of the induced cell field in FP32:
-// J_c = (1/V) sum_f s A_f x 1/2 (b_c + b_nb), b_c alone on faces with one cell
-__global__ void __launch_bounds__(128) k_mx_current(MV m, const float4 *__restrict__ bi, float4 *__restrict__ J)
-{
-    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
-    if (c >= m.no_cells)
-    {
-        J[c] = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
-    const int32_t ff[4] = {fi.x, fi.y, fi.z, fi.w};
-    const float3 bc = f3(bi[c]);
-    float3 sum = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-    {
-        const int32_t f = ff[j];
-        const int32_t L = m.face_L[f], R = m.face_R[f];
-        const int32_t o = L == c ? R : L;
-        float3 bf = bc;
-        if (o >= 0)
-        {
-            const float3 bo = f3(bi[o]);
-            bf = make_float3(0.5f * (bc.x + bo.x), 0.5f * (bc.y + bo.y), 0.5f * (bc.z + bo.z));
-        }
-        const float4 nf4 = m.fn[f];
-        const float sa = static_cast<float>(m.c2f_sgn[4 * (int64_t)c + j]) * nf4.w;
-        const float3 cr = fcross(make_float3(sa * nf4.x, sa * nf4.y, sa * nf4.z), bf);
-        sum.x += cr.x;
-        sum.y += cr.y;
-        sum.z += cr.z;
-    }
-    const float iv = m.vol_inv[c];
-    J[c] = make_float4(sum.x * iv, sum.y * iv, sum.z * iv, 0.f);
-}
-
 // rhs gathered from the face fluxes, U (FP64) += dt rhs, floors, SSP-RK2 average in stage 2
 __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, const float *__restrict__ F, const double *__restrict__ Ub,
                                                    double *__restrict__ Uo, const double *__restrict__ dtp, int stage2,
-                                                   const float4 *__restrict__ W, const float4 *__restrict__ J, const float4 *__restrict__ bt)
+                                                   const float4 *__restrict__ W, const float4 *__restrict__ G, const float4 *__restrict__ bt)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y, s = s0 + g;
@@ -563,14 +525,28 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, con
         for (int q = 0; q < 5; ++q) u[q] += dtv * r[q];
         if (p.src_on)
         {
-            // J x B force of mercury::add_sources_n (MercurySources.cpp:29-47) in FP32, added to the FP64 update
-            const float4 wH = W[2 * (int64_t)c], wN = W[2 * ((int64_t)n + c)], ws4 = W[2 * ((int64_t)s * n + c)];
-            const float nH = fmaxf(wH.x, 0.f) / p.mass[0] * p.M_ref, nN = fmaxf(wN.x, 0.f) / p.mass[1] * p.M_ref;
-            const float ne = nH + nN, ne_eff = sqrtf(ne * ne + p.ne_floor * p.ne_floor);
-            const float wsp = (s == 0 ? nH : nN) / ne_eff;
-            const float3 Sv = fcross(f3(J[c]), f3(bt[c]));
-            const float k = p.inver_MA2 * wsp;
-            const float Sx = k * Sv.x, Sy = k * Sv.y, Sz = k * Sv.z;
+            // J x B force of mercury::add_sources_n (MercurySources.cpp:29-47) in FP32, with the work of the
+            // mid-point velocity, added to the FP64 update.  J_c = (1/V) sum_f s_f G_f (the face terms of
+            // k_mx_face_cand, same faces as the flux gather), S = inver_MA2 n_s / n_e,eff (J x B_tot).
+            float3 Jc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const float4 g = G[ff[j]];
+                const float sj = sv[j] < 0.0 ? 1.f : -1.f; // +1 where the canonical normal points out of c
+                Jc.x += sj * g.x;
+                Jc.y += sj * g.y;
+                Jc.z += sj * g.z;
+            }
+            const float iv = m.vol_inv[c];
+            Jc = make_float3(iv * Jc.x, iv * Jc.y, iv * Jc.z);
+            const float4 ws4 = W[2 * ((int64_t)s * n + c)];
+            const float nH = fmaxf(W[2 * (int64_t)c].x, 0.f) / p.mass[0] * p.M_ref;
+            const float nN = fmaxf(W[2 * (n + c)].x, 0.f) / p.mass[1] * p.M_ref;
+            const float ne = nH + nN;
+            const float k = p.inver_MA2 * (s == 0 ? nH : nN) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
+            const float3 jb = fcross(Jc, f3(bt[c]));
+            const float Sx = k * jb.x, Sy = k * jb.y, Sz = k * jb.z;
             const float rho = fmaxf(ws4.x, 0.f);
             const double dt = *dtp;
             const float work = ws4.y * Sx + ws4.z * Sy + ws4.w * Sz +
@@ -599,9 +575,12 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, con
 }
 
 // face EMF candidates E_f = -n x F_f (IdealEMF.cpp:32-55), 3 per face (structure of arrays)
+// With G: also the face term of the cell current, G_f = A_f x b_f, b_f = (b_L + b_R)/2 or the one
+// cell's b (mhd::cell_current, Common/induction/Current.cpp:9-31); cell c sums +-G over its faces.
 __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__restrict__ up, const float4 *__restrict__ bt,
                                                       const float4 *__restrict__ bi, const double *__restrict__ phi,
-                                                      const double *__restrict__ phi_add, float *__restrict__ Ef)
+                                                      const double *__restrict__ phi_add, float *__restrict__ Ef,
+                                                      float4 *__restrict__ G)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf) return;
@@ -626,6 +605,13 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
     }
     else
         F = flux(L >= 0 ? L : R);
+    if (G)
+    {
+        const float3 bL = L >= 0 ? f3(bi[L]) : f3(bi[R]), bR = R >= 0 ? f3(bi[R]) : bL;
+        const float3 bf = L >= 0 && R >= 0 ? make_float3(0.5f * (bL.x + bR.x), 0.5f * (bL.y + bR.y), 0.5f * (bL.z + bR.z)) : bL;
+        const float3 g = fcross(make_float3(nf4.w * n.x, nf4.w * n.y, nf4.w * n.z), bf);
+        G[f] = make_float4(g.x, g.y, g.z, 0.f);
+    }
     const float3 E = fcross(n, F);
     Ef[f] = -E.x;
     Ef[nf + f] = -E.y;
@@ -787,7 +773,7 @@ void mixed_setup(MhdState *st)
     int32_t nnz_e2f = 0;
     MHD_CUDA(cudaMemcpy(&nnz_e2f, m.e2f_ptr + m.ne, sizeof(int32_t), cudaMemcpyDeviceToHost));
     t.wd.alloc(12 * nc); t.dx.alloc(12 * nc); t.inv.alloc(6 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
-    if (st->src.on) st->J32.alloc(nc);
+    if (st->src.on) st->g32.alloc(nf);
     t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
     t.eth.alloc(ne); t.ee1.alloc(ne); t.ee2.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
     if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.wd.p, t.dx.p, t.inv.p, t.recon.p, t.vol_inv.p);
@@ -826,12 +812,6 @@ void mixed_prepare(MhdState *st, const double *Us, const double *phis, bool cfl,
     k_mx_prepare<<<gc, 128, 0, s>>>(m, p, Us, phis, st->badd32.p, W4, st->up32.p, st->bt32.p, st->bi32.p);
     MHD_LAUNCH_CHECK();
     ++st->launches;
-    if (st->src.on) // J of the induced field (Solver.cpp:123)
-    {
-        k_mx_current<<<gc, 128, 0, s>>>(m, st->bi32.p, st->J32.p);
-        MHD_LAUNCH_CHECK();
-        ++st->launches;
-    }
     P.end(KP_PREPARE, s);
     if (cfl)
     {
@@ -858,6 +838,13 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     if (!m.nc) return;
     float4 *W4 = reinterpret_cast<float4 *>(st->W32.p);
     mixed_prepare(st, Us, phis, cfl, dt_max);
+    // face EMF candidates first: with the J x B force on, this pass also leaves the face terms of the
+    // cell current that the update gathers
+    P.begin(KP_FACE_CAND, s);
+    k_mx_face_cand<<<gf, 128, 0, s>>>(m, st->up32.p, st->bt32.p, st->bi32.p, phis, st->phi_add.p, st->Ef32.p,
+                                      st->src.on ? st->g32.p : nullptr);
+    MHD_LAUNCH_CHECK();
+    P.end(KP_FACE_CAND, s);
     for (int s0 = 0; s0 < st->nsp; s0 += st->group)
     {
         const int ng = std::min(st->group, st->nsp - s0);
@@ -870,7 +857,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         MHD_LAUNCH_CHECK();
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
-        k_mx_update<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->J32.p, st->bt32.p);
+        k_mx_update<<<dim3(gc, ng), 128, 0, s>>>(m, p, s0, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p);
         MHD_LAUNCH_CHECK();
         P.end(KP_UPDATE, s);
         st->launches += 3;
@@ -878,10 +865,6 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     const float3 Einf = make_float3(static_cast<float>(-(st->prm.u_inf[1] * st->prm.B_imf[2] - st->prm.u_inf[2] * st->prm.B_imf[1])),
                                     static_cast<float>(-(st->prm.u_inf[2] * st->prm.B_imf[0] - st->prm.u_inf[0] * st->prm.B_imf[2])),
                                     static_cast<float>(-(st->prm.u_inf[0] * st->prm.B_imf[1] - st->prm.u_inf[1] * st->prm.B_imf[0])));
-    P.begin(KP_FACE_CAND, s);
-    k_mx_face_cand<<<gf, 128, 0, s>>>(m, st->up32.p, st->bt32.p, st->bi32.p, phis, st->phi_add.p, st->Ef32.p);
-    MHD_LAUNCH_CHECK();
-    P.end(KP_FACE_CAND, s);
     P.begin(KP_EDGE_EMF, s);
     k_mx_edge<<<ge, 128, 0, s>>>(m, st->Ef32.p, st->up32.p, phis, static_cast<float>(st->prm.cuct), Einf, st->E32.p);
     MHD_LAUNCH_CHECK();

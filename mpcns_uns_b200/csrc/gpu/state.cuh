@@ -9,9 +9,9 @@
 namespace mhd
 {
 // Kernel classes of the step, timed with CUDA events on the handle's stream when profiling is on.
-enum StepKernel { KP_PREPARE = 0, KP_CFL, KP_GRAD, KP_FLUX, KP_UPDATE, KP_FACE_CAND, KP_EDGE_EMF, KP_CT, KP_COUNT };
-static const char *const kStepKernelNames[KP_COUNT] = {"prepare", "cfl", "limited_gradients", "face_flux",
-                                                        "update",  "face_candidate", "edge_emf", "ct"};
+enum StepKernel { KP_PREPARE = 0, KP_CFL, KP_GRAD, KP_FLUX, KP_UPDATE, KP_FACE_CAND, KP_EDGE_EMF, KP_CT, KP_GYRATE, KP_COUNT };
+static const char *const kStepKernelNames[KP_COUNT] = {"prepare", "cfl",            "limited_gradients", "face_flux", "update",
+                                                        "face_candidate", "edge_emf", "ct",                "gyrate"};
 
 using Profiler = EventProfiler<KP_COUNT>;
 
@@ -42,7 +42,7 @@ struct MhdState
     mhd::DBuf<double> U0, U1, W, grad, F, phi0, phi1, phi_add, badd, bind, btot, up, Ef, E, mass, stage;
     mhd::SrcParams src;     // two-ion J x B force and gyration (off unless params.lorentz)
     mhd::DBuf<double> J;    // cell current of the induced field (3 per cell) when the J x B force is on
-    mhd::DBuf<float4> J32;  // the same for the mixed-precision stage
+    mhd::DBuf<float4> g32;  // mixed precision: face terms A_f x b_f of the cell current (per face)
     mhd::DBuf<double> scal; // [0] dt
     mhd::DBuf<unsigned long long> dt_bits;
     mhd::DBuf<int> flag;

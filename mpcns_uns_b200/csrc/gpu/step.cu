@@ -593,24 +593,38 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
             if (split)
             {
                 mixed_prepare(st, st->U0.p, st->phi0.p, cfl, dt_max);
+                st->prof.begin(KP_GYRATE, s);
                 launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
+                st->prof.end(KP_GYRATE, s);
                 st->launches += m.no_cells ? 1 : 0;
             }
             mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max);
             mixed_stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
-            if (split) launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
+            if (split)
+            {
+                st->prof.begin(KP_GYRATE, s);
+                launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
+                st->prof.end(KP_GYRATE, s);
+            }
         }
         else
         {
             if (split)
             {
                 prepare_cfl(st, st->U0.p, st->phi0.p, cfl, dt_max);
+                st->prof.begin(KP_GYRATE, s);
                 launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
+                st->prof.end(KP_GYRATE, s);
                 st->launches += m.no_cells ? 1 : 0;
             }
             stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max);
             stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
-            if (split) launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
+            if (split)
+            {
+                st->prof.begin(KP_GYRATE, s);
+                launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
+                st->prof.end(KP_GYRATE, s);
+            }
         }
         if (split && m.no_cells) ++st->launches;
         if (dt_used) read_dt(st, dt_used);

@@ -13,7 +13,8 @@ box comes from the splitmix64 stream of the native mesh builder.
              two ions (H+, Na+ of mass 23) upstream u = (-8, 0, 0), p = 0.05; Na+ density
              1e-3 * lognormal(0, 0.5) * exp(-(r - 1)/0.2); IMF (0, 0, -0.5) and a dipole of
              moment 1 at (0, 0, 0.2) in the static background flux; wall at the inner surface,
-             far field outside.
+             far field outside.  sources=True adds the two-ion J x B force and the exact gyration
+             (inver_MA2 = 1, induce_coeff = 1 in these units).
 """
 from __future__ import annotations
 
@@ -79,6 +80,9 @@ class Workload:
     cfl: float = 0.4
     steps: int = 20
     extra: dict = field(default_factory=dict)
+    lorentz: bool = False          # two-ion J x B force (mercury::add_sources_n)
+    induce_coeff: float = 0.0      # > 0: exact gyration, Strang-split around the step (mercury::gyrate)
+    inver_MA2: float = 1.0
 
 
 def box(n=16, seed=0, jitter=0.15, tets=True):
@@ -120,7 +124,7 @@ def geometric_stretch(nr, r_in, r_out, first):
     return 0.5 * (lo + hi)
 
 
-def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0)):
+def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False):
     if stretch is None:
         # first layer as thick as the angular spacing at r_in
         stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
@@ -146,9 +150,11 @@ def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, mas
         U.append(to_cons(W, GAMMA).ravel())
     B_imf = (0.0, 0.0, -0.5)
     PhiAdd = background(m, B_imf, (0.0, 0.0, 1.0), (0.0, 0.0, 0.2))
+    two = n_species == 2
     return Workload(name=f"shell6x{ncube}x{ncube}x{nr}x6", mesh=m, n_species=n_species, gamma=GAMMA, U=U,
                     Phi=np.zeros(m.n_faces), PhiAdd=PhiAdd, fs=fs, mass=masses, u_inf=tuple(u_inf), B_imf=B_imf,
-                    cfl=0.4, steps=100, extra=dict(stretch=stretch))
+                    cfl=0.4, steps=100, extra=dict(stretch=stretch), lorentz=two and sources,
+                    induce_coeff=1.0 if two and sources else 0.0)
 
 
 def dipole_field(x, m=(0.0, 0.0, 1.0), c=(0.0, 0.0, 0.2), B_imf=(0.0, 0.0, -0.5)):
