@@ -215,14 +215,10 @@ __device__ __forceinline__ void rusanov32(const F5 &L, const F5 &R, float3 n, fl
     F[4] = 0.5f * (unL * (EL + L.p) + unR * (ER + R.p)) - 0.5f * s * (ER - EL);
 }
 
-// primitives (FP32), cell field fit, total field, charge-weighted velocity
-__global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const double *__restrict__ U, const double *__restrict__ phi,
-                                                     const float4 *__restrict__ badd, float4 *__restrict__ W, float4 *__restrict__ up,
-                                                     float4 *__restrict__ bt, float4 *__restrict__ bi)
+// per-cell primitives (FP32, 32 bytes per species) and the charge-weighted velocity u+ of cell c
+__device__ __forceinline__ void mx_prims(const MxParams &p, int64_t n, const double *__restrict__ U, float4 *__restrict__ W,
+                                         float4 *__restrict__ up, int32_t c, bool fluid)
 {
-    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc) return;
-    const int64_t n = m.nc;
     float ne = 0.f;
     for (int s = 0; s < p.nsp; ++s)
     {
@@ -236,6 +232,29 @@ __global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const doub
         Wc[1] = make_float4(static_cast<float>(pr), 0.f, 0.f, 0.f);
         ne += static_cast<float>(r) / p.mass[s] * p.M_ref;
     }
+    float u3[3] = {0.f, 0.f, 0.f};
+    if (fluid)
+        for (int s = 0; s < p.nsp; ++s)
+        {
+            // number density and velocity re-read from the primitives this thread has just written
+            const float4 wv = W[2 * ((int64_t)s * n + c)];
+            const float chi = ne > 1e-30f ? (wv.x / p.mass[s] * p.M_ref) / ne : (s == 0 ? 1.f : 0.f);
+            u3[0] += chi * wv.y;
+            u3[1] += chi * wv.z;
+            u3[2] += chi * wv.w;
+        }
+    up[c] = make_float4(u3[0], u3[1], u3[2], 0.f);
+}
+
+// primitives (FP32), cell field fit, total field, charge-weighted velocity
+__global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const double *__restrict__ U, const double *__restrict__ phi,
+                                                     const float4 *__restrict__ badd, float4 *__restrict__ W, float4 *__restrict__ up,
+                                                     float4 *__restrict__ bt, float4 *__restrict__ bi)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    const int64_t n = m.nc;
+    mx_prims(p, n, U, W, up, c, m.material[c] == 0);
     const int4 fi = *reinterpret_cast<const int4 *>(m.c2f_idx + 4 * (int64_t)c);
     const float ph[4] = {static_cast<float>(phi[fi.x]), static_cast<float>(phi[fi.y]), static_cast<float>(phi[fi.z]),
                          static_cast<float>(phi[fi.w])};
@@ -247,18 +266,31 @@ __global__ void __launch_bounds__(128) k_mx_prepare(MV m, MxParams p, const doub
     const float4 ba = badd[c];
     bi[c] = make_float4(b[0], b[1], b[2], 0.f);
     bt[c] = make_float4(b[0] + ba.x, b[1] + ba.y, b[2] + ba.z, 0.f);
-    float u3[3] = {0.f, 0.f, 0.f};
-    if (m.material[c] == 0)
-        for (int s = 0; s < p.nsp; ++s)
-        {
-            // number density and velocity re-read from the primitives this thread has just written
-            const float4 wv = W[2 * ((int64_t)s * n + c)];
-            const float chi = ne > 1e-30f ? (wv.x / p.mass[s] * p.M_ref) / ne : (s == 0 ? 1.f : 0.f);
-            u3[0] += chi * wv.y;
-            u3[1] += chi * wv.z;
-            u3[2] += chi * wv.w;
-        }
-    up[c] = make_float4(u3[0], u3[1], u3[2], 0.f);
+}
+
+// The opening half-step gyration (mercury::gyrate, FP64 on the FP64 state, FP32 total field) with the
+// primitives and u+ of the cells it turns renewed, so that stage 1 starts prepared (B_ind and B_tot
+// depend on Phi alone)
+__global__ void __launch_bounds__(128) k_mx_gyrate(MV m, MxParams p, SrcParams sp, const float4 *__restrict__ bt,
+                                                   const double *__restrict__ dtp, double scale, double *__restrict__ U,
+                                                   float4 *__restrict__ W, float4 *__restrict__ up)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.no_cells || m.material[c] == 1) return;
+    const int64_t n = m.nc;
+    double uh[5], un[5];
+    for (int q = 0; q < 5; ++q)
+    {
+        uh[q] = U[q * n + c];
+        un[q] = U[(5 + q) * n + c];
+    }
+    gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), scale * *dtp, uh, un);
+    for (int q = 1; q < 5; ++q)
+    {
+        U[q * n + c] = uh[q];
+        U[(5 + q) * n + c] = un[q];
+    }
+    mx_prims(p, n, U, W, up, c, m.material[c] == 0);
 }
 
 __global__ void __launch_bounds__(128) k_mx_cfl(MV m, MxParams p, float cfl, float inver_MA2, float rho_floor_dt,
@@ -826,7 +858,18 @@ void mixed_prepare(MhdState *st, const double *Us, const double *phis, bool cfl,
     }
 }
 
-void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max)
+void mixed_gyrate_open(MhdState *st)
+{
+    const MV m = make_view(st->mesh->v, st->mt);
+    if (!m.no_cells) return;
+    k_mx_gyrate<<<grid_for(m.no_cells, 128), 128, 0, st->mesh->stream>>>(m, mx_params(st), st->src, st->bt32.p, st->scal.p, 0.5,
+                                                                            st->U0.p, reinterpret_cast<float4 *>(st->W32.p), st->up32.p);
+    MHD_LAUNCH_CHECK();
+    ++st->launches;
+}
+
+void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
+                 bool prepared)
 {
     MhdMesh *mesh = st->mesh;
     const MeshView &mv = mesh->v;
@@ -837,7 +880,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     const int gc = grid_for(m.nc, 128), gf = grid_for(m.nf, 128), ge = grid_for(m.ne, 128);
     if (!m.nc) return;
     float4 *W4 = reinterpret_cast<float4 *>(st->W32.p);
-    mixed_prepare(st, Us, phis, cfl, dt_max);
+    if (!prepared) mixed_prepare(st, Us, phis, cfl, dt_max);
     // face EMF candidates first: with the J x B force on, this pass also leaves the face terms of the
     // cell current that the update gathers
     P.begin(KP_FACE_CAND, s);

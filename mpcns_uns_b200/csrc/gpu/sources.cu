@@ -13,7 +13,7 @@ namespace
 // angle from dt_val, or scale * (*dtp) when dtp is set
 __global__ void __launch_bounds__(128) k_gyrate(MeshView m, SrcParams p, const double *__restrict__ B3, const float4 *__restrict__ B4,
                                                  const double *__restrict__ dtp, double scale, double dt_val, SField<double> UH,
-                                                 SField<double> UN)
+                                                 SField<double> UN, Reprepare rp)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.no_cells || m.material[c] == 1) return;
@@ -30,6 +30,12 @@ __global__ void __launch_bounds__(128) k_gyrate(MeshView m, SrcParams p, const d
     {
         UH(0, c, q) = uh[q];
         UN(0, c, q) = un[q];
+    }
+    if (rp.on)
+    {
+        double u[3];
+        prepare_prims(rp.fp, rp.mass, rp.M_ref, rp.U, rp.W, c, true, u);
+        st3(rp.up, c, mk(u[0], u[1], u[2]));
     }
 }
 
@@ -66,12 +72,12 @@ SrcParams src_params(const MhdStepParams &q)
 }
 
 void launch_gyrate(const MeshView &m, const SrcParams &p, const double *B3, const float4 *B4, const double *dtp, double scale,
-                   double *U, cudaStream_t s)
+                   double *U, cudaStream_t s, const Reprepare &rp)
 {
     if (!m.no_cells || !p.on || !(p.induce > 0)) return;
     const int64_t nc = m.nc;
     k_gyrate<<<grid_for(m.no_cells, 128), 128, 0, s>>>(m, p, B3, B4, dtp, scale, 0.0, SField<double>{U, 0, 1, nc},
-                                                        SField<double>{U + 5 * nc, 0, 1, nc});
+                                                        SField<double>{U + 5 * nc, 0, 1, nc}, rp);
     MHD_LAUNCH_CHECK();
 }
 } // namespace mhd
@@ -105,7 +111,7 @@ int mhd_gpu_gyrate(MhdMesh *mesh, const MhdStepParams *params, const double *B, 
         const SrcParams p = src_params(*params);
         if (!m.no_cells || !p.on || !(p.induce > 0)) return; // gyrate_n returns at once (Gyration.cpp)
         k_gyrate<<<grid_for(m.no_cells, 128), 128, 0, mesh->stream>>>(m, p, B, nullptr, nullptr, 1.0, dt, SField<double>{UH, 0, 5, 1},
-                                                                       SField<double>{UNa, 0, 5, 1});
+                                                                       SField<double>{UNa, 0, 5, 1}, Reprepare{});
         MHD_LAUNCH_CHECK();
     });
 }

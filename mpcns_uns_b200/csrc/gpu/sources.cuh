@@ -97,6 +97,43 @@ __device__ __forceinline__ void gyrate_cell(const SrcParams &p, V3 b, double dt,
     un[4] += 0.5 * rho * (dot(uN2, uN2) - dot(uN, uN));
 }
 
+// Per-cell part of Solver::prepare (Solver.cpp:101-118): primitives of every species and the
+// charge-weighted ion velocity u+ (mhd::Scales::numinfo generalised to n species; the number
+// densities are recomputed from the primitives just written)
+__device__ __forceinline__ void prepare_prims(const FluidParams &p, const double *__restrict__ mass, double M_ref, SField<const double> U,
+                                              SField<double> W, int32_t c, bool fluid, double *u)
+{
+    double ne = 0;
+    for (int s = 0; s < p.nsp; ++s)
+    {
+        const Prim5 w = to_prim(U(s, c, 0), U(s, c, 1), U(s, c, 2), U(s, c, 3), U(s, c, 4), p.gamma, p.rho_floor, p.p_floor);
+        W(s, c, 0) = w.rho; W(s, c, 1) = w.u; W(s, c, 2) = w.v; W(s, c, 3) = w.w; W(s, c, 4) = w.p;
+        ne += dmax(w.rho, 0.0) / mass[s] * M_ref;
+    }
+    u[0] = u[1] = u[2] = 0;
+    if (fluid)
+        for (int s = 0; s < p.nsp; ++s)
+        {
+            const double ns = dmax(W(s, c, 0), 0.0) / mass[s] * M_ref;
+            const double chi = ne > 1e-300 ? ns / ne : (s == 0 ? 1.0 : 0.0);
+            for (int a = 0; a < 3; ++a) u[a] += chi * W(s, c, 1 + a);
+        }
+}
+
+// After the opening half-step gyration the next prepare would only renew what the gyration changed:
+// the primitives and u+ (B_ind, B_tot and J depend on Phi alone).  With on, the gyration kernel writes
+// them for the cells it turns, so that stage 1 needs no prepare pass.
+struct Reprepare
+{
+    int on = 0;
+    FluidParams fp;
+    const double *mass = nullptr;
+    double M_ref = 1;
+    SField<const double> U;
+    SField<double> W;
+    double *up = nullptr;
+};
+
 // the source parameters of a step's parameters (species 0 and 1 are the model's H+ and Na+)
 SrcParams src_params(const MhdStepParams &q);
 
@@ -105,7 +142,7 @@ SrcParams src_params(const MhdStepParams &q);
 // species, [(s*5 + m)*nc + c]); the field is B3 (3 doubles per cell) or, if null, B4 (float4 per cell);
 // the angle uses scale * (*dtp).
 void launch_gyrate(const MeshView &m, const SrcParams &p, const double *B3, const float4 *B4, const double *dtp, double scale,
-                   double *U, cudaStream_t s);
+                   double *U, cudaStream_t s, const Reprepare &rp = Reprepare{});
 // mhd::cell_current (induction.cu)
 void launch_cell_current(const MeshView &m, const double *B, double *J, cudaStream_t s);
 } // namespace mhd

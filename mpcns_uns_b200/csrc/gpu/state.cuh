@@ -62,7 +62,10 @@ struct MhdState
 namespace mhd
 {
 void mixed_setup(MhdState *st);
-void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max);
+void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
+                 bool prepared = false);
+// the opening half-step gyration of U0, renewing its primitives and u+ (stage 1 then runs prepared)
+void mixed_gyrate_open(MhdState *st);
 void mixed_badd(MhdState *st);
 // primitives, cell fields (and with cfl the device CFL step) of (Us, phis) in mixed precision
 void mixed_prepare(MhdState *st, const double *Us, const double *phis, bool cfl, double dt_max);

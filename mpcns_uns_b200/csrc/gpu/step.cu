@@ -44,26 +44,11 @@ __global__ void __launch_bounds__(128) k_prepare(MeshView m, FluidParams p, cons
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
-    // charge-weighted ion velocity: mhd::Scales::numinfo (Common/physics/Scales.cpp:50-62) generalised to n
-    // species; the number densities are recomputed from the primitives this thread has just written
-    double ne = 0;
-    for (int s = 0; s < p.nsp; ++s)
-    {
-        const Prim5 w = to_prim(U(s, c, 0), U(s, c, 1), U(s, c, 2), U(s, c, 3), U(s, c, 4), p.gamma, p.rho_floor, p.p_floor);
-        W(s, c, 0) = w.rho; W(s, c, 1) = w.u; W(s, c, 2) = w.v; W(s, c, 3) = w.w; W(s, c, 4) = w.p;
-        ne += dmax(w.rho, 0.0) / mass[s] * M_ref;
-    }
+    double u[3];
+    prepare_prims(p, mass, M_ref, U, W, c, m.material[c] == 0, u);
     const V3 b = cell_vector(m, phi, c);
     st3(Bind, c, b);
     st3(Btot, c, mk(b.x + Badd[3 * (int64_t)c], b.y + Badd[3 * (int64_t)c + 1], b.z + Badd[3 * (int64_t)c + 2]));
-    double u[3] = {0, 0, 0};
-    if (m.material[c] == 0)
-        for (int s = 0; s < p.nsp; ++s)
-        {
-            const double ns = dmax(W(s, c, 0), 0.0) / mass[s] * M_ref;
-            const double chi = ne > 1e-300 ? ns / ne : (s == 0 ? 1.0 : 0.0);
-            for (int a = 0; a < 3; ++a) u[a] += chi * W(s, c, 1 + a);
-        }
     st3(up, c, mk(u[0], u[1], u[2]));
 }
 
@@ -594,11 +579,10 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
             {
                 mixed_prepare(st, st->U0.p, st->phi0.p, cfl, dt_max);
                 st->prof.begin(KP_GYRATE, s);
-                launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
+                mixed_gyrate_open(st);
                 st->prof.end(KP_GYRATE, s);
-                st->launches += m.no_cells ? 1 : 0;
             }
-            mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max);
+            mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max, split);
             mixed_stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
             if (split)
             {
@@ -612,12 +596,21 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
             if (split)
             {
                 prepare_cfl(st, st->U0.p, st->phi0.p, cfl, dt_max);
+                // the gyration renews the primitives and u+ of the cells it turns: stage 1 starts prepared
+                Reprepare rp;
+                rp.on = 1;
+                rp.fp = st->fp;
+                rp.mass = st->mass.p;
+                rp.M_ref = st->prm.M_ref;
+                rp.U = soa_cstate(st->U0.p, m.nc);
+                rp.W = soa_state(st->W.p, m.nc);
+                rp.up = st->up.p;
                 st->prof.begin(KP_GYRATE, s);
-                launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
+                launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s, rp);
                 st->prof.end(KP_GYRATE, s);
                 st->launches += m.no_cells ? 1 : 0;
             }
-            stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max);
+            stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max, split);
             stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
             if (split)
             {
