@@ -120,7 +120,7 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that one ncu capture measured
 # on the 6 x 32 x 32 x 48 x 6 shell of the same construction, with the entity count it scales with;
 # the bench line reports it scaled to its own workload (the traffic grows in proportion to that count).
-NCU_TRAFFIC = {("edge_emf", "mixed"): (595.06e6, "ne", 2082912)}
+NCU_TRAFFIC = {("edge_emf", "mixed"): (595.86e6, "ne", 2082912)}
 
 
 def ncu_traffic(kernel, precision, counts):
