@@ -48,7 +48,8 @@ struct MhdState
     mhd::DBuf<int> flag;
     // mixed precision: FP32 bulk arrays (the state U and the face fluxes Phi stay FP64)
     mhd::MixedTables mt;
-    mhd::DBuf<float> W32, grad32, F32, Ef32, E32;
+    mhd::DBuf<float> W32, grad32, F32, E32;
+    mhd::DBuf<float4> Ef32; // per face: EMF candidate E_f (3) and Phi_ind / |A|
     mhd::DBuf<float4> up32, bt32, bi32, badd32;
     double *pinned = nullptr;
     int64_t launches = 0; // kernels launched by the step since creation
