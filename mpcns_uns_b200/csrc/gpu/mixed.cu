@@ -527,10 +527,9 @@ __device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int 
 __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, int s0, int g, int32_t c, const float *__restrict__ F,
                                               const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
                                               int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
-                                              const float4 *__restrict__ bt)
+                                              const float4 *__restrict__ bt, double *__restrict__ res)
 {
     const int s = s0 + g;
-    if (c >= m.nc) return;
     const int64_t n = m.nc, nf = m.nf;
     const double *ub = Ub + (int64_t)s * 5 * n;
     double *uo = Uo + (int64_t)s * 5 * n;
@@ -598,10 +597,10 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
     }
     if (stage2)
 #pragma unroll
-        for (int q = 0; q < 5; ++q) uo[q * n + c] = 0.5 * (uo[q * n + c] + u[q]);
+        for (int q = 0; q < 5; ++q) res[q] = 0.5 * (uo[q * n + c] + u[q]);
     else
 #pragma unroll
-        for (int q = 0; q < 5; ++q) uo[q * n + c] = u[q];
+        for (int q = 0; q < 5; ++q) res[q] = u[q];
 }
 
 // face EMF candidates E_f = -n x F_f (IdealEMF.cpp:32-55), 3 per face (structure of arrays)
@@ -617,7 +616,7 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
     const int64_t nf = m.nf;
     const float4 nf4 = m.fn[f];
     const float3 n = f3(nf4);
-    const float Bn = static_cast<float>((phi[f] + phi_add[f]) / static_cast<double>(nf4.w));
+    const float Bn = static_cast<float>(phi[f] + phi_add[f]) / nf4.w;
     const int32_t L = m.face_L[f], R = m.face_R[f];
     float3 F;
     auto flux = [&](int32_t c) {
@@ -645,7 +644,7 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
     const float3 E = fcross(n, F);
     // with Phi_ind / |A| of the face, which the edge pass needs for its dissipation term: one 16-byte
     // gather per (edge, face) there
-    Ef[f] = make_float4(-E.x, -E.y, -E.z, static_cast<float>(phi[f] / static_cast<double>(nf4.w)));
+    Ef[f] = make_float4(-E.x, -E.y, -E.z, static_cast<float>(phi[f]) / nf4.w);
 }
 
 // UCT edge EMF (IdealEMF.cpp:59-128) with the boundary edge values (Solver.cpp:162-167)
@@ -785,15 +784,27 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, int n
     mx_flux_one(m, p, s0, blockIdx.y, f, G, F);
 }
 
+// gyr: the closing half-step gyration of the Strang splitting (mercury::gyrate, FP64 on the averaged
+// state, with the total field of the stage-2 prepare) applied to the cell's two ions before they are
+// written, instead of in a pass of its own
 __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int ng, const float *__restrict__ F,
                                                    const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
                                                    int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
-                                                   const float4 *__restrict__ bt)
+                                                   const float4 *__restrict__ bt, SrcParams sp, int gyr)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
-#pragma unroll 1
-    for (int g = 0; g < ng; ++g) mx_update_one(m, p, s0, g, c, F, Ub, Uo, dtp, stage2, W, G, bt);
+    const int64_t n = m.nc;
+    double r0[5], r1[5];
+    mx_update_one(m, p, s0, 0, c, F, Ub, Uo, dtp, stage2, W, G, bt, r0);
+    if (ng > 1) mx_update_one(m, p, s0, 1, c, F, Ub, Uo, dtp, stage2, W, G, bt, r1);
+    if (gyr && ng == 2 && c < m.no_cells && m.material[c] != 1) gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), 0.5 * *dtp, r0, r1);
+    double *u0 = Uo + (int64_t)s0 * 5 * n;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) u0[q * n + c] = r0[q];
+    if (ng > 1)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) u0[(5 + q) * n + c] = r1[q];
 }
 
 MxParams mx_params(const MhdState *st)
@@ -898,7 +909,7 @@ void mixed_gyrate_open(MhdState *st)
 }
 
 void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
-                 bool prepared)
+                 bool prepared, bool gyrate_close)
 {
     MhdMesh *mesh = st->mesh;
     const MeshView &mv = mesh->v;
@@ -929,7 +940,8 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         MHD_LAUNCH_CHECK();
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
-        k_mx_update<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p);
+        k_mx_update<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
+                                       gyrate_close && s0 == 0 ? 1 : 0);
         MHD_LAUNCH_CHECK();
         P.end(KP_UPDATE, s);
         st->launches += 3;

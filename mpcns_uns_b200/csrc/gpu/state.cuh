@@ -63,8 +63,9 @@ struct MhdState
 namespace mhd
 {
 void mixed_setup(MhdState *st);
+// gyrate_close: stage 2 applies the closing half-step gyration in its update (two-ion sources on)
 void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
-                 bool prepared = false);
+                 bool prepared = false, bool gyrate_close = false);
 // the opening half-step gyration of U0, renewing its primitives and u+ (stage 1 then runs prepared)
 void mixed_gyrate_open(MhdState *st);
 void mixed_badd(MhdState *st);

@@ -583,13 +583,7 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
                 st->prof.end(KP_GYRATE, s);
             }
             mixed_stage(st, st->U0.p, st->phi0.p, st->U1.p, st->phi1.p, false, cfl && !split, dt_max, split);
-            mixed_stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max);
-            if (split)
-            {
-                st->prof.begin(KP_GYRATE, s);
-                launch_gyrate(m, st->src, nullptr, st->bt32.p, st->scal.p, 0.5, st->U0.p, s);
-                st->prof.end(KP_GYRATE, s);
-            }
+            mixed_stage(st, st->U1.p, st->phi1.p, st->U0.p, st->phi0.p, true, false, dt_max, false, split);
         }
         else
         {
@@ -619,7 +613,7 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
                 st->prof.end(KP_GYRATE, s);
             }
         }
-        if (split && m.no_cells) ++st->launches;
+        if (split && m.no_cells && !st->mixed) ++st->launches; // the FP64 closing gyration
         if (dt_used) read_dt(st, dt_used);
     });
 }
