@@ -226,6 +226,56 @@ int mhd_gpu_add_sources(MhdMesh *mesh, const MhdStepParams *params, int32_t spec
  * lorentz != 0 and induce_coeff > 0, as in the reference. */
 int mhd_gpu_gyrate(MhdMesh *mesh, const MhdStepParams *params, const double *B, double dt, double *UH, double *UNa);
 
+/* Explicit resistive EMF of the FP64 step: with m_edge (host, one value per edge: m_e = eta_e / star1_e)
+ * every stage adds m_e (d1^T star2 Phi)_e to the EMF of the owned edges after the ideal UCT EMF and the
+ * boundary edge values.  The term is the resistive part of ImplicitInduction::apply_F
+ * (Common/induction/ImplicitInduction.cpp:133-137, 182) evaluated explicitly; NULL switches it off. */
+int mhd_gpu_state_set_resistivity(MhdState *state, const double *m_edge);
+
+/* ------------------------------------------------------------------ differentiated explicit run
+ * Forward / backward (adjoint) / tangent Function of n_steps FP64 SSP-RK2 steps at a fixed dt (the
+ * state's parameters, no model sources, one or two species, tetrahedral mesh) with the explicit
+ * resistive EMF of the per-cell resistivity eta (m_e = mean of eta over the edge's cells / star1_e),
+ * for the functional J = sum over the marked cells of |B_tot|^2 V of the final state.  Parameters:
+ * eta (per cell) and the inflow velocity u_inf (every species' free-stream velocity and the inflow
+ * edge EMF -u_inf x B_imf); the face kinds and edge modes stay as built.  The run starts from the
+ * state's U and Phi at creation.  The reference has no adjoint: this interface is this library's own. */
+typedef struct MhdFnParams {
+    int32_t n_steps;          /* explicit steps of the run */
+    int32_t checkpoint_every; /* the forward run keeps the state every this many steps; the backward
+                                 sweep recomputes each segment from its checkpoint */
+    double dt;                /* fixed step */
+    int32_t uniform_flow;     /* 1: the initial flow moves with the free stream: every species' velocity in
+                                 every fluid cell is shifted by u_inf - (u_inf at creation), density and
+                                 pressure kept, so J depends on u_inf through the initial state too */
+    int32_t pad;
+} MhdFnParams;
+typedef struct MhdFn MhdFn;
+
+/* eta: per-cell resistivity (host, n_cells); mask: cells of the functional (host int8, n_cells) */
+int mhd_gpu_fn_create(MhdState *state, const MhdFnParams *params, const double *eta, const int8_t *mask, MhdFn **out);
+int mhd_gpu_fn_destroy(MhdFn *fn);
+/* new parameters (either may be NULL: unchanged); sets the state's free-stream velocities and u_inf */
+int mhd_gpu_fn_set_params(MhdFn *fn, const double *eta, const double *u_inf);
+/* copy the initial state back into the MhdState */
+int mhd_gpu_fn_reset(MhdFn *fn);
+/* J of the run; keeps the checkpoints and leaves the final state in the MhdState */
+int mhd_gpu_fn_forward(MhdFn *fn, double *J);
+/* dJ/deta (host, n_cells; may be NULL) and dJ/du_inf (3; may be NULL) by the adjoint sweep; needs a
+ * forward run with the current parameters */
+int mhd_gpu_fn_backward(MhdFn *fn, double *grad_eta, double *grad_u);
+/* tangent-linear run: J and its derivative along (d_eta, d_u) (either may be NULL: zero) */
+int mhd_gpu_fn_tangent(MhdFn *fn, const double *d_eta, const double *d_u, double *J, double *dJ);
+/* One stage as an operator, for dot-product checks.  Host arrays in the state's device layout
+ * (U: [(s*5 + m)*n_cells + c], Phi per face, E per edge).  The stage maps (U, Phi; eta, u_inf) to
+ * U~ = floors(U + dt rhs) and the edge EMF E.  _tangent: the derivatives of U~ and E along
+ * (dU, dPhi, d_eta, d_u).  _adjoint: given adjoints of U~ and E, the adjoints of U, Phi, eta (n_cells)
+ * and u_inf (3). */
+int mhd_gpu_fn_stage_tangent(MhdFn *fn, const double *U, const double *Phi, const double *dU, const double *dPhi, const double *d_eta,
+                             const double *d_u, double *dUt, double *dE);
+int mhd_gpu_fn_stage_adjoint(MhdFn *fn, const double *U, const double *Phi, const double *lUt, const double *lE, double *lU, double *lPhi,
+                             double *l_eta, double *l_u);
+
 /* Live per-kernel timing of the fused step (CUDA events recorded on the handle's stream around
  * every launch while enabled).  _read synchronises, returns per kernel class its name (32 chars
  * each), summed milliseconds and launch count, and restarts the accumulation. */

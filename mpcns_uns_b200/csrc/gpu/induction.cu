@@ -133,10 +133,13 @@ __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__re
 
 // EdgeEMF::begin (zero) + add_ideal_emf + the boundary edge values of Solver::rhs (Solver.cpp:150-167).
 // Wall and inflow edges are overwritten by the reference, so their UCT value is not evaluated.
+// With mres, the explicit resistive EMF m_e (d1^T star2 Phi)_e is added on every owned edge: the resistive
+// part of ImplicitInduction::apply_F (ImplicitInduction.cpp:133-137) with its sum m p0 + p1 + p2 (:182), the
+// faces of an edge in ascending order (the e2f rows), as the reference's face loop scatters them.
 template <int MAXV>
 __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                           const double *__restrict__ phi_ind, double cuct, V3 E_inf,
-                                                          double *__restrict__ E)
+                                                          const double *__restrict__ mres, double *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
@@ -151,6 +154,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const do
             double v;
             if (edge_uct<MAXV>(m, e, Ef, u, phi_ind, cuct, v)) val += v;
         }
+        if (mres) val += mres[e] * resistive_p0(m, phi_ind, e) + 0.0 + 0.0;
     }
     E[e] = val;
 }
@@ -164,11 +168,11 @@ void launch_face_candidate(const MeshView &m, const double *u, const double *Bt,
 }
 
 void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
-                            double *E, cudaStream_t s)
+                            double *E, cudaStream_t s, const double *mres)
 {
     if (!m.ne) return;
-    if (m.max_valence <= 8) k_edge_emf_assign<8><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, E);
-    else k_edge_emf_assign<kMaxValence><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, E);
+    if (m.max_valence <= 8) k_edge_emf_assign<8><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, E);
+    else k_edge_emf_assign<kMaxValence><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, E);
     MHD_LAUNCH_CHECK();
 }
 

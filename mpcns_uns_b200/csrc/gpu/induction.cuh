@@ -43,4 +43,17 @@ __device__ __forceinline__ V3 cell_vector(const MeshView &m, const double *__res
     return mk(I[0][0] * r[0] + I[0][1] * r[1] + I[0][2] * r[2], I[1][0] * r[0] + I[1][1] * r[1] + I[1][2] * r[2],
               I[2][0] * r[0] + I[2][1] * r[1] + I[2][2] * r[2]);
 }
+
+// (d1^T star2 phi)_e: the resistive current flux of ImplicitInduction::apply_F (ImplicitInduction.cpp:133-137)
+// at edge e, its faces in ascending order (e2f rows), each term sgn * (star2_f phi_f)
+__device__ __forceinline__ double resistive_p0(const MeshView &m, const double *__restrict__ phi, int32_t e)
+{
+    double p0 = 0.0;
+    for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k)
+    {
+        const int32_t f = m.e2f_idx[k];
+        p0 += m.e2f_sgn[k] * (m.star2[f] * phi[f]);
+    }
+    return p0;
+}
 } // namespace mhd

@@ -43,6 +43,8 @@ struct MhdState
     mhd::SrcParams src;     // two-ion J x B force and gyration (off unless params.lorentz)
     mhd::DBuf<double> J;    // cell current of the induced field (3 per cell) when the J x B force is on
     mhd::DBuf<float4> g32;  // mixed precision: face terms A_f x b_f of the cell current (per face)
+    mhd::DBuf<double> mres; // explicit resistive EMF: m_e = eta_e / star1_e per edge (empty: off)
+    int8_t *floor_flags = nullptr; // when set, the update records the floors it applied ([s*nc + c])
     mhd::DBuf<double> scal; // [0] dt
     mhd::DBuf<unsigned long long> dt_bits;
     mhd::DBuf<int> flag;
@@ -63,6 +65,10 @@ struct MhdState
 namespace mhd
 {
 void mixed_setup(MhdState *st);
+// one FP64 stage (Us, phis) -> (Uo, phio) at the step size in st->scal[0]; stage2 averages with Uo, phio in place
+void fp64_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2);
+// its first half alone: primitives, cell fields, u+ and limited gradients of (Us, phis) into st's buffers
+void fp64_prepare_grad(MhdState *st, const double *Us, const double *phis);
 // gyrate_close: stage 2 applies the closing half-step gyration in its update (two-ion sources on)
 void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
                  bool prepared = false, bool gyrate_close = false);

@@ -144,10 +144,11 @@ struct SrcView
 // fluid cells, Solver::enforce_floors (:171-191); stage 2 averages with U0 in place (Solver.cpp:505-506).
 // NF = 4: tetrahedral mesh, the four faces of the cell unrolled (all flux gathers in flight together);
 // NF = 0: any polyhedra.  One thread per (cell, species of the group = blockIdx.y).
+// fl (optional): which floor each owned fluid cell and species met, [s*nc + c]: 0 none, 1 density, 2 pressure.
 template <int NF>
 __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s0, int ng, const double *__restrict__ F,
                                                  SField<const double> Ub, SField<double> Uo, const double *__restrict__ dtp, int stage2,
-                                                 SrcView sv)
+                                                 SrcView sv, int8_t *__restrict__ fl)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     const int g = blockIdx.y;
@@ -202,9 +203,18 @@ __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s
             }
             for (int q = 0; q < 5; ++q) u[q] += dt * r[q];
             const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
-            if (!(u[0] >= p.rho_floor)) to_cons5(Prim5{p.rho_floor, 0, 0, 0, p.p_floor}, p.gamma, u);
+            int8_t which = 0;
+            if (!(u[0] >= p.rho_floor))
+            {
+                to_cons5(Prim5{p.rho_floor, 0, 0, 0, p.p_floor}, p.gamma, u);
+                which = 1;
+            }
             else if ((p.gamma - 1.0) * (u[4] - ke) < p.p_floor)
+            {
                 to_cons5(to_prim(u[0], u[1], u[2], u[3], u[4], p.gamma, p.rho_floor, p.p_floor), p.gamma, u);
+                which = 2;
+            }
+            if (fl) fl[(int64_t)s * m.nc + c] = which;
         }
         if (stage2)
             for (int q = 0; q < 5; ++q) Uo(s, c, q) = 0.5 * (Uo(s, c, q) + u[q]);
@@ -336,10 +346,10 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
             const dim3 grid(grid_for(m.nc, 128), ng);
             if (m.faces_per_cell == 4)
                 k_update<4><<<grid, 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
-                                                 stage2 ? 1 : 0, sv);
+                                                 stage2 ? 1 : 0, sv, st->floor_flags);
             else
                 k_update<0><<<grid, 128, 0, s>>>(m, st->fp, s0, ng, st->F.p, soa_cstate(Us, nc), soa_state(Uo, nc), st->scal.p,
-                                                 stage2 ? 1 : 0, sv);
+                                                 stage2 ? 1 : 0, sv, st->floor_flags);
             MHD_LAUNCH_CHECK();
             P.end(KP_UPDATE, s);
         }
@@ -351,7 +361,7 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     launch_face_candidate(m, st->up.p, st->btot.p, st->bind.p, phis, st->phi_add.p, st->Ef.p, s);
     P.end(KP_FACE_CAND, s);
     P.begin(KP_EDGE_EMF, s);
-    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s);
+    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s, st->mres.n ? st->mres.p : nullptr);
     P.end(KP_EDGE_EMF, s);
     st->launches += (m.nf ? 1 : 0) + (m.ne ? 1 : 0);
     if (m.nf)
@@ -364,6 +374,30 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     }
 }
 
+} // namespace
+
+// One FP64 stage at the step size already in st->scal[0] (no CFL), for the differentiated run
+void fp64_stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2)
+{
+    stage(st, Us, phis, Uo, phio, stage2, false, 0.0);
+}
+
+// The first half of a stage: primitives, cell fields, u+ and the limited gradients of every species
+// (one species group) of (Us, phis), as fp64_stage leaves them
+void fp64_prepare_grad(MhdState *st, const double *Us, const double *phis)
+{
+    MHD_REQUIRE(st->nsp <= st->group, "one species group");
+    prepare_cfl(st, Us, phis, false, 0.0);
+    const MeshView &m = st->mesh->v;
+    const int64_t nc = m.nc;
+    const SField<const double> Wg{st->W.p, 5 * nc, 1, nc};
+    const SField<double> Gg{st->grad.p, 15 * nc, 1, nc};
+    if (st->prm.second_order) launch_limited_gradients(m, st->fp, Wg, Gg, st->mesh->stream);
+    else if (nc) MHD_CUDA(cudaMemsetAsync(st->grad.p, 0, (size_t)15 * st->nsp * nc * sizeof(double), st->mesh->stream));
+}
+
+namespace
+{
 void read_dt(MhdState *st, double *dt_host)
 {
     cudaStream_t s = st->mesh->stream;

@@ -97,6 +97,16 @@ _SIGS = {
     "mhd_gpu_induction_profile": ([vp, i32], ctypes.c_int),
     "mhd_gpu_induction_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+    "mhd_gpu_state_set_resistivity": ([vp, vp], ctypes.c_int),
+    "mhd_gpu_fn_create": ([vp, vp, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
+    "mhd_gpu_fn_destroy": ([vp], ctypes.c_int),
+    "mhd_gpu_fn_set_params": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_fn_reset": ([vp], ctypes.c_int),
+    "mhd_gpu_fn_forward": ([vp, ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_fn_backward": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_fn_tangent": ([vp, vp, vp, ctypes.POINTER(dbl), ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_fn_stage_tangent": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_fn_stage_adjoint": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
 }
 
 
@@ -437,6 +447,94 @@ class ResidentState:
         v = i64()
         check(lib().mhd_gpu_state_launches(self._h, ctypes.byref(v)))
         return v.value
+
+    def set_resistivity(self, m_edge):
+        """Explicit resistive EMF m_e (d1^T star2 Phi)_e per stage (m_edge per edge; None: off)."""
+        if m_edge is None:
+            check(lib().mhd_gpu_state_set_resistivity(self._h, None))
+            return
+        a = np.ascontiguousarray(m_edge, np.float64)
+        check(lib().mhd_gpu_state_set_resistivity(self._h, a.ctypes.data_as(vp)))
+
+
+class FnParams(ctypes.Structure):
+    _fields_ = [("n_steps", i32), ("checkpoint_every", i32), ("dt", dbl), ("uniform_flow", i32), ("pad", i32)]
+
+
+def _vp(a):
+    return None if a is None else a.ctypes.data_as(vp)
+
+
+class DeviceFunction:
+    """Differentiated explicit run (MhdFn of include/mhd_gpu.h): J = sum over `mask` of |B_tot|^2 V after
+    n_steps FP64 steps at the fixed dt, with its adjoint gradient with respect to the per-cell resistivity
+    and the inflow velocity, and its tangent-linear derivative.  Starts from the state's current U, Phi."""
+
+    def __init__(self, state: ResidentState, eta, mask, n_steps, checkpoint_every, dt, uniform_flow=True):
+        self.state = state
+        self.n_cells = state.mesh.n_cells
+        self.n_faces = state.mesh.n_faces
+        self.n_edges = state.mesh.n_edges
+        self.n_species = state.n_species
+        p = FnParams(int(n_steps), int(checkpoint_every), float(dt), int(bool(uniform_flow)), 0)
+        e = np.ascontiguousarray(eta, np.float64)
+        mk = np.ascontiguousarray(mask, np.int8)
+        h = vp()
+        check(lib().mhd_gpu_fn_create(state.handle, ctypes.byref(p), _vp(e), _vp(mk), ctypes.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.mhd_gpu_fn_destroy(self._h)
+            self._h = None
+
+    def set_params(self, eta=None, u_inf=None):
+        e = None if eta is None else np.ascontiguousarray(eta, np.float64)
+        u = None if u_inf is None else np.ascontiguousarray(u_inf, np.float64)
+        check(lib().mhd_gpu_fn_set_params(self._h, _vp(e), _vp(u)))
+
+    def reset(self):
+        check(lib().mhd_gpu_fn_reset(self._h))
+
+    def forward(self):
+        J = dbl()
+        check(lib().mhd_gpu_fn_forward(self._h, ctypes.byref(J)))
+        return J.value
+
+    def backward(self):
+        """(dJ/deta per cell, dJ/du_inf (3,)) of the last forward run."""
+        ge = np.empty(self.n_cells)
+        gu = np.empty(3)
+        check(lib().mhd_gpu_fn_backward(self._h, _vp(ge), _vp(gu)))
+        return ge, gu
+
+    def tangent(self, d_eta=None, d_u=None):
+        """(J, dJ) of a tangent-linear run along (d_eta, d_u)."""
+        de = None if d_eta is None else np.ascontiguousarray(d_eta, np.float64)
+        du = None if d_u is None else np.ascontiguousarray(d_u, np.float64)
+        J, dJ = dbl(), dbl()
+        check(lib().mhd_gpu_fn_tangent(self._h, _vp(de), _vp(du), ctypes.byref(J), ctypes.byref(dJ)))
+        return J.value, dJ.value
+
+    def stage_tangent(self, U, Phi, dU, dPhi, d_eta=None, d_u=None):
+        """Derivatives of one stage's U~ and E along (dU, dPhi, d_eta, d_u); U in the device layout."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (U, Phi, dU, dPhi)]
+        de = None if d_eta is None else np.ascontiguousarray(d_eta, np.float64)
+        du = None if d_u is None else np.ascontiguousarray(d_u, np.float64)
+        dUt = np.empty(5 * self.n_species * self.n_cells)
+        dE = np.empty(self.n_edges)
+        check(lib().mhd_gpu_fn_stage_tangent(self._h, *[_vp(x) for x in a], _vp(de), _vp(du), _vp(dUt), _vp(dE)))
+        return dUt, dE
+
+    def stage_adjoint(self, U, Phi, lUt, lE):
+        """Adjoints of one stage's inputs (U, Phi, eta, u_inf) from those of its U~ and E."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (U, Phi, lUt, lE)]
+        lU = np.empty(5 * self.n_species * self.n_cells)
+        lP = np.empty(self.n_faces)
+        le = np.empty(self.n_cells)
+        lu = np.empty(3)
+        check(lib().mhd_gpu_fn_stage_adjoint(self._h, *[_vp(x) for x in a], _vp(lU), _vp(lP), _vp(le), _vp(lu)))
+        return lU, lP, le, lu
 
 
 class DeviceInduction:

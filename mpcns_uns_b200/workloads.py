@@ -37,6 +37,16 @@ def to_cons(W, gamma):
     return U
 
 
+def prims(U, gamma):
+    """Primitives (n, 5) of conservative AoS values (no floors: the inverse of to_cons)."""
+    U = np.asarray(U, np.float64).reshape(-1, 5)
+    W = np.empty_like(U)
+    W[:, 0] = U[:, 0]
+    W[:, 1:4] = U[:, 1:4] / U[:, :1]
+    W[:, 4] = (gamma - 1.0) * (U[:, 4] - 0.5 * W[:, 0] * (W[:, 1:4] ** 2).sum(1))
+    return W
+
+
 def d1(mesh: HostMesh, A):
     """(d1 A)_f = sum_e f2e[f,e] A_e."""
     ptr, idx, sgn = mesh["f2e_ptr"], mesh["f2e_idx"], mesh["f2e_sgn"]
@@ -219,3 +229,60 @@ def induction_case(ncube=48, nr=96, r_in=0.8, r_out=6.0, eta_inner=1.0, eta_oute
     return InductionCase(name=f"shell6x{ncube}x{ncube}x{nr}x6_r{r_in:g}-{r_out:g}", mesh=m, m_edge=m_edge, B0=B0, ne=ne, Phi=Phi,
                          E_expl=E_expl, dirichlet=dirichlet, dt=dt_factor * dtw, dt_whistler=dtw, hall_coef=hall_coef,
                          hall_r_min=hall_r_min, hall_r_max=hall_r_max)
+
+
+def edge_resistivity(mesh: HostMesh, eta_cell):
+    """Per-edge coefficient m_e = eta_e / star1_e of the explicit resistive EMF, eta_e the mean of the per-cell
+    resistivity over the cells around edge e (summed in the edge's cell-list order, then divided by the count)."""
+    ptr, cells = np.asarray(mesh["ec_ptr"]), np.asarray(mesh["ec_cell"])
+    eta = np.asarray(eta_cell, np.float64)
+    out = np.zeros(mesh.n_edges)
+    for e in range(mesh.n_edges):
+        a, b = int(ptr[e]), int(ptr[e + 1])
+        acc = 0.0
+        for k in range(a, b):
+            acc += eta[cells[k]]
+        out[e] = (acc / (b - a)) / mesh["star1"][e] if b > a else 0.0
+    return out
+
+
+@dataclass
+class AdjointCase:
+    """Inputs of the gradient of J = sum |B_tot|^2 V over the dayside cells with r in [r_lo, r_hi] after n_steps
+    explicit steps at a fixed dt, with respect to the per-cell resistivity and the inflow velocity."""
+    wl: Workload
+    eta: np.ndarray          # per-cell resistivity, log-uniform in [eta_lo, eta_hi] (seeded)
+    mask: np.ndarray         # int8 per cell: the cells of the functional
+    n_steps: int
+    checkpoint_every: int
+
+
+def adjoint_case(ncube=32, nr=64, r_in=1.0, r_out=6.0, n_steps=40, checkpoint_every=8, eta_lo=1e-4, eta_hi=1e-2, r_lo=1.2,
+                 r_hi=1.6, induced_amp=0.05, noise=0.01, seed=0):
+    """The two-ion shell of the explicit step (no model sources) with a seeded per-cell resistivity; ncube = 32,
+    nr = 64 is the 2.36M-cell case.  Dayside: x > 0 (the inflow comes from +x).  The induced flux starts as d1
+    of 8 seeded Fourier modes of amplitude induced_amp (the box's potential without B0), so that the resistive
+    EMF acts from the first step; the dipole and the IMF stay in the background flux.  Every species' density
+    and pressure carry seeded uniform noise of relative size `noise` and its velocity noise of size
+    noise * |u_inf| per component (as the box's state does): without it the free stream's exactly equal
+    neighbour values put every limiter and wave-speed max / min on a tie, where J has no derivative."""
+    wl = shell(ncube, nr, r_in, r_out, seed=seed)
+    if induced_amp:
+        wl.Phi = d1(wl.mesh, fourier_potential(wl.mesh, seed + 2, amp=induced_amp, B0=(0.0, 0.0, 0.0)))
+    if noise:
+        rng_n = np.random.default_rng(seed + 11)
+        nc = wl.mesh.n_cells
+        U = []
+        for u in wl.U:
+            W = prims(u, wl.gamma)
+            W[:, 0] *= 1 + noise * rng_n.uniform(-1, 1, nc)
+            W[:, 4] *= 1 + noise * rng_n.uniform(-1, 1, nc)
+            W[:, 1:4] += noise * np.linalg.norm(wl.u_inf) * rng_n.uniform(-1, 1, (nc, 3))
+            U.append(to_cons(W, wl.gamma).ravel())
+        wl.U = U
+    rng = np.random.default_rng(seed + 7)
+    eta = 10.0 ** rng.uniform(np.log10(eta_lo), np.log10(eta_hi), wl.mesh.n_cells)
+    x = np.asarray(wl.mesh["cell_center"])
+    r = np.linalg.norm(x, axis=1)
+    mask = ((r >= r_lo) & (r <= r_hi) & (x[:, 0] > 0)).astype(np.int8)
+    return AdjointCase(wl=wl, eta=eta, mask=mask, n_steps=n_steps, checkpoint_every=checkpoint_every)

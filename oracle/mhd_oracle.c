@@ -598,6 +598,21 @@ void or_gyrate(const OrMesh *m, const OrStepParams *p, const double *B, double d
     }
 }
 
+/* E_e += m_e p0_e + 0 + 0, p0 = d1^T star2 Phi scattered face by face in ascending order: the resistive part of
+ * ImplicitInduction::apply_F (ImplicitInduction.cpp:133-137) and its sum out = m p0 + p1 + p2 (:182) with the Hall
+ * and ideal parts off, added to the owned edges' EMF */
+void or_resistive_emf(const OrMesh *m, const double *m_res, const double *phi, double *E)
+{
+    double *p0 = (double *)calloc((size_t)(m->n_edges > 0 ? m->n_edges : 1), sizeof(double));
+    for (int32_t f = 0; f < m->n_faces; ++f)
+    {
+        const double v = m->star2[f] * phi[f];
+        for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) p0[m->f2e_idx[k]] += m->f2e_sgn[k] * v;
+    }
+    for (int32_t e = 0; e < m->n_owned_edges; ++e) E[e] += m_res[e] * p0[e] + 0.0 + 0.0;
+    free(p0);
+}
+
 int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
 {
     const int32_t nc = m->n_cells, nf = m->n_faces, ne = m->n_edges, ns = p->n_species;
@@ -658,6 +673,7 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
         memset(E, 0, sizeof(double) * (size_t)ne);
         or_ideal_emf(m, up, Bt, Bi, Pt, phis, p->cuct, E);
         or_edge_modes(m, p->u_inf, p->B_imf, E);
+        if (p->m_res) or_resistive_emf(m, p->m_res, phis, E);
         for (int s = 0; s < ns; ++s)
         {
             memcpy(Uo[s], Ui[s], sizeof(double) * c5);

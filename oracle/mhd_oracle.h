@@ -53,12 +53,18 @@ typedef struct OrStepParams {
     /* two-ion model sources: J x B force and the Strang-split exact gyration (needs n_species == 2) */
     int32_t lorentz;
     double induce_coeff, inver_MA2;
+    /* explicit resistive EMF: E_e += m_res[e] (d1^T star2 Phi)_e on the owned edges, the resistive part of
+     * ImplicitInduction::apply_F (Common/induction/ImplicitInduction.cpp:133-137, 182) with m_e = eta_e / star1_e
+     * (NULL: off) */
+    const double *m_res;
 } OrStepParams;
 /* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part, species s: rhs += S */
 void or_add_sources(const OrMesh *m, const OrStepParams *p, int32_t s, const double *WH, const double *WNa, const double *B,
                     const double *J, double dt, double *rhs);
 /* mercury::gyrate (MercuryUns/physics/Gyration.cpp): exact rotation of the relative ion velocity about B */
 void or_gyrate(const OrMesh *m, const OrStepParams *p, const double *B, double dt, double *UH, double *UNa);
+/* explicit resistive EMF (see OrStepParams.m_res): E_e += m_e (d1^T star2 phi)_e on the owned edges */
+void or_resistive_emf(const OrMesh *m, const double *m_res, const double *phi, double *E);
 int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell,
                 double dt);
 

@@ -34,7 +34,7 @@ class OrStepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl), ("cuct", dbl),
                 ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3),
                 ("mass", dbl * 16), ("fs", OrPrim * 16), ("absorb", ctypes.c_int8 * 16), ("lorentz", i32),
-                ("induce_coeff", dbl), ("inver_MA2", dbl)]
+                ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p)]
 
 
 class OrIndParams(ctypes.Structure):
@@ -202,10 +202,13 @@ class PortMesh:
         """mercury::gyrate (oracle restatement); UH, UNa in place."""
         lib().or_gyrate(self.ref, ctypes.byref(p), _p(_f(B)), dt, _p(UH), _p(UNa))
 
-    def rk2_step(self, wl, U_list, Phi, Badd, dt, absorb=None, lorentz=False, induce_coeff=0.0, inver_MA2=1.0):
+    def rk2_step(self, wl, U_list, Phi, Badd, dt, absorb=None, lorentz=False, induce_coeff=0.0, inver_MA2=1.0, m_res=None):
         """One SSP-RK2 step of the hot path for a Workload's parameters; U_list and Phi updated in place.
-        With lorentz: the J x B source and (induce_coeff > 0) the Strang-split gyration of the two-ion model."""
+        With lorentz: the J x B source and (induce_coeff > 0) the Strang-split gyration of the two-ion model;
+        with m_res (per edge): the explicit resistive EMF E_e += m_e (d1^T star2 Phi)_e."""
         p = self.step_params(wl, absorb, lorentz, induce_coeff, inver_MA2)
+        mr = None if m_res is None else _f(m_res)
+        p.m_res = None if mr is None else mr.ctypes.data
         arr = (ctypes.c_void_p * len(U_list))(*[u.ctypes.data for u in U_list])
         rc = lib().or_rk2_step(self.ref, ctypes.byref(p), ctypes.cast(arr, ctypes.c_void_p), _p(Phi), _p(_f(wl.PhiAdd)), _p(_f(Badd)), dt)
         if rc != 0:

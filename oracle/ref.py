@@ -32,7 +32,7 @@ class StepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
                 ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("u_inf", dbl * 3),
                 ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", (dbl * 5) * 16), ("lorentz", i32), ("pad", i32),
-                ("induce_coeff", dbl), ("inver_MA2", dbl)]
+                ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p)]
 
 
 def lib():
@@ -290,7 +290,8 @@ class RefMesh:
 
     def rk2_step(self, params: StepParams, U_list, Phi, PhiAdd, BaddCell, dt):
         """One SSP-RK2 step of the hot path (Solver::step; with params.lorentz the J x B source and the
-        Strang-split gyration of the two-ion model); U_list and Phi in place."""
+        Strang-split gyration of the two-ion model; with params.m_res the explicit resistive EMF
+        E += ImplicitInduction::apply_F(Phi), resistive part, per-edge m_e); U_list and Phi in place."""
         arr = (ctypes.c_void_p * len(U_list))(*[a.ctypes.data for a in U_list])
         PhiAdd = np.ascontiguousarray(PhiAdd, np.float64)
         BaddCell = np.ascontiguousarray(BaddCell, np.float64)

@@ -57,6 +57,9 @@ struct RefMesh
     Config cfg;
     std::unique_ptr<Stencil> stencil;
     std::vector<char> active;
+    // resistive operator of the explicit resistive EMF (declared after res_ex: destroyed first)
+    std::unique_ptr<comm::Exchanger> res_ex;
+    std::unique_ptr<ImplicitInduction> res_op;
 };
 
 thread_local std::string g_err;
@@ -485,6 +488,9 @@ struct RefStepParams
     // model sources of the two-ion step: J x B force (add_sources_n) and the exact gyration (gyrate)
     int32_t lorentz, pad;
     double induce_coeff, inver_MA2;
+    // explicit resistive EMF: E += ImplicitInduction::apply_F(Phi) with only the resistive part on and the
+    // per-edge m_e = eta_e / star1_e given here (null: off), added to the owned edges
+    const double *m_res;
 };
 
 namespace
@@ -524,7 +530,7 @@ namespace
 struct StepWork
 {
     std::vector<std::vector<double>> W, grad, rhs, U1, U2;
-    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2, J;
+    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2, J, Eres;
 };
 
 // charge-weighted ion velocity of Solver::prepare (Solver.cpp:108-118) with mhd::Scales::numinfo (Scales.cpp:50-62)
@@ -594,6 +600,23 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
         if (lorentz && ns != 2) throw std::runtime_error("the source terms are those of the two-ion model");
         const Config scfg = source_config(r, p);
         const bool split = lorentz && p.induce_coeff > 0; // Strang splitting of the gyration (Solver.cpp:492-498)
+        // the resistive operator of ImplicitInduction (Hall and ideal parts off) with the given per-edge m_e
+        ImplicitInduction *res = nullptr;
+        if (p.m_res)
+        {
+            if (!r->res_op)
+            {
+                ensure_geo(r);
+                r->res_ex = std::make_unique<comm::Exchanger>(MPI_COMM_SELF, r->lm);
+                Config c;
+                c.resistive = true; c.sc.inver_Rem = 1.0; c.hall = false;
+                r->res_op = std::make_unique<ImplicitInduction>(r->lm, r->geo, *r->res_ex, c);
+            }
+            res = r->res_op.get();
+            std::copy(p.m_res, p.m_res + res->m_.size(), res->m_.begin());
+            res->resistive_ = true; res->hall_ = false; res->ideal_ = false;
+            w.Eres.assign(ne, 0.0);
+        }
 
         // prepare + rhs of one stage on (Us, phis); the stage result goes to (Uo, phio)
         auto stage = [&](std::vector<double *> &Us, const double *phis, std::vector<double *> &Uo, double *phio) {
@@ -638,6 +661,11 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
             {
                 if (r->bc.edge_mode[e] == 1) w.E[e] = 0.0;
                 else if (r->bc.edge_mode[e] == 2) w.E[e] = dot(E_inf, r->geo.edge_vec[e]);
+            }
+            if (res)
+            {
+                res->apply_F(phis, w.Eres.data());
+                for (Id e = 0; e < cx.ent[1].n_owned; ++e) w.E[e] += w.Eres[e];
             }
             // advance: out = base + dt * rhs on the owned fluid cells, CT on the active faces, floors
             for (int k = 0; k < ns; ++k)

@@ -193,3 +193,37 @@ def test_lorentz_sources_gyration_and_step():
     o.rk2_step(wl, Ua, Pa, Badd, dt)
     o.rk2_step(wl, Ub, Pb, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8)
     assert np.linalg.norm(Ua[0] - Ub[0]) > 1e-6 * np.linalg.norm(Ua[0])
+
+
+def test_resistive_emf_step():
+    """The step with the explicit resistive EMF (ImplicitInduction::apply_F, resistive part, per-edge m_e),
+    oracle restatement against the compiled reference, bit for bit."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5)
+    h = wl.mesh
+    r = ref_twin(h, SHELL_TAGS).boundary(*SHELL_BC)
+    o = port.PortMesh(h)
+    rng = np.random.default_rng(5)
+    eta = 10.0 ** rng.uniform(-4, -2, h.n_cells)
+    m_res = workloads.edge_resistivity(h, eta)
+    assert (m_res > 0).all()
+    rp = _ref_params(wl, False, 0.0, 1.0)
+    rp.m_res = m_res.ctypes.data
+    Badd = r.cell_vector(wl.PhiAdd)
+    Uo = [np.array(u) for u in wl.U]
+    Ur = [np.array(u) for u in wl.U]
+    Po = np.array(wl.Phi) + rng.uniform(-1e-2, 1e-2, h.n_faces)
+    Pr = Po.copy()
+    for _ in range(3):
+        o.rk2_step(wl, Uo, Po, Badd, 2e-3, m_res=m_res)
+        r.rk2_step(rp, Ur, Pr, wl.PhiAdd, Badd, 2e-3)
+        for a, b in zip(Uo, Ur):
+            same(a, b)
+        same(Po, Pr)
+    # the resistive EMF acts
+    Pb = np.array(wl.Phi) + rng.uniform(-1e-2, 1e-2, h.n_faces)
+    Pa = Pb.copy()
+    Ua, Ub = [np.array(u) for u in wl.U], [np.array(u) for u in wl.U]
+    o.rk2_step(wl, Ua, Pa, Badd, 2e-3)
+    o.rk2_step(wl, Ub, Pb, Badd, 2e-3, m_res=m_res)
+    assert np.abs(Pa - Pb).max() > 1e-9
