@@ -21,6 +21,12 @@ on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, c
 --gmres-max-it iterations: seconds per solve in FP64 and mixed precision, per-kernel GB/s, and the
 reference's own solve on a bounded sample beside it.
 
+The "adjoint" object: the gradient of J = sum |B_tot|^2 V over the dayside cells with r in [1.2, 1.6]
+after 40 FP64 steps on the 6 x 32 x 32 x 64 x 6 shell (2,359,296 cells, two ions, explicit resistive
+EMF of a seeded per-cell resistivity) with respect to the resistivity and the inflow velocity: device
+seconds of the forward run, the checkpointed adjoint sweep and the tangent-linear run, and the
+gradient's agreement with tangent-linear dot products and central differences (--no-adjoint: skip).
+
 Under torchrun (N > 1) every rank runs an independent replica on its own GPU (the hot path
 has no data-path exchange on one mesh per GPU); value = all ranks' cell-updates / max time.
 """
@@ -313,6 +319,98 @@ def bench_gmres(args, peak):
     return out
 
 
+def bench_adjoint(args):
+    """Gradient of J = sum |B_tot|^2 V over the dayside cells with r in [1.2, 1.6] after 40 FP64 steps (fixed CFL
+    step of the initial state) on the 6 x 32 x 32 x 64 shell (2.36M tets, two ions, explicit resistive EMF with a
+    seeded log-uniform per-cell resistivity 1e-4..1e-2), with respect to the resistivity and the inflow velocity:
+    device time of the forward run (checkpoint every 8 steps), the adjoint sweep and the tangent-linear run; the
+    adjoint against the tangent-linear run (dot products) and against central differences of the forward run
+    (which is bit-identical to the reference's step) along 16 seeded directions at h = 1e-6 and 1e-7."""
+    import torch
+    from mpcns_uns_b200 import gpu, workloads
+    t = time.time()
+    case = workloads.adjoint_case(args.adj_ncube, args.adj_nr, n_steps=args.adj_steps, checkpoint_every=args.adj_checkpoint)
+    wl = case.wl
+    h = wl.mesh
+    log(f"[bench] adjoint workload {wl.name}: {h.n_cells} cells (setup {time.time() - t:.1f}s)")
+    dm = gpu.DeviceMesh(h)
+    p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl)
+    st = gpu.ResidentState(dm, p)
+    st.set(wl.U, wl.Phi, wl.PhiAdd)
+    dt = st.cfl_dt()
+    free0 = torch.cuda.mem_get_info()[0]
+    fn = gpu.DeviceFunction(st, case.eta, case.mask, case.n_steps, case.checkpoint_every, dt)
+    fn.forward()
+    fn.backward()   # warm-up: allocates the checkpoints and the recorded segment
+    torch.cuda.synchronize()
+    mem = free0 - torch.cuda.mem_get_info()[0]
+
+    def dev_time(f, reps=2):
+        ms = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(dm.stream)
+            r = f()
+            e1.record(dm.stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms)), r
+
+    l0 = st.launches()
+    fwd_ms, J = dev_time(fn.forward)
+    step_launches = (st.launches() - l0) // 2
+    bwd_ms, (ge, gu) = dev_time(fn.backward)
+    rng = np.random.default_rng(23)
+    nc = h.n_cells
+    u0 = np.asarray(wl.u_inf, np.float64)
+    d_eta = rng.standard_normal(nc) * case.eta
+    d_u = rng.standard_normal(3) * np.linalg.norm(u0)
+    tan_ms, (Jt, dJ) = dev_time(lambda: fn.tangent(d_eta, d_u), reps=1)
+    adj = float(ge @ d_eta + gu @ d_u)
+    dots = [abs(adj - dJ) / abs(dJ)]
+    for _ in range(2):
+        de = rng.standard_normal(nc) * case.eta
+        du = rng.standard_normal(3) * np.linalg.norm(u0)
+        _, dj = fn.tangent(de, du)
+        dots.append(abs(float(ge @ de + gu @ du) - dj) / abs(dj))
+    fd = {}
+    dirs = [(rng.standard_normal(nc) * case.eta, rng.standard_normal(3) * np.linalg.norm(u0)) for _ in range(args.adj_fd_dirs)]
+    for hh in (1e-6, 1e-7):
+        errs = []
+        for de, du in dirs:
+            fn.set_params(eta=case.eta + hh * de, u_inf=u0 + hh * du)
+            Jp = fn.forward()
+            fn.set_params(eta=case.eta - hh * de, u_inf=u0 - hh * du)
+            Jm = fn.forward()
+            f = (Jp - Jm) / (2 * hh)
+            errs.append(abs(float(ge @ de + gu @ du) - f) / abs(f))
+        fd[f"h={hh:g}"] = {"max_rel_err": max(errs), "median_rel_err": float(np.median(errs)), "directions": len(errs)}
+    fn.set_params(eta=case.eta, u_inf=u0)
+    # the eta part alone is smooth (the resistive EMF is linear in eta): h = 1e-4 clears the round-off
+    errs = []
+    for de, _ in dirs[:4]:
+        fn.set_params(eta=case.eta + 1e-4 * de)
+        Jp = fn.forward()
+        fn.set_params(eta=case.eta - 1e-4 * de)
+        Jm = fn.forward()
+        f = (Jp - Jm) / 2e-4
+        errs.append(abs(float(ge @ de) - f) / abs(f))
+    fn.set_params(eta=case.eta)
+    fd["eta_only_h=1e-4"] = {"max_rel_err": max(errs), "directions": len(errs)}
+    out = {"workload": wl.name, "cells": nc, "faces": h.n_faces, "edges": h.n_edges, "n_species": wl.n_species,
+           "steps": case.n_steps, "checkpoint_every": case.checkpoint_every, "dt": dt, "J": J,
+           "functional": "sum |B_tot|^2 V over the dayside cells with 1.2 <= r <= 1.6",
+           "parameters": "per-cell resistivity (log-uniform 1e-4..1e-2) and the inflow velocity (3)",
+           "forward_s": fwd_ms / 1e3, "backward_s": bwd_ms / 1e3, "tangent_s": tan_ms / 1e3,
+           "backward_over_forward": bwd_ms / fwd_ms, "forward_plus_backward_over_forward": (fwd_ms + bwd_ms) / fwd_ms,
+           "tangent_over_forward": tan_ms / fwd_ms, "step_launches_per_forward": step_launches,
+           "device_memory_GB": mem / 1e9, "dot_test_rel_err_max": max(dots), "fd": fd, "grad_u": [float(x) for x in gu],
+           "grad_eta_abs_max": float(np.abs(ge).max())}
+    del fn, st, dm
+    torch.cuda.empty_cache()
+    return out
+
+
 def gmres_cpu_baseline(max_it=60):
     """ImplicitInduction::solve of the reference (oracle/_ref, np = 1, one core) on the same construction at
     6 x 16 x 16 x 24 (262,704 edges), cold start, `max_it` iterations: seconds per GMRES iteration."""
@@ -363,6 +461,12 @@ def main():
     ap.add_argument("--gmres-nr", type=int, default=96)
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adj-ncube", type=int, default=32)
+    ap.add_argument("--adj-nr", type=int, default=64)
+    ap.add_argument("--adj-steps", type=int, default=40)
+    ap.add_argument("--adj-checkpoint", type=int, default=8)
+    ap.add_argument("--adj-fd-dirs", type=int, default=16)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -537,6 +641,13 @@ def main():
             except Exception as e:
                 log(f"[bench] gmres cpu baseline failed: {e}")
 
+    adj = None
+    if rank == 0 and not args.no_adjoint:
+        if args.no_gmres:
+            del st64, st32, st
+            torch.cuda.empty_cache()
+        adj = bench_adjoint(args)
+
     if rank == 0:
         out = {"metric": METRIC, "value": rmx["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": rmx["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -558,7 +669,7 @@ def main():
                         "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
                "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm}
+               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "adjoint": adj}
         print(json.dumps(out))
     if dist:
         dist.barrier()
