@@ -373,6 +373,12 @@ def bench_adjoint(args):
         du = rng.standard_normal(3) * np.linalg.norm(u0)
         _, dj = fn.tangent(de, du)
         dots.append(abs(float(ge @ de + gu @ du) - dj) / abs(dj))
+    fn.profile(True)
+    fn.forward()
+    fn.backward()
+    prof = fn.profile_read()
+    fn.profile(False)
+    classes = {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items() if v[1]}
     fd = {}
     dirs = [(rng.standard_normal(nc) * case.eta, rng.standard_normal(3) * np.linalg.norm(u0)) for _ in range(args.adj_fd_dirs)]
     for hh in (1e-6, 1e-7):
@@ -404,7 +410,8 @@ def bench_adjoint(args):
            "forward_s": fwd_ms / 1e3, "backward_s": bwd_ms / 1e3, "tangent_s": tan_ms / 1e3,
            "backward_over_forward": bwd_ms / fwd_ms, "forward_plus_backward_over_forward": (fwd_ms + bwd_ms) / fwd_ms,
            "tangent_over_forward": tan_ms / fwd_ms, "step_launches_per_forward": step_launches,
-           "device_memory_GB": mem / 1e9, "dot_test_rel_err_max": max(dots), "fd": fd, "grad_u": [float(x) for x in gu],
+           "device_memory_GB": mem / 1e9, "classes_forward_plus_backward": classes,
+           "dot_test_rel_err_max": max(dots), "fd": fd, "grad_u": [float(x) for x in gu],
            "grad_eta_abs_max": float(np.abs(ge).max())}
     del fn, st, dm
     torch.cuda.empty_cache()

@@ -275,6 +275,11 @@ int mhd_gpu_fn_stage_tangent(MhdFn *fn, const double *U, const double *Phi, cons
                              const double *d_u, double *dUt, double *dE);
 int mhd_gpu_fn_stage_adjoint(MhdFn *fn, const double *U, const double *Phi, const double *lUt, const double *lE, double *lU, double *lPhi,
                              double *l_eta, double *l_u);
+/* Per-class device time of the Function's runs (CUDA events on the mesh stream while enabled; classes:
+ * forward_steps, record_steps, adj_floors, adj_edge_emf, adj_face_candidate, adj_cell, adj_face_flux,
+ * adj_limited_gradients, adj_prim, adj_misc, tangent_steps), read as in mhd_gpu_state_profile_read. */
+int mhd_gpu_fn_profile(MhdFn *fn, int32_t enable);
+int mhd_gpu_fn_profile_read(MhdFn *fn, int32_t max_kernels, char *names, double *ms_total, int64_t *count, int32_t *n_out);
 
 /* Live per-kernel timing of the fused step (CUDA events recorded on the handle's stream around
  * every launch while enabled).  _read synchronises, returns per kernel class its name (32 chars

@@ -1065,6 +1065,8 @@ __global__ void __launch_bounds__(128) k_a_flux(MeshView m, FluidParams p, const
 // K5: per (cell, species): the face-state transpose (lW, lG from the cell's four face slots), then the
 // reverse of k_limited_gradients_tet.  lW holds the u+ part on entry and the cell's own total on exit;
 // slot[((s*4 + j)*5 + q)*nc + c] receives the adjoint of neighbour j's primitive q as this cell's stencil saw it.
+// Every loop over the four slots and five variables is unrolled and the winning slots of the min / max
+// terms are selected by predicates, so the per-thread arrays stay in registers.
 __global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const double *__restrict__ W, const double *__restrict__ G,
                                                  const double *__restrict__ lface, double *__restrict__ lW, double *__restrict__ slot,
                                                  double *__restrict__ lfs)
@@ -1074,24 +1076,27 @@ __global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const
     if (c >= m.nc || s >= p.nsp) return;
     const int64_t n = m.nc, nf = m.nf;
     double wc[5], g[15], lw[5], lG[15];
+#pragma unroll
     for (int q = 0; q < 5; ++q)
     {
         wc[q] = W[ui(s, q, c, n)];
         lw[q] = lW[ui(s, q, c, n)];
     }
+#pragma unroll
     for (int q = 0; q < 15; ++q)
     {
         g[q] = G[gi(s, q, c, n)];
         lG[q] = 0.0;
     }
     const V3 xc = ld3(m.cell_center, c);
-    const Prim5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
+#pragma unroll
     for (int j = 0; j < 4; ++j)
     {
         const int32_t f = m.c2f_idx[4 * c + j];
         const int side = m.c2f_sgn[4 * c + j] > 0 ? 0 : 1;
         double lf[5];
         bool any = false;
+#pragma unroll
         for (int q = 0; q < 5; ++q)
         {
             lf[q] = lface[((int64_t)(s * 2 + side) * 5 + q) * nf + f];
@@ -1100,7 +1105,8 @@ __global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const
         if (!any) continue;
         const V3 dx = ld3(m.face_center, f) - xc;
         // face_state extrapolates unless the extrapolated density or pressure is not positive
-        const bool extrap = wcp.rho + g[0] * dx.x + g[1] * dx.y + g[2] * dx.z > 0 && wcp.p + g[12] * dx.x + g[13] * dx.y + g[14] * dx.z > 0;
+        const bool extrap = wc[0] + g[0] * dx.x + g[1] * dx.y + g[2] * dx.z > 0 && wc[4] + g[12] * dx.x + g[13] * dx.y + g[14] * dx.z > 0;
+#pragma unroll
         for (int q = 0; q < 5; ++q)
         {
             lw[q] += lf[q];
@@ -1113,38 +1119,62 @@ __global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const
         }
     }
     double lwn[4][5];
-    for (int j = 0; j < 4; ++j)
-        for (int q = 0; q < 5; ++q) lwn[j][q] = 0.0;
     int32_t nb[4];
-    for (int j = 0; j < 4; ++j) nb[j] = m.t_nb[j * n + c];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+    {
+        nb[j] = m.t_nb[j * n + c];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) lwn[j][q] = 0.0;
+    }
     const bool valid = c < m.no_cells && m.st_valid[c];
     if (valid)
     {
-        double wn[4][5];
+        const Prim5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
+        double wn[4][5], wd[12], dxs[12];
+#pragma unroll
         for (int j = 0; j < 4; ++j)
+        {
             if (nb[j] >= 0)
+            {
+#pragma unroll
                 for (int q = 0; q < 5; ++q) wn[j][q] = W[ui(s, q, nb[j], n)];
-        for (int j = 0; j < 4; ++j)
-            if (nb[j] < 0 && nb[j] != INT32_MIN)
+            }
+            else if (nb[j] != INT32_MIN)
             {
                 const int32_t f = -(nb[j] + 1);
                 const V3 nrm = (double(m.t_sg[j * n + c]) / m.face_area_mag[f]) * ld3(m.face_area, f);
-                prim_arr(ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, nrm, p.fs[s]), wn[j]);
+                const Prim5 gh = ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, nrm, p.fs[s]);
+                wn[j][0] = gh.rho; wn[j][1] = gh.u; wn[j][2] = gh.v; wn[j][3] = gh.w; wn[j][4] = gh.p;
             }
+            else
+            {
+#pragma unroll
+                for (int q = 0; q < 5; ++q) wn[j][q] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 12; ++i)
+        {
+            wd[i] = m.t_wd[i * n + c];
+            dxs[i] = m.t_dx[i * n + c];
+        }
         const double I00 = m.t_inv[c], I01 = m.t_inv[n + c], I02 = m.t_inv[2 * n + c], I11 = m.t_inv[3 * n + c],
                      I12 = m.t_inv[4 * n + c], I22 = m.t_inv[5 * n + c];
+#pragma unroll
         for (int q = 0; q < 5; ++q)
         {
             if (lG[3 * q] == 0.0 && lG[3 * q + 1] == 0.0 && lG[3 * q + 2] == 0.0) continue;
             double r0 = 0, r1 = 0, r2 = 0, lo = wc[q], hi = wc[q];
             int jlo = -1, jhi = -1;
+#pragma unroll
             for (int j = 0; j < 4; ++j)
             {
                 if (nb[j] == INT32_MIN) continue;
                 const double dq = wn[j][q] - wc[q];
-                r0 += m.t_wd[(3 * j) * n + c] * dq;
-                r1 += m.t_wd[(3 * j + 1) * n + c] * dq;
-                r2 += m.t_wd[(3 * j + 2) * n + c] * dq;
+                r0 += wd[3 * j] * dq;
+                r1 += wd[3 * j + 1] * dq;
+                r2 += wd[3 * j + 2] * dq;
                 if (wn[j][q] < lo)
                 {
                     lo = wn[j][q];
@@ -1159,37 +1189,45 @@ __global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const
             const double g0 = I00 * r0 + I01 * r1 + I02 * r2;
             const double g1 = I01 * r0 + I11 * r1 + I12 * r2;
             const double g2 = I02 * r0 + I12 * r1 + I22 * r2;
-            double psi = 1.0;
-            int win = -1, wtype = 0; // the limiter term that set psi: 0 hi, 1 lo, 2 relative
-            double wdl = 0;
+            double psi = 1.0, wdl = 0, wx = 0, wy = 0, wz = 0;
+            int wtype = -1; // the limiter term that set psi: 0 hi, 1 lo, 2 relative
             if (p.limit)
             {
+#pragma unroll
                 for (int j = 0; j < 4; ++j)
                 {
-                    const double d = g0 * m.t_dx[(3 * j) * n + c] + g1 * m.t_dx[(3 * j + 1) * n + c] + g2 * m.t_dx[(3 * j + 2) * n + c];
-                    double x;
-                    int ty;
+                    const double d = g0 * dxs[3 * j] + g1 * dxs[3 * j + 1] + g2 * dxs[3 * j + 2];
+                    double x = psi;
+                    int ty = -1;
                     if (d > 1e-300) { x = (hi - wc[q]) / d; ty = 0; }
                     else if (d < -1e-300) { x = (lo - wc[q]) / d; ty = 1; }
-                    else continue;
-                    if (x < psi) { psi = x; win = j; wtype = ty; wdl = d; }
+                    if (ty >= 0 && x < psi)
+                    {
+                        psi = x; wtype = ty; wdl = d;
+                        wx = dxs[3 * j]; wy = dxs[3 * j + 1]; wz = dxs[3 * j + 2];
+                    }
                 }
                 if (p.rel_limit > 0 && (q == 0 || q == 4))
+#pragma unroll
                     for (int j = 0; j < 4; ++j)
                     {
-                        const double d = g0 * m.t_dx[(3 * j) * n + c] + g1 * m.t_dx[(3 * j + 1) * n + c] + g2 * m.t_dx[(3 * j + 2) * n + c];
+                        const double d = g0 * dxs[3 * j] + g1 * dxs[3 * j + 1] + g2 * dxs[3 * j + 2];
                         const double da = fabs(d);
                         if (da > 1e-300)
                         {
                             const double x = p.rel_limit * wc[q] / da;
-                            if (x < psi) { psi = x; win = j; wtype = 2; wdl = d; }
+                            if (x < psi)
+                            {
+                                psi = x; wtype = 2; wdl = d;
+                                wx = dxs[3 * j]; wy = dxs[3 * j + 1]; wz = dxs[3 * j + 2];
+                            }
                         }
                     }
             }
             const double ps = dmax(0.0, dmin(1.0, psi));
             double lg0 = ps * lG[3 * q], lg1 = ps * lG[3 * q + 1], lg2 = ps * lG[3 * q + 2];
             double lwc = 0, lhi = 0, llo = 0;
-            if (psi < 1.0 && 0.0 < psi && win >= 0)
+            if (psi < 1.0 && 0.0 < psi && wtype >= 0)
             {
                 const double lpsi = lG[3 * q] * g0 + lG[3 * q + 1] * g1 + lG[3 * q + 2] * g2;
                 double ldl;
@@ -1206,37 +1244,43 @@ __global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const
                     lwc -= lpsi / wdl;
                     ldl = -psi * lpsi / wdl;
                 }
-                lg0 += ldl * m.t_dx[(3 * win) * n + c];
-                lg1 += ldl * m.t_dx[(3 * win + 1) * n + c];
-                lg2 += ldl * m.t_dx[(3 * win + 2) * n + c];
+                lg0 += ldl * wx;
+                lg1 += ldl * wy;
+                lg2 += ldl * wz;
             }
-            if (jhi >= 0) lwn[jhi][q] += lhi;
-            else lwc += lhi;
-            if (jlo >= 0) lwn[jlo][q] += llo;
-            else lwc += llo;
+            if (jhi < 0) lwc += lhi;
+            if (jlo < 0) lwc += llo;
             const double lr0 = I00 * lg0 + I01 * lg1 + I02 * lg2;
             const double lr1 = I01 * lg0 + I11 * lg1 + I12 * lg2;
             const double lr2 = I02 * lg0 + I12 * lg1 + I22 * lg2;
+#pragma unroll
             for (int j = 0; j < 4; ++j)
             {
-                if (nb[j] == INT32_MIN) continue;
-                const double d = m.t_wd[(3 * j) * n + c] * lr0 + m.t_wd[(3 * j + 1) * n + c] * lr1 + m.t_wd[(3 * j + 2) * n + c] * lr2;
-                lwn[j][q] += d;
-                lwc -= d;
+                double a = (j == jhi ? lhi : 0.0) + (j == jlo ? llo : 0.0);
+                if (nb[j] != INT32_MIN)
+                {
+                    const double d = wd[3 * j] * lr0 + wd[3 * j + 1] * lr1 + wd[3 * j + 2] * lr2;
+                    a += d;
+                    lwc -= d;
+                }
+                lwn[j][q] += a;
             }
             lw[q] += lwc;
         }
+#pragma unroll
         for (int j = 0; j < 4; ++j)
             if (nb[j] < 0 && nb[j] != INT32_MIN)
             {
                 const int32_t f = -(nb[j] + 1);
                 const V3 nrm = (double(m.t_sg[j * n + c]) / m.face_area_mag[f]) * ld3(m.face_area, f);
                 ghost_T(m.face_kind[f], p.absorb[s] != 0, nrm, lwn[j], lw, lfs + 5 * s);
-                for (int q = 0; q < 5; ++q) lwn[j][q] = 0.0;
             }
     }
+#pragma unroll
     for (int j = 0; j < 4; ++j)
+#pragma unroll
         for (int q = 0; q < 5; ++q) slot[((int64_t)(s * 4 + j) * 5 + q) * n + c] = nb[j] >= 0 ? lwn[j][q] : 0.0;
+#pragma unroll
     for (int q = 0; q < 5; ++q) lW[ui(s, q, c, n)] = lw[q];
 }
 
@@ -1348,6 +1392,13 @@ constexpr int kJBlocks = 296; // 2 x 148 SMs: fixed, so the functional's sum has
 
 using namespace mhd;
 
+// kernel classes of the differentiated run, timed with CUDA events while profiling is on
+enum FnKernel { FN_FORWARD = 0, FN_RECORD, FN_ADJ_FLOORS, FN_ADJ_EDGE, FN_ADJ_FACE, FN_ADJ_CELL, FN_ADJ_FLUX, FN_ADJ_GRAD, FN_ADJ_PRIM,
+                FN_ADJ_MISC, FN_TANGENT, FN_COUNT };
+static const char *const kFnKernelNames[FN_COUNT] = {"forward_steps", "record_steps", "adj_floors", "adj_edge_emf", "adj_face_candidate",
+                                                     "adj_cell", "adj_face_flux", "adj_limited_gradients", "adj_prim", "adj_misc",
+                                                     "tangent_steps"};
+
 struct MhdFn
 {
     MhdState *st = nullptr;
@@ -1360,12 +1411,20 @@ struct MhdFn
     DBuf<int32_t> efpos;
     std::vector<std::unique_ptr<DBuf<double>>> ckU, ckP;
     // recorded segment: per step the stage inputs, U~ of stage 2 and the floor flags of both stages
+    // a stage's primitives, limited gradients and cell fields, as the stage left them in the state's buffers
+    struct StageFields
+    {
+        DBuf<double> W, G, up, bind, btot;
+    };
     struct TapeStep
     {
         DBuf<double> U0, P0, U1, P1, Ut2;
         DBuf<int8_t> fl1, fl2;
+        StageFields sf[2];
     };
     std::vector<std::unique_ptr<TapeStep>> tape;
+    int tape_seg = -1; // the segment whose steps the tape holds (-1: none)
+    mhd::EventProfiler<FN_COUNT> prof;
     // adjoint work arrays
     DBuf<double> lU, lP, lU1, lP1, lUt, lE, lrV, lc, efphi, lres, lm, lup, lB, y, lW, lface, slot, lpar, geta, part, red, phiscratch;
     // tangent arrays
@@ -1556,37 +1615,120 @@ void adjoint_stage(MhdFn *fn, const double *Uin, const double *Pin, const double
     cudaStream_t s = stream_of(fn);
     const int64_t nc = m.nc;
     const int nsp = fn->nsp;
+    auto &P = fn->prof;
     if (nc)
+    {
+        P.begin(FN_ADJ_FLOORS, s);
         k_a_floors<<<dim3(g128(nc), nsp), 128, 0, s>>>(m, st->fp, flags, Ut, lUt, fn->prm.dt, fn->lrV.p, lUin);
+        P.end(FN_ADJ_FLOORS, s);
+    }
     if (m.ne)
     {
         const double *mr = st->mres.n ? st->mres.p : nullptr;
+        P.begin(FN_ADJ_EDGE, s);
         if (m.max_valence <= 8)
             k_a_edge<8><<<g128(m.ne), 128, 0, s>>>(m, st->up.p, Pin, st->prm.cuct, mr, fn->lE.p, fn->lc.p, fn->efphi.p, fn->lres.p,
                                                     fn->lm.p, fn->lpar.p, fn->lup.p);
         else
             k_a_edge<kMaxValence><<<g128(m.ne), 128, 0, s>>>(m, st->up.p, Pin, st->prm.cuct, mr, fn->lE.p, fn->lc.p, fn->efphi.p,
                                                               fn->lres.p, fn->lm.p, fn->lpar.p, fn->lup.p);
+        P.end(FN_ADJ_EDGE, s);
     }
     if (m.nf)
+    {
+        P.begin(FN_ADJ_FACE, s);
         k_a_face_cand<<<g128(m.nf), 128, 0, s>>>(m, st->up.p, st->btot.p, st->bind.p, Pin, st->phi_add.p, fn->lc.p, fn->fw.p,
                                                   fn->efpos.p, fn->efphi.p, fn->lres.p, fn->lup.p, fn->lB.p, lPin);
-    if (nc) k_a_cell<<<g128(nc), 128, 0, s>>>(m, nsp, st->mass.p, st->prm.M_ref, st->W.p, fn->lup.p, fn->lB.p, fn->y.p, fn->lW.p);
-    if (m.nf)
-        k_a_flux<<<dim3(g128(m.nf), nsp), 128, 0, s>>>(m, st->fp, st->W.p, st->grad.p, fn->lrV.p, fn->lface.p, fn->lpar.p + 3, fn->y.p,
-                                                        lPin);
+        P.end(FN_ADJ_FACE, s);
+    }
     if (nc)
     {
+        P.begin(FN_ADJ_CELL, s);
+        k_a_cell<<<g128(nc), 128, 0, s>>>(m, nsp, st->mass.p, st->prm.M_ref, st->W.p, fn->lup.p, fn->lB.p, fn->y.p, fn->lW.p);
+        P.end(FN_ADJ_CELL, s);
+    }
+    if (m.nf)
+    {
+        P.begin(FN_ADJ_FLUX, s);
+        k_a_flux<<<dim3(g128(m.nf), nsp), 128, 0, s>>>(m, st->fp, st->W.p, st->grad.p, fn->lrV.p, fn->lface.p, fn->lpar.p + 3, fn->y.p,
+                                                        lPin);
+        P.end(FN_ADJ_FLUX, s);
+    }
+    if (nc)
+    {
+        P.begin(FN_ADJ_GRAD, s);
         k_a_grad<<<dim3(g128(nc), nsp), 128, 0, s>>>(m, st->fp, st->W.p, st->grad.p, fn->lface.p, fn->lW.p, fn->slot.p, fn->lpar.p + 3);
+        P.end(FN_ADJ_GRAD, s);
+        P.begin(FN_ADJ_PRIM, s);
         k_a_prim<<<dim3(g128(nc), nsp), 128, 0, s>>>(m, st->fp, Uin, fn->lW.p, fn->slot.p, fn->rslot.p, lUin);
+        P.end(FN_ADJ_PRIM, s);
     }
     MHD_LAUNCH_CHECK();
 }
 
-// primitives, cell fields and limited gradients of a stage input (the first half of the stage, no fluxes)
-void recompute_inputs(MhdFn *fn, const double *U, const double *P)
+// exchange the state's stage buffers with a recorded set (equal sizes: ownership stays consistent)
+void swap_fields(MhdState *st, MhdFn::StageFields &f)
 {
-    fp64_prepare_grad(fn->st, U, P);
+    std::swap(st->W.p, f.W.p);
+    std::swap(st->grad.p, f.G.p);
+    std::swap(st->up.p, f.up.p);
+    std::swap(st->bind.p, f.bind.p);
+    std::swap(st->btot.p, f.btot.p);
+}
+
+void alloc_step(MhdFn *fn, MhdFn::TapeStep &T)
+{
+    const MeshView &m = fn->st->mesh->v;
+    const size_t nc = m.nc, nf = m.nf, nU = 5 * (size_t)fn->nsp * nc;
+    T.U0.alloc(nU); T.P0.alloc(nf); T.U1.alloc(nU); T.P1.alloc(nf); T.Ut2.alloc(nU);
+    T.fl1.alloc(fn->nsp * nc); T.fl2.alloc(fn->nsp * nc);
+    for (auto &f : T.sf)
+    {
+        f.W.alloc(fn->st->W.n); f.G.alloc(fn->st->grad.n); f.up.alloc(3 * nc); f.bind.alloc(3 * nc); f.btot.alloc(3 * nc);
+    }
+}
+
+// one step from (T.U0, T.P0), recording both stages' inputs, floor flags and fields; the step's result
+// (the SSP-RK2 average) goes to (Uout, Pout).  Bit-identical to the plain step.
+void record_step(MhdFn *fn, MhdFn::TapeStep &T, double *Uout, double *Pout)
+{
+    MhdState *st = fn->st;
+    const MeshView &m = st->mesh->v;
+    cudaStream_t s = stream_of(fn);
+    const size_t nU = 5 * (size_t)fn->nsp * m.nc, nf = m.nf;
+    swap_fields(st, T.sf[0]);
+    st->floor_flags = T.fl1.p;
+    fp64_stage(st, T.U0.p, T.P0.p, T.U1.p, T.P1.p, false);
+    swap_fields(st, T.sf[0]);
+    swap_fields(st, T.sf[1]);
+    st->floor_flags = T.fl2.p;
+    fp64_stage(st, T.U1.p, T.P1.p, T.Ut2.p, st->phi1.p, false);
+    swap_fields(st, T.sf[1]);
+    st->floor_flags = nullptr;
+    copy_d(Uout, T.U0.p, nU, s);
+    copy_d(Pout, T.P0.p, nf, s);
+    if (nU) k_average<<<g256(nU), 256, 0, s>>>(nU, T.Ut2.p, Uout, nullptr, nullptr);
+    if (nf) k_average<<<g256(nf), 256, 0, s>>>(nf, st->phi1.p, Pout, nullptr, nullptr);
+    MHD_LAUNCH_CHECK();
+}
+
+// steps [n0, n1) from (U, P), recorded in the tape; the result of the last goes to (Uend, Pend)
+void record_segment(MhdFn *fn, int n0, int n1, const double *U, const double *P, double *Uend, double *Pend)
+{
+    MhdState *st = fn->st;
+    const MeshView &m = st->mesh->v;
+    cudaStream_t s = stream_of(fn);
+    const size_t nU = 5 * (size_t)fn->nsp * m.nc;
+    while ((int)fn->tape.size() < n1 - n0) fn->tape.emplace_back(new MhdFn::TapeStep);
+    for (int n = n0; n < n1; ++n) alloc_step(fn, *fn->tape[n - n0]);
+    copy_d(fn->tape[0]->U0.p, U, nU, s);
+    copy_d(fn->tape[0]->P0.p, P, m.nf, s);
+    for (int n = n0; n < n1; ++n)
+    {
+        MhdFn::TapeStep &T = *fn->tape[n - n0];
+        const bool last = n + 1 == n1;
+        record_step(fn, T, last ? Uend : fn->tape[n + 1 - n0]->U0.p, last ? Pend : fn->tape[n + 1 - n0]->P0.p);
+    }
 }
 
 void alloc_adjoint(MhdFn *fn)
@@ -1764,7 +1906,11 @@ int mhd_gpu_fn_forward(MhdFn *fn, double *J)
             fn->ckU.emplace_back(new DBuf<double>);
             fn->ckP.emplace_back(new DBuf<double>);
         }
-        for (int n = 0; n < N; ++n)
+        // every segment but the last runs plain steps after its checkpoint; the last is recorded for the
+        // backward sweep as it runs
+        const int last_seg = (N - 1) / K;
+        fn->prof.begin(FN_FORWARD, s);
+        for (int n = 0; n < last_seg * K; ++n)
         {
             if (n % K == 0)
             {
@@ -1776,6 +1922,15 @@ int mhd_gpu_fn_forward(MhdFn *fn, double *J)
             }
             plain_step(fn);
         }
+        fn->ckU[last_seg]->alloc(nU);
+        fn->ckP[last_seg]->alloc(nf);
+        copy_d(fn->ckU[last_seg]->p, st->U0.p, nU, s);
+        copy_d(fn->ckP[last_seg]->p, st->phi0.p, nf, s);
+        fn->prof.end(FN_FORWARD, s);
+        fn->prof.begin(FN_RECORD, s);
+        record_segment(fn, last_seg * K, N, st->U0.p, st->phi0.p, st->U0.p, st->phi0.p);
+        fn->prof.end(FN_RECORD, s);
+        fn->tape_seg = last_seg;
         functional(fn, st->phi0.p, nullptr, J, nullptr);
         fn->forward_done = true;
     });
@@ -1806,55 +1961,42 @@ int mhd_gpu_fn_backward(MhdFn *fn, double *grad_eta, double *grad_u)
         if (nf) k_a_recon_faces<<<g256(nf), 256, 0, s>>>(m, fn->y.p, fn->lP.p);
         MHD_LAUNCH_CHECK();
         const int K = fn->prm.checkpoint_every, N = fn->prm.n_steps;
-        while ((int)fn->tape.size() < K) fn->tape.emplace_back(new MhdFn::TapeStep);
         const double dt = fn->prm.dt;
         for (int seg = (N - 1) / K; seg >= 0; --seg)
         {
             const int n0 = seg * K, n1 = std::min(N, n0 + K);
-            // recompute the segment, recording the stage inputs, U~ of stage 2 and the floor flags
-            for (int n = n0; n < n1; ++n)
+            if (fn->tape_seg != seg)
             {
-                MhdFn::TapeStep &T = *fn->tape[n - n0];
-                T.U0.alloc(nU); T.P0.alloc(nf); T.U1.alloc(nU); T.P1.alloc(nf); T.Ut2.alloc(nU);
-                T.fl1.alloc(fn->nsp * (size_t)nc); T.fl2.alloc(fn->nsp * (size_t)nc);
-                if (n == n0)
-                {
-                    copy_d(T.U0.p, fn->ckU[seg]->p, nU, s);
-                    copy_d(T.P0.p, fn->ckP[seg]->p, nf, s);
-                }
-                st->floor_flags = T.fl1.p;
-                fp64_stage(st, T.U0.p, T.P0.p, T.U1.p, T.P1.p, false);
-                st->floor_flags = T.fl2.p;
-                fp64_stage(st, T.U1.p, T.P1.p, T.Ut2.p, st->phi1.p, false);
-                st->floor_flags = nullptr;
-                if (n + 1 < n1)
-                {
-                    MhdFn::TapeStep &Nx = *fn->tape[n + 1 - n0];
-                    Nx.U0.alloc(nU); Nx.P0.alloc(nf);
-                    copy_d(Nx.U0.p, T.U0.p, nU, s);
-                    copy_d(Nx.P0.p, T.P0.p, nf, s);
-                    if (nU) k_average<<<g256(nU), 256, 0, s>>>(nU, T.Ut2.p, Nx.U0.p, nullptr, nullptr);
-                    if (nf) k_average<<<g256(nf), 256, 0, s>>>(nf, st->phi1.p, Nx.P0.p, nullptr, nullptr);
-                    MHD_LAUNCH_CHECK();
-                }
+                // recompute the segment from its checkpoint, recording it (the end state is not needed)
+                fn->prof.begin(FN_RECORD, s);
+                fn->phiscratch.alloc(nf);
+                record_segment(fn, n0, n1, fn->ckU[seg]->p, fn->ckP[seg]->p, st->U1.p, fn->phiscratch.p);
+                fn->prof.end(FN_RECORD, s);
+                fn->tape_seg = seg;
             }
             for (int n = n1 - 1; n >= n0; --n)
             {
                 MhdFn::TapeStep &T = *fn->tape[n - n0];
                 // stage 2: U = (U0 + U~2)/2, Phi = (Phi0 + Phi1 - dt d1 E1)/2
+                fn->prof.begin(FN_ADJ_MISC, s);
                 if (nU) k_scale2<<<g256(nU), 256, 0, s>>>(nU, fn->lU.p, 0.5, fn->lUt.p, 0.5, fn->lU.p);
                 if (m.ne) k_a_ct<<<g256(m.ne), 256, 0, s>>>(m, fn->active.p, fn->lP.p, 0.5 * dt, fn->lE.p);
                 if (nf) k_scale2<<<g256(nf), 256, 0, s>>>(nf, fn->lP.p, 0.5, fn->lP1.p, 0.5, fn->lP.p);
                 MHD_LAUNCH_CHECK();
                 fill_zero(fn->lU1, s);
-                recompute_inputs(fn, T.U1.p, T.P1.p);
+                fn->prof.end(FN_ADJ_MISC, s);
+                swap_fields(st, T.sf[1]);
                 adjoint_stage(fn, T.U1.p, T.P1.p, T.Ut2.p, T.fl2.p, fn->lUt.p, fn->lU1.p, fn->lP1.p);
+                swap_fields(st, T.sf[1]);
                 // stage 1: U1 = U~1, Phi1 = Phi0 - dt d1 E0
+                fn->prof.begin(FN_ADJ_MISC, s);
                 if (m.ne) k_a_ct<<<g256(m.ne), 256, 0, s>>>(m, fn->active.p, fn->lP1.p, dt, fn->lE.p);
                 if (nf) k_axpy<<<g256(nf), 256, 0, s>>>(nf, 1.0, fn->lP1.p, fn->lP.p);
                 MHD_LAUNCH_CHECK();
-                recompute_inputs(fn, T.U0.p, T.P0.p);
+                fn->prof.end(FN_ADJ_MISC, s);
+                swap_fields(st, T.sf[0]);
                 adjoint_stage(fn, T.U0.p, T.P0.p, T.U1.p, T.fl1.p, fn->lU1.p, fn->lU.p, fn->lP.p);
+                swap_fields(st, T.sf[0]);
             }
         }
         if (fn->prm.uniform_flow && nc)
@@ -1884,6 +2026,7 @@ int mhd_gpu_fn_tangent(MhdFn *fn, const double *d_eta, const double *d_u, double
         initial_state(fn, fn->tU[0].p, fn->tP[0].p, d_u, fn->dU[0].p);
         fill_zero(fn->dP[0], s);
         fill_zero(fn->dP[2], s);
+        fn->prof.begin(FN_TANGENT, s);
         for (int n = 0; n < fn->prm.n_steps; ++n)
         {
             tangent_stage(fn, TanBufs{fn->tU[0].p, fn->dU[0].p, fn->tP[0].p, fn->dP[0].p, fn->tU[1].p, fn->dU[1].p, fn->tP[1].p, fn->dP[1].p},
@@ -1899,6 +2042,7 @@ int mhd_gpu_fn_tangent(MhdFn *fn, const double *d_eta, const double *d_u, double
             std::swap(fn->tP[0].p, fn->tP[2].p);
             std::swap(fn->dP[0].p, fn->dP[2].p);
         }
+        fn->prof.end(FN_TANGENT, s);
         functional(fn, fn->tP[0].p, fn->dP[0].p, J, dJ);
         // the final state of the tangent run's values, for comparison with the forward run
         copy_d(st->U0.p, fn->tU[0].p, nU, s);
@@ -1964,6 +2108,32 @@ int mhd_gpu_fn_stage_adjoint(MhdFn *fn, const double *U, const double *Phi, cons
         MHD_CUDA(cudaMemcpyAsync(lPhi, fn->lP.p, nf * sizeof(double), cudaMemcpyDeviceToHost, s));
         fn->tape.pop_back();
         finish_gradient(fn, l_eta, l_u);
+    });
+}
+
+int mhd_gpu_fn_profile(MhdFn *fn, int32_t enable)
+{
+    return guarded([&] {
+        MHD_REQUIRE(fn, "null function");
+        MHD_CUDA(cudaStreamSynchronize(stream_of(fn)));
+        fn->prof.on = enable != 0;
+        for (auto &u : fn->prof.used) u = 0;
+    });
+}
+
+int mhd_gpu_fn_profile_read(MhdFn *fn, int32_t max_kernels, char *names, double *ms_total, int64_t *count, int32_t *n_out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(fn && names && ms_total && count && n_out, "null argument");
+        MHD_CUDA(cudaStreamSynchronize(stream_of(fn)));
+        int n = 0;
+        for (int k = 0; k < FN_COUNT && n < max_kernels; ++k, ++n)
+        {
+            std::strncpy(names + 32 * n, kFnKernelNames[k], 31);
+            names[32 * n + 31] = 0;
+            fn->prof.read(k, ms_total[n], count[n]);
+        }
+        *n_out = n;
     });
 }
 

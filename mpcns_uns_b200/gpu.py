@@ -107,6 +107,8 @@ _SIGS = {
     "mhd_gpu_fn_tangent": ([vp, vp, vp, ctypes.POINTER(dbl), ctypes.POINTER(dbl)], ctypes.c_int),
     "mhd_gpu_fn_stage_tangent": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_fn_stage_adjoint": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_fn_profile": ([vp, i32], ctypes.c_int),
+    "mhd_gpu_fn_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
 }
 
 
@@ -525,6 +527,13 @@ class DeviceFunction:
         dE = np.empty(self.n_edges)
         check(lib().mhd_gpu_fn_stage_tangent(self._h, *[_vp(x) for x in a], _vp(de), _vp(du), _vp(dUt), _vp(dE)))
         return dUt, dE
+
+    def profile(self, enable=True):
+        check(lib().mhd_gpu_fn_profile(self._h, int(bool(enable))))
+
+    def profile_read(self):
+        """{kernel class: (summed ms, launches)} since the last read (synchronises)."""
+        return _read_profile(lib().mhd_gpu_fn_profile_read, self._h)
 
     def stage_adjoint(self, U, Phi, lUt, lE):
         """Adjoints of one stage's inputs (U, Phi, eta, u_inf) from those of its U~ and E."""
