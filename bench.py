@@ -469,6 +469,7 @@ def main():
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint section and print it as its own JSON line")
     ap.add_argument("--adj-ncube", type=int, default=32)
     ap.add_argument("--adj-nr", type=int, default=64)
     ap.add_argument("--adj-steps", type=int, default=40)
@@ -503,6 +504,10 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
+    if args.adjoint_only:
+        if rank == 0:
+            print(json.dumps({"adjoint": bench_adjoint(args)}))
+        return
     dist = None
     if world > 1:
         import datetime

@@ -645,7 +645,7 @@ __global__ void __launch_bounds__(128) k_a_floors(MeshView m, FluidParams p, con
 // the inflow edge value (lpar[0..2] += t lE), and the reverse of edge_uct: lc = lE (the central part, gathered by
 // the faces), efphi per e2f entry (the upwind part's Phi_ind derivative), lup (atomic) through a_ef.
 template <int MAXV>
-__global__ void __launch_bounds__(128) k_a_edge(MeshView m, const double *__restrict__ u, const double *__restrict__ phi, double cuct,
+__global__ void __launch_bounds__(128, 4) k_a_edge(MeshView m, const double *__restrict__ u, const double *__restrict__ phi, double cuct,
                                                  const double *__restrict__ mres, const double *__restrict__ lE, double *__restrict__ lc,
                                                  double *__restrict__ efphi, double *__restrict__ lres, double *__restrict__ lm,
                                                  double *__restrict__ lpar, double *__restrict__ lup)
@@ -1067,7 +1067,7 @@ __global__ void __launch_bounds__(128) k_a_flux(MeshView m, FluidParams p, const
 // slot[((s*4 + j)*5 + q)*nc + c] receives the adjoint of neighbour j's primitive q as this cell's stencil saw it.
 // Every loop over the four slots and five variables is unrolled and the winning slots of the min / max
 // terms are selected by predicates, so the per-thread arrays stay in registers.
-__global__ void __launch_bounds__(128) k_a_grad(MeshView m, FluidParams p, const double *__restrict__ W, const double *__restrict__ G,
+__global__ void __launch_bounds__(128, 3) k_a_grad(MeshView m, FluidParams p, const double *__restrict__ W, const double *__restrict__ G,
                                                  const double *__restrict__ lface, double *__restrict__ lW, double *__restrict__ slot,
                                                  double *__restrict__ lfs)
 {
