@@ -365,6 +365,7 @@ def bench_adjoint(args):
     u0 = np.asarray(wl.u_inf, np.float64)
     d_eta = rng.standard_normal(nc) * case.eta
     d_u = rng.standard_normal(3) * np.linalg.norm(u0)
+    fn.tangent(d_eta, d_u)   # warm-up: allocates the tangent arrays
     tan_ms, (Jt, dJ) = dev_time(lambda: fn.tangent(d_eta, d_u), reps=1)
     adj = float(ge @ d_eta + gu @ d_u)
     dots = [abs(adj - dJ) / abs(dJ)]
