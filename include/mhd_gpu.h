@@ -54,6 +54,9 @@ typedef struct MhdMeshDesc {
     const double *star1, *star2;
     const int8_t *face_kind;               /* 0 Interior 1 Wall 2 Inflow 3 Outflow 4 Skip */
     const int8_t *edge_mode;               /* 0 free 1 wall (E = 0) 2 inflow */
+    /* optional: start and end node of every edge (2 per edge, uns::CellComplex::edge_nodes); with it the
+     * handle builds the node -> fluid-cell lists of mercury::AmbipolarEMF (MercuryUns/physics/Ambipolar.cpp:35-50) */
+    const int32_t *edge_nodes;
 } MhdMeshDesc;
 
 /* Primitive state W = (rho, u, v, w, p) of mhd::Prim (Common/physics/Euler.h:7-10). */
@@ -188,6 +191,14 @@ typedef struct MhdStepParams {
      * mercury::Solver::step, Solver.cpp:492-510).  Zero-initialised parameters leave them off. */
     int32_t lorentz;
     double induce_coeff;
+    /* The rest of add_sources_n (MercurySources.cpp:44-60) and the ambipolar EMF of Solver::rhs
+     * (Solver.cpp:158): ambipolar != 0 adds the electron-pressure force -w_s grad p_e (grad p_e by
+     * mercury::electron_pressure_gradient, Ambipolar.cpp:10-31) and -pressure_coef d0 p_e / n_e,eff to the
+     * edge EMF (AmbipolarEMF::add, :52-88; needs the mesh's edge_nodes); chemistry != 0 adds the drag,
+     * temperature relaxation, thermal drift and Na+ production of the source fields set by
+     * mhd_gpu_state_set_source_fields.  The constants are those of mhd::Scales / Config::chem. */
+    int32_t ambipolar, chemistry;
+    double pressure_coef, a1_Na, a4, a5, a6, state_coeff_H, state_coeff_Na, T_ref, Tn0;
 } MhdStepParams;
 
 /* FP64 reference-exact: every operation rounds as in the reference's host code.
@@ -215,12 +226,24 @@ int mhd_gpu_cfl_dt(MhdState *state, double dt_max, double *host_dt);
  * and makes the call synchronous; with NULL the step is only enqueued (no host round trip). */
 int mhd_gpu_step_rk2(MhdState *state, double dt_fixed, double dt_max, double *dt_used);
 
-/* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part, for species 0 or 1 of
- * the two-ion model (params: n_species 2, mass[0..1], M_ref, ne_floor, inver_MA2, lorentz): rhs += the
- * source on the owned fluid cells.  WH, WNa: primitives (5 per cell); B total field, J current
- * (3 per cell); FP64 in the reference's operation order. */
+/* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63) for species 0 or 1 of the two-ion
+ * model (params: n_species 2, mass[0..1], M_ref, ne_floor, inver_MA2, lorentz, ambipolar, chemistry and
+ * their constants): rhs += the source on the owned fluid cells.  WH, WNa: primitives (5 per cell); B total
+ * field, J current (3 per cell); the SourceFields dpe (grad p_e, 3 per cell), photo and vst (1 per cell)
+ * may be NULL, as in the reference; FP64 in the reference's operation order. */
 int mhd_gpu_add_sources(MhdMesh *mesh, const MhdStepParams *params, int32_t species, const double *WH, const double *WNa,
-                        const double *B, const double *J, double dt, double *rhs);
+                        const double *B, const double *J, const double *dpe, const double *photo, const double *vst, double dt,
+                        double *rhs);
+/* mercury::electron_pressure_gradient (MercuryUns/physics/Ambipolar.cpp:10-31): grad p_e of the owned
+ * fluid cells by Gauss' theorem with face-averaged p_e = p_H + p_Na (3 per cell, zero elsewhere). */
+int mhd_gpu_electron_pressure_gradient(MhdMesh *mesh, const double *WH, const double *WNa, double *dpe);
+/* mercury::AmbipolarEMF::add (Ambipolar.cpp:52-88): E -= pressure_coef (p_b - p_a) / n_e,eff on the owned
+ * edges touching fluid cells (nodal p_e volume-averaged over the node's fluid cells, n_e,eff from the
+ * edge-averaged densities); needs the mesh's edge_nodes. */
+int mhd_gpu_ambipolar_emf(MhdMesh *mesh, const MhdStepParams *params, const double *WH, const double *WNa, double *E);
+/* The external source fields of the chemistry terms (mercury::SourceFields photo and vst, host arrays of
+ * one value per cell; NULL clears a field, which then contributes nothing, as in the reference). */
+int mhd_gpu_state_set_source_fields(MhdState *state, const double *photo, const double *vst);
 /* mercury::gyrate (MercuryUns/physics/Gyration.cpp): exact rotation of the ions' relative velocity
  * about B over dt on the owned fluid cells, UH and UNa (5 per cell) in place; a no-op unless
  * lorentz != 0 and induce_coeff > 0, as in the reference. */

@@ -165,6 +165,10 @@ struct MeshView
     const double *st_wd;     // w * d (3 per c2f entry)
     const double *st_inv;    // 6 per cell: I00 I01 I02 I11 I12 I22 of the symmetric inverse
     const int8_t *st_valid;  // per cell
+    // optional (the mesh descriptor's edge_nodes): start and end node per edge, and per node its fluid
+    // cells in ascending order (mercury::AmbipolarEMF's node lists); null without edge_nodes
+    const int32_t *e_nodes;
+    const int32_t *n2c_ptr, *n2c_cell;
 };
 
 constexpr int kMaxValence = 32; // faces per edge handled by the UCT edge kernel (checked at mesh creation)
@@ -232,7 +236,7 @@ struct MhdMesh
     mhd::DBuf<int8_t> c2f_sgn, f2e_sgn, e2f_sgn, f2c_sgn, material, face_kind, edge_mode, st_valid, cfa_sgn;
     mhd::DBuf<double> edge_vec, edge_mid, edge_len, face_area, face_center, face_area_mag, cell_center, cell_volume, ec_weight,
         ef_weight, star1, star2, st_wd, st_inv, st_dx, t_wd, t_dx, t_inv;
-    mhd::DBuf<int32_t> t_nb;
+    mhd::DBuf<int32_t> t_nb, e_nodes, n2c_ptr, n2c_cell;
     mhd::DBuf<int8_t> t_sg;
     // scratch reused across calls (stream ordered): face fluxes, face EMF candidates, reductions
     mhd::DBuf<double> scratch_face, scratch_face3, scratch_red;

@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__re
 template <int MAXV>
 __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                           const double *__restrict__ phi_ind, double cuct, V3 E_inf,
-                                                          const double *__restrict__ mres, double *__restrict__ E)
+                                                          const double *__restrict__ mres, AmbArgs amb, double *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
@@ -153,6 +153,13 @@ __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const do
         {
             double v;
             if (edge_uct<MAXV>(m, e, Ef, u, phi_ind, cuct, v)) val += v;
+            // AmbipolarEMF::add (Ambipolar.cpp:69-87) after the ideal EMF; on wall and inflow edges the
+            // reference overwrites it with the boundary value
+            if (amb.on)
+            {
+                const int64_t nc = m.nc;
+                if (ambipolar_edge(m, amb.p, e, [&](int32_t c, int s) { return amb.W[(s * 5) * nc + c]; }, amb.pn, amb.pok, v)) val -= v;
+            }
         }
         if (mres) val += mres[e] * resistive_p0(m, phi_ind, e) + 0.0 + 0.0;
     }
@@ -168,11 +175,11 @@ void launch_face_candidate(const MeshView &m, const double *u, const double *Bt,
 }
 
 void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
-                            double *E, cudaStream_t s, const double *mres)
+                            double *E, cudaStream_t s, const double *mres, const AmbArgs &amb)
 {
     if (!m.ne) return;
-    if (m.max_valence <= 8) k_edge_emf_assign<8><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, E);
-    else k_edge_emf_assign<kMaxValence><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, E);
+    if (m.max_valence <= 8) k_edge_emf_assign<8><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E);
+    else k_edge_emf_assign<kMaxValence><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E);
     MHD_LAUNCH_CHECK();
 }
 

@@ -1,7 +1,7 @@
 // Host-side launchers of the hot-path kernels, shared between the translation units that
 // define the kernels and the fused step.
 #pragma once
-#include "fluid.cuh"
+#include "sources.cuh"
 
 namespace mhd
 {
@@ -13,7 +13,8 @@ void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const doub
 void launch_face_candidate(const MeshView &m, const double *u, const double *Bt, const double *Bi, const double *phi_tot,
                            const double *phi_add, double *Ef, cudaStream_t s);
 // E = begin (0) + ideal UCT EMF of the owned edges, then the boundary edge values (wall 0, inflow E_inf . t);
-// mres (per edge, optional): plus the explicit resistive EMF m_e (d1^T star2 phi_ind)_e on the owned edges
+// mres (per edge, optional): plus the explicit resistive EMF m_e (d1^T star2 phi_ind)_e on the owned edges;
+// amb.on: minus the ambipolar EMF on the owned free edges
 void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
-                            double *E, cudaStream_t s, const double *mres = nullptr);
+                            double *E, cudaStream_t s, const double *mres = nullptr, const AmbArgs &amb = AmbArgs{});
 } // namespace mhd

@@ -1,6 +1,7 @@
 // nvcc-flags: -fmad=false
 // Device mesh: upload of one rank's complex, metric and boundary classification, and the
 // one-time derived tables (face -> L/R cells, least-squares stencil of mhd::Stencil).
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -246,6 +247,43 @@ int mhd_gpu_mesh_create(const MhdMeshDesc *d, MhdMesh **out)
         v.cell_center = m->cell_center.p; v.cell_volume = m->cell_volume.p;
         v.ec_ptr = m->ec_ptr.p; v.ec_cell = m->ec_cell.p; v.ec_weight = m->ec_weight.p; v.ef_weight = m->ef_weight.p;
         v.star1 = m->star1.p; v.star2 = m->star2.p;
+        if (d->edge_nodes)
+        {
+            // AmbipolarEMF::AmbipolarEMF (MercuryUns/physics/Ambipolar.cpp:35-50): per node its fluid cells, a
+            // cell's nodes being the sorted end points of its faces' edges (uns::CellComplex::cell_nodes)
+            check_range(d->edge_nodes, 2 * ne, d->n_nodes, "edge_nodes");
+            const int64_t nn = d->n_nodes;
+            std::vector<int32_t> cnt(nn + 1, 0), cn;
+            std::vector<std::pair<int32_t, int32_t>> pr;
+            for (int64_t c = 0; c < nc; ++c)
+            {
+                if (mat[c] == 1) continue;
+                cn.clear();
+                for (int32_t k = c2fp[c]; k < c2fp[c + 1]; ++k)
+                {
+                    const int32_t f = d->c2f_idx[k];
+                    for (int32_t q = f2ep[f]; q < f2ep[f + 1]; ++q)
+                    {
+                        const int32_t e = d->f2e_idx[q];
+                        cn.push_back(d->edge_nodes[2 * (int64_t)e]);
+                        cn.push_back(d->edge_nodes[2 * (int64_t)e + 1]);
+                    }
+                }
+                std::sort(cn.begin(), cn.end());
+                cn.erase(std::unique(cn.begin(), cn.end()), cn.end());
+                for (int32_t nd : cn) pr.emplace_back(nd, static_cast<int32_t>(c));
+            }
+            for (auto &q : pr) ++cnt[q.first + 1];
+            for (int64_t nd = 0; nd < nn; ++nd) cnt[nd + 1] += cnt[nd];
+            std::vector<int32_t> cells(pr.size()), fill(cnt.begin(), cnt.end() - 1);
+            for (auto &q : pr) cells[fill[q.first]++] = q.second;
+            m->e_nodes.upload(d->edge_nodes, 2 * ne);
+            m->n2c_ptr.upload(cnt);
+            m->n2c_cell.upload(cells);
+            v.e_nodes = m->e_nodes.p;
+            v.n2c_ptr = m->n2c_ptr.p;
+            v.n2c_cell = m->n2c_cell.p;
+        }
         MHD_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
         m->own_stream = true;
         MHD_CUDA(cudaMallocHost(&m->pinned, 64 * sizeof(double)));

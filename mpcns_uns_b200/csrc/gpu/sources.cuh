@@ -1,9 +1,11 @@
 // Source terms of the two-ion model, FP64 in the reference's operation order (compiled with
 // -fmad=false wherever they are used):
-//   * the J x B force of mercury::add_sources_n (MercuryUns/fluid/MercurySources.cpp:20-63);
+//   * mercury::add_sources_n (MercuryUns/fluid/MercurySources.cpp:20-63): the J x B force, the
+//     electron-pressure (ambipolar) force and the chemistry terms of the external source fields;
+//   * mercury::electron_pressure_gradient and the ambipolar edge EMF of mercury::AmbipolarEMF
+//     (MercuryUns/physics/Ambipolar.cpp);
 //   * the exact gyration of mercury::gyrate_n (MercuryUns/physics/Gyration.cpp), which the step
 //     applies as half steps around the SSP-RK2 stages (Strang splitting, Solver.cpp:492-510).
-// Chemistry and the ambipolar terms of add_sources_n need external source fields and are not here.
 #pragma once
 #include "fluid.cuh"
 
@@ -16,6 +18,10 @@ struct SrcParams
     double M_ref = 1, mH = 1, mNa = 23; // Scales::M_ref, M_H, M_Na
     double ne_floor = 0.01;             // Scales::ne_floor
     double gamma = 5.0 / 3.0, rho_floor = 1e-10, p_floor = 1e-12;
+    int ambi = 0, chem = 0;             // Config::ambipolar, Config::chemistry
+    double pressure_coef = 0;           // Scales::pressure_coef
+    double a1_Na = 0, a4 = 0, a5 = 0, a6 = 0, sch = 1, scn = 1, T_ref = 1, Tn0 = 0; // Scales, Config::chem.Tn0
+    __host__ __device__ bool any() const { return on || ambi || chem; }
 };
 
 struct NumInfo2
@@ -46,22 +52,108 @@ __device__ __forceinline__ NumInfo2 numinfo2(const SrcParams &p, double rhoH, do
     return n;
 }
 
-// add_sources_n for one owned fluid cell and species s (:29-47): S = inver_MA2 w_s (J x B),
-// rhs_m += S, rhs_E += u.S + dt |S|^2 / (2 rho).  w: primitives of species s; rhoH, rhoNa: the
-// primitive densities of the two ions.
-__device__ __forceinline__ void lorentz_source(const SrcParams &p, int s, double rhoH, double rhoNa, const double *w, V3 J, V3 B,
-                                               double dt, double *r)
+// add_sources_n for one owned fluid cell and species s (:29-60).  w: primitives of species s; rhoH,
+// rhoNa: the primitive densities of the two ions; dpe (grad p_e), photo and vst: the cell's source
+// field values, null where the field is absent.
+//   S = inver_MA2 w_s (J x B) - w_s grad p_e;  rhs_m += S, rhs_E += u.S + dt |S|^2 / (2 rho);
+//   chemistry: drag, temperature relaxation, thermal drift, Na+ production (legacy AddSourceToRHS_Fluid).
+__device__ __forceinline__ void add_sources_cell(const SrcParams &p, int s, double rhoH, double rhoNa, const double *w, V3 J, V3 B,
+                                                 const V3 *dpe, const double *photo, const double *vst, double dt, double *r)
 {
     const NumInfo2 ni = numinfo2(p, rhoH, rhoNa);
-    const double ws = s == 0 ? ni.wH : ni.wNa;
+    const double ns = s == 0 ? ni.nH : ni.nNa, ws = s == 0 ? ni.wH : ni.wNa;
     const double rho = dmax(w[0], 0.0);
     const V3 u = mk(w[1], w[2], w[3]);
     V3 S = mk(0, 0, 0);
     if (p.on) S = S + (p.inver_MA2 * ws) * cross(J, B);
+    if (p.ambi && dpe) S = S - ws * *dpe;
     r[1] += S.x;
     r[2] += S.y;
     r[3] += S.z;
     r[4] += dot(u, S) + (rho > 1e-30 ? 0.5 * dt * dot(S, S) / rho : 0.0);
+    if (p.chem && vst)
+    {
+        const double v = *vst, u2 = dot(u, u);
+        const double Ts = w[4] / (rho > 0 ? rho : 1e-300) / (s == 0 ? p.sch : p.scn) * p.T_ref;
+        const double Msum = p.mH + p.mNa;
+        const double b1 = v * (p.Tn0 - Ts) * (s == 0 ? p.mH / Msum : 0.5);
+        const double b2 = (s == 0 ? p.mNa / Msum : 0.5) * v;
+        r[1] -= p.a4 * rho * u.x * v;
+        r[2] -= p.a4 * rho * u.y * v;
+        r[3] -= p.a4 * rho * u.z * v;
+        r[4] -= p.a4 * rho * u2 * v;
+        r[4] += p.a5 * ns * b1;
+        r[4] += p.a4 * rho * u2 * b2;
+        if (s == 1 && photo)
+        {
+            r[0] += p.a1_Na * *photo;
+            r[4] += p.a6 * *photo * p.Tn0;
+        }
+    }
+}
+
+// mercury::electron_pressure_gradient (Ambipolar.cpp:10-31) of one owned fluid cell: Gauss' theorem with
+// the face-averaged p_e (the mean with the fluid neighbour across an interior face, the cell's own value
+// elsewhere).  pe(c) = p_H + p_Na.
+template <class PE>
+__device__ __forceinline__ V3 electron_pressure_gradient(const MeshView &m, int32_t c, PE pe)
+{
+    V3 sum = mk(0, 0, 0);
+    const double pc = pe(c);
+    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    {
+        const int32_t f = m.c2f_idx[k];
+        double pf = pc;
+        const int32_t b = m.f2c_ptr[f];
+        if (m.f2c_ptr[f + 1] - b == 2)
+        {
+            const int32_t o = m.f2c_idx[b] == c ? m.f2c_idx[b + 1] : m.f2c_idx[b];
+            if (m.material[o] == 0) pf = 0.5 * (pf + pe(o));
+        }
+        sum = sum + (pf * static_cast<double>(m.c2f_sgn[k])) * ld3(m.face_area, f);
+    }
+    const double iv = 1.0 / m.cell_volume[c];
+    return mk(sum.x * iv, sum.y * iv, sum.z * iv);
+}
+
+// nodal p_e of AmbipolarEMF::add (Ambipolar.cpp:57-68): the volume-weighted mean over the node's fluid
+// cells (ascending cell order); ok = the node has fluid cells
+template <class PE>
+__device__ __forceinline__ double node_pressure(const MeshView &m, int32_t v, PE pe, bool &ok)
+{
+    double s = 0, w = 0;
+    const int32_t k0 = m.n2c_ptr[v], k1 = m.n2c_ptr[v + 1];
+    for (int32_t k = k0; k < k1; ++k)
+    {
+        const int32_t c = m.n2c_cell[k];
+        s += m.cell_volume[c] * pe(c);
+        w += m.cell_volume[c];
+    }
+    ok = k1 > k0;
+    return w > 0 ? s / w : 0.0;
+}
+
+// the ambipolar EMF of one owned edge (Ambipolar.cpp:69-87): returns false where the reference adds nothing.
+// rho(c, s): primitive density of species s; pn, pok: nodal p_e and its flag
+template <class RHO>
+__device__ __forceinline__ bool ambipolar_edge(const MeshView &m, const SrcParams &p, int32_t e, RHO rho, const double *__restrict__ pn,
+                                               const int8_t *__restrict__ pok, double &out)
+{
+    double rH = 0, rN = 0, wsum = 0;
+    for (int32_t k = m.ec_ptr[e]; k < m.ec_ptr[e + 1]; ++k)
+    {
+        const int32_t c = m.ec_cell[k];
+        if (m.material[c] == 1) continue;
+        rH += m.ec_weight[k] * rho(c, 0);
+        rN += m.ec_weight[k] * rho(c, 1);
+        wsum += m.ec_weight[k];
+    }
+    if (wsum <= 0) return false;
+    const NumInfo2 ni = numinfo2(p, rH / wsum, rN / wsum);
+    const int32_t a = m.e_nodes[2 * (int64_t)e], b = m.e_nodes[2 * (int64_t)e + 1];
+    if (!pok[a] || !pok[b]) return false;
+    out = p.pressure_coef * (pn[b] - pn[a]) / ni.ne_eff;
+    return true;
 }
 
 // gyrate_n for one owned fluid cell: the relative velocity w = u_H - u_Na turns by
@@ -137,7 +229,21 @@ struct Reprepare
 // the source parameters of a step's parameters (species 0 and 1 are the model's H+ and Na+)
 SrcParams src_params(const MhdStepParams &q);
 
+// inputs of the ambipolar edge EMF in the step's edge kernel (species-major SoA primitives)
+struct AmbArgs
+{
+    int on = 0;
+    SrcParams p;
+    const double *W = nullptr; // W[(s*5 + q)*nc + c]
+    const double *pn = nullptr;
+    const int8_t *pok = nullptr;
+};
+
 // launchers (sources.cu)
+// grad p_e (3 per cell) of species-major SoA primitives, zero outside the owned fluid cells
+void launch_dpe(const MeshView &m, const double *W, double *dpe, cudaStream_t s);
+// nodal p_e and its flag of species-major SoA primitives
+void launch_node_pressure(const MeshView &m, const double *W, double *pn, int8_t *pok, cudaStream_t s);
 // gyrate_n on the owned fluid cells of species 0 and 1 of a species-major SoA state U (5 per cell and
 // species, [(s*5 + m)*nc + c]); the field is B3 (3 doubles per cell) or, if null, B4 (float4 per cell);
 // the angle uses scale * (*dtp).

@@ -42,6 +42,10 @@ struct MhdState
     mhd::DBuf<double> U0, U1, W, grad, F, phi0, phi1, phi_add, badd, bind, btot, up, Ef, E, mass, stage;
     mhd::SrcParams src;     // two-ion J x B force and gyration (off unless params.lorentz)
     mhd::DBuf<double> J;    // cell current of the induced field (3 per cell) when the J x B force is on
+    mhd::DBuf<double> dpe;  // grad p_e (3 per cell) when the ambipolar terms are on
+    mhd::DBuf<double> pn;   // nodal p_e of the ambipolar EMF
+    mhd::DBuf<int8_t> pok;  // the node has fluid cells
+    mhd::DBuf<double> photo, vst; // source fields of the chemistry terms (empty: absent)
     mhd::DBuf<float4> g32;  // mixed precision: face terms A_f x b_f of the cell current (per face)
     mhd::DBuf<double> mres; // explicit resistive EMF: m_e = eta_e / star1_e per edge (empty: off)
     int8_t *floor_flags = nullptr; // when set, the update records the floors it applied ([s*nc + c])

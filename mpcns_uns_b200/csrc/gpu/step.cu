@@ -137,6 +137,7 @@ struct SrcView
     SrcParams p;
     SField<const double> W; // primitives of all species
     const double *J, *Bt;   // cell current of the induced field, total cell field
+    const double *dpe, *photo, *vst; // source fields (null: absent)
 };
 
 // Solver::advance (Solver.cpp:194-206) for one species group: rhs gathered from the face fluxes in the
@@ -196,10 +197,13 @@ __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s
                         r[q] = out ? r[q] - v : r[q] + v;
                     }
                 }
-            if (sv.p.on)
+            if (sv.p.any()) // mercury::add_sources after the flux gather (Solver.cpp:146-149)
             {
                 const double w[5] = {sv.W(s, c, 0), sv.W(s, c, 1), sv.W(s, c, 2), sv.W(s, c, 3), sv.W(s, c, 4)};
-                lorentz_source(sv.p, s, sv.W(0, c, 0), sv.W(1, c, 0), w, ld3(sv.J, c), ld3(sv.Bt, c), dt, r);
+                const V3 d = sv.dpe ? ld3(sv.dpe, c) : mk(0, 0, 0);
+                add_sources_cell(sv.p, s, sv.W(0, c, 0), sv.W(1, c, 0), w, sv.p.on ? ld3(sv.J, c) : mk(0, 0, 0),
+                                 sv.p.on ? ld3(sv.Bt, c) : mk(0, 0, 0), sv.dpe ? &d : nullptr, sv.photo ? sv.photo + c : nullptr,
+                                 sv.vst ? sv.vst + c : nullptr, dt, r);
             }
             for (int q = 0; q < 5; ++q) u[q] += dt * r[q];
             const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
@@ -294,6 +298,12 @@ void prepare_cfl(MhdState *st, const double *Us, const double *phis, bool cfl, d
             launch_cell_current(m, st->bind.p, st->J.p, s);
             ++st->launches;
         }
+        if (st->src.ambi) // grad p_e (Solver.cpp:124) and the nodal p_e of the ambipolar EMF
+        {
+            launch_dpe(m, st->W.p, st->dpe.p, s);
+            launch_node_pressure(m, st->W.p, st->pn.p, st->pok.p, s);
+            st->launches += 1 + (m.nn ? 1 : 0);
+        }
         P.end(KP_PREPARE, s);
     }
     if (cfl)
@@ -320,7 +330,13 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     const int nsp = st->nsp;
     Profiler &P = st->prof;
     if (!prepared) prepare_cfl(st, Us, phis, cfl, dt_max);
-    const SrcView sv{st->src, soa_cstate(st->W.p, nc), st->J.p, st->btot.p};
+    const SrcView sv{st->src,
+                     soa_cstate(st->W.p, nc),
+                     st->J.p,
+                     st->btot.p,
+                     st->src.ambi ? st->dpe.p : nullptr,
+                     st->src.chem && st->photo.n ? st->photo.p : nullptr,
+                     st->src.chem && st->vst.n ? st->vst.p : nullptr};
     for (int s0 = 0; s0 < nsp; s0 += st->group)
     {
         const int ng = std::min(st->group, nsp - s0);
@@ -361,7 +377,13 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     launch_face_candidate(m, st->up.p, st->btot.p, st->bind.p, phis, st->phi_add.p, st->Ef.p, s);
     P.end(KP_FACE_CAND, s);
     P.begin(KP_EDGE_EMF, s);
-    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s, st->mres.n ? st->mres.p : nullptr);
+    AmbArgs amb;
+    amb.on = st->src.ambi;
+    amb.p = st->src;
+    amb.W = st->W.p;
+    amb.pn = st->pn.p;
+    amb.pok = st->pok.p;
+    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s, st->mres.n ? st->mres.p : nullptr, amb);
     P.end(KP_EDGE_EMF, s);
     st->launches += (m.nf ? 1 : 0) + (m.ne ? 1 : 0);
     if (m.nf)
@@ -425,6 +447,11 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         MHD_REQUIRE(p->gamma > 1.0, "gamma must exceed 1");
         for (int s = 0; s < p->n_species; ++s) MHD_REQUIRE(p->mass[s] > 0, "species masses must be positive");
         MHD_REQUIRE(!p->lorentz || p->n_species == 2, "the J x B force and the gyration are those of the two-ion model (n_species == 2)");
+        MHD_REQUIRE(!(p->ambipolar || p->chemistry) || p->n_species == 2,
+                    "the ambipolar and chemistry terms are those of the two-ion model (n_species == 2)");
+        MHD_REQUIRE(!(p->ambipolar || p->chemistry) || p->precision == MHD_PREC_FP64,
+                    "the ambipolar and chemistry terms are part of the FP64 step");
+        MHD_REQUIRE(!p->ambipolar || mesh->v.e_nodes, "the ambipolar EMF needs the mesh's edge_nodes");
         st = new MhdState;
         st->mesh = mesh;
         st->prm = *p;
@@ -465,6 +492,12 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         st->mass.upload(p->mass, st->nsp);
         st->src = src_params(*p);
         if (st->src.on) st->J.alloc(3 * nc);
+        if (st->src.ambi)
+        {
+            st->dpe.alloc(3 * nc);
+            st->pn.alloc(m.nn ? (size_t)m.nn : 1);
+            st->pok.alloc(m.nn ? (size_t)m.nn : 1);
+        }
         MHD_CUDA(cudaMallocHost(&st->pinned, 8 * sizeof(double)));
         MHD_REQUIRE(p->precision == MHD_PREC_FP64 || p->precision == MHD_PREC_MIXED, "unknown precision");
         st->mixed = p->precision == MHD_PREC_MIXED;
@@ -552,6 +585,18 @@ int mhd_gpu_state_download(MhdState *st, int32_t field, int32_t species, double 
         else
             MHD_REQUIRE(false, "unknown field");
         MHD_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+int mhd_gpu_state_set_source_fields(MhdState *st, const double *photo, const double *vst)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st, "null state");
+        const size_t nc = st->mesh->v.nc;
+        if (photo) st->photo.upload(photo, nc);
+        else st->photo.release();
+        if (vst) st->vst.upload(vst, nc);
+        else st->vst.release();
     });
 }
 

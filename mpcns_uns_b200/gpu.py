@@ -33,7 +33,7 @@ class MeshDesc(ctypes.Structure):
                                   "e2f_ptr", "e2f_idx", "e2f_sgn", "f2c_ptr", "f2c_idx", "f2c_sgn", "cell_material",
                                   "edge_vec", "edge_mid", "edge_len", "face_area", "face_center", "face_area_mag",
                                   "cell_center", "cell_volume", "ec_ptr", "ec_cell", "ec_weight", "ef_weight",
-                                  "star1", "star2", "face_kind", "edge_mode")]
+                                  "star1", "star2", "face_kind", "edge_mode", "edge_nodes")]
 
 
 class Prim(ctypes.Structure):
@@ -46,7 +46,9 @@ class StepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
                 ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("cfl", dbl), ("inver_MA2", dbl),
                 ("rho_floor_dt", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", Prim * 16),
-                ("absorb", ctypes.c_int8 * 16), ("precision", i32), ("lorentz", i32), ("induce_coeff", dbl)]
+                ("absorb", ctypes.c_int8 * 16), ("precision", i32), ("lorentz", i32), ("induce_coeff", dbl),
+                ("ambipolar", i32), ("chemistry", i32), ("pressure_coef", dbl), ("a1_Na", dbl), ("a4", dbl), ("a5", dbl),
+                ("a6", dbl), ("state_coeff_H", dbl), ("state_coeff_Na", dbl), ("T_ref", dbl), ("Tn0", dbl)]
 
 
 class InductionParams(ctypes.Structure):
@@ -86,7 +88,10 @@ _SIGS = {
     "mhd_gpu_faraday_edge_dt": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_div_b": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_cell_current": ([vp, vp, vp], ctypes.c_int),
-    "mhd_gpu_add_sources": ([vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_add_sources": ([vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, vp, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_electron_pressure_gradient": ([vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_ambipolar_emf": ([vp, ctypes.POINTER(StepParams), vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_state_set_source_fields": ([vp, vp, vp], ctypes.c_int),
     "mhd_gpu_gyrate": ([vp, ctypes.POINTER(StepParams), vp, dbl, vp, vp], ctypes.c_int),
     "mhd_gpu_induction_create": ([vp, ctypes.POINTER(InductionParams), vp, ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_induction_destroy": ([vp], ctypes.c_int),
@@ -197,6 +202,7 @@ class DeviceMesh:
         d.ec_cell = arr("ec_cell", np.int32)
         d.face_kind = arr("face_kind", np.int8)
         d.edge_mode = arr("edge_mode", np.int8)
+        d.edge_nodes = arr("e2n_idx", np.int32)   # start, end per edge: the ambipolar EMF's node lists
         h = vp()
         torch.cuda.init()
         check(lib().mhd_gpu_mesh_create(ctypes.byref(d), ctypes.byref(h)))
@@ -320,15 +326,35 @@ class DeviceMesh:
         check(lib().mhd_gpu_div_b(self._h, ptr(B), ptr(ex), out.ctypes.data_as(vp)))
         return dict(max_abs=float(out[0]), max_rel=float(out[1]), worst_cell_gid=int(out[2]))
 
-    def add_sources(self, params, species, WH, WNa, B, J, dt, rhs):
-        """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part; returns rhs + source."""
-        WH, WNa, B, J = dev(WH), dev(WNa), dev(B), dev(J)
+    def add_sources(self, params, species, WH, WNa, B, J, dt, rhs, dpe=None, photo=None, vst=None):
+        """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63); returns rhs + source."""
+        WH, WNa = dev(WH), dev(WNa)
+        B, J, dpe, photo, vst = (None if x is None else dev(x) for x in (B, J, dpe, photo, vst))
         rhs = dev(rhs).clone()
         self._enter()
-        check(lib().mhd_gpu_add_sources(self._h, ctypes.byref(params), int(species), ptr(WH), ptr(WNa), ptr(B), ptr(J), float(dt),
-                                         ptr(rhs)))
+        check(lib().mhd_gpu_add_sources(self._h, ctypes.byref(params), int(species), ptr(WH), ptr(WNa), ptr(B), ptr(J), ptr(dpe),
+                                         ptr(photo), ptr(vst), float(dt), ptr(rhs)))
         self._leave()
         return rhs
+
+    def electron_pressure_gradient(self, WH, WNa):
+        """mercury::electron_pressure_gradient (MercuryUns/physics/Ambipolar.cpp:10-31): 3 per cell."""
+        torch = _torch()
+        WH, WNa = dev(WH), dev(WNa)
+        out = torch.empty(3 * self.n_cells, dtype=torch.float64, device="cuda")
+        self._enter()
+        check(lib().mhd_gpu_electron_pressure_gradient(self._h, ptr(WH), ptr(WNa), ptr(out)))
+        self._leave()
+        return out
+
+    def ambipolar_emf(self, params, WH, WNa, E):
+        """mercury::AmbipolarEMF::add (Ambipolar.cpp:52-88): returns E minus the ambipolar EMF."""
+        WH, WNa = dev(WH), dev(WNa)
+        E = dev(E).clone()
+        self._enter()
+        check(lib().mhd_gpu_ambipolar_emf(self._h, ctypes.byref(params), ptr(WH), ptr(WNa), ptr(E)))
+        self._leave()
+        return E
 
     def gyrate(self, params, B, dt, UH, UNa):
         """mercury::gyrate (MercuryUns/physics/Gyration.cpp); returns the updated copies of UH, UNa."""
@@ -352,9 +378,16 @@ class DeviceMesh:
 
 def step_params(n_species, gamma=5.0 / 3.0, fs=None, mass=None, u_inf=(0.0, 0.0, 0.0), B_imf=(0.0, 0.0, 0.0), cuct=0.5,
                 second_order=True, rho_floor=1e-10, p_floor=1e-12, rel_limit=0.0, cfl=0.4, inver_MA2=1.0, rho_floor_dt=1e-2,
-                M_ref=1.0, ne_floor=0.01, absorb=None, precision="fp64", lorentz=False, induce_coeff=0.0):
-    """MhdStepParams with the reference's Config / Scales defaults (Common/config/Config.h:19-96)."""
+                M_ref=1.0, ne_floor=0.01, absorb=None, precision="fp64", lorentz=False, induce_coeff=0.0, extra=None):
+    """MhdStepParams with the reference's Config / Scales defaults (Common/config/Config.h:19-96); extra: the
+    ambipolar and chemistry switches and constants (keys ambipolar, chemistry, pressure_coef, a1_Na, a4, a5, a6,
+    state_coeff_H, state_coeff_Na, T_ref, Tn0)."""
     p = StepParams()
+    p.state_coeff_H = p.state_coeff_Na = p.T_ref = 1.0
+    for k, v in (extra or {}).items():
+        if k in ("photo", "vst"):
+            continue
+        setattr(p, k, int(bool(v)) if k in ("ambipolar", "chemistry") else float(v))
     p.precision = PREC_MIXED if precision == "mixed" else PREC_FP64
     p.lorentz, p.induce_coeff = int(bool(lorentz)), float(induce_coeff)
     p.n_species, p.second_order = int(n_species), int(bool(second_order))
@@ -449,6 +482,11 @@ class ResidentState:
         v = i64()
         check(lib().mhd_gpu_state_launches(self._h, ctypes.byref(v)))
         return v.value
+
+    def set_source_fields(self, photo=None, vst=None):
+        """The chemistry terms' source fields (one value per cell; None: absent)."""
+        a = [None if x is None else np.ascontiguousarray(x, np.float64) for x in (photo, vst)]
+        check(lib().mhd_gpu_state_set_source_fields(self._h, *[None if x is None else x.ctypes.data_as(vp) for x in a]))
 
     def set_resistivity(self, m_edge):
         """Explicit resistive EMF m_e (d1^T star2 Phi)_e per stage (m_edge per edge; None: off)."""

@@ -544,7 +544,7 @@ static OrNumInfo numinfo(const OrStepParams *p, double rhoH, double rhoNa)
 /* mercury::add_sources_n (MercuryUns/fluid/MercurySources.cpp:20-63) with the Lorentz force only:
  * S = inver_MA2 w_s (J x B); rhs_m += S, rhs_E += u.S + dt |S|^2 / (2 rho) (mid-point velocity work) */
 void or_add_sources(const OrMesh *m, const OrStepParams *p, int32_t s, const double *WH, const double *WNa, const double *B,
-                    const double *J, double dt, double *rhs)
+                    const double *J, const double *dpe, const double *photo, const double *vst, double dt, double *rhs)
 {
     const double *W = s == 0 ? WH : WNa;
     for (int32_t c = 0; c < m->n_owned_cells; ++c)
@@ -552,15 +552,145 @@ void or_add_sources(const OrMesh *m, const OrStepParams *p, int32_t s, const dou
         if (m->cell_material[c] == 1) continue;
         const size_t i = (size_t)c;
         const OrNumInfo ni = numinfo(p, WH[5 * i], WNa[5 * i]);
-        const double ws = s == 0 ? ni.wH : ni.wNa;
+        const double ns = s == 0 ? ni.nH : ni.nNa, ws = s == 0 ? ni.wH : ni.wNa;
         const double rho = dmax(W[5 * i], 0.0);
         const v3 u = mk3(W[5 * i + 1], W[5 * i + 2], W[5 * i + 3]);
         double *r = rhs + 5 * i;
         v3 S = mk3(0, 0, 0);
         if (p->lorentz) S = add3(S, scl(p->inver_MA2 * ws, cross3(ld(J, c), ld(B, c))));
+        if (p->ambipolar && dpe) S = sub3(S, scl(ws, ld(dpe, c)));
         r[1] += S.x; r[2] += S.y; r[3] += S.z;
         r[4] += dot3(u, S) + (rho > 1e-30 ? 0.5 * dt * dot3(S, S) / rho : 0.0);
+        if (p->chemistry && vst)
+        {
+            /* drag, temperature relaxation, thermal drift, Na+ production (MercurySources.cpp:48-60) */
+            const double v = vst[i], u2 = dot3(u, u);
+            const double Ts = W[5 * i + 4] / (rho > 0 ? rho : 1e-300) / (s == 0 ? p->state_coeff_H : p->state_coeff_Na) * p->T_ref;
+            const double Msum = p->mass[0] + p->mass[1];
+            const double b1 = v * (p->Tn0 - Ts) * (s == 0 ? p->mass[0] / Msum : 0.5);
+            const double b2 = (s == 0 ? p->mass[1] / Msum : 0.5) * v;
+            r[1] -= p->a4 * rho * u.x * v; r[2] -= p->a4 * rho * u.y * v; r[3] -= p->a4 * rho * u.z * v;
+            r[4] -= p->a4 * rho * u2 * v;
+            r[4] += p->a5 * ns * b1;
+            r[4] += p->a4 * rho * u2 * b2;
+            if (s == 1 && photo)
+            {
+                r[0] += p->a1_Na * photo[i];
+                r[4] += p->a6 * photo[i] * p->Tn0;
+            }
+        }
     }
+}
+
+static double pe_of(const double *WH, const double *WNa, int32_t c) { return WH[5 * (size_t)c + 4] + WNa[5 * (size_t)c + 4]; }
+
+void or_electron_pressure_gradient(const OrMesh *m, const double *WH, const double *WNa, double *dpe)
+{
+    memset(dpe, 0, 3 * sizeof(double) * (size_t)m->n_cells);
+    for (int32_t c = 0; c < m->n_owned_cells; ++c)
+    {
+        if (m->cell_material[c] == 1) continue;
+        v3 sum = mk3(0, 0, 0);
+        for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+        {
+            const int32_t f = m->c2f_idx[k];
+            double pf = pe_of(WH, WNa, c);
+            const int64_t b = m->f2c_ptr[f];
+            if (m->f2c_ptr[f + 1] - b == 2)
+            {
+                const int32_t o = m->f2c_idx[b] == c ? m->f2c_idx[b + 1] : m->f2c_idx[b];
+                if (m->cell_material[o] == 0) pf = 0.5 * (pf + pe_of(WH, WNa, o));
+            }
+            sum = add3(sum, scl(pf * (double)m->c2f_sgn[k], ld(m->face_area, f)));
+        }
+        const double iv = 1.0 / m->cell_volume[c];
+        dpe[3 * (size_t)c] = sum.x * iv; dpe[3 * (size_t)c + 1] = sum.y * iv; dpe[3 * (size_t)c + 2] = sum.z * iv;
+    }
+}
+
+static int cmp_i32(const void *a, const void *b)
+{
+    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+void or_ambipolar_emf(const OrMesh *m, const OrStepParams *p, const double *WH, const double *WNa, double *E)
+{
+    const int32_t nn = m->n_nodes, nc = m->n_cells;
+    /* per node its fluid cells, ascending: a cell's nodes are the sorted end points of its faces' edges */
+    int64_t *cnt = (int64_t *)calloc((size_t)nn + 1, sizeof(int64_t));
+    int64_t npairs = 0;
+    int32_t buf[512];
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        int32_t *cells = NULL;
+        int64_t *fill = NULL;
+        if (pass == 1)
+        {
+            for (int32_t v = 0; v < nn; ++v) cnt[v + 1] += cnt[v];
+            npairs = cnt[nn];
+            cells = (int32_t *)malloc(sizeof(int32_t) * (size_t)(npairs > 0 ? npairs : 1));
+            fill = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nn > 0 ? nn : 1));
+            for (int32_t v = 0; v < nn; ++v) fill[v] = cnt[v];
+        }
+        for (int32_t c = 0; c < nc; ++c)
+        {
+            if (m->cell_material[c] == 1) continue;
+            int n = 0;
+            for (int64_t k = m->c2f_ptr[c]; k < m->c2f_ptr[c + 1]; ++k)
+            {
+                const int32_t f = m->c2f_idx[k];
+                for (int64_t q = m->f2e_ptr[f]; q < m->f2e_ptr[f + 1] && n + 2 <= 512; ++q)
+                {
+                    buf[n++] = m->edge_nodes[2 * (size_t)m->f2e_idx[q]];
+                    buf[n++] = m->edge_nodes[2 * (size_t)m->f2e_idx[q] + 1];
+                }
+            }
+            qsort(buf, (size_t)n, sizeof(int32_t), cmp_i32);
+            for (int i = 0; i < n; ++i)
+            {
+                if (i > 0 && buf[i] == buf[i - 1]) continue;
+                if (pass == 0) ++cnt[buf[i] + 1];
+                else cells[fill[buf[i]]++] = c;
+            }
+        }
+        if (pass == 1)
+        {
+            double *pn = (double *)malloc(sizeof(double) * (size_t)(nn > 0 ? nn : 1));
+            for (int32_t v = 0; v < nn; ++v)
+            {
+                double sp = 0, w = 0;
+                for (int64_t k = cnt[v]; k < cnt[v + 1]; ++k)
+                {
+                    const int32_t cc = cells[k];
+                    sp += m->cell_volume[cc] * pe_of(WH, WNa, cc);
+                    w += m->cell_volume[cc];
+                }
+                pn[v] = w > 0 ? sp / w : 0.0;
+            }
+            for (int32_t e = 0; e < m->n_owned_edges; ++e)
+            {
+                double rH = 0, rN = 0, wsum = 0;
+                for (int64_t k = m->ec_ptr[e]; k < m->ec_ptr[e + 1]; ++k)
+                {
+                    const int32_t cc = m->ec_cell[k];
+                    if (m->cell_material[cc] == 1) continue;
+                    rH += m->ec_weight[k] * WH[5 * (size_t)cc];
+                    rN += m->ec_weight[k] * WNa[5 * (size_t)cc];
+                    wsum += m->ec_weight[k];
+                }
+                if (wsum <= 0) continue;
+                const OrNumInfo ni = numinfo(p, rH / wsum, rN / wsum);
+                const int32_t a = m->edge_nodes[2 * (size_t)e], b = m->edge_nodes[2 * (size_t)e + 1];
+                if (cnt[a + 1] == cnt[a] || cnt[b + 1] == cnt[b]) continue;
+                E[e] -= p->pressure_coef * (pn[b] - pn[a]) / ni.ne_eff;
+            }
+            free(pn);
+            free(cells);
+            free(fill);
+        }
+    }
+    free(cnt);
 }
 
 /* mercury::gyrate_n (MercuryUns/physics/Gyration.cpp): w = u_H - u_Na rotated by
@@ -624,8 +754,9 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
     double *E = P2 + nf;
     double *Us[16], *U1s[16], *U2s[16];
     const int lorentz = p->lorentz != 0, split = lorentz && p->induce_coeff > 0;
-    if (lorentz && ns != 2) { free(mem); return -1; }
+    if ((lorentz || p->ambipolar || p->chemistry) && ns != 2) { free(mem); return -1; }
     double *Jc = lorentz ? (double *)malloc(sizeof(double) * 3 * (size_t)(nc > 0 ? nc : 1)) : NULL;
+    double *dpe = p->ambipolar ? (double *)malloc(sizeof(double) * 3 * (size_t)(nc > 0 ? nc : 1)) : NULL;
     for (int s = 0; s < ns; ++s) { Us[s] = U[s]; U1s[s] = U1 + s * c5; U2s[s] = U2 + s * c5; }
     if (split)
     {
@@ -665,13 +796,14 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
             else memset(G + 3 * s * c5, 0, sizeof(double) * 3 * c5);
             or_flux_rhs(m, p->gamma, p->absorb[s], &p->fs[s], W + s * c5, G + 3 * s * c5, R + s * c5);
         }
-        if (lorentz) /* Solver::rhs (Solver.cpp:146-149): J of the induced field, sources after both flux passes */
-        {
-            or_cell_current(m, Bi, Jc);
-            for (int s = 0; s < ns; ++s) or_add_sources(m, p, s, W, W + c5, Bt, Jc, dt, R + s * c5);
-        }
+        if (lorentz) or_cell_current(m, Bi, Jc); /* Solver::prepare (Solver.cpp:123) */
+        if (p->ambipolar) or_electron_pressure_gradient(m, W, W + c5, dpe); /* :124 */
+        if (lorentz || p->ambipolar || p->chemistry) /* Solver::rhs (Solver.cpp:146-149): sources after both flux passes */
+            for (int s = 0; s < ns; ++s)
+                or_add_sources(m, p, s, W, W + c5, Bt, Jc, p->ambipolar ? dpe : NULL, p->photo, p->vst, dt, R + s * c5);
         memset(E, 0, sizeof(double) * (size_t)ne);
         or_ideal_emf(m, up, Bt, Bi, Pt, phis, p->cuct, E);
+        if (p->ambipolar) or_ambipolar_emf(m, p, W, W + c5, E); /* Solver.cpp:158 */
         or_edge_modes(m, p->u_inf, p->B_imf, E);
         if (p->m_res) or_resistive_emf(m, p->m_res, phis, E);
         for (int s = 0; s < ns; ++s)
@@ -693,6 +825,7 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
     /* the closing half step with Btot of the stage-2 input (Solver.cpp:510) */
     if (split) or_gyrate(m, p, Bt, 0.5 * dt, Us[0], Us[1]);
     free(Jc);
+    free(dpe);
     free(mem);
     return 0;
 }
@@ -713,12 +846,6 @@ struct OrInduction
     int32_t *ce_edge;
     double *phi, *bcell, *part, *tmp;
 };
-
-static int cmp_i32(const void *a, const void *b)
-{
-    const int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
-    return (x > y) - (x < y);
-}
 
 OrInduction *or_ind_create(const OrMesh *m, const OrIndParams *p, const double *m_edge)
 {

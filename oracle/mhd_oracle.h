@@ -22,6 +22,7 @@ typedef struct OrMesh {
     const double *edge_vec, *edge_mid, *edge_len, *face_area, *face_center, *face_area_mag, *cell_center, *cell_volume;
     const int64_t *ec_ptr; const int32_t *ec_cell; const double *ec_weight, *ef_weight, *star1, *star2;
     const int8_t *face_kind, *edge_mode;
+    const int32_t *edge_nodes; /* start and end node per edge (uns::CellComplex::edge_nodes), for the ambipolar EMF */
 } OrMesh;
 
 typedef struct OrPrim { double rho, u, v, w, p; } OrPrim;
@@ -57,10 +58,19 @@ typedef struct OrStepParams {
      * ImplicitInduction::apply_F (Common/induction/ImplicitInduction.cpp:133-137, 182) with m_e = eta_e / star1_e
      * (NULL: off) */
     const double *m_res;
+    /* the rest of add_sources_n and the ambipolar EMF: switches, Scales constants, the chemistry's source fields */
+    int32_t ambipolar, chemistry;
+    double pressure_coef, a1_Na, a4, a5, a6, state_coeff_H, state_coeff_Na, T_ref, Tn0;
+    const double *photo, *vst;
 } OrStepParams;
-/* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part, species s: rhs += S */
+/* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), species s: rhs += S; dpe, photo, vst: the
+ * SourceFields (NULL: absent) */
 void or_add_sources(const OrMesh *m, const OrStepParams *p, int32_t s, const double *WH, const double *WNa, const double *B,
-                    const double *J, double dt, double *rhs);
+                    const double *J, const double *dpe, const double *photo, const double *vst, double dt, double *rhs);
+/* mercury::electron_pressure_gradient (MercuryUns/physics/Ambipolar.cpp:10-31) */
+void or_electron_pressure_gradient(const OrMesh *m, const double *WH, const double *WNa, double *dpe);
+/* mercury::AmbipolarEMF (Ambipolar.cpp:35-88): node lists and E -= pressure_coef d0 p_e / n_e,eff, E in place */
+void or_ambipolar_emf(const OrMesh *m, const OrStepParams *p, const double *WH, const double *WNa, double *E);
 /* mercury::gyrate (MercuryUns/physics/Gyration.cpp): exact rotation of the relative ion velocity about B */
 void or_gyrate(const OrMesh *m, const OrStepParams *p, const double *B, double dt, double *UH, double *UNa);
 /* explicit resistive EMF (see OrStepParams.m_res): E_e += m_e (d1^T star2 phi)_e on the owned edges */

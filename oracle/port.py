@@ -23,18 +23,43 @@ class OrMesh(ctypes.Structure):
                [(n, vp) for n in ("c2f_ptr", "c2f_idx", "c2f_sgn", "f2e_ptr", "f2e_idx", "f2e_sgn", "e2f_ptr", "e2f_idx",
                                   "e2f_sgn", "f2c_ptr", "f2c_idx", "f2c_sgn", "cell_material", "edge_vec", "edge_mid",
                                   "edge_len", "face_area", "face_center", "face_area_mag", "cell_center", "cell_volume",
-                                  "ec_ptr", "ec_cell", "ec_weight", "ef_weight", "star1", "star2", "face_kind", "edge_mode")]
+                                  "ec_ptr", "ec_cell", "ec_weight", "ef_weight", "star1", "star2", "face_kind", "edge_mode",
+                                  "edge_nodes")]
 
 
 class OrPrim(ctypes.Structure):
     _fields_ = [("rho", dbl), ("u", dbl), ("v", dbl), ("w", dbl), ("p", dbl)]
 
 
+# Scales / Config::chem constants of the ambipolar and chemistry terms, in the order of the C structs
+SOURCE_CONSTANTS = ("pressure_coef", "a1_Na", "a4", "a5", "a6", "state_coeff_H", "state_coeff_Na", "T_ref", "Tn0")
+
+
+def set_source_terms(p, extra):
+    """Fill the ambipolar / chemistry fields of a step-parameter struct from a dict (switches, constants, and
+    the source fields photo / vst as arrays); returns the arrays the struct points to (keep them alive)."""
+    keep = []
+    if not extra:
+        return keep
+    p.ambipolar = int(bool(extra.get("ambipolar", False)))
+    p.chemistry = int(bool(extra.get("chemistry", False)))
+    for n in SOURCE_CONSTANTS:
+        setattr(p, n, float(extra.get(n, 1.0 if n.startswith("state_coeff") or n == "T_ref" else 0.0)))
+    for n in ("photo", "vst"):
+        a = extra.get(n)
+        if a is not None:
+            a = np.ascontiguousarray(a, np.float64)
+            keep.append(a)
+            setattr(p, n, a.ctypes.data)
+    return keep
+
+
 class OrStepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl), ("cuct", dbl),
                 ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("u_inf", dbl * 3), ("B_imf", dbl * 3),
                 ("mass", dbl * 16), ("fs", OrPrim * 16), ("absorb", ctypes.c_int8 * 16), ("lorentz", i32),
-                ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p)]
+                ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p), ("ambipolar", i32), ("chemistry", i32)] + \
+               [(n, dbl) for n in SOURCE_CONSTANTS] + [("photo", ctypes.c_void_p), ("vst", ctypes.c_void_p)]
 
 
 class OrIndParams(ctypes.Structure):
@@ -65,7 +90,9 @@ def lib():
             ("or_cell_current", [P(OrMesh), vp, vp], None),
             ("or_local_time_step", [P(OrMesh), i32, vp, vp, dbl, dbl, dbl, dbl], dbl),
             ("or_rk2_step", [P(OrMesh), P(OrStepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
-            ("or_add_sources", [P(OrMesh), P(OrStepParams), i32, vp, vp, vp, vp, dbl, vp], None),
+            ("or_add_sources", [P(OrMesh), P(OrStepParams), i32, vp, vp, vp, vp, vp, vp, vp, dbl, vp], None),
+            ("or_electron_pressure_gradient", [P(OrMesh), vp, vp, vp], None),
+            ("or_ambipolar_emf", [P(OrMesh), P(OrStepParams), vp, vp, vp], None),
             ("or_gyrate", [P(OrMesh), P(OrStepParams), vp, dbl, vp, vp], None),
             ("or_ind_create", [P(OrMesh), P(OrIndParams), vp], vp),
             ("or_ind_free", [vp], None),
@@ -100,6 +127,11 @@ class PortMesh:
         d.n_nodes, d.n_edges, d.n_faces, d.n_cells = h.n_nodes, h.n_edges, h.n_faces, h.n_cells
         d.n_owned_cells, d.n_owned_edges = h.n_cells, h.n_edges
         for name, _ in OrMesh._fields_[6:]:
+            if name == "edge_nodes":
+                a = np.ascontiguousarray(np.asarray(h["e2n_idx"]).ravel(), np.int32)
+                self._keep[name] = a
+                d.edge_nodes = ctypes.c_void_p(a.ctypes.data)
+                continue
             if name in ("cell_material",):
                 dt = np.int32
             elif name in ("face_kind", "edge_mode"):
@@ -194,19 +226,34 @@ class PortMesh:
         p.lorentz, p.induce_coeff, p.inver_MA2 = int(bool(lorentz)), float(induce_coeff), float(inver_MA2)
         return p
 
-    def add_sources(self, p, species, WH, WNa, B, J, dt, rhs):
-        """mercury::add_sources, J x B part (oracle restatement); rhs in place."""
-        lib().or_add_sources(self.ref, ctypes.byref(p), species, _p(_f(WH)), _p(_f(WNa)), _p(_f(B)), _p(_f(J)), dt, _p(rhs))
+    def add_sources(self, p, species, WH, WNa, B, J, dt, rhs, dpe=None, photo=None, vst=None):
+        """mercury::add_sources (oracle restatement); rhs in place."""
+        opt = [None if x is None else _f(x) for x in (B, J, dpe, photo, vst)]
+        lib().or_add_sources(self.ref, ctypes.byref(p), species, _p(_f(WH)), _p(_f(WNa)), *[_p(x) for x in opt], dt, _p(rhs))
+
+    def electron_pressure_gradient(self, WH, WNa):
+        out = np.zeros(3 * self.n_cells)
+        lib().or_electron_pressure_gradient(self.ref, _p(_f(WH)), _p(_f(WNa)), _p(out))
+        return out
+
+    def ambipolar_emf(self, p, WH, WNa, E):
+        """E minus the ambipolar EMF (a new array)."""
+        E = np.array(E, np.float64)
+        lib().or_ambipolar_emf(self.ref, ctypes.byref(p), _p(_f(WH)), _p(_f(WNa)), _p(E))
+        return E
 
     def gyrate(self, p, B, dt, UH, UNa):
         """mercury::gyrate (oracle restatement); UH, UNa in place."""
         lib().or_gyrate(self.ref, ctypes.byref(p), _p(_f(B)), dt, _p(UH), _p(UNa))
 
-    def rk2_step(self, wl, U_list, Phi, Badd, dt, absorb=None, lorentz=False, induce_coeff=0.0, inver_MA2=1.0, m_res=None):
+    def rk2_step(self, wl, U_list, Phi, Badd, dt, absorb=None, lorentz=False, induce_coeff=0.0, inver_MA2=1.0, m_res=None,
+                 extra=None):
         """One SSP-RK2 step of the hot path for a Workload's parameters; U_list and Phi updated in place.
         With lorentz: the J x B source and (induce_coeff > 0) the Strang-split gyration of the two-ion model;
-        with m_res (per edge): the explicit resistive EMF E_e += m_e (d1^T star2 Phi)_e."""
+        with m_res (per edge): the explicit resistive EMF E_e += m_e (d1^T star2 Phi)_e; extra: the ambipolar
+        and chemistry terms (set_source_terms)."""
         p = self.step_params(wl, absorb, lorentz, induce_coeff, inver_MA2)
+        keep = set_source_terms(p, extra)
         mr = None if m_res is None else _f(m_res)
         p.m_res = None if mr is None else mr.ctypes.data
         arr = (ctypes.c_void_p * len(U_list))(*[u.ctypes.data for u in U_list])

@@ -32,7 +32,9 @@ class StepParams(ctypes.Structure):
     _fields_ = [("n_species", i32), ("second_order", i32), ("gamma", dbl), ("rho_floor", dbl), ("p_floor", dbl),
                 ("cuct", dbl), ("M_ref", dbl), ("ne_floor", dbl), ("rel_limit", dbl), ("u_inf", dbl * 3),
                 ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", (dbl * 5) * 16), ("lorentz", i32), ("pad", i32),
-                ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p)]
+                ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p), ("ambipolar", i32), ("chemistry", i32),
+                ("pressure_coef", dbl), ("a1_Na", dbl), ("a4", dbl), ("a5", dbl), ("a6", dbl), ("state_coeff_H", dbl),
+                ("state_coeff_Na", dbl), ("T_ref", dbl), ("Tn0", dbl), ("photo", ctypes.c_void_p), ("vst", ctypes.c_void_p)]
 
 
 def lib():
@@ -73,7 +75,9 @@ def lib():
             ("ref_ind_apply_A", [vp, vp, dbl, vp], None),
             ("ref_ind_solve", [vp, vp, vp, vp, dbl, i32, vp, vp], i32),
             ("ref_rk2_step", [vp, ctypes.POINTER(StepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
-            ("ref_add_sources", [vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, dbl, vp], None),
+            ("ref_add_sources", [vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp], None),
+            ("ref_electron_pressure_gradient", [vp, vp, vp, vp], None),
+            ("ref_ambipolar_emf", [vp, ctypes.POINTER(StepParams), vp, vp, vp], None),
             ("ref_gyrate", [vp, ctypes.POINTER(StepParams), vp, dbl, vp, vp], None),
         ]:
             f = getattr(L, name)
@@ -278,10 +282,24 @@ class RefMesh:
         arrs = [np.ascontiguousarray(a, np.float64) for a in (WH, WNa, B)]
         return lib().ref_local_time_step(self._h, gamma, cfl, inver_MA2, rho_floor_dt, *[_p(a) for a in arrs])
 
-    def add_sources(self, params: StepParams, species, WH, WNa, up, B, J, dt, rhs):
-        """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63), J x B part; rhs in place."""
-        a = [np.ascontiguousarray(x, np.float64) for x in (WH, WNa, up, B, J)]
+    def add_sources(self, params: StepParams, species, WH, WNa, up, B, J, dt, rhs, dpe=None, photo=None, vst=None):
+        """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63); rhs in place."""
+        a = [None if x is None else np.ascontiguousarray(x, np.float64) for x in (WH, WNa, up, B, J, dpe, photo, vst)]
         lib().ref_add_sources(self._h, ctypes.byref(params), species, *[_p(x) for x in a], dt, _p(rhs))
+
+    def electron_pressure_gradient(self, WH, WNa):
+        """mercury::electron_pressure_gradient (MercuryUns/physics/Ambipolar.cpp:10-31)."""
+        WH, WNa = (np.ascontiguousarray(x, np.float64) for x in (WH, WNa))
+        out = np.zeros(3 * (WH.size // 5))
+        lib().ref_electron_pressure_gradient(self._h, _p(WH), _p(WNa), _p(out))
+        return out
+
+    def ambipolar_emf(self, params: StepParams, WH, WNa, E):
+        """mercury::AmbipolarEMF::add (Ambipolar.cpp:52-88): E minus the ambipolar EMF (a new array)."""
+        E = np.array(E, np.float64)
+        WH, WNa = (np.ascontiguousarray(x, np.float64) for x in (WH, WNa))
+        lib().ref_ambipolar_emf(self._h, ctypes.byref(params), _p(WH), _p(WNa), _p(E))
+        return E
 
     def gyrate(self, params: StepParams, B, dt, UH, UNa):
         """mercury::gyrate (MercuryUns/physics/Gyration.cpp); UH, UNa in place."""

@@ -23,6 +23,7 @@
 #include "fluid/FluxRHS.h"
 #include "fluid/MercurySources.h"
 #include "fluid/Reconstruction.h"
+#include "physics/Ambipolar.h"
 #include "physics/Gyration.h"
 #include "induction/Current.h"
 #include "induction/EdgeEMF.h"
@@ -60,6 +61,7 @@ struct RefMesh
     // resistive operator of the explicit resistive EMF (declared after res_ex: destroyed first)
     std::unique_ptr<comm::Exchanger> res_ex;
     std::unique_ptr<ImplicitInduction> res_op;
+    std::unique_ptr<mercury::AmbipolarEMF> amb;
 };
 
 thread_local std::string g_err;
@@ -491,6 +493,11 @@ struct RefStepParams
     // explicit resistive EMF: E += ImplicitInduction::apply_F(Phi) with only the resistive part on and the
     // per-edge m_e = eta_e / star1_e given here (null: off), added to the owned edges
     const double *m_res;
+    // the rest of add_sources_n and the ambipolar EMF (Config::ambipolar / chemistry, Scales constants),
+    // with the chemistry's source fields photo and vst (one per cell, null: absent)
+    int32_t ambipolar, chemistry;
+    double pressure_coef, a1_Na, a4, a5, a6, state_coeff_H, state_coeff_Na, T_ref, Tn0;
+    const double *photo, *vst;
 };
 
 namespace
@@ -502,19 +509,40 @@ Config source_config(const RefMesh *r, const RefStepParams &p)
     c.sc.gamma = p.gamma; c.sc.M_ref = p.M_ref; c.sc.M_H = p.mass[0]; c.sc.M_Na = p.mass[1];
     c.sc.ne_floor = p.ne_floor; c.sc.inver_MA2 = p.inver_MA2; c.sc.induce_coeff = p.induce_coeff;
     c.rho_floor = p.rho_floor; c.p_floor = p.p_floor;
-    c.lorentz_force = p.lorentz != 0; c.ambipolar = false; c.chemistry = false;
+    c.lorentz_force = p.lorentz != 0; c.ambipolar = p.ambipolar != 0; c.chemistry = p.chemistry != 0;
+    c.sc.pressure_coef = p.pressure_coef; c.sc.a1_Na = p.a1_Na; c.sc.a4 = p.a4; c.sc.a5 = p.a5; c.sc.a6 = p.a6;
+    c.sc.state_coeff_H = p.state_coeff_H; c.sc.state_coeff_Na = p.state_coeff_Na; c.sc.T_ref = p.T_ref; c.chem.Tn0 = p.Tn0;
     return c;
 }
 } // namespace
 
-// mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63) for species s, J x B part
+// mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63) for species s; dpe, photo, vst: the
+// SourceFields (null: absent)
 void ref_add_sources(void *h, const RefStepParams *p, int32_t s, const double *WH, const double *WNa, const double *up,
-                     const double *B, const double *J, double dt, double *rhs)
+                     const double *B, const double *J, const double *dpe, const double *photo, const double *vst, double dt, double *rhs)
 {
     RefMesh *r = static_cast<RefMesh *>(h);
     const Config c = source_config(r, *p);
     mercury::SourceFields sf;
+    sf.dpe = dpe; sf.photo = photo; sf.vst = vst;
     mercury::add_sources(r->lm, c, s, WH, WNa, up, B, J, sf, dt, rhs, nullptr);
+}
+
+// mercury::electron_pressure_gradient (MercuryUns/physics/Ambipolar.cpp:10-31)
+void ref_electron_pressure_gradient(void *h, const double *WH, const double *WNa, double *dpe)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    mercury::electron_pressure_gradient(r->lm, r->geo, WH, WNa, dpe);
+}
+
+// mercury::AmbipolarEMF::add (Ambipolar.cpp:52-88), E in place
+void ref_ambipolar_emf(void *h, const RefStepParams *p, const double *WH, const double *WNa, double *E)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    ensure_geo(r);
+    if (!r->amb) r->amb = std::make_unique<mercury::AmbipolarEMF>(r->lm, r->geo);
+    r->amb->add(source_config(r, *p), WH, WNa, E);
 }
 
 // mercury::gyrate (MercuryUns/physics/Gyration.cpp), in place on UH, UNa
@@ -530,7 +558,7 @@ namespace
 struct StepWork
 {
     std::vector<std::vector<double>> W, grad, rhs, U1, U2;
-    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2, J, Eres;
+    std::vector<double> Bind, Btot, uplus, PhiTot, E, Phi1, Phi2, J, Eres, dpe;
 };
 
 // charge-weighted ion velocity of Solver::prepare (Solver.cpp:108-118) with mhd::Scales::numinfo (Scales.cpp:50-62)
@@ -596,8 +624,8 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
         r->stencil->set_rel_limit(p.rel_limit);
         const Vec3 uinf(p.u_inf[0], p.u_inf[1], p.u_inf[2]), bimf(p.B_imf[0], p.B_imf[1], p.B_imf[2]);
         const Vec3 E_inf = -1.0 * cross(uinf, bimf);
-        const bool lorentz = p.lorentz != 0;
-        if (lorentz && ns != 2) throw std::runtime_error("the source terms are those of the two-ion model");
+        const bool lorentz = p.lorentz != 0, ambipolar = p.ambipolar != 0, chemistry = p.chemistry != 0;
+        if ((lorentz || ambipolar || chemistry) && ns != 2) throw std::runtime_error("the source terms are those of the two-ion model");
         const Config scfg = source_config(r, p);
         const bool split = lorentz && p.induce_coeff > 0; // Strang splitting of the gyration (Solver.cpp:492-498)
         // the resistive operator of ImplicitInduction (Hall and ideal parts off) with the given per-edge m_e
@@ -636,6 +664,11 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
                 w.J.assign(3 * static_cast<size_t>(nc), 0.0);
                 cell_current(r->lm, r->geo, w.Bind.data(), w.J.data());
             }
+            if (ambipolar) // Solver::prepare (Solver.cpp:124)
+            {
+                w.dpe.assign(3 * static_cast<size_t>(nc), 0.0);
+                mercury::electron_pressure_gradient(r->lm, r->geo, w.W[0].data(), w.W[1].data(), w.dpe.data());
+            }
             for (int k = 0; k < ns; ++k)
             {
                 const Prim fs{p.fs[k][0], p.fs[k][1], p.fs[k][2], p.fs[k][3], p.fs[k][4]};
@@ -643,12 +676,13 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
                 else std::fill(w.grad[k].begin(), w.grad[k].end(), 0.0);
                 fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, k, fs, w.W[k].data(), w.grad[k].data(), w.rhs[k].data());
             }
-            if (lorentz) // Solver::rhs (Solver.cpp:146-149): sources of both species after both flux passes
+            if (lorentz || ambipolar || chemistry) // Solver::rhs (Solver.cpp:146-149): sources of both species after both flux passes
             {
                 mercury::SourceFields sf;
+                sf.photo = p.photo; sf.vst = p.vst; sf.dpe = ambipolar ? w.dpe.data() : nullptr;
                 for (int k = 0; k < ns; ++k)
-                    mercury::add_sources(r->lm, scfg, k, w.W[0].data(), w.W[1].data(), w.uplus.data(), w.Btot.data(), w.J.data(), sf, dt,
-                                         w.rhs[k].data(), nullptr);
+                    mercury::add_sources(r->lm, scfg, k, w.W[0].data(), w.W[1].data(), w.uplus.data(), w.Btot.data(),
+                                         lorentz ? w.J.data() : nullptr, sf, dt, w.rhs[k].data(), nullptr);
             }
             std::fill(w.E.begin(), w.E.end(), 0.0);
             IdealInputs in;
@@ -657,6 +691,11 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
             IdealParams ip;
             ip.cuct = p.cuct;
             add_ideal_emf(r->lm, r->geo, in, ip, w.E.data());
+            if (ambipolar) // Solver::rhs (Solver.cpp:158), before the boundary edge values
+            {
+                if (!r->amb) r->amb = std::make_unique<mercury::AmbipolarEMF>(r->lm, r->geo);
+                r->amb->add(scfg, w.W[0].data(), w.W[1].data(), w.E.data());
+            }
             for (Id e = 0; e < cx.ent[1].n_owned; ++e)
             {
                 if (r->bc.edge_mode[e] == 1) w.E[e] = 0.0;

@@ -63,3 +63,16 @@ def random_prims(n, rng, rho=(0.5, 1.5), p=(0.05, 0.15), u=1.0):
     W[:, 1:4] = rng.uniform(-u, u, (n, 3))
     W[:, 4] = rng.uniform(*p, n)
     return W.ravel()
+
+
+# Switches and constants of the ambipolar and chemistry terms used by the parity tests (the sizes of the
+# terms are moderate against the fluxes of the shell workload; the source fields are seeded per test)
+SOURCE_EXTRA = dict(ambipolar=True, chemistry=True, pressure_coef=0.3, a1_Na=0.5, a4=0.2, a5=1e-6, a6=1e-7,
+                    state_coeff_H=1.0, state_coeff_Na=1.0 / 23.0, T_ref=1e4, Tn0=600.0)
+
+
+def source_fields(n_cells, seed=31):
+    """Seeded photo (Na+ production) and vst (drag frequency) fields of the chemistry terms."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return rng.uniform(0.0, 1e-3, n_cells), rng.uniform(0.0, 2e-2, n_cells)

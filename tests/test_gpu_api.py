@@ -202,6 +202,32 @@ def test_add_sources(meshes, lorentz):
         assert rel_err(_np(d.add_sources(p, s, WH, WN, B, J, 0.02, rhs)), want) < TOL
 
 
+def test_ambipolar_and_chemistry_sources(meshes):
+    """mercury::electron_pressure_gradient, AmbipolarEMF::add and add_sources with the ambipolar force and the
+    chemistry terms of seeded source fields, both ions."""
+    from helpers import SOURCE_EXTRA, source_fields
+    from mpcns_uns_b200 import gpu
+    from oracle import port
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(703)
+    p = gpu.step_params(2, mass=[1.0, 23.0], lorentz=True, induce_coeff=0.6, inver_MA2=0.9, ne_floor=0.02, extra=SOURCE_EXTRA)
+    _, rp = _two_ion_params(True)
+    keep = port.set_source_terms(rp, SOURCE_EXTRA)
+    WH, WN = random_prims(h.n_cells, rng), random_prims(h.n_cells, rng, rho=(1e-4, 1e-2))
+    dpe = r.electron_pressure_gradient(WH, WN)
+    assert rel_err(_np(d.electron_pressure_gradient(WH, WN)), dpe) < TOL
+    E0 = rng.uniform(-1, 1, h.n_edges)
+    assert rel_err(_np(d.ambipolar_emf(p, WH, WN, E0)), r.ambipolar_emf(rp, WH, WN, E0)) < TOL
+    photo, vst = source_fields(h.n_cells)
+    B, J = rng.uniform(-2, 2, 3 * h.n_cells), rng.uniform(-1, 1, 3 * h.n_cells)
+    for s in (0, 1):
+        rhs = rng.uniform(-1, 1, 5 * h.n_cells)
+        want = rhs.copy()
+        r.add_sources(rp, s, WH, WN, np.zeros(3 * h.n_cells), B, J, 0.02, want, dpe, photo, vst)
+        assert rel_err(_np(d.add_sources(p, s, WH, WN, B, J, 0.02, rhs, dpe, photo, vst)), want) < TOL
+    del keep
+
+
 def test_gyrate(meshes):
     """mercury::gyrate: exact rotation of the relative ion velocity about B."""
     from mpcns_uns_b200 import workloads

@@ -30,10 +30,13 @@ def ref_params(p):
         f = p.fs[s]
         rp.fs[s][:] = [f.rho, f.u, f.v, f.w, f.p]
     rp.lorentz, rp.induce_coeff, rp.inver_MA2 = p.lorentz, p.induce_coeff, p.inver_MA2
+    rp.ambipolar, rp.chemistry = p.ambipolar, p.chemistry
+    for n in ("pressure_coef", "a1_Na", "a4", "a5", "a6", "state_coeff_H", "state_coeff_Na", "T_ref", "Tn0"):
+        setattr(rp, n, getattr(p, n))
     return rp
 
 
-def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True):
+def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None):
     from mpcns_uns_b200 import gpu
     h = wl.mesh
     r = ref_twin(h, tags).boundary(*bc)
@@ -47,6 +50,10 @@ def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True):
     U = [np.array(u, np.float64) for u in wl.U]
     Phi = np.array(wl.Phi, np.float64)
     rp = ref_params(p)
+    if fields is not None:   # the chemistry's source fields (photo, vst) on both sides
+        st.set_source_fields(*fields)
+        keep = [np.ascontiguousarray(x, np.float64) for x in fields]
+        rp.photo, rp.vst = keep[0].ctypes.data, keep[1].ctypes.data
     for k in range(nsteps):
         if use_cfl and wl.n_species == 2:
             W = [r.to_prim(u, wl.gamma) for u in U]
@@ -111,4 +118,16 @@ def test_step_shell_two_ions_lorentz(induce):
     from mpcns_uns_b200 import workloads
     wl = workloads.shell(4, 5, r_in=1.0, r_out=6.0)
     div = run_pair(wl, SHELL_TAGS, SHELL_BC, 4, params_kw=dict(lorentz=True, induce_coeff=induce, inver_MA2=0.7))
+    assert div < 1e-12
+
+
+@pytest.mark.parametrize("induce", [0.0, 0.8])
+def test_step_shell_two_ions_all_sources(induce):
+    """The two-ion step with every model term of the hot path on: J x B, the ambipolar force and edge EMF,
+    the chemistry terms of seeded source fields (and, induce > 0, the Strang-split gyration)."""
+    from helpers import SOURCE_EXTRA, source_fields
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5, r_in=1.0, r_out=6.0)
+    div = run_pair(wl, SHELL_TAGS, SHELL_BC, 4, params_kw=dict(lorentz=True, induce_coeff=induce, inver_MA2=0.7, extra=SOURCE_EXTRA),
+                   fields=source_fields(wl.mesh.n_cells))
     assert div < 1e-12

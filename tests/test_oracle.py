@@ -227,3 +227,60 @@ def test_resistive_emf_step():
     o.rk2_step(wl, Ua, Pa, Badd, 2e-3)
     o.rk2_step(wl, Ub, Pb, Badd, 2e-3, m_res=m_res)
     assert np.abs(Pa - Pb).max() > 1e-9
+
+
+def test_ambipolar_and_chemistry():
+    """The rest of add_sources_n (ambipolar force, chemistry), the electron-pressure gradient, the ambipolar
+    edge EMF, and the two-ion step with every source term on: oracle restatement against the compiled
+    reference, bit for bit."""
+    from helpers import SOURCE_EXTRA, source_fields
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5)
+    h = wl.mesh
+    r = ref_twin(h, SHELL_TAGS).boundary(*SHELL_BC)
+    o = port.PortMesh(h)
+    rng = np.random.default_rng(41)
+    photo, vst = source_fields(h.n_cells)
+    extra = dict(SOURCE_EXTRA, photo=photo, vst=vst)
+    rp = _ref_params(wl, True, 0.7, 0.8)
+    keep_r = port.set_source_terms(rp, extra)
+    op = o.step_params(wl, lorentz=True, induce_coeff=0.7, inver_MA2=0.8)
+    keep_o = port.set_source_terms(op, extra)
+    W = [r.to_prim(u, wl.gamma) for u in wl.U]
+    W[0][4::5] *= 1 + 0.1 * rng.uniform(-1, 1, h.n_cells)   # pressure structure for grad p_e
+    dpe = r.electron_pressure_gradient(W[0], W[1])
+    same(o.electron_pressure_gradient(W[0], W[1]), dpe)
+    assert np.abs(dpe).max() > 0
+    E0 = rng.uniform(-1, 1, h.n_edges)
+    Er = r.ambipolar_emf(rp, W[0], W[1], E0)
+    same(o.ambipolar_emf(op, W[0], W[1], E0), Er)
+    assert np.abs(Er - E0).max() > 0
+    B = rng.uniform(-2, 2, 3 * h.n_cells)
+    J = rng.uniform(-1, 1, 3 * h.n_cells)
+    for s in range(2):
+        ro = rng.uniform(-1, 1, 5 * h.n_cells)
+        rr = ro.copy()
+        o.add_sources(op, s, W[0], W[1], B, J, 0.03, ro, dpe, photo, vst)
+        r.add_sources(rp, s, W[0], W[1], np.zeros(3 * h.n_cells), B, J, 0.03, rr, dpe, photo, vst)
+        same(ro, rr)
+    Badd = r.cell_vector(wl.PhiAdd)
+    Uo = [np.array(u) for u in wl.U]
+    Ur = [np.array(u) for u in wl.U]
+    Po, Pr = np.array(wl.Phi), np.array(wl.Phi)
+    for _ in range(3):
+        Wr = [r.to_prim(u, wl.gamma) for u in Ur]
+        dt = r.local_time_step(wl.gamma, 0.4, 0.8, 1e-2, Wr[0], Wr[1], r.cell_vector(Pr) + Badd)
+        o.rk2_step(wl, Uo, Po, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8, extra=extra)
+        r.rk2_step(rp, Ur, Pr, wl.PhiAdd, Badd, dt)
+        for a, b in zip(Uo, Ur):
+            same(a, b)
+        same(Po, Pr)
+    # the terms act
+    Ua = [np.array(u) for u in wl.U]
+    Pa = np.array(wl.Phi)
+    o.rk2_step(wl, Ua, Pa, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8)
+    Ub = [np.array(u) for u in wl.U]
+    Pb = np.array(wl.Phi)
+    o.rk2_step(wl, Ub, Pb, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8, extra=extra)
+    assert np.abs(Ua[1] - Ub[1]).max() > 0 and np.abs(Pa - Pb).max() > 0
+    del keep_r, keep_o
