@@ -68,6 +68,23 @@ int mhdm_boundary(MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const
  * star0..star3, face_kind, edge_mode.  The pointer stays valid until mhdm_free. */
 const void *mhdm_array(const MhdHostMesh *m, const char *name, int64_t *count);
 
+/* ------------------------------------------------------------------ UNSBIN field files
+ * uns::io::write_fields / read_fields (src/uns/io/MeshIO.cpp:117-150) over the UNSBIN container of
+ * src/uns/io/BinContainer.cpp (little endian: magic "UNSBIN\0\1", u64 record count, records of u32 name
+ * length | name | u8 dtype | 3 pad bytes | u32 cols | u64 rows | payload padded to 8 bytes).  The files are
+ * the reference's restart / coarse-solution files (docs/FileFormats.md, "Coarse / restart solution").
+ * dims: uns::Dim (0 node, 1 edge, 2 face, 3 cell); values[i] holds counts[i] doubles (entities x ncomp). */
+int mhdm_write_fields(const char *path, uint64_t topology_hash, int32_t n, const char *const *names, const int32_t *dims,
+                      const int32_t *ncomps, const int64_t *counts, const double *const *values);
+typedef struct MhdFieldFile MhdFieldFile;
+/* read a field file; the records come in the order of its index */
+int mhdm_read_fields(const char *path, MhdFieldFile **out);
+void mhdm_fields_free(MhdFieldFile *f);
+/* record count and the stored topology hash */
+int32_t mhdm_fields_count(const MhdFieldFile *f, uint64_t *topology_hash);
+/* record i: name (len bytes incl. the terminator), dim, ncomp, value count; values copied when out != NULL */
+int mhdm_field(const MhdFieldFile *f, int32_t i, char *name, int32_t len, int32_t *dim, int32_t *ncomp, int64_t *count, double *out);
+
 #ifdef __cplusplus
 }
 #endif

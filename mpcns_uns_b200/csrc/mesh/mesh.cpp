@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <limits>
 #include <map>
@@ -869,4 +870,219 @@ const void *mhdm_array(const MhdHostMesh *m, const char *cname, int64_t *count)
     return nullptr;
 }
 
+
+} // extern "C"
+
+// ------------------------------------------------------------------ UNSBIN field files
+namespace
+{
+// dtype codes of uns::io::DType (include/uns/io/BinContainer.h): I8 0, I32 1, I64 2, F32 3, F64 4
+struct BinRec
+{
+    uint8_t type;
+    uint32_t cols;
+    uint64_t rows;
+    std::vector<char> bytes;
+};
+size_t bin_elem(uint8_t t) { return t == 0 ? 1 : (t == 1 || t == 3) ? 4 : 8; }
+const char kBinMagic[8] = {'U', 'N', 'S', 'B', 'I', 'N', 0, 1};
+
+struct BinOut
+{
+    std::vector<std::pair<std::string, BinRec>> recs;
+    template <class T> void put(const std::string &name, uint8_t type, const T *p, size_t n, uint32_t cols)
+    {
+        BinRec r;
+        r.type = type;
+        r.cols = cols;
+        r.rows = cols ? n / cols : 0;
+        r.bytes.assign(reinterpret_cast<const char *>(p), reinterpret_cast<const char *>(p) + n * sizeof(T));
+        recs.emplace_back(name, std::move(r));
+    }
+    void write(const std::string &path) const
+    {
+        std::FILE *f = std::fopen(path.c_str(), "wb");
+        if (!f) throw std::runtime_error("cannot open '" + path + "' (wb)");
+        auto wr = [&](const void *p, size_t n) {
+            if (n && std::fwrite(p, 1, n, f) != n)
+            {
+                std::fclose(f);
+                throw std::runtime_error("write failed");
+            }
+        };
+        wr(kBinMagic, 8);
+        const uint64_t n = recs.size();
+        wr(&n, 8);
+        static const char zeros[8] = {0};
+        for (const auto &kv : recs)
+        {
+            const uint32_t nl = static_cast<uint32_t>(kv.first.size());
+            wr(&nl, 4);
+            wr(kv.first.data(), nl);
+            const uint8_t t[4] = {kv.second.type, 0, 0, 0};
+            wr(t, 4);
+            wr(&kv.second.cols, 4);
+            wr(&kv.second.rows, 8);
+            wr(kv.second.bytes.data(), kv.second.bytes.size());
+            wr(zeros, (8 - kv.second.bytes.size() % 8) % 8);
+        }
+        if (std::fclose(f) != 0) throw std::runtime_error("write failed");
+    }
+};
+
+// records by name; a repeated name keeps the first, as the reference's std::map::emplace does
+std::map<std::string, BinRec> bin_read(const std::string &path)
+{
+    std::FILE *f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error("cannot open '" + path + "' (rb)");
+    std::map<std::string, BinRec> recs;
+    auto rd = [&](void *p, size_t n) {
+        if (n && std::fread(p, 1, n, f) != n)
+        {
+            std::fclose(f);
+            throw std::runtime_error("read failed / truncated file");
+        }
+    };
+    char magic[8];
+    rd(magic, 8);
+    if (std::memcmp(magic, kBinMagic, 8) != 0)
+    {
+        std::fclose(f);
+        throw std::runtime_error("'" + path + "' is not an UNSBIN file");
+    }
+    uint64_t n;
+    rd(&n, 8);
+    for (uint64_t i = 0; i < n; ++i)
+    {
+        uint32_t nl;
+        rd(&nl, 4);
+        std::string name(nl, '\0');
+        rd(name.data(), nl);
+        uint8_t t[4];
+        rd(t, 4);
+        BinRec r;
+        r.type = t[0];
+        rd(&r.cols, 4);
+        rd(&r.rows, 8);
+        r.bytes.resize(r.rows * r.cols * bin_elem(r.type));
+        rd(r.bytes.data(), r.bytes.size());
+        char pad[8];
+        rd(pad, (8 - r.bytes.size() % 8) % 8);
+        recs.emplace(std::move(name), std::move(r));
+    }
+    std::fclose(f);
+    return recs;
+}
+
+const BinRec &bin_find(const std::map<std::string, BinRec> &recs, const std::string &name, uint8_t type)
+{
+    auto it = recs.find(name);
+    if (it == recs.end()) throw std::runtime_error("UNSBIN: missing record '" + name + "'");
+    if (it->second.type != type) throw std::runtime_error("UNSBIN: record '" + name + "' has a different data type");
+    return it->second;
+}
+
+struct FieldRec
+{
+    std::string name;
+    int32_t dim, ncomp;
+    std::vector<double> values;
+};
+} // namespace
+
+struct MhdFieldFile
+{
+    uint64_t hash = 0;
+    std::vector<FieldRec> fields;
+};
+
+extern "C" {
+int mhdm_write_fields(const char *path, uint64_t topology_hash, int32_t n, const char *const *names, const int32_t *dims,
+                      const int32_t *ncomps, const int64_t *counts, const double *const *values)
+{
+    return guarded([&] {
+        if (!path || (n > 0 && (!names || !dims || !ncomps || !counts || !values))) throw std::runtime_error("null argument");
+        BinOut w;
+        const int64_t h = static_cast<int64_t>(topology_hash);
+        w.put("hash", 2, &h, 1, 1);
+        std::string index;
+        for (int32_t i = 0; i < n; ++i)
+        {
+            if (ncomps[i] < 1 || counts[i] < 0 || counts[i] % ncomps[i] != 0)
+                throw std::runtime_error(std::string("field '") + names[i] + "': count must be a multiple of ncomp");
+            const std::string name = names[i];
+            index += name + "\n";
+            const int32_t info[2] = {dims[i], ncomps[i]};
+            w.put("f." + name + ".info", 1, info, 2, 1);
+            w.put("f." + name, 4, values[i], static_cast<size_t>(counts[i]), static_cast<uint32_t>(ncomps[i]));
+        }
+        w.put("index", 0, reinterpret_cast<const int8_t *>(index.data()), index.size(), 1);
+        w.write(path);
+    });
+}
+
+int mhdm_read_fields(const char *path, MhdFieldFile **out)
+{
+    MhdFieldFile *ff = nullptr;
+    int rc = guarded([&] {
+        if (!path || !out) throw std::runtime_error("null argument");
+        const auto recs = bin_read(path);
+        ff = new MhdFieldFile;
+        const BinRec &h = bin_find(recs, "hash", 2);
+        if (h.bytes.size() < 8) throw std::runtime_error("UNSBIN: empty hash record");
+        int64_t hv;
+        std::memcpy(&hv, h.bytes.data(), 8);
+        ff->hash = static_cast<uint64_t>(hv);
+        const BinRec &ix = bin_find(recs, "index", 0);
+        const std::string index(ix.bytes.begin(), ix.bytes.end());
+        size_t a = 0;
+        while (a < index.size())
+        {
+            size_t b = index.find('\n', a);
+            if (b == std::string::npos) b = index.size();
+            FieldRec f;
+            f.name = index.substr(a, b - a);
+            a = b + 1;
+            const BinRec &inf = bin_find(recs, "f." + f.name + ".info", 1);
+            if (inf.bytes.size() < 8) throw std::runtime_error("UNSBIN: short info record of '" + f.name + "'");
+            int32_t info[2];
+            std::memcpy(info, inf.bytes.data(), 8);
+            f.dim = info[0];
+            f.ncomp = info[1];
+            const BinRec &v = bin_find(recs, "f." + f.name, 4);
+            f.values.resize(v.bytes.size() / 8);
+            std::memcpy(f.values.data(), v.bytes.data(), f.values.size() * 8);
+            ff->fields.push_back(std::move(f));
+        }
+        *out = ff;
+    });
+    if (rc != 0) delete ff;
+    return rc;
+}
+
+void mhdm_fields_free(MhdFieldFile *f) { delete f; }
+
+int32_t mhdm_fields_count(const MhdFieldFile *f, uint64_t *topology_hash)
+{
+    if (!f) return -1;
+    if (topology_hash) *topology_hash = f->hash;
+    return static_cast<int32_t>(f->fields.size());
+}
+
+int mhdm_field(const MhdFieldFile *f, int32_t i, char *name, int32_t len, int32_t *dim, int32_t *ncomp, int64_t *count, double *out)
+{
+    return guarded([&] {
+        if (!f || i < 0 || i >= static_cast<int32_t>(f->fields.size())) throw std::runtime_error("no such record");
+        const FieldRec &r = f->fields[static_cast<size_t>(i)];
+        if (name && len > 0)
+        {
+            std::strncpy(name, r.name.c_str(), static_cast<size_t>(len - 1));
+            name[len - 1] = 0;
+        }
+        if (dim) *dim = r.dim;
+        if (ncomp) *ncomp = r.ncomp;
+        if (count) *count = static_cast<int64_t>(r.values.size());
+        if (out) std::memcpy(out, r.values.data(), r.values.size() * sizeof(double));
+    });
+}
 } // extern "C"

@@ -77,6 +77,9 @@ def lib():
             ("ref_rk2_step", [vp, ctypes.POINTER(StepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
             ("ref_add_sources", [vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp], None),
             ("ref_electron_pressure_gradient", [vp, vp, vp, vp], None),
+            ("ref_write_fields", [ctypes.c_char_p, ctypes.c_uint64, i32, vp, vp, vp, vp, vp], ctypes.c_int),
+            ("ref_read_fields", [ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)], i32),
+            ("ref_fields_get", [i32, ctypes.c_char_p, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64), vp], None),
             ("ref_ambipolar_emf", [vp, ctypes.POINTER(StepParams), vp, vp, vp], None),
             ("ref_gyrate", [vp, ctypes.POINTER(StepParams), vp, dbl, vp, vp], None),
         ]:
@@ -384,3 +387,33 @@ class RefInduction:
         rr = ctypes.c_double()
         it = lib().ref_ind_solve(self._h, _p(Phi), _p(Ee), _p(d), dt, int(warm), _p(E), ctypes.byref(rr))
         return E, int(it), rr.value
+
+
+def write_fields(path, topology_hash, records):
+    """uns::io::write_fields (src/uns/io/MeshIO.cpp:117-130); records: (name, dim, ncomp, values)."""
+    recs = list(records)
+    vals = [np.ascontiguousarray(v, np.float64).ravel() for _, _, _, v in recs]
+    names = (ctypes.c_char_p * max(1, len(recs)))(*[r[0].encode() for r in recs])
+    dims = np.array([r[1] for r in recs] or [0], np.int32)
+    ncomps = np.array([r[2] for r in recs] or [1], np.int32)
+    counts = np.array([v.size for v in vals] or [0], np.int64)
+    ptrs = (ctypes.c_void_p * max(1, len(recs)))(*[v.ctypes.data for v in vals])
+    _check(lib().ref_write_fields(path.encode(), topology_hash, len(recs), ctypes.cast(names, ctypes.c_void_p), _p(dims), _p(ncomps),
+                                  _p(counts), ctypes.cast(ptrs, ctypes.c_void_p)))
+
+
+def read_fields(path):
+    """uns::io::read_fields (MeshIO.cpp:132-150): ([(name, dim, ncomp, values)], hash)."""
+    h = ctypes.c_uint64()
+    n = lib().ref_read_fields(path.encode(), ctypes.byref(h))
+    if n < 0:
+        raise RuntimeError(lib().ref_last_error().decode())
+    out = []
+    name = ctypes.create_string_buffer(4096)
+    for i in range(n):
+        d, c, k = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64()
+        lib().ref_fields_get(i, name, 4096, ctypes.byref(d), ctypes.byref(c), ctypes.byref(k), None)
+        v = np.empty(k.value)
+        lib().ref_fields_get(i, name, 4096, ctypes.byref(d), ctypes.byref(c), ctypes.byref(k), _p(v))
+        out.append((name.value.decode(), d.value, c.value, v))
+    return out, h.value

@@ -32,6 +32,7 @@
 #include "uns/complex/ComplexBuilder.h"
 #include "uns/complex/Validate.h"
 #include "uns/generate/HexMesh.h"
+#include "uns/io/MeshIO.h"
 #include "uns/geometry/Geometry.h"
 #include "uns/geometry/Reconstruct.h"
 #include "uns/refine/Refine.h"
@@ -749,6 +750,54 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
         // the closing half step uses Btot of the last prepare, that of the stage-2 input (Solver.cpp:510)
         if (split) mercury::gyrate(r->lm, scfg, w.Btot.data(), 0.5 * dt, U0[0], U0[1]);
     });
+}
+
+// uns::io::write_fields (src/uns/io/MeshIO.cpp:117-130): n records, values[i] holding counts[i] doubles
+int ref_write_fields(const char *path, uint64_t hash, int32_t n, const char *const *names, const int32_t *dims, const int32_t *ncomps,
+                     const int64_t *counts, const double *const *values)
+{
+    return guarded([&] {
+        std::vector<io::FieldRecord> fs;
+        for (int32_t i = 0; i < n; ++i)
+        {
+            io::FieldRecord f;
+            f.name = names[i];
+            f.dim = static_cast<Dim>(dims[i]);
+            f.ncomp = ncomps[i];
+            f.values.assign(values[i], values[i] + counts[i]);
+            fs.push_back(std::move(f));
+        }
+        io::write_fields(path, hash, fs);
+    });
+}
+
+// uns::io::read_fields (MeshIO.cpp:132-150): the records in file order; query with ref_fields_get
+namespace
+{
+thread_local std::vector<io::FieldRecord> g_fields;
+thread_local uint64_t g_hash = 0;
+} // namespace
+int32_t ref_read_fields(const char *path, uint64_t *hash)
+{
+    int32_t n = -1;
+    guarded([&] {
+        g_fields = io::read_fields(path, &g_hash);
+        n = static_cast<int32_t>(g_fields.size());
+    });
+    if (hash) *hash = g_hash;
+    return n;
+}
+// the i-th record of the last ref_read_fields: name (into a buffer of len chars), dim, ncomp, count;
+// values copied when out is given
+void ref_fields_get(int32_t i, char *name, int32_t len, int32_t *dim, int32_t *ncomp, int64_t *count, double *out)
+{
+    const io::FieldRecord &f = g_fields.at(static_cast<size_t>(i));
+    std::strncpy(name, f.name.c_str(), static_cast<size_t>(len - 1));
+    name[len - 1] = 0;
+    *dim = static_cast<int32_t>(f.dim);
+    *ncomp = f.ncomp;
+    *count = static_cast<int64_t>(f.values.size());
+    if (out) std::copy(f.values.begin(), f.values.end(), out);
 }
 
 } // extern "C"
