@@ -189,7 +189,7 @@ def make_workload(args):
     if args.config == "box":
         wl = workloads.box(args.ncube or 16)
     else:
-        wl = workloads.shell(args.ncube or 64, args.nr or 96, r_in=1.0, r_out=6.0, sources=not args.no_sources)
+        wl = workloads.shell(args.ncube or 64, args.nr or 96, r_in=1.0, r_out=6.0, sources=not args.no_sources, device_geometry=True)
     log(f"[bench] workload {wl.name}: {wl.mesh.n_cells} cells, {wl.mesh.n_faces} faces, {wl.mesh.n_edges} edges "
         f"(setup {time.time() - t:.1f}s)")
     return wl
@@ -270,7 +270,7 @@ def bench_gmres(args, peak):
     import torch
     from mpcns_uns_b200 import gpu, workloads
     t = time.time()
-    case = workloads.induction_case(args.gmres_ncube, args.gmres_nr)
+    case = workloads.induction_case(args.gmres_ncube, args.gmres_nr, device_geometry=True)
     h = case.mesh
     log(f"[bench] induction workload {case.name}: {h.n_cells} cells, {h.n_edges} edges (setup {time.time() - t:.1f}s)")
     dm = gpu.DeviceMesh(h)
@@ -329,7 +329,8 @@ def bench_adjoint(args):
     import torch
     from mpcns_uns_b200 import gpu, workloads
     t = time.time()
-    case = workloads.adjoint_case(args.adj_ncube, args.adj_nr, n_steps=args.adj_steps, checkpoint_every=args.adj_checkpoint)
+    case = workloads.adjoint_case(args.adj_ncube, args.adj_nr, n_steps=args.adj_steps, checkpoint_every=args.adj_checkpoint,
+                                  device_geometry=True)
     wl = case.wl
     h = wl.mesh
     log(f"[bench] adjoint workload {wl.name}: {h.n_cells} cells (setup {time.time() - t:.1f}s)")

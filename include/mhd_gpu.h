@@ -65,6 +65,31 @@ typedef struct MhdPrim { double rho, u, v, w, p; } MhdPrim;
 const char *mhd_gpu_last_error(void);
 int mhd_gpu_device_info(char *name, size_t name_len, int *sm_count);
 
+/* uns::compute_geometry (src/uns/geometry/Geometry.cpp:17-169) on the device, bit-identical to the
+ * reference's host computation: topology (reference CSR layouts) and node coordinates in, every uns::Geometry
+ * array out into the caller's host arrays (any output may be NULL: skipped).  ec_cell / ec_weight hold
+ * ec_capacity entries; 2 * e2f_ptr[n_edges] always suffices, the count used is ec_ptr[n_edges].
+ * Limits: face loops of at most 16 nodes, cells of at most 64 nodes, edges of at most 32 faces. */
+typedef struct MhdGeometryArgs {
+    int32_t n_nodes, n_edges, n_faces, n_cells;
+    const double *x;              /* 3 per node */
+    const int32_t *edge_nodes;    /* start, end per edge (uns::CellComplex::edge_nodes) */
+    const int64_t *f2e_ptr; const int32_t *f2e_idx; const int8_t *f2e_sgn;
+    const int64_t *c2f_ptr; const int32_t *c2f_idx; const int8_t *c2f_sgn;
+    const int64_t *e2f_ptr; const int32_t *e2f_idx;   /* rows in ascending face order */
+    const int64_t *f2c_ptr; const int32_t *f2c_idx;
+    double *edge_vec, *edge_mid, *edge_len;           /* 3, 3, 1 per edge */
+    double *face_area, *face_center, *face_area_mag;  /* 3, 3, 1 per face */
+    double *cell_center, *cell_volume, *cell_min_tet_volume;
+    double *star0, *star1, *star2, *star3;            /* per node, edge, face, cell */
+    double *edge_dual_area;                           /* 3 per edge */
+    int32_t *ec_misoriented;                          /* per edge */
+    double *ef_weight;                                /* aligned with e2f */
+    int64_t *ec_ptr;                                  /* n_edges + 1 */
+    int32_t *ec_cell; double *ec_weight; int64_t ec_capacity;
+} MhdGeometryArgs;
+int mhd_gpu_compute_geometry(const MhdGeometryArgs *args);
+
 /* Upload a mesh; replaces the reference's per-call use of LocalMesh + Geometry + BoundaryInfo
  * and the one-time setup of mhd::Stencil::Stencil (Common/fluid/Reconstruction.cpp:26-78). */
 int mhd_gpu_mesh_create(const MhdMeshDesc *desc, MhdMesh **out);

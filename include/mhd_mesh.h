@@ -68,6 +68,16 @@ int mhdm_boundary(MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const
  * star0..star3, face_kind, edge_mode.  The pointer stays valid until mhdm_free. */
 const void *mhdm_array(const MhdHostMesh *m, const char *name, int64_t *count);
 
+/* Install a geometry computed elsewhere (mhd_gpu_compute_geometry) in place of mhdm_compute_geometry's:
+ * the arrays are copied (sizes as in MhdGeometryArgs; ec lists of ec_ptr[n_edges] entries). */
+typedef struct MhdGeometryArrays {
+    const double *edge_vec, *edge_mid, *edge_len, *face_area, *face_center, *face_area_mag, *cell_center, *cell_volume,
+        *cell_min_tet_volume, *edge_dual_area, *ec_weight, *ef_weight, *star0, *star1, *star2, *star3;
+    const int64_t *ec_ptr;
+    const int32_t *ec_cell, *ec_misoriented;
+} MhdGeometryArrays;
+int mhdm_set_geometry(MhdHostMesh *m, const MhdGeometryArrays *g);
+
 /* ------------------------------------------------------------------ UNSBIN field files
  * uns::io::write_fields / read_fields (src/uns/io/MeshIO.cpp:117-150) over the UNSBIN container of
  * src/uns/io/BinContainer.cpp (little endian: magic "UNSBIN\0\1", u64 record count, records of u32 name

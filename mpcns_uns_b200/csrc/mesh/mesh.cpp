@@ -803,6 +803,31 @@ uint64_t mhdm_topology_hash(const MhdHostMesh *m)
     return h;
 }
 
+int mhdm_set_geometry(MhdHostMesh *m, const MhdGeometryArrays *g)
+{
+    return guarded([&] {
+        if (!m || !g || !g->ec_ptr) throw std::runtime_error("null argument");
+        const size_t ne = m->ne(), nf = m->nf(), nc = m->nc(), nn = m->n_nodes;
+        auto cp = [](std::vector<double> &v, const double *p, size_t n) {
+            if (!p) throw std::runtime_error("missing geometry array");
+            v.assign(p, p + n);
+        };
+        cp(m->edge_vec, g->edge_vec, 3 * ne); cp(m->edge_mid, g->edge_mid, 3 * ne); cp(m->edge_len, g->edge_len, ne);
+        cp(m->face_area, g->face_area, 3 * nf); cp(m->face_center, g->face_center, 3 * nf); cp(m->face_area_mag, g->face_area_mag, nf);
+        cp(m->cell_center, g->cell_center, 3 * nc); cp(m->cell_volume, g->cell_volume, nc);
+        cp(m->cell_min_tet_volume, g->cell_min_tet_volume, nc); cp(m->edge_dual_area, g->edge_dual_area, 3 * ne);
+        cp(m->star0, g->star0, nn); cp(m->star1, g->star1, ne); cp(m->star2, g->star2, nf); cp(m->star3, g->star3, nc);
+        m->ec_ptr.assign(g->ec_ptr, g->ec_ptr + ne + 1);
+        const size_t nec = static_cast<size_t>(m->ec_ptr[ne]);
+        if (!g->ec_cell || !g->ec_misoriented) throw std::runtime_error("missing geometry array");
+        m->ec_cell.assign(g->ec_cell, g->ec_cell + nec);
+        cp(m->ec_weight, g->ec_weight, nec);
+        cp(m->ef_weight, g->ef_weight, m->e2f.idx.size());
+        m->ec_misoriented.assign(g->ec_misoriented, g->ec_misoriented + ne);
+        m->have_geo = true;
+    });
+}
+
 int mhdm_compute_geometry(MhdHostMesh *m)
 {
     return guarded([&] { if (!m->have_geo) compute_geometry(*m); });

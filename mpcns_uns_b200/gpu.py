@@ -103,6 +103,7 @@ _SIGS = {
     "mhd_gpu_induction_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
     "mhd_gpu_state_set_resistivity": ([vp, vp], ctypes.c_int),
+    "mhd_gpu_compute_geometry": ([vp], ctypes.c_int),
     "mhd_gpu_fn_create": ([vp, vp, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_fn_destroy": ([vp], ctypes.c_int),
     "mhd_gpu_fn_set_params": ([vp, vp, vp], ctypes.c_int),
@@ -495,6 +496,60 @@ class ResidentState:
             return
         a = np.ascontiguousarray(m_edge, np.float64)
         check(lib().mhd_gpu_state_set_resistivity(self._h, a.ctypes.data_as(vp)))
+
+
+class GeometryArgs(ctypes.Structure):
+    """MhdGeometryArgs of include/mhd_gpu.h."""
+    _fields_ = [("n_nodes", i32), ("n_edges", i32), ("n_faces", i32), ("n_cells", i32)] + \
+               [(n, vp) for n in ("x", "edge_nodes", "f2e_ptr", "f2e_idx", "f2e_sgn", "c2f_ptr", "c2f_idx", "c2f_sgn", "e2f_ptr",
+                                  "e2f_idx", "f2c_ptr", "f2c_idx", "edge_vec", "edge_mid", "edge_len", "face_area", "face_center",
+                                  "face_area_mag", "cell_center", "cell_volume", "cell_min_tet_volume", "star0", "star1", "star2",
+                                  "star3", "edge_dual_area", "ec_misoriented", "ef_weight", "ec_ptr", "ec_cell", "ec_weight")] + \
+               [("ec_capacity", i64)]
+
+
+_GEO_OUT = {"edge_vec": 3, "edge_mid": 3, "edge_len": 1, "face_area": 3, "face_center": 3, "face_area_mag": 1, "cell_center": 3,
+            "cell_volume": 1, "cell_min_tet_volume": 1, "star0": 1, "star1": 1, "star2": 1, "star3": 1, "edge_dual_area": 3}
+_GEO_ENT = {"edge_vec": "e", "edge_mid": "e", "edge_len": "e", "face_area": "f", "face_center": "f", "face_area_mag": "f",
+            "cell_center": "c", "cell_volume": "c", "cell_min_tet_volume": "c", "star0": "n", "star1": "e", "star2": "f", "star3": "c",
+            "edge_dual_area": "e"}
+
+
+def compute_geometry(host_mesh):
+    """uns::compute_geometry on the device for a host mesh's topology and coordinates: a dict of every
+    geometry array (bit-identical to the host computation)."""
+    h = host_mesh
+    keep = {}
+
+    def inp(name, dtype, src=None):
+        a = np.ascontiguousarray(np.asarray(h[src or name]).ravel(), dtype)
+        keep[name] = a
+        return ctypes.c_void_p(a.ctypes.data)
+
+    g = GeometryArgs()
+    g.n_nodes, g.n_edges, g.n_faces, g.n_cells = h.n_nodes, h.n_edges, h.n_faces, h.n_cells
+    g.x = inp("x", np.float64)
+    g.edge_nodes = inp("edge_nodes", np.int32, "e2n_idx")
+    for t in ("f2e", "c2f", "e2f", "f2c"):
+        setattr(g, t + "_ptr", inp(t + "_ptr", np.int64))
+        setattr(g, t + "_idx", inp(t + "_idx", np.int32))
+    g.f2e_sgn = inp("f2e_sgn", np.int8)
+    g.c2f_sgn = inp("c2f_sgn", np.int8)
+    n = {"n": h.n_nodes, "e": h.n_edges, "f": h.n_faces, "c": h.n_cells}
+    out = {k: np.empty(n[_GEO_ENT[k]] * w) for k, w in _GEO_OUT.items()}
+    out["ec_misoriented"] = np.empty(h.n_edges, np.int32)
+    out["ef_weight"] = np.empty(int(np.asarray(h["e2f_ptr"])[-1]))
+    out["ec_ptr"] = np.empty(h.n_edges + 1, np.int64)
+    cap = 2 * out["ef_weight"].size
+    out["ec_cell"] = np.empty(cap, np.int32)
+    out["ec_weight"] = np.empty(cap)
+    for k, a in out.items():
+        setattr(g, k, ctypes.c_void_p(a.ctypes.data))
+    g.ec_capacity = cap
+    check(lib().mhd_gpu_compute_geometry(ctypes.byref(g)))
+    m = int(out["ec_ptr"][-1])
+    out["ec_cell"], out["ec_weight"] = out["ec_cell"][:m].copy(), out["ec_weight"][:m].copy()
+    return out
 
 
 class FnParams(ctypes.Structure):

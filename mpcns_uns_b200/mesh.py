@@ -28,6 +28,14 @@ _DT = {
 _VEC3 = {"x", "edge_vec", "edge_mid", "face_area", "face_center", "cell_center", "edge_dual_area"}
 
 
+class _GeometryArrays(ctypes.Structure):
+    """MhdGeometryArrays of include/mhd_mesh.h."""
+    _fields_ = [(n, ctypes.c_void_p) for n in ("edge_vec", "edge_mid", "edge_len", "face_area", "face_center", "face_area_mag",
+                                               "cell_center", "cell_volume", "cell_min_tet_volume", "edge_dual_area", "ec_weight",
+                                               "ef_weight", "star0", "star1", "star2", "star3", "ec_ptr", "ec_cell",
+                                               "ec_misoriented")]
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -45,6 +53,7 @@ def lib():
         L.mhdm_topology_hash.argtypes = [vp]
         L.mhdm_topology_hash.restype = ctypes.c_uint64
         L.mhdm_compute_geometry.argtypes = [vp]
+        L.mhdm_set_geometry.argtypes = [vp, vp]
         L.mhdm_boundary.argtypes = [vp, ctypes.c_char_p, i32, vp, vp, vp]
         L.mhdm_array.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i64)]
         L.mhdm_array.restype = vp
@@ -127,8 +136,20 @@ class HostMesh:
     def topology_hash(self) -> int:
         return int(lib().mhdm_topology_hash(self._h))
 
-    def compute_geometry(self) -> "HostMesh":
-        _check(lib().mhdm_compute_geometry(self._h))
+    def compute_geometry(self, device=False) -> "HostMesh":
+        """uns::compute_geometry (src/uns/geometry/Geometry.cpp:17-169) on the host, or with device=True on the
+        GPU (mhd_gpu_compute_geometry, bit-identical) and installed in this mesh."""
+        if device:
+            from . import gpu
+            g = gpu.compute_geometry(self)
+            names = ("edge_vec", "edge_mid", "edge_len", "face_area", "face_center", "face_area_mag", "cell_center", "cell_volume",
+                     "cell_min_tet_volume", "edge_dual_area", "ec_weight", "ef_weight", "star0", "star1", "star2", "star3")
+            arr = _GeometryArrays(*[ctypes.c_void_p(g[k].ctypes.data) for k in names],
+                                  ctypes.c_void_p(g["ec_ptr"].ctypes.data), ctypes.c_void_p(g["ec_cell"].ctypes.data),
+                                  ctypes.c_void_p(g["ec_misoriented"].ctypes.data))
+            _check(lib().mhdm_set_geometry(self._h, ctypes.byref(arr)))
+        else:
+            _check(lib().mhdm_compute_geometry(self._h))
         self._cache.clear()
         return self
 

@@ -134,11 +134,13 @@ def geometric_stretch(nr, r_in, r_out, first):
     return 0.5 * (lo + hi)
 
 
-def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False):
+def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False,
+          device_geometry=False):
+    """device_geometry: compute the metric on the GPU (bit-identical, faster for large shells)."""
     if stretch is None:
         # first layer as thick as the angular spacing at r_in
         stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
-    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry()
+    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry(device=device_geometry)
     m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
     rng = np.random.default_rng(seed)
     nc = m.n_cells
@@ -207,14 +209,14 @@ class InductionCase:
 
 
 def induction_case(ncube=48, nr=96, r_in=0.8, r_out=6.0, eta_inner=1.0, eta_outer=1e-3, r_eta=1.0, hall_coef=1.0,
-                   hall_r_min=1.0, hall_r_max=1.012, dt_factor=20.0, seed=0, u_inf=(-8.0, 0.0, 0.0)):
+                   hall_r_min=1.0, hall_r_max=1.012, dt_factor=20.0, seed=0, u_inf=(-8.0, 0.0, 0.0), device_geometry=False):
     """The semi-implicit Hall + resistive solve on a cubed-sphere shell r in [r_in, r_out] (6 tetrahedra per hexahedron,
     nr geometric layers): eta = eta_inner below r_eta and eta_outer above it, set per edge as m_e = eta / star1_e; Hall
     on with the reference's radial taper; B0 = dipole of moment 1 at (0, 0, 0.2) plus the IMF (0, 0, -0.5) at the cell
     centres; n_e = 1 + U(0, 0.5) (seeded); Phi^n = d1 of 8 seeded Fourier modes of amplitude 0.05; E_expl = (-u x B0) . t
     at the edge midpoints; dt = dt_factor x the explicit whistler limit.  ncube = 48, nr = 96 is the 7.96M-cell case."""
     stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
-    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry()
+    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry(device=device_geometry)
     m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
     rng = np.random.default_rng(seed)
     r_e = np.linalg.norm(np.asarray(m["edge_mid"]), axis=1)
@@ -258,7 +260,7 @@ class AdjointCase:
 
 
 def adjoint_case(ncube=32, nr=64, r_in=1.0, r_out=6.0, n_steps=40, checkpoint_every=8, eta_lo=1e-4, eta_hi=1e-2, r_lo=1.2,
-                 r_hi=1.6, induced_amp=0.05, noise=0.01, seed=0):
+                 r_hi=1.6, induced_amp=0.05, noise=0.01, seed=0, device_geometry=False):
     """The two-ion shell of the explicit step (no model sources) with a seeded per-cell resistivity; ncube = 32,
     nr = 64 is the 2.36M-cell case.  Dayside: x > 0 (the inflow comes from +x).  The induced flux starts as d1
     of 8 seeded Fourier modes of amplitude induced_amp (the box's potential without B0), so that the resistive
@@ -266,7 +268,7 @@ def adjoint_case(ncube=32, nr=64, r_in=1.0, r_out=6.0, n_steps=40, checkpoint_ev
     and pressure carry seeded uniform noise of relative size `noise` and its velocity noise of size
     noise * |u_inf| per component (as the box's state does): without it the free stream's exactly equal
     neighbour values put every limiter and wave-speed max / min on a tie, where J has no derivative."""
-    wl = shell(ncube, nr, r_in, r_out, seed=seed)
+    wl = shell(ncube, nr, r_in, r_out, seed=seed, device_geometry=device_geometry)
     if induced_amp:
         wl.Phi = d1(wl.mesh, fourier_potential(wl.mesh, seed + 2, amp=induced_amp, B0=(0.0, 0.0, 0.0)))
     if noise:
