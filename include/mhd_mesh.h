@@ -48,6 +48,13 @@ int mhdm_box(int32_t nx, int32_t ny, int32_t nz, const double *lo, const double 
 int mhdm_shell(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch, int32_t as_tets,
                MhdHostMesh **out);
 
+/* The same complex built again with its cells in the given order (new cell i = old cell order[i]):
+ * faces and edges are numbered in creation order of the new cell sequence, tags and materials carried
+ * over, geometry not computed.  With a locality order (HostMesh.locality_order: Morton order of the cell
+ * centres) this is the locality renumbering of a mesh that arrives in an arbitrary order; reordering by
+ * the inverse permutation rebuilds the original numbering exactly (same uns::topology_hash). */
+int mhdm_reorder_cells(const MhdHostMesh *m, const int32_t *order, MhdHostMesh **out);
+
 void mhdm_free(MhdHostMesh *m);
 
 /* counts[0..3] = nodes, edges, faces, cells */

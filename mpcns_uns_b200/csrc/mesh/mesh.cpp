@@ -743,6 +743,70 @@ int mhdm_from_cells(int32_t n_nodes, const double *x, int32_t n_cells, const int
     });
 }
 
+int mhdm_reorder_cells(const MhdHostMesh *src, const int32_t *order, MhdHostMesh **out)
+{
+    return guarded([&] {
+        if (!src || !order || !out) throw std::runtime_error("null argument");
+        const HostMesh &m = *src;
+        const int32_t nc = m.nc();
+        std::vector<char> seen(nc, 0);
+        for (int32_t i = 0; i < nc; ++i)
+        {
+            if (order[i] < 0 || order[i] >= nc || seen[order[i]]) throw std::runtime_error("order is not a permutation of the cells");
+            seen[order[i]] = 1;
+        }
+        // the loop of face f as the builder stored it: the node at which each edge is entered
+        auto face_loop = [&](int32_t f, std::vector<int32_t> &loop) {
+            loop.clear();
+            for (int64_t k = m.f2e.ptr[f]; k < m.f2e.ptr[f + 1]; ++k)
+            {
+                const int32_t e = m.f2e.idx[k];
+                int32_t a = -1, b = -1;
+                for (int64_t q = m.e2n.ptr[e]; q < m.e2n.ptr[e + 1]; ++q) (m.e2n.sgn[q] < 0 ? a : b) = m.e2n.idx[q];
+                loop.push_back(m.f2e.sgn[k] > 0 ? a : b);
+            }
+        };
+        auto *r = new MhdHostMesh;
+        try
+        {
+            r->n_nodes = m.n_nodes;
+            r->x = m.x;
+            r->tag_names = m.tag_names;
+            Builder b(m.n_nodes, static_cast<size_t>(nc) * 4 + 1024);
+            std::vector<std::vector<int32_t>> loops;
+            std::vector<const int32_t *> lp;
+            std::vector<int> sz;
+            for (int32_t i = 0; i < nc; ++i)
+            {
+                const int32_t c = order[i];
+                const int64_t k0 = m.c2f.ptr[c], k1 = m.c2f.ptr[c + 1];
+                loops.resize(static_cast<size_t>(k1 - k0));
+                lp.clear();
+                sz.clear();
+                for (int64_t k = k0; k < k1; ++k)
+                {
+                    auto &l = loops[static_cast<size_t>(k - k0)];
+                    face_loop(m.c2f.idx[k], l);
+                    if (m.c2f.sgn[k] < 0) std::reverse(l.begin(), l.end()); // outward
+                    lp.push_back(l.data());
+                    sz.push_back(static_cast<int>(l.size()));
+                }
+                b.add_cell(lp.data(), sz.data(), static_cast<int>(lp.size()), m.cell_material[c]);
+            }
+            std::vector<int32_t> l;
+            for (int32_t f = 0; f < m.nf(); ++f)
+                if (m.face_tag[f] > 0)
+                {
+                    face_loop(f, l);
+                    b.tag_face(l.data(), static_cast<int>(l.size()), m.face_tag[f]);
+                }
+            finish_mesh(*r, b);
+        }
+        catch (...) { delete r; throw; }
+        *out = r;
+    });
+}
+
 int mhdm_box(int32_t nx, int32_t ny, int32_t nz, const double *lo, const double *hi, int32_t as_tets, double jitter, uint64_t seed,
              MhdHostMesh **out)
 {

@@ -54,6 +54,7 @@ def lib():
         L.mhdm_topology_hash.restype = ctypes.c_uint64
         L.mhdm_compute_geometry.argtypes = [vp]
         L.mhdm_set_geometry.argtypes = [vp, vp]
+        L.mhdm_reorder_cells.argtypes = [vp, vp, ctypes.POINTER(vp)]
         L.mhdm_boundary.argtypes = [vp, ctypes.c_char_p, i32, vp, vp, vp]
         L.mhdm_array.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i64)]
         L.mhdm_array.restype = vp
@@ -135,6 +136,32 @@ class HostMesh:
     # ------------------------------------------------------------- services
     def topology_hash(self) -> int:
         return int(lib().mhdm_topology_hash(self._h))
+
+    def reordered(self, order) -> "HostMesh":
+        """The same complex rebuilt with its cells in `order` (new cell i = old cell order[i]); faces and edges
+        are renumbered by the builder in the new creation order.  No geometry yet."""
+        o = np.ascontiguousarray(order, np.int32)
+        if o.size != self.n_cells:
+            raise ValueError("order must list every cell once")
+        out = ctypes.c_void_p()
+        _check(lib().mhdm_reorder_cells(self._h, o.ctypes.data, ctypes.byref(out)))
+        return HostMesh(out.value)
+
+    def locality_order(self):
+        """Morton (Z-order) permutation of the cell centres, 21 bits per axis: cells close in space get close ids."""
+        cc = np.asarray(self["cell_center"], np.float64).reshape(-1, 3)
+        span = max(float((cc.max(0) - cc.min(0)).max()), 1e-300)
+        q = ((cc - cc.min(0)) / span * (2 ** 21 - 1)).astype(np.uint64)
+
+        def spread(v):
+            v = v & np.uint64(0x1FFFFF)
+            for sh, mask in ((32, 0x1F00000000FFFF), (16, 0x1F0000FF0000FF), (8, 0x100F00F00F00F00F), (4, 0x10C30C30C30C30C3),
+                             (2, 0x1249249249249249)):
+                v = (v | (v << np.uint64(sh))) & np.uint64(mask)
+            return v
+
+        key = spread(q[:, 0]) | (spread(q[:, 1]) << np.uint64(1)) | (spread(q[:, 2]) << np.uint64(2))
+        return np.argsort(key, kind="stable").astype(np.int32)
 
     def compute_geometry(self, device=False) -> "HostMesh":
         """uns::compute_geometry (src/uns/geometry/Geometry.cpp:17-169) on the host, or with device=True on the
