@@ -21,6 +21,10 @@ on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, c
 --gmres-max-it iterations: seconds per solve in FP64 and mixed precision, per-kernel GB/s, and the
 reference's own solve on a bounded sample beside it.
 
+The "ten_ion" object (with --ten-ion, or alone with --ten-ion-only): config 5, the ten-ion shell r in
+[1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background field: mixed and FP64 steps and
+the mixed state's error after 50 steps.
+
 The "adjoint" object: the gradient of J = sum |B_tot|^2 V over the dayside cells with r in [1.2, 1.6]
 after 40 FP64 steps on the 6 x 32 x 32 x 64 x 6 shell (2,359,296 cells, two ions, explicit resistive
 EMF of a seeded per-cell resistivity) with respect to the resistivity and the inflow velocity: device
@@ -420,6 +424,68 @@ def bench_adjoint(args):
     return out
 
 
+def bench_ten_ion(args, peak):
+    """Config 5: the ten-ion shell r in [1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background
+    field, no model sources: mixed and FP64 steps (CFL 0.4 on the device), per-kernel times, and the mixed state's
+    error against the FP64 state after --ten-accuracy-steps steps from the same start."""
+    import torch
+    from mpcns_uns_b200 import gpu, workloads
+    t = time.time()
+    wl = workloads.ten_ion(args.ten_ncube, args.ten_nr, device_geometry=True)
+    h = wl.mesh
+    log(f"[bench] ten-ion workload {wl.name}: {h.n_cells} cells (setup {time.time() - t:.1f}s)")
+    dm = gpu.DeviceMesh(h)
+    counts = mesh_counts(h)
+    cu = h.n_cells * wl.n_species * 2
+    out = {"workload": wl.name, "cells": h.n_cells, "faces": h.n_faces, "edges": h.n_edges, "n_species": wl.n_species,
+           "masses": list(wl.mass), "steps_timed": args.ten_steps, "dt": "CFL 0.4 on device", "sources": "none"}
+    final = {}
+    for prec in ("fp64", "mixed"):
+        p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl,
+                            precision=prec)
+        st = gpu.ResidentState(dm, p)
+        st.set(wl.U, wl.Phi, wl.PhiAdd)
+        for _ in range(2):
+            st.step(0.0)
+        torch.cuda.synchronize()
+        st.profile(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(dm.stream)
+        for _ in range(args.ten_steps):
+            st.step(0.0, sync=False)
+        e1.record(dm.stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.ten_steps
+        prof = st.profile_read()
+        st.profile(False)
+        kern = {k: {"ms_per_step": v[0] / args.ten_steps,
+                    "GBps": algorithmic_bytes(k, counts, wl.n_species, 2, prec, False) / (v[0] / v[1] / 1e3) / 1e9}
+                for k, v in prof.items() if v[1]}
+        out[prec] = {"ms_per_step": ms, "value": cu / (ms / 1e3), "kernels": kern}
+        if args.ten_accuracy_steps > 0:
+            st.set(wl.U, wl.Phi, wl.PhiAdd)
+            for _ in range(args.ten_accuracy_steps):
+                st.step(0.0, sync=False)
+            final[prec] = ([st.U(s) for s in range(wl.n_species)], st.Phi())
+        del st
+        torch.cuda.empty_cache()
+    out["speedup_mixed"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if final:
+        (U64, P64), (U32, P32) = final["fp64"], final["mixed"]
+        num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(U32, U64))
+        den = sum(float(np.sum(b ** 2)) for b in U64)
+        out["accuracy_mixed_vs_fp64"] = {"steps": args.ten_accuracy_steps, "U_all_rel_l2": float(np.sqrt(num / den)),
+                                         "U_H_rel_l2": float(np.linalg.norm(U32[0] - U64[0]) / np.linalg.norm(U64[0])),
+                                         "Phi_rel_l2": float(np.linalg.norm(P32 - P64) / np.linalg.norm(P64 + wl.PhiAdd)),
+                                         "div_b_max_rel_mixed": dm.div_b(P32, wl.PhiAdd)["max_rel"]}
+    out["roofline_top_mixed"] = max(out["mixed"]["kernels"].items(), key=lambda kv: kv[1]["ms_per_step"])[0]
+    k = out["mixed"]["kernels"][out["roofline_top_mixed"]]
+    out["roofline_top_mixed_frac"] = k["GBps"] / peak
+    del dm
+    torch.cuda.empty_cache()
+    return out
+
+
 def gmres_cpu_baseline(max_it=60):
     """ImplicitInduction::solve of the reference (oracle/_ref, np = 1, one core) on the same construction at
     6 x 16 x 16 x 24 (262,704 edges), cold start, `max_it` iterations: seconds per GMRES iteration."""
@@ -471,6 +537,12 @@ def main():
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--ten-ion", action="store_true", help="add the ten-ion shell (config 5; its 42.5M-cell mesh takes minutes to build)")
+    ap.add_argument("--ten-ion-only", action="store_true", help="run only the ten-ion section and print it as its own JSON line")
+    ap.add_argument("--ten-ncube", type=int, default=96)
+    ap.add_argument("--ten-nr", type=int, default=128)
+    ap.add_argument("--ten-steps", type=int, default=5)
+    ap.add_argument("--ten-accuracy-steps", type=int, default=50)
     ap.add_argument("--adjoint-only", action="store_true", help="run only the adjoint section and print it as its own JSON line")
     ap.add_argument("--adj-ncube", type=int, default=32)
     ap.add_argument("--adj-nr", type=int, default=64)
@@ -506,9 +578,10 @@ def main():
 
     import torch
     torch.cuda.set_device(local)
-    if args.adjoint_only:
+    if args.adjoint_only or args.ten_ion_only:
         if rank == 0:
-            print(json.dumps({"adjoint": bench_adjoint(args)}))
+            peak, _ = peaks()
+            print(json.dumps({"adjoint": bench_adjoint(args)} if args.adjoint_only else {"ten_ion": bench_ten_ion(args, peak)}))
         return
     dist = None
     if world > 1:
@@ -643,6 +716,10 @@ def main():
             log(f"[bench] cpu baseline failed: {e}")
 
     gm = None
+    # the configuration sections run once, on a single-GPU run (under torchrun the replicas time the step only)
+    if world > 1:
+        args.no_gmres = args.no_adjoint = True
+        args.ten_ion = False
     if rank == 0 and not args.no_gmres:
         del st64, st32, st
         torch.cuda.empty_cache()
@@ -661,6 +738,13 @@ def main():
             del st64, st32, st
             torch.cuda.empty_cache()
         adj = bench_adjoint(args)
+    ten = None
+    if rank == 0 and args.ten_ion:
+        if args.no_gmres and args.no_adjoint:
+            del st64, st32, st
+        del dm
+        torch.cuda.empty_cache()
+        ten = bench_ten_ion(args, peak)
 
     if rank == 0:
         out = {"metric": METRIC, "value": rmx["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -683,7 +767,7 @@ def main():
                         "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
                "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "adjoint": adj}
+               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "adjoint": adj, "ten_ion": ten}
         print(json.dumps(out))
     if dist:
         dist.barrier()

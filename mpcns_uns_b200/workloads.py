@@ -288,3 +288,57 @@ def adjoint_case(ncube=32, nr=64, r_in=1.0, r_out=6.0, n_steps=40, checkpoint_ev
     r = np.linalg.norm(x, axis=1)
     mask = ((r >= r_lo) & (r <= r_hi) & (x[:, 0] > 0)).astype(np.int8)
     return AdjointCase(wl=wl, eta=eta, mask=mask, n_steps=n_steps, checkpoint_every=checkpoint_every)
+
+
+TEN_ION_MASSES = [1.0, 2.0, 4.0, 12.0, 14.0, 16.0, 28.0, 30.0, 32.0, 44.0]
+
+
+def crustal_background(mesh: HostMesh, seed=0, n_dipoles=16, r_src=0.95, moment=0.05, global_moment=0.01, B_imf=(0.0, 0.0, -0.5),
+                       soft=1e-3):
+    """Static background flux of a crustal field: n_dipoles seeded point dipoles at radius r_src (uniform seeded
+    directions, seeded orientations, strengths uniform in [0.5, 1] x moment) plus a weak global dipole of moment
+    global_moment along z and the IMF, each as d1 of its edge vector potential (the set_background form)."""
+    rng = np.random.default_rng(seed)
+    x = np.asarray(mesh["edge_mid"])
+    t = np.asarray(mesh["edge_vec"])
+    a = np.zeros_like(x)
+    sources = [((0.0, 0.0, 0.0), (0.0, 0.0, global_moment))]
+    for _ in range(n_dipoles):
+        d = rng.normal(size=3)
+        pos = r_src * d / np.linalg.norm(d)
+        m = rng.normal(size=3)
+        m *= moment * rng.uniform(0.5, 1.0) / np.linalg.norm(m)
+        sources.append((tuple(pos), tuple(m)))
+    for c, m in sources:
+        r = x - np.asarray(c, np.float64)
+        d2 = (r * r).sum(1) + soft * soft
+        a += np.cross(np.asarray(m, np.float64), r) / (d2 * np.sqrt(d2))[:, None]
+    return np.asarray(mesh["face_area"]) @ np.asarray(B_imf, np.float64) + d1(mesh, (a * t).sum(1))
+
+
+def ten_ion(ncube=96, nr=128, r_in=1.0, r_out=8.0, seed=0, device_geometry=False):
+    """The ten-ion multi-fluid shell: r in [r_in, r_out], 6 x ncube^2 x nr hexahedra x 6 tetrahedra (96, 128: the
+    42.5M-cell case), ion masses 1, 2, 4, 12, 14, 16, 28, 30, 32, 44; H+ upstream density 1 and the others seeded
+    log-uniform in [1e-4, 1] relative to it, each with the seeded exosphere profile of shell(); the crustal
+    background field of crustal_background; wall inside, far field outside; no model sources."""
+    wl = shell(ncube, nr, r_in, r_out, seed=seed, n_species=10, masses=list(TEN_ION_MASSES), device_geometry=device_geometry)
+    # upstream densities log-uniform in [1e-4, 1] relative to H+ (seeded); inside, the free stream enhanced by the
+    # seeded exosphere profile 1 + lognormal(0, 0.5) exp(-(r - r_in)/0.2); pressure 0.05 rho, flow u_inf
+    rng = np.random.default_rng(seed + 3)
+    m = wl.mesh
+    r = np.linalg.norm(np.asarray(m["cell_center"]), axis=1)
+    nc = m.n_cells
+    U, fs = [], []
+    for s in range(10):
+        rho0 = 1.0 if s == 0 else 10.0 ** rng.uniform(-4.0, 0.0)
+        W = np.zeros((nc, 5))
+        W[:, 0] = rho0 if s == 0 else rho0 * (1.0 + rng.lognormal(0.0, 0.5, nc) * np.exp(-(r - r_in) / 0.2))
+        W[:, 1:4] = np.asarray(wl.u_inf)
+        W[:, 4] = 0.05 * W[:, 0]
+        U.append(to_cons(W, wl.gamma).ravel())
+        fs.append((rho0, *wl.u_inf, 0.05 * rho0))
+    wl.U, wl.fs = U, fs
+    wl.PhiAdd = crustal_background(m, seed + 5)
+    wl.name = f"shell6x{ncube}x{ncube}x{nr}x6_r{r_in:g}-{r_out:g}_10ions"
+    wl.steps = 50
+    return wl

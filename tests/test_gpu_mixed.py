@@ -58,3 +58,17 @@ def test_mixed_vs_fp64_lorentz_gyration():
     assert _l2(U32[0], U64[0]) < L2_TOL
     assert dm.div_b(P32)["max_rel"] < DIVB_TOL
     assert _l2(Un[0], U64[0]) > 1e-6       # the sources act on this workload
+
+
+def test_mixed_vs_fp64_ten_ions():
+    """Ten ions (five species groups per stage) with the crustal background: the mixed step against the FP64 step."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.ten_ion(6, 8)
+    n = 10
+    U64, P64, dt64, dm = _run(wl, "fp64", n)
+    U32, P32, dt32, _ = _run(wl, "mixed", n)
+    assert np.allclose(dt32, dt64, rtol=1e-5)
+    num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(U32, U64))
+    den = sum(float(np.sum(b ** 2)) for b in U64)
+    assert np.sqrt(num / den) < L2_TOL
+    assert dm.div_b(P32)["max_rel"] < DIVB_TOL

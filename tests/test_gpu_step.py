@@ -131,3 +131,12 @@ def test_step_shell_two_ions_all_sources(induce):
     div = run_pair(wl, SHELL_TAGS, SHELL_BC, 4, params_kw=dict(lorentz=True, induce_coeff=induce, inver_MA2=0.7, extra=SOURCE_EXTRA),
                    fields=source_fields(wl.mesh.n_cells))
     assert div < 1e-12
+
+
+def test_step_shell_ten_ions():
+    """The ten-ion shell (masses 1..44, log-uniform upstream densities, crustal background field): five
+    species groups per stage."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.ten_ion(4, 5)
+    div = run_pair(wl, SHELL_TAGS, SHELL_BC, 3, use_cfl=False)
+    assert div < 1e-12
