@@ -60,6 +60,13 @@ __device__ __forceinline__ float3 fcross(float3 a, float3 b)
     return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
 
+// the FP64 electron pressure of cell c that mx_prims leaves in the padding of species 0's pressure slot
+__device__ __forceinline__ double mx_pe(const float4 *__restrict__ W, int32_t c)
+{
+    const float4 b = W[2 * (int64_t)c + 1];
+    return __hiloint2double(__float_as_int(b.z), __float_as_int(b.w));
+}
+
 // ------------------------------------------------------------------ one-time tables (FP64 in, FP32 out)
 __global__ void k_mx_cells(MeshView m, float *wd, float *dx, float *inv, float *recon, float *vol_inv)
 {
@@ -181,6 +188,8 @@ struct MxParams
     float M_ref;
     int src_on;                 // two-ion J x B force (species 0 = H+, 1 = Na+)
     float inver_MA2, ne_floor;
+    int ambi, chem;             // ambipolar force, chemistry terms (two-ion model)
+    double a1_Na, a4, a5, a6, sch, scn, T_ref, Tn0;
 };
 
 __device__ __forceinline__ F5 ghost32(int kind, bool absorb, const F5 &in, float3 n, const F5 &fs)
@@ -220,6 +229,7 @@ __device__ __forceinline__ void mx_prims(const MxParams &p, int64_t n, const dou
                                          float4 *__restrict__ up, int32_t c, bool fluid)
 {
     float ne = 0.f;
+    double pe = 0.0;
     for (int s = 0; s < p.nsp; ++s)
     {
         const double *Us = U + (int64_t)s * 5 * n;
@@ -231,7 +241,14 @@ __device__ __forceinline__ void mx_prims(const MxParams &p, int64_t n, const dou
         Wc[0] = make_float4(static_cast<float>(r), static_cast<float>(u), static_cast<float>(v), static_cast<float>(w));
         Wc[1] = make_float4(static_cast<float>(pr), 0.f, 0.f, 0.f);
         ne += static_cast<float>(r) / p.mass[s] * p.M_ref;
+        if (s < 2) pe += pr;
     }
+    // with the ambipolar terms on, the FP64 electron pressure p_H + p_Na rides in the padding of species 0's
+    // pressure slot (.z = high word, .w = low word): the gradients of p_e are differences of nearly equal
+    // values that FP32 pressures would not resolve
+    if (p.ambi)
+        W[2 * (int64_t)c + 1] = make_float4(W[2 * (int64_t)c + 1].x, 0.f, __int_as_float(__double2hiint(pe)),
+                                            __int_as_float(__double2loint(pe)));
     float u3[3] = {0.f, 0.f, 0.f};
     if (fluid)
         for (int s = 0; s < p.nsp; ++s)
@@ -527,7 +544,8 @@ __device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int 
 __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, int s0, int g, int32_t c, const float *__restrict__ F,
                                               const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
                                               int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
-                                              const float4 *__restrict__ bt, double *__restrict__ res)
+                                              const float4 *__restrict__ bt, const float4 *__restrict__ D, const double *__restrict__ photo,
+                                              const double *__restrict__ vst, double *__restrict__ res)
 {
     const int s = s0 + g;
     const int64_t n = m.nc, nf = m.nf;
@@ -552,30 +570,54 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
         const double dtv = *dtp / m.cell_volume[c];
 #pragma unroll
         for (int q = 0; q < 5; ++q) u[q] += dtv * r[q];
-        if (p.src_on)
+        if (p.src_on || p.ambi || p.chem)
         {
-            // J x B force of mercury::add_sources_n (MercurySources.cpp:29-47) in FP32, with the work of the
-            // mid-point velocity, added to the FP64 update.  J_c = (1/V) sum_f s_f G_f (the face terms of
-            // k_mx_face_cand, same faces as the flux gather), S = inver_MA2 n_s / n_e,eff (J x B_tot).
-            float3 Jc = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-            {
-                const float4 g = G[ff[j]];
-                const float sj = sv[j] < 0.0 ? 1.f : -1.f; // +1 where the canonical normal points out of c
-                Jc.x += sj * g.x;
-                Jc.y += sj * g.y;
-                Jc.z += sj * g.z;
-            }
+            // mercury::add_sources_n (MercurySources.cpp:29-60).  The J x B force in FP32 with the work of the
+            // mid-point velocity, added to the FP64 update: J_c = (1/V) sum_f s_f G_f (the face terms of
+            // k_mx_face_cand, same faces as the flux gather), S = inver_MA2 n_s / n_e,eff (J x B_tot).  The
+            // ambipolar force -w_s grad p_e with grad p_e = (1/V) sum_f D_f.  The chemistry terms in FP64
+            // from the FP32 primitives.
             const float iv = m.vol_inv[c];
-            Jc = make_float3(iv * Jc.x, iv * Jc.y, iv * Jc.z);
             const float4 ws4 = W[2 * ((int64_t)s * n + c)];
             const float nH = fmaxf(W[2 * (int64_t)c].x, 0.f) / p.mass[0] * p.M_ref;
             const float nN = fmaxf(W[2 * (n + c)].x, 0.f) / p.mass[1] * p.M_ref;
             const float ne = nH + nN;
-            const float k = p.inver_MA2 * (s == 0 ? nH : nN) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
-            const float3 jb = fcross(Jc, f3(bt[c]));
-            const float Sx = k * jb.x, Sy = k * jb.y, Sz = k * jb.z;
+            float Sx = 0.f, Sy = 0.f, Sz = 0.f;
+            if (p.src_on)
+            {
+                float3 Jc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const float4 g = G[ff[j]];
+                    const float sj = sv[j] < 0.0 ? 1.f : -1.f; // +1 where the canonical normal points out of c
+                    Jc.x += sj * g.x;
+                    Jc.y += sj * g.y;
+                    Jc.z += sj * g.z;
+                }
+                Jc = make_float3(iv * Jc.x, iv * Jc.y, iv * Jc.z);
+                const float k = p.inver_MA2 * (s == 0 ? nH : nN) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
+                const float3 jb = fcross(Jc, f3(bt[c]));
+                Sx = k * jb.x;
+                Sy = k * jb.y;
+                Sz = k * jb.z;
+            }
+            if (p.ambi)
+            {
+                float3 d = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                    const float4 g = D[ff[j]]; // already oriented: the same vector for both cells of the face
+                    d.x += g.x;
+                    d.y += g.y;
+                    d.z += g.z;
+                }
+                const float ws = (s == 0 ? nH : nN) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
+                Sx -= ws * iv * d.x;
+                Sy -= ws * iv * d.y;
+                Sz -= ws * iv * d.z;
+            }
             const float rho = fmaxf(ws4.x, 0.f);
             const double dt = *dtp;
             const float work = ws4.y * Sx + ws4.z * Sy + ws4.w * Sz +
@@ -584,6 +626,25 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
             u[2] += dt * static_cast<double>(Sy);
             u[3] += dt * static_cast<double>(Sz);
             u[4] += dt * static_cast<double>(work);
+            if (p.chem && vst)
+            {
+                const double v = vst[c], r = rho, ux = ws4.y, uy = ws4.z, uz = ws4.w, ps = W[2 * ((int64_t)s * n + c) + 1].x;
+                const double u2 = ux * ux + uy * uy + uz * uz;
+                const double Ts = ps / (r > 0 ? r : 1e-300) / (s == 0 ? p.sch : p.scn) * p.T_ref;
+                const double mH = p.mass[0], mN = p.mass[1], Msum = mH + mN;
+                const double b1 = v * (p.Tn0 - Ts) * (s == 0 ? mH / Msum : 0.5);
+                const double b2 = (s == 0 ? mN / Msum : 0.5) * v;
+                const double ns = s == 0 ? nH : nN;
+                u[1] -= dt * (p.a4 * r * ux * v);
+                u[2] -= dt * (p.a4 * r * uy * v);
+                u[3] -= dt * (p.a4 * r * uz * v);
+                u[4] += dt * (-p.a4 * r * u2 * v + p.a5 * ns * b1 + p.a4 * r * u2 * b2);
+                if (s == 1 && photo)
+                {
+                    u[0] += dt * (p.a1_Na * photo[c]);
+                    u[4] += dt * (p.a6 * photo[c] * p.Tn0);
+                }
+            }
         }
         const double ke = u[0] > 0 ? 0.5 * (u[1] * u[1] + u[2] * u[2] + u[3] * u[3]) / u[0] : 0.0;
         const double gm = p.gamma_d;
@@ -609,7 +670,7 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
 __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__restrict__ up, const float4 *__restrict__ bt,
                                                       const float4 *__restrict__ bi, const double *__restrict__ phi,
                                                       const double *__restrict__ phi_add, float4 *__restrict__ Ef,
-                                                      float4 *__restrict__ G)
+                                                      float4 *__restrict__ G, const float4 *__restrict__ W, float4 *__restrict__ D)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf) return;
@@ -640,6 +701,16 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
         const float3 bf = L >= 0 && R >= 0 ? make_float3(0.5f * (bL.x + bR.x), 0.5f * (bL.y + bR.y), 0.5f * (bL.z + bR.z)) : bL;
         const float3 g = fcross(make_float3(nf4.w * n.x, nf4.w * n.y, nf4.w * n.z), bf);
         G[f] = make_float4(g.x, g.y, g.z, 0.f);
+    }
+    if (D)
+    {
+        // mercury::electron_pressure_gradient (Ambipolar.cpp:10-31) sums p_f s_f A_f over the cell's faces with
+        // p_f the mean with a fluid neighbour, the cell's own p_c elsewhere.  As sum (p_f - p_c) s_f A_f (the
+        // faces of a cell close: sum s_f A_f = 0) only faces between two fluid cells contribute, and both
+        // cells receive the same vector (p_R - p_L) A_f / 2, formed from the FP64 p_e
+        float dp = 0.f;
+        if (L >= 0 && R >= 0 && m.material[L] == 0 && m.material[R] == 0) dp = static_cast<float>(0.5 * (mx_pe(W, R) - mx_pe(W, L)));
+        D[f] = make_float4(dp * nf4.w * n.x, dp * nf4.w * n.y, dp * nf4.w * n.z, 0.f);
     }
     const float3 E = fcross(n, F);
     // with Phi_ind / |A| of the face, which the edge pass needs for its dissipation term: one 16-byte
@@ -794,14 +865,15 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, int n
 __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int ng, const float *__restrict__ F,
                                                    const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
                                                    int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
-                                                   const float4 *__restrict__ bt, SrcParams sp, int gyr)
+                                                   const float4 *__restrict__ bt, SrcParams sp, int gyr, const float4 *__restrict__ D,
+                                                   const double *__restrict__ photo, const double *__restrict__ vst)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
     const int64_t n = m.nc;
     double r0[5], r1[5];
-    mx_update_one(m, p, s0, 0, c, F, Ub, Uo, dtp, stage2, W, G, bt, r0);
-    if (ng > 1) mx_update_one(m, p, s0, 1, c, F, Ub, Uo, dtp, stage2, W, G, bt, r1);
+    mx_update_one(m, p, s0, 0, c, F, Ub, Uo, dtp, stage2, W, G, bt, D, photo, vst, r0);
+    if (ng > 1) mx_update_one(m, p, s0, 1, c, F, Ub, Uo, dtp, stage2, W, G, bt, D, photo, vst, r1);
     if (gyr && ng == 2 && c < m.no_cells && m.material[c] != 1) gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), 0.5 * *dtp, r0, r1);
     double *u0 = Uo + (int64_t)s0 * 5 * n;
 #pragma unroll
@@ -809,6 +881,48 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int
     if (ng > 1)
 #pragma unroll
         for (int q = 0; q < 5; ++q) u0[(5 + q) * n + c] = r1[q];
+}
+
+// nodal p_e of AmbipolarEMF::add (Ambipolar.cpp:57-68) from the FP64 p_e of the cells
+__global__ void k_mx_node_pressure(int32_t nn, const int32_t *__restrict__ n2c_ptr, const int32_t *__restrict__ n2c_cell,
+                                   const double *__restrict__ vol, const float4 *__restrict__ W, double *__restrict__ pn,
+                                   int8_t *__restrict__ pok)
+{
+    const int32_t v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nn) return;
+    double s = 0, w = 0;
+    for (int32_t k = n2c_ptr[v]; k < n2c_ptr[v + 1]; ++k)
+    {
+        const int32_t c = n2c_cell[k];
+        s += vol[c] * mx_pe(W, c);
+        w += vol[c];
+    }
+    pn[v] = w > 0 ? s / w : 0.0;
+    pok[v] = n2c_ptr[v + 1] > n2c_ptr[v] ? 1 : 0;
+}
+
+// AmbipolarEMF::add on the owned free edges (the reference overwrites wall and inflow edges), FP32, E in place
+__global__ void k_mx_ambipolar(MV m, MxParams p, const float4 *__restrict__ W, const double *__restrict__ ecw, const int32_t *__restrict__ en,
+                               const double *__restrict__ pn, const int8_t *__restrict__ pok, float coef, float *__restrict__ E)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.no_edges || m.edge_mode[e] != 0) return;
+    float rH = 0.f, rN = 0.f, wsum = 0.f;
+    for (int32_t k = m.ec_ptr[e]; k < m.ec_ptr[e + 1]; ++k)
+    {
+        const int32_t c = m.ec_cell[k];
+        if (m.material[c] == 1) continue;
+        const float w = static_cast<float>(ecw[k]);
+        rH += w * W[2 * (int64_t)c].x;
+        rN += w * W[2 * ((int64_t)m.nc + c)].x;
+        wsum += w;
+    }
+    if (wsum <= 0.f) return;
+    const float nH = fmaxf(rH / wsum, 0.f) / p.mass[0] * p.M_ref, nN = fmaxf(rN / wsum, 0.f) / p.mass[1] * p.M_ref;
+    const float ne = nH + nN;
+    const int32_t a = en[2 * (int64_t)e], b = en[2 * (int64_t)e + 1];
+    if (!pok[a] || !pok[b]) return;
+    E[e] -= coef * static_cast<float>(pn[b] - pn[a]) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
 }
 
 MxParams mx_params(const MhdState *st)
@@ -828,6 +942,10 @@ MxParams mx_params(const MhdState *st)
     p.src_on = st->src.on;
     p.inver_MA2 = static_cast<float>(q.inver_MA2);
     p.ne_floor = static_cast<float>(q.ne_floor);
+    p.ambi = st->src.ambi;
+    p.chem = st->src.chem;
+    p.a1_Na = q.a1_Na; p.a4 = q.a4; p.a5 = q.a5; p.a6 = q.a6;
+    p.sch = q.state_coeff_H; p.scn = q.state_coeff_Na; p.T_ref = q.T_ref; p.Tn0 = q.Tn0;
     for (int s = 0; s < st->nsp; ++s)
     {
         p.fs[s] = F5{static_cast<float>(q.fs[s].rho), static_cast<float>(q.fs[s].u), static_cast<float>(q.fs[s].v),
@@ -850,6 +968,7 @@ void mixed_setup(MhdState *st)
     MHD_CUDA(cudaMemcpy(&nnz_e2f, m.e2f_ptr + m.ne, sizeof(int32_t), cudaMemcpyDeviceToHost));
     t.wd.alloc(12 * nc); t.dx.alloc(12 * nc); t.inv.alloc(6 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
     if (st->src.on) st->g32.alloc(nf);
+    if (st->src.ambi) st->d32.alloc(nf);
     t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
     t.eth.alloc(ne); t.ee1.alloc(ne); t.ee2.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
     if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.wd.p, t.dx.p, t.inv.p, t.recon.p, t.vol_inv.p);
@@ -929,7 +1048,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     // cell current that the update gathers
     P.begin(KP_FACE_CAND, s);
     k_mx_face_cand<<<gf, 128, 0, s>>>(m, st->up32.p, st->bt32.p, st->bi32.p, phis, st->phi_add.p, st->Ef32.p,
-                                      st->src.on ? st->g32.p : nullptr);
+                                      st->src.on ? st->g32.p : nullptr, W4, st->src.ambi ? st->d32.p : nullptr);
     MHD_LAUNCH_CHECK();
     P.end(KP_FACE_CAND, s);
     for (int s0 = 0; s0 < st->nsp; s0 += st->group)
@@ -945,7 +1064,8 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
         k_mx_update<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
-                                       gyrate_close && s0 == 0 ? 1 : 0);
+                                       gyrate_close && s0 == 0 ? 1 : 0, st->src.ambi ? st->d32.p : nullptr,
+                                       st->src.chem && st->photo.n ? st->photo.p : nullptr, st->src.chem && st->vst.n ? st->vst.p : nullptr);
         MHD_LAUNCH_CHECK();
         P.end(KP_UPDATE, s);
         st->launches += 3;
@@ -956,6 +1076,16 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     P.begin(KP_EDGE_EMF, s);
     k_mx_edge<<<ge, 128, 0, s>>>(m, st->Ef32.p, st->up32.p, phis, static_cast<float>(st->prm.cuct), Einf, st->E32.p);
     MHD_LAUNCH_CHECK();
+    if (st->src.ambi)
+    {
+        if (mv.nn)
+            k_mx_node_pressure<<<grid_for(mv.nn, 128), 128, 0, s>>>(mv.nn, mv.n2c_ptr, mv.n2c_cell, mv.cell_volume, W4, st->pn.p,
+                                                                    st->pok.p);
+        k_mx_ambipolar<<<grid_for(m.ne, 128), 128, 0, s>>>(m, p, W4, mv.ec_weight, mv.e_nodes, st->pn.p, st->pok.p,
+                                                            static_cast<float>(st->prm.pressure_coef), st->E32.p);
+        MHD_LAUNCH_CHECK();
+        st->launches += 1 + (mv.nn ? 1 : 0);
+    }
     P.end(KP_EDGE_EMF, s);
     P.begin(KP_CT, s);
     k_mx_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m, st->E32.p, phis, phio, st->scal.p, stage2 ? 1 : 0);

@@ -298,7 +298,7 @@ void prepare_cfl(MhdState *st, const double *Us, const double *phis, bool cfl, d
             launch_cell_current(m, st->bind.p, st->J.p, s);
             ++st->launches;
         }
-        if (st->src.ambi) // grad p_e (Solver.cpp:124) and the nodal p_e of the ambipolar EMF
+        if (st->src.ambi && !st->mixed) // grad p_e (Solver.cpp:124) and the nodal p_e of the ambipolar EMF
         {
             launch_dpe(m, st->W.p, st->dpe.p, s);
             launch_node_pressure(m, st->W.p, st->pn.p, st->pok.p, s);
@@ -449,8 +449,6 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         MHD_REQUIRE(!p->lorentz || p->n_species == 2, "the J x B force and the gyration are those of the two-ion model (n_species == 2)");
         MHD_REQUIRE(!(p->ambipolar || p->chemistry) || p->n_species == 2,
                     "the ambipolar and chemistry terms are those of the two-ion model (n_species == 2)");
-        MHD_REQUIRE(!(p->ambipolar || p->chemistry) || p->precision == MHD_PREC_FP64,
-                    "the ambipolar and chemistry terms are part of the FP64 step");
         MHD_REQUIRE(!p->ambipolar || mesh->v.e_nodes, "the ambipolar EMF needs the mesh's edge_nodes");
         st = new MhdState;
         st->mesh = mesh;
@@ -494,7 +492,7 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         if (st->src.on) st->J.alloc(3 * nc);
         if (st->src.ambi)
         {
-            st->dpe.alloc(3 * nc);
+            if (p->precision != MHD_PREC_MIXED) st->dpe.alloc(3 * nc); // the mixed update gathers grad p_e itself
             st->pn.alloc(m.nn ? (size_t)m.nn : 1);
             st->pok.alloc(m.nn ? (size_t)m.nn : 1);
         }

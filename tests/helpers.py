@@ -76,3 +76,13 @@ def source_fields(n_cells, seed=31):
     import numpy as np
     rng = np.random.default_rng(seed)
     return rng.uniform(0.0, 1e-3, n_cells), rng.uniform(0.0, 2e-2, n_cells)
+
+
+def exosphere_source_fields(mesh, r_in=1.0, scale_height=0.5):
+    """Smooth photo and vst fields of an exosphere-like profile: both fall off as exp(-(r - r_in) / H) with the
+    radius of the cell centre, photo-ionisation stronger on the sunward (+x) side."""
+    import numpy as np
+    cc = np.asarray(mesh["cell_center"], np.float64).reshape(-1, 3)
+    r = np.linalg.norm(cc, axis=1)
+    prof = np.exp(-(r - r_in) / scale_height)
+    return 1e-3 * prof * 0.5 * (1.0 + cc[:, 0] / r), 2e-2 * prof
