@@ -113,6 +113,18 @@ int mhd_gpu_limited_gradients(MhdMesh *mesh, const double *W, int32_t species, c
 int mhd_gpu_flux_rhs(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim *freestream, const double *W,
                      const double *grad, double *rhs);
 
+/* The same two passes with a Dirichlet wall table: the GhostFn argument of limited_gradients and
+ * fluid_flux_rhs (Common/fluid/Reconstruction.h:21, FluxRHS.h:10-12) as the ten-ion solver binds it
+ * (MarsUns/driver/MarsSolver.cpp:124-128): on each listed face (kind wall) the ghost state is
+ * wall_prims[5*i .. 5*i+4] (rho u v w p of this species), whatever the inside state; every other face
+ * keeps ghost_state.  Device pointers; the faces must be distinct faces of kind wall (MHD_EINVAL
+ * otherwise).  n_wall = 0 is the plain pass. */
+int mhd_gpu_limited_gradients_wall(MhdMesh *mesh, const double *W, int32_t species, const MhdPrim *freestream, int32_t limit,
+                                   double rel_limit, int32_t n_wall, const int32_t *wall_faces, const double *wall_prims,
+                                   double *grad);
+int mhd_gpu_flux_rhs_wall(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim *freestream, const double *W,
+                          const double *grad, int32_t n_wall, const int32_t *wall_faces, const double *wall_prims, double *rhs);
+
 /* uns::reconstruct_cell_vector (include/uns/geometry/Reconstruct.h:14, src/uns/geometry/Reconstruct.cpp:8-46):
  * face flux (canonical orientation) -> 3 per cell for the cells [0, ncells). */
 int mhd_gpu_cell_vector(MhdMesh *mesh, const double *flux, int32_t ncells, double *out);
@@ -268,6 +280,12 @@ int mhd_gpu_electron_pressure_gradient(MhdMesh *mesh, const double *WH, const do
 int mhd_gpu_ambipolar_emf(MhdMesh *mesh, const MhdStepParams *params, const double *WH, const double *WNa, double *E);
 /* The external source fields of the chemistry terms (mercury::SourceFields photo and vst, host arrays of
  * one value per cell; NULL clears a field, which then contributes nothing, as in the reference). */
+/* The step's Dirichlet wall table (the ten-ion solver's wall_state_, MarsSolver.cpp:147-165, cached per
+ * face): host arrays faces[n_wall] (distinct faces of kind wall) and prims[n_species][n_wall][5]; the
+ * FP64 and mixed steps use it in the gradients and the face fluxes.  n_wall = 0 removes it.  The
+ * differentiated run (mhd_gpu_fn_*) does not take a state with a wall table. */
+int mhd_gpu_state_set_wall_ghosts(MhdState *state, int32_t n_wall, const int32_t *faces, const double *prims);
+
 int mhd_gpu_state_set_source_fields(MhdState *state, const double *photo, const double *vst);
 /* mercury::gyrate (MercuryUns/physics/Gyration.cpp): exact rotation of the ions' relative velocity
  * about B over dt on the owned fluid cells, UH and UNa (5 per cell) in place; a no-op unless

@@ -1813,6 +1813,7 @@ int mhd_gpu_fn_create(MhdState *st, const MhdFnParams *p, const double *eta, con
         MHD_REQUIRE(st && p && eta && mask && out, "null argument");
         const MeshView &m = st->mesh->v;
         MHD_REQUIRE(!st->mixed, "the differentiated run is FP64");
+        MHD_REQUIRE(!st->fp.wall_slot, "the differentiated run has no Dirichlet wall table");
         MHD_REQUIRE(!st->src.any(), "the differentiated run has no model sources (lorentz, ambipolar and chemistry must be 0)");
         MHD_REQUIRE(st->nsp <= kMaxFnSpecies, "the differentiated run supports one or two species");
         MHD_REQUIRE(m.faces_per_cell == 4, "the differentiated run needs a tetrahedral mesh");

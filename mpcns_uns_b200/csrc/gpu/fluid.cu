@@ -74,8 +74,10 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
                 const int kind = m.face_kind[f];
                 const V3 n = (double(m.c2f_sgn[k]) / m.face_area_mag[f]) * ld3(m.face_area, f);
                 const bool vel = kind == 1 && !p.absorb[s] && q >= 1 && q <= 3;
-                wn = ghost_component(kind, p.absorb[s] != 0, q, wc, vel ? W(s, c, 1) : 0.0, vel ? W(s, c, 2) : 0.0,
-                                     vel ? W(s, c, 3) : 0.0, n, p.fs[s]);
+                const double *wg = wall_ghost(p, kind, f, s);
+                wn = wg ? wg[q]
+                        : ghost_component(kind, p.absorb[s] != 0, q, wc, vel ? W(s, c, 1) : 0.0, vel ? W(s, c, 2) : 0.0,
+                                          vel ? W(s, c, 3) : 0.0, n, p.fs[s]);
             }
             const double dq = wn - wc;
             r0 += m.st_wd[3 * (int64_t)k] * dq;
@@ -155,7 +157,12 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
         {
             const int32_t f = -(nb[j] + 1);
             const V3 nrm = (double(m.t_sg[j * n + c]) / m.face_area_mag[f]) * ld3(m.face_area, f);
-            prim_arr(ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, nrm, p.fs[s]), wn[j]);
+            const double *wg = wall_ghost(p, m.face_kind[f], f, s);
+            if (wg)
+#pragma unroll
+                for (int q = 0; q < 5; ++q) wn[j][q] = wg[q];
+            else
+                prim_arr(ghost_state(m.face_kind[f], p.absorb[s] != 0, wcp, nrm, p.fs[s]), wn[j]);
         }
 #pragma unroll
     for (int q = 0; q < 5; ++q)
@@ -261,7 +268,8 @@ __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SF
         else
         {
             const Prim5 in = state_of(c);
-            const Prim5 gh = ghost_state(kind, p.absorb[s] != 0, in, double(sgn) * n, p.fs[s]);
+            const double *wg = wall_ghost(p, kind, f, s);
+            const Prim5 gh = wg ? Prim5{wg[0], wg[1], wg[2], wg[3], wg[4]} : ghost_state(kind, p.absorb[s] != 0, in, double(sgn) * n, p.fs[s]);
             if (sgn > 0) { L = in; R = gh; }
             else { R = in; L = gh; }
         }
@@ -319,6 +327,35 @@ void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const doub
     MHD_LAUNCH_CHECK();
 }
 
+__global__ void k_wall_slots(MeshView m, const int32_t *__restrict__ faces, int32_t n, int32_t *__restrict__ slot, int *__restrict__ err)
+{
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int32_t f = faces[i];
+    if (f < 0 || f >= m.nf || m.face_kind[f] != 1)
+    {
+        atomicOr(err, 1);
+        return;
+    }
+    if (atomicCAS(slot + f, -1, i) != -1) atomicOr(err, 2);
+}
+
+void build_wall_slots(const MeshView &m, const int32_t *faces, int32_t n, int32_t *slot, cudaStream_t s)
+{
+    if (m.nf) MHD_CUDA(cudaMemsetAsync(slot, 0xff, (size_t)m.nf * sizeof(int32_t), s));
+    if (!n) return;
+    DBuf<int> err;
+    err.alloc(1);
+    MHD_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+    k_wall_slots<<<grid_for(n, 128), 128, 0, s>>>(m, faces, n, slot, err.p);
+    MHD_LAUNCH_CHECK();
+    int h = 0;
+    MHD_CUDA(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaStreamSynchronize(s));
+    MHD_REQUIRE(!(h & 1), "wall ghost faces must be faces of kind wall");
+    MHD_REQUIRE(!(h & 2), "wall ghost faces must be distinct");
+}
+
 static FluidParams single_species(int32_t species, const MhdPrim *fs, double gamma, int limit, double rel_limit)
 {
     FluidParams p{};
@@ -357,6 +394,53 @@ int mhd_gpu_limited_gradients(MhdMesh *mesh, const double *W, int32_t species, c
         if (!m.nc) return;
         const FluidParams p = single_species(species, fs, 0.0, limit, rel_limit);
         launch_limited_gradients(m, p, SField<const double>{W, 0, 5, 1}, SField<double>{grad, 0, 15, 1}, mesh->stream);
+    });
+}
+
+int mhd_gpu_limited_gradients_wall(MhdMesh *mesh, const double *W, int32_t species, const MhdPrim *fs, int32_t limit, double rel_limit,
+                                   int32_t n_wall, const int32_t *wall_faces, const double *wall_prims, double *grad)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && W && grad && fs, "bad argument");
+        MHD_REQUIRE(species >= 0, "negative species");
+        MHD_REQUIRE(n_wall >= 0 && (!n_wall || (wall_faces && wall_prims)), "bad wall ghost table");
+        const MeshView &m = mesh->v;
+        if (!m.nc) return;
+        FluidParams p = single_species(species, fs, 0.0, limit, rel_limit);
+        DBuf<int32_t> slot;
+        slot.alloc(m.nf ? (size_t)m.nf : 1);
+        build_wall_slots(m, wall_faces, n_wall, slot.p, mesh->stream);
+        p.wall_slot = slot.p;
+        p.wall_prim = wall_prims;
+        p.wall_n = n_wall;
+        launch_limited_gradients(m, p, SField<const double>{W, 0, 5, 1}, SField<double>{grad, 0, 15, 1}, mesh->stream);
+        MHD_CUDA(cudaStreamSynchronize(mesh->stream)); // the slot map is freed on return
+    });
+}
+
+int mhd_gpu_flux_rhs_wall(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim *fs, const double *W, const double *grad,
+                          int32_t n_wall, const int32_t *wall_faces, const double *wall_prims, double *rhs)
+{
+    return guarded([&] {
+        MHD_REQUIRE(mesh && W && grad && rhs && fs, "bad argument");
+        MHD_REQUIRE(gamma > 1.0, "gamma must exceed 1");
+        MHD_REQUIRE(n_wall >= 0 && (!n_wall || (wall_faces && wall_prims)), "bad wall ghost table");
+        const MeshView &m = mesh->v;
+        if (!m.nc) return;
+        FluidParams p = single_species(species, fs, gamma, 1, 0.0);
+        DBuf<int32_t> slot;
+        slot.alloc(m.nf ? (size_t)m.nf : 1);
+        build_wall_slots(m, wall_faces, n_wall, slot.p, mesh->stream);
+        p.wall_slot = slot.p;
+        p.wall_prim = wall_prims;
+        p.wall_n = n_wall;
+        mesh->scratch_face.alloc(5 * static_cast<size_t>(m.nf));
+        k_face_flux<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
+                                                                   SField<const double>{grad, 0, 15, 1}, mesh->scratch_face.p);
+        MHD_LAUNCH_CHECK();
+        k_gather_rhs<<<grid_for(m.nc, 256), 256, 0, mesh->stream>>>(m, 1, mesh->scratch_face.p, SField<double>{rhs, 0, 5, 1});
+        MHD_LAUNCH_CHECK();
+        MHD_CUDA(cudaStreamSynchronize(mesh->stream));
     });
 }
 

@@ -17,6 +17,11 @@ struct FluidParams
     double gamma, rel_limit, rho_floor, p_floor;
     Prim5 fs[kMaxSpecies];          // free-stream (inflow ghost) state per species
     int8_t absorb[kMaxSpecies];     // wall ghost: 1 = absorbing floor state, 0 = slip reflection
+    // the caller's Dirichlet wall states (null: none): per face the slot of its state, -1 where the face
+    // keeps ghost_state; wall_prim[(s * wall_n + slot) * 5 + m] the primitives of species s (this launch's)
+    const int32_t *wall_slot = nullptr;
+    const double *wall_prim = nullptr;
+    int64_t wall_n = 0;
 };
 
 // Species-indexed strided field: value(s, i, m) = p[s * ss + i * si + m * sm]
@@ -63,6 +68,16 @@ __device__ __forceinline__ void prim_arr(const Prim5 &w, double *a)
     a[0] = w.rho; a[1] = w.u; a[2] = w.v; a[3] = w.w; a[4] = w.p;
 }
 
+// The Dirichlet wall ghost of a GhostFn (Common/fluid/Reconstruction.h:21) as the ten-ion solver builds it
+// (MarsUns/driver/MarsSolver.cpp:124-128 over its cached wall_state_, :147-165): on a listed wall face the
+// ghost of species s is the caller's state whatever the inside state.  Null where the face keeps ghost_state.
+__device__ __forceinline__ const double *wall_ghost(const FluidParams &p, int kind, int32_t f, int s)
+{
+    if (kind != 1 || !p.wall_slot) return nullptr;
+    const int32_t k = p.wall_slot[f];
+    return k < 0 ? nullptr : p.wall_prim + 5 * ((int64_t)s * p.wall_n + k);
+}
+
 // mhd::rusanov (Common/physics/Euler.h:30-49): flux per unit area through unit normal n (L -> R)
 __device__ __forceinline__ void rusanov(const Prim5 &L, const Prim5 &R, V3 n, double gamma, double *F)
 {
@@ -95,4 +110,7 @@ __device__ __forceinline__ Prim5 face_state(const Prim5 &w, const double *g, V3 
     r.p = w.p + g[12] * dx.x + g[13] * dx.y + g[14] * dx.z;
     return (r.rho > 0 && r.p > 0) ? r : w;
 }
+// Slot map of the caller's wall states: slot[f] = i for faces[i] (device ids), -1 elsewhere (slot holds nf
+// entries).  Throws unless every listed face is a distinct face of kind wall.
+void build_wall_slots(const MeshView &m, const int32_t *faces, int32_t n, int32_t *slot, cudaStream_t s);
 } // namespace mhd

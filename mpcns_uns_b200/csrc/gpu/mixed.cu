@@ -190,7 +190,22 @@ struct MxParams
     float inver_MA2, ne_floor;
     int ambi, chem;             // ambipolar force, chemistry terms (two-ion model)
     double a1_Na, a4, a5, a6, sch, scn, T_ref, Tn0;
+    const int32_t *wall_slot;   // the caller's Dirichlet wall states (FluidParams), global species index
+    const double *wall_prim;
+    int64_t wall_n;
 };
+
+// the caller's wall ghost of face f, species s, in FP32 (FluidParams wall table); false where ghost32 applies
+__device__ __forceinline__ bool wall_ghost32(const MxParams &p, int kind, int32_t f, int s, F5 &g)
+{
+    if (kind != 1 || !p.wall_slot) return false;
+    const int32_t k = p.wall_slot[f];
+    if (k < 0) return false;
+    const double *w = p.wall_prim + 5 * ((int64_t)s * p.wall_n + k);
+    g = F5{static_cast<float>(w[0]), static_cast<float>(w[1]), static_cast<float>(w[2]), static_cast<float>(w[3]),
+           static_cast<float>(w[4])};
+    return true;
+}
 
 __device__ __forceinline__ F5 ghost32(int kind, bool absorb, const F5 &in, float3 n, const F5 &fs)
 {
@@ -409,7 +424,9 @@ __device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int 
             const int32_t f = -(nb[j] + 1);
             const float4 nf = m.fn[f];
             const float sg = m.t_sg[j * n + c];
-            const F5 gh = ghost32(m.face_kind[f], p.absorb[s] != 0, wcp, make_float3(sg * nf.x, sg * nf.y, sg * nf.z), p.fs[s]);
+            F5 gh;
+            if (!wall_ghost32(p, m.face_kind[f], f, s, gh))
+                gh = ghost32(m.face_kind[f], p.absorb[s] != 0, wcp, make_float3(sg * nf.x, sg * nf.y, sg * nf.z), p.fs[s]);
             wn[j][0] = gh.rho; wn[j][1] = gh.u; wn[j][2] = gh.v; wn[j][3] = gh.w; wn[j][4] = gh.p;
         }
     (void)U;
@@ -530,7 +547,8 @@ __device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int 
         }
         const F5 in = state(c, sgn > 0 ? 0 : 1);
         const float sf = static_cast<float>(sgn);
-        const F5 gh = ghost32(kind, p.absorb[s] != 0, in, make_float3(sf * nr.x, sf * nr.y, sf * nr.z), p.fs[s]);
+        F5 gh;
+        if (!wall_ghost32(p, kind, f, s, gh)) gh = ghost32(kind, p.absorb[s] != 0, in, make_float3(sf * nr.x, sf * nr.y, sf * nr.z), p.fs[s]);
         if (sgn > 0) { Ls = in; Rs = gh; }
         else { Rs = in; Ls = gh; }
     }
@@ -946,6 +964,9 @@ MxParams mx_params(const MhdState *st)
     p.chem = st->src.chem;
     p.a1_Na = q.a1_Na; p.a4 = q.a4; p.a5 = q.a5; p.a6 = q.a6;
     p.sch = q.state_coeff_H; p.scn = q.state_coeff_Na; p.T_ref = q.T_ref; p.Tn0 = q.Tn0;
+    p.wall_slot = st->fp.wall_slot;
+    p.wall_prim = st->fp.wall_prim;
+    p.wall_n = st->fp.wall_n;
     for (int s = 0; s < st->nsp; ++s)
     {
         p.fs[s] = F5{static_cast<float>(q.fs[s].rho), static_cast<float>(q.fs[s].u), static_cast<float>(q.fs[s].v),

@@ -47,7 +47,9 @@ struct MhdState
     mhd::DBuf<int8_t> pok;  // the node has fluid cells
     mhd::DBuf<double> photo, vst; // source fields of the chemistry terms (empty: absent)
     mhd::DBuf<float4> g32;  // mixed precision: face terms A_f x b_f of the cell current (per face)
-    mhd::DBuf<float4> d32;  // mixed precision: face terms p_e,f A_f of grad p_e (per face)
+    mhd::DBuf<float4> d32;  // mixed precision: face terms (p_R - p_L) A_f / 2 of grad p_e (per face)
+    mhd::DBuf<int32_t> wall_slot; // the caller's Dirichlet wall states: slot per face (-1: ghost_state)
+    mhd::DBuf<double> wall_prim;  // [species][slot][5]
     mhd::DBuf<double> mres; // explicit resistive EMF: m_e = eta_e / star1_e per edge (empty: off)
     int8_t *floor_flags = nullptr; // when set, the update records the floors it applied ([s*nc + c])
     mhd::DBuf<double> scal; // [0] dt

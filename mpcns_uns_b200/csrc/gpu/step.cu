@@ -347,6 +347,7 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
             gp.fs[g] = st->fp.fs[s0 + g];
             gp.absorb[g] = st->fp.absorb[s0 + g];
         }
+        if (gp.wall_prim) gp.wall_prim = st->fp.wall_prim + (int64_t)s0 * 5 * st->fp.wall_n;
         const SField<const double> Wg{st->W.p + (int64_t)s0 * 5 * nc, 5 * nc, 1, nc};
         const SField<double> Gg{st->grad.p, 15 * nc, 1, nc};
         P.begin(KP_GRAD, s);
@@ -437,6 +438,39 @@ void read_dt(MhdState *st, double *dt_host)
 using namespace mhd;
 
 extern "C" {
+
+int mhd_gpu_state_set_wall_ghosts(MhdState *st, int32_t n_wall, const int32_t *faces, const double *prims)
+{
+    return guarded([&] {
+        MHD_REQUIRE(st, "null state");
+        MHD_REQUIRE(n_wall >= 0 && (!n_wall || (faces && prims)), "bad wall ghost table");
+        st->fp.wall_slot = nullptr;
+        st->fp.wall_prim = nullptr;
+        st->fp.wall_n = 0;
+        st->wall_slot.release();
+        st->wall_prim.release();
+        if (!n_wall) return;
+        const MeshView &m = st->mesh->v;
+        cudaStream_t s = st->mesh->stream;
+        DBuf<int32_t> df;
+        df.upload(faces, (size_t)n_wall);
+        st->wall_slot.alloc(m.nf ? (size_t)m.nf : 1);
+        try
+        {
+            build_wall_slots(m, df.p, n_wall, st->wall_slot.p, s);
+        }
+        catch (...)
+        {
+            st->wall_slot.release();
+            throw;
+        }
+        st->wall_prim.upload(prims, (size_t)st->nsp * n_wall * 5);
+        MHD_CUDA(cudaStreamSynchronize(s));
+        st->fp.wall_slot = st->wall_slot.p;
+        st->fp.wall_prim = st->wall_prim.p;
+        st->fp.wall_n = n_wall;
+    });
+}
 
 int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
 {

@@ -81,6 +81,9 @@ _SIGS = {
     "mhd_gpu_to_prim": ([vp, vp, i32, dbl, dbl, dbl, vp], ctypes.c_int),
     "mhd_gpu_limited_gradients": ([vp, vp, i32, ctypes.POINTER(Prim), i32, dbl, vp], ctypes.c_int),
     "mhd_gpu_flux_rhs": ([vp, dbl, i32, ctypes.POINTER(Prim), vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_limited_gradients_wall": ([vp, vp, i32, ctypes.POINTER(Prim), i32, dbl, i32, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_flux_rhs_wall": ([vp, dbl, i32, ctypes.POINTER(Prim), vp, vp, i32, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_state_set_wall_ghosts": ([vp, i32, vp, vp], ctypes.c_int),
     "mhd_gpu_cell_vector": ([vp, vp, i32, vp], ctypes.c_int),
     "mhd_gpu_ideal_emf": ([vp, vp, vp, vp, vp, vp, dbl, vp], ctypes.c_int),
     "mhd_gpu_edge_modes": ([vp, vp, vp, vp], ctypes.c_int),
@@ -247,26 +250,37 @@ class DeviceMesh:
         self._leave()
         return W
 
-    def limited_gradients(self, W, species, freestream, limit=True, rel_limit=0.0):
-        """Stencil::limited_gradients (Common/fluid/Reconstruction.cpp:80-142): 15 per cell."""
+    def limited_gradients(self, W, species, freestream, limit=True, rel_limit=0.0, wall=None):
+        """Stencil::limited_gradients (Common/fluid/Reconstruction.cpp:80-142): 15 per cell.  wall: (faces,
+        prims n_wall x 5 of this species), the Dirichlet wall table of the GhostFn argument."""
         torch = _torch()
         W = dev(W)
         g = torch.empty(15 * self.n_cells, dtype=torch.float64, device="cuda")
         fs = Prim(*[float(v) for v in freestream])
         self._enter()
-        check(lib().mhd_gpu_limited_gradients(self._h, ptr(W), int(species), ctypes.byref(fs), int(bool(limit)),
-                                              float(rel_limit), ptr(g)))
+        if wall is None:
+            check(lib().mhd_gpu_limited_gradients(self._h, ptr(W), int(species), ctypes.byref(fs), int(bool(limit)),
+                                                  float(rel_limit), ptr(g)))
+        else:
+            fc, pr = _wall_dev(wall)
+            check(lib().mhd_gpu_limited_gradients_wall(self._h, ptr(W), int(species), ctypes.byref(fs), int(bool(limit)),
+                                                       float(rel_limit), fc.numel(), ptr(fc), ptr(pr), ptr(g)))
         self._leave()
         return g
 
-    def fluid_flux_rhs(self, gamma, species, freestream, W, grad):
-        """mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:30-74): 5 per cell."""
+    def fluid_flux_rhs(self, gamma, species, freestream, W, grad, wall=None):
+        """mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:30-74): 5 per cell.  wall: as limited_gradients."""
         torch = _torch()
         W, grad = dev(W), dev(grad)
         r = torch.empty(5 * self.n_cells, dtype=torch.float64, device="cuda")
         fs = Prim(*[float(v) for v in freestream])
         self._enter()
-        check(lib().mhd_gpu_flux_rhs(self._h, float(gamma), int(species), ctypes.byref(fs), ptr(W), ptr(grad), ptr(r)))
+        if wall is None:
+            check(lib().mhd_gpu_flux_rhs(self._h, float(gamma), int(species), ctypes.byref(fs), ptr(W), ptr(grad), ptr(r)))
+        else:
+            fc, pr = _wall_dev(wall)
+            check(lib().mhd_gpu_flux_rhs_wall(self._h, float(gamma), int(species), ctypes.byref(fs), ptr(W), ptr(grad), fc.numel(),
+                                              ptr(fc), ptr(pr), ptr(r)))
         self._leave()
         return r
 
@@ -489,6 +503,18 @@ class ResidentState:
         a = [None if x is None else np.ascontiguousarray(x, np.float64) for x in (photo, vst)]
         check(lib().mhd_gpu_state_set_source_fields(self._h, *[None if x is None else x.ctypes.data_as(vp) for x in a]))
 
+    def set_wall_ghosts(self, faces=None, prims=None):
+        """The step's Dirichlet wall table: faces (distinct faces of kind wall) and prims (n_species x n_wall x 5);
+        None removes it."""
+        if faces is None or len(faces) == 0:
+            check(lib().mhd_gpu_state_set_wall_ghosts(self._h, 0, None, None))
+            return
+        fc = np.ascontiguousarray(faces, np.int32)
+        pr = np.ascontiguousarray(prims, np.float64)
+        if pr.size != self.params.n_species * fc.size * 5:
+            raise ValueError("prims must hold n_species x n_wall x 5 values")
+        check(lib().mhd_gpu_state_set_wall_ghosts(self._h, fc.size, fc.ctypes.data_as(vp), pr.ctypes.data_as(vp)))
+
     def set_resistivity(self, m_edge):
         """Explicit resistive EMF m_e (d1^T star2 Phi)_e per stage (m_edge per edge; None: off)."""
         if m_edge is None:
@@ -496,6 +522,14 @@ class ResidentState:
             return
         a = np.ascontiguousarray(m_edge, np.float64)
         check(lib().mhd_gpu_state_set_resistivity(self._h, a.ctypes.data_as(vp)))
+
+
+def _wall_dev(wall):
+    torch = _torch()
+    faces, prims = wall
+    fc = torch.as_tensor(np.ascontiguousarray(faces, np.int32)).to("cuda")
+    pr = dev(np.ascontiguousarray(prims, np.float64).ravel())
+    return fc, pr
 
 
 class GeometryArgs(ctypes.Structure):

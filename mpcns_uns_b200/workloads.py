@@ -290,6 +290,24 @@ def adjoint_case(ncube=32, nr=64, r_in=1.0, r_out=6.0, n_steps=40, checkpoint_ev
     return AdjointCase(wl=wl, eta=eta, mask=mask, n_steps=n_steps, checkpoint_every=checkpoint_every)
 
 
+def wall_states(mesh: HostMesh, rho_up, masses, T_wall=0.05, seed=0):
+    """A Dirichlet wall table in the form of the ten-ion solver's wall ghost (MarsUns/driver/MarsSolver.cpp:147-165:
+    a photochemical-equilibrium ion density at the wall face centre, at rest, p = n k T_wall), with a seeded stand-in
+    for the atmosphere model: per wall face and species rho = rho_up[s] 10^U(0, 1) (1 + 0.5 x/r) (dayside-enhanced),
+    u = 0, p = rho / m_s * T_wall.  Returns (faces int32, prims n_species x n_wall x 5)."""
+    kind = np.asarray(mesh["face_kind"])
+    faces = np.nonzero(kind == 1)[0].astype(np.int32)
+    fc = np.asarray(mesh["face_center"], np.float64).reshape(-1, 3)[faces]
+    r = np.linalg.norm(fc, axis=1)
+    rng = np.random.default_rng(seed)
+    prims = np.zeros((len(rho_up), faces.size, 5))
+    for s, (rho0, m) in enumerate(zip(rho_up, masses)):
+        rho = rho0 * 10.0 ** rng.uniform(0.0, 1.0, faces.size) * (1.0 + 0.5 * fc[:, 0] / r)
+        prims[s, :, 0] = rho
+        prims[s, :, 4] = rho / m * T_wall
+    return faces, prims
+
+
 TEN_ION_MASSES = [1.0, 2.0, 4.0, 12.0, 14.0, 16.0, 28.0, 30.0, 32.0, 44.0]
 
 

@@ -34,7 +34,8 @@ class StepParams(ctypes.Structure):
                 ("B_imf", dbl * 3), ("mass", dbl * 16), ("fs", (dbl * 5) * 16), ("lorentz", i32), ("pad", i32),
                 ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p), ("ambipolar", i32), ("chemistry", i32),
                 ("pressure_coef", dbl), ("a1_Na", dbl), ("a4", dbl), ("a5", dbl), ("a6", dbl), ("state_coeff_H", dbl),
-                ("state_coeff_Na", dbl), ("T_ref", dbl), ("Tn0", dbl), ("photo", ctypes.c_void_p), ("vst", ctypes.c_void_p)]
+                ("state_coeff_Na", dbl), ("T_ref", dbl), ("Tn0", dbl), ("photo", ctypes.c_void_p), ("vst", ctypes.c_void_p),
+                ("n_wall", i32), ("pad2", i32), ("wall_faces", ctypes.c_void_p), ("wall_prims", ctypes.c_void_p)]
 
 
 def lib():
@@ -59,6 +60,8 @@ def lib():
             ("ref_to_prim", [vp, i64, dbl, dbl, dbl, vp], None),
             ("ref_limited_gradients", [vp, vp, i32, vp, i32, dbl, vp], ctypes.c_int),
             ("ref_flux_rhs", [vp, dbl, i32, vp, vp, vp, vp], ctypes.c_int),
+            ("ref_limited_gradients_wall", [vp, vp, i32, vp, i32, dbl, i32, vp, vp, vp], ctypes.c_int),
+            ("ref_flux_rhs_wall", [vp, dbl, i32, vp, vp, vp, i32, vp, vp, vp], ctypes.c_int),
             ("ref_cell_vector", [vp, vp, vp], None),
             ("ref_ideal_emf", [vp, vp, vp, vp, vp, vp, dbl, vp], None),
             ("ref_faraday", [vp, vp, vp, dbl], None),
@@ -234,6 +237,27 @@ class RefMesh:
         g = np.zeros(15 * self.n_cells)
         _check(lib().ref_limited_gradients(self._h, _p(W), species, _p(fs_), int(limit), rel_limit, _p(g)))
         return g
+
+    def limited_gradients_wall(self, W, species, fs, faces, prims, limit=True, rel_limit=0.0):
+        """limited_gradients with the Dirichlet wall table (prims: n_wall x 5 of this species)."""
+        W = np.ascontiguousarray(W, np.float64)
+        fs_ = np.asarray(fs, np.float64)
+        fc = np.ascontiguousarray(faces, np.int32)
+        pr = np.ascontiguousarray(prims, np.float64)
+        g = np.zeros(15 * self.n_cells)
+        _check(lib().ref_limited_gradients_wall(self._h, _p(W), species, _p(fs_), int(limit), rel_limit, fc.size, _p(fc), _p(pr), _p(g)))
+        return g
+
+    def flux_rhs_wall(self, W, grad, species, fs, gamma, faces, prims):
+        """fluid_flux_rhs with the Dirichlet wall table (prims: n_wall x 5 of this species)."""
+        W = np.ascontiguousarray(W, np.float64)
+        grad = np.ascontiguousarray(grad, np.float64)
+        fs_ = np.asarray(fs, np.float64)
+        fc = np.ascontiguousarray(faces, np.int32)
+        pr = np.ascontiguousarray(prims, np.float64)
+        r = np.zeros(5 * self.n_cells)
+        _check(lib().ref_flux_rhs_wall(self._h, gamma, species, _p(fs_), _p(W), _p(grad), fc.size, _p(fc), _p(pr), _p(r)))
+        return r
 
     def flux_rhs(self, W, grad, species, fs, gamma):
         W = np.ascontiguousarray(W, np.float64)

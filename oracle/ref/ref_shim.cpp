@@ -16,6 +16,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "boundary/BoundaryInfo.h"
@@ -317,6 +318,61 @@ int ref_limited_gradients(void *h, const double *W, int32_t species, const doubl
     });
 }
 
+// A GhostFn (Common/fluid/Reconstruction.h:21) over a per-face table, bound as the ten-ion solver binds
+// its ghost_ (MarsUns/driver/MarsSolver.cpp:124-128): listed wall faces return the table's state of the
+// species, every other face ghost_state.  prims: [species][i][5] with species_stride entries per species.
+static GhostFn table_ghost(const RefMesh *r, int32_t n_wall, const int32_t *faces, const double *prims, int64_t species_stride,
+                    std::unordered_map<Id, int32_t> &slot, const Prim *fs_all, bool species_relative)
+{
+    slot.clear();
+    for (int32_t i = 0; i < n_wall; ++i) slot.emplace(faces[i], i);
+    const BoundaryInfo *bc = &r->bc;
+    return [bc, &slot, prims, species_stride, fs_all, species_relative](Id f, int s, const Prim &in, const Vec3 &n) -> Prim {
+        const FaceKind k = bc->face_kind[f];
+        if (k == FaceKind::Wall)
+        {
+            auto it = slot.find(f);
+            if (it != slot.end())
+            {
+                const double *w = prims + 5 * (species_stride * (species_relative ? 0 : s) + it->second);
+                return Prim{w[0], w[1], w[2], w[3], w[4]};
+            }
+        }
+        return ghost_state(k, s, in, n, fs_all[species_relative ? 0 : s]);
+    };
+}
+
+// limited_gradients with the table GhostFn; prims [n_wall][5] of this species
+int ref_limited_gradients_wall(void *h, const double *W, int32_t species, const double *fs, int32_t limit, double rel_limit,
+                               int32_t n_wall, const int32_t *faces, const double *prims, double *grad)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        if (!r->have_bc) throw std::runtime_error("boundary classification missing");
+        ensure_stencil(r);
+        r->stencil->set_rel_limit(rel_limit);
+        const Prim p{fs[0], fs[1], fs[2], fs[3], fs[4]};
+        std::unordered_map<Id, int32_t> slot;
+        const GhostFn g = table_ghost(r, n_wall, faces, prims, n_wall, slot, &p, true);
+        r->stencil->limited_gradients(r->lm, r->geo, r->bc, W, species, p, limit != 0, grad, &g);
+    });
+}
+
+// fluid_flux_rhs with the table GhostFn; prims [n_wall][5] of this species
+int ref_flux_rhs_wall(void *h, double gamma, int32_t species, const double *fs, const double *W, const double *grad, int32_t n_wall,
+                      const int32_t *faces, const double *prims, double *rhs)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        if (!r->have_bc) throw std::runtime_error("boundary classification missing");
+        r->cfg.sc.gamma = gamma;
+        const Prim p{fs[0], fs[1], fs[2], fs[3], fs[4]};
+        std::unordered_map<Id, int32_t> slot;
+        const GhostFn g = table_ghost(r, n_wall, faces, prims, n_wall, slot, &p, true);
+        fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, species, p, W, grad, rhs, &g);
+    });
+}
+
 // mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:30-74)
 int ref_flux_rhs(void *h, double gamma, int32_t species, const double *fs, const double *W, const double *grad, double *rhs)
 {
@@ -499,6 +555,10 @@ struct RefStepParams
     int32_t ambipolar, chemistry;
     double pressure_coef, a1_Na, a4, a5, a6, state_coeff_H, state_coeff_Na, T_ref, Tn0;
     const double *photo, *vst;
+    // Dirichlet wall table (the ten-ion solver's GhostFn): faces[n_wall], prims[species][n_wall][5]
+    int32_t n_wall, pad2;
+    const int32_t *wall_faces;
+    const double *wall_prims;
 };
 
 namespace
@@ -670,12 +730,17 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
                 w.dpe.assign(3 * static_cast<size_t>(nc), 0.0);
                 mercury::electron_pressure_gradient(r->lm, r->geo, w.W[0].data(), w.W[1].data(), w.dpe.data());
             }
+            Prim fs_all[16];
+            for (int k = 0; k < ns; ++k) fs_all[k] = Prim{p.fs[k][0], p.fs[k][1], p.fs[k][2], p.fs[k][3], p.fs[k][4]};
+            std::unordered_map<Id, int32_t> wslot;
+            const GhostFn wg = p.n_wall > 0 ? table_ghost(r, p.n_wall, p.wall_faces, p.wall_prims, p.n_wall, wslot, fs_all, false) : GhostFn{};
+            const GhostFn *gp = p.n_wall > 0 ? &wg : nullptr;
             for (int k = 0; k < ns; ++k)
             {
-                const Prim fs{p.fs[k][0], p.fs[k][1], p.fs[k][2], p.fs[k][3], p.fs[k][4]};
-                if (p.second_order) r->stencil->limited_gradients(r->lm, r->geo, r->bc, w.W[k].data(), k, fs, true, w.grad[k].data());
+                const Prim &fs = fs_all[k];
+                if (p.second_order) r->stencil->limited_gradients(r->lm, r->geo, r->bc, w.W[k].data(), k, fs, true, w.grad[k].data(), gp);
                 else std::fill(w.grad[k].begin(), w.grad[k].end(), 0.0);
-                fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, k, fs, w.W[k].data(), w.grad[k].data(), w.rhs[k].data());
+                fluid_flux_rhs(r->lm, r->geo, r->bc, r->cfg, k, fs, w.W[k].data(), w.grad[k].data(), w.rhs[k].data(), gp);
             }
             if (lorentz || ambipolar || chemistry) // Solver::rhs (Solver.cpp:146-149): sources of both species after both flux passes
             {

@@ -98,6 +98,50 @@ def test_flux_rhs(meshes, species):
     assert rel_err(rhs, rr) < TOL
 
 
+def _wall_table(h, rng):
+    walls = np.nonzero(np.asarray(h["face_kind"]) == 1)[0].astype(np.int32)
+    faces = walls[::2]   # every other wall face: the rest keep ghost_state
+    prims = np.column_stack([rng.uniform(0.2, 2.0, faces.size), rng.uniform(-0.3, 0.3, (faces.size, 3)),
+                             rng.uniform(0.05, 0.5, faces.size)])
+    return faces, prims
+
+
+@pytest.mark.parametrize("species", [0, 1])
+def test_limited_gradients_and_flux_wall_table(meshes, species):
+    """The GhostFn argument of limited_gradients / fluid_flux_rhs as a Dirichlet wall table (the ten-ion
+    solver's wall ghost), seeded states on every other wall face, against the reference with the same table."""
+    h, r, d, bc = meshes
+    rng = np.random.default_rng(300 + species)
+    faces, prims = _wall_table(h, rng)
+    if faces.size == 0:
+        pytest.skip("mesh without wall faces")
+    W = random_prims(h.n_cells, rng)
+    fs = (1.1, 0.3, -0.2, 0.1, 0.12)
+    g = _np(d.limited_gradients(W, species, fs, True, 0.0, wall=(faces, prims)))
+    gr = r.limited_gradients_wall(W, species, fs, faces, prims)
+    assert rel_err(g, gr) < TOL
+    assert not np.array_equal(gr, r.limited_gradients(W, species, fs, True, 0.0))   # the table acts
+    rhs = _np(d.fluid_flux_rhs(5 / 3, species, fs, W, gr, wall=(faces, prims)))
+    rr = r.flux_rhs_wall(W, gr, species, fs, 5 / 3, faces, prims)
+    assert rel_err(rhs, rr) < TOL
+    assert not np.array_equal(rr, r.flux_rhs(W, gr, species, fs, 5 / 3))
+
+
+def test_wall_table_rejects_bad_faces(meshes):
+    from mpcns_uns_b200.gpu import MhdError
+    h, r, d, bc = meshes
+    kind = np.asarray(h["face_kind"])
+    W = random_prims(h.n_cells, np.random.default_rng(5))
+    fs = (1.0, 0.0, 0.0, 0.0, 0.1)
+    other = np.nonzero(kind != 1)[0][:1].astype(np.int32)
+    with pytest.raises(MhdError, match="kind wall"):
+        d.limited_gradients(W, 0, fs, wall=(other, np.ones((1, 5))))
+    walls = np.nonzero(kind == 1)[0].astype(np.int32)
+    if walls.size:
+        with pytest.raises(MhdError, match="distinct"):
+            d.limited_gradients(W, 0, fs, wall=(np.array([walls[0], walls[0]], np.int32), np.ones((2, 5))))
+
+
 def test_cell_vector(meshes):
     h, r, d, bc = meshes
     rng = np.random.default_rng(300)

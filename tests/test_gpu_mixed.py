@@ -12,7 +12,7 @@ L2_TOL = 1e-5
 DIVB_TOL = 1e-12
 
 
-def _run(wl, precision, nsteps, fields=None, **kw):
+def _run(wl, precision, nsteps, fields=None, wall=None, **kw):
     from mpcns_uns_b200 import gpu
     dm = gpu.DeviceMesh(wl.mesh)
     p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, precision=precision, **kw)
@@ -20,6 +20,8 @@ def _run(wl, precision, nsteps, fields=None, **kw):
     st.set(wl.U, wl.Phi, wl.PhiAdd)
     if fields is not None:
         st.set_source_fields(*fields)
+    if wall is not None:
+        st.set_wall_ghosts(*wall)
     dts = [st.step(0.0) for _ in range(nsteps)]
     return [st.U(s) for s in range(wl.n_species)], st.Phi(), dts, dm
 
@@ -108,3 +110,21 @@ def test_mixed_vs_fp64_all_sources(induce):
     # the ambipolar and chemistry terms act on this workload, well above the tolerance
     assert _l2(Ul[1], U64[1]) > 1e-2
     assert np.linalg.norm(Pl - P64) / np.linalg.norm(P64 + wl.PhiAdd) > 1e-4
+
+
+def test_mixed_vs_fp64_ten_ions_wall_table():
+    """Ten ions with the Dirichlet wall table: the mixed step against the FP64 step."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.ten_ion(6, 8)
+    wall = workloads.wall_states(wl.mesh, [f[0] for f in wl.fs], wl.mass, seed=5)
+    n = 10
+    U64, P64, dt64, dm = _run(wl, "fp64", n, wall=wall)
+    U32, P32, dt32, _ = _run(wl, "mixed", n, wall=wall)
+    Un, _, _, _ = _run(wl, "fp64", n)
+    assert np.allclose(dt32, dt64, rtol=1e-5)
+    num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(U32, U64))
+    den = sum(float(np.sum(b ** 2)) for b in U64)
+    assert np.sqrt(num / den) < L2_TOL
+    assert dm.div_b(P32)["max_rel"] < DIVB_TOL
+    num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(Un, U64))
+    assert np.sqrt(num / den) > 1e-6      # the table acts

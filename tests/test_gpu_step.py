@@ -36,7 +36,7 @@ def ref_params(p):
     return rp
 
 
-def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None):
+def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None, wall=None):
     from mpcns_uns_b200 import gpu
     h = wl.mesh
     r = ref_twin(h, tags).boundary(*bc)
@@ -54,6 +54,10 @@ def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None):
         st.set_source_fields(*fields)
         keep = [np.ascontiguousarray(x, np.float64) for x in fields]
         rp.photo, rp.vst = keep[0].ctypes.data, keep[1].ctypes.data
+    if wall is not None:     # the Dirichlet wall table (faces, prims n_species x n_wall x 5) on both sides
+        st.set_wall_ghosts(*wall)
+        wkeep = (np.ascontiguousarray(wall[0], np.int32), np.ascontiguousarray(wall[1], np.float64))
+        rp.n_wall, rp.wall_faces, rp.wall_prims = wkeep[0].size, wkeep[0].ctypes.data, wkeep[1].ctypes.data
     for k in range(nsteps):
         if use_cfl and wl.n_species == 2:
             W = [r.to_prim(u, wl.gamma) for u in U]
@@ -139,4 +143,23 @@ def test_step_shell_ten_ions():
     from mpcns_uns_b200 import workloads
     wl = workloads.ten_ion(4, 5)
     div = run_pair(wl, SHELL_TAGS, SHELL_BC, 3, use_cfl=False)
+    assert div < 1e-12
+
+
+def test_step_shell_two_ions_wall_table():
+    """The two-ion step with the Dirichlet wall table of the ten-ion solver's GhostFn on every wall face."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5, r_in=1.0, r_out=6.0)
+    wall = workloads.wall_states(wl.mesh, [f[0] for f in wl.fs], wl.mass, seed=3)
+    assert wall[0].size > 0
+    div = run_pair(wl, SHELL_TAGS, SHELL_BC, 4, params_kw=dict(lorentz=True, induce_coeff=0.8, inver_MA2=0.7), wall=wall)
+    assert div < 1e-12
+
+
+def test_step_shell_ten_ions_wall_table():
+    """Ten ions (five species groups per stage) with the wall table: each group reads its own species' states."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.ten_ion(4, 5)
+    wall = workloads.wall_states(wl.mesh, [f[0] for f in wl.fs], wl.mass, seed=4)
+    div = run_pair(wl, SHELL_TAGS, SHELL_BC, 3, use_cfl=False, wall=wall)
     assert div < 1e-12
