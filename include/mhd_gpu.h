@@ -280,6 +280,46 @@ int mhd_gpu_electron_pressure_gradient(MhdMesh *mesh, const double *WH, const do
 int mhd_gpu_ambipolar_emf(MhdMesh *mesh, const MhdStepParams *params, const double *WH, const double *WNa, double *E);
 /* The external source fields of the chemistry terms (mercury::SourceFields photo and vst, host arrays of
  * one value per cell; NULL clears a field, which then contributes nothing, as in the reference). */
+/* ---------------------------------------------------------------- the ten-ion (Mars) source pieces
+ * mars::MarsSolver (MarsUns/driver/MarsSolver.cpp) as device passes.  Ion arrays are species-major with 5
+ * values per cell: U[(s * n_cells + c) * 5 + m] (W likewise, primitives); cell vectors 3 per cell.  The
+ * scales are those of MarsParams::from_params (:40-110). */
+typedef struct MhdMarsParams {
+    int32_t n_species;        /* MARS::NumSpecies (ten ions) */
+    int32_t n_neutral;        /* reactive neutrals of the drag (MARS::NumReactiveNeutral): neutral n has mass[n] */
+    int32_t neutral_stride;   /* values per cell of the neutral array (MARS::NumNeutral) */
+    int32_t ambipolar;        /* is_Ambipolar_Efield */
+    double mass[16];          /* MARS::ParticleMass [kg] */
+    double rho_ref, n_ref, p_ref, time_ref, kB, L, U, q, B;
+    double mag_scale, pressure_scale, ne_floor, rho_floor, p_floor, gamma;
+} MhdMarsParams;
+
+/* MarsSolver::prepare (:287-303): n_e, n_e,eff = sqrt(n_e^2 + ne_floor^2), p_e = sum_s p_s per cell and u+
+ * (3 per cell, zero outside fluid cells) from U and W. */
+int mhd_gpu_mars_plasma(MhdMesh *mesh, const MhdMarsParams *params, const double *U, const double *W, double *ne, double *ne_eff,
+                        double *pe, double *uplus);
+/* grad p by Gauss' theorem with the face-averaged p (MarsSolver.cpp:305-325; Ambipolar.cpp:10-31): 3 per cell,
+ * zero outside the owned non-solid cells. */
+int mhd_gpu_pressure_gradient(MhdMesh *mesh, const double *pe, double *dpe);
+/* The explicit sources of fluid_and_sources_ (:400-418): per ion rhs += (w mag_scale J x B - w grad p_e,
+ * (the same) . u) with w = n_s / n_e,eff; rhs is added to. */
+int mhd_gpu_mars_explicit_sources(MhdMesh *mesh, const MhdMarsParams *params, const double *U, const double *W, const double *Btot,
+                                  const double *J, const double *dpe, const double *ne_eff, double *rhs);
+/* MarsSolver::ambipolar_emf_ (:529-562): E -= pressure_scale (p_b - p_a) / n_e,eff of the edge, on the owned
+ * edges (nodal p_e volume-weighted over the node's fluid cells); needs the mesh's edge_nodes. */
+int mhd_gpu_mars_ambipolar_emf(MhdMesh *mesh, const MhdMarsParams *params, const double *pe, const double *ne, double *E);
+/* MarsSolver::local_dt_ (:330-376) with its global minimum: each ion alone and the plasma's fast mode. */
+int mhd_gpu_mars_time_step(MhdMesh *mesh, const MhdMarsParams *params, double cfl, const double *U, const double *W, const double *Btot,
+                           const double *uplus, double *host_dt);
+/* MarsSolver::implicit_sources_ (:420-520) on U in place: Crank-Nicolson gyration of the coupled ions,
+ * ion-neutral drag and thermal relaxation (backward Euler); neutral: neutral_stride densities per cell [cm^-3]. */
+int mhd_gpu_mars_implicit_sources(MhdMesh *mesh, const MhdMarsParams *params, const double *Btot, const double *neutral, double dt,
+                                  double *U);
+/* The forward-Euler update of MarsSolver::step (:719-726): U += dt rhs on the owned non-solid cells. */
+int mhd_gpu_mars_advance(MhdMesh *mesh, int32_t n_species, const double *rhs, double dt, double *U);
+/* MarsSolver::floors_ (:686-702). */
+int mhd_gpu_mars_floors(MhdMesh *mesh, const MhdMarsParams *params, double *U);
+
 /* The step's Dirichlet wall table (the ten-ion solver's wall_state_, MarsSolver.cpp:147-165, cached per
  * face): host arrays faces[n_wall] (distinct faces of kind wall) and prims[n_species][n_wall][5]; the
  * FP64 and mixed steps use it in the gradients and the face fluxes.  n_wall = 0 removes it.  The

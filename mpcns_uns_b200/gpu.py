@@ -84,6 +84,14 @@ _SIGS = {
     "mhd_gpu_limited_gradients_wall": ([vp, vp, i32, ctypes.POINTER(Prim), i32, dbl, i32, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_flux_rhs_wall": ([vp, dbl, i32, ctypes.POINTER(Prim), vp, vp, i32, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_state_set_wall_ghosts": ([vp, i32, vp, vp], ctypes.c_int),
+    "mhd_gpu_mars_plasma": ([vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_pressure_gradient": ([vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_mars_explicit_sources": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_mars_ambipolar_emf": ([vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_mars_time_step": ([vp, vp, dbl, vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_mars_implicit_sources": ([vp, vp, vp, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_mars_advance": ([vp, i32, vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_mars_floors": ([vp, vp, vp], ctypes.c_int),
     "mhd_gpu_cell_vector": ([vp, vp, i32, vp], ctypes.c_int),
     "mhd_gpu_ideal_emf": ([vp, vp, vp, vp, vp, vp, dbl, vp], ctypes.c_int),
     "mhd_gpu_edge_modes": ([vp, vp, vp, vp], ctypes.c_int),
@@ -389,6 +397,83 @@ class DeviceMesh:
         check(lib().mhd_gpu_cell_current(self._h, ptr(B), ptr(J)))
         self._leave()
         return J
+
+    # ------------------------------------------------------------- the ten-ion (Mars) source pieces
+    # ion arrays species-major, 5 values per cell; mp: MarsParams
+    def mars_plasma(self, mp, U, W):
+        """MarsSolver::prepare (MarsUns/driver/MarsSolver.cpp:287-303): (n_e, n_e,eff, p_e, u+)."""
+        torch = _torch()
+        U, W = dev(U), dev(W)
+        ne, nee, pe = (torch.empty(self.n_cells, dtype=torch.float64, device="cuda") for _ in range(3))
+        up = torch.empty(3 * self.n_cells, dtype=torch.float64, device="cuda")
+        self._enter()
+        check(lib().mhd_gpu_mars_plasma(self._h, ctypes.byref(mp), ptr(U), ptr(W), ptr(ne), ptr(nee), ptr(pe), ptr(up)))
+        self._leave()
+        return ne, nee, pe, up
+
+    def pressure_gradient(self, pe):
+        """grad p by Gauss' theorem with the face-averaged p (MarsSolver.cpp:305-325): 3 per cell."""
+        torch = _torch()
+        pe = dev(pe)
+        d = torch.empty(3 * self.n_cells, dtype=torch.float64, device="cuda")
+        self._enter()
+        check(lib().mhd_gpu_pressure_gradient(self._h, ptr(pe), ptr(d)))
+        self._leave()
+        return d
+
+    def mars_explicit_sources(self, mp, U, W, Btot, J, dpe, ne_eff, rhs):
+        """The explicit J x B and ambipolar force of MarsSolver::fluid_and_sources_ (:400-418), added to rhs in place."""
+        args = [dev(a) for a in (U, W, Btot, J, dpe, ne_eff)]
+        self._enter()
+        check(lib().mhd_gpu_mars_explicit_sources(self._h, ctypes.byref(mp), *[ptr(a) for a in args], ptr(rhs)))
+        self._leave()
+        return rhs
+
+    def mars_ambipolar_emf(self, mp, pe, ne, E):
+        """MarsSolver::ambipolar_emf_ (:529-562), E in place."""
+        pe, ne = dev(pe), dev(ne)
+        self._enter()
+        check(lib().mhd_gpu_mars_ambipolar_emf(self._h, ctypes.byref(mp), ptr(pe), ptr(ne), ptr(E)))
+        self._leave()
+        return E
+
+    def mars_time_step(self, mp, cfl, U, W, Btot, uplus):
+        """MarsSolver::local_dt_ (:330-376)."""
+        args = [dev(a) for a in (U, W, Btot, uplus)]
+        out = ctypes.c_double()
+        self._enter()
+        check(lib().mhd_gpu_mars_time_step(self._h, ctypes.byref(mp), float(cfl), *[ptr(a) for a in args], ctypes.byref(out)))
+        return out.value
+
+    def mars_implicit_sources(self, mp, Btot, neutral, dt, U):
+        """MarsSolver::implicit_sources_ (:420-520), U in place."""
+        Btot, neutral = dev(Btot), dev(neutral)
+        self._enter()
+        check(lib().mhd_gpu_mars_implicit_sources(self._h, ctypes.byref(mp), ptr(Btot), ptr(neutral), float(dt), ptr(U)))
+        self._leave()
+        return U
+
+    def mars_advance(self, n_species, rhs, dt, U):
+        """U += dt rhs on the owned non-solid cells (MarsSolver::step :719-726), in place."""
+        rhs = dev(rhs)
+        self._enter()
+        check(lib().mhd_gpu_mars_advance(self._h, int(n_species), ptr(rhs), float(dt), ptr(U)))
+        self._leave()
+        return U
+
+    def mars_floors(self, mp, U):
+        """MarsSolver::floors_ (:686-702), U in place."""
+        self._enter()
+        check(lib().mhd_gpu_mars_floors(self._h, ctypes.byref(mp), ptr(U)))
+        self._leave()
+        return U
+
+
+class MarsParams(ctypes.Structure):
+    """MhdMarsParams of include/mhd_gpu.h (the scales of MarsParams::from_params, MarsSolver.cpp:40-110)."""
+    _fields_ = [("n_species", i32), ("n_neutral", i32), ("neutral_stride", i32), ("ambipolar", i32), ("mass", dbl * 16)] + \
+               [(n, dbl) for n in ("rho_ref", "n_ref", "p_ref", "time_ref", "kB", "L", "U", "q", "B", "mag_scale", "pressure_scale",
+                                   "ne_floor", "rho_floor", "p_floor", "gamma")]
 
 
 def step_params(n_species, gamma=5.0 / 3.0, fs=None, mass=None, u_inf=(0.0, 0.0, 0.0), B_imf=(0.0, 0.0, 0.0), cuct=0.5,

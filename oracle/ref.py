@@ -60,6 +60,23 @@ def lib():
             ("ref_to_prim", [vp, i64, dbl, dbl, dbl, vp], None),
             ("ref_limited_gradients", [vp, vp, i32, vp, i32, dbl, vp], ctypes.c_int),
             ("ref_flux_rhs", [vp, dbl, i32, vp, vp, vp, vp], ctypes.c_int),
+            ("ref_mars_create", [vp, i32, vp], vp),
+            ("ref_mars_free", [vp], None),
+            ("ref_mars_params", [vp, vp], None),
+            ("ref_mars_freestream", [vp, vp], None),
+            ("ref_mars_size", [vp, ctypes.c_char_p], ctypes.c_int64),
+            ("ref_mars_get", [vp, ctypes.c_char_p, vp], ctypes.c_int),
+            ("ref_mars_set", [vp, ctypes.c_char_p, vp], ctypes.c_int),
+            ("ref_mars_prepare", [vp], ctypes.c_int),
+            ("ref_mars_local_dt", [vp, vp], ctypes.c_int),
+            ("ref_mars_fluid_and_sources", [vp, dbl], ctypes.c_int),
+            ("ref_mars_ambipolar_emf", [vp, vp], ctypes.c_int),
+            ("ref_mars_implicit_sources", [vp, dbl], ctypes.c_int),
+            ("ref_mars_floors", [vp], ctypes.c_int),
+            ("ref_mars_emf", [vp, vp], ctypes.c_int),
+            ("ref_mars_step_nochem", [vp, dbl, vp], ctypes.c_int),
+            ("ref_mars_wall_table", [vp, vp, vp], i32),
+            ("ref_mars_boundary", [vp, vp, vp], None),
             ("ref_limited_gradients_wall", [vp, vp, i32, vp, i32, dbl, i32, vp, vp, vp], ctypes.c_int),
             ("ref_flux_rhs_wall", [vp, dbl, i32, vp, vp, vp, i32, vp, vp, vp], ctypes.c_int),
             ("ref_cell_vector", [vp, vp, vp], None),
@@ -441,3 +458,93 @@ def read_fields(path):
         lib().ref_fields_get(i, name, 4096, ctypes.byref(d), ctypes.byref(c), ctypes.byref(k), _p(v))
         out.append((name.value.decode(), d.value, c.value, v))
     return out, h.value
+
+
+MARS_PARAM_NAMES = ("rho_ref", "n_ref", "p_ref", "time_ref", "kB", "L", "U", "q", "B", "mag_scale", "pressure_scale", "ne_floor",
+                    "rho_floor", "p_floor", "gamma", "cfl", "sw_ux", "sw_uy", "sw_uz", "sw_Bx", "sw_By", "sw_Bz", "ambipolar", "hall",
+                    "second_order", "cuct", "rel_limit")
+
+
+class RefMars:
+    """mars::MarsSolver on a reference mesh (the mesh must outlive it), initialised, with each phase of its step
+    callable alone.  Ion arrays are species-major, 5 values per cell."""
+
+    NS = 10
+
+    def __init__(self, mesh: RefMesh, overrides=()):
+        self.mesh = mesh
+        enc = [o.encode() for o in overrides]
+        arr = (ctypes.c_char_p * max(1, len(enc)))(*enc)
+        h = lib().ref_mars_create(mesh._h, len(enc), ctypes.cast(arr, ctypes.c_void_p))
+        if not h:
+            raise RuntimeError(lib().ref_last_error().decode())
+        self._h = ctypes.c_void_p(h)
+        v = np.zeros(len(MARS_PARAM_NAMES))
+        lib().ref_mars_params(self._h, _p(v))
+        self.params = dict(zip(MARS_PARAM_NAMES, v.tolist()))
+        fs = np.zeros(5 * self.NS)
+        lib().ref_mars_freestream(self._h, _p(fs))
+        self.freestream = fs.reshape(self.NS, 5)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.ref_mars_free(self._h)
+
+    def get(self, name):
+        n = lib().ref_mars_size(self._h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        _check(lib().ref_mars_get(self._h, name.encode(), _p(out)))
+        return out
+
+    def set(self, name, values):
+        v = np.ascontiguousarray(values, np.float64)
+        if v.size != lib().ref_mars_size(self._h, name.encode()):
+            raise ValueError(f"{name}: size mismatch")
+        _check(lib().ref_mars_set(self._h, name.encode(), _p(v)))
+
+    def prepare(self):
+        _check(lib().ref_mars_prepare(self._h))
+
+    def local_dt(self):
+        d = np.zeros(1)
+        _check(lib().ref_mars_local_dt(self._h, _p(d)))
+        return float(d[0])
+
+    def fluid_and_sources(self, dt):
+        _check(lib().ref_mars_fluid_and_sources(self._h, dt))
+
+    def ambipolar_emf(self, E):
+        E = np.array(E, np.float64)
+        _check(lib().ref_mars_ambipolar_emf(self._h, _p(E)))
+        return E
+
+    def emf(self):
+        E = np.zeros(self.mesh.n_edges)
+        _check(lib().ref_mars_emf(self._h, _p(E)))
+        return E
+
+    def implicit_sources(self, dt):
+        _check(lib().ref_mars_implicit_sources(self._h, dt))
+
+    def floors(self):
+        _check(lib().ref_mars_floors(self._h))
+
+    def step_nochem(self, dt_max=1e300):
+        d = np.zeros(1)
+        _check(lib().ref_mars_step_nochem(self._h, dt_max, _p(d)))
+        return float(d[0])
+
+    def wall_table(self):
+        n = lib().ref_mars_wall_table(self._h, None, None)
+        faces = np.zeros(n, np.int32)
+        prims = np.zeros((self.NS, n, 5))
+        lib().ref_mars_wall_table(self._h, _p(faces), _p(prims))
+        return faces, prims
+
+    def boundary(self):
+        fk = np.zeros(self.mesh.n_faces, np.int8)
+        em = np.zeros(self.mesh.n_edges, np.int8)
+        lib().ref_mars_boundary(self._h, _p(fk), _p(em))
+        return fk, em

@@ -866,3 +866,216 @@ void ref_fields_get(int32_t i, char *name, int32_t len, int32_t *dim, int32_t *n
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------- the ten-ion solver
+// mars::MarsSolver (MarsUns/driver/MarsSolver.cpp) built on a checker mesh, with its private members opened
+// to this file only (the class layout is unchanged), so that each phase of MarsSolver::step runs alone and
+// its arrays can be read and set.  Ion arrays cross this boundary species-major, 5 values per cell.
+#include <array>
+#include <complex>
+#include <istream>
+#include <string_view>
+
+#include "induction/IdealEMF.h"
+#include "induction/ImplicitInduction.h"
+#include "physics/MarsAtmosphereModel.h"
+#include "physics/MarsChemistry.h"
+#include "physics/MarsDipoles.h"
+#include "physics/MarsSpecies.h"
+#include "uns/comm/Exchanger.h"
+#include "uns/core/Params.h"
+#define private public
+#include "driver/MarsSolver.h"
+#undef private
+
+struct RefMars
+{
+    mars::MarsParams prm;
+    std::unique_ptr<mars::MarsSolver> s;
+    std::vector<double> rhs_sum; // scratch
+};
+
+extern "C" {
+
+// MarsParams::from_params of the given "name=value" overrides, the solver on the mesh, initialize()
+void *ref_mars_create(void *mesh, int32_t n_overrides, const char *const *overrides)
+{
+    RefMars *out = nullptr;
+    guarded([&] {
+        RefMesh *r = static_cast<RefMesh *>(mesh);
+        Params p;
+        for (int32_t i = 0; i < n_overrides; ++i) p.set_override(overrides[i]);
+        auto *m = new RefMars;
+        m->prm = mars::MarsParams::from_params(p);
+        m->s = std::make_unique<mars::MarsSolver>(MPI_COMM_SELF, r->lm, m->prm);
+        m->s->initialize();
+        out = m;
+    });
+    return out;
+}
+
+void ref_mars_free(void *h) { delete static_cast<RefMars *>(h); }
+
+// the scales in the order of MhdMarsParams: rho_ref n_ref p_ref time_ref kB L U q B mag_scale pressure_scale
+// ne_floor rho_floor p_floor gamma, then cfl sw_u(3) sw_B(3) ambipolar hall second_order cuct rel_limit
+void ref_mars_params(void *h, double *out)
+{
+    const mars::MarsParams &q = static_cast<RefMars *>(h)->prm;
+    const double v[] = {q.rho_ref, q.n, q.p_ref, q.time_ref, q.kB, q.L, q.U, q.q, q.B, q.mag_scale, q.pressure_scale, q.ne_floor,
+                        q.rho_floor, q.p_floor, q.cfg.sc.gamma, q.cfg.cfl, q.sw_u.x, q.sw_u.y, q.sw_u.z, q.sw_B.x, q.sw_B.y, q.sw_B.z,
+                        q.ambipolar ? 1.0 : 0.0, q.hall ? 1.0 : 0.0, q.cfg.second_order ? 1.0 : 0.0, q.cfg.ideal.cuct,
+                        q.cfg.recon_rel_limit};
+    std::memcpy(out, v, sizeof(v));
+}
+
+// the free streams fs_ of the ions (the inflow ghosts), 5 per species
+void ref_mars_freestream(void *h, double *out)
+{
+    const mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+    for (int k = 0; k < mars::NS; ++k)
+    {
+        const Prim &f = s.fs_[k];
+        out[5 * k] = f.rho; out[5 * k + 1] = f.u; out[5 * k + 2] = f.v; out[5 * k + 3] = f.w; out[5 * k + 4] = f.p;
+    }
+}
+
+namespace
+{
+std::vector<double> *mars_array(mars::MarsSolver &s, const std::string &n)
+{
+    if (n == "Phi") return &s.Phi_;
+    if (n == "PhiAdd") return &s.PhiAdd_;
+    if (n == "PhiTot") return &s.PhiTot_;
+    if (n == "BaddCell") return &s.BaddCell_;
+    if (n == "Bind") return &s.Bind_;
+    if (n == "Btot") return &s.Btot_;
+    if (n == "J") return &s.J_;
+    if (n == "uplus") return &s.uplus_;
+    if (n == "ne") return &s.ne_;
+    if (n == "ne_eff") return &s.ne_eff_;
+    if (n == "pe") return &s.pe_;
+    if (n == "dpe") return &s.dpe_;
+    if (n == "neutral") return &s.neutral_;
+    if (n == "photo") return &s.photo_;
+    return nullptr;
+}
+std::vector<double> *mars_species(mars::MarsSolver &s, const std::string &n)
+{
+    if (n == "U") return s.U_;
+    if (n == "W") return s.W_;
+    if (n == "grad") return s.grad_;
+    if (n == "rhs") return s.rhs_;
+    return nullptr;
+}
+} // namespace
+
+// size of a named array (species arrays: all species)
+int64_t ref_mars_size(void *h, const char *name)
+{
+    mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+    if (auto *a = mars_array(s, name)) return static_cast<int64_t>(a->size());
+    if (auto *a = mars_species(s, name)) return static_cast<int64_t>(a[0].size()) * mars::NS;
+    return -1;
+}
+
+int ref_mars_get(void *h, const char *name, double *out)
+{
+    return guarded([&] {
+        mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+        if (auto *a = mars_array(s, name)) { std::copy(a->begin(), a->end(), out); return; }
+        auto *sp = mars_species(s, name);
+        if (!sp) throw std::runtime_error(std::string("unknown array ") + name);
+        for (int k = 0; k < mars::NS; ++k) std::copy(sp[k].begin(), sp[k].end(), out + k * sp[0].size());
+    });
+}
+
+int ref_mars_set(void *h, const char *name, const double *in)
+{
+    return guarded([&] {
+        mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+        if (auto *a = mars_array(s, name)) { std::copy(in, in + a->size(), a->begin()); return; }
+        auto *sp = mars_species(s, name);
+        if (!sp) throw std::runtime_error(std::string("unknown array ") + name);
+        for (int k = 0; k < mars::NS; ++k) std::copy(in + k * sp[0].size(), in + (k + 1) * sp[0].size(), sp[k].begin());
+    });
+}
+
+int ref_mars_prepare(void *h) { return guarded([&] { static_cast<RefMars *>(h)->s->prepare(); }); }
+int ref_mars_local_dt(void *h, double *dt) { return guarded([&] { *dt = static_cast<RefMars *>(h)->s->local_dt_(); }); }
+int ref_mars_fluid_and_sources(void *h, double dt) { return guarded([&] { static_cast<RefMars *>(h)->s->fluid_and_sources_(dt); }); }
+int ref_mars_ambipolar_emf(void *h, double *E) { return guarded([&] { static_cast<RefMars *>(h)->s->ambipolar_emf_(E); }); }
+int ref_mars_implicit_sources(void *h, double dt) { return guarded([&] { static_cast<RefMars *>(h)->s->implicit_sources_(dt); }); }
+int ref_mars_floors(void *h) { return guarded([&] { static_cast<RefMars *>(h)->s->floors_(); }); }
+
+// emf_ (ideal + ambipolar + the boundary edge values) into E (n_edges)
+int ref_mars_emf(void *h, double *E)
+{
+    return guarded([&] {
+        mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+        std::vector<double> e;
+        s.emf_(e);
+        std::copy(e.begin(), e.end(), E);
+    });
+}
+
+// MarsSolver::step (:705-744) without the photochemistry (chemistry_), the Hall solve only if the solver
+// has it on: prepare, dt, fluxes and explicit sources, EMF, forward Euler, Faraday, implicit sources, floors
+int ref_mars_step_nochem(void *h, double dt_max, double *dt_used)
+{
+    return guarded([&] {
+        mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+        const CellComplex &cx = s.lm_.mesh.cx;
+        s.prepare();
+        double dt = std::min(s.local_dt_(), dt_max);
+        if (!std::isfinite(dt) || dt <= 0) throw std::runtime_error("invalid time step");
+        s.fluid_and_sources_(dt);
+        std::vector<double> E;
+        s.emf_(E);
+        for (int k = 0; k < mars::NS; ++k)
+            for (Id c = 0; c < cx.ent[3].n_owned; ++c)
+            {
+                if (cx.cell_material[c] == kSolid) continue;
+                for (int m = 0; m < 5; ++m) s.U_[k][5 * static_cast<std::size_t>(c) + m] += dt * s.rhs_[k][5 * static_cast<std::size_t>(c) + m];
+            }
+        if (s.ind_.active()) throw std::runtime_error("the checker's ten-ion step runs without the Hall term");
+        faraday_update(cx, s.active_, E.data(), s.Phi_.data(), dt);
+        s.implicit_sources_(dt);
+        s.floors_();
+        *dt_used = dt;
+    });
+}
+
+// the wall ghost of every wall face (wall_state_, :147-165): faces[n], prims[species][n][5]; returns n
+int32_t ref_mars_wall_table(void *h, int32_t *faces, double *prims)
+{
+    int32_t n = 0;
+    guarded([&] {
+        mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+        const CellComplex &cx = s.lm_.mesh.cx;
+        std::vector<Id> wf;
+        for (Id f = 0; f < cx.n_faces(); ++f)
+            if (s.bc_.face_kind[f] == FaceKind::Wall) wf.push_back(f);
+        n = static_cast<int32_t>(wf.size());
+        if (!faces) return;
+        for (int32_t i = 0; i < n; ++i) faces[i] = static_cast<int32_t>(wf[i]);
+        for (int k = 0; k < mars::NS; ++k)
+            for (int32_t i = 0; i < n; ++i)
+            {
+                const Prim w = s.wall_state_(wf[i], k);
+                double *o = prims + (static_cast<std::size_t>(k) * n + i) * 5;
+                o[0] = w.rho; o[1] = w.u; o[2] = w.v; o[3] = w.w; o[4] = w.p;
+            }
+    });
+    return n;
+}
+
+// the solver's boundary classification (face_kind, edge_mode), for the device mesh
+void ref_mars_boundary(void *h, int8_t *face_kind, int8_t *edge_mode)
+{
+    mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+    const CellComplex &cx = s.lm_.mesh.cx;
+    for (Id f = 0; f < cx.n_faces(); ++f) face_kind[f] = static_cast<int8_t>(s.bc_.face_kind[f]);
+    for (Id e = 0; e < cx.n_edges(); ++e) edge_mode[e] = static_cast<int8_t>(s.bc_.edge_mode[e]);
+}
+
+} // extern "C"
