@@ -100,7 +100,7 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
             "face_flux": 20 * g * nc + 60 * g * nc + 16 * nf + 24 * nf + 8 * nf + 14 * nf + nf + nc + 20 * g * nf,
             "update": 20 * g * nf + 20 * nc + 40 * g * nc + 60 * g * nc + 4 * nc + nc,
             "face_candidate": 48 * nc + 16 * nf + 16 * nf + 8 * nf + 12 * nf,
-            "edge_emf": 48 * ne + 4 * ne + 24 * e2f + 4 * ne + 4 * ec + nc + 12 * nf + 16 * nf + 8 * nf + 16 * nc + ne + 4 * ne,
+            "edge_emf": 16 * ne + 4 * ne + 24 * e2f + 4 * ne + 4 * ec + nc + 12 * nf + 16 * nf + 8 * nf + 16 * nc + ne + 4 * ne,
             "ct": 4 * ne + 20 * nf + 4 * nf + 5 * f2e + 12 * nf,
         }.get(k, 0.0)
     p = 8
@@ -130,7 +130,7 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that one ncu capture measured
 # on the 6 x 32 x 32 x 48 x 6 shell of the same construction, with the entity count it scales with;
 # the bench line reports it scaled to its own workload (the traffic grows in proportion to that count).
-NCU_TRAFFIC = {("edge_emf", "mixed"): (595.86e6, "ne", 2082912)}
+NCU_TRAFFIC = {("edge_emf", "mixed"): (513.56e6, "ne", 2082912), ("update", "mixed"): (680.87e6, "nc", 1769472)}
 
 
 def ncu_traffic(kernel, precision, counts):

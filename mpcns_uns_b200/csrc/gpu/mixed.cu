@@ -32,7 +32,7 @@ struct MV
         *ec_cell;
     const int8_t *c2f_sgn, *cfa_sgn, *t_sg, *material, *face_kind, *edge_mode, *st_valid, *f2c_sgn, *f2e_sgn;
     const float *wd, *dx, *inv, *recon, *fdx, *ew, *vol_inv;
-    const float4 *fn, *eth, *ee1, *ee2, *em;
+    const float4 *fn, *eth, *em;
     const char2 *fslot;
     const double *cell_volume; // FP64: the update divides the FP64-summed fluxes by it
 };
@@ -47,7 +47,7 @@ MV make_view(const MeshView &m, const MixedTables &t)
     v.c2f_sgn = m.c2f_sgn; v.cfa_sgn = m.cfa_sgn; v.t_sg = m.t_sg; v.material = m.material; v.face_kind = m.face_kind;
     v.edge_mode = m.edge_mode; v.st_valid = m.st_valid; v.f2c_sgn = m.f2c_sgn; v.f2e_sgn = m.f2e_sgn;
     v.wd = t.wd.p; v.dx = t.dx.p; v.inv = t.inv.p; v.recon = t.recon.p; v.fdx = t.fdx.p; v.ew = t.ew.p; v.vol_inv = t.vol_inv.p;
-    v.fn = t.fn.p; v.eth = t.eth.p; v.ee1 = t.ee1.p; v.ee2 = t.ee2.p; v.em = t.em.p;
+    v.fn = t.fn.p; v.eth = t.eth.p; v.em = t.em.p;
     v.fslot = t.fslot.p;
     v.cell_volume = m.cell_volume;
     return v;
@@ -139,20 +139,13 @@ __global__ void k_mx_faces(MeshView m, float4 *fn, float *fdx, char2 *fslot)
     fdx[3 * n + f] = static_cast<float>(dR.x); fdx[4 * n + f] = static_cast<float>(dR.y); fdx[5 * n + f] = static_cast<float>(dR.z);
 }
 
-__global__ void k_mx_edges(MeshView m, float4 *eth, float4 *ee1, float4 *ee2, float4 *em, float *ew)
+__global__ void k_mx_edges(MeshView m, float4 *eth, float4 *em, float *ew)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
     const double L = m.edge_len[e];
     const V3 th = L > 0 ? (1.0 / L) * ld3(m.edge_vec, e) : mk(0, 0, 0);
-    const V3 ax = fabs(th.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
-    V3 e1 = cross(th, ax);
-    const double n1 = sqrt(dot(e1, e1));
-    e1 = n1 > 0 ? (1.0 / n1) * e1 : mk(0, 0, 0);
-    const V3 e2 = cross(th, e1);
     eth[e] = make_float4(static_cast<float>(th.x), static_cast<float>(th.y), static_cast<float>(th.z), static_cast<float>(L));
-    ee1[e] = make_float4(static_cast<float>(e1.x), static_cast<float>(e1.y), static_cast<float>(e1.z), 0.f);
-    ee2[e] = make_float4(static_cast<float>(e2.x), static_cast<float>(e2.y), static_cast<float>(e2.z), 0.f);
     const V3 mid = ld3(m.edge_mid, e);
     for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k)
     {
@@ -736,20 +729,24 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
     Ef[f] = make_float4(-E.x, -E.y, -E.z, static_cast<float>(phi[f]) / nf4.w);
 }
 
-// UCT edge EMF (IdealEMF.cpp:59-128) with the boundary edge values (Solver.cpp:162-167)
-__global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float4 *__restrict__ Ef, const float4 *__restrict__ up,
-                                                 const double *__restrict__ phi, float cuct, float3 E_inf, float *__restrict__ E)
+// UCT edge EMF (IdealEMF.cpp:59-128) with the boundary edge values (Solver.cpp:162-167), one thread per
+// edge.  The faces' terms enter only through sums, so one pass over the faces accumulates them: with
+// q_i = (q_a, q_b), w_i the face weight and x_i = w_i a_i sigma_i Phi_i/|A_i|,
+//   M = sum w q q^T, g = sum w q, E_u = sum (1 - q . l) x = sum x - l . sum q x,  l = M^-1 g,
+// so no per-face state is kept between two passes.  The basis (e1, e2) of the plane normal to the edge
+// is rebuilt from the unit tangent as the tables build it (the result does not depend on the choice of
+// orthonormal basis).
+__global__ void __launch_bounds__(128) k_mx_edge(MV m, const float4 *__restrict__ Ef, const float4 *__restrict__ up,
+                                                    const double *__restrict__ phi, float cuct, float3 E_inf, float *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
-    const int64_t nf = m.nf;
     float val = 0.f;
     const float4 t4 = m.eth[e];
     const float Lg = t4.w;
     const float3 th = f3(t4);
     const int mode = e < m.no_edges ? m.edge_mode[e] : -1;
-    if (mode == 1) val = 0.f;
-    else if (mode == 2) val = Lg * fdot(E_inf, th);
+    if (mode == 2) val = Lg * fdot(E_inf, th);
     else if (mode == 0)
     {
         const int32_t f0 = m.e2f_ptr[e], nfe = m.e2f_ptr[e + 1] - f0;
@@ -769,15 +766,15 @@ __global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float4 *__restri
         }
         if (nfe > 0 && Lg > 0.f && any_fluid)
         {
-            const float3 e1 = f3(m.ee1[e]), e2 = f3(m.ee2[e]);
-            // per face: q (2 components in the edge-normal plane) and w a sigma Phi/A; three arrays
-            // instead of six keep the kernel at 6 resident blocks of 128 threads
-            float qa[8], qb[8], wx[8];
-            float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
+            const float3 ax = fabsf(th.x) < 0.9f ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
+            float3 e1 = fcross(th, ax);
+            const float n1 = sqrtf(fdot(e1, e1));
+            e1 = n1 > 0.f ? make_float3(e1.x / n1, e1.y / n1, e1.z / n1) : make_float3(0.f, 0.f, 0.f);
+            const float3 e2 = fcross(th, e1);
+            float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f, S0 = 0.f, S1 = 0.f, S2 = 0.f;
+#pragma unroll 1
+            for (int i = 0; i < nfe; ++i)
             {
-                if (i >= nfe) break;
                 const int32_t f = m.e2f_idx[f0 + i];
                 const float4 mi4 = m.em[f0 + i];
                 const float3 mi = f3(mi4);
@@ -791,14 +788,17 @@ __global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float4 *__restri
                 else
                     for (int32_t k = q0; k < q1; ++k) a = fmaxf(a, fabsf(fdot(f3(up[m.ec_cell[k]]), mi)));
                 const float as = a * mi4.w;
-                qa[i] = as * (nf4.x * e1.x + nf4.y * e1.y + nf4.z * e1.z);
-                qb[i] = as * (nf4.x * e2.x + nf4.y * e2.y + nf4.z * e2.z);
-                wx[i] = w * as * ef.w;
-                M11 += w * qa[i] * qa[i];
-                M12 += w * qa[i] * qb[i];
-                M22 += w * qb[i] * qb[i];
-                g1 += w * qa[i];
-                g2 += w * qb[i];
+                const float qa = as * (nf4.x * e1.x + nf4.y * e1.y + nf4.z * e1.z);
+                const float qb = as * (nf4.x * e2.x + nf4.y * e2.y + nf4.z * e2.z);
+                const float wx = w * as * ef.w;
+                M11 += w * qa * qa;
+                M12 += w * qa * qb;
+                M22 += w * qb * qb;
+                g1 += w * qa;
+                g2 += w * qb;
+                S0 += wx;
+                S1 += qa * wx;
+                S2 += qb * wx;
             }
             const float tr = M11 + M22;
             const float eps = 1e-14f * tr;
@@ -809,13 +809,7 @@ __global__ void __launch_bounds__(128, 6) k_mx_edge(MV m, const float4 *__restri
                 l1 = ((M22 + eps) * g1 - M12 * g2) / det;
                 l2 = ((M11 + eps) * g2 - M12 * g1) / det;
             }
-            float Eu = 0.f;
-#pragma unroll
-            for (int i = 0; i < 8; ++i)
-            {
-                if (i >= nfe) break;
-                Eu += (1.f - (qa[i] * l1 + qb[i] * l2)) * wx[i];
-            }
+            const float Eu = S0 - (l1 * S1 + l2 * S2);
             val = Lg * Ec + 2.f * cuct * Lg * Eu;
         }
     }
@@ -880,6 +874,7 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, int n
 // gyr: the closing half-step gyration of the Strang splitting (mercury::gyrate, FP64 on the averaged
 // state, with the total field of the stage-2 prepare) applied to the cell's two ions before they are
 // written, instead of in a pass of its own
+template <bool GYR>
 __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int ng, const float *__restrict__ F,
                                                    const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
                                                    int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
@@ -892,7 +887,7 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int
     double r0[5], r1[5];
     mx_update_one(m, p, s0, 0, c, F, Ub, Uo, dtp, stage2, W, G, bt, D, photo, vst, r0);
     if (ng > 1) mx_update_one(m, p, s0, 1, c, F, Ub, Uo, dtp, stage2, W, G, bt, D, photo, vst, r1);
-    if (gyr && ng == 2 && c < m.no_cells && m.material[c] != 1) gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), 0.5 * *dtp, r0, r1);
+    if (GYR && gyr && ng == 2 && c < m.no_cells && m.material[c] != 1) gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), 0.5 * *dtp, r0, r1);
     double *u0 = Uo + (int64_t)s0 * 5 * n;
 #pragma unroll
     for (int q = 0; q < 5; ++q) u0[q * n + c] = r0[q];
@@ -991,10 +986,10 @@ void mixed_setup(MhdState *st)
     if (st->src.on) st->g32.alloc(nf);
     if (st->src.ambi) st->d32.alloc(nf);
     t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
-    t.eth.alloc(ne); t.ee1.alloc(ne); t.ee2.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
+    t.eth.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
     if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.wd.p, t.dx.p, t.inv.p, t.recon.p, t.vol_inv.p);
     if (nf) k_mx_faces<<<grid_for(nf, 256), 256, 0, s>>>(m, t.fn.p, t.fdx.p, t.fslot.p);
-    if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.ee1.p, t.ee2.p, t.em.p, t.ew.p);
+    if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.em.p, t.ew.p);
     MHD_LAUNCH_CHECK();
     st->W32.alloc(8 * nc * st->nsp); // 8 floats per (species, cell): rho u v w | p, padded to 32 bytes
     st->grad32.alloc(20 * nc * st->group); // limited face values, 5 variables x 4 faces per cell
@@ -1084,9 +1079,11 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         MHD_LAUNCH_CHECK();
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
-        k_mx_update<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
-                                       gyrate_close && s0 == 0 ? 1 : 0, st->src.ambi ? st->d32.p : nullptr,
-                                       st->src.chem && st->photo.n ? st->photo.p : nullptr, st->src.chem && st->vst.n ? st->vst.p : nullptr);
+        // the instance with the closing gyration fused carries its registers; the other stages use the lean one
+        auto upd = gyrate_close && s0 == 0 ? k_mx_update<true> : k_mx_update<false>;
+        upd<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
+                               gyrate_close && s0 == 0 ? 1 : 0, st->src.ambi ? st->d32.p : nullptr,
+                               st->src.chem && st->photo.n ? st->photo.p : nullptr, st->src.chem && st->vst.n ? st->vst.p : nullptr);
         MHD_LAUNCH_CHECK();
         P.end(KP_UPDATE, s);
         st->launches += 3;

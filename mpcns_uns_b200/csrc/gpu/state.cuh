@@ -25,7 +25,6 @@ struct MixedTables
     DBuf<float> fdx;            // per face: x_f - x_L (3), x_f - x_R (3): [6][nf]
     DBuf<char2> fslot;          // per face: its position in the c2f rows of L and R
     DBuf<float4> eth;           // per edge: unit tangent, length
-    DBuf<float4> ee1, ee2;      // per edge: orthonormal basis of the plane normal to the edge
     DBuf<float4> em;            // per e2f entry: in-face unit direction away from the edge, sigma = t.(m x n)
     DBuf<float> ew;             // per e2f entry: w_ef
     DBuf<float> vol_inv;        // per cell: 1 / V
