@@ -130,7 +130,8 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that one ncu capture measured
 # on the 6 x 32 x 32 x 48 x 6 shell of the same construction, with the entity count it scales with;
 # the bench line reports it scaled to its own workload (the traffic grows in proportion to that count).
-NCU_TRAFFIC = {("edge_emf", "mixed"): (513.56e6, "ne", 2082912), ("update", "mixed"): (680.87e6, "nc", 1769472)}
+NCU_TRAFFIC = {("edge_emf", "mixed"): (513.56e6, "ne", 2082912), ("update", "mixed"): (680.87e6, "nc", 1769472),
+               ("limited_gradients", "mixed"): (620.48e6, "nc", 1769472)}
 
 
 def ncu_traffic(kernel, precision, counts):

@@ -92,20 +92,24 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
         double psi = 1.0;
         if (p.limit)
         {
+            // min over the faces of (hi - w)/dl (dl > 0) and (lo - w)/dl (dl < 0): a correctly rounded
+            // quotient is monotone in dl, so the minimum is the quotient at the largest and at the most
+            // negative dl, bit for bit (min is exact and order-free); likewise for the relative limiter
+            double dpos = 0, dneg = 0;
             for (int32_t k = k0; k < k1; ++k)
             {
                 const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
                 const double dl = g0 * dx.x + g1 * dx.y + g2 * dx.z;
-                if (dl > 1e-300) psi = dmin(psi, (hi - wc) / dl);
-                else if (dl < -1e-300) psi = dmin(psi, (lo - wc) / dl);
+                if (dl > dpos) dpos = dl;
+                if (dl < dneg) dneg = dl;
             }
+            if (dpos > 1e-300) psi = dmin(psi, (hi - wc) / dpos);
+            if (dneg < -1e-300) psi = dmin(psi, (lo - wc) / dneg);
             if (p.rel_limit > 0 && (q == 0 || q == 4))
-                for (int32_t k = k0; k < k1; ++k)
-                {
-                    const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
-                    const double dl = fabs(g0 * dx.x + g1 * dx.y + g2 * dx.z);
-                    if (dl > 1e-300) psi = dmin(psi, p.rel_limit * wc / dl);
-                }
+            {
+                const double a = dmax(dpos, -dneg);
+                if (a > 1e-300) psi = dmin(psi, p.rel_limit * wc / a);
+            }
         }
         const double ps = dmax(0.0, dmin(1.0, psi));
         G(s, c, 3 * q) = ps * g0;
@@ -185,20 +189,23 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
         double psi = 1.0;
         if (p.limit)
         {
+            // two quotients instead of four: the minimum sits at the largest and the most negative dl
+            // (monotone correctly rounded quotients, exact min), bit for bit the reference's psi
+            double dpos = 0, dneg = 0;
 #pragma unroll
             for (int j = 0; j < 4; ++j)
             {
                 const double dl = g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2];
-                if (dl > 1e-300) psi = dmin(psi, (hi - wc[q]) / dl);
-                else if (dl < -1e-300) psi = dmin(psi, (lo - wc[q]) / dl);
+                if (dl > dpos) dpos = dl;
+                if (dl < dneg) dneg = dl;
             }
+            if (dpos > 1e-300) psi = dmin(psi, (hi - wc[q]) / dpos);
+            if (dneg < -1e-300) psi = dmin(psi, (lo - wc[q]) / dneg);
             if (p.rel_limit > 0 && (q == 0 || q == 4))
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                {
-                    const double dl = fabs(g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2]);
-                    if (dl > 1e-300) psi = dmin(psi, p.rel_limit * wc[q] / dl);
-                }
+            {
+                const double a = dmax(dpos, -dneg);
+                if (a > 1e-300) psi = dmin(psi, p.rel_limit * wc[q] / a);
+            }
         }
         const double ps = dmax(0.0, dmin(1.0, psi));
         G(s, c, 3 * q) = ps * g0;

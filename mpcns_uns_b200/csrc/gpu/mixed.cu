@@ -449,35 +449,40 @@ __device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int 
         float dl[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) dl[j] = g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2];
+        // Barth-Jespersen psi = min over the faces of (hi - w)/dl for dl > 0 and (lo - w)/dl for dl < 0: with
+        // hi - w >= 0 >= lo - w the minimum is taken at the largest and at the most negative dl, so two
+        // quotients per variable instead of four (likewise one for the relative limiter, at the largest |dl|)
+        float dpos = 0.f, dneg = 0.f;
+        int jpos = -1, jneg = -1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            if (dl[j] > dpos) { dpos = dl[j]; jpos = j; }
+            if (dl[j] < dneg) { dneg = dl[j]; jneg = j; }
+        }
         float psi = 1.f, bound = 0.f;
         int jb = -1;
         if (p.limit)
         {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
+            if (dpos > 1e-30f)
             {
-                if (dl[j] > 1e-30f)
-                {
-                    const float r = (hi - wc[q]) / dl[j];
-                    if (r < psi) { psi = r; jb = j; bound = hi; }
-                }
-                else if (dl[j] < -1e-30f)
-                {
-                    const float r = (lo - wc[q]) / dl[j];
-                    if (r < psi) { psi = r; jb = j; bound = lo; }
-                }
+                const float r = (hi - wc[q]) / dpos;
+                if (r < psi) { psi = r; jb = jpos; bound = hi; }
+            }
+            if (dneg < -1e-30f)
+            {
+                const float r = (lo - wc[q]) / dneg;
+                if (r < psi) { psi = r; jb = jneg; bound = lo; }
             }
             if (p.rel_limit > 0.f && (q == 0 || q == 4))
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
+            {
+                const float a = fmaxf(dpos, -dneg);
+                if (a > 1e-30f)
                 {
-                    const float a = fabsf(dl[j]);
-                    if (a > 1e-30f)
-                    {
-                        const float r = p.rel_limit * wc[q] / a;
-                        if (r < psi) { psi = r; jb = -1; }
-                    }
+                    const float r = p.rel_limit * wc[q] / a;
+                    if (r < psi) { psi = r; jb = -1; }
                 }
+            }
         }
         if (psi < 0.f) { psi = 0.f; jb = -1; }
         psi = fminf(1.f, psi);
