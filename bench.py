@@ -21,7 +21,7 @@ on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, c
 --gmres-max-it iterations: seconds per solve in FP64 and mixed precision, per-kernel GB/s, and the
 reference's own solve on a bounded sample beside it.
 
-The "ten_ion" object (with --ten-ion, or alone with --ten-ion-only): config 5, the ten-ion shell r in
+The "ten_ion" object (with --ten-ion, or alone with --ten-ion-only): the ten-ion shell r in
 [1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background field: mixed and FP64 steps and
 the mixed state's error after 50 steps.
 
@@ -42,6 +42,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -145,10 +146,10 @@ def ncu_traffic(kernel, precision, counts):
 class ClockSampler:
     def __init__(self, gpu_index):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = None
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.fh = open(self.path, "w")
+            fd, self.path = tempfile.mkstemp(prefix="mhd_clocks_", suffix=".csv")
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(gpu_index),
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -170,18 +171,20 @@ class ClockSampler:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as fh:
-            for line in fh:
-                f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    sm.append(float(f[1]))
-                    mx = float(f[2])
-                except ValueError:
-                    continue
-                for n, v in zip(names, f[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(n)
+            lines = fh.readlines()
+        os.unlink(self.path)
+        for line in lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
@@ -538,7 +541,7 @@ def main():
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--ten-ion", action="store_true", help="add the ten-ion shell (config 5; its 42.5M-cell mesh takes minutes to build)")
+    ap.add_argument("--ten-ion", action="store_true", help="add the ten-ion shell (its 42.5M-cell mesh takes minutes to build)")
     ap.add_argument("--ten-ion-only", action="store_true", help="run only the ten-ion section and print it as its own JSON line")
     ap.add_argument("--ten-ncube", type=int, default=96)
     ap.add_argument("--ten-nr", type=int, default=128)
