@@ -155,9 +155,18 @@ class ClockSampler:
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "50"], stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            if self.path:
+                self.fh.close()
+                os.unlink(self.path)
+            return
+        # nvidia-smi takes a fraction of a second to start; wait (at most 2 s) for its first sample
+        # so that the samples cover the steps that follow, not its start-up
+        t0 = time.time()
+        while time.time() - t0 < 2.0 and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
