@@ -76,17 +76,25 @@ def mesh_counts(h):
 def algorithmic_bytes(k, c, nsp, group, precision="fp64", sources=False):
     """Compulsory bytes of one launch of kernel class k: every array the pass needs, counted once
     (perfect reuse within the pass); values 8 bytes (FP64) or 4 (FP32 bulk of the mixed path; the
-    state U and the face fluxes Phi stay 8), indices 4, signs / flags 1.  With the two-ion sources,
-    `prepare` includes the cell-current pass and `update` reads the J x B inputs; `gyrate` reads and
-    rewrites both ions' state."""
+    state U and the face fluxes Phi stay 8), indices 4, signs / flags 1.  With the two-ion sources:
+    * FP64: `prepare` includes the cell-current pass and `update` reads the J x B inputs.
+    * Mixed: the face-candidate pass also writes the face terms of J (16 bytes per face), which the
+      update gathers with the total field.
+    * `gyrate` reads both ions' state and rewrites their momenta and energies, with the total field.
+      The opening half step also renews the primitives and u+ of the cells it turns.  FP64 has two
+      launches per step (opening, closing) and the figure is their mean.  Mixed has only the opening
+      launch, since the update applies the closing half step."""
     base = _algorithmic_bytes(k, c, nsp, group, precision)
     if not sources:
         return base
     nc, nf = c["nc"], c["nf"]
+    gyr = 80 * nc + 64 * nc + nc        # U of both ions in, momenta and energies out, material
     if precision == "mixed":
-        extra = {"prepare": 52 * nc + 24 * nf, "update": 64 * nc, "gyrate": 144 * nc + 16 * nc + nc}
+        extra = {"face_candidate": 16 * nf, "update": 64 * nc,
+                 "gyrate": gyr + 16 * nc + 20 * nsp * nc + 16 * nc}
     else:
-        extra = {"prepare": 64 * nc + c["c2f"] * 5 + 36 * nf, "update": (2 + 3 + 3) * 8 * nc, "gyrate": 144 * nc + 24 * nc + nc}
+        extra = {"prepare": 64 * nc + c["c2f"] * 5 + 36 * nf, "update": (2 + 3 + 3) * 8 * nc,
+                 "gyrate": gyr + 24 * nc + (40 * nsp * nc + 24 * nc) / 2}
     return base + extra.get(k, 0.0)
 
 
