@@ -741,7 +741,7 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
 // so no per-face state is kept between two passes.  The basis (e1, e2) of the plane normal to the edge
 // is rebuilt from the unit tangent as the tables build it (the result does not depend on the choice of
 // orthonormal basis).
-__global__ void __launch_bounds__(128) k_mx_edge(MV m, const float4 *__restrict__ Ef, const float4 *__restrict__ up,
+__global__ void __launch_bounds__(128, 8) k_mx_edge(MV m, const float4 *__restrict__ Ef, const float4 *__restrict__ up,
                                                     const double *__restrict__ phi, float cuct, float3 E_inf, float *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
@@ -777,10 +777,14 @@ __global__ void __launch_bounds__(128) k_mx_edge(MV m, const float4 *__restrict_
             e1 = n1 > 0.f ? make_float3(e1.x / n1, e1.y / n1, e1.z / n1) : make_float3(0.f, 0.f, 0.f);
             const float3 e2 = fcross(th, e1);
             float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f, S0 = 0.f, S1 = 0.f, S2 = 0.f;
+            // the next face's index is loaded one iteration ahead, so that the gathers of a face wait
+            // on one load instead of two
+            int32_t f_next = m.e2f_idx[f0];
 #pragma unroll 1
             for (int i = 0; i < nfe; ++i)
             {
-                const int32_t f = m.e2f_idx[f0 + i];
+                const int32_t f = f_next;
+                if (i + 1 < nfe) f_next = m.e2f_idx[f0 + i + 1];
                 const float4 mi4 = m.em[f0 + i];
                 const float3 mi = f3(mi4);
                 const float4 nf4 = m.fn[f];
