@@ -221,23 +221,44 @@ def make_workload(args):
 
 
 def cpu_sample(args):
-    """Bounded sample of the same workload for the CPU reference: the same shell construction at
-    6 x 16 x 16 x 24 (221,184 cells), two ions."""
-    from mpcns_uns_b200 import workloads
+    """Bounded sample of the same workload for the CPU baseline of this arm: the same shell construction at
+    6 x 16 x 16 x 24 (221,184 cells), two ions, built by the reference's own code (reference_workload)."""
     if args.config == "box":
-        return workloads.box(12)
-    return workloads.shell(16, 24, r_in=1.0, r_out=6.0, sources=not args.no_sources)
+        return reference_workload("box", 12, 0, args)
+    return reference_workload("shell", 16, 24, args)
+
+
+def reference_workload(config, ncube, nr, args):
+    """The benchmark's workload built by the reference's own code, with no library of this repository loaded:
+    the cubed-sphere shell of uns::make_cubed_sphere_shell cut into tetrahedra and numbered by the reference's
+    ComplexBuilder (oracle/_ref: ref_mesh_shell_tets), its uns::compute_geometry and BoundaryInfo::build, and
+    the seeded state of workloads.shell_state (numpy) on that mesh.  Entity for entity and bit for bit the
+    mesh, metric and state of workloads.shell (same uns::topology_hash; tests/test_oracle.py checks it).
+    The box (--config box) has no reference generator with the workload's node jitter, so its sample is the
+    reference's unjittered box."""
+    from oracle import ref
+    from mpcns_uns_b200 import workloads
+    if config == "box":
+        r = ref.RefMesh.box(ncube, ncube, ncube).boundary("outflow", {}, (1.0, 0.0, 0.0))
+        rng = np.random.default_rng(1)
+        nc = r.n_cells
+        W = np.zeros((nc, 5))
+        W[:, 0], W[:, 1], W[:, 4] = 1.0 + 0.01 * rng.uniform(-1, 1, nc), 1.0, 0.1
+        return workloads.Workload(name=f"refbox{ncube}^3", mesh=r, n_species=1, gamma=workloads.GAMMA,
+                                  U=[workloads.to_cons(W, workloads.GAMMA).ravel()], Phi=np.zeros(r.n_faces),
+                                  PhiAdd=np.zeros(r.n_faces), fs=[(1.0, 1.0, 0.0, 0.0, 0.1)], mass=[1.0], u_inf=(1.0, 0.0, 0.0),
+                                  B_imf=(0.0, 0.0, 0.0))
+    stretch = workloads.shell_stretch(ncube, nr, 1.0, 6.0)
+    r = ref.RefMesh.shell_tets(ncube, nr, 1.0, 6.0, stretch)
+    r.boundary("outflow", {"inner": "wall", "outer": "farfield"}, (-8.0, 0.0, 0.0))
+    return workloads.shell_state(r, f"shell6x{ncube}x{ncube}x{nr}x6", 1.0, stretch, sources=not args.no_sources)
 
 
 def time_reference(wl, steps, warmup):
-    """The reference's own hot-path step (oracle/_ref, np = 1, one core) on workload wl."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    """The reference's own hot-path step (oracle/_ref, np = 1, one core) on workload wl, whose mesh is a
+    reference mesh (oracle.ref.RefMesh): seconds per step, median of `steps` after `warmup`."""
     from oracle import ref
-    from helpers import BOX_TAGS, SHELL_TAGS, ref_twin
-    from mpcns_uns_b200 import gpu as _g
-    tags = SHELL_TAGS if wl.name.startswith("shell") else BOX_TAGS
-    bc = ("outflow", {"inner": "wall", "outer": "farfield"}, wl.u_inf) if tags is SHELL_TAGS else ("outflow", {}, wl.u_inf)
-    r = ref_twin(wl.mesh, tags).boundary(*bc)
+    r = wl.mesh
     p = ref.StepParams()
     p.n_species, p.second_order = wl.n_species, 1
     p.gamma, p.rho_floor, p.p_floor, p.cuct, p.M_ref, p.ne_floor, p.rel_limit = wl.gamma, 1e-10, 1e-12, 0.5, 1.0, 0.01, 0.0
@@ -259,10 +280,11 @@ def time_reference(wl, steps, warmup):
         if wl.n_species == 2:
             dt = r.local_time_step(wl.gamma, 0.4, 1.0, 1e-2, W[0], W[1], Btot)
         else:
-            dt = dt or 0.2 * float(np.min(np.asarray(wl.mesh["edge_len"])))
+            dt = dt or 0.2 * float(np.min(np.asarray(r["edge_len"])))
         r.rk2_step(p, U, Phi, wl.PhiAdd, Badd, dt)
         if k >= warmup:
             times.append(time.perf_counter() - t0)
+        log(f"[bench] reference step {k + 1}/{warmup + steps}: {time.perf_counter() - t0:.2f} s")
     per_step = float(np.median(times))
     return wl.mesh.n_cells * wl.n_species * 2 / per_step, per_step
 
@@ -528,6 +550,45 @@ def gmres_cpu_baseline(max_it=60):
             "edges": case.mesh.n_edges}
 
 
+def _r(x, d=4):
+    """x rounded to d significant digits (None stays None)."""
+    if x is None:
+        return None
+    return float(f"{x:.{d}g}")
+
+
+def summary(out):
+    """The figures of the line in a compact object printed last, so that they survive a cut of the output
+    to its last 1500 characters: the mixed and FP64 steps, the mixed state's error after the accuracy run,
+    div B, the GMRES solves, the adjoint's cost and checks, and the ten-ion steps when run."""
+    sm = {"mixed_ms": _r(out["ms_per_step"]), "fp64_ms": _r(out["fp64"]["ms_per_step"]),
+          "speedup_mixed": _r(out["fp64"]["speedup_mixed"]), "e2e": _r(out["e2e"]["value"]),
+          "roofline_frac": _r(out["roofline"]["frac"], 3), "roofline_kernel": out["roofline"]["kernel"],
+          "clocks_mhz": [(c or {}).get("sm_mhz") for c in (out["clocks"], out["fp64"].get("clocks"))]}
+    a = out.get("accuracy_mixed_vs_fp64")
+    if a:
+        sm["acc"] = {"steps": a["steps"], "U": _r(a["U_all_rel_l2"], 3),
+                     "U_sp": [_r(a[k], 3) for k in sorted(a) if k.startswith("U") and k.endswith("_rel_l2") and k[1].isdigit()],
+                     "U_sp_fp64_pert": [_r(a[k], 3) for k in sorted(a) if k.endswith("_perturbed_1e-7")],
+                     "Phi": _r(a["Phi_rel_l2"], 3), "divB": [_r(a["div_b_max_rel_mixed"], 3), _r(a["div_b_max_rel_fp64"], 3)]}
+    g = out.get("gmres")
+    if g:
+        sm["gmres"] = {p: [_r(g[p]["s_per_solve"]), g[p]["iterations"], _r(g[p]["rel_res"], 3)] for p in ("fp64", "mixed")}
+        sm["gmres"]["speedup_mixed"] = _r(g["speedup_mixed"])
+        sm["gmres"]["cols"] = "s_per_solve, iterations, rel_res"
+    d = out.get("adjoint")
+    if d:
+        fd = d["fd"]
+        sm["adjoint"] = {"fwd_s": _r(d["forward_s"]), "fwd_bwd_over_fwd": _r(d["forward_plus_backward_over_forward"]),
+                         "dot": _r(d["dot_test_rel_err_max"], 2),
+                         "fd": {k: [_r(v.get("max_rel_err"), 2), _r(v.get("median_rel_err"), 2)] for k, v in fd.items()}}
+    t = out.get("ten_ion")
+    if t:
+        sm["ten_ion"] = {"mixed_ms": _r(t["mixed"]["ms_per_step"]), "fp64_ms": _r(t["fp64"]["ms_per_step"]),
+                         "U": _r((t.get("accuracy_mixed_vs_fp64") or {}).get("U_all_rel_l2"), 3)}
+    return sm
+
+
 def max_over_ranks(ms, dist, device):
     """The slowest rank's device time: every rank's K steps count once, the job ends with the last."""
     if dist is None:
@@ -549,6 +610,7 @@ def main():
     ap.add_argument("--ncube", type=int, default=0)
     ap.add_argument("--nr", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-max-steps", type=int, default=3, help="cap of the reference arm's timed steps")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--accuracy-steps", type=int, default=100)
     ap.add_argument("--no-gmres", action="store_true")
@@ -579,21 +641,35 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        wl = cpu_sample(args)
         from oracle import ref
         if not ref.available():
             print(json.dumps({"impl": "reference", "unavailable": "reference checker oracle/_ref not built"}))
             return
-        steps = max(1, min(args.steps, 5))
+        # the same workload as this arm's own: the full configuration, built by the reference's code
+        t0 = time.time()
+        if args.config == "box":
+            wl = reference_workload("box", args.ncube or 16, 0, args)
+        else:
+            wl = reference_workload("shell", args.ncube or 64, args.nr or 96, args)
+        setup_s = time.time() - t0
+        log(f"[bench] reference workload {wl.name}: {wl.mesh.n_cells} cells (setup {setup_s:.1f}s)")
+        # one core takes about half a minute per step of the 14.2M-cell shell: the step count is capped
+        steps = max(1, min(args.steps, args.ref_max_steps))
         warm = 1 if args.warmup > 0 else 0
         v, per = time_reference(wl, steps, warm)
-        cfgd = {"workload": wl.name + " (bounded sample of the 6x64x64x96x6 shell)", "n_species": wl.n_species,
-                "cells": wl.mesh.n_cells, "l2": "inputs > L2"}
+        cfgd = {"workload": wl.name, "n_species": wl.n_species, "cells": wl.mesh.n_cells, "faces": wl.mesh.n_faces,
+                "edges": wl.mesh.n_edges, "topology_hash": wl.mesh.topology_hash(), "l2": "inputs > L2",
+                "sources": "J x B force + Strang-split exact gyration" if wl.lorentz else "none",
+                "mesh": "uns::make_cubed_sphere_shell cut into 6 tetrahedra per hexahedron, numbered by the reference's "
+                        "ComplexBuilder (no library of this repository loaded)",
+                "steps_cap": f"min(--steps, {args.ref_max_steps}) timed steps after min(--warmup, 1) warm-up",
+                "setup_s": setup_s}
         print(json.dumps({"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
                           "steps": steps, "warmup": warm, "ms_per_step": per * 1e3, "higher_is_better": True,
                           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfgd,
                           "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "reference",
-                                           "sample": f"{wl.name}, {steps} steps, np=1"},
+                                           "sample": f"the full {wl.name} workload, {steps} steps after {warm} warm-up, np=1 "
+                                                     "(the reference has no threads; no MPI on this host)"},
                           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
@@ -663,7 +739,9 @@ def main():
                     bytes_launch=bl, achieved=bl / (k_ms / k_n / 1e3) / 1e9, kernels=breakdown)
 
     st64 = new_state("fp64")
+    sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     r64 = timed(st64, "fp64")
+    clocks64 = sampler.stop() if sampler else None
     st32 = new_state("mixed")
     sampler = ClockSampler(torch.cuda.current_device()) if rank == 0 else None
     rmx = timed(st32, "mixed")
@@ -772,6 +850,7 @@ def main():
                "warmup": args.warmup, "ms_per_step": rmx["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32/f64 mixed", "data": "synthetic",
                "config": {"workload": wl.name, "cells": h.n_cells, "faces": h.n_faces, "edges": h.n_edges,
+                          "topology_hash": h.topology_hash(),
                           "n_species": wl.n_species, "global_cells": h.n_cells * world,
                           "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                           "dt": "CFL 0.4 on device", "l2": "inputs > L2 (no flush needed)",
@@ -784,11 +863,12 @@ def main():
                             "algorithmic_bytes_per_launch": rmx["bytes_launch"]},
                "kernels": rmx["kernels"],
                "fp64": {"value": r64["value"], "ms_per_step": r64["ms"] / args.steps, "speedup_mixed": rmx["value"] / r64["value"],
-                        "precision": "fp64 reference-exact", "kernels": r64["kernels"],
+                        "precision": "fp64 reference-exact", "kernels": r64["kernels"], "clocks": clocks64,
                         "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
                "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
                "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "adjoint": adj, "ten_ion": ten}
+        out["summary"] = summary(out)
         print(json.dumps(out))
     if dist:
         dist.barrier()

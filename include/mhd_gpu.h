@@ -144,23 +144,34 @@ int mhd_gpu_faraday(MhdMesh *mesh, const double *E, double *B, double dt);
 int mhd_gpu_faraday_edge_dt(MhdMesh *mesh, const double *E, const double *dt_edge, double *B);
 
 /* mhd::div_b (Common/diagnostics/DivB.h:15, .cpp:8-24) over the owned cells, FP64.
- * host_out[0] = max |d2 B|, host_out[1] = max relative, host_out[2] = id of the worst cell. */
+ * host_out[0] = max |d2 B|, host_out[1] = max relative, host_out[2] = the handle's local index of the
+ * worst cell (-1 if d2 B vanishes everywhere).  The reference reports the cell's global id
+ * (cx.ent[3].gid[c], DivB.cpp:20); a caller with a per-rank mesh maps the index through its gid table
+ * (on one rank built by ComplexBuilder, gid[c] = c).  The call synchronises the handle's stream. */
 int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *host_out);
 
-/* The div B diagnostic of mhd_gpu_div_b for callers that cannot allocate device memory: code
- * running inside a CUDA stream capture, under an external memory budget or pool that forbids
- * cudaMalloc, or in a host that must not grow its footprint after start-up.  This entry point
- * has no counterpart in the reference.  It calls no cudaMalloc / cudaFree and no allocating
- * library routine: its block partials and result live in one static device array of
- * MHD_NOALLOC_DIVB_MAX_BLOCKS partials (1.5 MiB), which every GPU that loads this library holds
- * until the process exits.  One block reduces 1024 cells, so a mesh may have at most
- * MHD_NOALLOC_DIVB_MAX_BLOCKS * 1024 owned cells; larger meshes are rejected with MHD_EINVAL.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current; make that first call before any stream capture.  Every call overwrites
- * the partials it reads, so nothing has to start at zero; calls that overlap on the GPU (other
- * streams, other threads) share the array and race.  Results equal mhd_gpu_div_b's. */
+/* The div B diagnostic of mhd_gpu_div_b for callers that must not allocate device memory once
+ * they run: a host application that hands all GPU memory to its own pool or arena at start-up (a
+ * cudaMalloc behind its back would fail or break its accounting), or a process under a fixed memory
+ * budget whose footprint must not grow after set-up.  This entry point has no counterpart in the
+ * reference.  It calls no cudaMalloc / cudaFree and no allocating library routine: its block
+ * partials and result live in one static device array of MHD_NOALLOC_DIVB_MAX_BLOCKS partials
+ * (1.5 MiB), which every GPU that loads this library holds until the process exits.  One block
+ * reduces 1024 cells, so a mesh may have at most MHD_NOALLOC_DIVB_MAX_BLOCKS * 1024 = 67,108,864
+ * owned cells; larger meshes are rejected with MHD_EINVAL (mhd_gpu_div_b_noalloc_blocks gives the
+ * block count of a mesh size, or that error, without touching the GPU).  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that device current; make that
+ * first call before any stream capture starts on the device.  Like
+ * mhd_gpu_div_b it copies the three results to host_out and synchronises the handle's stream before
+ * returning.  Every call overwrites the partials it reads, so nothing has to start at zero; calls
+ * that overlap on the GPU (other streams, other threads) share the array and race.  Results equal
+ * mhd_gpu_div_b's. */
 #define MHD_NOALLOC_DIVB_MAX_BLOCKS 65536
 int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, double *host_out);
+int mhd_gpu_div_b_noalloc_blocks(int64_t n_owned_cells, int64_t *blocks);
+/* Number of cudaMalloc and cudaFree calls this library has made since it was loaded (every device
+ * buffer of every handle); no GPU work. */
+int mhd_gpu_alloc_calls(int64_t *out);
 
 /* mhd::cell_current (Common/induction/Current.cpp:9-31): B 3 per cell -> J 3 per cell. */
 int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -53,6 +54,10 @@ template <class F> int guarded(F &&f)
 }
 
 // ---------------------------------------------------------------- device buffers
+// Every device allocation of the library goes through DBuf; this counts its cudaMalloc and cudaFree
+// calls since the library was loaded (mhd_gpu_alloc_calls).
+inline std::atomic<int64_t> g_alloc_calls{0};
+
 template <class T> struct DBuf
 {
     T *p = nullptr;
@@ -63,7 +68,11 @@ template <class T> struct DBuf
     ~DBuf() { release(); }
     void release()
     {
-        if (p) cudaFree(p);
+        if (p)
+        {
+            cudaFree(p);
+            g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+        }
         p = nullptr;
         n = 0;
     }
@@ -71,7 +80,11 @@ template <class T> struct DBuf
     {
         if (count == n && p) return;
         release();
-        if (count) MHD_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        if (count)
+        {
+            g_alloc_calls.fetch_add(1, std::memory_order_relaxed);
+            MHD_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        }
         n = count;
     }
     void upload(const T *h, size_t count)

@@ -475,6 +475,28 @@ int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *h
     });
 }
 
+int mhd_gpu_div_b_noalloc_blocks(int64_t n_owned_cells, int64_t *blocks)
+{
+    return guarded([&] {
+        MHD_REQUIRE(blocks && n_owned_cells >= 0, "bad argument");
+        const int64_t nb = (n_owned_cells + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock;
+        MHD_REQUIRE(nb <= MHD_NOALLOC_DIVB_MAX_BLOCKS,
+                    "div_b_noalloc: the static scratch holds " + std::to_string(MHD_NOALLOC_DIVB_MAX_BLOCKS) +
+                        " block partials, i.e. at most " +
+                        std::to_string(static_cast<int64_t>(MHD_NOALLOC_DIVB_MAX_BLOCKS) * kNoAllocCellsPerBlock) +
+                        " owned cells; this mesh has " + std::to_string(n_owned_cells));
+        *blocks = nb;
+    });
+}
+
+int mhd_gpu_alloc_calls(int64_t *out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(out, "bad argument");
+        *out = g_alloc_calls.load(std::memory_order_relaxed);
+    });
+}
+
 int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, double *host_out)
 {
     return guarded([&] {
@@ -486,12 +508,9 @@ int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, d
             host_out[2] = -1.0;
             return;
         }
-        const int64_t nb = (static_cast<int64_t>(m.no_cells) + kNoAllocCellsPerBlock - 1) / kNoAllocCellsPerBlock;
-        MHD_REQUIRE(nb <= MHD_NOALLOC_DIVB_MAX_BLOCKS,
-                    "div_b_noalloc: the static scratch holds " + std::to_string(MHD_NOALLOC_DIVB_MAX_BLOCKS) +
-                        " block partials, i.e. at most " +
-                        std::to_string(static_cast<int64_t>(MHD_NOALLOC_DIVB_MAX_BLOCKS) * kNoAllocCellsPerBlock) +
-                        " owned cells; this mesh has " + std::to_string(m.no_cells));
+        int64_t nb = 0;
+        const int rc = mhd_gpu_div_b_noalloc_blocks(m.no_cells, &nb);
+        if (rc != MHD_OK) throw ApiError(rc, mhd_gpu_last_error());
         double *scratch = noalloc_scratch();
         DivPart *part = reinterpret_cast<DivPart *>(scratch);
         double *res = scratch + 3 * MHD_NOALLOC_DIVB_MAX_BLOCKS;

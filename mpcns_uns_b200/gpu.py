@@ -340,14 +340,21 @@ class DeviceMesh:
         self._leave()
         return B
 
-    def div_b(self, B, extra=None):
-        """mhd::div_b (Common/diagnostics/DivB.cpp:8-24) -> dict(max_abs, max_rel, worst_cell_gid)."""
+    def div_b(self, B, extra=None, gid=None):
+        """mhd::div_b (Common/diagnostics/DivB.cpp:8-24) -> dict(max_abs, max_rel, worst_cell, worst_cell_gid).
+
+        worst_cell is the handle's local index of the worst owned cell (-1: none).  The reference
+        reports its global id cx.ent[3].gid[c] (DivB.cpp:20): worst_cell_gid = gid[worst_cell] with the
+        caller's gid table, or the local index when gid is None (one rank built by ComplexBuilder,
+        whose gid is the identity)."""
         B = dev(B)
         ex = None if extra is None else dev(extra)
         out = np.zeros(3)
         self._enter()
         check(lib().mhd_gpu_div_b(self._h, ptr(B), ptr(ex), out.ctypes.data_as(vp)))
-        return dict(max_abs=float(out[0]), max_rel=float(out[1]), worst_cell_gid=int(out[2]))
+        c = int(out[2])
+        g = c if (gid is None or c < 0) else int(np.asarray(gid)[c])
+        return dict(max_abs=float(out[0]), max_rel=float(out[1]), worst_cell=c, worst_cell_gid=g)
 
     def add_sources(self, params, species, WH, WNa, B, J, dt, rhs, dpe=None, photo=None, vst=None):
         """mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63); returns rhs + source."""

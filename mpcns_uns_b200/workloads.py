@@ -113,11 +113,11 @@ def box(n=16, seed=0, jitter=0.15, tets=True):
 
 def background(mesh: HostMesh, B_imf, dipole_m, dipole_c, soft=1e-3):
     """Static background flux of mercury::set_background (MercuryUns/initial/Initial.cpp:66-84)."""
-    PhiAdd = np.asarray(mesh["face_area"]) @ np.asarray(B_imf, np.float64)
-    r = np.asarray(mesh["edge_mid"]) - np.asarray(dipole_c, np.float64)
+    PhiAdd = np.asarray(mesh["face_area"]).reshape(-1, 3) @ np.asarray(B_imf, np.float64)
+    r = np.asarray(mesh["edge_mid"]).reshape(-1, 3) - np.asarray(dipole_c, np.float64)
     d2 = (r * r).sum(1) + soft * soft
     a = np.cross(np.asarray(dipole_m, np.float64), r) / (d2 * np.sqrt(d2))[:, None]
-    A = (a * np.asarray(mesh["edge_vec"])).sum(1)
+    A = (a * np.asarray(mesh["edge_vec"]).reshape(-1, 3)).sum(1)
     return PhiAdd + d1(mesh, A)
 
 
@@ -134,17 +134,27 @@ def geometric_stretch(nr, r_in, r_out, first):
     return 0.5 * (lo + hi)
 
 
+def shell_stretch(ncube, nr, r_in=1.0, r_out=6.0):
+    """Radial stretch of the shell workloads: the first layer as thick as the angular spacing at r_in."""
+    return geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
+
+
 def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False,
           device_geometry=False):
     """device_geometry: compute the metric on the GPU (bit-identical, faster for large shells)."""
     if stretch is None:
-        # first layer as thick as the angular spacing at r_in
-        stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
+        stretch = shell_stretch(ncube, nr, r_in, r_out)
     m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry(device=device_geometry)
     m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
+    return shell_state(m, f"shell6x{ncube}x{ncube}x{nr}x6", r_in, stretch, seed, n_species, masses, u_inf, sources)
+
+
+def shell_state(m, name, r_in=1.0, stretch=1.0, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False):
+    """The shell workload's seeded state on a built shell mesh `m` (any object with n_cells, n_faces and the
+    reference's named arrays: cell_center, face_area, edge_mid, edge_vec, f2e_*), numpy only."""
     rng = np.random.default_rng(seed)
     nc = m.n_cells
-    r = np.linalg.norm(np.asarray(m["cell_center"]), axis=1)
+    r = np.linalg.norm(np.asarray(m["cell_center"]).reshape(-1, 3), axis=1)
     masses = masses or ([1.0, 23.0] if n_species == 2 else [1.0] * n_species)
     U, fs = [], []
     for s in range(n_species):
@@ -163,7 +173,7 @@ def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, mas
     B_imf = (0.0, 0.0, -0.5)
     PhiAdd = background(m, B_imf, (0.0, 0.0, 1.0), (0.0, 0.0, 0.2))
     two = n_species == 2
-    return Workload(name=f"shell6x{ncube}x{ncube}x{nr}x6", mesh=m, n_species=n_species, gamma=GAMMA, U=U,
+    return Workload(name=name, mesh=m, n_species=n_species, gamma=GAMMA, U=U,
                     Phi=np.zeros(m.n_faces), PhiAdd=PhiAdd, fs=fs, mass=masses, u_inf=tuple(u_inf), B_imf=B_imf,
                     cfl=0.4, steps=100, extra=dict(stretch=stretch), lorentz=two and sources,
                     induce_coeff=1.0 if two and sources else 0.0)

@@ -49,6 +49,7 @@ def lib():
             ("ref_mesh_from_cells", [i32, vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, i32, vp], vp),
             ("ref_mesh_box", [i32, i32, i32, vp, vp], vp),
             ("ref_mesh_shell", [i32, i32, i32, dbl, dbl, dbl], vp),
+            ("ref_mesh_shell_tets", [i32, i32, i32, dbl, dbl, dbl], vp),
             ("ref_mesh_hanging_box", [i32, i32, i32, vp, vp, i32], vp),
             ("ref_mesh_free", [vp], None),
             ("ref_mesh_counts", [vp, vp], None),
@@ -148,6 +149,13 @@ class RefMesh:
     @classmethod
     def shell(cls, ncube, nr, r_in=1.0, r_out=10.0, r_stretch=1.0, n_solid=0):
         return cls(lib().ref_mesh_shell(ncube, nr, n_solid, r_in, r_out, r_stretch))
+
+    @classmethod
+    def shell_tets(cls, ncube, nr, r_in=1.0, r_out=10.0, r_stretch=1.0, n_solid=0):
+        """The reference's cubed-sphere shell with every hexahedron cut into 6 tetrahedra, built by the
+        reference's ComplexBuilder alone (ref_mesh_shell_tets): the benchmark's shell without this
+        library's mesh services."""
+        return cls(lib().ref_mesh_shell_tets(ncube, nr, n_solid, r_in, r_out, r_stretch))
 
     @classmethod
     def hanging_box(cls, nx=5, ny=4, nz=4, hi=(5, 4, 4), sphere=(2.2, 1.8, 2.1, 1.3), level=2):

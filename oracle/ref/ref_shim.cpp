@@ -170,6 +170,76 @@ void *ref_mesh_shell(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, do
     return out;
 }
 
+// The cubed-sphere shell of uns::make_cubed_sphere_shell (src/uns/generate/CubedSphereMesh.cpp:12-83) with
+// every hexahedron cut into 6 tetrahedra, built by the reference's ComplexBuilder (add_cell, tag_face,
+// finish: src/uns/complex/ComplexBuilder.cpp:45-134).  The reference generates hexahedra only; the split
+// is the one of the benchmark workloads: the Kuhn paths 0 -> a -> a|b -> 7 of the hexahedron's local
+// corner bits (corner i at (i&1, (i>>1)&1, (i>>2)&1)), one tetrahedron per order of the three axis bits,
+// each given its four outward loops; a tagged quad becomes the two triangles on either side of the
+// diagonal joining its lowest and highest local corners.  Cells, faces and edges come out in the
+// creation order of the split hexahedra, so this mesh is the benchmark's shell, entity for entity.
+void *ref_mesh_shell_tets(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch)
+{
+    RefMesh *out = nullptr;
+    guarded([&] {
+        CubedSphereSpec s;
+        s.ncube = ncube; s.nr = nr; s.n_solid = n_solid; s.r_in = r_in; s.r_out = r_out; s.r_stretch = r_stretch;
+        HexMesh h = make_cubed_sphere_shell(s);
+        ComplexBuilder b(static_cast<Id>(h.x.size()));
+        static const int P[6][3] = {{1, 2, 4}, {1, 4, 2}, {2, 1, 4}, {2, 4, 1}, {4, 1, 2}, {4, 2, 1}};
+        static const int PAR[6] = {+1, -1, -1, +1, +1, -1};
+        static const int L[6][4] = {{0, 4, 6, 2}, {1, 3, 7, 5}, {0, 1, 5, 4}, {2, 6, 7, 3}, {0, 2, 3, 1}, {4, 5, 7, 6}};
+        std::vector<std::vector<Id>> loops(4, std::vector<Id>(3));
+        for (size_t c = 0; c < h.hex.size(); ++c)
+        {
+            const auto &v = h.hex[c];
+            for (int t = 0; t < 6; ++t)
+            {
+                Id p[4] = {v[0], v[P[t][0]], v[P[t][0] | P[t][1]], v[7]};
+                if (PAR[t] < 0) std::swap(p[1], p[2]);
+                loops[0] = {p[0], p[2], p[1]};
+                loops[1] = {p[0], p[1], p[3]};
+                loops[2] = {p[1], p[2], p[3]};
+                loops[3] = {p[0], p[3], p[2]};
+                b.add_cell(loops, h.material.empty() ? kFluid : h.material[c]);
+            }
+        }
+        // tagged quads: find each one's hexahedron face to know its local corners
+        std::map<std::array<Id, 4>, int> tag_of;
+        for (const auto &t : h.tagged)
+        {
+            std::array<Id, 4> k = t.nodes;
+            std::sort(k.begin(), k.end());
+            tag_of[k] = t.tag;
+        }
+        for (size_t c = 0; c < h.hex.size() && !tag_of.empty(); ++c)
+        {
+            const auto &v = h.hex[c];
+            for (int f = 0; f < 6; ++f)
+            {
+                std::array<Id, 4> k = {v[L[f][0]], v[L[f][1]], v[L[f][2]], v[L[f][3]]};
+                std::sort(k.begin(), k.end());
+                auto it = tag_of.find(k);
+                if (it == tag_of.end()) continue;
+                int lo = 7, hi = 0;
+                for (int q = 0; q < 4; ++q) { lo &= L[f][q]; hi |= L[f][q]; }
+                for (int q = 0; q < 4; ++q)
+                {
+                    const int lq = L[f][q];
+                    if (lq == lo || lq == hi) continue;
+                    b.tag_face({v[lo], v[lq], v[hi]}, it->second);
+                }
+            }
+        }
+        Mesh m;
+        m.cx = b.finish();
+        m.x = h.x;
+        m.tag_names = h.tag_names;
+        out = wrap(std::move(m));
+    });
+    return out;
+}
+
 // Hanging-node polyhedra: a box refined inside a sphere, as in tests/test_ideal_emf.cpp:357-364
 // (uns::build_refined_mesh, src/uns/refine/RefineMesh.cpp).
 void *ref_mesh_hanging_box(int32_t nx, int32_t ny, int32_t nz, const double *hi, const double *sphere, int32_t level)

@@ -286,3 +286,34 @@ def test_gyrate(meshes):
     gH, gN = d.gyrate(p, B, 0.07, UH, UN)
     assert rel_err(_np(gH), UHr) < TOL and rel_err(_np(gN), UNr) < TOL
     assert rel_err(UHr, UH) > 1e-6          # the rotation did something
+
+
+def _face_keys(m):
+    """Sorted node triple/quad of every face, as a tuple per face."""
+    e2n = np.asarray(m["e2n_idx"]).reshape(-1, 2)
+    fp, fi = np.asarray(m["f2e_ptr"]), np.asarray(m["f2e_idx"])
+    return [tuple(sorted(set(e2n[fi[fp[f]:fp[f + 1]]].ravel().tolist()))) for f in range(m.n_faces)]
+
+
+def test_div_b_worst_cell_after_renumbering():
+    """On a renumbered mesh the device reports its local index of the worst cell; mapped through the
+    caller's gid table (new cell i = old cell order[i]) it is the cell the reference names on the mesh
+    in its original numbering (DivB.cpp:20 returns cx.ent[3].gid[c])."""
+    from mpcns_uns_b200.gpu import DeviceMesh
+    h0 = HostMesh.box(6, 5, 4, tets=True, jitter=0.1, seed=5)
+    order = np.random.default_rng(8).permutation(h0.n_cells).astype(np.int32)
+    h0.compute_geometry().boundary("outflow")
+    hr = h0.reordered(order).compute_geometry().boundary("outflow")
+    r0 = ref_twin(h0, BOX_TAGS).boundary("outflow", {}, (1.0, 0.0, 0.0))
+    where = {k: f for f, k in enumerate(_face_keys(h0))}
+    fmap = np.array([where[k] for k in _face_keys(hr)])
+    rng = np.random.default_rng(9)
+    B0 = rng.uniform(-1, 1, h0.n_faces)
+    dr = DeviceMesh(hr)
+    for ex in (None, rng.uniform(-1, 1, h0.n_faces)):
+        rr = r0.div_b(B0, ex)
+        g = dr.div_b(B0[fmap], None if ex is None else ex[fmap], gid=order)
+        assert abs(g["max_abs"] - rr["max_abs"]) <= TOL * rr["max_abs"]
+        assert abs(g["max_rel"] - rr["max_rel"]) <= TOL * rr["max_rel"]
+        assert g["worst_cell_gid"] == rr["worst_cell_gid"] and order[g["worst_cell"]] == rr["worst_cell_gid"]
+        assert g["worst_cell"] != rr["worst_cell_gid"] or order[g["worst_cell"]] == g["worst_cell"]

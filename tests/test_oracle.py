@@ -284,3 +284,23 @@ def test_ambipolar_and_chemistry():
     o.rk2_step(wl, Ub, Pb, Badd, dt, lorentz=True, induce_coeff=0.7, inver_MA2=0.8, extra=extra)
     assert np.abs(Ua[1] - Ub[1]).max() > 0 and np.abs(Pa - Pb).max() > 0
     del keep_r, keep_o
+
+
+@pytest.mark.parametrize("ncube,nr,n_solid", [(8, 6, 0), (5, 4, 1)])
+def test_reference_built_shell_is_the_workload_shell(ncube, nr, n_solid):
+    """The bench's reference arm builds its shell with the reference's code alone (make_cubed_sphere_shell,
+    the tetrahedral split through ComplexBuilder, compute_geometry, BoundaryInfo::build) and its state with
+    workloads.shell_state: the same complex (topology hash), metric, boundary classification and state as the
+    workload of this library's own generator, bit for bit."""
+    from mpcns_uns_b200 import workloads
+    st = workloads.shell_stretch(ncube, nr)
+    h = HostMesh.shell(ncube, nr, 1.0, 6.0, st, n_solid=n_solid, tets=True).compute_geometry().boundary(*SHELL_BC)
+    r = ref.RefMesh.shell_tets(ncube, nr, 1.0, 6.0, st, n_solid=n_solid).boundary(*SHELL_BC)
+    assert h.topology_hash() == r.topology_hash()
+    for k in ("x", "cell_material", "face_tag", "face_kind", "edge_mode", "cell_center", "cell_volume", "face_area",
+              "face_center", "edge_vec", "edge_mid", "star1", "star2", "ec_cell", "ec_weight", "ef_weight"):
+        a, b = np.asarray(h[k]).ravel(), np.asarray(r[k]).ravel()
+        assert a.shape == b.shape and np.array_equal(a, b), k
+    wh = workloads.shell_state(h, "h", 1.0, st, sources=True)
+    wr = workloads.shell_state(r, "r", 1.0, st, sources=True)
+    assert all(np.array_equal(a, b) for a, b in zip(wh.U, wr.U)) and np.array_equal(wh.PhiAdd, wr.PhiAdd)
