@@ -177,11 +177,12 @@ int mhd_gpu_mesh_create(const MhdMeshDesc *d, MhdMesh **out)
         check_range(d->e2f_idx, e2fp[ne], nf, "e2f_idx");
         check_range(d->f2c_idx, f2cp[nf], nc, "f2c_idx");
         check_range(d->ec_cell, ecp[ne], nc, "ec_cell");
-        int32_t max_valence = 0;
+        int32_t max_valence = 0, max_edge_cells = 0;
         for (int64_t e = 0; e < ne; ++e)
         {
             MHD_REQUIRE(e2fp[e + 1] - e2fp[e] <= kMaxValence, "edge valence above " + std::to_string(kMaxValence) + " is not supported");
             max_valence = std::max(max_valence, e2fp[e + 1] - e2fp[e]);
+            max_edge_cells = std::max(max_edge_cells, ecp[e + 1] - ecp[e]);
         }
         MHD_REQUIRE(d->cell_material && d->face_kind && d->edge_mode, "missing material / boundary classification");
         MHD_REQUIRE(d->edge_vec && d->edge_mid && d->edge_len && d->face_area && d->face_center && d->face_area_mag &&
@@ -221,6 +222,7 @@ int mhd_gpu_mesh_create(const MhdMeshDesc *d, MhdMesh **out)
         v.nn = d->n_nodes; v.ne = d->n_edges; v.nf = d->n_faces; v.nc = d->n_cells;
         v.no_cells = d->n_owned_cells; v.no_edges = d->n_owned_edges;
         v.max_valence = max_valence;
+        v.max_edge_cells = max_edge_cells;
         m->c2f_ptr.upload(c2fp); m->c2f_idx.upload(d->c2f_idx, c2fp[nc]); m->c2f_sgn.upload(d->c2f_sgn, c2fp[nc]);
         m->f2e_ptr.upload(f2ep); m->f2e_idx.upload(d->f2e_idx, f2ep[nf]); m->f2e_sgn.upload(d->f2e_sgn, f2ep[nf]);
         m->e2f_ptr.upload(e2fp); m->e2f_idx.upload(d->e2f_idx, e2fp[ne]); m->e2f_sgn.upload(d->e2f_sgn, e2fp[ne]);

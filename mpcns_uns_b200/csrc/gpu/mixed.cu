@@ -30,9 +30,10 @@ struct MV
     int32_t nc, nf, ne, no_cells, no_edges;
     const int32_t *c2f_idx, *cfa_idx, *t_nb, *face_L, *face_R, *f2c_ptr, *f2c_idx, *f2e_ptr, *f2e_idx, *e2f_ptr, *e2f_idx, *ec_ptr,
         *ec_cell;
-    const int8_t *c2f_sgn, *cfa_sgn, *t_sg, *material, *face_kind, *edge_mode, *st_valid, *f2c_sgn, *f2e_sgn;
-    const float *wd, *dx, *inv, *recon, *fdx, *ew, *vol_inv;
-    const float4 *fn, *eth, *em;
+    const int8_t *c2f_sgn, *cfa_sgn, *t_sg, *material, *face_kind, *edge_mode, *st_valid, *f2c_sgn, *f2e_sgn, *emode;
+    const float *K, *recon, *fdx, *vol_inv;
+    const float4 *fn, *eth, *emn;
+    const float2 *esw;
     const char2 *fslot;
     const double *cell_volume; // FP64: the update divides the FP64-summed fluxes by it
 };
@@ -46,8 +47,8 @@ MV make_view(const MeshView &m, const MixedTables &t)
     v.e2f_idx = m.e2f_idx; v.ec_ptr = m.ec_ptr; v.ec_cell = m.ec_cell;
     v.c2f_sgn = m.c2f_sgn; v.cfa_sgn = m.cfa_sgn; v.t_sg = m.t_sg; v.material = m.material; v.face_kind = m.face_kind;
     v.edge_mode = m.edge_mode; v.st_valid = m.st_valid; v.f2c_sgn = m.f2c_sgn; v.f2e_sgn = m.f2e_sgn;
-    v.wd = t.wd.p; v.dx = t.dx.p; v.inv = t.inv.p; v.recon = t.recon.p; v.fdx = t.fdx.p; v.ew = t.ew.p; v.vol_inv = t.vol_inv.p;
-    v.fn = t.fn.p; v.eth = t.eth.p; v.em = t.em.p;
+    v.K = t.K.p; v.recon = t.recon.p; v.fdx = t.fdx.p; v.vol_inv = t.vol_inv.p;
+    v.fn = t.fn.p; v.eth = t.eth.p; v.emn = t.emn.p; v.esw = t.esw.p; v.emode = t.emode.p;
     v.fslot = t.fslot.p;
     v.cell_volume = m.cell_volume;
     return v;
@@ -68,17 +69,29 @@ __device__ __forceinline__ double mx_pe(const float4 *__restrict__ W, int32_t c)
 }
 
 // ------------------------------------------------------------------ one-time tables (FP64 in, FP32 out)
-__global__ void k_mx_cells(MeshView m, float *wd, float *dx, float *inv, float *recon, float *vol_inv)
+__global__ void k_mx_cells(MeshView m, float *K, float *recon, float *vol_inv)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
     const int64_t n = m.nc;
-    for (int i = 0; i < 12; ++i)
+    // The least-squares gradient g = I sum_k wd_k dq_k projected on the face offsets dx_j, dl_j = dx_j . g,
+    // is linear in the neighbour differences: dl_j = sum_k K_jk dq_k with K_jk = dx_j^T I wd_k (FP64 here,
+    // stored in FP32; skipped faces take no part in the sum)
     {
-        wd[i * n + c] = static_cast<float>(m.t_wd[i * n + c]);
-        dx[i * n + c] = static_cast<float>(m.t_dx[i * n + c]);
+        const double I00 = m.t_inv[c], I01 = m.t_inv[n + c], I02 = m.t_inv[2 * n + c], I11 = m.t_inv[3 * n + c],
+                     I12 = m.t_inv[4 * n + c], I22 = m.t_inv[5 * n + c];
+        for (int k = 0; k < 4; ++k)
+        {
+            const double w0 = m.t_wd[(3 * k) * n + c], w1 = m.t_wd[(3 * k + 1) * n + c], w2 = m.t_wd[(3 * k + 2) * n + c];
+            const double h0 = I00 * w0 + I01 * w1 + I02 * w2, h1 = I01 * w0 + I11 * w1 + I12 * w2, h2 = I02 * w0 + I12 * w1 + I22 * w2;
+            const bool skip = m.t_nb[k * n + c] == INT32_MIN;
+            for (int j = 0; j < 4; ++j)
+            {
+                const double v = m.t_dx[(3 * j) * n + c] * h0 + m.t_dx[(3 * j + 1) * n + c] * h1 + m.t_dx[(3 * j + 2) * n + c] * h2;
+                K[(4 * j + k) * n + c] = skip ? 0.f : static_cast<float>(v);
+            }
+        }
     }
-    for (int i = 0; i < 6; ++i) inv[i * n + c] = static_cast<float>(m.t_inv[i * n + c]);
     vol_inv[c] = static_cast<float>(1.0 / m.cell_volume[c]);
     // cell-field coefficients B_c = sum_j recon_j Phi_j of ImplicitInduction's constructor
     // (Common/induction/ImplicitInduction.cpp:34-62): recon_j = M^-1 n_j, M = sum A n n^T
@@ -139,13 +152,39 @@ __global__ void k_mx_faces(MeshView m, float4 *fn, float *fdx, char2 *fslot)
     fdx[3 * n + f] = static_cast<float>(dR.x); fdx[4 * n + f] = static_cast<float>(dR.y); fdx[5 * n + f] = static_cast<float>(dR.z);
 }
 
-__global__ void k_mx_edges(MeshView m, float4 *eth, float4 *em, float *ew)
+// Orthonormal basis (e1, e2) of the plane normal to the unit tangent th, built in single precision; the
+// table builder and the edge pass both call it on the same single-precision tangent, so they pick the
+// same helper axis and the same basis up to rounding.
+__host__ __device__ __forceinline__ void edge_basis(float3 th, float3 &e1, float3 &e2)
+{
+    const float3 ax = fabsf(th.x) < 0.9f ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
+    e1 = make_float3(th.y * ax.z - th.z * ax.y, th.z * ax.x - th.x * ax.z, th.x * ax.y - th.y * ax.x);
+    const float n1 = sqrtf(e1.x * e1.x + e1.y * e1.y + e1.z * e1.z);
+    e1 = n1 > 0.f ? make_float3(e1.x / n1, e1.y / n1, e1.z / n1) : make_float3(0.f, 0.f, 0.f);
+    e2 = make_float3(th.y * e1.z - th.z * e1.y, th.z * e1.x - th.x * e1.z, th.x * e1.y - th.y * e1.x);
+}
+
+__global__ void k_mx_edges(MeshView m, float4 *eth, int8_t *emode, float4 *emn, float2 *esw)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
     const double L = m.edge_len[e];
     const V3 th = L > 0 ? (1.0 / L) * ld3(m.edge_vec, e) : mk(0, 0, 0);
-    eth[e] = make_float4(static_cast<float>(th.x), static_cast<float>(th.y), static_cast<float>(th.z), static_cast<float>(L));
+    const float4 t4 = make_float4(static_cast<float>(th.x), static_cast<float>(th.y), static_cast<float>(th.z), static_cast<float>(L));
+    eth[e] = t4;
+    // the edge's mode in the mixed edge pass: edges that are not owned, or have no face, no length or no
+    // fluid cell get E = 0 like wall edges (IdealEMF.cpp:59-70 skips them; Solver.cpp:162-167)
+    int mode = e < m.no_edges ? m.edge_mode[e] : 1;
+    if (mode == 0)
+    {
+        bool fluid = false;
+        for (int32_t k = m.ec_ptr[e]; k < m.ec_ptr[e + 1]; ++k) fluid |= m.material[m.ec_cell[k]] == 0;
+        if (!fluid || t4.w <= 0.f || m.e2f_ptr[e + 1] == m.e2f_ptr[e]) mode = 1;
+    }
+    emode[e] = static_cast<int8_t>(mode);
+    float3 e1f, e2f;
+    edge_basis(make_float3(t4.x, t4.y, t4.z), e1f, e2f);
+    const V3 e1 = mk(e1f.x, e1f.y, e1f.z), e2 = mk(e2f.x, e2f.y, e2f.z);
     const V3 mid = ld3(m.edge_mid, e);
     for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k)
     {
@@ -156,8 +195,9 @@ __global__ void k_mx_edges(MeshView m, float4 *eth, float4 *em, float *ew)
         const V3 mi = nv > 0 ? (1.0 / nv) * v : mk(0, 0, 0);
         const V3 nrm = (1.0 / m.face_area_mag[f]) * ld3(m.face_area, f);
         const double sig = dot(th, cross(mi, nrm));
-        em[k] = make_float4(static_cast<float>(mi.x), static_cast<float>(mi.y), static_cast<float>(mi.z), static_cast<float>(sig));
-        ew[k] = static_cast<float>(m.ef_weight[k]);
+        emn[k] = make_float4(static_cast<float>(dot(mi, e1)), static_cast<float>(dot(mi, e2)), static_cast<float>(dot(nrm, e1)),
+                             static_cast<float>(dot(nrm, e2)));
+        esw[k] = make_float2(static_cast<float>(sig), static_cast<float>(m.ef_weight[k]));
     }
 }
 
@@ -179,6 +219,7 @@ struct MxParams
     int8_t absorb[kMaxSpecies];
     float mass[kMaxSpecies];
     float M_ref;
+    int update_ng;              // species in the group of the flux records the update gathers
     int src_on;                 // two-ion J x B force (species 0 = H+, 1 = Na+)
     float inver_MA2, ne_floor;
     int ambi, chem;             // ambipolar force, chemistry terms (two-ion model)
@@ -370,49 +411,51 @@ __global__ void __launch_bounds__(128) k_mx_cfl(MV m, MxParams p, float cfl, flo
     }
 }
 
-// limited face values (see below) of cell c for species s0 + g
-__device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int s0, int g, int32_t c, const float4 *__restrict__ W,
-                                            const double *__restrict__ U, float *__restrict__ G)
+// limited face values (see below) of cell c for species s0 + g of a group of ng: FV[(q*n + c)*ng + g] holds
+// variable q at the cell's four faces (c2f order) as one float4
+__device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int s0, int g, int ng, int32_t c,
+                                            const float4 *__restrict__ W, float4 *__restrict__ FV)
 {
     const int s = s0 + g;
-    if (c >= m.nc) return;
     const int64_t n = m.nc;
-    float *Gs = G + (int64_t)g * 20 * n;
     // primitives of species s: 8 floats per cell (rho u v w | p - - -), one 32-byte sector per gather
     const float4 *Ws = W + 2 * (int64_t)s * n;
     auto prim = [&](int32_t cc, float *q5) {
         const float4 a = Ws[2 * (int64_t)cc], b = Ws[2 * (int64_t)cc + 1];
         q5[0] = a.x; q5[1] = a.y; q5[2] = a.z; q5[3] = a.w; q5[4] = b.x;
     };
+    float4 *out = FV + (int64_t)c * ng + g;
+    const int64_t qs = n * ng; // stride of variable q
     if (c >= m.no_cells || !m.st_valid[c])
     {
         // zero gradient: every face value is the cell value
         float w5[5];
         prim(c, w5);
-        for (int q = 0; q < 5; ++q)
-            for (int j = 0; j < 4; ++j) Gs[(4 * q + j) * n + c] = w5[q];
+#pragma unroll
+        for (int q = 0; q < 5; ++q) out[q * qs] = make_float4(w5[q], w5[q], w5[q], w5[q]);
         return;
     }
     int32_t nb[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) nb[j] = m.t_nb[j * n + c];
-    float wc[5], wn[4][5], wd[12], dx[12];
+    float wc[5], wn[4][5], K[16];
     prim(c, wc);
 #pragma unroll
     for (int j = 0; j < 4; ++j)
         if (nb[j] >= 0) prim(nb[j], wn[j]);
 #pragma unroll
-    for (int i = 0; i < 12; ++i)
-    {
-        wd[i] = m.wd[i * n + c];
-        dx[i] = m.dx[i * n + c];
-    }
-    const float I00 = m.inv[c], I01 = m.inv[n + c], I02 = m.inv[2 * n + c], I11 = m.inv[3 * n + c], I12 = m.inv[4 * n + c],
-                I22 = m.inv[5 * n + c];
+    for (int i = 0; i < 16; ++i) K[i] = m.K[i * n + c];
     const F5 wcp{wc[0], wc[1], wc[2], wc[3], wc[4]};
 #pragma unroll
     for (int j = 0; j < 4; ++j)
-        if (nb[j] < 0 && nb[j] != INT32_MIN)
+    {
+        if (nb[j] == INT32_MIN)
+        {
+            // skipped face: no neighbour value (its column of K is zero, and it takes no part in the bounds)
+#pragma unroll
+            for (int q = 0; q < 5; ++q) wn[j][q] = wc[q];
+        }
+        else if (nb[j] < 0)
         {
             const int32_t f = -(nb[j] + 1);
             const float4 nf = m.fn[f];
@@ -422,33 +465,26 @@ __device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int 
                 gh = ghost32(m.face_kind[f], p.absorb[s] != 0, wcp, make_float3(sg * nf.x, sg * nf.y, sg * nf.z), p.fs[s]);
             wn[j][0] = gh.rho; wn[j][1] = gh.u; wn[j][2] = gh.v; wn[j][3] = gh.w; wn[j][4] = gh.p;
         }
-    (void)U;
-    // Limited face values v_j = w + psi g.dx_j (the face_state of FluxRHS.cpp:16-27 before its positivity
-    // test) instead of the gradient.  The face that sets the Barth-Jespersen psi is snapped to its bound,
-    // which exact arithmetic gives (w + (b - w)/dl * dl = b): near an absorbing wall the bound is the
+    }
+    // Limited face values v_j = w + psi dl_j, dl_j = g . dx_j (the face_state of FluxRHS.cpp:16-27 before its
+    // positivity test) instead of the gradient.  The face that sets the Barth-Jespersen psi is snapped to its
+    // bound, which exact arithmetic gives (w + (b - w)/dl * dl = b): near an absorbing wall the bound is the
     // 1e-12 floor state and the single-precision sum w + psi dl, with w ~ 1e-3, could not resolve it.
     float fv[5][4];
 #pragma unroll
     for (int q = 0; q < 5; ++q)
     {
-        float r0 = 0.f, r1 = 0.f, r2 = 0.f, lo = wc[q], hi = wc[q];
+        float dq[4], lo = wc[q], hi = wc[q];
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int k = 0; k < 4; ++k)
         {
-            if (nb[j] == INT32_MIN) continue;
-            const float dq = wn[j][q] - wc[q];
-            r0 += wd[3 * j] * dq;
-            r1 += wd[3 * j + 1] * dq;
-            r2 += wd[3 * j + 2] * dq;
-            lo = fminf(lo, wn[j][q]);
-            hi = fmaxf(hi, wn[j][q]);
+            dq[k] = wn[k][q] - wc[q];
+            lo = fminf(lo, wn[k][q]);
+            hi = fmaxf(hi, wn[k][q]);
         }
-        const float g0 = I00 * r0 + I01 * r1 + I02 * r2;
-        const float g1 = I01 * r0 + I11 * r1 + I12 * r2;
-        const float g2 = I02 * r0 + I12 * r1 + I22 * r2;
         float dl[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dl[j] = g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2];
+        for (int j = 0; j < 4; ++j) dl[j] = K[4 * j] * dq[0] + K[4 * j + 1] * dq[1] + K[4 * j + 2] * dq[2] + K[4 * j + 3] * dq[3];
         // Barth-Jespersen psi = min over the faces of (hi - w)/dl for dl > 0 and (lo - w)/dl for dl < 0: with
         // hi - w >= 0 >= lo - w the minimum is taken at the largest and at the most negative dl, so two
         // quotients per variable instead of four (likewise one for the relative limiter, at the largest |dl|)
@@ -490,23 +526,22 @@ __device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int 
         for (int j = 0; j < 4; ++j) fv[q][j] = j == jb ? bound : wc[q] + psi * dl[j];
     }
     // positivity fallback of face_state: a face with rho <= 0 or p <= 0 takes the cell state
+    bool ok[4];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
-    {
-        const bool ok = fv[0][j] > 0.f && fv[4][j] > 0.f;
+    for (int j = 0; j < 4; ++j) ok[j] = fv[0][j] > 0.f && fv[4][j] > 0.f;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Gs[(4 * q + j) * n + c] = ok ? fv[q][j] : wc[q];
-    }
+    for (int q = 0; q < 5; ++q)
+        out[q * qs] = make_float4(ok[0] ? fv[q][0] : wc[q], ok[1] ? fv[q][1] : wc[q], ok[2] ? fv[q][2] : wc[q], ok[3] ? fv[q][3] : wc[q]);
 }
 
-// Rusanov face flux times |A| of face f for species s0 + g
-__device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int s0, int g, int32_t f, const float *__restrict__ G,
-                                            float *__restrict__ F)
+// Rusanov face flux times |A| of face f for species s0 + g of a group of ng: F[(f*ng + g)*5 + q], so that a
+// face's fluxes of the whole group are one contiguous record for the update's gather
+__device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int s0, int g, int ng, int32_t f,
+                                            const float *__restrict__ FV, float *__restrict__ F)
 {
     const int s = s0 + g;
-    if (f >= m.nf) return;
-    const int64_t nf = m.nf, n = m.nc;
-    float *Fs = F + (int64_t)g * 5 * nf;
+    const int64_t n = m.nc;
+    float *Fo = F + ((int64_t)f * ng + g) * 5;
     const int kind = m.face_kind[f];
     const int32_t p0 = m.f2c_ptr[f], cnt = m.f2c_ptr[f + 1] - p0;
     const int32_t L = m.face_L[f], R = m.face_R[f];
@@ -515,17 +550,19 @@ __device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int 
     if (R >= 0) any |= R < m.no_cells && m.material[R] == 0;
     if (kind == 4 || !any)
     {
-        for (int q = 0; q < 5; ++q) Fs[q * nf + f] = 0.f;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) Fo[q] = 0.f;
         return;
     }
-    const float *Gs = G + (int64_t)g * 20 * n;
     const float4 nf4 = m.fn[f];
     const float3 nr = f3(nf4);
     const char2 sl = m.fslot[f];
-    // reconstructed face state of cell c (positivity fallback already applied by k_mx_grad)
+    // reconstructed face state of cell c (positivity fallback already applied by k_mx_grad): slot j of the
+    // cell's float4 of each variable
+    const int64_t qs = 4 * n * ng;
     auto state = [&](int32_t c, int side) {
-        const int j = side == 0 ? sl.x : sl.y;
-        return F5{Gs[(0 + j) * n + c], Gs[(4 + j) * n + c], Gs[(8 + j) * n + c], Gs[(12 + j) * n + c], Gs[(16 + j) * n + c]};
+        const float *b = FV + ((int64_t)c * ng + g) * 4 + (side == 0 ? sl.x : sl.y);
+        return F5{b[0], b[qs], b[2 * qs], b[3 * qs], b[4 * qs]};
     };
     F5 Ls, Rs;
     if (cnt == 2 && kind == 0)
@@ -553,7 +590,7 @@ __device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int 
     float Fl[5];
     rusanov32(Ls, Rs, nr, p.gamma, Fl);
 #pragma unroll
-    for (int q = 0; q < 5; ++q) Fs[q * nf + f] = Fl[q] * nf4.w;
+    for (int q = 0; q < 5; ++q) Fo[q] = Fl[q] * nf4.w;
 }
 
 // rhs gathered from the face fluxes, U (FP64) += dt rhs, floors, SSP-RK2 average in stage 2; cell c, species s0 + g
@@ -564,10 +601,10 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
                                               const double *__restrict__ vst, double *__restrict__ res)
 {
     const int s = s0 + g;
-    const int64_t n = m.nc, nf = m.nf;
+    const int64_t n = m.nc;
     const double *ub = Ub + (int64_t)s * 5 * n;
     double *uo = Uo + (int64_t)s * 5 * n;
-    const float *Fs = F + (int64_t)g * 5 * nf;
+    const int ng = p.update_ng;
     double u[5];
 #pragma unroll
     for (int q = 0; q < 5; ++q) u[q] = ub[q * n + c];
@@ -582,7 +619,7 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
 #pragma unroll
         for (int j = 0; j < 4; ++j)
 #pragma unroll
-            for (int q = 0; q < 5; ++q) r[q] += sv[j] * static_cast<double>(Fs[q * nf + ff[j]]);
+            for (int q = 0; q < 5; ++q) r[q] += sv[j] * static_cast<double>(F[((int64_t)ff[j] * ng + g) * 5 + q]);
         const double dtv = *dtp / m.cell_volume[c];
 #pragma unroll
         for (int q = 0; q < 5; ++q) u[q] += dtv * r[q];
@@ -690,7 +727,6 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf) return;
-    const int64_t nf = m.nf;
     const float4 nf4 = m.fn[f];
     const float3 n = f3(nf4);
     const float Bn = static_cast<float>(phi[f] + phi_add[f]) / nf4.w;
@@ -738,11 +774,13 @@ __global__ void __launch_bounds__(128) k_mx_face_cand(MV m, const float4 *__rest
 // edge.  The faces' terms enter only through sums, so one pass over the faces accumulates them: with
 // q_i = (q_a, q_b), w_i the face weight and x_i = w_i a_i sigma_i Phi_i/|A_i|,
 //   M = sum w q q^T, g = sum w q, E_u = sum (1 - q . l) x = sum x - l . sum q x,  l = M^-1 g,
-// so no per-face state is kept between two passes.  The basis (e1, e2) of the plane normal to the edge
-// is rebuilt from the unit tangent as the tables build it (the result does not depend on the choice of
-// orthonormal basis).
+// so no per-face state is kept between two passes.  Everything happens in the plane normal to the edge,
+// in the basis (e1, e2) of edge_basis: the in-face directions m_f and the face normals come from the
+// per-(edge, face) table in that basis, and the velocities of the edge's cells (at most 8 on the meshes
+// the mixed path takes) are projected onto it once and held in registers, so a_f = max_c |u_c . m_f| costs
+// no memory traffic per face.  Per face the pass gathers only the 16-byte EMF candidate record.
 __global__ void __launch_bounds__(128, 8) k_mx_edge(MV m, const float4 *__restrict__ Ef, const float4 *__restrict__ up,
-                                                    const double *__restrict__ phi, float cuct, float3 E_inf, float *__restrict__ E)
+                                                    float cuct, float3 E_inf, float *__restrict__ E)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
@@ -750,77 +788,69 @@ __global__ void __launch_bounds__(128, 8) k_mx_edge(MV m, const float4 *__restri
     const float4 t4 = m.eth[e];
     const float Lg = t4.w;
     const float3 th = f3(t4);
-    const int mode = e < m.no_edges ? m.edge_mode[e] : -1;
+    const int mode = m.emode[e];
     if (mode == 2) val = Lg * fdot(E_inf, th);
     else if (mode == 0)
     {
+        float3 e1, e2;
+        edge_basis(th, e1, e2);
+        const int32_t q0 = m.ec_ptr[e], nce = m.ec_ptr[e + 1] - q0;
         const int32_t f0 = m.e2f_ptr[e], nfe = m.e2f_ptr[e + 1] - f0;
-        const int32_t q0 = m.ec_ptr[e], q1 = m.ec_ptr[e + 1];
-        // the velocities of the edge's cells, gathered once into this thread's column of shared
-        // memory (every face of the edge takes the maximum over them); edges with more cells than
-        // the column holds gather them per face
+        // the velocities of the edge's cells in the plane normal to the edge (the mesh check admits at most 8)
         constexpr int kCells = 8;
-        __shared__ float4 s_up[kCells][128];
-        const bool cached = q1 - q0 <= kCells;
-        bool any_fluid = false;
-        for (int32_t k = q0; k < q1; ++k)
+        float pa[kCells], pb[kCells];
+#pragma unroll
+        for (int k = 0; k < kCells; ++k)
         {
-            const int32_t c = m.ec_cell[k];
-            any_fluid |= m.material[c] == 0;
-            if (cached) s_up[k - q0][threadIdx.x] = up[c];
+            pa[k] = 0.f;
+            pb[k] = 0.f;
+            if (k < nce)
+            {
+                const float3 u = f3(up[m.ec_cell[q0 + k]]);
+                pa[k] = fdot(u, e1);
+                pb[k] = fdot(u, e2);
+            }
         }
-        if (nfe > 0 && Lg > 0.f && any_fluid)
-        {
-            const float3 ax = fabsf(th.x) < 0.9f ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
-            float3 e1 = fcross(th, ax);
-            const float n1 = sqrtf(fdot(e1, e1));
-            e1 = n1 > 0.f ? make_float3(e1.x / n1, e1.y / n1, e1.z / n1) : make_float3(0.f, 0.f, 0.f);
-            const float3 e2 = fcross(th, e1);
-            float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f, S0 = 0.f, S1 = 0.f, S2 = 0.f;
-            // the next face's index is loaded one iteration ahead, so that the gathers of a face wait
-            // on one load instead of two
-            int32_t f_next = m.e2f_idx[f0];
+        float Ec = 0.f, M11 = 0.f, M12 = 0.f, M22 = 0.f, g1 = 0.f, g2 = 0.f, S0 = 0.f, S1 = 0.f, S2 = 0.f;
+        // the next face's index is loaded one iteration ahead, so that a face's gather waits on one load
+        int32_t f_next = m.e2f_idx[f0];
 #pragma unroll 1
-            for (int i = 0; i < nfe; ++i)
-            {
-                const int32_t f = f_next;
-                if (i + 1 < nfe) f_next = m.e2f_idx[f0 + i + 1];
-                const float4 mi4 = m.em[f0 + i];
-                const float3 mi = f3(mi4);
-                const float4 nf4 = m.fn[f];
-                const float w = m.ew[f0 + i];
-                const float4 ef = Ef[f];
-                Ec += w * (ef.x * th.x + ef.y * th.y + ef.z * th.z);
-                float a = 0.f;
-                if (cached)
-                    for (int32_t k = 0; k < q1 - q0; ++k) a = fmaxf(a, fabsf(fdot(f3(s_up[k][threadIdx.x]), mi)));
-                else
-                    for (int32_t k = q0; k < q1; ++k) a = fmaxf(a, fabsf(fdot(f3(up[m.ec_cell[k]]), mi)));
-                const float as = a * mi4.w;
-                const float qa = as * (nf4.x * e1.x + nf4.y * e1.y + nf4.z * e1.z);
-                const float qb = as * (nf4.x * e2.x + nf4.y * e2.y + nf4.z * e2.z);
-                const float wx = w * as * ef.w;
-                M11 += w * qa * qa;
-                M12 += w * qa * qb;
-                M22 += w * qb * qb;
-                g1 += w * qa;
-                g2 += w * qb;
-                S0 += wx;
-                S1 += qa * wx;
-                S2 += qb * wx;
-            }
-            const float tr = M11 + M22;
-            const float eps = 1e-14f * tr;
-            const float det = (M11 + eps) * (M22 + eps) - M12 * M12;
-            float l1 = 0.f, l2 = 0.f;
-            if (tr > 0.f && det > 0.f)
-            {
-                l1 = ((M22 + eps) * g1 - M12 * g2) / det;
-                l2 = ((M11 + eps) * g2 - M12 * g1) / det;
-            }
-            const float Eu = S0 - (l1 * S1 + l2 * S2);
-            val = Lg * Ec + 2.f * cuct * Lg * Eu;
+        for (int i = 0; i < nfe; ++i)
+        {
+            const int32_t f = f_next;
+            if (i + 1 < nfe) f_next = m.e2f_idx[f0 + i + 1];
+            const float4 mn = m.emn[f0 + i];
+            const float2 sw = m.esw[f0 + i];
+            const float4 ef = Ef[f];
+            const float w = sw.y;
+            Ec += w * (ef.x * th.x + ef.y * th.y + ef.z * th.z);
+            float a = 0.f;
+#pragma unroll
+            for (int k = 0; k < kCells; ++k) a = fmaxf(a, fabsf(pa[k] * mn.x + pb[k] * mn.y));
+            const float as = a * sw.x;
+            const float qa = as * mn.z;
+            const float qb = as * mn.w;
+            const float wx = w * as * ef.w;
+            M11 += w * qa * qa;
+            M12 += w * qa * qb;
+            M22 += w * qb * qb;
+            g1 += w * qa;
+            g2 += w * qb;
+            S0 += wx;
+            S1 += qa * wx;
+            S2 += qb * wx;
         }
+        const float tr = M11 + M22;
+        const float eps = 1e-14f * tr;
+        const float det = (M11 + eps) * (M22 + eps) - M12 * M12;
+        float l1 = 0.f, l2 = 0.f;
+        if (tr > 0.f && det > 0.f)
+        {
+            l1 = ((M22 + eps) * g1 - M12 * g2) / det;
+            l2 = ((M11 + eps) * g2 - M12 * g1) / det;
+        }
+        const float Eu = S0 - (l1 * S1 + l2 * S2);
+        val = Lg * Ec + 2.f * cuct * Lg * Eu;
     }
     E[e] = val;
 }
@@ -857,27 +887,27 @@ __global__ void k_mx_cfl_final(const unsigned long long *dt_bits, double dt_max,
     *dt = g;
 }
 
-// Face values: one species per block, the group's species interleaved; fluxes: one species per grid row.  The update: the species of a group
-// share one thread per cell, so the second one re-reads the cell's face indices, current terms and
-// fields from L1 / L2 rather than DRAM (measured 2.91 -> 2.72 ms per step on the 14.2M-cell shell;
-// the same change made the face-value and flux passes slower, so they keep one species per row).
-// Face values: blocks interleave the species of the group (block b: species b % ng, cells b / ng), so the
-// blocks of both species of the same cells run together and the second reads the stencil tables from L2
-// (2.96 -> 2.84 ms per step on the 14.2M-cell shell).  The flux pass keeps one species per grid row:
-// interleaved it measured 1.83 -> 1.99 ms.
+// Face values and fluxes: the species of a group run as adjacent threads (thread t: cell or face t / ng,
+// species t % ng).  The two threads of a cell read the same stencil tables (one load serves both), write
+// the adjacent float4s of its face values, and the two threads of a face read adjacent face values and
+// write adjacent halves of the face's flux record, so every gather and store of the pair shares its
+// sectors.  The update keeps the group's species in one thread per cell and gathers each face's record
+// once for both.
 __global__ void __launch_bounds__(128) k_mx_grad(MV m, MxParams p, int s0, int ng, const float4 *__restrict__ W,
-                                                 const double *__restrict__ U, float *__restrict__ G)
+                                                 float4 *__restrict__ FV)
 {
-    const int32_t c = (blockIdx.x / ng) * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t c = ng == 2 ? t >> 1 : t;
     if (c >= m.nc) return;
-    mx_grad_one(m, p, s0, blockIdx.x % ng, c, W, U, G);
+    mx_grad_one(m, p, s0, ng == 2 ? static_cast<int>(t & 1) : 0, ng, static_cast<int32_t>(c), W, FV);
 }
 
-__global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, int ng, const float *__restrict__ G, float *__restrict__ F)
+__global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, int ng, const float *__restrict__ FV, float *__restrict__ F)
 {
-    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t f = ng == 2 ? t >> 1 : t;
     if (f >= m.nf) return;
-    mx_flux_one(m, p, s0, blockIdx.y, f, G, F);
+    mx_flux_one(m, p, s0, ng == 2 ? static_cast<int>(t & 1) : 0, ng, static_cast<int32_t>(f), FV, F);
 }
 
 // gyr: the closing half-step gyration of the Strang splitting (mercury::gyrate, FP64 on the averaged
@@ -991,14 +1021,14 @@ void mixed_setup(MhdState *st)
     const size_t nc = m.nc, nf = m.nf, ne = m.ne;
     int32_t nnz_e2f = 0;
     MHD_CUDA(cudaMemcpy(&nnz_e2f, m.e2f_ptr + m.ne, sizeof(int32_t), cudaMemcpyDeviceToHost));
-    t.wd.alloc(12 * nc); t.dx.alloc(12 * nc); t.inv.alloc(6 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
+    t.K.alloc(16 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
     if (st->src.on) st->g32.alloc(nf);
     if (st->src.ambi) st->d32.alloc(nf);
     t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
-    t.eth.alloc(ne); t.em.alloc(nnz_e2f); t.ew.alloc(nnz_e2f);
-    if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.wd.p, t.dx.p, t.inv.p, t.recon.p, t.vol_inv.p);
+    t.eth.alloc(ne); t.emode.alloc(ne); t.emn.alloc(nnz_e2f); t.esw.alloc(nnz_e2f);
+    if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.K.p, t.recon.p, t.vol_inv.p);
     if (nf) k_mx_faces<<<grid_for(nf, 256), 256, 0, s>>>(m, t.fn.p, t.fdx.p, t.fslot.p);
-    if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.em.p, t.ew.p);
+    if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.emode.p, t.emn.p, t.esw.p);
     MHD_LAUNCH_CHECK();
     st->W32.alloc(8 * nc * st->nsp); // 8 floats per (species, cell): rho u v w | p, padded to 32 bytes
     st->grad32.alloc(20 * nc * st->group); // limited face values, 5 variables x 4 faces per cell
@@ -1080,17 +1110,20 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     {
         const int ng = std::min(st->group, st->nsp - s0);
         P.begin(KP_GRAD, s);
-        k_mx_grad<<<gc * ng, 128, 0, s>>>(m, p, s0, ng, W4, Us, st->grad32.p);
+        k_mx_grad<<<grid_for(static_cast<int64_t>(m.nc) * ng, 128), 128, 0, s>>>(m, p, s0, ng, W4,
+                                                                                   reinterpret_cast<float4 *>(st->grad32.p));
         MHD_LAUNCH_CHECK();
         P.end(KP_GRAD, s);
         P.begin(KP_FLUX, s);
-        k_mx_flux<<<dim3(gf, ng), 128, 0, s>>>(m, p, s0, ng, st->grad32.p, st->F32.p);
+        k_mx_flux<<<grid_for(static_cast<int64_t>(m.nf) * ng, 128), 128, 0, s>>>(m, p, s0, ng, st->grad32.p, st->F32.p);
         MHD_LAUNCH_CHECK();
         P.end(KP_FLUX, s);
         P.begin(KP_UPDATE, s);
         // the instance with the closing gyration fused carries its registers; the other stages use the lean one
         auto upd = gyrate_close && s0 == 0 ? k_mx_update<true> : k_mx_update<false>;
-        upd<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
+        MxParams pu = p;
+        pu.update_ng = ng;
+        upd<<<gc, 128, 0, s>>>(m, pu, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
                                gyrate_close && s0 == 0 ? 1 : 0, st->src.ambi ? st->d32.p : nullptr,
                                st->src.chem && st->photo.n ? st->photo.p : nullptr, st->src.chem && st->vst.n ? st->vst.p : nullptr);
         MHD_LAUNCH_CHECK();
@@ -1101,7 +1134,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
                                     static_cast<float>(-(st->prm.u_inf[2] * st->prm.B_imf[0] - st->prm.u_inf[0] * st->prm.B_imf[2])),
                                     static_cast<float>(-(st->prm.u_inf[0] * st->prm.B_imf[1] - st->prm.u_inf[1] * st->prm.B_imf[0])));
     P.begin(KP_EDGE_EMF, s);
-    k_mx_edge<<<ge, 128, 0, s>>>(m, st->Ef32.p, st->up32.p, phis, static_cast<float>(st->prm.cuct), Einf, st->E32.p);
+    k_mx_edge<<<ge, 128, 0, s>>>(m, st->Ef32.p, st->up32.p, static_cast<float>(st->prm.cuct), Einf, st->E32.p);
     MHD_LAUNCH_CHECK();
     if (st->src.ambi)
     {

@@ -19,14 +19,18 @@ using Profiler = EventProfiler<KP_COUNT>;
 // structure of arrays over cells / faces / edges so that every warp load is coalesced.
 struct MixedTables
 {
-    DBuf<float> wd, dx, inv;    // stencil: [12][nc], [12][nc], [6][nc]
+    DBuf<float> K;              // stencil: dl_j = sum_k K_jk (w_k - w_c), K_jk = dx_j^T I wd_k, [16][nc]
     DBuf<float> recon;          // cell field from face fluxes: B_c = sum_j recon[j] Phi_{f_j}, [12][nc]
     DBuf<float4> fn;            // per face: canonical unit normal, |A|
     DBuf<float> fdx;            // per face: x_f - x_L (3), x_f - x_R (3): [6][nf]
     DBuf<char2> fslot;          // per face: its position in the c2f rows of L and R
     DBuf<float4> eth;           // per edge: unit tangent, length
-    DBuf<float4> em;            // per e2f entry: in-face unit direction away from the edge, sigma = t.(m x n)
-    DBuf<float> ew;             // per e2f entry: w_ef
+    DBuf<int8_t> emode;         // per edge: 0 UCT, 1 zero (wall edge, not owned, no fluid cell, no face), 2 inflow
+    // per e2f entry, in the orthonormal basis (e1, e2) of the plane normal to the edge that edge_basis builds
+    // from the single-precision tangent: the in-face unit direction m away from the edge and the face's unit
+    // normal n, (m.e1, m.e2, n.e1, n.e2); and (sigma = t.(m x n), w_ef)
+    DBuf<float4> emn;
+    DBuf<float2> esw;
     DBuf<float> vol_inv;        // per cell: 1 / V
 };
 } // namespace mhd
