@@ -79,7 +79,7 @@ def algorithmic_bytes(k, c, nsp, group, precision="fp64", sources=False):
     state U and the face fluxes Phi stay 8), indices 4, signs / flags 1.  With the two-ion sources:
     * FP64: `prepare` includes the cell-current pass and `update` reads the J x B inputs.
     * Mixed: the face-candidate pass also writes the face terms of J (16 bytes per face), which the
-      update gathers with the total field.
+      update gathers with the total field (16 bytes per cell).
     * `gyrate` reads both ions' state and rewrites their momenta and energies, with the total field.
       The opening half step also renews the primitives and u+ of the cells it turns.  FP64 has two
       launches per step (opening, closing) and the figure is their mean.  Mixed has only the opening
@@ -90,7 +90,7 @@ def algorithmic_bytes(k, c, nsp, group, precision="fp64", sources=False):
     nc, nf = c["nc"], c["nf"]
     gyr = 80 * nc + 64 * nc + nc        # U of both ions in, momenta and energies out, material
     if precision == "mixed":
-        extra = {"face_candidate": 16 * nf, "update": 64 * nc,
+        extra = {"face_candidate": 16 * nf, "update": 16 * nf + 16 * nc,
                  "gyrate": gyr + 16 * nc + 20 * nsp * nc + 16 * nc}
     else:
         extra = {"prepare": 64 * nc + c["c2f"] * 5 + 36 * nf, "update": (2 + 3 + 3) * 8 * nc,
@@ -102,15 +102,23 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
     nc, nf, ne = c["nc"], c["nf"], c["ne"]
     if precision == "mixed":
         g, e2f, f2e, ec = group, c["e2f"], c["f2e"], c["ec"]
+        # limited_gradients: primitives (32 B per cell and species), stencil operator K (64 B) and neighbour ids (16 B),
+        #   validity, face values out (80 B per cell and species)
+        # face_flux: face values of both sides, flux records out, per-face normal, slots, L/R, kind, f2c row
+        # update: flux records, face ids and signs, U in and out, U of the averaged stage (stage 2: the mean over
+        #   the two launches is 20 B per species), 1/V, material
+        # edge_emf: tangent + length, mode, row pointers, E out; per (edge, face) id and the 24-byte plane table;
+        #   per (edge, cell) id; the faces' 16-byte EMF records and the cells' velocities
+        # ct: the packed face-edge record, Phi in, Phi out, the averaged Phi (mean 4 B), E
         return {
             "prepare": 40 * nsp * nc + 20 * nsp * nc + 16 * nc + 48 * nc + 8 * nf + 16 * nc + 48 * nc + nc,
             "cfl": 20 * nsp * nc + 16 * nc + 16 * nc + 16 * nf + 4 * nc + nc,
-            "limited_gradients": 20 * g * nc + 16 * nc + 120 * nc + nc + 60 * g * nc + 4 * nc,
-            "face_flux": 20 * g * nc + 60 * g * nc + 16 * nf + 24 * nf + 8 * nf + 14 * nf + nf + nc + 20 * g * nf,
-            "update": 20 * g * nf + 20 * nc + 40 * g * nc + 60 * g * nc + 4 * nc + nc,
+            "limited_gradients": 32 * g * nc + 64 * nc + 16 * nc + nc + 80 * g * nc,
+            "face_flux": 80 * g * nc + 20 * g * nf + 35 * nf + nc,
+            "update": 20 * g * nf + 20 * nc + 40 * g * nc + 40 * g * nc + 20 * g * nc + 4 * nc + nc,
             "face_candidate": 48 * nc + 16 * nf + 16 * nf + 8 * nf + 12 * nf,
-            "edge_emf": 16 * ne + 4 * ne + 24 * e2f + 4 * ne + 4 * ec + nc + 12 * nf + 16 * nf + 8 * nf + 16 * nc + ne + 4 * ne,
-            "ct": 4 * ne + 20 * nf + 4 * nf + 5 * f2e + 12 * nf,
+            "edge_emf": 29 * ne + 28 * e2f + 4 * ec + 16 * nf + 16 * nc,
+            "ct": 36 * nf + 4 * ne,
         }.get(k, 0.0)
     p = 8
     csr_c2f = c["c2f"] * 5 + nc * 4          # idx + sgn + ptr

@@ -150,6 +150,7 @@ struct MeshView
     int32_t nn, ne, nf, nc, no_cells, no_edges;
     int32_t max_valence; // largest number of faces at an edge
     int32_t max_edge_cells; // largest number of cells at an edge (ec rows)
+    int32_t tri_faces;      // 1 when every face is a triangle
     int32_t faces_per_cell; // 4 when every cell is a tetrahedron (c2f row k of cell c at 4c), else 0
     const double *st_dx; // face_center - cell_center per c2f entry (3 each)
     // tetrahedral meshes only: the stencil as structure of arrays over cells, slot j of cell c at

@@ -223,6 +223,8 @@ int mhd_gpu_mesh_create(const MhdMeshDesc *d, MhdMesh **out)
         v.no_cells = d->n_owned_cells; v.no_edges = d->n_owned_edges;
         v.max_valence = max_valence;
         v.max_edge_cells = max_edge_cells;
+        v.tri_faces = 1;
+        for (int64_t f = 0; f < nf && v.tri_faces; ++f) v.tri_faces = f2ep[f + 1] - f2ep[f] == 3;
         m->c2f_ptr.upload(c2fp); m->c2f_idx.upload(d->c2f_idx, c2fp[nc]); m->c2f_sgn.upload(d->c2f_sgn, c2fp[nc]);
         m->f2e_ptr.upload(f2ep); m->f2e_idx.upload(d->f2e_idx, f2ep[nf]); m->f2e_sgn.upload(d->f2e_sgn, f2ep[nf]);
         m->e2f_ptr.upload(e2fp); m->e2f_idx.upload(d->e2f_idx, e2fp[ne]); m->e2f_sgn.upload(d->e2f_sgn, e2fp[ne]);

@@ -593,34 +593,38 @@ __device__ __forceinline__ void mx_flux_one(const MV &m, const MxParams &p, int 
     for (int q = 0; q < 5; ++q) Fo[q] = Fl[q] * nf4.w;
 }
 
-// rhs gathered from the face fluxes, U (FP64) += dt rhs, floors, SSP-RK2 average in stage 2; cell c, species s0 + g
-__device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, int s0, int g, int32_t c, const float *__restrict__ F,
-                                              const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
-                                              int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
-                                              const float4 *__restrict__ bt, const float4 *__restrict__ D, const double *__restrict__ photo,
+// The stage's primitives of one species from its FP64 conservative state, as mx_prims forms them (the same
+// FP64 operations, rounded to FP32): the update takes them from the state it holds instead of re-reading
+// the FP32 primitive records
+struct Prim32
+{
+    float rho, u, v, w, p;
+};
+__device__ __forceinline__ Prim32 prims_of(const MxParams &p, const double *u)
+{
+    const double r = fmax(u[0], p.rho_floor_d);
+    const double ir = 1.0 / r;
+    const double vx = u[1] * ir, vy = u[2] * ir, vz = u[3] * ir;
+    const double pr = fmax((p.gamma_d - 1.0) * (u[4] - 0.5 * r * (vx * vx + vy * vy + vz * vz)), p.p_floor_d);
+    return Prim32{static_cast<float>(r), static_cast<float>(vx), static_cast<float>(vy), static_cast<float>(vz), static_cast<float>(pr)};
+}
+
+// U (FP64) += dt rhs, floors, SSP-RK2 average in stage 2; cell c, species s0 + g.  u holds the species'
+// stage state on entry, r the FP64 sum of its face fluxes (the caller gathered them); ws, nH, nN are the
+// stage primitives of this species and the ion number densities, jb = J x B_tot and d = V grad p_e of the
+// cell (used by the two-ion sources only).
+__device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, int s0, int g, int32_t c, bool fluid, const double *r,
+                                              double *__restrict__ u, double *__restrict__ Uo, const double *__restrict__ dtp, int stage2,
+                                              const Prim32 &ws, float nH, float nN, float3 jb, float3 d, const double *__restrict__ photo,
                                               const double *__restrict__ vst, double *__restrict__ res)
 {
     const int s = s0 + g;
     const int64_t n = m.nc;
-    const double *ub = Ub + (int64_t)s * 5 * n;
     double *uo = Uo + (int64_t)s * 5 * n;
-    const int ng = p.update_ng;
-    double u[5];
-#pragma unroll
-    for (int q = 0; q < 5; ++q) u[q] = ub[q * n + c];
-    if (c < m.no_cells && m.material[c] == 0)
+    if (fluid)
     {
-        const int4 fi = *reinterpret_cast<const int4 *>(m.cfa_idx + 4 * (int64_t)c);
-        const char4 sg = *reinterpret_cast<const char4 *>(m.cfa_sgn + 4 * (int64_t)c);
-        const int32_t ff[4] = {fi.x, fi.y, fi.z, fi.w};
-        const double sv[4] = {sg.x > 0 ? -1.0 : 1.0, sg.y > 0 ? -1.0 : 1.0, sg.z > 0 ? -1.0 : 1.0, sg.w > 0 ? -1.0 : 1.0};
-        // the face fluxes are summed in FP64: the rhs is a difference of fluxes that can nearly cancel
-        double r[5] = {0, 0, 0, 0, 0};
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-#pragma unroll
-            for (int q = 0; q < 5; ++q) r[q] += sv[j] * static_cast<double>(F[((int64_t)ff[j] * ng + g) * 5 + q]);
-        const double dtv = *dtp / m.cell_volume[c];
+        const float iv = m.vol_inv[c];
+        const double dtv = *dtp * static_cast<double>(iv);
 #pragma unroll
         for (int q = 0; q < 5; ++q) u[q] += dtv * r[q];
         if (p.src_on || p.ambi || p.chem)
@@ -630,50 +634,25 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
             // k_mx_face_cand, same faces as the flux gather), S = inver_MA2 n_s / n_e,eff (J x B_tot).  The
             // ambipolar force -w_s grad p_e with grad p_e = (1/V) sum_f D_f.  The chemistry terms in FP64
             // from the FP32 primitives.
-            const float iv = m.vol_inv[c];
-            const float4 ws4 = W[2 * ((int64_t)s * n + c)];
-            const float nH = fmaxf(W[2 * (int64_t)c].x, 0.f) / p.mass[0] * p.M_ref;
-            const float nN = fmaxf(W[2 * (n + c)].x, 0.f) / p.mass[1] * p.M_ref;
             const float ne = nH + nN;
             float Sx = 0.f, Sy = 0.f, Sz = 0.f;
             if (p.src_on)
             {
-                float3 Jc = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                {
-                    const float4 g = G[ff[j]];
-                    const float sj = sv[j] < 0.0 ? 1.f : -1.f; // +1 where the canonical normal points out of c
-                    Jc.x += sj * g.x;
-                    Jc.y += sj * g.y;
-                    Jc.z += sj * g.z;
-                }
-                Jc = make_float3(iv * Jc.x, iv * Jc.y, iv * Jc.z);
                 const float k = p.inver_MA2 * (s == 0 ? nH : nN) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
-                const float3 jb = fcross(Jc, f3(bt[c]));
                 Sx = k * jb.x;
                 Sy = k * jb.y;
                 Sz = k * jb.z;
             }
             if (p.ambi)
             {
-                float3 d = make_float3(0.f, 0.f, 0.f);
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                {
-                    const float4 g = D[ff[j]]; // already oriented: the same vector for both cells of the face
-                    d.x += g.x;
-                    d.y += g.y;
-                    d.z += g.z;
-                }
                 const float ws = (s == 0 ? nH : nN) / sqrtf(ne * ne + p.ne_floor * p.ne_floor);
                 Sx -= ws * iv * d.x;
                 Sy -= ws * iv * d.y;
                 Sz -= ws * iv * d.z;
             }
-            const float rho = fmaxf(ws4.x, 0.f);
+            const float rho = fmaxf(ws.rho, 0.f);
             const double dt = *dtp;
-            const float work = ws4.y * Sx + ws4.z * Sy + ws4.w * Sz +
+            const float work = ws.u * Sx + ws.v * Sy + ws.w * Sz +
                                (rho > 1e-30f ? 0.5f * static_cast<float>(dt) * (Sx * Sx + Sy * Sy + Sz * Sz) / rho : 0.f);
             u[1] += dt * static_cast<double>(Sx);
             u[2] += dt * static_cast<double>(Sy);
@@ -681,7 +660,7 @@ __device__ __forceinline__ void mx_update_one(const MV &m, const MxParams &p, in
             u[4] += dt * static_cast<double>(work);
             if (p.chem && vst)
             {
-                const double v = vst[c], r = rho, ux = ws4.y, uy = ws4.z, uz = ws4.w, ps = W[2 * ((int64_t)s * n + c) + 1].x;
+                const double v = vst[c], r = rho, ux = ws.u, uy = ws.v, uz = ws.w, ps = ws.p;
                 const double u2 = ux * ux + uy * uy + uz * uz;
                 const double Ts = ps / (r > 0 ? r : 1e-300) / (s == 0 ? p.sch : p.scn) * p.T_ref;
                 const double mH = p.mass[0], mN = p.mass[1], Msum = mH + mN;
@@ -855,22 +834,37 @@ __global__ void __launch_bounds__(128, 8) k_mx_edge(MV m, const float4 *__restri
     E[e] = val;
 }
 
-// Phi -= dt d1 E on the active faces, E summed in FP64; stage 2 averages with Phi0
-__global__ void __launch_bounds__(256) k_mx_ct(MV m, const float *__restrict__ E, const double *__restrict__ phis,
-                                               double *__restrict__ phio, const double *__restrict__ dtp, int stage2)
+// Phi -= dt d1 E on the active faces (mhd::active_faces, Faraday.cpp:7-13), E summed in FP64; stage 2
+// averages with Phi0.  The faces of a tetrahedral mesh are triangles: one 16-byte record per face holds its
+// three edges (f2e order) and, in the last word, the edges' negative signs (bits 0-2) and the active flag
+// (bit 3), so the pass reads one coalesced record instead of the CSR rows of f2e and f2c.
+__global__ void __launch_bounds__(256) k_mx_ct(int32_t nf, const int4 *__restrict__ fe, const float *__restrict__ E,
+                                               const double *__restrict__ phis, double *__restrict__ phio, const double *__restrict__ dtp,
+                                               int stage2)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const int4 r = fe[f];
+    double v = phis[f];
+    if (r.w & 8)
+    {
+        const double e0 = E[r.x], e1 = E[r.y], e2 = E[r.z];
+        const double circ = ((r.w & 1) ? -e0 : e0) + ((r.w & 2) ? -e1 : e1) + ((r.w & 4) ? -e2 : e2);
+        v -= *dtp * circ;
+    }
+    phio[f] = stage2 ? 0.5 * (phio[f] + v) : v;
+}
+
+__global__ void k_mx_face_edges(MeshView m, int4 *fe)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf) return;
     bool active = false;
     for (int32_t k = m.f2c_ptr[f]; k < m.f2c_ptr[f + 1]; ++k) active |= m.f2c_idx[k] < m.no_cells;
-    double v = phis[f];
-    if (active)
-    {
-        double circ = 0.0;
-        for (int32_t k = m.f2e_ptr[f]; k < m.f2e_ptr[f + 1]; ++k) circ += m.f2e_sgn[k] * static_cast<double>(E[m.f2e_idx[k]]);
-        v -= *dtp * circ;
-    }
-    phio[f] = stage2 ? 0.5 * (phio[f] + v) : v;
+    const int32_t k0 = m.f2e_ptr[f];
+    int w = active ? 8 : 0;
+    for (int i = 0; i < 3; ++i) w |= m.f2e_sgn[k0 + i] < 0 ? (1 << i) : 0;
+    fe[f] = make_int4(m.f2e_idx[k0], m.f2e_idx[k0 + 1], m.f2e_idx[k0 + 2], w);
 }
 
 __global__ void k_mx_cfl_init(unsigned long long *dt_bits, int *flag)
@@ -923,16 +917,95 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc) return;
     const int64_t n = m.nc;
-    double r0[5], r1[5];
-    mx_update_one(m, p, s0, 0, c, F, Ub, Uo, dtp, stage2, W, G, bt, D, photo, vst, r0);
-    if (ng > 1) mx_update_one(m, p, s0, 1, c, F, Ub, Uo, dtp, stage2, W, G, bt, D, photo, vst, r1);
-    if (GYR && gyr && ng == 2 && c < m.no_cells && m.material[c] != 1) gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), 0.5 * *dtp, r0, r1);
-    double *u0 = Uo + (int64_t)s0 * 5 * n;
+    double r0[5], r1[5], u0[5], u1[5];
+    const double *ub = Ub + (int64_t)s0 * 5 * n;
 #pragma unroll
-    for (int q = 0; q < 5; ++q) u0[q * n + c] = r0[q];
+    for (int q = 0; q < 5; ++q)
+    {
+        u0[q] = ub[q * n + c];
+        u1[q] = ng > 1 ? ub[(5 + q) * n + c] : 0.0;
+    }
+    // the four faces' flux records, summed in FP64 (the rhs is a difference of fluxes that can nearly cancel);
+    // with two species a face's record is 10 floats at an 8-byte boundary, read as five float2
+    const bool fluid = c < m.no_cells && m.material[c] == 0;
+    int32_t ff[4] = {0, 0, 0, 0};
+    double sv[4] = {0, 0, 0, 0}, f0[5] = {0, 0, 0, 0, 0}, f1[5] = {0, 0, 0, 0, 0};
+    if (fluid)
+    {
+        const int4 fi = *reinterpret_cast<const int4 *>(m.cfa_idx + 4 * (int64_t)c);
+        const char4 sg = *reinterpret_cast<const char4 *>(m.cfa_sgn + 4 * (int64_t)c);
+        ff[0] = fi.x; ff[1] = fi.y; ff[2] = fi.z; ff[3] = fi.w;
+        sv[0] = sg.x > 0 ? -1.0 : 1.0; sv[1] = sg.y > 0 ? -1.0 : 1.0; sv[2] = sg.z > 0 ? -1.0 : 1.0; sv[3] = sg.w > 0 ? -1.0 : 1.0;
+        if (ng == 2)
+        {
+            const float2 *R = reinterpret_cast<const float2 *>(F);
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+            {
+                const float2 a = R[5 * (int64_t)ff[j]], b = R[5 * (int64_t)ff[j] + 1], d = R[5 * (int64_t)ff[j] + 2],
+                             e = R[5 * (int64_t)ff[j] + 3], h = R[5 * (int64_t)ff[j] + 4];
+                f0[0] += sv[j] * static_cast<double>(a.x); f0[1] += sv[j] * static_cast<double>(a.y);
+                f0[2] += sv[j] * static_cast<double>(b.x); f0[3] += sv[j] * static_cast<double>(b.y);
+                f0[4] += sv[j] * static_cast<double>(d.x);
+                f1[0] += sv[j] * static_cast<double>(d.y); f1[1] += sv[j] * static_cast<double>(e.x);
+                f1[2] += sv[j] * static_cast<double>(e.y); f1[3] += sv[j] * static_cast<double>(h.x);
+                f1[4] += sv[j] * static_cast<double>(h.y);
+            }
+        }
+        else
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int q = 0; q < 5; ++q) f0[q] += sv[j] * static_cast<double>(F[5 * (int64_t)ff[j] + q]);
+    }
+    // the two-ion sources (their switches require exactly the species 0 and 1 in this thread) need the stage
+    // primitives of both ions
+    Prim32 w0{}, w1{};
+    float nH = 0.f, nN = 0.f;
+    if (p.src_on || p.ambi || p.chem)
+    {
+        w0 = prims_of(p, u0);
+        w1 = prims_of(p, u1);
+        nH = fmaxf(w0.rho, 0.f) / p.mass[0] * p.M_ref;
+        nN = fmaxf(w1.rho, 0.f) / p.mass[1] * p.M_ref;
+    }
+    // the cell current from the face terms of the face-candidate pass, J_c = (1/V) sum_f s_f G_f over the
+    // faces of the flux gather, and J x B_tot; the face terms D_f of grad p_e (already oriented: the same
+    // vector for both cells of the face)
+    float3 jb = make_float3(0.f, 0.f, 0.f), dsum = make_float3(0.f, 0.f, 0.f);
+    if (fluid && p.src_on)
+    {
+        float3 Jc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const float4 g = G[ff[j]];
+            const float sj = sv[j] < 0.0 ? 1.f : -1.f; // +1 where the canonical normal points out of c
+            Jc.x += sj * g.x;
+            Jc.y += sj * g.y;
+            Jc.z += sj * g.z;
+        }
+        const float iv = m.vol_inv[c];
+        jb = fcross(make_float3(iv * Jc.x, iv * Jc.y, iv * Jc.z), f3(bt[c]));
+    }
+    if (fluid && p.ambi)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+        {
+            const float4 g = D[ff[j]];
+            dsum.x += g.x;
+            dsum.y += g.y;
+            dsum.z += g.z;
+        }
+    mx_update_one(m, p, s0, 0, c, fluid, f0, u0, Uo, dtp, stage2, w0, nH, nN, jb, dsum, photo, vst, r0);
+    if (ng > 1) mx_update_one(m, p, s0, 1, c, fluid, f1, u1, Uo, dtp, stage2, w1, nH, nN, jb, dsum, photo, vst, r1);
+    if (GYR && gyr && ng == 2 && c < m.no_cells && m.material[c] != 1) gyrate_cell(sp, mk(bt[c].x, bt[c].y, bt[c].z), 0.5 * *dtp, r0, r1);
+    double *uo = Uo + (int64_t)s0 * 5 * n;
+#pragma unroll
+    for (int q = 0; q < 5; ++q) uo[q * n + c] = r0[q];
     if (ng > 1)
 #pragma unroll
-        for (int q = 0; q < 5; ++q) u0[(5 + q) * n + c] = r1[q];
+        for (int q = 0; q < 5; ++q) uo[(5 + q) * n + c] = r1[q];
 }
 
 // nodal p_e of AmbipolarEMF::add (Ambipolar.cpp:57-68) from the FP64 p_e of the cells
@@ -1024,10 +1097,11 @@ void mixed_setup(MhdState *st)
     t.K.alloc(16 * nc); t.recon.alloc(12 * nc); t.vol_inv.alloc(nc);
     if (st->src.on) st->g32.alloc(nf);
     if (st->src.ambi) st->d32.alloc(nf);
-    t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf);
+    t.fn.alloc(nf); t.fdx.alloc(6 * nf); t.fslot.alloc(nf); t.fe.alloc(nf);
     t.eth.alloc(ne); t.emode.alloc(ne); t.emn.alloc(nnz_e2f); t.esw.alloc(nnz_e2f);
     if (nc) k_mx_cells<<<grid_for(nc, 128), 128, 0, s>>>(m, t.K.p, t.recon.p, t.vol_inv.p);
     if (nf) k_mx_faces<<<grid_for(nf, 256), 256, 0, s>>>(m, t.fn.p, t.fdx.p, t.fslot.p);
+    if (nf) k_mx_face_edges<<<grid_for(nf, 256), 256, 0, s>>>(m, t.fe.p);
     if (ne) k_mx_edges<<<grid_for(ne, 128), 128, 0, s>>>(m, t.eth.p, t.emode.p, t.emn.p, t.esw.p);
     MHD_LAUNCH_CHECK();
     st->W32.alloc(8 * nc * st->nsp); // 8 floats per (species, cell): rho u v w | p, padded to 32 bytes
@@ -1148,7 +1222,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
     }
     P.end(KP_EDGE_EMF, s);
     P.begin(KP_CT, s);
-    k_mx_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m, st->E32.p, phis, phio, st->scal.p, stage2 ? 1 : 0);
+    k_mx_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m.nf, st->mt.fe.p, st->E32.p, phis, phio, st->scal.p, stage2 ? 1 : 0);
     MHD_LAUNCH_CHECK();
     P.end(KP_CT, s);
     st->launches += 3;

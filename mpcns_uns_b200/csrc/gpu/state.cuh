@@ -24,6 +24,7 @@ struct MixedTables
     DBuf<float4> fn;            // per face: canonical unit normal, |A|
     DBuf<float> fdx;            // per face: x_f - x_L (3), x_f - x_R (3): [6][nf]
     DBuf<char2> fslot;          // per face: its position in the c2f rows of L and R
+    DBuf<int4> fe;              // per (triangular) face: its 3 edges, negative-sign bits 0-2 and active bit 3
     DBuf<float4> eth;           // per edge: unit tangent, length
     DBuf<int8_t> emode;         // per edge: 0 UCT, 1 zero (wall edge, not owned, no fluid cell, no face), 2 inflow
     // per e2f entry, in the orthonormal basis (e1, e2) of the plane normal to the edge that edge_basis builds

@@ -535,7 +535,7 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         st->mixed = p->precision == MHD_PREC_MIXED;
         if (st->mixed)
         {
-            MHD_REQUIRE(m.faces_per_cell == 4, "mixed precision needs a tetrahedral mesh");
+            MHD_REQUIRE(m.faces_per_cell == 4 && m.tri_faces, "mixed precision needs a tetrahedral mesh");
             MHD_REQUIRE(m.max_valence <= 8 && m.max_edge_cells <= 8, "mixed precision needs edge valence <= 8");
             mixed_setup(st);
         }
