@@ -297,12 +297,15 @@ def time_reference(wl, steps, warmup):
     return wl.mesh.n_cells * wl.n_species * 2 / per_step, per_step
 
 
-def gmres_bytes(k, c, precision, steps, mgs_launches):
+def gmres_bytes(k, c, precision, steps, launches, reorth=0):
     """Compulsory bytes of one launch of kernel class k of the induction solve, in the form the
-    Arnoldi step runs it (preconditioned input, lazily normalised basis vector, Dirichlet mask, dot
-    with V_0).  q = bytes of the operator's arrays (8 FP64, 4 for the FP32 operator of the mixed solve);
-    Krylov vectors are FP64.  mgs: one launch reads w, V_{i-1}, V_i and writes w (the last of a step
-    reads w and V_j only), so a solve of `steps` Arnoldi steps and L launches moves (4L - steps) vectors."""
+    Arnoldi step runs it (preconditioned input, lazily normalised basis vector, Dirichlet mask).
+    q = bytes of the operator's arrays (8 FP64, 4 for the FP32 operator of the mixed solve); Krylov
+    vectors are FP64.  gram_schmidt: Arnoldi step j (j + 1 basis vectors) reads w and V_0..V_j in its
+    dot pass, reads them again and writes w and the next matvec's input (8 bytes, 4 in mixed
+    precision) in its update pass, and once more in the second pass where one ran (`reorth` of them);
+    `launches` counts the class's launches (three per step, the second pass's gated ones included),
+    so the figure is the solve's bytes over its launches."""
     q = 4 if precision == "mixed" else 8
     nc, nf, ne = c["nc"], c["nf"], c["ne"]
     if k == "face_d1":
@@ -313,8 +316,17 @@ def gmres_bytes(k, c, precision, steps, mgs_launches):
         return 4 * nc + 5 * c["c2f"] + 4 * nf + 4 * c["f2c"] + 3 * q * nf + 11 * q * nc + nc
     if k == "edge_gather":
         return 8 * ne + 5 * c["e2f"] + q * nf + (4 + q) * c["ec"] + 4 * q * ne + 3 * q * nc + 41 * ne
-    if k == "mgs":
-        return (4 * mgs_launches - steps) * 8 * ne / max(mgs_launches, 1)
+    if k == "gram_schmidt":
+        # steps run in cycles of 30: column j of a cycle has j + 1 basis vectors
+        vec = 0.0
+        zs = 4 if precision == "mixed" else 8
+        for t in range(steps):
+            j = t % 30
+            vec += (j + 2) * 8 + (j + 2) * 8 + 8 + zs
+        if steps:
+            jm = sum(t % 30 for t in range(steps)) / steps
+            vec += reorth * ((jm + 2) * 8 + 8 + zs)
+        return vec * ne / max(launches, 1)
     return 0
 
 
@@ -354,16 +366,17 @@ def bench_gmres(args, peak):
         di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)
         prof = di.profile_read()
         di.profile(False)
-        mgs_l = prof.get("mgs", (0, 0))[1]
+        gs_l = prof.get("gram_schmidt", (0, 0))[1]
+        reorth = di.reorth_passes()
         kern = {}
         for k, (kms, n) in prof.items():
             if not n:
                 continue
-            b = gmres_bytes(k, counts, prec, it, mgs_l)
+            b = gmres_bytes(k, counts, prec, it, gs_l, reorth)
             kern[k] = {"ms_per_solve": kms, "launches_per_solve": n, "GBps": b / (kms / n / 1e3) / 1e9 if b else None}
         top = max((k for k in kern if kern[k]["GBps"]), key=lambda k: kern[k]["ms_per_solve"])
         E[prec] = Ed.double().cpu().numpy()
-        out[prec] = {"s_per_solve": ms / 1e3, "iterations": it, "rel_res": rr, "converged": rr <= 1e-8,
+        out[prec] = {"s_per_solve": ms / 1e3, "iterations": it, "rel_res": rr, "converged": rr <= 1e-8, "reorth_passes": reorth,
                      "ms_per_iteration": ms / max(it, 1), "gpu_launches_per_solve": launches, "kernels": kern,
                      "roofline": {"bound": "hbm", "kernel": top, "achieved": kern[top]["GBps"], "peak": peak, "unit": "GB/s",
                                   "frac": kern[top]["GBps"] / peak}}
@@ -581,9 +594,10 @@ def summary(out):
                      "Phi": _r(a["Phi_rel_l2"], 3), "divB": [_r(a["div_b_max_rel_mixed"], 3), _r(a["div_b_max_rel_fp64"], 3)]}
     g = out.get("gmres")
     if g:
-        sm["gmres"] = {p: [_r(g[p]["s_per_solve"]), g[p]["iterations"], _r(g[p]["rel_res"], 3)] for p in ("fp64", "mixed")}
+        sm["gmres"] = {p: [_r(g[p]["s_per_solve"]), g[p]["iterations"], _r(g[p]["rel_res"], 3), g[p].get("reorth_passes")]
+                       for p in ("fp64", "mixed")}
         sm["gmres"]["speedup_mixed"] = _r(g["speedup_mixed"])
-        sm["gmres"]["cols"] = "s_per_solve, iterations, rel_res"
+        sm["gmres"]["cols"] = "s_per_solve, iterations, rel_res, Gram-Schmidt second passes"
     d = out.get("adjoint")
     if d:
         fd = d["fd"]

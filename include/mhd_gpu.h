@@ -179,8 +179,11 @@ int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);
 /* ------------------------------------------------------------------ semi-implicit induction
  * mhd::ImplicitInduction (Common/induction/ImplicitInduction.h:27-94): the operator
  *   F(Phi) = M d1^T S2 Phi + H(Phi),  A x = x + dt F(d1 x)
- * and the restarted GMRES(m) with modified Gram-Schmidt, Givens rotations, Jacobi right
- * preconditioner, true residual at every restart and warm start (.cpp:299-390).  The resistive
+ * and the restarted GMRES(m) with Givens rotations, Jacobi right preconditioner, true residual at
+ * every restart and warm start (.cpp:299-390).  The reference orthogonalises with modified
+ * Gram-Schmidt; here (restart <= 31) classical Gram-Schmidt with a second pass where the first
+ * cancelled and left components above round-off: the same Krylov space and Hessenberg matrix to
+ * rounding, two or three passes over the basis per Arnoldi step (restart > 31: modified Gram-Schmidt).  The resistive
  * coefficient m_e = eta_e / star1_e is given per edge (host array, may be NULL), which covers the
  * reference's tanh window and any other profile.  Mixed precision: the operator and the
  * preconditioner inside the Arnoldi cycles in FP32; Krylov basis, Gram-Schmidt, Hessenberg,
@@ -205,13 +208,15 @@ int mhd_gpu_induction_apply_A(MhdInduction *ind, const double *x, double dt, dou
 int mhd_gpu_induction_solve(MhdInduction *ind, const double *Phi, const double *E_expl, const int8_t *dirichlet, double dt,
                             int32_t warm, double *E, int32_t *iterations, double *rel_res);
 /* Per-kernel-class device time of the solve (CUDA events on the mesh stream while enabled; classes:
- * face_d1, cell_field, hall_emf, edge_gather, mgs, krylov_scalar, krylov_vector; a profiled solve
+ * face_d1, cell_field, hall_emf, edge_gather, gram_schmidt, krylov_scalar, krylov_vector; a profiled solve
  * launches its kernels one by one instead of replaying the restart-cycle graph), read as
  * in mhd_gpu_state_profile_read; and the number of kernels the handle has launched. */
 int mhd_gpu_induction_profile(MhdInduction *ind, int32_t enable);
 int mhd_gpu_induction_profile_read(MhdInduction *ind, int32_t max_kernels, char *names, double *ms_total, int64_t *count,
                                    int32_t *n_out);
 int mhd_gpu_induction_launches(MhdInduction *ind, int64_t *out);
+/* Gram-Schmidt second passes (re-orthogonalisations) the last solve ran; no GPU work. */
+int mhd_gpu_induction_last_solve_stats(MhdInduction *ind, int32_t *reorth_passes);
 
 /* ------------------------------------------------------------------ resident state, fused step
  * The explicit step of mercury::Solver::step (MercuryUns/driver/Solver.cpp:481-516) restricted to

@@ -21,80 +21,15 @@
 //   * every dot finishes in the kernel that produces it (the last block adds the block partials), and
 //     a restart cycle runs as one CUDA graph whose steps test a device-side flag, so the host waits
 //     once per restart instead of once per Arnoldi step.
-#include <algorithm>
-#include <cmath>
-#include <cstring>
-#include <vector>
+#include <array>
+#include <utility>
 
-#include "common.cuh"
+#include "induction_op.cuh"
 
 namespace mhd
 {
 namespace
 {
-constexpr int kRedBlocks = 8 * 148; // streaming reductions: 8 resident 256-thread blocks per SM
-
-// kernel classes of the solve, timed with CUDA events on the handle's stream when profiling is on
-enum IndKernel { KI_FACE = 0, KI_BCELL, KI_HALL, KI_EDGE, KI_MGS, KI_SCALAR, KI_VECTOR, KI_COUNT };
-const char *const kIndKernelNames[KI_COUNT] = {"face_d1", "cell_field", "hall_emf",     "edge_gather",
-                                               "mgs",     "krylov_scalar", "krylov_vector"};
-
-__device__ __forceinline__ double block_sum(double v)
-{
-    __shared__ double sh[32];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if (lane == 0) sh[wid] = v;
-    __syncthreads();
-    if (wid == 0)
-    {
-        v = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    }
-    return v;
-}
-
-// Device-side control of one restart cycle: the Arnoldi steps of a cycle are enqueued (or replayed as
-// one CUDA graph) without host round trips; a step whose predecessor met the tolerance, or that lies
-// beyond the iteration limit, returns at once.
-struct Ctl
-{
-    int done, jend, limit, pad;
-    double tol, dt;
-};
-struct Gate
-{
-    const Ctl *ctl = nullptr;
-    int j = 0;
-    __device__ __forceinline__ bool off() const { return ctl && (ctl->done || j >= ctl->limit); }
-};
-
-// Block partials of a grid-wide sum; the last block to finish adds them in block order (deterministic)
-// and stores op(sum) to *out (op 0: the sum, 1: its square root, 2: sqrt(max(sum, 1e-300))), then
-// re-arms the counter.  No block waits for another.
-__device__ __forceinline__ void grid_sum_tail(double v, double *part, unsigned *counter, int op, double *out)
-{
-    __shared__ bool last;
-    v = block_sum(v);
-    if (threadIdx.x == 0)
-    {
-        part[blockIdx.x] = v;
-        __threadfence();
-        last = atomicAdd(counter, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    double s = 0.0;
-    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) s += __ldcg(part + i);
-    s = block_sum(s);
-    if (threadIdx.x == 0)
-    {
-        *out = op == 0 ? s : (op == 1 ? sqrt(s) : sqrt(dmax(s, 1e-300)));
-        *counter = 0;
-    }
-}
-
 // ---------------------------------------------------------------- one-time tables
 // cell-field coefficients of the constructor (:34-62): B_c = sum_k recon_k Phi_{f_k}
 __global__ void k_ind_recon(MeshView m, double *recon)
@@ -192,60 +127,10 @@ __global__ void k_to_float(const double *a, float *b, int64_t n)
     if (i < n) b[i] = static_cast<float>(a[i]);
 }
 
-// ---------------------------------------------------------------- operator
-// Input of a matvec: x_e directly (apply_A), or the preconditioned Krylov vector
-// x_e = (src_e / *hs) * pd_e with pd_e = dir_e ? 0 : 1 / (1 + dt m_e d2_e)  (:338)
-// The face pass gathers one edge vector: x itself, or zs = w_prev * pd (stored by the last
-// Gram-Schmidt pass of the previous step, FP32 for the FP32 operator) whose d1 it divides by *hs.
-struct MatIn
-{
-    const double *x = nullptr;
-    const double *src = nullptr, *hs = nullptr, *pd = nullptr;
-    const double *zs = nullptr;
-    const float *zs32 = nullptr;
-};
-
-// Phi' = d1 x on every face (:185-190), with star2 Phi' for the resistive current flux (:131-136).
-// FP64 sums in both precisions; the FP32 operator stores the rounded results.
-template <class T>
-__global__ void k_ind_face(MeshView m, Gate gt, MatIn in, int hall, int resistive, T *__restrict__ phi, T *__restrict__ s2phi)
-{
-    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
-    if (f >= m.nf || gt.off()) return;
-    double s = 0;
-    const int32_t k0 = m.f2e_ptr[f], k1 = m.f2e_ptr[f + 1];
-    if (in.zs32)
-        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * static_cast<double>(in.zs32[m.f2e_idx[k]]);
-    else if (in.zs)
-        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.zs[m.f2e_idx[k]];
-    else
-        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.x[m.f2e_idx[k]];
-    if ((in.zs || in.zs32) && in.hs) s = s / *in.hs;
-    if (hall) phi[f] = static_cast<T>(s);
-    if (resistive) s2phi[f] = static_cast<T>(m.star2[f] * s);
-}
-
 __global__ void k_ind_s2phi(MeshView m, const double *__restrict__ phi, double *__restrict__ s2phi)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f < m.nf) s2phi[f] = m.star2[f] * phi[f];
-}
-
-// cell field from the face fluxes (:139-149)
-template <class T>
-__global__ void k_ind_bcell(MeshView m, Gate gt, const T *__restrict__ recon, const T *__restrict__ phi, T *__restrict__ b)
-{
-    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.nc || gt.off()) return;
-    T bx = 0, by = 0, bz = 0;
-    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
-    {
-        const T v = phi[m.c2f_idx[k]];
-        bx += recon[3 * (int64_t)k] * v;
-        by += recon[3 * (int64_t)k + 1] * v;
-        bz += recon[3 * (int64_t)k + 2] * v;
-    }
-    b[3 * (int64_t)c] = bx; b[3 * (int64_t)c + 1] = by; b[3 * (int64_t)c + 2] = bz;
 }
 
 // Hall EMF per owned cell (:159-178): J_c = (1/V) sum s A x 1/2 (b_c + b_nb), g_c = alpha_c J_c x B0_c.
@@ -273,108 +158,6 @@ __global__ void k_ind_hall(MeshView m, Gate gt, const int32_t *__restrict__ slot
     }
     const V3 J = (1.0 / m.cell_volume[c]) * sum;
     st3(g, c, alpha[c] * cross(J, ld3(B0, c)));
-}
-
-__global__ void k_ind_hall32(MeshView m, Gate gt, const float4 *__restrict__ slot32, const float *__restrict__ b,
-                             const float *__restrict__ alpha, const float *__restrict__ B0, const float *__restrict__ vinv,
-                             float *__restrict__ g)
-{
-    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= m.no_cells || gt.off()) return;
-    const float a = alpha[c];
-    if (a == 0.f || m.material[c] != 0)
-    {
-        g[3 * (int64_t)c] = g[3 * (int64_t)c + 1] = g[3 * (int64_t)c + 2] = 0.f;
-        return;
-    }
-    float sx = 0.f, sy = 0.f, sz = 0.f;
-    const float bcx = b[3 * (int64_t)c], bcy = b[3 * (int64_t)c + 1], bcz = b[3 * (int64_t)c + 2];
-    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
-    {
-        const float4 sl = slot32[k];
-        const int32_t o = __float_as_int(sl.w);
-        float bx = bcx, by = bcy, bz = bcz;
-        if (o >= 0)
-        {
-            bx = 0.5f * (bcx + b[3 * (int64_t)o]);
-            by = 0.5f * (bcy + b[3 * (int64_t)o + 1]);
-            bz = 0.5f * (bcz + b[3 * (int64_t)o + 2]);
-        }
-        const float ax = sl.x, ay = sl.y, az = sl.z;
-        sx += ay * bz - az * by;
-        sy += az * bx - ax * bz;
-        sz += ax * by - ay * bx;
-    }
-    const float iv = vinv[c];
-    const float Jx = iv * sx, Jy = iv * sy, Jz = iv * sz;
-    const float Bx = B0[3 * (int64_t)c], By = B0[3 * (int64_t)c + 1], Bz = B0[3 * (int64_t)c + 2];
-    g[3 * (int64_t)c] = a * (Jy * Bz - Jz * By);
-    g[3 * (int64_t)c + 1] = a * (Jz * Bx - Jx * Bz);
-    g[3 * (int64_t)c + 2] = a * (Jx * By - Jy * Bx);
-}
-
-template <class T> struct EdgeArgs
-{
-    int resistive = 0, hall = 0;
-    const T *s2phi = nullptr, *g = nullptr, *mcoef = nullptr, *ecw = nullptr, *tvec = nullptr;
-    MatIn in;                    // x of y = x + dt F; no input: y = F (apply_F)
-    double dt = 0;
-    const double *dtp = nullptr; // dt read from the cycle control instead
-    double *vout = nullptr;      // stores src / *hs (the lazily normalised Krylov vector V_j)
-    const int8_t *dir = nullptr; // zero y on Dirichlet edges (:339)
-    const double *v0 = nullptr;  // y . v0 over the owned edges, stored to *dot
-    double *part = nullptr, *dot = nullptr;
-    unsigned *counter = nullptr;
-    double *out = nullptr;
-    Gate gt;
-};
-
-// Per edge: part0 = sum_f s star2 Phi' (resistive, ascending faces), part1 = sum_c g_c . (w_ec t_e)
-// (Hall, ascending cells), F = m part0 + part1 + part2 (:176-182); y = F, or y = x + dt F (:191-197).
-template <class T>
-__global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
-{
-    if (a.gt.off()) return;
-    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
-    double contrib = 0.0;
-    if (e < m.ne)
-    {
-        T p0 = 0, p1 = 0;
-        if (a.resistive)
-            for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k) p0 += static_cast<T>(m.e2f_sgn[k]) * a.s2phi[m.e2f_idx[k]];
-        if (a.hall)
-        {
-            const T tx = a.tvec[3 * (int64_t)e], ty = a.tvec[3 * (int64_t)e + 1], tz = a.tvec[3 * (int64_t)e + 2];
-            for (int32_t k = m.ec_ptr[e]; k < m.ec_ptr[e + 1]; ++k)
-            {
-                const int32_t c = m.ec_cell[k];
-                if (c >= m.no_cells) continue;
-                const T w = a.ecw[k];
-                const T wx = w * tx, wy = w * ty, wz = w * tz;
-                p1 += a.g[3 * (int64_t)c] * wx + a.g[3 * (int64_t)c + 1] * wy + a.g[3 * (int64_t)c + 2] * wz;
-            }
-        }
-        const T F = a.mcoef[e] * p0 + p1 + static_cast<T>(0);
-        double y = static_cast<double>(F);
-        if (a.in.src || a.in.x)
-        {
-            double xe;
-            if (a.in.src)
-            {
-                double v = a.in.src[e];
-                if (a.in.hs) v = v / *a.in.hs;
-                if (a.vout) a.vout[e] = v;
-                xe = v * a.in.pd[e];
-            }
-            else
-                xe = a.in.x[e];
-            y = xe + (a.dtp ? *a.dtp : a.dt) * static_cast<double>(F);
-        }
-        if (a.dir && a.dir[e]) y = 0.0;
-        a.out[e] = y;
-        if (a.v0 && e < m.no_edges) contrib = y * a.v0[e];
-    }
-    if (a.v0) grid_sum_tail(contrib, a.part, a.counter, 0, a.dot);
 }
 
 // ---------------------------------------------------------------- Krylov vectors (FP64)
@@ -430,6 +213,233 @@ __global__ void __launch_bounds__(256) k_mgs(Gate gt, double *__restrict__ w, co
     grid_sum_tail(s, part, counter, Vi ? 0 : 1, out);
 }
 
+// ---------------------------------------------------------------- classical Gram-Schmidt, twice if needed
+// The Arnoldi step orthogonalises w against V_0..V_j with classical Gram-Schmidt and one conditional
+// re-orthogonalisation (the "twice is enough" criterion: again only if |w'| < |w| / sqrt(2), Giraud,
+// Langou, Rozloznik, "The loss of orthogonality in the Gram-Schmidt orthogonalization process", Comput.
+// Math. Appl. 50, 2005), skipped when the dots of the first result against the basis, which the update
+// pass forms anyway, are already at round-off (|V^T w'| <= 1e-12 |w'|: the new vector is orthogonal to
+// working accuracy).  It spans the same space and produces the same Hessenberg column as the
+// reference's modified Gram-Schmidt (ImplicitInduction.cpp:340-345) up to rounding, in two or three
+// passes over the basis instead of j + 1: every pass reads w and V_0..V_j once and forms all its dot
+// products together.
+constexpr int kCgsMax = 31; // basis vectors one pass handles (restart <= 31); the 32nd partial is |w|^2
+
+// Warp reduce-scatter of 32 partial sums: afterwards lane l holds the warp's sum of acc[l] in acc[0].
+__device__ __forceinline__ double warp_reduce_scatter32(double (&acc)[32])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1)
+    {
+        const bool up = lane & o;
+#pragma unroll
+        for (int k = 0; k < o; ++k)
+        {
+            const double send = up ? acc[k] : acc[k + o];
+            const double keep = up ? acc[k + o] : acc[k];
+            acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    return acc[0];
+}
+
+// The 32 grid-wide sums whose warp sums lane l of every warp holds for index l: block partials, then the
+// last block to finish adds them (in a fixed order: deterministic) into out[0..31] and re-arms the counter.
+// Returns true in that last block (all of its threads), after out is written and visible to them.
+__device__ __forceinline__ bool grid_sum32(double v, double *part, unsigned *counter, double *out)
+{
+    __shared__ double sh[8][32];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    sh[wid][lane] = v;
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w][threadIdx.x];
+        part[(int64_t)blockIdx.x * 32 + threadIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    // every thread of the last block: value v = t % 32 over the blocks b = t / 32 (mod warps), four
+    // accumulators so that the loads overlap; then the warps' sums in warp order
+    {
+        const int k = threadIdx.x >> 5, nk = blockDim.x >> 5;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        unsigned b = k;
+        for (; b + 3u * nk < gridDim.x; b += 4u * nk)
+        {
+            a0 += __ldcg(part + (int64_t)b * 32 + lane);
+            a1 += __ldcg(part + (int64_t)(b + nk) * 32 + lane);
+            a2 += __ldcg(part + (int64_t)(b + 2 * nk) * 32 + lane);
+            a3 += __ldcg(part + (int64_t)(b + 3 * nk) * 32 + lane);
+        }
+        for (; b < gridDim.x; b += nk) a0 += __ldcg(part + (int64_t)b * 32 + lane);
+        sh[k][lane] = (a0 + a1) + (a2 + a3);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[w][threadIdx.x];
+        out[threadIdx.x] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0;
+    __syncthreads();
+    return true;
+}
+
+// The passes are instantiated for every number NV = j + 1 of basis vectors (1..31), so that a thread
+// holds exactly NV + 1 running sums and NV basis values, all loads are unconditional and the registers
+// (and so the resident warps) follow the column.  A thread adds its edges' products into its running
+// sums; the sums meet once, at the end, in the warp reduce-scatter and the grid tail.
+
+// Pass 1: h_i = V_i . w (i < NV) into H(i, j), and |w|^2 into red[32], over the owned edges.  red holds 96
+// doubles: [0, 31) the re-orthogonalisation dots, [32] |w|^2 before the update, [64, 96) the last pass's sums.
+template <int NV>
+__global__ void __launch_bounds__(256) k_cgs_dots(Gate gt, const double *__restrict__ w, const double *__restrict__ V, int64_t ldv,
+                                                   int32_t n_owned, double *part, unsigned *counter, double *red, double *H, int mcols)
+{
+    if (gt.off()) return;
+    constexpr int j = NV - 1;
+    double acc[NV + 1];
+#pragma unroll
+    for (int i = 0; i <= NV; ++i) acc[i] = 0.0;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_owned; e += (int64_t)gridDim.x * blockDim.x)
+    {
+        const double we = w[e];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) acc[i] += V[i * ldv + e] * we;
+        acc[NV] += we * we;
+    }
+    double p[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) p[i] = i < NV ? acc[i] : (i == 31 ? acc[NV] : 0.0);
+    if (!grid_sum32(warp_reduce_scatter32(p), part, counter, red + 64)) return;
+    if (threadIdx.x <= j) H[threadIdx.x * mcols + j] = red[64 + threadIdx.x];
+    if (threadIdx.x == 31) red[32] = red[64 + 31];
+}
+
+// Pass 2 (and 3): w -= sum_i c_i V_i on every edge, with c = H(:, j) (pass 2) or the re-orthogonalisation
+// dots red[0..j] (pass 3); the next face pass's input zs = w * pd; and over the owned edges the dots
+// s_i = V_i . w and |w|^2 of the result.  Pass 2 (reorth == 0) then decides: if the subtraction cancelled
+// (|w|^2 < |w_before|^2 / 2, red[32] holds |w_before|^2 from pass 1) and the remaining components along
+// the basis are above round-off (|s| > 1e-12 |w|), it leaves s in red[0..j] and raises ctl->reorth; else it
+// stores H(j+1, j) = |w|.  Pass 3 (reorth == 1) runs only when raised: it adds c to H(:, j), stores
+// H(j+1, j) = |w| and lowers the flag.
+template <int NV, bool F32>
+__global__ void __launch_bounds__(256) k_cgs_update(Gate gt, Ctl *ctl, int reorth, double *__restrict__ w, const double *__restrict__ V,
+                                                     int64_t ldv, int32_t n_all, int32_t n_owned, int reverse, double *part,
+                                                     unsigned *counter, double *red, double *H, int mcols, const double *__restrict__ pd,
+                                                     double *__restrict__ zs, float *__restrict__ zs32)
+{
+    if (gt.off() || (reorth && !ctl->reorth)) return;
+    constexpr int j = NV - 1;
+    __shared__ double csh[NV];
+    if (threadIdx.x < NV) csh[threadIdx.x] = reorth ? red[threadIdx.x] : H[threadIdx.x * mcols + j];
+    __syncthreads();
+    double c[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) c[i] = csh[i];
+    double acc[NV + 1];
+#pragma unroll
+    for (int i = 0; i <= NV; ++i) acc[i] = 0.0;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_all; t += (int64_t)gridDim.x * blockDim.x)
+    {
+        const int64_t e = reverse ? n_all - 1 - t : t;
+        double v[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) v[i] = V[i * ldv + e];
+        double we = w[e];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) we -= c[i] * v[i];
+        w[e] = we;
+        if (F32) zs32[e] = static_cast<float>(we * pd[e]);
+        else zs[e] = we * pd[e];
+        if (e < n_owned)
+        {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) acc[i] += v[i] * we;
+            acc[NV] += we * we;
+        }
+    }
+    double p[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) p[i] = i < NV ? acc[i] : (i == 31 ? acc[NV] : 0.0);
+    // the sums of s and |w|^2 go to red[64..95]; red[32] keeps |w_before|^2 of pass 1
+    const bool last = grid_sum32(warp_reduce_scatter32(p), part, counter, red + 64);
+    if (!last || threadIdx.x != 0) return;
+    const double nn = red[64 + 31];
+    double ss = 0.0;
+    for (int i = 0; i < NV; ++i) ss += red[64 + i] * red[64 + i];
+    if (!reorth && nn < 0.5 * red[32] && ss > 1e-24 * nn)
+    {
+        for (int i = 0; i < NV; ++i) red[i] = red[64 + i];
+        ctl->reorth = 1;
+        ++ctl->n_reorth;
+        return;
+    }
+    if (reorth)
+        for (int i = 0; i < NV; ++i) H[i * mcols + j] += c[i];
+    H[(j + 1) * mcols + j] = sqrt(nn);
+    ctl->reorth = 0;
+}
+
+// Launchers of the instances for NV = 1..31, and their grids (resident blocks on every SM)
+struct CgsArgs
+{
+    Gate gt;
+    Ctl *ctl;
+    double *w;
+    const double *V;
+    int64_t ldv;
+    int32_t n_all, n_owned;
+    double *part, *red, *H;
+    unsigned *counter;
+    int mcols;
+    const double *pd;
+    double *zs;
+    float *zs32;
+};
+template <int NV> void cgs_step(const CgsArgs &a, const int *grid, cudaStream_t s, int pass)
+{
+    if (pass == 0)
+        k_cgs_dots<NV><<<grid[0], 256, 0, s>>>(a.gt, a.w, a.V, a.ldv, a.n_owned, a.part, a.counter, a.red, a.H, a.mcols);
+    else if (a.zs32)
+        k_cgs_update<NV, true><<<grid[1], 256, 0, s>>>(a.gt, a.ctl, pass - 1, a.w, a.V, a.ldv, a.n_all, a.n_owned, pass == 1, a.part,
+                                                       a.counter, a.red, a.H, a.mcols, a.pd, nullptr, a.zs32);
+    else
+        k_cgs_update<NV, false><<<grid[1], 256, 0, s>>>(a.gt, a.ctl, pass - 1, a.w, a.V, a.ldv, a.n_all, a.n_owned, pass == 1, a.part,
+                                                        a.counter, a.red, a.H, a.mcols, a.pd, a.zs, nullptr);
+}
+template <int NV> void cgs_grids(int sms, int *grid)
+{
+    int per = 0;
+    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cgs_dots<NV>, 256, 0));
+    grid[0] = std::max(1, std::min(kRedBlocks, sms * std::max(per, 1)));
+    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cgs_update<NV, false>, 256, 0));
+    int per32 = 0;
+    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_cgs_update<NV, true>, 256, 0));
+    grid[1] = std::max(1, std::min(kRedBlocks, sms * std::max(std::min(per, per32), 1)));
+}
+using CgsStepFn = void (*)(const CgsArgs &, const int *, cudaStream_t, int);
+using CgsGridFn = void (*)(int, int *);
+template <int... N> constexpr std::array<CgsStepFn, sizeof...(N)> cgs_step_table(std::integer_sequence<int, N...>)
+{
+    return {cgs_step<N + 1>...};
+}
+template <int... N> constexpr std::array<CgsGridFn, sizeof...(N)> cgs_grid_table(std::integer_sequence<int, N...>)
+{
+    return {cgs_grids<N + 1>...};
+}
+const std::array<CgsStepFn, kCgsMax> kCgsStep = cgs_step_table(std::make_integer_sequence<int, kCgsMax>{});
+const std::array<CgsGridFn, kCgsMax> kCgsGrid = cgs_grid_table(std::make_integer_sequence<int, kCgsMax>{});
+
 __global__ void k_vec_x0(int32_t n, const double *Ee, const double *corr, const int8_t *dir, double *x0, double *delta)
 {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -473,6 +483,8 @@ __global__ void k_cycle_init(Ctl *ctl, int limit, double tol, double dt, double 
     ctl->done = 0;
     ctl->jend = 0;
     ctl->limit = limit;
+    ctl->reorth = 0;
+    ctl->n_reorth = 0;
     ctl->tol = tol;
     ctl->dt = dt;
     for (int i = 0; i < n; ++i) g[i] = 0.0;
@@ -513,7 +525,8 @@ __global__ void k_backsub(const Ctl *ctl, const double *H, int mcols, const doub
         for (int k = i + 1; k < j; ++k) s -= H[i * mcols + k] * y[k];
         y[i] = s / H[i * mcols + i];
     }
-    *jend_out = j;
+    jend_out[0] = j;
+    jend_out[1] = ctl->n_reorth;
 }
 
 // delta += dir ? 0 : (sum_i y_i V_i) / (1 + dt m d2)  (:355-364); z = x0 + delta for the true residual
@@ -544,63 +557,10 @@ __global__ void k_vec_final(int32_t n, const double *x0, const double *delta, co
 
 using namespace mhd;
 
-struct MhdInduction
-{
-    MhdMesh *mesh = nullptr;
-    MhdInductionParams p{};
-    bool resistive = false, hall = false, mixed = false, have_corr = false;
-    int edge_blocks = 0;
-    DBuf<double> mcoef, taper, alpha, B0, recon, d2, corr, phi, s2phi, bcell, g;
-    DBuf<double> V, w, z, r, b, x0, delta, Ax, pd, Fn, part, H, cs, sn, gv, yv, nrm, scal;
-    DBuf<float> recon32, m32, ecw32, tv32, vinv32, alpha32, B0_32, phi32, s2phi32, b32, g32, zs32;
-    DBuf<double> slot_sa, zs;
-    DBuf<int32_t> slot_nb;
-    DBuf<float4> slot32;
-    DBuf<int8_t> dirc;
-    DBuf<unsigned> counter;
-    DBuf<Ctl> ctl;
-    double *pinned = nullptr;
-    EventProfiler<KI_COUNT> prof;
-    int64_t launches = 0;
-    // one restart cycle (mr Arnoldi steps) captured as a CUDA graph on the first unprofiled solve
-    cudaGraphExec_t cycle = nullptr;
-    bool cycle_tried = false;
-    int64_t cycle_kernels = 0;
-    bool capturing = false;
-    ~MhdInduction()
-    {
-        if (cycle) cudaGraphExecDestroy(cycle);
-        if (pinned) cudaFreeHost(pinned);
-    }
-};
-
 namespace mhd
 {
 namespace
 {
-int g1(int64_t n) { return grid_for(n, 256); }
-
-// one launch of kernel class k on the handle's stream, counted and (when profiling, outside a graph
-// capture) timed
-#define IND_LAUNCH(I, k, s, ...)                                                                                         \
-    do                                                                                                                   \
-    {                                                                                                                    \
-        if (!(I)->capturing) (I)->prof.begin(k, s);                                                                      \
-        __VA_ARGS__;                                                                                                     \
-        if (!(I)->capturing) (I)->prof.end(k, s);                                                                        \
-        ++(I)->launches;                                                                                                 \
-    } while (0)
-
-struct Fused
-{
-    double *vout = nullptr;
-    const int8_t *dir = nullptr;
-    const double *v0 = nullptr;
-    double *dot = nullptr;
-    const double *dtp = nullptr;
-    Gate gt;
-};
-
 // y = F(phi) (no input in `in`, phi given) or y = A x; optional fused outputs as in EdgeArgs.
 void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, double *y, const Fused &fz = Fused{})
 {
@@ -629,29 +589,6 @@ void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, dou
     a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
     a.part = I->part.p; a.counter = I->counter.p; a.out = y;
     if (m.ne) IND_LAUNCH(I, KI_EDGE, s, k_ind_edge<double><<<I->edge_blocks, 256, 0, s>>>(m, a));
-}
-
-// the same Arnoldi matvec with the FP32 operator (mixed precision inner iterations)
-void op32(MhdInduction *I, const MatIn &in, double dt, double *y, const Fused &fz)
-{
-    const MeshView &m = I->mesh->v;
-    cudaStream_t s = I->mesh->stream;
-    if (m.nf)
-        IND_LAUNCH(I, KI_FACE, s, k_ind_face<float><<<g1(m.nf), 256, 0, s>>>(m, fz.gt, in, I->hall, I->resistive, I->phi32.p, I->s2phi32.p));
-    if (I->hall && m.nc)
-    {
-        IND_LAUNCH(I, KI_BCELL, s, k_ind_bcell<float><<<g1(m.nc), 256, 0, s>>>(m, fz.gt, I->recon32.p, I->phi32.p, I->b32.p));
-        if (m.no_cells)
-            IND_LAUNCH(I, KI_HALL, s,
-                       k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot32.p, I->b32.p, I->alpha32.p, I->B0_32.p, I->vinv32.p,
-                                                                   I->g32.p));
-    }
-    EdgeArgs<float> a;
-    a.resistive = I->resistive; a.hall = I->hall;
-    a.s2phi = I->s2phi32.p; a.g = I->g32.p; a.mcoef = I->m32.p; a.ecw = I->ecw32.p; a.tvec = I->tv32.p;
-    a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
-    a.part = I->part.p; a.counter = I->counter.p; a.out = y;
-    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, k_ind_edge<float><<<I->edge_blocks, 256, 0, s>>>(m, a));
 }
 
 void apply_plain(MhdInduction *I, const double *x, double dt, double *y)
@@ -692,12 +629,21 @@ void enqueue_cycle(MhdInduction *I)
         Fused fz;
         fz.vout = j == 0 ? nullptr : V + (int64_t)j * ne;
         fz.dir = I->dirc.p;
-        fz.v0 = V;
-        fz.dot = H + j;
+        const bool cgs = mr <= kCgsMax;
+        fz.v0 = cgs ? nullptr : V;
+        fz.dot = cgs ? nullptr : H + j;
         fz.dtp = &I->ctl.p->dt;
         fz.gt = gt;
         if (I->mixed) op32(I, in, 0.0, I->w.p, fz);
         else op64(I, in, nullptr, 0.0, I->w.p, fz);
+        if (cgs)
+        {
+            CgsArgs ca{gt, I->ctl.p, I->w.p, V, ne, ne, m.no_edges, I->part.p, I->red.p, H, I->counter.p, mr, I->pd.p,
+                       I->mixed ? nullptr : I->zs.p, I->mixed ? I->zs32.p : nullptr};
+            for (int pass = 0; pass < 3; ++pass) IND_LAUNCH(I, KI_MGS, s, kCgsStep[j](ca, I->cgs_grid + 2 * j, s, pass));
+            IND_LAUNCH(I, KI_SCALAR, s, k_givens<<<1, 1, 0, s>>>(I->ctl.p, H, mr, j, I->cs.p, I->sn.p, I->gv.p, I->nrm.p));
+            continue;
+        }
         for (int i = 1; i <= j + 1; ++i)
         {
             const bool last = i == j + 1; // the norm of w, and the next face pass's input w * pd
@@ -746,10 +692,10 @@ void build_cycle_graph(MhdInduction *I)
     I->cycle = exec;
 }
 
-void host_read2(MhdInduction *I, const double *dev)
+void host_read(MhdInduction *I, const double *dev, int n)
 {
     cudaStream_t s = I->mesh->stream;
-    MHD_CUDA(cudaMemcpyAsync(I->pinned, dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaMemcpyAsync(I->pinned, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     MHD_CUDA(cudaStreamSynchronize(s));
 }
 } // namespace
@@ -773,6 +719,13 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
         I->hall = p->hall && p->hall_coef > 0;
         I->mixed = p->precision == MHD_PREC_MIXED;
         I->edge_blocks = g1(m.ne);
+        {
+            int dev = 0, sms = 0, per = 0;
+            MHD_CUDA(cudaGetDevice(&dev));
+            MHD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+            (void)per;
+            for (int k = 0; k < kCgsMax; ++k) kCgsGrid[k](sms, I->cgs_grid + 2 * k);
+        }
         const size_t ne = m.ne, nf = m.nf, nc = m.nc;
         std::vector<double> mc(ne, 0.0);
         if (m_edge_host)
@@ -808,7 +761,8 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
         const int mr = I->p.restart;
         I->V.alloc((size_t)(mr + 1) * ne); I->w.alloc(ne); I->z.alloc(ne); I->r.alloc(ne); I->b.alloc(ne); I->x0.alloc(ne);
         I->delta.alloc(ne); I->Ax.alloc(ne); I->pd.alloc(ne); I->Fn.alloc(ne); I->dirc.alloc(ne);
-        I->part.alloc((size_t)std::max(kRedBlocks, I->edge_blocks));
+        I->part.alloc((size_t)std::max(32 * kRedBlocks, I->edge_blocks));
+        I->red.alloc(96);
         I->H.alloc((size_t)(mr + 1) * mr); I->cs.alloc(mr); I->sn.alloc(mr); I->gv.alloc(mr + 1); I->yv.alloc(mr);
         I->nrm.alloc(mr + 1); I->scal.alloc(8); I->counter.alloc(1); I->ctl.alloc(1);
         I->slot_nb.alloc(nnz_c); I->slot_sa.alloc(3 * (size_t)nnz_c);
@@ -912,6 +866,7 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         const int mr = I->p.restart;
         const int ge = g1(ne);
         if (!warm) I->have_corr = false;
+        I->last_reorth = 0;
         double *sc = I->scal.p; // [0] |b|  [1] beta  [2] steps of the last cycle
         IND_LAUNCH(I, KI_VECTOR, s, k_vec_x0<<<ge, 256, 0, s>>>(ne, Ee, I->have_corr ? I->corr.p : nullptr, dir, I->x0.p, I->delta.p));
         op64(I, MatIn{}, Phi, 0.0, I->Fn.p);                                                      // F(Phi^n)
@@ -922,7 +877,7 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         dev_dot(I, I->b.p, I->b.p, 2, sc + 0);
         dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
         MHD_LAUNCH_CHECK();
-        host_read2(I, sc + 0);
+        host_read(I, sc + 0, 2);
         const double bnorm = I->pinned[0];
         double beta = I->pinned[1];
         const double tol = I->p.rtol * bnorm;
@@ -950,9 +905,10 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
             IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
             dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
             MHD_LAUNCH_CHECK();
-            host_read2(I, sc + 1);
+            host_read(I, sc + 1, 3);
             beta = I->pinned[0];
             total += static_cast<int>(I->pinned[1]);
+            I->last_reorth += static_cast<int32_t>(I->pinned[2]);
         }
         IND_LAUNCH(I, KI_VECTOR, s, k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p));
         MHD_LAUNCH_CHECK();
@@ -988,6 +944,14 @@ int mhd_gpu_induction_profile_read(MhdInduction *I, int32_t max_kernels, char *n
             I->prof.read(k, ms_total[n], count[n]);
         }
         *n_out = n;
+    });
+}
+
+int mhd_gpu_induction_last_solve_stats(MhdInduction *I, int32_t *reorth_passes)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && reorth_passes, "null argument");
+        *reorth_passes = I->last_reorth;
     });
 }
 

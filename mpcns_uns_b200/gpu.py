@@ -113,6 +113,7 @@ _SIGS = {
     "mhd_gpu_induction_profile": ([vp, i32], ctypes.c_int),
     "mhd_gpu_induction_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+    "mhd_gpu_induction_last_solve_stats": ([vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_state_set_resistivity": ([vp, vp], ctypes.c_int),
     "mhd_gpu_compute_geometry": ([vp], ctypes.c_int),
     "mhd_gpu_fn_create": ([vp, vp, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
@@ -843,6 +844,12 @@ class DeviceInduction:
     def launches(self):
         v = i64()
         check(lib().mhd_gpu_induction_launches(self._h, ctypes.byref(v)))
+        return v.value
+
+    def reorth_passes(self):
+        """Gram-Schmidt second passes (re-orthogonalisations) of the last solve."""
+        v = i32()
+        check(lib().mhd_gpu_induction_last_solve_stats(self._h, ctypes.byref(v)))
         return v.value
 
 
