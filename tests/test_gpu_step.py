@@ -36,10 +36,11 @@ def ref_params(p):
     return rp
 
 
-def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None, wall=None):
+def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None, wall=None, ref_mesh=None):
     from mpcns_uns_b200 import gpu
     h = wl.mesh
-    r = ref_twin(h, tags).boundary(*bc)
+    r = (ref_mesh if ref_mesh is not None else ref_twin(h, tags)).boundary(*bc)
+    assert r.topology_hash() == h.topology_hash()
     dm = gpu.DeviceMesh(h)
     p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf,
                         **(params_kw or {}))
@@ -59,8 +60,12 @@ def run_pair(wl, tags, bc, nsteps, params_kw=None, use_cfl=True, fields=None, wa
         wkeep = (np.ascontiguousarray(wall[0], np.int32), np.ascontiguousarray(wall[1], np.float64))
         rp.n_wall, rp.wall_faces, rp.wall_prims = wkeep[0].size, wkeep[0].ctypes.data, wkeep[1].ctypes.data
     for k in range(nsteps):
-        if use_cfl and wl.n_species == 2:
+        if use_cfl and wl.n_species <= 2:
+            # mercury::local_time_step is the two-ion form; one ion is the same step with an empty second species
+            # (its sound speed is zero and its velocity term vanishes, so the first species sets every cell's step)
             W = [r.to_prim(u, wl.gamma) for u in U]
+            if wl.n_species == 1:
+                W.append(np.zeros_like(W[0]))
             Btot = r.cell_vector(Phi) + Badd
             dt_ref = r.local_time_step(wl.gamma, p.cfl, p.inver_MA2, p.rho_floor_dt, W[0], W[1], Btot)
             dt_gpu = st.cfl_dt()
@@ -162,4 +167,33 @@ def test_step_shell_ten_ions_wall_table():
     wl = workloads.ten_ion(4, 5)
     wall = workloads.wall_states(wl.mesh, [f[0] for f in wl.fs], wl.mass, seed=4)
     div = run_pair(wl, SHELL_TAGS, SHELL_BC, 3, use_cfl=False, wall=wall)
+    assert div < 1e-12
+
+
+def test_config1_box_twenty_cfl_steps():
+    """Config 1 itself: the unit cube of 16^3 hexahedra x 6 tetrahedra (24,576 cells), interior nodes jittered
+    +-0.15 h with seed 0, rho = 1, p = 0.1, u = (1, 0, 0) with 1% seeded noise, gamma = 5/3, B = d1 of 8 seeded
+    Fourier modes of amplitude 0.05 plus B0 = (0.1, 0.2, 0), outflow everywhere; the reference's limited
+    least-squares gradients with the Barth-Jespersen limiter (the only limiter the reference has), Rusanov
+    fluxes, UCT EMF and CT; 20 steps at CFL 0.4 (device CFL step equal to the reference's).  Every step agrees
+    to 1e-12 and div B stays at round-off."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.box(16)
+    assert wl.mesh.n_cells == 24576 and wl.cfl == 0.4 and wl.steps == 20
+    div = run_pair(wl, BOX_TAGS, ("outflow", {}, wl.u_inf), wl.steps, params_kw=dict(cfl=wl.cfl))
+    assert div < 1e-12
+
+
+def test_shell_two_ions_config2_construction_221k_cells():
+    """The config-2 construction at 6 x 16 x 16 x 24 x 6 (221,184 cells): two ions (H+, Na+ of mass 23 with the
+    seeded exosphere profile), inflow u = (-8, 0, 0), IMF and the offset dipole in the background flux, wall at
+    r = 1, the J x B force and the Strang-split exact gyration; 5 steps at the device's CFL 0.4 step.  The
+    reference side's mesh is built by the reference's own generator (the cubed sphere cut into tetrahedra by
+    its ComplexBuilder), which must be this mesh entity for entity (same topology hash)."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(16, 24, r_in=1.0, r_out=6.0, sources=True)
+    assert wl.mesh.n_cells == 221184
+    rm = ref.RefMesh.shell_tets(16, 24, 1.0, 6.0, wl.extra["stretch"])
+    div = run_pair(wl, SHELL_TAGS, SHELL_BC, 5, ref_mesh=rm,
+                   params_kw=dict(cfl=wl.cfl, lorentz=wl.lorentz, induce_coeff=wl.induce_coeff, inver_MA2=wl.inver_MA2))
     assert div < 1e-12
