@@ -199,6 +199,9 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *params, co
 int mhd_gpu_induction_destroy(MhdInduction *ind);
 /* ImplicitInduction::set_frozen_state (:105-111): B0 3 per cell, n_e,eff 1 per cell (device). */
 int mhd_gpu_induction_set_frozen(MhdInduction *ind, const double *B0, const double *ne_eff);
+/* The same frozen state with the Hall coefficient given per cell, alpha_c = taper_c hall_coef / n_e,eff,c
+ * (ImplicitInduction::alpha_, :110), for a caller that keeps its own taper (device arrays). */
+int mhd_gpu_induction_set_frozen_alpha(MhdInduction *ind, const double *B0, const double *alpha);
 /* ImplicitInduction::apply_F (:127-183) and apply_A (:185-198) in FP64 (device arrays). */
 int mhd_gpu_induction_apply_F(MhdInduction *ind, const double *phi, double *out);
 int mhd_gpu_induction_apply_A(MhdInduction *ind, const double *x, double dt, double *y);

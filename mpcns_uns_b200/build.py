@@ -79,6 +79,29 @@ def build_gpu(force: bool = False, extra: list[str] | None = None) -> str:
     return GPU_SO
 
 
+DROPIN_SO = os.path.join(LIBDIR, "libmhd_dropin.so")
+CUDA_LIB = os.environ.get("CUDA_LIB", "/usr/local/cuda/lib64")
+
+
+def build_dropin(reference_tree: str, force: bool = False) -> str | None:
+    """The drop-in library (csrc/dropin/dropin.cpp): the reference's own hot-path signatures over the C-ABI.
+    It compiles against the reference's headers, so it is built only where the reference tree is present
+    (the built library travels with the package).  MHD_MPI_INCLUDE names the directory of the mpi.h the
+    reference is built with; without it, the single-rank header of the checker build (oracle/ref), which is
+    what the reference in this repository is compiled against."""
+    if not os.path.isdir(os.path.join(reference_tree, "Common")):
+        return None
+    src = os.path.join(PKG, "csrc", "dropin", "dropin.cpp")
+    gpu = build_gpu(force)
+    if force or _stale(DROPIN_SO, [src, gpu] + glob.glob(os.path.join(INCLUDE, "*.h"))):
+        mpi_inc = os.environ.get("MHD_MPI_INCLUDE", os.path.join(ROOT, "oracle", "ref"))
+        inc = ["-I" + INCLUDE, "-I" + mpi_inc, "-I/usr/local/cuda/include"] + [
+            "-I" + os.path.join(reference_tree, d) for d in ("include", "src/uns", "Common", "MercuryUns")]
+        _run(["g++", "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", *inc, "-o", DROPIN_SO, src,
+              "-L" + LIBDIR, "-lmhd_gpu", "-L" + CUDA_LIB, "-lcudart", "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + CUDA_LIB])
+    return DROPIN_SO
+
+
 def build_all(force: bool = False) -> None:
     build_mesh(force)
     build_gpu(force)

@@ -833,6 +833,24 @@ int mhd_gpu_induction_set_frozen(MhdInduction *I, const double *B0, const double
     });
 }
 
+int mhd_gpu_induction_set_frozen_alpha(MhdInduction *I, const double *B0, const double *alpha)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && B0 && alpha, "null argument");
+        const MeshView &m = I->mesh->v;
+        cudaStream_t s = I->mesh->stream;
+        if (!m.nc) return;
+        MHD_CUDA(cudaMemcpyAsync(I->B0.p, B0, 3 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        MHD_CUDA(cudaMemcpyAsync(I->alpha.p, alpha, (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        if (I->mixed)
+        {
+            k_to_float<<<g1(3 * (int64_t)m.nc), 256, 0, s>>>(I->B0.p, I->B0_32.p, 3 * (int64_t)m.nc);
+            k_to_float<<<g1(m.nc), 256, 0, s>>>(I->alpha.p, I->alpha32.p, m.nc);
+        }
+        MHD_LAUNCH_CHECK();
+    });
+}
+
 int mhd_gpu_induction_apply_F(MhdInduction *I, const double *phi, double *out)
 {
     return guarded([&] {

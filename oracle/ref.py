@@ -50,6 +50,8 @@ def lib():
             ("ref_mesh_box", [i32, i32, i32, vp, vp], vp),
             ("ref_mesh_shell", [i32, i32, i32, dbl, dbl, dbl], vp),
             ("ref_mesh_shell_tets", [i32, i32, i32, dbl, dbl, dbl], vp),
+            ("ref_mesh_objects", [vp, vp], ctypes.c_int),
+            ("ref_ind_object", [vp], vp),
             ("ref_mesh_hanging_box", [i32, i32, i32, vp, vp, i32], vp),
             ("ref_mesh_free", [vp], None),
             ("ref_mesh_counts", [vp, vp], None),
@@ -212,6 +214,12 @@ class RefMesh:
 
     def topology_hash(self):
         return int(lib().ref_topology_hash(self._h))
+
+    def objects(self):
+        """Addresses of the reference objects (LocalMesh, Geometry, BoundaryInfo, Config, Stencil) of this mesh."""
+        out = (ctypes.c_void_p * 5)()
+        _check(lib().ref_mesh_objects(self._h, out))
+        return [out[i] for i in range(5)]
 
     def validate(self):
         o = np.zeros(5, np.int64)
@@ -401,6 +409,10 @@ class RefInduction:
     def set_m(self, m):
         m = np.ascontiguousarray(m, np.float64)
         lib().ref_ind_set_m(self._h, _p(m))
+
+    def object(self):
+        """Address of the reference's mhd::ImplicitInduction object."""
+        return lib().ref_ind_object(self._h)
 
     def array(self, name):
         n = lib().ref_ind_array(self._h, name.encode(), None)

@@ -533,6 +533,18 @@ struct RefInd
     RefInd(RefMesh *m) : mesh(m), ex(MPI_COMM_SELF, m->lm) {}
 };
 
+// The reference objects behind a RefMesh handle (LocalMesh, Geometry, BoundaryInfo, Config, Stencil), for
+// the drop-in test driver, which calls the reference's signatures on them: out[0..4].
+int ref_mesh_objects(void *h, void **out)
+{
+    RefMesh *r = static_cast<RefMesh *>(h);
+    return guarded([&] {
+        if (!r->have_bc) throw std::runtime_error("boundary classification not built");
+        ensure_stencil(r);
+        out[0] = &r->lm; out[1] = &r->geo; out[2] = &r->bc; out[3] = &r->cfg; out[4] = r->stencil.get();
+    });
+}
+
 // mhd::ImplicitInduction::ImplicitInduction (Common/induction/ImplicitInduction.cpp:10-103)
 void *ref_ind_create(void *h, const RefIndParams *p)
 {
@@ -554,6 +566,7 @@ void *ref_ind_create(void *h, const RefIndParams *p)
 }
 
 void ref_ind_free(void *h) { delete static_cast<RefInd *>(h); }
+void *ref_ind_object(void *h) { return static_cast<RefInd *>(h)->ind.get(); }
 
 // Per-edge resistive coefficient m_e (eta_e / star1_e) in place of the constructor's tanh window.
 void ref_ind_set_m(void *h, const double *m)
