@@ -21,7 +21,7 @@ on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, c
 --gmres-max-it iterations: seconds per solve in FP64 and mixed precision, per-kernel GB/s, and the
 reference's own solve on a bounded sample beside it.
 
-The "ten_ion" object (with --ten-ion, or alone with --ten-ion-only): the ten-ion shell r in
+The "ten_ion" object (left out with --no-ten-ion, alone with --ten-ion-only): the ten-ion shell r in
 [1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background field: mixed and FP64 steps and
 the mixed state's error after 50 steps.
 
@@ -642,7 +642,7 @@ def main():
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
     ap.add_argument("--no-adjoint", action="store_true")
-    ap.add_argument("--ten-ion", action="store_true", help="add the ten-ion shell (its 42.5M-cell mesh takes minutes to build)")
+    ap.add_argument("--no-ten-ion", action="store_true", help="leave out the ten-ion shell (config 5, 42.5M cells)")
     ap.add_argument("--ten-ion-only", action="store_true", help="run only the ten-ion section and print it as its own JSON line")
     ap.add_argument("--ten-ncube", type=int, default=96)
     ap.add_argument("--ten-nr", type=int, default=128)
@@ -840,7 +840,7 @@ def main():
     # the configuration sections run once, on a single-GPU run (under torchrun the replicas time the step only)
     if world > 1:
         args.no_gmres = args.no_adjoint = True
-        args.ten_ion = False
+        args.no_ten_ion = True
     if rank == 0 and not args.no_gmres:
         del st64, st32, st
         torch.cuda.empty_cache()
@@ -860,7 +860,7 @@ def main():
             torch.cuda.empty_cache()
         adj = bench_adjoint(args)
     ten = None
-    if rank == 0 and args.ten_ion:
+    if rank == 0 and not args.no_ten_ion:
         if args.no_gmres and args.no_adjoint:
             del st64, st32, st
         del dm

@@ -90,6 +90,31 @@ typedef struct MhdGeometryArgs {
 } MhdGeometryArgs;
 int mhd_gpu_compute_geometry(const MhdGeometryArgs *args);
 
+/* The tetrahedral cell complex of a hexahedral list on the device: every hexahedron (8 node ids in the
+ * reference's local corner order, corner i at (i&1, (i>>1)&1, (i>>2)&1)) cut into the 6 Kuhn tetrahedra of
+ * its body diagonal, numbered exactly as uns::ComplexBuilder numbers them when the tetrahedra are added in
+ * that order (src/uns/complex/ComplexBuilder.cpp:45-134: add_cell, tag_face, finish; the same complex and
+ * uns::topology_hash as the host library's mhdm_shell / mhdm_box with as_tets), with the upward
+ * incidences of CellComplex::build_up (n2e, e2f, f2c: rows in ascending order of their entries).
+ * tag_tri: 3 nodes per tagged triangle (any order), tag_id its tag; later tags of a face win.  Host
+ * inputs; the complex stays on the device until copied out.  Faces shared by more than two cells are
+ * rejected with MHD_EINVAL. */
+typedef struct MhdTetBuild MhdTetBuild;
+int mhd_gpu_tet_build(int32_t n_nodes, int64_t n_hex, const int32_t *hex8, const int32_t *hex_material, int32_t n_tags,
+                      const int32_t *tag_tri, const int32_t *tag_id, MhdTetBuild **out);
+/* counts[0..3] = nodes, edges, faces, cells */
+int mhd_gpu_tet_build_counts(const MhdTetBuild *b, int64_t *counts);
+/* Host outputs (any may be NULL: skipped), tables in the order e2n, f2e, c2f, n2e, e2f, f2c: ptr rows + 1
+ * entries, idx and sgn one per incidence; cell_material per cell, face_tag per face. */
+typedef struct MhdComplexOut {
+    int64_t *ptr[6];
+    int32_t *idx[6];
+    int8_t *sgn[6];
+    int32_t *cell_material, *face_tag;
+} MhdComplexOut;
+int mhd_gpu_tet_build_copy(const MhdTetBuild *b, const MhdComplexOut *out);
+int mhd_gpu_tet_build_free(MhdTetBuild *b);
+
 /* Upload a mesh; replaces the reference's per-call use of LocalMesh + Geometry + BoundaryInfo
  * and the one-time setup of mhd::Stencil::Stencil (Common/fluid/Reconstruction.cpp:26-78). */
 int mhd_gpu_mesh_create(const MhdMeshDesc *desc, MhdMesh **out);

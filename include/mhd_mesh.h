@@ -48,6 +48,19 @@ int mhdm_box(int32_t nx, int32_t ny, int32_t nz, const double *lo, const double 
 int mhdm_shell(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch, int32_t as_tets,
                MhdHostMesh **out);
 
+/* The shell's hexahedral list alone, for a complex built elsewhere (mhd_gpu_tet_build): nodes and tag
+ * names as mhdm_shell makes them, and the arrays "hex" (8 nodes per hexahedron, the reference's local
+ * corner order), "hex_material", "tag_tri" (3 nodes per tagged triangle of the tetrahedral split, in the
+ * order mhdm_shell tags them) and "tag_tri_id"; no complex yet (counts: nodes only). */
+int mhdm_shell_hexes(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch, MhdHostMesh **out);
+/* Size the complex of such a mesh (faces_per_cell entries per c2f row, edges_per_face per f2e row, 2 per
+ * e2n row; the upward tables likewise) for the caller to fill through mhdm_array_mut; drops the hexahedral
+ * list and any geometry or boundary classification. */
+int mhdm_reserve_complex(MhdHostMesh *m, int64_t n_edges, int64_t n_faces, int64_t n_cells, int32_t faces_per_cell,
+                         int32_t edges_per_face);
+/* mhdm_array with a writable pointer */
+void *mhdm_array_mut(MhdHostMesh *m, const char *name, int64_t *count);
+
 /* The same complex built again with its cells in the given order (new cell i = old cell order[i]):
  * faces and edges are numbered in creation order of the new cell sequence, tags and materials carried
  * over, geometry not computed.  With a locality order (HostMesh.locality_order: Morton order of the cell

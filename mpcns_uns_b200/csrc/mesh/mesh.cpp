@@ -391,6 +391,10 @@ struct HostMesh
     bool have_bc = false;
     std::vector<int8_t> face_kind, edge_mode;
 
+    // a hexahedral list before its complex is built elsewhere (mhdm_shell_hexes): 8 nodes per hexahedron,
+    // its material, and the tagged triangles of the tetrahedral split (3 nodes each) with their tag ids
+    std::vector<int32_t> hex8, hex_material, tag_tri, tag_tri_id;
+
     int32_t ne() const { return e2n.rows(); }
     int32_t nf() const { return f2e.rows(); }
     int32_t nc() const { return c2f.rows(); }
@@ -403,6 +407,24 @@ void finish_mesh(HostMesh &m, Builder &b)
     m.n2e = m.e2n.transpose(m.n_nodes);
     m.e2f = m.f2e.transpose(m.ne());
     m.f2c = m.c2f.transpose(m.nf());
+}
+
+// The two triangles of a tagged quad of the tetrahedral split: the quad is cut along its lattice diagonal,
+// from the AND to the OR of its 4 local corner indices; fn(tri nodes, tag) in the builder's tag order.
+template <class F> void split_tags(const HexList &h, F &&fn)
+{
+    for (const auto &t : h.tagged)
+    {
+        int lo = 7, hi = 0;
+        for (int q : t.local) { lo &= q; hi |= q; }
+        const auto &v = h.hex[t.cell];
+        for (int q : t.local)
+        {
+            if (q == lo || q == hi) continue;
+            const int32_t tri[3] = {v[lo], v[q], v[hi]};
+            fn(tri, t.tag);
+        }
+    }
 }
 
 // Cells of a hexahedral list: the hexahedron itself (reference ComplexBuilder::add_hex,
@@ -453,20 +475,10 @@ HostMesh build_hexes(HexList &&h, bool as_tets)
             b.add_cell(lp, sz, 4, h.material[c]);
         }
     }
-    for (const auto &t : h.tagged)
-    {
-        if (!as_tets) { b.tag_face(t.nodes.data(), 4, t.tag); continue; }
-        // the quad is cut along its lattice diagonal: local corners (AND, OR) of its 4 local indices
-        int lo = 7, hi = 0;
-        for (int q : t.local) { lo &= q; hi |= q; }
-        const auto &v = h.hex[t.cell];
-        for (int q : t.local)
-        {
-            if (q == lo || q == hi) continue;
-            const int32_t tri[3] = {v[lo], v[q], v[hi]};
-            b.tag_face(tri, 3, t.tag);
-        }
-    }
+    if (as_tets)
+        split_tags(h, [&](const int32_t *tri, int tag) { b.tag_face(tri, 3, tag); });
+    else
+        for (const auto &t : h.tagged) b.tag_face(t.nodes.data(), 4, t.tag);
     finish_mesh(m, b);
     return m;
 }
@@ -843,6 +855,56 @@ int mhdm_shell(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r
     });
 }
 
+int mhdm_shell_hexes(int32_t ncube, int32_t nr, int32_t n_solid, double r_in, double r_out, double r_stretch, MhdHostMesh **out)
+{
+    return guarded([&] {
+        if (ncube < 1 || nr < 1 || ncube > 4096 || nr > 65534) throw std::runtime_error("shell: bad resolution");
+        HexList h = make_shell(ncube, nr, n_solid, r_in, r_out, r_stretch);
+        auto *m = new MhdHostMesh;
+        m->n_nodes = static_cast<int32_t>(h.x.size());
+        m->x.resize(3 * h.x.size());
+        for (size_t i = 0; i < h.x.size(); ++i) { m->x[3 * i] = h.x[i].x; m->x[3 * i + 1] = h.x[i].y; m->x[3 * i + 2] = h.x[i].z; }
+        m->tag_names = h.tag_names;
+        m->hex8.resize(8 * h.hex.size());
+        for (size_t c = 0; c < h.hex.size(); ++c) std::copy(h.hex[c].begin(), h.hex[c].end(), m->hex8.begin() + 8 * c);
+        m->hex_material.assign(h.material.begin(), h.material.end());
+        split_tags(h, [&](const int32_t *tri, int tag) {
+            m->tag_tri.insert(m->tag_tri.end(), tri, tri + 3);
+            m->tag_tri_id.push_back(tag);
+        });
+        *out = m;
+    });
+}
+
+int mhdm_reserve_complex(MhdHostMesh *m, int64_t n_edges, int64_t n_faces, int64_t n_cells, int32_t faces_per_cell,
+                         int32_t edges_per_face)
+{
+    return guarded([&] {
+        if (!m || n_edges < 0 || n_faces < 0 || n_cells < 0 || n_edges > INT32_MAX || n_faces > INT32_MAX || n_cells > INT32_MAX)
+            throw std::runtime_error("bad argument");
+        auto size = [](Csr &t, int64_t rows, int64_t nnz) {
+            t.ptr.assign(static_cast<size_t>(rows) + 1, 0);
+            t.idx.assign(static_cast<size_t>(nnz), 0);
+            t.sgn.assign(static_cast<size_t>(nnz), 0);
+        };
+        const int64_t n_c2f = n_cells * faces_per_cell, n_f2e = n_faces * edges_per_face;
+        size(m->e2n, n_edges, 2 * n_edges); size(m->f2e, n_faces, n_f2e); size(m->c2f, n_cells, n_c2f);
+        size(m->n2e, m->n_nodes, 2 * n_edges); size(m->e2f, n_edges, n_f2e); size(m->f2c, n_faces, n_c2f);
+        m->cell_material.assign(static_cast<size_t>(n_cells), 0);
+        m->face_tag.assign(static_cast<size_t>(n_faces), 0);
+        std::vector<int32_t>().swap(m->hex8);
+        std::vector<int32_t>().swap(m->hex_material);
+        std::vector<int32_t>().swap(m->tag_tri);
+        std::vector<int32_t>().swap(m->tag_tri_id);
+        m->have_geo = m->have_bc = false;
+    });
+}
+
+void *mhdm_array_mut(MhdHostMesh *m, const char *name, int64_t *count)
+{
+    return const_cast<void *>(mhdm_array(m, name, count));
+}
+
 void mhdm_free(MhdHostMesh *m) { delete m; }
 
 void mhdm_counts(const MhdHostMesh *m, int32_t *counts)
@@ -926,6 +988,10 @@ const void *mhdm_array(const MhdHostMesh *m, const char *cname, int64_t *count)
         }
     }
     if (n == "x") return ret(m->x);
+    if (n == "hex") return ret(m->hex8);
+    if (n == "hex_material") return ret(m->hex_material);
+    if (n == "tag_tri") return ret(m->tag_tri);
+    if (n == "tag_tri_id") return ret(m->tag_tri_id);
     if (n == "cell_material") return ret(m->cell_material);
     if (n == "face_tag") return ret(m->face_tag);
     if (m->have_bc)

@@ -114,6 +114,10 @@ _SIGS = {
     "mhd_gpu_induction_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
     "mhd_gpu_induction_last_solve_stats": ([vp, ctypes.POINTER(i32)], ctypes.c_int),
+    "mhd_gpu_tet_build": ([i32, i64, vp, vp, i32, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
+    "mhd_gpu_tet_build_counts": ([vp, vp], ctypes.c_int),
+    "mhd_gpu_tet_build_copy": ([vp, vp], ctypes.c_int),
+    "mhd_gpu_tet_build_free": ([vp], ctypes.c_int),
     "mhd_gpu_state_set_resistivity": ([vp, vp], ctypes.c_int),
     "mhd_gpu_compute_geometry": ([vp], ctypes.c_int),
     "mhd_gpu_fn_create": ([vp, vp, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
@@ -851,6 +855,45 @@ class DeviceInduction:
         v = i32()
         check(lib().mhd_gpu_induction_last_solve_stats(self._h, ctypes.byref(v)))
         return v.value
+
+
+class ComplexOut(ctypes.Structure):
+    """MhdComplexOut of include/mhd_gpu.h: host outputs of the device tetrahedral builder."""
+    _fields_ = [("ptr", vp * 6), ("idx", vp * 6), ("sgn", vp * 6), ("cell_material", vp), ("face_tag", vp)]
+
+
+def build_tets(m):
+    """The tetrahedral complex of a HostMesh that holds a hexahedral list (mhdm_shell_hexes), numbered on the
+    device (mhd_gpu_tet_build) and installed in m: the complex of uns::ComplexBuilder fed the Kuhn tetrahedra."""
+    from . import mesh as _mesh
+    L = lib()
+    hexes = np.ascontiguousarray(m["hex"], np.int32)
+    mat = np.ascontiguousarray(m["hex_material"], np.int32)
+    tri = np.ascontiguousarray(m["tag_tri"], np.int32)
+    tid = np.ascontiguousarray(m["tag_tri_id"], np.int32)
+    b = vp()
+    check(L.mhd_gpu_tet_build(int(m.n_nodes), hexes.size // 8, hexes.ctypes.data_as(vp), mat.ctypes.data_as(vp), tid.size,
+                              tri.ctypes.data_as(vp), tid.ctypes.data_as(vp), ctypes.byref(b)))
+    try:
+        counts = np.zeros(4, np.int64)
+        check(L.mhd_gpu_tet_build_counts(b, counts.ctypes.data_as(vp)))
+        del hexes, mat, tri, tid
+        m._cache.clear()
+        ML = _mesh.lib()
+        _mesh._check(ML.mhdm_reserve_complex(m._h, int(counts[1]), int(counts[2]), int(counts[3]), 4, 3))
+        out = ComplexOut()
+
+        def arr(name):
+            n = i64()
+            return ML.mhdm_array_mut(m._h, name.encode(), ctypes.byref(n))
+        for k, t in enumerate(("e2n", "f2e", "c2f", "n2e", "e2f", "f2c")):
+            out.ptr[k], out.idx[k], out.sgn[k] = arr(t + "_ptr"), arr(t + "_idx"), arr(t + "_sgn")
+        out.cell_material, out.face_tag = arr("cell_material"), arr("face_tag")
+        check(L.mhd_gpu_tet_build_copy(b, ctypes.byref(out)))
+    finally:
+        L.mhd_gpu_tet_build_free(b)
+    m._recount()
+    return m
 
 
 def _read_profile(fn, h):

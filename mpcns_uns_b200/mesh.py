@@ -21,7 +21,8 @@ _lib = None
 INTERIOR, WALL, INFLOW, OUTFLOW, SKIP = 0, 1, 2, 3, 4
 
 _DT = {
-    "x": np.float64, "cell_material": np.int32, "face_tag": np.int32,
+    "x": np.float64, "cell_material": np.int32, "face_tag": np.int32, "hex": np.int32, "hex_material": np.int32,
+    "tag_tri": np.int32, "tag_tri_id": np.int32,
     "face_kind": np.int8, "edge_mode": np.int8, "ec_ptr": np.int64, "ec_cell": np.int32,
     "ec_misoriented": np.int32,
 }
@@ -47,6 +48,10 @@ def lib():
         L.mhdm_last_error.restype = ctypes.c_char_p
         L.mhdm_box.argtypes = [i32, i32, i32, vp, vp, i32, dbl, ctypes.c_uint64, ctypes.POINTER(vp)]
         L.mhdm_shell.argtypes = [i32, i32, i32, dbl, dbl, dbl, i32, ctypes.POINTER(vp)]
+        L.mhdm_shell_hexes.argtypes = [i32, i32, i32, dbl, dbl, dbl, ctypes.POINTER(vp)]
+        L.mhdm_reserve_complex.argtypes = [vp, i64, i64, i64, i32, i32]
+        L.mhdm_array_mut.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i64)]
+        L.mhdm_array_mut.restype = vp
         L.mhdm_from_cells.argtypes = [i32, vp, i32, vp, vp, vp, vp, i32, vp, vp, vp, i32, vp, ctypes.POINTER(vp)]
         L.mhdm_free.argtypes = [vp]
         L.mhdm_counts.argtypes = [vp, vp]
@@ -98,11 +103,27 @@ class HostMesh:
         return cls(out.value)
 
     @classmethod
-    def shell(cls, ncube, nr, r_in=1.0, r_out=10.0, r_stretch=1.0, n_solid=0, tets=False):
-        """uns::make_cubed_sphere_shell (src/uns/generate/CubedSphereMesh.cpp:12-83)."""
+    def shell(cls, ncube, nr, r_in=1.0, r_out=10.0, r_stretch=1.0, n_solid=0, tets=False, device_build=False):
+        """uns::make_cubed_sphere_shell (src/uns/generate/CubedSphereMesh.cpp:12-83).  device_build (with tets):
+        the hexahedral list on the host, the tetrahedral complex numbered on the GPU (mhd_gpu_tet_build: the same
+        complex, same topology hash, in a fraction of the time for large shells)."""
         out = ctypes.c_void_p()
+        if device_build:
+            if not tets:
+                raise ValueError("device_build builds the tetrahedral split")
+            _check(lib().mhdm_shell_hexes(ncube, nr, n_solid, float(r_in), float(r_out), float(r_stretch), ctypes.byref(out)))
+            m = cls(out.value)
+            from . import gpu
+            gpu.build_tets(m)
+            return m
         _check(lib().mhdm_shell(ncube, nr, n_solid, float(r_in), float(r_out), float(r_stretch), int(tets), ctypes.byref(out)))
         return cls(out.value)
+
+    def _recount(self):
+        c = np.zeros(4, np.int32)
+        lib().mhdm_counts(self._h, c.ctypes.data)
+        self.n_nodes, self.n_edges, self.n_faces, self.n_cells = (int(v) for v in c)
+        self._cache.clear()
 
     @classmethod
     def from_cells(cls, x, cells, material=None, tagged=(), tag_names=("",)):

@@ -48,12 +48,10 @@ def prims(U, gamma):
 
 
 def d1(mesh: HostMesh, A):
-    """(d1 A)_f = sum_e f2e[f,e] A_e."""
-    ptr, idx, sgn = mesh["f2e_ptr"], mesh["f2e_idx"], mesh["f2e_sgn"]
+    """(d1 A)_f = sum_e f2e[f,e] A_e, each row summed in f2e order."""
+    ptr, idx, sgn = np.asarray(mesh["f2e_ptr"]), np.asarray(mesh["f2e_idx"]), np.asarray(mesh["f2e_sgn"])
     rows = np.repeat(np.arange(mesh.n_faces), np.diff(ptr))
-    out = np.zeros(mesh.n_faces)
-    np.add.at(out, rows, sgn * np.asarray(A)[idx])
-    return out
+    return np.bincount(rows, weights=sgn * np.asarray(A)[idx], minlength=mesh.n_faces)
 
 
 def fourier_potential(mesh: HostMesh, seed, modes=8, amp=0.05, B0=(0.1, 0.2, 0.0)):
@@ -139,13 +137,21 @@ def shell_stretch(ncube, nr, r_in=1.0, r_out=6.0):
     return geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
 
 
-def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False,
-          device_geometry=False):
-    """device_geometry: compute the metric on the GPU (bit-identical, faster for large shells)."""
+def shell_mesh(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, u_inf=(-8.0, 0.0, 0.0), device_geometry=False):
+    """The shell workloads' mesh: cubed sphere, 6 tetrahedra per hexahedron, wall inside, far field outside.
+    device_geometry: number the complex and compute the metric on the GPU (bit-identical, much faster for
+    large shells)."""
     if stretch is None:
         stretch = shell_stretch(ncube, nr, r_in, r_out)
-    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry(device=device_geometry)
+    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True, device_build=device_geometry).compute_geometry(device=device_geometry)
     m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
+    return m, stretch
+
+
+def shell(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, seed=0, n_species=2, masses=None, u_inf=(-8.0, 0.0, 0.0), sources=False,
+          device_geometry=False):
+    """device_geometry: build the complex and compute the metric on the GPU (bit-identical, faster for large shells)."""
+    m, stretch = shell_mesh(ncube, nr, r_in, r_out, stretch, u_inf, device_geometry)
     return shell_state(m, f"shell6x{ncube}x{ncube}x{nr}x6", r_in, stretch, seed, n_species, masses, u_inf, sources)
 
 
@@ -225,9 +231,7 @@ def induction_case(ncube=48, nr=96, r_in=0.8, r_out=6.0, eta_inner=1.0, eta_oute
     on with the reference's radial taper; B0 = dipole of moment 1 at (0, 0, 0.2) plus the IMF (0, 0, -0.5) at the cell
     centres; n_e = 1 + U(0, 0.5) (seeded); Phi^n = d1 of 8 seeded Fourier modes of amplitude 0.05; E_expl = (-u x B0) . t
     at the edge midpoints; dt = dt_factor x the explicit whistler limit.  ncube = 48, nr = 96 is the 7.96M-cell case."""
-    stretch = geometric_stretch(nr, r_in, r_out, r_in * (np.pi / 2) / ncube)
-    m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True).compute_geometry(device=device_geometry)
-    m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
+    m, _ = shell_mesh(ncube, nr, r_in, r_out, None, u_inf, device_geometry)
     rng = np.random.default_rng(seed)
     r_e = np.linalg.norm(np.asarray(m["edge_mid"]), axis=1)
     m_edge = np.where(r_e < r_eta, eta_inner, eta_outer) / np.asarray(m["star1"])
@@ -329,7 +333,6 @@ def crustal_background(mesh: HostMesh, seed=0, n_dipoles=16, r_src=0.95, moment=
     rng = np.random.default_rng(seed)
     x = np.asarray(mesh["edge_mid"])
     t = np.asarray(mesh["edge_vec"])
-    a = np.zeros_like(x)
     sources = [((0.0, 0.0, 0.0), (0.0, 0.0, global_moment))]
     for _ in range(n_dipoles):
         d = rng.normal(size=3)
@@ -337,11 +340,40 @@ def crustal_background(mesh: HostMesh, seed=0, n_dipoles=16, r_src=0.95, moment=
         m = rng.normal(size=3)
         m *= moment * rng.uniform(0.5, 1.0) / np.linalg.norm(m)
         sources.append((tuple(pos), tuple(m)))
+    return np.asarray(mesh["face_area"]) @ np.asarray(B_imf, np.float64) + d1(mesh, _dipole_potential(x, t, sources, soft))
+
+
+def _dipole_potential(x, t, sources, soft):
+    """A_e = (sum over the point dipoles (c, m) of m x r / |r|_soft^3, r = x_e - c) . t_e, one elementwise
+    operation at a time in a fixed order, so that numpy and torch (on the GPU when there is one, for the
+    large meshes) give the same bits."""
+    try:
+        import torch
+        dev = "cuda" if torch.cuda.is_available() else None
+    except ImportError:
+        dev = None
+    if dev:
+        xp = torch.from_numpy(np.array(x, np.float64)).to(dev)
+        tp = torch.from_numpy(np.array(t, np.float64)).to(dev)
+        sqrt = torch.sqrt
+    else:
+        xp, tp, sqrt = np.asarray(x, np.float64), np.asarray(t, np.float64), np.sqrt
+    X, Y, Z = xp[:, 0], xp[:, 1], xp[:, 2]
+    ax = ay = az = 0.0
     for c, m in sources:
-        r = x - np.asarray(c, np.float64)
-        d2 = (r * r).sum(1) + soft * soft
-        a += np.cross(np.asarray(m, np.float64), r) / (d2 * np.sqrt(d2))[:, None]
-    return np.asarray(mesh["face_area"]) @ np.asarray(B_imf, np.float64) + d1(mesh, (a * t).sum(1))
+        rx, ry, rz = X - c[0], Y - c[1], Z - c[2]
+        d2 = rx * rx
+        d2 = d2 + ry * ry
+        d2 = d2 + rz * rz
+        d2 = d2 + soft * soft
+        inv = 1.0 / (d2 * sqrt(d2))
+        ax = ax + (m[1] * rz - m[2] * ry) * inv
+        ay = ay + (m[2] * rx - m[0] * rz) * inv
+        az = az + (m[0] * ry - m[1] * rx) * inv
+    A = ax * tp[:, 0]
+    A = A + ay * tp[:, 1]
+    A = A + az * tp[:, 2]
+    return A.cpu().numpy() if dev else A
 
 
 def ten_ion(ncube=96, nr=128, r_in=1.0, r_out=8.0, seed=0, device_geometry=False):
@@ -349,23 +381,33 @@ def ten_ion(ncube=96, nr=128, r_in=1.0, r_out=8.0, seed=0, device_geometry=False
     42.5M-cell case), ion masses 1, 2, 4, 12, 14, 16, 28, 30, 32, 44; H+ upstream density 1 and the others seeded
     log-uniform in [1e-4, 1] relative to it, each with the seeded exosphere profile of shell(); the crustal
     background field of crustal_background; wall inside, far field outside; no model sources."""
-    wl = shell(ncube, nr, r_in, r_out, seed=seed, n_species=10, masses=list(TEN_ION_MASSES), device_geometry=device_geometry)
+    m, stretch = shell_mesh(ncube, nr, r_in, r_out, device_geometry=device_geometry)
+    u_inf = (-8.0, 0.0, 0.0)
+    wl = Workload(name="", mesh=m, n_species=10, gamma=GAMMA, U=[], Phi=np.zeros(m.n_faces), PhiAdd=None, fs=[],
+                  mass=list(TEN_ION_MASSES), u_inf=u_inf, B_imf=(0.0, 0.0, -0.5), cfl=0.4, extra=dict(stretch=stretch))
     # upstream densities log-uniform in [1e-4, 1] relative to H+ (seeded); inside, the free stream enhanced by the
-    # seeded exosphere profile 1 + lognormal(0, 0.5) exp(-(r - r_in)/0.2); pressure 0.05 rho, flow u_inf
+    # seeded exosphere profile 1 + lognormal(0, 0.5) exp(-(r - r_in)/0.2); pressure 0.05 rho, flow u_inf.  The
+    # densities come from one seeded stream, the profiles from one child stream per species (SeedSequence.spawn),
+    # so the species are generated in parallel threads and the state does not depend on the thread count.
     rng = np.random.default_rng(seed + 3)
-    m = wl.mesh
+    rho0s = [1.0] + [10.0 ** rng.uniform(-4.0, 0.0) for _ in range(9)]
+    children = np.random.SeedSequence(seed + 4).spawn(10)
     r = np.linalg.norm(np.asarray(m["cell_center"]), axis=1)
+    prof = np.exp(-(r - r_in) / 0.2)
     nc = m.n_cells
-    U, fs = [], []
-    for s in range(10):
-        rho0 = 1.0 if s == 0 else 10.0 ** rng.uniform(-4.0, 0.0)
-        W = np.zeros((nc, 5))
-        W[:, 0] = rho0 if s == 0 else rho0 * (1.0 + rng.lognormal(0.0, 0.5, nc) * np.exp(-(r - r_in) / 0.2))
-        W[:, 1:4] = np.asarray(wl.u_inf)
+
+    def species(s):
+        rho0 = rho0s[s]
+        W = np.empty((nc, 5))
+        W[:, 0] = rho0 if s == 0 else rho0 * (1.0 + np.random.default_rng(children[s]).lognormal(0.0, 0.5, nc) * prof)
+        W[:, 1:4] = np.asarray(u_inf)
         W[:, 4] = 0.05 * W[:, 0]
-        U.append(to_cons(W, wl.gamma).ravel())
-        fs.append((rho0, *wl.u_inf, 0.05 * rho0))
-    wl.U, wl.fs = U, fs
+        return to_cons(W, GAMMA).ravel()
+
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max_workers=10) as ex:
+        U = list(ex.map(species, range(10)))
+    wl.U, wl.fs = U, [(rho0s[s], *u_inf, 0.05 * rho0s[s]) for s in range(10)]
     wl.PhiAdd = crustal_background(m, seed + 5)
     wl.name = f"shell6x{ncube}x{ncube}x{nr}x6_r{r_in:g}-{r_out:g}_10ions"
     wl.steps = 50
