@@ -919,6 +919,15 @@ __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int
     const int64_t n = m.nc;
     double r0[5], r1[5], u0[5], u1[5];
     const double *ub = Ub + (int64_t)s0 * 5 * n;
+    if (stage2)
+    {
+        // the step's opening state, read at the end of the second stage, on its way to L2 while the flux
+        // records are gathered
+        const double *un = Uo + (int64_t)s0 * 5 * n + c;
+#pragma unroll
+        for (int q = 0; q < 10; ++q)
+            if (q < 5 * ng) asm volatile("prefetch.global.L2 [%0];" ::"l"(un + q * n));
+    }
 #pragma unroll
     for (int q = 0; q < 5; ++q)
     {
