@@ -393,7 +393,8 @@ def bench_adjoint(args):
     seeded log-uniform per-cell resistivity 1e-4..1e-2), with respect to the resistivity and the inflow velocity:
     device time of the forward run (checkpoint every 8 steps), the adjoint sweep and the tangent-linear run; the
     adjoint against the tangent-linear run (dot products) and against central differences of the forward run
-    (which is bit-identical to the reference's step) along 16 seeded directions at h = 1e-6 and 1e-7."""
+    (which is bit-identical to the reference's step) along 16 seeded directions in (eta, u_inf) and 6 in eta at
+    h = 1e-6 and 1e-7, split by the forward run's switch log into switch-free and switch-crossing directions."""
     import torch
     from mpcns_uns_b200 import gpu, workloads
     t = time.time()
@@ -449,30 +450,38 @@ def bench_adjoint(args):
     prof = fn.profile_read()
     fn.profile(False)
     classes = {k: {"ms": v[0], "launches": v[1]} for k, v in prof.items() if v[1]}
+    # Central differences of the forward run (bit-identical to the reference's step; J summed in double-double,
+    # so that the difference of two runs is not limited by J's own ulp), split by the forward run's switch log
+    # into the directions along which the J(p + h d) and J(p - h d) runs made the same discrete choices
+    # everywhere (switch-free) and those that crossed a switch (limiter bound, Rusanov wave-speed side or sign,
+    # edge upwind cell or sign, floor), where J is only piecewise smooth.  Directions: --adj-fd-dirs with an
+    # eta and an inflow part, and 6 in eta alone (switch-free by construction without model sources).
     fd = {}
     dirs = [(rng.standard_normal(nc) * case.eta, rng.standard_normal(3) * np.linalg.norm(u0)) for _ in range(args.adj_fd_dirs)]
+    dirs += [(rng.standard_normal(nc) * case.eta, np.zeros(3)) for _ in range(6)]
+    fn.switch_log(True)
     for hh in (1e-6, 1e-7):
-        errs = []
+        rows = []
         for de, du in dirs:
             fn.set_params(eta=case.eta + hh * de, u_inf=u0 + hh * du)
-            Jp = fn.forward()
+            fn.forward()
+            Jp, sp = fn.last_J(), fn.switches()
             fn.set_params(eta=case.eta - hh * de, u_inf=u0 - hh * du)
-            Jm = fn.forward()
-            f = (Jp - Jm) / (2 * hh)
-            errs.append(abs(float(ge @ de + gu @ du) - f) / abs(f))
-        fd[f"h={hh:g}"] = {"max_rel_err": max(errs), "median_rel_err": float(np.median(errs)), "directions": len(errs)}
+            fn.forward()
+            Jm, sm = fn.last_J(), fn.switches()
+            f = fn.central_difference(Jp, Jm, hh)
+            rows.append((abs(float(ge @ de + gu @ du) - f) / abs(f), fn.switch_flips(sp, sm), bool(np.any(du))))
+        free = [r for r in rows if sum(r[1].values()) == 0]
+        cross = [r for r in rows if sum(r[1].values()) > 0]
+        fd[f"h={hh:g}"] = {
+            "switch_free": {"directions": len(free), "max_rel_err": max((r[0] for r in free), default=None),
+                            "with_inflow_part": sum(r[2] for r in free)},
+            "crossing": {"directions": len(cross), "max_rel_err": max((r[0] for r in cross), default=None),
+                         "median_rel_err": float(np.median([r[0] for r in cross])) if cross else None,
+                         "median_flips": {k: float(np.median([r[1][k] for r in cross])) for k in gpu.DeviceFunction.SWITCH_KINDS} if cross else None},
+            "per_direction": [{"rel_err": r[0], "flips": r[1], "inflow_part": r[2]} for r in rows]}
+    fn.switch_log(False)
     fn.set_params(eta=case.eta, u_inf=u0)
-    # the eta part alone is smooth (the resistive EMF is linear in eta): h = 1e-4 clears the round-off
-    errs = []
-    for de, _ in dirs[:4]:
-        fn.set_params(eta=case.eta + 1e-4 * de)
-        Jp = fn.forward()
-        fn.set_params(eta=case.eta - 1e-4 * de)
-        Jm = fn.forward()
-        f = (Jp - Jm) / 2e-4
-        errs.append(abs(float(ge @ de) - f) / abs(f))
-    fn.set_params(eta=case.eta)
-    fd["eta_only_h=1e-4"] = {"max_rel_err": max(errs), "directions": len(errs)}
     out = {"workload": wl.name, "cells": nc, "faces": h.n_faces, "edges": h.n_edges, "n_species": wl.n_species,
            "steps": case.n_steps, "checkpoint_every": case.checkpoint_every, "dt": dt, "J": J,
            "functional": "sum |B_tot|^2 V over the dayside cells with 1.2 <= r <= 1.6",
@@ -603,7 +612,10 @@ def summary(out):
         fd = d["fd"]
         sm["adjoint"] = {"fwd_s": _r(d["forward_s"]), "fwd_bwd_over_fwd": _r(d["forward_plus_backward_over_forward"]),
                          "dot": _r(d["dot_test_rel_err_max"], 2),
-                         "fd": {k: [_r(v.get("max_rel_err"), 2), _r(v.get("median_rel_err"), 2)] for k, v in fd.items()}}
+                         "fd": {k: {"free": [v["switch_free"]["directions"], _r(v["switch_free"]["max_rel_err"], 2)],
+                                    "crossing": [v["crossing"]["directions"], _r(v["crossing"]["max_rel_err"], 2),
+                                                 _r(v["crossing"]["median_rel_err"], 2)]} for k, v in fd.items()},
+                         "fd_cols": "free: directions, max rel err; crossing: directions, max, median rel err"}
     t = out.get("ten_ion")
     if t:
         sm["ten_ion"] = {"mixed_ms": _r(t["mixed"]["ms_per_step"]), "fp64_ms": _r(t["fp64"]["ms_per_step"]),

@@ -411,6 +411,10 @@ int mhd_gpu_fn_set_params(MhdFn *fn, const double *eta, const double *u_inf);
 int mhd_gpu_fn_reset(MhdFn *fn);
 /* J of the run; keeps the checkpoints and leaves the final state in the MhdState */
 int mhd_gpu_fn_forward(MhdFn *fn, double *J);
+/* The last J (of a forward or tangent run) as the double-double J_hi_lo[0] + J_hi_lo[1]: J is summed in
+ * double-double, so the difference of two runs' J is kept below J's own ulp (finite differences at small
+ * steps: (Jp_hi - Jm_hi) + (Jp_lo - Jm_lo)). */
+int mhd_gpu_fn_last_J(MhdFn *fn, double *J_hi_lo);
 /* dJ/deta (host, n_cells; may be NULL) and dJ/du_inf (3; may be NULL) by the adjoint sweep; needs a
  * forward run with the current parameters */
 int mhd_gpu_fn_backward(MhdFn *fn, double *grad_eta, double *grad_u);
@@ -430,6 +434,21 @@ int mhd_gpu_fn_stage_adjoint(MhdFn *fn, const double *U, const double *Phi, cons
  * adj_limited_gradients, adj_prim, adj_misc, tangent_steps), read as in mhd_gpu_state_profile_read. */
 int mhd_gpu_fn_profile(MhdFn *fn, int32_t enable);
 int mhd_gpu_fn_profile_read(MhdFn *fn, int32_t max_kernels, char *names, double *ms_total, int64_t *count, int32_t *n_out);
+/* Switch log of the forward run.  While enabled, every mhd_gpu_fn_forward clears and then fills, per
+ * entity, a running 32-bit hash of the discrete choices that the forward kernels make over all steps and
+ * stages, so that two runs (J at p + h d and at p - h d) can be compared entity by entity: an entry that
+ * differs is an entity where the run crossed a switch, where J is not differentiable along d.  Kinds:
+ *   0 limiter [(s*5 + q)*n_cells + c]: which term sets Barth-Jespersen psi (none, upper, lower, relative
+ *     bound, clamp at 0) with the neighbour and face slots of the extremes it uses;
+ *   1 flux [s*n_faces + f]: the side of the larger Rusanov wave speed, the sign of that side's normal
+ *     velocity (not recorded where the two face states are the same state, as on zero-gradient faces,
+ *     where the wave speed multiplies zero), and the face states' positivity fallbacks;
+ *   2 edge [n_edges]: per face of the edge the cell with the largest |u . m| and its sign, and whether the
+ *     2x2 upwind solve ran;
+ *   3 floor [s*n_cells + c]: the floor that the update applied (none, density, pressure).
+ * Disabling frees the tables.  _read copies one kind's table (n: its size) to the host. */
+int mhd_gpu_fn_switch_log(MhdFn *fn, int32_t enable);
+int mhd_gpu_fn_switch_read(MhdFn *fn, int32_t kind, uint32_t *out, int64_t n);
 
 /* Live per-kernel timing of the fused step (CUDA events recorded on the handle's stream around
  * every launch while enabled).  _read synchronises, returns per kernel class its name (32 chars

@@ -482,54 +482,80 @@ __global__ void k_m_to_eta(MeshView m, const double *__restrict__ lm, double *__
 
 // ================================================================ functional J = sum_mask |B_tot|^2 V
 // block partial sums (deterministic: a fixed grid, then k_sum_final adds the parts in order)
+// Knuth's TwoSum: s + e == a + b exactly (additions only, so contraction cannot alter it)
+__device__ __forceinline__ void two_sum(double a, double b, double &s, double &e)
+{
+    s = a + b;
+    const double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+
+// (hi, lo) += (bh, bl) in double-double, renormalised so that |lo| <= ulp(hi) / 2
+__device__ __forceinline__ void dd_add(double &hi, double &lo, double bh, double bl)
+{
+    double s, e;
+    two_sum(hi, bh, s, e);
+    e += lo + bl;
+    hi = s + e;
+    lo = e - (hi - s);
+}
+
+// J = sum over the marked cells of |B_tot|^2 V (and its tangent), the value summed in double-double: the
+// run's J differs from a neighbouring run's by far less than J's own ulp when the parameters move by 1e-6,
+// and the unevaluated sum hi + lo keeps that difference (part: per block hi, lo, tangent)
 __global__ void __launch_bounds__(256) k_J_partial(MeshView m, DCPtr phi, const double *__restrict__ Badd, const int8_t *__restrict__ mask,
                                                     double *__restrict__ part)
 {
-    double jv = 0, jd = 0;
+    double jh = 0, jl = 0, jd = 0;
     for (int32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < m.nc; c += gridDim.x * blockDim.x)
     {
         if (!mask[c]) continue;
         const DV3 b = cell_vector_d(m, phi, c);
         const DV3 bt = dmk(b.x + Badd[3 * (int64_t)c], b.y + Badd[3 * (int64_t)c + 1], b.z + Badd[3 * (int64_t)c + 2]);
         const Dual j = dot(bt, bt) * m.cell_volume[c];
-        jv += j.v;
+        dd_add(jh, jl, j.v, 0.0);
         jd += j.d;
     }
-    __shared__ double sh[2][8];
+    __shared__ double sh[3][8];
     for (int o = 16; o > 0; o >>= 1)
     {
-        jv += __shfl_down_sync(0xffffffffu, jv, o);
+        const double oh = __shfl_down_sync(0xffffffffu, jh, o), ol = __shfl_down_sync(0xffffffffu, jl, o);
+        dd_add(jh, jl, oh, ol);
         jd += __shfl_down_sync(0xffffffffu, jd, o);
     }
     if ((threadIdx.x & 31) == 0)
     {
-        sh[0][threadIdx.x >> 5] = jv;
-        sh[1][threadIdx.x >> 5] = jd;
+        sh[0][threadIdx.x >> 5] = jh;
+        sh[1][threadIdx.x >> 5] = jl;
+        sh[2][threadIdx.x >> 5] = jd;
     }
     __syncthreads();
     if (threadIdx.x == 0)
     {
-        double a = 0, b = 0;
+        double h = 0, l = 0, d = 0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
         {
-            a += sh[0][w];
-            b += sh[1][w];
+            dd_add(h, l, sh[0][w], sh[1][w]);
+            d += sh[2][w];
         }
-        part[2 * blockIdx.x] = a;
-        part[2 * blockIdx.x + 1] = b;
+        part[3 * blockIdx.x] = h;
+        part[3 * blockIdx.x + 1] = l;
+        part[3 * blockIdx.x + 2] = d;
     }
 }
 
+// out: J (hi), its tangent, J's low part
 __global__ void k_sum_final(const double *__restrict__ part, int nparts, double *__restrict__ out)
 {
-    double a = 0, b = 0;
+    double h = 0, l = 0, d = 0;
     for (int i = 0; i < nparts; ++i)
     {
-        a += part[2 * i];
-        b += part[2 * i + 1];
+        dd_add(h, l, part[3 * i], part[3 * i + 1]);
+        d += part[3 * i + 2];
     }
-    out[0] = a;
-    out[1] = b;
+    out[0] = h;
+    out[1] = d;
+    out[2] = l;
 }
 
 // dJ/dB_c = 2 V_c B_tot,c on the marked cells, into lB
@@ -1430,6 +1456,11 @@ struct MhdFn
     // tangent arrays
     DBuf<double> deta, dm, tU[3], dU[3], tP[3], dP[3], dW, dG, dF, dup, dbi, dbt, dEf, dE;
     bool forward_done = false;
+    double J_hi = 0.0, J_lo = 0.0; // the last J (forward or tangent run) as the double-double hi + lo
+    bool J_valid = false;
+    // switch log of the forward run (mhd_gpu_fn_switch_log): limiter, flux, edge and floor hashes
+    DBuf<uint32_t> sw[4];
+    bool sw_on = false;
     double *pinned = nullptr;
     ~MhdFn()
     {
@@ -1478,8 +1509,8 @@ void functional(MhdFn *fn, const double *phi, const double *dphi, double *J, dou
     MhdState *st = fn->st;
     const MeshView &m = st->mesh->v;
     cudaStream_t s = stream_of(fn);
-    fn->part.alloc(2 * kJBlocks);
-    fn->red.alloc(2);
+    fn->part.alloc(3 * kJBlocks);
+    fn->red.alloc(3);
     if (!dphi)
     {
         fn->phiscratch.alloc(m.nf);
@@ -1489,9 +1520,11 @@ void functional(MhdFn *fn, const double *phi, const double *dphi, double *J, dou
     k_J_partial<<<kJBlocks, 256, 0, s>>>(m, DCPtr{phi, dphi}, st->badd.p, fn->mask.p, fn->part.p);
     k_sum_final<<<1, 1, 0, s>>>(fn->part.p, kJBlocks, fn->red.p);
     MHD_LAUNCH_CHECK();
-    MHD_CUDA(cudaMemcpyAsync(fn->pinned, fn->red.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    MHD_CUDA(cudaMemcpyAsync(fn->pinned, fn->red.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
     MHD_CUDA(cudaStreamSynchronize(s));
-    *J = fn->pinned[0];
+    *J = fn->J_hi = fn->pinned[0];
+    fn->J_lo = fn->pinned[2];
+    fn->J_valid = true;
     if (dJ) *dJ = fn->pinned[1];
 }
 
@@ -1889,6 +1922,85 @@ int mhd_gpu_fn_reset(MhdFn *fn)
     });
 }
 
+namespace mhd
+{
+namespace
+{
+// The switch log's arrays on the state's kernels for the duration of one forward run: cleared first, taken
+// off the state again however the run ends (the backward sweep's recomputed segments are not logged).
+struct SwitchScope
+{
+    MhdFn *fn;
+    explicit SwitchScope(MhdFn *f) : fn(f)
+    {
+        if (!fn->sw_on) return;
+        MhdState *st = fn->st;
+        for (auto &b : fn->sw)
+            if (b.n) MHD_CUDA(cudaMemsetAsync(b.p, 0, b.n * sizeof(uint32_t), stream_of(fn)));
+        st->fp.sw_lim = fn->sw[0].p;
+        st->fp.sw_flux = fn->sw[1].p;
+        st->sw_edge = fn->sw[2].p;
+        st->fp.sw_floor = fn->sw[3].p;
+    }
+    ~SwitchScope()
+    {
+        MhdState *st = fn->st;
+        st->fp.sw_lim = st->fp.sw_flux = st->fp.sw_floor = nullptr;
+        st->sw_edge = nullptr;
+    }
+};
+
+size_t switch_size(const MhdFn *fn, int kind)
+{
+    const MeshView &m = fn->st->mesh->v;
+    const size_t ns = fn->nsp;
+    switch (kind)
+    {
+    case 0: return ns * 5 * m.nc;
+    case 1: return ns * m.nf;
+    case 2: return m.ne;
+    default: return ns * m.nc;
+    }
+}
+} // namespace
+} // namespace mhd
+
+int mhd_gpu_fn_switch_log(MhdFn *fn, int32_t enable)
+{
+    return guarded([&] {
+        MHD_REQUIRE(fn, "null function");
+        fn->sw_on = enable != 0;
+        for (int k = 0; k < 4; ++k)
+        {
+            if (fn->sw_on) fn->sw[k].alloc(switch_size(fn, k));
+            else fn->sw[k].release();
+        }
+    });
+}
+
+int mhd_gpu_fn_switch_read(MhdFn *fn, int32_t kind, uint32_t *out, int64_t n)
+{
+    return guarded([&] {
+        MHD_REQUIRE(fn && out, "null argument");
+        MHD_REQUIRE(fn->sw_on, "the switch log is off (mhd_gpu_fn_switch_log)");
+        MHD_REQUIRE(kind >= 0 && kind < 4, "kind: 0 limiter, 1 flux, 2 edge, 3 floor");
+        MHD_REQUIRE(n == (int64_t)switch_size(fn, kind), "n must be the size of the kind's table");
+        if (n)
+            MHD_CUDA(cudaMemcpyAsync(out, fn->sw[kind].p, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_of(fn)));
+        MHD_CUDA(cudaStreamSynchronize(stream_of(fn)));
+    });
+}
+
+int mhd_gpu_fn_last_J(MhdFn *fn, double *J_hi_lo)
+{
+    return guarded([&] {
+        MHD_REQUIRE(fn && J_hi_lo, "null argument");
+        MHD_REQUIRE(fn->J_valid, "no forward or tangent run yet");
+        J_hi_lo[0] = fn->J_hi;
+        J_hi_lo[1] = fn->J_lo;
+    });
+}
+
 int mhd_gpu_fn_forward(MhdFn *fn, double *J)
 {
     return guarded([&] {
@@ -1897,6 +2009,7 @@ int mhd_gpu_fn_forward(MhdFn *fn, double *J)
         const MeshView &m = st->mesh->v;
         cudaStream_t s = stream_of(fn);
         const size_t nU = 5 * (size_t)fn->nsp * m.nc, nf = m.nf;
+        const SwitchScope sw_scope(fn);
         apply_params(fn);
         set_dt(fn);
         initial_state(fn, st->U0.p, st->phi0.p, nullptr, nullptr);

@@ -43,6 +43,7 @@ __device__ __forceinline__ double ghost_component(int kind, bool absorb, int q, 
 // q of 32 consecutive cells.  Each variable's fit and limiter are independent of the others (wall
 // ghosts only read the velocity), so the per-thread state is small, occupancy high, and the five
 // warps share the cell's geometry through L1.  The reference's arithmetic order is kept per variable.
+template <bool LOG>
 __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidParams p, SField<const double> W, SField<double> G)
 {
     const int32_t c = blockIdx.x * 32 + threadIdx.x;
@@ -62,6 +63,7 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
     {
         const double wc = W(s, c, q);
         double lo = wc, hi = wc, r0 = 0, r1 = 0, r2 = 0;
+        int jlo = 7, jhi = 7, jpos = 7, jneg = 7; // switch log: the slots of the extremes
         for (int32_t k = k0; k < k1; ++k)
         {
             const int32_t nb = m.st_nb[k];
@@ -83,6 +85,8 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
             r0 += m.st_wd[3 * (int64_t)k] * dq;
             r1 += m.st_wd[3 * (int64_t)k + 1] * dq;
             r2 += m.st_wd[3 * (int64_t)k + 2] * dq;
+            if (LOG && wn < lo) jlo = k - k0;
+            if (LOG && hi < wn) jhi = k - k0;
             lo = dmin(lo, wn);
             hi = dmax(hi, wn);
         }
@@ -100,6 +104,8 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
             {
                 const V3 dx = ld3(m.face_center, m.c2f_idx[k]) - xc;
                 const double dl = g0 * dx.x + g1 * dx.y + g2 * dx.z;
+                if (LOG && dl > dpos) jpos = k - k0;
+                if (LOG && dl < dneg) jneg = k - k0;
                 if (dl > dpos) dpos = dl;
                 if (dl < dneg) dneg = dl;
             }
@@ -110,6 +116,9 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
                 const double a = dmax(dpos, -dneg);
                 if (a > 1e-300) psi = dmin(psi, p.rel_limit * wc / a);
             }
+            if (LOG)
+                sw_log(p.sw_lim, (s * 5 + q) * (int64_t)m.nc + c,
+                       limiter_code(psi, wc, lo, hi, dpos, dneg, jlo, jhi, jpos, jneg, p.rel_limit, p.rel_limit > 0 && (q == 0 || q == 4)));
         }
         const double ps = dmax(0.0, dmin(1.0, psi));
         G(s, c, 3 * q) = ps * g0;
@@ -122,6 +131,7 @@ __global__ void __launch_bounds__(160) k_limited_gradients_v(MeshView m, FluidPa
 // four slots unrolled at compile time so that every stencil load (coalesced structure-of-arrays
 // tables) and the twenty neighbour gathers are in flight together.  Per variable the arithmetic and
 // its order are those of the reference (slots and faces in c2f order).
+template <bool LOG>
 __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, FluidParams p, SField<const double> W, SField<double> G)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,6 +182,7 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
     for (int q = 0; q < 5; ++q)
     {
         double r0 = 0, r1 = 0, r2 = 0, lo = wc[q], hi = wc[q];
+        int jlo = 7, jhi = 7, jpos = 7, jneg = 7; // switch log: the slots of the extremes
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
@@ -180,6 +191,8 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
             r0 += wd[3 * j] * dq;
             r1 += wd[3 * j + 1] * dq;
             r2 += wd[3 * j + 2] * dq;
+            if (LOG && wn[j][q] < lo) jlo = j;
+            if (LOG && hi < wn[j][q]) jhi = j;
             lo = dmin(lo, wn[j][q]);
             hi = dmax(hi, wn[j][q]);
         }
@@ -196,6 +209,8 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
             for (int j = 0; j < 4; ++j)
             {
                 const double dl = g0 * dx[3 * j] + g1 * dx[3 * j + 1] + g2 * dx[3 * j + 2];
+                if (LOG && dl > dpos) jpos = j;
+                if (LOG && dl < dneg) jneg = j;
                 if (dl > dpos) dpos = dl;
                 if (dl < dneg) dneg = dl;
             }
@@ -206,6 +221,9 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
                 const double a = dmax(dpos, -dneg);
                 if (a > 1e-300) psi = dmin(psi, p.rel_limit * wc[q] / a);
             }
+            if (LOG)
+                sw_log(p.sw_lim, (s * 5 + q) * (int64_t)m.nc + c,
+                       limiter_code(psi, wc[q], lo, hi, dpos, dneg, jlo, jhi, jpos, jneg, p.rel_limit, p.rel_limit > 0 && (q == 0 || q == 4)));
         }
         const double ps = dmax(0.0, dmin(1.0, psi));
         G(s, c, 3 * q) = ps * g0;
@@ -217,6 +235,7 @@ __global__ void __launch_bounds__(128, 4) k_limited_gradients_tet(MeshView m, Fl
 // Face loop of mhd::fluid_flux_rhs (Common/fluid/FluxRHS.cpp:36-69): Rusanov flux of the
 // reconstructed face states times |A|, per face and species (SoA: F[(s*5 + m)*nf + f]).
 // Faces that the reference skips (Skip kind, no owned fluid cell) get zero.
+template <bool LOG>
 __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SField<const double> W, SField<const double> G,
                                                    double *__restrict__ F)
 {
@@ -262,19 +281,21 @@ __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SF
     {
         Prim5 L, R;
         double g[15];
-        auto state_of = [&](int32_t cc) {
+        uint32_t code = 0; // switch log: the face states' positivity fallbacks (bits 2, 3), Rusanov's choices
+        auto state_of = [&](int32_t cc, uint32_t bit) {
             const Prim5 w{W(s, cc, 0), W(s, cc, 1), W(s, cc, 2), W(s, cc, 3), W(s, cc, 4)};
             for (int q = 0; q < 15; ++q) g[q] = G(s, cc, q);
+            if (LOG && face_state_fallback(w, g, xf - ld3(m.cell_center, cc))) code |= bit;
             return face_state(w, g, xf - ld3(m.cell_center, cc));
         };
         if (interior)
         {
-            L = state_of(cL);
-            R = state_of(cR);
+            L = state_of(cL, 4u);
+            R = state_of(cR, 8u);
         }
         else
         {
-            const Prim5 in = state_of(c);
+            const Prim5 in = state_of(c, 4u);
             const double *wg = wall_ghost(p, kind, f, s);
             const Prim5 gh = wg ? Prim5{wg[0], wg[1], wg[2], wg[3], wg[4]} : ghost_state(kind, p.absorb[s] != 0, in, double(sgn) * n, p.fs[s]);
             if (sgn > 0) { L = in; R = gh; }
@@ -282,6 +303,9 @@ __global__ void __launch_bounds__(128) k_face_flux(MeshView m, FluidParams p, SF
         }
         double Fl[5];
         rusanov(L, R, n, p.gamma, Fl);
+        if (LOG)
+            sw_log(p.sw_flux, s * nf + f,
+                   code | rusanov_code(L, R, n, p.gamma, !interior && kind == 1 && !p.absorb[s] && !wall_ghost(p, kind, f, s)));
         for (int q = 0; q < 5; ++q) F[(s * 5 + q) * nf + f] = Fl[q] * A;
     }
 }
@@ -322,15 +346,17 @@ __global__ void k_gather_rhs(MeshView m, int nsp, const double *__restrict__ F, 
 void launch_limited_gradients(const MeshView &m, const FluidParams &p, SField<const double> W, SField<double> G, cudaStream_t s)
 {
     if (!m.nc) return;
-    if (m.faces_per_cell == 4) k_limited_gradients_tet<<<dim3(grid_for(m.nc, 128), p.nsp), 128, 0, s>>>(m, p, W, G);
-    else k_limited_gradients_v<<<grid_for(m.nc, 32), dim3(32, 5), 0, s>>>(m, p, W, G);
+    const bool log = p.sw_lim && p.limit;
+    if (m.faces_per_cell == 4)
+        (log ? k_limited_gradients_tet<true> : k_limited_gradients_tet<false>)<<<dim3(grid_for(m.nc, 128), p.nsp), 128, 0, s>>>(m, p, W, G);
+    else (log ? k_limited_gradients_v<true> : k_limited_gradients_v<false>)<<<grid_for(m.nc, 32), dim3(32, 5), 0, s>>>(m, p, W, G);
     MHD_LAUNCH_CHECK();
 }
 
 void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const double> W, SField<const double> G, double *F, cudaStream_t s)
 {
     if (!m.nf) return;
-    k_face_flux<<<dim3(grid_for(m.nf, 128), p.nsp), 128, 0, s>>>(m, p, W, G, F);
+    (p.sw_flux ? k_face_flux<true> : k_face_flux<false>)<<<dim3(grid_for(m.nf, 128), p.nsp), 128, 0, s>>>(m, p, W, G, F);
     MHD_LAUNCH_CHECK();
 }
 
@@ -442,7 +468,7 @@ int mhd_gpu_flux_rhs_wall(MhdMesh *mesh, double gamma, int32_t species, const Mh
         p.wall_prim = wall_prims;
         p.wall_n = n_wall;
         mesh->scratch_face.alloc(5 * static_cast<size_t>(m.nf));
-        k_face_flux<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
+        k_face_flux<false><<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
                                                                    SField<const double>{grad, 0, 15, 1}, mesh->scratch_face.p);
         MHD_LAUNCH_CHECK();
         k_gather_rhs<<<grid_for(m.nc, 256), 256, 0, mesh->stream>>>(m, 1, mesh->scratch_face.p, SField<double>{rhs, 0, 5, 1});
@@ -460,7 +486,7 @@ int mhd_gpu_flux_rhs(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim
         if (!m.nc) return;
         const FluidParams p = single_species(species, fs, gamma, 1, 0.0);
         mesh->scratch_face.alloc(5 * static_cast<size_t>(m.nf));
-        k_face_flux<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
+        k_face_flux<false><<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, p, SField<const double>{W, 0, 5, 1},
                                                                    SField<const double>{grad, 0, 15, 1}, mesh->scratch_face.p);
         MHD_LAUNCH_CHECK();
         k_gather_rhs<<<grid_for(m.nc, 256), 256, 0, mesh->stream>>>(m, 1, mesh->scratch_face.p, SField<double>{rhs, 0, 5, 1});

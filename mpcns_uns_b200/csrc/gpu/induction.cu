@@ -53,9 +53,11 @@ __global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const
 // Returns false for the edges the reference skips (no faces, zero length, no fluid cell).
 // MAXV bounds the faces per edge: the per-face values live in registers when the loops over
 // [0, MAXV) unroll (MAXV = 8 covers every tetrahedral split mesh), in local memory for MAXV = 32.
-template <int MAXV>
+// LOG: code receives the switch-log hash of the edge's choices: per face the slot of the cell with the
+// largest |u . m| and the sign of u . m there, and whether the 2x2 solve ran.
+template <int MAXV, bool LOG = false>
 __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const double *__restrict__ Ef, const double *__restrict__ u,
-                                         const double *__restrict__ phi_ind, double cuct, double &out)
+                                         const double *__restrict__ phi_ind, double cuct, double &out, uint32_t *code = nullptr)
 {
     const int32_t f0 = m.e2f_ptr[e], nf = m.e2f_ptr[e + 1] - f0;
     const double L = m.edge_len[e];
@@ -87,7 +89,24 @@ __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const dou
         const V3 mi = nv > 0 ? (1.0 / nv) * v : mk(0, 0, 0);
         const V3 nrm = (1.0 / m.face_area_mag[f]) * ld3(m.face_area, f);
         double a = 0;
-        for (int32_t k = q0; k < q1; ++k) a = dmax(a, fabs(dot(ld3(u, m.ec_cell[k]), mi)));
+        if (LOG)
+        {
+            int ka = 31;
+            bool neg = false;
+            for (int32_t k = q0; k < q1; ++k)
+            {
+                const double d = dot(ld3(u, m.ec_cell[k]), mi);
+                if (a < fabs(d))
+                {
+                    ka = k - q0;
+                    neg = d < 0;
+                }
+                a = dmax(a, fabs(d));
+            }
+            *code = sw_step(*code, uint32_t(ka & 31) | (neg ? 32u : 0u));
+        }
+        else
+            for (int32_t k = q0; k < q1; ++k) a = dmax(a, fabs(dot(ld3(u, m.ec_cell[k]), mi)));
         aef[i] = a;
         sg[i] = dot(th, cross(mi, nrm));
         const V3 qv = (a * sg[i]) * nrm;
@@ -103,6 +122,7 @@ __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const dou
     const double eps = 1e-14 * tr;
     const double det = (M11 + eps) * (M22 + eps) - M12 * M12;
     double l1 = 0, l2 = 0;
+    if (LOG) *code = sw_step(*code, tr > 0 && det > 0 ? 64u : 128u);
     if (tr > 0 && det > 0)
     {
         l1 = ((M22 + eps) * g1 - M12 * g2) / det;
@@ -136,10 +156,11 @@ __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__re
 // With mres, the explicit resistive EMF m_e (d1^T star2 Phi)_e is added on every owned edge: the resistive
 // part of ImplicitInduction::apply_F (ImplicitInduction.cpp:133-137) with its sum m p0 + p1 + p2 (:182), the
 // faces of an edge in ascending order (the e2f rows), as the reference's face loop scatters them.
-template <int MAXV>
+template <int MAXV, bool LOG>
 __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                           const double *__restrict__ phi_ind, double cuct, V3 E_inf,
-                                                          const double *__restrict__ mres, AmbArgs amb, double *__restrict__ E)
+                                                          const double *__restrict__ mres, AmbArgs amb, double *__restrict__ E,
+                                                          uint32_t *__restrict__ sw)
 {
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
@@ -152,7 +173,9 @@ __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const do
         else
         {
             double v;
-            if (edge_uct<MAXV>(m, e, Ef, u, phi_ind, cuct, v)) val += v;
+            uint32_t code = 0;
+            if (edge_uct<MAXV, LOG>(m, e, Ef, u, phi_ind, cuct, v, &code)) val += v;
+            if (LOG) sw_log(sw, e, code);
             // AmbipolarEMF::add (Ambipolar.cpp:69-87) after the ideal EMF; on wall and inflow edges the
             // reference overwrites it with the boundary value
             if (amb.on)
@@ -175,11 +198,15 @@ void launch_face_candidate(const MeshView &m, const double *u, const double *Bt,
 }
 
 void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
-                            double *E, cudaStream_t s, const double *mres, const AmbArgs &amb)
+                            double *E, cudaStream_t s, const double *mres, const AmbArgs &amb, uint32_t *sw)
 {
     if (!m.ne) return;
-    if (m.max_valence <= 8) k_edge_emf_assign<8><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E);
-    else k_edge_emf_assign<kMaxValence><<<grid_for(m.ne, 128), 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E);
+    const int g = grid_for(m.ne, 128);
+    if (m.max_valence <= 8)
+        (sw ? k_edge_emf_assign<8, true> : k_edge_emf_assign<8, false>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E, sw);
+    else
+        (sw ? k_edge_emf_assign<kMaxValence, true> : k_edge_emf_assign<kMaxValence, false>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf,
+                                                                                                           mres, amb, E, sw);
     MHD_LAUNCH_CHECK();
 }
 

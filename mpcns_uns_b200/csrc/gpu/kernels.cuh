@@ -14,7 +14,9 @@ void launch_face_candidate(const MeshView &m, const double *u, const double *Bt,
                            const double *phi_add, double *Ef, cudaStream_t s);
 // E = begin (0) + ideal UCT EMF of the owned edges, then the boundary edge values (wall 0, inflow E_inf . t);
 // mres (per edge, optional): plus the explicit resistive EMF m_e (d1^T star2 phi_ind)_e on the owned edges;
-// amb.on: minus the ambipolar EMF on the owned free edges
+// amb.on: minus the ambipolar EMF on the owned free edges; sw (per edge, optional): the switch log of the
+// upwind choices (per face of the edge the cell of the largest |u . m| and its sign, the 2x2 solve's branch)
 void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
-                            double *E, cudaStream_t s, const double *mres = nullptr, const AmbArgs &amb = AmbArgs{});
+                            double *E, cudaStream_t s, const double *mres = nullptr, const AmbArgs &amb = AmbArgs{},
+                            uint32_t *sw = nullptr);
 } // namespace mhd

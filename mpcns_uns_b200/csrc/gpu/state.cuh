@@ -56,6 +56,7 @@ struct MhdState
     mhd::DBuf<double> wall_prim;  // [species][slot][5]
     mhd::DBuf<double> mres; // explicit resistive EMF: m_e = eta_e / star1_e per edge (empty: off)
     int8_t *floor_flags = nullptr; // when set, the update records the floors it applied ([s*nc + c])
+    uint32_t *sw_edge = nullptr;   // switch log of the edge EMF (null: off), with fp.sw_lim, sw_flux, sw_floor
     mhd::DBuf<double> scal; // [0] dt
     mhd::DBuf<unsigned long long> dt_bits;
     mhd::DBuf<int> flag;

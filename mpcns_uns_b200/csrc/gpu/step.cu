@@ -219,6 +219,7 @@ __global__ void __launch_bounds__(128) k_update(MeshView m, FluidParams p, int s
                 which = 2;
             }
             if (fl) fl[(int64_t)s * m.nc + c] = which;
+            if (p.sw_floor) sw_log(p.sw_floor, (int64_t)s * m.nc + c, static_cast<uint32_t>(which));
         }
         if (stage2)
             for (int q = 0; q < 5; ++q) Uo(s, c, q) = 0.5 * (Uo(s, c, q) + u[q]);
@@ -348,6 +349,8 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
             gp.absorb[g] = st->fp.absorb[s0 + g];
         }
         if (gp.wall_prim) gp.wall_prim = st->fp.wall_prim + (int64_t)s0 * 5 * st->fp.wall_n;
+        if (gp.sw_lim) gp.sw_lim += (int64_t)s0 * 5 * nc;
+        if (gp.sw_flux) gp.sw_flux += (int64_t)s0 * m.nf;
         const SField<const double> Wg{st->W.p + (int64_t)s0 * 5 * nc, 5 * nc, 1, nc};
         const SField<double> Gg{st->grad.p, 15 * nc, 1, nc};
         P.begin(KP_GRAD, s);
@@ -384,7 +387,8 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     amb.W = st->W.p;
     amb.pn = st->pn.p;
     amb.pok = st->pok.p;
-    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s, st->mres.n ? st->mres.p : nullptr, amb);
+    launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s, st->mres.n ? st->mres.p : nullptr, amb,
+                           st->sw_edge);
     P.end(KP_EDGE_EMF, s);
     st->launches += (m.nf ? 1 : 0) + (m.ne ? 1 : 0);
     if (m.nf)

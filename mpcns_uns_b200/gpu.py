@@ -130,6 +130,9 @@ _SIGS = {
     "mhd_gpu_fn_stage_tangent": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_fn_stage_adjoint": ([vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_fn_profile": ([vp, i32], ctypes.c_int),
+    "mhd_gpu_fn_switch_log": ([vp, i32], ctypes.c_int),
+    "mhd_gpu_fn_last_J": ([vp, vp], ctypes.c_int),
+    "mhd_gpu_fn_switch_read": ([vp, i32, vp, ctypes.c_int64], ctypes.c_int),
     "mhd_gpu_fn_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
 }
 
@@ -727,6 +730,17 @@ class DeviceFunction:
         check(lib().mhd_gpu_fn_forward(self._h, ctypes.byref(J)))
         return J.value
 
+    def last_J(self):
+        """(hi, lo): the last run's J as a double-double, for differences finer than J's ulp."""
+        a = np.empty(2)
+        check(lib().mhd_gpu_fn_last_J(self._h, _vp(a)))
+        return float(a[0]), float(a[1])
+
+    @staticmethod
+    def central_difference(Jp, Jm, h):
+        """(J(p + h d) - J(p - h d)) / 2h from two last_J() pairs."""
+        return ((Jp[0] - Jm[0]) + (Jp[1] - Jm[1])) / (2 * h)
+
     def backward(self):
         """(dJ/deta per cell, dJ/du_inf (3,)) of the last forward run."""
         ge = np.empty(self.n_cells)
@@ -758,6 +772,28 @@ class DeviceFunction:
     def profile_read(self):
         """{kernel class: (summed ms, launches)} since the last read (synchronises)."""
         return _read_profile(lib().mhd_gpu_fn_profile_read, self._h)
+
+    SWITCH_KINDS = ("limiter", "flux", "edge", "floor")
+
+    def switch_log(self, enable=True):
+        """While enabled, each forward run leaves per entity a hash of the discrete choices it made
+        (mhd_gpu_fn_switch_log)."""
+        check(lib().mhd_gpu_fn_switch_log(self._h, int(bool(enable))))
+
+    def switches(self):
+        """{kind: uint32 hashes} of the last forward run (kinds: limiter, flux, edge, floor)."""
+        ns, nc, nf, ne = self.n_species, self.n_cells, self.n_faces, self.n_edges
+        out = {}
+        for k, (name, n) in enumerate(zip(self.SWITCH_KINDS, (ns * 5 * nc, ns * nf, ne, ns * nc))):
+            a = np.empty(n, np.uint32)
+            check(lib().mhd_gpu_fn_switch_read(self._h, k, _vp(a), n))
+            out[name] = a
+        return out
+
+    @staticmethod
+    def switch_flips(a, b):
+        """{kind: entities whose choices differ} between two switches() results."""
+        return {k: int(np.count_nonzero(a[k] != b[k])) for k in a}
 
     def stage_adjoint(self, U, Phi, lUt, lE):
         """Adjoints of one stage's inputs (U, Phi, eta, u_inf) from those of its U~ and E."""
