@@ -147,8 +147,11 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
 # DRAM traffic per launch (dram__bytes_read.sum + dram__bytes_write.sum) that one ncu capture measured
 # on the 6 x 32 x 32 x 48 x 6 shell of the same construction, with the entity count it scales with;
 # the bench line reports it scaled to its own workload (the traffic grows in proportion to that count).
-NCU_TRAFFIC = {("edge_emf", "mixed"): (513.56e6, "ne", 2082912), ("update", "mixed"): (680.87e6, "nc", 1769472),
-               ("limited_gradients", "mixed"): (620.48e6, "nc", 1769472)}
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch in the ncu capture of the 6x32x32x48x6 shell
+# (1,769,472 cells, 2,082,912 edges), scaled by the entity count the traffic grows with; the update's
+# captured launch is a stage-1 launch (the stage-2 launch also reads the step's opening state)
+NCU_TRAFFIC = {("edge_emf", "mixed"): (493.91e6, "ne", 2082912), ("update", "mixed"): (543.20e6, "nc", 1769472),
+               ("limited_gradients", "mixed"): (511.77e6, "nc", 1769472)}
 
 
 def ncu_traffic(kernel, precision, counts):
