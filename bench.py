@@ -133,10 +133,12 @@ def _algorithmic_bytes(k, c, nsp, group, precision="fp64"):
     if k == "update":
         g = group
         return (5 * g * nf + 12.5 * g * nc + nc) * p + c["c2f"] * 5 + nc * 4 + nc   # stage 1 / 2 averaged (U0 read in stage 2)
+    # face_candidate also writes phi_ind / |A| per face for the edge pass; edge_emf reads the per-(edge, slot)
+    # face geometry (m, n, sigma, w: 8 values per e2f entry) instead of the faces' centres and areas
     if k == "face_candidate":
-        return (9 * nc + 4 * nf + 2 * nf + 3 * nf) * p + c["f2c"] * 5 + nf * 4 + 2 * nf * 4
+        return (9 * nc + 4 * nf + 2 * nf + 3 * nf + nf) * p + c["f2c"] * 5 + nf * 4 + 2 * nf * 4
     if k == "edge_emf":
-        return (c["e2f"] + 7 * ne + 7 * nf + 3 * nf + nf + 3 * nc + ne) * p + c["e2f"] * 4 + ne * 8 + c["ec"] * 4 + nc + ne
+        return (8 * c["e2f"] + 4 * ne + 3 * nf + nf + 3 * nc + ne) * p + c["e2f"] * 4 + ne * 8 + c["ec"] * 4 + nc + ne
     if k == "ct":
         return (ne + 2.5 * nf) * p + c["f2e"] * 5 + nf * 4 + c["f2c"] * 4 + nf * 4
     if k == "cfl":

@@ -445,7 +445,8 @@ int mhd_gpu_fn_profile_read(MhdFn *fn, int32_t max_kernels, char *names, double 
  *     where the wave speed multiplies zero), and the face states' positivity fallbacks;
  *   2 edge [n_edges]: per face of the edge the cell with the largest |u . m| and its sign, and whether the
  *     2x2 upwind solve ran;
- *   3 floor [s*n_cells + c]: the floor that the update applied (none, density, pressure).
+ *   3 floor [s*n_cells + c]: the floor that the update applied (none, density, pressure);
+ *   4 face EMF [n_faces]: the face candidate's a_f, the side of the larger |u . n| and its sign.
  * Disabling frees the tables.  _read copies one kind's table (n: its size) to the host. */
 int mhd_gpu_fn_switch_log(MhdFn *fn, int32_t enable);
 int mhd_gpu_fn_switch_read(MhdFn *fn, int32_t kind, uint32_t *out, int64_t n);

@@ -1458,8 +1458,8 @@ struct MhdFn
     bool forward_done = false;
     double J_hi = 0.0, J_lo = 0.0; // the last J (forward or tangent run) as the double-double hi + lo
     bool J_valid = false;
-    // switch log of the forward run (mhd_gpu_fn_switch_log): limiter, flux, edge and floor hashes
-    DBuf<uint32_t> sw[4];
+    // switch log of the forward run (mhd_gpu_fn_switch_log): limiter, flux, edge, floor and face-EMF hashes
+    DBuf<uint32_t> sw[5];
     bool sw_on = false;
     double *pinned = nullptr;
     ~MhdFn()
@@ -1941,12 +1941,13 @@ struct SwitchScope
         st->fp.sw_flux = fn->sw[1].p;
         st->sw_edge = fn->sw[2].p;
         st->fp.sw_floor = fn->sw[3].p;
+        st->sw_face = fn->sw[4].p;
     }
     ~SwitchScope()
     {
         MhdState *st = fn->st;
         st->fp.sw_lim = st->fp.sw_flux = st->fp.sw_floor = nullptr;
-        st->sw_edge = nullptr;
+        st->sw_edge = st->sw_face = nullptr;
     }
 };
 
@@ -1959,6 +1960,7 @@ size_t switch_size(const MhdFn *fn, int kind)
     case 0: return ns * 5 * m.nc;
     case 1: return ns * m.nf;
     case 2: return m.ne;
+    case 4: return m.nf;
     default: return ns * m.nc;
     }
 }
@@ -1970,7 +1972,7 @@ int mhd_gpu_fn_switch_log(MhdFn *fn, int32_t enable)
     return guarded([&] {
         MHD_REQUIRE(fn, "null function");
         fn->sw_on = enable != 0;
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < 5; ++k)
         {
             if (fn->sw_on) fn->sw[k].alloc(switch_size(fn, k));
             else fn->sw[k].release();
@@ -1983,7 +1985,7 @@ int mhd_gpu_fn_switch_read(MhdFn *fn, int32_t kind, uint32_t *out, int64_t n)
     return guarded([&] {
         MHD_REQUIRE(fn && out, "null argument");
         MHD_REQUIRE(fn->sw_on, "the switch log is off (mhd_gpu_fn_switch_log)");
-        MHD_REQUIRE(kind >= 0 && kind < 4, "kind: 0 limiter, 1 flux, 2 edge, 3 floor");
+        MHD_REQUIRE(kind >= 0 && kind < 5, "kind: 0 limiter, 1 flux, 2 edge, 3 floor, 4 face EMF");
         MHD_REQUIRE(n == (int64_t)switch_size(fn, kind), "n must be the size of the kind's table");
         if (n)
             MHD_CUDA(cudaMemcpyAsync(out, fn->sw[kind].p, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_of(fn)));

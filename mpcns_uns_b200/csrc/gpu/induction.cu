@@ -21,12 +21,17 @@ __global__ void k_cell_vector(MeshView m, const double *__restrict__ flux, int32
 // Face candidate of mhd::add_ideal_emf (Common/induction/IdealEMF.cpp:32-55):
 // E_f = -n x [ 1/2 (F_L + F_R) - 1/2 a_f (B_R^ind - B_L^ind) ],  F_X = (u_X.n) B_X^tot - u_X B_n^tot
 // phi_add (optional): static background flux, phi_tot = phi + phi_add as in Solver::prepare (Solver.cpp:119)
+// pa (optional): phi_tot / |A| per face (phi_tot before phi_add is added: the induced flux that the edge pass
+// divides by |A|, the same quotient).  sw (optional): the switch log of the face's choice of a_f (which side's
+// |u . n| is the larger, and the sign of u . n there), one running hash per face.
 __global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const double *__restrict__ Bt, const double *__restrict__ Bi,
-                                 const double *__restrict__ phi_tot, const double *__restrict__ phi_add, double *__restrict__ Ef)
+                                 const double *__restrict__ phi_tot, const double *__restrict__ phi_add, double *__restrict__ Ef,
+                                 double *__restrict__ pa, uint32_t *__restrict__ sw)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf) return;
     const double A = m.face_area_mag[f];
+    if (pa) pa[f] = phi_tot[f] / A;
     const V3 n = (1.0 / A) * ld3(m.face_area, f);
     const double pt = phi_add ? phi_tot[f] + phi_add[f] : phi_tot[f];
     const double Bn = pt / A;
@@ -41,6 +46,12 @@ __global__ void k_face_candidate(MeshView m, const double *__restrict__ u, const
         const int32_t L = m.face_L[f], R = m.face_R[f];
         const double a = dmax(fabs(dot(ld3(u, L), n)), fabs(dot(ld3(u, R), n)));
         F = 0.5 * (flux(L) + flux(R)) - (0.5 * a) * (ld3(Bi, R) - ld3(Bi, L));
+        if (sw)
+        {
+            const double dL = dot(ld3(u, L), n), dR = dot(ld3(u, R), n);
+            const bool r = fabs(dL) < fabs(dR);
+            sw[f] = sw_step(sw[f], (r ? 1u : 0u) | ((r ? dR : dL) < 0.0 ? 2u : 0u));
+        }
     }
     else
         F = flux(m.f2c_idx[p0]);
@@ -141,6 +152,165 @@ __device__ __forceinline__ bool edge_uct(const MeshView &m, int32_t e, const dou
     return true;
 }
 
+// The geometry of edge_uct's face loop, once per (edge e, slot i < 8 of its e2f row), formed by the same
+// operations in the same order: the face's unit in-plane direction m away from the edge, its unit normal n,
+// sigma = t.(m x n) and the weight w_ef, component c (m.x m.y m.z n.x n.y n.z sigma w) of slot i at
+// geo[(8 * c + i) * ne + e], so that a warp's edges read each component of a slot as consecutive words.
+// Slots past an edge's row and edges that edge_uct skips (no faces, zero length, more than 8 faces) are
+// left unset and never read.
+constexpr int kGeoSlots = 8;
+__global__ void k_edge_face_geo(MeshView m, double *__restrict__ geo)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= m.ne) return;
+    const int32_t f0 = m.e2f_ptr[e], nf = m.e2f_ptr[e + 1] - f0;
+    const double L = m.edge_len[e];
+    if (nf == 0 || nf > kGeoSlots || L <= 0) return;
+    const int64_t ne = m.ne;
+    const V3 t = ld3(m.edge_vec, e);
+    const V3 th = (1.0 / L) * t;
+    const V3 mid = ld3(m.edge_mid, e);
+    for (int32_t i = 0; i < nf; ++i)
+    {
+        const int32_t f = m.e2f_idx[f0 + i];
+        V3 v = ld3(m.face_center, f) - mid;
+        v = v - dot(v, th) * th;
+        const double nv = sqrt(dot(v, v));
+        const V3 mi = nv > 0 ? (1.0 / nv) * v : mk(0, 0, 0);
+        const V3 nrm = (1.0 / m.face_area_mag[f]) * ld3(m.face_area, f);
+        const double c8[8] = {mi.x, mi.y, mi.z, nrm.x, nrm.y, nrm.z, dot(th, cross(mi, nrm)), m.ef_weight[f0 + i]};
+        for (int c = 0; c < 8; ++c) geo[(8 * c + i) * ne + e] = c8[c];
+    }
+}
+
+void build_edge_face_geo(const MeshView &m, double *geo, cudaStream_t s)
+{
+    if (!m.ne) return;
+    k_edge_face_geo<<<grid_for(m.ne, 128), 128, 0, s>>>(m, geo);
+    MHD_LAUNCH_CHECK();
+}
+
+// edge_uct from the per-slot geometry table, for edges of at most kGeoCells cells and kGeoSlots faces: the
+// cells' velocities are staged once in this thread's column of shared memory (su[(3 * k + a) * 128 + lane]),
+// and the face loop runs twice, the second pass forming each face's upwind terms again from the table instead of
+// holding them, so that no per-face array lives in registers.  Every value and every sum is formed by
+// the operations of edge_uct in its order: the results are the same bits.
+constexpr int kGeoCells = 8;
+// pa: phi_ind / |A| per face (k_face_candidate's pa)
+template <bool LOG>
+__device__ __forceinline__ bool edge_uct_geo(const MeshView &m, int32_t e, const double *__restrict__ Ef, const double *__restrict__ u,
+                                             const double *__restrict__ pa, double cuct, const double *__restrict__ geo,
+                                             double *__restrict__ su, double &out, uint32_t *code)
+{
+    const int32_t f0 = m.e2f_ptr[e], nf = m.e2f_ptr[e + 1] - f0;
+    const double L = m.edge_len[e];
+    if (nf == 0 || L <= 0) return false;
+    const int32_t q0 = m.ec_ptr[e], q1 = m.ec_ptr[e + 1];
+    bool any_fluid = false;
+    for (int32_t k = q0; k < q1 && !any_fluid; ++k) any_fluid = m.material[m.ec_cell[k]] == 0;
+    if (!any_fluid) return false;
+    const int nce = q1 - q0;
+    // unrolled over the bound so that every cell's id and velocity loads are in flight together
+#pragma unroll
+    for (int k = 0; k < kGeoCells; ++k)
+        if (k < nce)
+        {
+            const V3 uk = ld3(u, m.ec_cell[q0 + k]);
+            su[(3 * k) * 128] = uk.x;
+            su[(3 * k + 1) * 128] = uk.y;
+            su[(3 * k + 2) * 128] = uk.z;
+        }
+    const V3 t = ld3(m.edge_vec, e);
+    const V3 th = (1.0 / L) * t;
+    // plane basis (IdealEMF.cpp:14-20)
+    const V3 ax = fabs(th.x) < 0.9 ? mk(1, 0, 0) : mk(0, 1, 0);
+    V3 e1 = cross(th, ax);
+    e1 = (1.0 / sqrt(dot(e1, e1))) * e1;
+    const V3 e2 = cross(th, e1);
+    // the face's largest |u . m| over the edge's cells (and, logged, which cell and its sign)
+    auto a_ef = [&](V3 mi) {
+        double a = 0;
+        int ka = 31;
+        bool neg = false;
+#pragma unroll
+        for (int k = 0; k < kGeoCells; ++k)
+        {
+            if (k >= nce) break;
+            const double d = dot(mk(su[(3 * k) * 128], su[(3 * k + 1) * 128], su[(3 * k + 2) * 128]), mi);
+            if (LOG && a < fabs(d))
+            {
+                ka = k;
+                neg = d < 0;
+            }
+            a = dmax(a, fabs(d));
+        }
+        if (LOG) *code = sw_step(*code, uint32_t(ka & 31) | (neg ? 32u : 0u));
+        return a;
+    };
+    struct Face
+    {
+        V3 mi, nrm;
+        double sg, w;
+    };
+    const int64_t ne = m.ne;
+    auto face = [&](int32_t i) {
+        const double *g = geo + i * ne + e;
+        return Face{mk(g[0], g[8 * ne], g[16 * ne]), mk(g[24 * ne], g[32 * ne], g[40 * ne]), g[48 * ne], g[56 * ne]};
+    };
+    double Ec = 0, M11 = 0, M12 = 0, M22 = 0, g1 = 0, g2 = 0;
+    // the face ids of the row, loaded together
+    int32_t fid[kGeoSlots];
+#pragma unroll
+    for (int i = 0; i < kGeoSlots; ++i) fid[i] = i < nf ? m.e2f_idx[f0 + i] : 0;
+#pragma unroll
+    for (int32_t i = 0; i < kGeoSlots; ++i)
+    {
+        if (i >= nf) break;
+        const int32_t f = fid[i];
+        const Face F = face(i);
+        Ec += F.w * dot(ld3(Ef, f), t);
+        const double a = a_ef(F.mi);
+        const V3 qv = (a * F.sg) * F.nrm;
+        const double qa = dot(qv, e1), qb = dot(qv, e2);
+        M11 += F.w * qa * qa;
+        M12 += F.w * qa * qb;
+        M22 += F.w * qb * qb;
+        g1 += F.w * qa;
+        g2 += F.w * qb;
+    }
+    const double tr = M11 + M22;
+    const double eps = 1e-14 * tr;
+    const double det = (M11 + eps) * (M22 + eps) - M12 * M12;
+    double l1 = 0, l2 = 0;
+    if (LOG) *code = sw_step(*code, tr > 0 && det > 0 ? 64u : 128u);
+    if (tr > 0 && det > 0)
+    {
+        l1 = ((M22 + eps) * g1 - M12 * g2) / det;
+        l2 = ((M11 + eps) * g2 - M12 * g1) / det;
+    }
+    double Eu = 0;
+#pragma unroll
+    for (int32_t i = 0; i < kGeoSlots; ++i)
+    {
+        if (i >= nf) break;
+        const int32_t f = fid[i];
+        const Face F = face(i);
+        double a = 0;
+#pragma unroll
+        for (int k = 0; k < kGeoCells; ++k)
+        {
+            if (k >= nce) break;
+            a = dmax(a, fabs(dot(mk(su[(3 * k) * 128], su[(3 * k + 1) * 128], su[(3 * k + 2) * 128]), F.mi)));
+        }
+        const V3 qv = (a * F.sg) * F.nrm;
+        const double qa = dot(qv, e1), qb = dot(qv, e2);
+        const double omega = F.w * (1.0 - (qa * l1 + qb * l2));
+        Eu += omega * a * F.sg * pa[f];
+    }
+    out = Ec + 2.0 * cuct * L * Eu;
+    return true;
+}
+
 template <int MAXV>
 __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
                                                    const double *__restrict__ phi_ind, double cuct, double *__restrict__ E)
@@ -156,12 +326,15 @@ __global__ void __launch_bounds__(128) k_edge_uct(MeshView m, const double *__re
 // With mres, the explicit resistive EMF m_e (d1^T star2 Phi)_e is added on every owned edge: the resistive
 // part of ImplicitInduction::apply_F (ImplicitInduction.cpp:133-137) with its sum m p0 + p1 + p2 (:182), the
 // faces of an edge in ascending order (the e2f rows), as the reference's face loop scatters them.
-template <int MAXV, bool LOG>
-__global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
-                                                          const double *__restrict__ phi_ind, double cuct, V3 E_inf,
-                                                          const double *__restrict__ mres, AmbArgs amb, double *__restrict__ E,
-                                                          uint32_t *__restrict__ sw)
+// GEO: the UCT value from the per-entry geometry table (edge_uct_geo; edges of at most kGeoCells cells)
+template <int MAXV, bool LOG, bool GEO>
+__global__ void __launch_bounds__(128, GEO ? 6 : 4) k_edge_emf_assign(MeshView m, const double *__restrict__ Ef, const double *__restrict__ u,
+                                                                    const double *__restrict__ phi_ind, double cuct, V3 E_inf,
+                                                                    const double *__restrict__ mres, AmbArgs amb, double *__restrict__ E,
+                                                                    uint32_t *__restrict__ sw, const double *__restrict__ geo,
+                                                                    const double *__restrict__ pa)
 {
+    __shared__ double su[GEO ? 3 * kGeoCells * 128 : 1];
     const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= m.ne) return;
     double val = 0.0;
@@ -174,7 +347,10 @@ __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const do
         {
             double v;
             uint32_t code = 0;
-            if (edge_uct<MAXV, LOG>(m, e, Ef, u, phi_ind, cuct, v, &code)) val += v;
+            bool ok;
+            if constexpr (GEO) ok = edge_uct_geo<LOG>(m, e, Ef, u, pa, cuct, geo, su + threadIdx.x, v, &code);
+            else ok = edge_uct<MAXV, LOG>(m, e, Ef, u, phi_ind, cuct, v, &code);
+            if (ok) val += v;
             if (LOG) sw_log(sw, e, code);
             // AmbipolarEMF::add (Ambipolar.cpp:69-87) after the ideal EMF; on wall and inflow edges the
             // reference overwrites it with the boundary value
@@ -190,23 +366,29 @@ __global__ void __launch_bounds__(128, 4) k_edge_emf_assign(MeshView m, const do
 }
 
 void launch_face_candidate(const MeshView &m, const double *u, const double *Bt, const double *Bi, const double *phi_tot,
-                           const double *phi_add, double *Ef, cudaStream_t s)
+                           const double *phi_add, double *Ef, cudaStream_t s, double *pa, uint32_t *sw)
 {
     if (!m.nf) return;
-    k_face_candidate<<<grid_for(m.nf, 128), 128, 0, s>>>(m, u, Bt, Bi, phi_tot, phi_add, Ef);
+    k_face_candidate<<<grid_for(m.nf, 128), 128, 0, s>>>(m, u, Bt, Bi, phi_tot, phi_add, Ef, pa, sw);
     MHD_LAUNCH_CHECK();
 }
 
 void launch_edge_emf_assign(const MeshView &m, const double *Ef, const double *u, const double *phi_ind, double cuct, V3 E_inf,
-                            double *E, cudaStream_t s, const double *mres, const AmbArgs &amb, uint32_t *sw)
+                            double *E, cudaStream_t s, const double *mres, const AmbArgs &amb, uint32_t *sw, const double *geo,
+                            const double *pa)
 {
     if (!m.ne) return;
     const int g = grid_for(m.ne, 128);
-    if (m.max_valence <= 8)
-        (sw ? k_edge_emf_assign<8, true> : k_edge_emf_assign<8, false>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E, sw);
+    if (geo && pa && m.max_edge_cells <= kGeoCells && m.max_valence <= kGeoSlots)
+        (sw ? k_edge_emf_assign<8, true, true> : k_edge_emf_assign<8, false, true>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres,
+                                                                                                      amb, E, sw, geo, pa);
+    else if (m.max_valence <= 8)
+        (sw ? k_edge_emf_assign<8, true, false> : k_edge_emf_assign<8, false, false>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres,
+                                                                                                        amb, E, sw, nullptr, nullptr);
     else
-        (sw ? k_edge_emf_assign<kMaxValence, true> : k_edge_emf_assign<kMaxValence, false>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf,
-                                                                                                           mres, amb, E, sw);
+        (sw ? k_edge_emf_assign<kMaxValence, true, false>
+            : k_edge_emf_assign<kMaxValence, false, false>)<<<g, 128, 0, s>>>(m, Ef, u, phi_ind, cuct, E_inf, mres, amb, E, sw, nullptr,
+                                                                               nullptr);
     MHD_LAUNCH_CHECK();
 }
 
@@ -430,7 +612,8 @@ int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const do
         const MeshView &m = mesh->v;
         if (!m.nf) return;
         mesh->scratch_face3.alloc(3 * static_cast<size_t>(m.nf));
-        k_face_candidate<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, u, Bt, Bi, phi_tot, nullptr, mesh->scratch_face3.p);
+        k_face_candidate<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, u, Bt, Bi, phi_tot, nullptr, mesh->scratch_face3.p, nullptr,
+                                                                         nullptr);
         MHD_LAUNCH_CHECK();
         if (m.no_edges)
         {

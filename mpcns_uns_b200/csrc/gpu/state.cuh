@@ -57,6 +57,9 @@ struct MhdState
     mhd::DBuf<double> mres; // explicit resistive EMF: m_e = eta_e / star1_e per edge (empty: off)
     int8_t *floor_flags = nullptr; // when set, the update records the floors it applied ([s*nc + c])
     uint32_t *sw_edge = nullptr;   // switch log of the edge EMF (null: off), with fp.sw_lim, sw_flux, sw_floor
+    uint32_t *sw_face = nullptr;   // switch log of the face EMF candidates' a_f (null: off)
+    mhd::DBuf<double> efgeo;       // FP64 state: the UCT's per-(edge, slot) face geometry (build_edge_face_geo), or empty
+    mhd::DBuf<double> pa;          // with efgeo: the stage's phi_ind / |A| per face, left by the face-candidate pass
     mhd::DBuf<double> scal; // [0] dt
     mhd::DBuf<unsigned long long> dt_bits;
     mhd::DBuf<int> flag;

@@ -378,7 +378,8 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     const V3 ui = mk(st->prm.u_inf[0], st->prm.u_inf[1], st->prm.u_inf[2]), bi = mk(st->prm.B_imf[0], st->prm.B_imf[1], st->prm.B_imf[2]);
     const V3 Einf = -1.0 * cross(ui, bi);
     P.begin(KP_FACE_CAND, s);
-    launch_face_candidate(m, st->up.p, st->btot.p, st->bind.p, phis, st->phi_add.p, st->Ef.p, s);
+    launch_face_candidate(m, st->up.p, st->btot.p, st->bind.p, phis, st->phi_add.p, st->Ef.p, s, st->efgeo.n ? st->pa.p : nullptr,
+                          st->sw_face);
     P.end(KP_FACE_CAND, s);
     P.begin(KP_EDGE_EMF, s);
     AmbArgs amb;
@@ -388,7 +389,7 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
     amb.pn = st->pn.p;
     amb.pok = st->pok.p;
     launch_edge_emf_assign(m, st->Ef.p, st->up.p, phis, st->prm.cuct, Einf, st->E.p, s, st->mres.n ? st->mres.p : nullptr, amb,
-                           st->sw_edge);
+                           st->sw_edge, st->efgeo.n ? st->efgeo.p : nullptr, st->efgeo.n ? st->pa.p : nullptr);
     P.end(KP_EDGE_EMF, s);
     st->launches += (m.nf ? 1 : 0) + (m.ne ? 1 : 0);
     if (m.nf)
@@ -542,6 +543,20 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
             MHD_REQUIRE(m.faces_per_cell == 4 && m.tri_faces, "mixed precision needs a tetrahedral mesh");
             MHD_REQUIRE(m.max_valence <= 8 && m.max_edge_cells <= 8, "mixed precision needs edge valence <= 8");
             mixed_setup(st);
+        }
+        else
+        {
+            // the FP64 UCT's face geometry per (edge, slot) (512 bytes per edge), where the memory allows it:
+            // without it the edge pass forms the same values inline
+            const size_t n_geo = size_t(64) * ne;
+            size_t free_b = 0, total_b = 0;
+            MHD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            if (n_geo && m.max_edge_cells <= 8 && m.max_valence <= 8 && free_b > n_geo * sizeof(double) + (size_t(8) << 30))
+            {
+                st->efgeo.alloc(n_geo);
+                st->pa.alloc(nf);
+                build_edge_face_geo(m, st->efgeo.p, mesh->stream);
+            }
         }
         cudaStream_t s = mesh->stream;
         if (nc) MHD_CUDA(cudaMemsetAsync(st->U0.p, 0, 5 * nc * st->nsp * sizeof(double), s));

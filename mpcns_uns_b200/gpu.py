@@ -773,7 +773,7 @@ class DeviceFunction:
         """{kernel class: (summed ms, launches)} since the last read (synchronises)."""
         return _read_profile(lib().mhd_gpu_fn_profile_read, self._h)
 
-    SWITCH_KINDS = ("limiter", "flux", "edge", "floor")
+    SWITCH_KINDS = ("limiter", "flux", "edge", "floor", "face_emf")
 
     def switch_log(self, enable=True):
         """While enabled, each forward run leaves per entity a hash of the discrete choices it made
@@ -781,10 +781,10 @@ class DeviceFunction:
         check(lib().mhd_gpu_fn_switch_log(self._h, int(bool(enable))))
 
     def switches(self):
-        """{kind: uint32 hashes} of the last forward run (kinds: limiter, flux, edge, floor)."""
+        """{kind: uint32 hashes} of the last forward run (kinds: limiter, flux, edge, floor, face_emf)."""
         ns, nc, nf, ne = self.n_species, self.n_cells, self.n_faces, self.n_edges
         out = {}
-        for k, (name, n) in enumerate(zip(self.SWITCH_KINDS, (ns * 5 * nc, ns * nf, ne, ns * nc))):
+        for k, (name, n) in enumerate(zip(self.SWITCH_KINDS, (ns * 5 * nc, ns * nf, ne, ns * nc, nf))):
             a = np.empty(n, np.uint32)
             check(lib().mhd_gpu_fn_switch_read(self._h, k, _vp(a), n))
             out[name] = a

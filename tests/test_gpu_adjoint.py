@@ -268,14 +268,14 @@ def test_switch_log_is_silent_and_repeatable():
     b = fn.switches()
     assert J0 == J1 == J2 and fn.last_J() == hi0
     assert hi0[0] == J0 and abs(hi0[1]) <= 0.5 * np.spacing(J0)
-    assert fn.switch_flips(a, b) == {"limiter": 0, "flux": 0, "edge": 0, "floor": 0}
+    assert fn.switch_flips(a, b) == {"limiter": 0, "flux": 0, "edge": 0, "floor": 0, "face_emf": 0}
     assert all(int(np.count_nonzero(v)) > 0 for k, v in a.items() if k != "floor")
     u0 = np.asarray(case.wl.u_inf, np.float64)
     fn.set_params(u_inf=u0 * (1 + 1e-3))
     fn.forward()
     c = fn.switches()
     flips = fn.switch_flips(a, c)
-    assert flips["limiter"] > 0 and flips["flux"] > 0 and flips["edge"] > 0, flips
+    assert flips["limiter"] > 0 and flips["flux"] > 0 and flips["edge"] > 0 and flips["face_emf"] > 0, flips
     fn.switch_log(False)
     with pytest.raises(gpu.MhdError, match="switch log is off"):
         fn.switches()
