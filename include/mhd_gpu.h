@@ -90,6 +90,25 @@ typedef struct MhdGeometryArgs {
 } MhdGeometryArgs;
 int mhd_gpu_compute_geometry(const MhdGeometryArgs *args);
 
+/* mhd::BoundaryInfo::build (Common/boundary/BoundaryInfo.cpp:9-49) on the device: face kinds (0 Interior,
+ * 1 Wall, 2 Inflow, 3 Outflow, 4 Skip) and edge modes (0 free, 1 wall, 2 inflow) into the caller's host arrays,
+ * equal to the reference's.  The caller resolves its tag-name -> type map: tag_type[t] for the tag ids
+ * 0 < t < n_tags, type_none for tag 0 and ids out of range (the reference's empty name), each 1 wall,
+ * 2 inflow, 3 outflow, 5 farfield or 0 unknown (MHD_EINVAL if a boundary face has it, as the reference
+ * throws).  Every face has one or two cells. */
+typedef struct MhdBoundaryArgs {
+    int32_t n_edges, n_faces, n_cells, n_tags;
+    const int64_t *f2c_ptr; const int32_t *f2c_idx; const int8_t *f2c_sgn;
+    const int64_t *e2f_ptr; const int32_t *e2f_idx;
+    const int32_t *cell_material, *face_tag;
+    const double *face_area, *face_area_mag;
+    const int8_t *tag_type;
+    int8_t type_none, pad[7];
+    double u_inf[3];
+    int8_t *face_kind, *edge_mode;
+} MhdBoundaryArgs;
+int mhd_gpu_boundary(const MhdBoundaryArgs *args);
+
 /* The tetrahedral cell complex of a hexahedral list on the device: every hexahedron (8 node ids in the
  * reference's local corner order, corner i at (i&1, (i>>1)&1, (i>>2)&1)) cut into the 6 Kuhn tetrahedra of
  * its body diagonal, numbered exactly as uns::ComplexBuilder numbers them when the tetrahedra are added in

@@ -80,6 +80,13 @@ int mhdm_compute_geometry(MhdHostMesh *m);
  * "farfield"); u_inf decides farfield faces. */
 int mhdm_boundary(MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const char *const *tag_names,
                   const char *const *types, const double *u_inf);
+/* The per-tag-id boundary types that mhdm_boundary would apply (for mhd_gpu_boundary): tag_type[t] for the
+ * mesh's tag ids t < n_tags (cap entries available), type_none for tag 0 and unknown ids; codes 1 wall,
+ * 2 inflow, 3 outflow, 5 farfield, 0 unknown type name. */
+int mhdm_tag_types(const MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const char *const *tag_names,
+                   const char *const *types, int32_t cap, int8_t *tag_type, int8_t *type_none, int32_t *n_tags);
+/* Install a boundary classification computed elsewhere (face kinds and edge modes, one per face / edge). */
+int mhdm_set_boundary(MhdHostMesh *m, const int8_t *face_kind, const int8_t *edge_mode);
 
 /* Pointer to the named array and its element count (NULL / -1 if unknown or not computed).
  * Names: x, e2n_ptr/idx/sgn, f2e_*, c2f_*, e2f_*, f2c_*, cell_material, face_tag, edge_vec,

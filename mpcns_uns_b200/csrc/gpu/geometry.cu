@@ -358,6 +358,60 @@ template <class T> void down(T *host, const DBuf<T> &d, size_t n)
     if (host && n) MHD_CUDA(cudaMemcpy(host, d.p, n * sizeof(T), cudaMemcpyDeviceToHost));
 }
 
+// mhd::BoundaryInfo::build (Common/boundary/BoundaryInfo.cpp:9-49), face loop: the kind of every face from its
+// cells' materials, its tag's boundary type (type_of[tag] for 0 < tag < n_tags, else type_none: 1 wall,
+// 2 inflow, 3 outflow, 5 farfield, 0 unknown, which raises *err) and, on farfield faces, the side of u_inf.
+__global__ void k_bc_faces(int32_t nf, const int32_t *__restrict__ f2c_ptr, const int32_t *__restrict__ f2c_idx,
+                           const int8_t *__restrict__ f2c_sgn, const int32_t *__restrict__ material, const int32_t *__restrict__ face_tag,
+                           const double *__restrict__ face_area, const double *__restrict__ face_area_mag, int32_t n_tags,
+                           const int8_t *__restrict__ type_of, int8_t type_none, V3 u_inf, int8_t *__restrict__ kind, int *err)
+{
+    const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const int32_t b = f2c_ptr[f];
+    if (f2c_ptr[f + 1] - b == 2)
+    {
+        const bool s0 = material[f2c_idx[b]] == 1, s1 = material[f2c_idx[b + 1]] == 1;
+        kind[f] = (s0 && s1) ? 4 : (s0 || s1) ? 1 : 0;
+        return;
+    }
+    if (material[f2c_idx[b]] == 1)
+    {
+        kind[f] = 4;
+        return;
+    }
+    const int32_t tag = face_tag[f];
+    const int8_t type = tag > 0 && tag < n_tags ? type_of[tag] : type_none;
+    if (type == 1 || type == 2 || type == 3) kind[f] = type;
+    else if (type == 5)
+    {
+        const double sc = f2c_sgn[b] / face_area_mag[f];
+        const V3 n = sc * ld3(face_area, f);
+        kind[f] = dot(u_inf, n) < 0 ? 2 : 3;
+    }
+    else
+    {
+        kind[f] = 0;
+        atomicOr(err, 1);
+    }
+}
+
+// its edge loop: an edge of a wall face is a wall edge (1), else an edge of an inflow face an inflow edge (2)
+__global__ void k_bc_edges(int32_t ne, const int32_t *__restrict__ e2f_ptr, const int32_t *__restrict__ e2f_idx,
+                           const int8_t *__restrict__ kind, int8_t *__restrict__ mode)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    bool wall = false, inflow = false;
+    for (int32_t k = e2f_ptr[e]; k < e2f_ptr[e + 1]; ++k)
+    {
+        const int8_t fk = kind[e2f_idx[k]];
+        wall |= fk == 1;
+        inflow |= fk == 2;
+    }
+    mode[e] = wall ? 1 : inflow ? 2 : 0;
+}
+
 std::vector<int32_t> to32(const int64_t *p, int64_t n, const char *what)
 {
     MHD_REQUIRE(p, std::string("missing ") + what);
@@ -459,4 +513,42 @@ int mhd_gpu_compute_geometry(const MhdGeometryArgs *a)
     });
 }
 
+int mhd_gpu_boundary(const MhdBoundaryArgs *a)
+{
+    return guarded([&] {
+        MHD_REQUIRE(a && a->face_kind && a->edge_mode, "null argument");
+        MHD_REQUIRE(a->n_edges >= 0 && a->n_faces >= 0 && a->n_cells >= 0 && a->n_tags >= 0, "negative count");
+        MHD_REQUIRE(a->cell_material && a->face_tag && a->f2c_idx && a->f2c_sgn && a->e2f_idx && a->face_area && a->face_area_mag,
+                    "missing array");
+        MHD_REQUIRE(!a->n_tags || a->tag_type, "missing tag types");
+        const int64_t ne = a->n_edges, nf = a->n_faces, nc = a->n_cells;
+        const auto f2c = to32(a->f2c_ptr, nf, "f2c_ptr"), e2f = to32(a->e2f_ptr, ne, "e2f_ptr");
+        for (int64_t f = 0; f < nf; ++f)
+            MHD_REQUIRE(f2c[f + 1] - f2c[f] == 1 || f2c[f + 1] - f2c[f] == 2, "every face needs one or two cells");
+        for (int64_t k = 0; k < f2c[nf]; ++k) MHD_REQUIRE(a->f2c_idx[k] >= 0 && a->f2c_idx[k] < nc, "f2c_idx out of range");
+        for (int64_t k = 0; k < e2f[ne]; ++k) MHD_REQUIRE(a->e2f_idx[k] >= 0 && a->e2f_idx[k] < nf, "e2f_idx out of range");
+        DBuf<int32_t> f2cp, f2ci, e2fp, e2fi, mat, tag;
+        DBuf<int8_t> f2cs, types, kind, mode;
+        DBuf<double> area, mag;
+        DBuf<int> err;
+        f2cp.upload(f2c); e2fp.upload(e2f);
+        f2ci.upload(a->f2c_idx, f2c[nf]); f2cs.upload(a->f2c_sgn, f2c[nf]); e2fi.upload(a->e2f_idx, e2f[ne]);
+        mat.upload(a->cell_material, nc); tag.upload(a->face_tag, nf);
+        area.upload(a->face_area, 3 * nf); mag.upload(a->face_area_mag, nf);
+        types.upload(a->tag_type, a->n_tags);
+        kind.alloc(nf); mode.alloc(ne); err.alloc(1);
+        MHD_CUDA(cudaMemset(err.p, 0, sizeof(int)));
+        const V3 u = mk(a->u_inf[0], a->u_inf[1], a->u_inf[2]);
+        if (nf)
+            k_bc_faces<<<grid_for(nf, 256), 256>>>(a->n_faces, f2cp.p, f2ci.p, f2cs.p, mat.p, tag.p, area.p, mag.p, a->n_tags, types.p,
+                                                   a->type_none, u, kind.p, err.p);
+        if (ne) k_bc_edges<<<grid_for(ne, 256), 256>>>(a->n_edges, e2fp.p, e2fi.p, kind.p, mode.p);
+        MHD_LAUNCH_CHECK();
+        int e = 0;
+        MHD_CUDA(cudaMemcpy(&e, err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        MHD_REQUIRE(e == 0, "unknown boundary type for a face tag (wall|farfield|inflow|outflow)");
+        down(a->face_kind, kind, nf);
+        down(a->edge_mode, mode, ne);
+    });
+}
 } // extern "C"

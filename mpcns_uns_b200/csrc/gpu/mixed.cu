@@ -489,26 +489,25 @@ __device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int 
         // hi - w >= 0 >= lo - w the minimum is taken at the largest and at the most negative dl, so two
         // quotients per variable instead of four (likewise one for the relative limiter, at the largest |dl|)
         float dpos = 0.f, dneg = 0.f;
-        int jpos = -1, jneg = -1;
 #pragma unroll
         for (int j = 0; j < 4; ++j)
         {
-            if (dl[j] > dpos) { dpos = dl[j]; jpos = j; }
-            if (dl[j] < dneg) { dneg = dl[j]; jneg = j; }
+            dpos = fmaxf(dpos, dl[j]);
+            dneg = fminf(dneg, dl[j]);
         }
-        float psi = 1.f, bound = 0.f;
-        int jb = -1;
+        // dsel: the extreme dl whose bound sets psi (0: none); every face at that dl is snapped to the bound
+        float psi = 1.f, bound = 0.f, dsel = 0.f;
         if (p.limit)
         {
             if (dpos > 1e-30f)
             {
                 const float r = (hi - wc[q]) / dpos;
-                if (r < psi) { psi = r; jb = jpos; bound = hi; }
+                if (r < psi) { psi = r; dsel = dpos; bound = hi; }
             }
             if (dneg < -1e-30f)
             {
                 const float r = (lo - wc[q]) / dneg;
-                if (r < psi) { psi = r; jb = jneg; bound = lo; }
+                if (r < psi) { psi = r; dsel = dneg; bound = lo; }
             }
             if (p.rel_limit > 0.f && (q == 0 || q == 4))
             {
@@ -516,14 +515,14 @@ __device__ __forceinline__ void mx_grad_one(const MV &m, const MxParams &p, int 
                 if (a > 1e-30f)
                 {
                     const float r = p.rel_limit * wc[q] / a;
-                    if (r < psi) { psi = r; jb = -1; }
+                    if (r < psi) { psi = r; dsel = 0.f; }
                 }
             }
         }
-        if (psi < 0.f) { psi = 0.f; jb = -1; }
+        if (psi < 0.f) { psi = 0.f; dsel = 0.f; }
         psi = fminf(1.f, psi);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) fv[q][j] = j == jb ? bound : wc[q] + psi * dl[j];
+        for (int j = 0; j < 4; ++j) fv[q][j] = (dsel != 0.f && dl[j] == dsel) ? bound : wc[q] + psi * dl[j];
     }
     // positivity fallback of face_state: a face with rho <= 0 or p <= 0 takes the cell state
     bool ok[4];

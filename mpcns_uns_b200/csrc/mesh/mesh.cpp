@@ -970,6 +970,37 @@ int mhdm_boundary(MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const
     });
 }
 
+int mhdm_tag_types(const MhdHostMesh *m, const char *bc_default, int32_t n_pairs, const char *const *tag_names, const char *const *types,
+                   int32_t cap, int8_t *tag_type, int8_t *type_none, int32_t *n_tags)
+{
+    return guarded([&] {
+        std::map<std::string, std::string> by;
+        for (int32_t i = 0; i < n_pairs; ++i) by[tag_names[i]] = types[i];
+        const std::string def = bc_default ? bc_default : "outflow";
+        // the type a face of tag name `name` takes in boundary(): its pair, else the default
+        auto code = [&](const std::string &name) -> int8_t {
+            const auto it = by.find(name);
+            const std::string t = it != by.end() ? it->second : def;
+            return t == "wall" ? 1 : t == "inflow" ? 2 : t == "outflow" ? 3 : t == "farfield" ? 5 : 0;
+        };
+        const int32_t nt = static_cast<int32_t>(m->tag_names.size());
+        if (cap < nt) throw std::runtime_error("tag_type holds fewer entries than the mesh has tag names");
+        for (int32_t t = 0; t < nt; ++t) tag_type[t] = t > 0 ? code(m->tag_names[t]) : code("");
+        *type_none = code("");
+        *n_tags = nt;
+    });
+}
+
+int mhdm_set_boundary(MhdHostMesh *m, const int8_t *face_kind, const int8_t *edge_mode)
+{
+    return guarded([&] {
+        if (!face_kind || !edge_mode) throw std::runtime_error("null argument");
+        m->face_kind.assign(face_kind, face_kind + m->nf());
+        m->edge_mode.assign(edge_mode, edge_mode + m->ne());
+        m->have_bc = true;
+    });
+}
+
 const void *mhdm_array(const MhdHostMesh *m, const char *cname, int64_t *count)
 {
     const std::string n(cname);

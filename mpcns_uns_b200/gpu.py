@@ -120,6 +120,7 @@ _SIGS = {
     "mhd_gpu_tet_build_free": ([vp], ctypes.c_int),
     "mhd_gpu_state_set_resistivity": ([vp, vp], ctypes.c_int),
     "mhd_gpu_compute_geometry": ([vp], ctypes.c_int),
+    "mhd_gpu_boundary": ([vp], ctypes.c_int),
     "mhd_gpu_fn_create": ([vp, vp, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_fn_destroy": ([vp], ctypes.c_int),
     "mhd_gpu_fn_set_params": ([vp, vp, vp], ctypes.c_int),
@@ -684,6 +685,42 @@ def compute_geometry(host_mesh):
     m = int(out["ec_ptr"][-1])
     out["ec_cell"], out["ec_weight"] = out["ec_cell"][:m].copy(), out["ec_weight"][:m].copy()
     return out
+
+
+class BoundaryArgs(ctypes.Structure):
+    _fields_ = [("n_edges", i32), ("n_faces", i32), ("n_cells", i32), ("n_tags", i32)] + \
+               [(k, vp) for k in ("f2c_ptr", "f2c_idx", "f2c_sgn", "e2f_ptr", "e2f_idx", "cell_material", "face_tag", "face_area",
+                                  "face_area_mag", "tag_type")] + \
+               [("type_none", ctypes.c_int8), ("pad", ctypes.c_int8 * 7), ("u_inf", dbl * 3), ("face_kind", vp), ("edge_mode", vp)]
+
+
+def boundary(host_mesh, tag_type, type_none, u_inf):
+    """mhd::BoundaryInfo::build on the device (mhd_gpu_boundary) for a host mesh with geometry and the per-tag-id
+    boundary types (HostMesh.boundary(device=True) resolves them): (face_kind int8, edge_mode int8)."""
+    h = host_mesh
+    keep = []
+
+    def inp(name, dtype, a=None):
+        a = np.ascontiguousarray(np.asarray(h[name] if a is None else a).ravel(), dtype)
+        keep.append(a)
+        return ctypes.c_void_p(a.ctypes.data)
+
+    b = BoundaryArgs()
+    b.n_edges, b.n_faces, b.n_cells = h.n_edges, h.n_faces, h.n_cells
+    tt = np.ascontiguousarray(tag_type, np.int8)
+    b.n_tags = tt.size
+    b.f2c_ptr, b.f2c_idx, b.f2c_sgn = inp("f2c_ptr", np.int64), inp("f2c_idx", np.int32), inp("f2c_sgn", np.int8)
+    b.e2f_ptr, b.e2f_idx = inp("e2f_ptr", np.int64), inp("e2f_idx", np.int32)
+    b.cell_material, b.face_tag = inp("cell_material", np.int32), inp("face_tag", np.int32)
+    b.face_area, b.face_area_mag = inp("face_area", np.float64), inp("face_area_mag", np.float64)
+    b.tag_type = inp(None, np.int8, tt)
+    b.type_none = int(type_none)
+    b.u_inf[:] = [float(x) for x in u_inf]
+    fk = np.empty(h.n_faces, np.int8)
+    em = np.empty(h.n_edges, np.int8)
+    b.face_kind, b.edge_mode = ctypes.c_void_p(fk.ctypes.data), ctypes.c_void_p(em.ctypes.data)
+    check(lib().mhd_gpu_boundary(ctypes.byref(b)))
+    return fk, em
 
 
 class FnParams(ctypes.Structure):

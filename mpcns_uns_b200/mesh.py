@@ -61,6 +61,8 @@ def lib():
         L.mhdm_set_geometry.argtypes = [vp, vp]
         L.mhdm_reorder_cells.argtypes = [vp, vp, ctypes.POINTER(vp)]
         L.mhdm_boundary.argtypes = [vp, ctypes.c_char_p, i32, vp, vp, vp]
+        L.mhdm_tag_types.argtypes = [vp, ctypes.c_char_p, i32, vp, vp, i32, vp, vp, vp]
+        L.mhdm_set_boundary.argtypes = [vp, vp, vp]
         L.mhdm_array.argtypes = [vp, ctypes.c_char_p, ctypes.POINTER(i64)]
         L.mhdm_array.restype = vp
         _lib = L
@@ -201,14 +203,29 @@ class HostMesh:
         self._cache.clear()
         return self
 
-    def boundary(self, bc_default="outflow", by_tag=None, u_inf=(0.0, 0.0, 0.0)) -> "HostMesh":
-        """mhd::BoundaryInfo::build (Common/boundary/BoundaryInfo.cpp:9-49)."""
+    def boundary(self, bc_default="outflow", by_tag=None, u_inf=(0.0, 0.0, 0.0), device=False) -> "HostMesh":
+        """mhd::BoundaryInfo::build (Common/boundary/BoundaryInfo.cpp:9-49) on the host, or with device=True on the
+        GPU (mhd_gpu_boundary: the same face kinds and edge modes) and installed in this mesh."""
         by_tag = dict(by_tag or {})
         tags = (ctypes.c_char_p * max(1, len(by_tag)))(*[k.encode() for k in by_tag])
         types = (ctypes.c_char_p * max(1, len(by_tag)))(*[v.encode() for v in by_tag.values()])
         u = np.asarray(u_inf, np.float64)
-        _check(lib().mhdm_boundary(self._h, bc_default.encode(), len(by_tag), ctypes.cast(tags, ctypes.c_void_p),
-                                   ctypes.cast(types, ctypes.c_void_p), u.ctypes.data))
+        if device:
+            from . import gpu
+            try:
+                self["face_area"]
+            except KeyError:
+                self.compute_geometry()
+            cap = 4096
+            tt = np.zeros(cap, np.int8)
+            tn, nt = ctypes.c_int8(), ctypes.c_int32()
+            _check(lib().mhdm_tag_types(self._h, bc_default.encode(), len(by_tag), ctypes.cast(tags, ctypes.c_void_p),
+                                        ctypes.cast(types, ctypes.c_void_p), cap, tt.ctypes.data, ctypes.byref(tn), ctypes.byref(nt)))
+            fk, em = gpu.boundary(self, tt[:nt.value], tn.value, u)
+            _check(lib().mhdm_set_boundary(self._h, fk.ctypes.data, em.ctypes.data))
+        else:
+            _check(lib().mhdm_boundary(self._h, bc_default.encode(), len(by_tag), ctypes.cast(tags, ctypes.c_void_p),
+                                       ctypes.cast(types, ctypes.c_void_p), u.ctypes.data))
         self._cache.clear()
         return self
 

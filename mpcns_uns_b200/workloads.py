@@ -139,12 +139,12 @@ def shell_stretch(ncube, nr, r_in=1.0, r_out=6.0):
 
 def shell_mesh(ncube, nr, r_in=1.0, r_out=6.0, stretch=None, u_inf=(-8.0, 0.0, 0.0), device_geometry=False):
     """The shell workloads' mesh: cubed sphere, 6 tetrahedra per hexahedron, wall inside, far field outside.
-    device_geometry: number the complex and compute the metric on the GPU (bit-identical, much faster for
-    large shells)."""
+    device_geometry: number the complex, compute the metric and classify the boundary on the GPU (bit-identical,
+    much faster for large shells)."""
     if stretch is None:
         stretch = shell_stretch(ncube, nr, r_in, r_out)
     m = HostMesh.shell(ncube, nr, r_in, r_out, stretch, tets=True, device_build=device_geometry).compute_geometry(device=device_geometry)
-    m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf)
+    m.boundary("outflow", {"inner": "wall", "outer": "farfield"}, u_inf, device=device_geometry)
     return m, stretch
 
 

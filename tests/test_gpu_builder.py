@@ -28,3 +28,36 @@ def test_device_build_equals_host_build(ncube, nr, n_solid, r_in, stretch):
     h.compute_geometry().boundary("outflow", {"inner": "wall", "outer": "farfield"}, (-8.0, 0.0, 0.0))
     for k in ("face_kind", "edge_mode", "cell_volume", "star1"):
         assert np.array_equal(np.asarray(d[k]), np.asarray(h[k])), k
+
+
+def _boundary_pairs():
+    from helpers import MIXED_BOX_BC, SHELL_BC
+    yield "box_tets_mixed", HostMesh.box(6, 5, 4, tets=True, jitter=0.1, seed=3), MIXED_BOX_BC
+    yield "box_hex_farfield", HostMesh.box(5, 4, 6), ("farfield", {}, (0.3, -0.7, 0.2))
+    yield "shell_solid", HostMesh.shell(5, 4, 0.8, 6.0, 1.2, n_solid=1, tets=True), SHELL_BC
+    yield "shell_default_wall", HostMesh.shell(4, 5, 1.0, 6.0, 1.3, tets=True), ("wall", {"outer": "inflow"}, (0.0, 0.0, 0.0))
+
+
+@pytest.mark.parametrize("name", ["box_tets_mixed", "box_hex_farfield", "shell_solid", "shell_default_wall"])
+def test_device_boundary_equals_host(name):
+    """mhd::BoundaryInfo::build on the device (mhd_gpu_boundary) gives the host classification's face kinds and
+    edge modes entry for entry: interior, solid-interface walls, skipped faces, tagged walls, inflow and outflow,
+    farfield faces split by the side of u_inf, wall edges winning over inflow edges."""
+    h, bc = next((m, b) for n, m, b in _boundary_pairs() if n == name)
+    d = next(m for n, m, b in _boundary_pairs() if n == name)   # a second, independent copy of the same complex
+    assert d.topology_hash() == h.topology_hash()
+    h.compute_geometry()
+    d.compute_geometry(device=True)
+    h.boundary(*bc)
+    d.boundary(*bc, device=True)
+    for k in ("face_kind", "edge_mode"):
+        a, b = np.asarray(d[k]), np.asarray(h[k])
+        assert np.array_equal(a, b), (k, np.count_nonzero(a != b))
+    assert len(np.unique(np.asarray(h["face_kind"]))) >= 3   # interior and at least two boundary kinds
+
+
+def test_device_boundary_rejects_unknown_type():
+    from mpcns_uns_b200.gpu import MhdError
+    h = HostMesh.shell(3, 2, 1.0, 6.0, 1.0, tets=True).compute_geometry()
+    with pytest.raises(MhdError, match="unknown boundary type"):
+        h.boundary("outflow", {"inner": "bogus"}, device=True)

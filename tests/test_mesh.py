@@ -92,3 +92,21 @@ def test_cell_reordering_round_trip_and_locality():
 
     local = scrambled.reordered(scrambled.locality_order())
     assert spread(local) < 0.05 * spread(scrambled)
+
+
+def test_tag_types_resolution():
+    """mhdm_tag_types resolves the tag names as mhdm_boundary does: a pair's type, else the default; tag 0 and
+    unknown ids take the empty name's type; unknown type names resolve to 0."""
+    import ctypes
+    from mpcns_uns_b200.mesh import lib
+    h = HostMesh.box(2, 2, 2)
+    pairs = {"xmin": "inflow", "xmax": "wall", "ymin": "farfield", "zmax": "bogus"}
+    tags = (ctypes.c_char_p * len(pairs))(*[k.encode() for k in pairs])
+    types = (ctypes.c_char_p * len(pairs))(*[v.encode() for v in pairs.values()])
+    tt = np.zeros(64, np.int8)
+    tn, nt = ctypes.c_int8(), ctypes.c_int32()
+    assert lib().mhdm_tag_types(h._h, b"outflow", len(pairs), ctypes.cast(tags, ctypes.c_void_p), ctypes.cast(types, ctypes.c_void_p),
+                                64, tt.ctypes.data, ctypes.byref(tn), ctypes.byref(nt)) == 0
+    # box tag ids: 1 xmin, 2 xmax, 3 ymin, 4 ymax, 5 zmin, 6 zmax
+    assert nt.value == 7 and tn.value == 3
+    assert tt[:7].tolist() == [3, 2, 1, 5, 3, 3, 0]
