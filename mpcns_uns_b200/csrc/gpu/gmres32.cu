@@ -12,13 +12,15 @@ void op32(MhdInduction *I, const MatIn &in, double dt, double *y, const Fused &f
     const MeshView &m = I->mesh->v;
     cudaStream_t s = I->mesh->stream;
     if (m.nf)
-        IND_LAUNCH(I, KI_FACE, s, k_ind_face<float><<<g1(m.nf), 256, 0, s>>>(m, fz.gt, in, I->hall, I->resistive, I->phi32.p, I->s2phi32.p));
+        IND_LAUNCH(I, KI_FACE, s, (m.tri_faces ? k_ind_face<float, true> : k_ind_face<float, false>)<<<g1(m.nf), 256, 0, s>>>(
+                                      m, fz.gt, in, I->hall, I->resistive, I->phi32.p, I->s2phi32.p));
     if (I->hall && m.nc)
     {
-        IND_LAUNCH(I, KI_BCELL, s, k_ind_bcell<float><<<g1(m.nc), 256, 0, s>>>(m, fz.gt, I->recon32.p, I->phi32.p, I->b32.p));
+        IND_LAUNCH(I, KI_BCELL, s, (m.faces_per_cell == 4 ? k_ind_bcell<float, true> : k_ind_bcell<float, false>)<<<g1(m.nc), 256, 0, s>>>(
+                                       m, fz.gt, I->recon32.p, I->phi32.p, I->b32.p));
         if (m.no_cells)
             IND_LAUNCH(I, KI_HALL, s,
-                       k_ind_hall32<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot32.p, I->b32.p, I->alpha32.p, I->B0_32.p, I->vinv32.p,
+                       (m.faces_per_cell == 4 ? k_ind_hall32<true> : k_ind_hall32<false>)<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot32.p, I->b32.p, I->alpha32.p, I->B0_32.p, I->vinv32.p,
                                                                    I->g32.p));
     }
     EdgeArgs<float> a;

@@ -36,6 +36,28 @@ struct Gate
     __device__ __forceinline__ bool off() const { return ctl && (ctl->done || j >= ctl->limit); }
 };
 
+// ---------------------------------------------------------------- classical Gram-Schmidt (gram_schmidt.cu)
+constexpr int kCgsMax = 31; // basis vectors one pass handles (restart <= 31); the 32nd partial is |w|^2
+struct CgsArgs
+{
+    Gate gt;
+    Ctl *ctl;
+    double *w;
+    const double *V;
+    int64_t ldv;
+    int32_t n_all, n_owned;
+    double *part, *red, *H;
+    unsigned *counter;
+    int mcols;
+    const double *pd;
+    double *zs;
+    float *zs32;
+};
+// pass 0: the dots; 1: the update; 2: the gated second update (column j = number of basis vectors - 1)
+void cgs_launch(int j, const CgsArgs &a, const int *grid, cudaStream_t s, int pass);
+// the resident grids of column k's passes (2 ints), for an SM count
+void cgs_grids_for(int k, int sms, int *grid);
+
 // ---------------------------------------------------------------- operator
 // Input of a matvec: x_e directly (apply_A), or the preconditioned Krylov vector
 // x_e = (src_e / *hs) * pd_e with pd_e = dir_e ? 0 : 1 / (1 + dt m_e d2_e)  (:338)
@@ -113,32 +135,52 @@ __device__ __forceinline__ void grid_sum_tail(double v, double *part, unsigned *
 
 // Phi' = d1 x on every face (:185-190), with star2 Phi' for the resistive current flux (:131-136).
 // FP64 sums in both precisions; the FP32 operator stores the rounded results.
-template <class T>
+// TRI: every face a triangle (f2e row of face f at 3f): the three gathers unrolled, in the row's order
+template <class T, bool TRI = false>
 __global__ void k_ind_face(MeshView m, Gate gt, MatIn in, int hall, int resistive, T *__restrict__ phi, T *__restrict__ s2phi)
 {
     const int32_t f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= m.nf || gt.off()) return;
     double s = 0;
-    const int32_t k0 = m.f2e_ptr[f], k1 = m.f2e_ptr[f + 1];
-    if (in.zs32)
-        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * static_cast<double>(in.zs32[m.f2e_idx[k]]);
-    else if (in.zs)
-        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.zs[m.f2e_idx[k]];
+    if constexpr (TRI)
+    {
+        const int64_t k0 = 3 * (int64_t)f;
+        const int32_t e0 = m.f2e_idx[k0], e1 = m.f2e_idx[k0 + 1], e2 = m.f2e_idx[k0 + 2];
+        const double s0 = m.f2e_sgn[k0], s1 = m.f2e_sgn[k0 + 1], s2 = m.f2e_sgn[k0 + 2];
+        double v0, v1, v2;
+        if (in.zs32) { v0 = in.zs32[e0]; v1 = in.zs32[e1]; v2 = in.zs32[e2]; }
+        else if (in.zs) { v0 = in.zs[e0]; v1 = in.zs[e1]; v2 = in.zs[e2]; }
+        else { v0 = in.x[e0]; v1 = in.x[e1]; v2 = in.x[e2]; }
+        s += s0 * v0;
+        s += s1 * v1;
+        s += s2 * v2;
+    }
     else
-        for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.x[m.f2e_idx[k]];
+    {
+        const int32_t k0 = m.f2e_ptr[f], k1 = m.f2e_ptr[f + 1];
+        if (in.zs32)
+            for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * static_cast<double>(in.zs32[m.f2e_idx[k]]);
+        else if (in.zs)
+            for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.zs[m.f2e_idx[k]];
+        else
+            for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.x[m.f2e_idx[k]];
+    }
     if ((in.zs || in.zs32) && in.hs) s = s / *in.hs;
     if (hall) phi[f] = static_cast<T>(s);
     if (resistive) s2phi[f] = static_cast<T>(m.star2[f] * s);
 }
 
-// cell field from the face fluxes (:139-149)
-template <class T>
+// cell field from the face fluxes (:139-149); TET: every cell a tetrahedron (c2f row of cell c at 4c), the
+// four slots unrolled in the row's order
+template <class T, bool TET = false>
 __global__ void k_ind_bcell(MeshView m, Gate gt, const T *__restrict__ recon, const T *__restrict__ phi, T *__restrict__ b)
 {
     const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= m.nc || gt.off()) return;
     T bx = 0, by = 0, bz = 0;
-    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    const int32_t kb = TET ? 4 * c : m.c2f_ptr[c], ke = TET ? 4 * c + 4 : m.c2f_ptr[c + 1];
+#pragma unroll 4
+    for (int32_t k = kb; k < ke; ++k)
     {
         const T v = phi[m.c2f_idx[k]];
         bx += recon[3 * (int64_t)k] * v;
@@ -148,6 +190,7 @@ __global__ void k_ind_bcell(MeshView m, Gate gt, const T *__restrict__ recon, co
     b[3 * (int64_t)c] = bx; b[3 * (int64_t)c + 1] = by; b[3 * (int64_t)c + 2] = bz;
 }
 
+template <bool TET = false>
 __global__ void k_ind_hall32(MeshView m, Gate gt, const float4 *__restrict__ slot32, const float *__restrict__ b,
                              const float *__restrict__ alpha, const float *__restrict__ B0, const float *__restrict__ vinv,
                              float *__restrict__ g)
@@ -162,7 +205,9 @@ __global__ void k_ind_hall32(MeshView m, Gate gt, const float4 *__restrict__ slo
     }
     float sx = 0.f, sy = 0.f, sz = 0.f;
     const float bcx = b[3 * (int64_t)c], bcy = b[3 * (int64_t)c + 1], bcz = b[3 * (int64_t)c + 2];
-    for (int32_t k = m.c2f_ptr[c]; k < m.c2f_ptr[c + 1]; ++k)
+    const int32_t kb = TET ? 4 * c : m.c2f_ptr[c], ke = TET ? 4 * c + 4 : m.c2f_ptr[c + 1];
+#pragma unroll 4
+    for (int32_t k = kb; k < ke; ++k)
     {
         const float4 sl = slot32[k];
         const int32_t o = __float_as_int(sl.w);
