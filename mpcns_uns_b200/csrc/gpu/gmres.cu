@@ -368,7 +368,7 @@ void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, dou
     a.s2phi = I->s2phi.p; a.g = I->g.p; a.mcoef = I->mcoef.p; a.ecw = m.ec_weight; a.tvec = m.edge_vec;
     a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
     a.part = I->part.p; a.counter = I->counter.p; a.out = y;
-    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, k_ind_edge<double><<<I->edge_blocks, 256, 0, s>>>(m, a));
+    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, (m.max_valence <= 8 && m.max_edge_cells <= 8 ? k_ind_edge<double, 8> : k_ind_edge<double, 0>)<<<I->edge_blocks, 256, 0, s>>>(m, a));
 }
 
 void apply_plain(MhdInduction *I, const double *x, double dt, double *y)

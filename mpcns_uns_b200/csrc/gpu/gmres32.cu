@@ -28,7 +28,7 @@ void op32(MhdInduction *I, const MatIn &in, double dt, double *y, const Fused &f
     a.s2phi = I->s2phi32.p; a.g = I->g32.p; a.mcoef = I->m32.p; a.ecw = I->ecw32.p; a.tvec = I->tv32.p;
     a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
     a.part = I->part.p; a.counter = I->counter.p; a.out = y;
-    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, k_ind_edge<float><<<I->edge_blocks, 256, 0, s>>>(m, a));
+    if (m.ne) IND_LAUNCH(I, KI_EDGE, s, (m.max_valence <= 8 && m.max_edge_cells <= 8 ? k_ind_edge<float, 8> : k_ind_edge<float, 0>)<<<I->edge_blocks, 256, 0, s>>>(m, a));
 }
 
 } // namespace mhd

@@ -233,7 +233,10 @@ __global__ void k_ind_hall32(MeshView m, Gate gt, const float4 *__restrict__ slo
 
 // Per edge: part0 = sum_f s star2 Phi' (resistive, ascending faces), part1 = sum_c g_c . (w_ec t_e)
 // (Hall, ascending cells), F = m part0 + part1 + part2 (:176-182); y = F, or y = x + dt F (:191-197).
-template <class T>
+// MAXK > 0: every edge has at most MAXK faces and MAXK cells (tetrahedral meshes: 8); both gathers are
+// unrolled over that bound (predicated beyond the row), so that a row's loads are in flight together.  The
+// sums run over the rows in their order either way.
+template <class T, int MAXK>
 __global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
 {
     if (a.gt.off()) return;
@@ -243,18 +246,36 @@ __global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
     {
         T p0 = 0, p1 = 0;
         if (a.resistive)
-            for (int32_t k = m.e2f_ptr[e]; k < m.e2f_ptr[e + 1]; ++k) p0 += static_cast<T>(m.e2f_sgn[k]) * a.s2phi[m.e2f_idx[k]];
+        {
+            const int32_t k0 = m.e2f_ptr[e], k1 = m.e2f_ptr[e + 1];
+            if constexpr (MAXK > 0)
+            {
+#pragma unroll
+                for (int i = 0; i < MAXK; ++i)
+                    if (k0 + i < k1) p0 += static_cast<T>(m.e2f_sgn[k0 + i]) * a.s2phi[m.e2f_idx[k0 + i]];
+            }
+            else
+                for (int32_t k = k0; k < k1; ++k) p0 += static_cast<T>(m.e2f_sgn[k]) * a.s2phi[m.e2f_idx[k]];
+        }
         if (a.hall)
         {
             const T tx = a.tvec[3 * (int64_t)e], ty = a.tvec[3 * (int64_t)e + 1], tz = a.tvec[3 * (int64_t)e + 2];
-            for (int32_t k = m.ec_ptr[e]; k < m.ec_ptr[e + 1]; ++k)
-            {
+            const int32_t k0 = m.ec_ptr[e], k1 = m.ec_ptr[e + 1];
+            auto term = [&](int32_t k) {
                 const int32_t c = m.ec_cell[k];
-                if (c >= m.no_cells) continue;
+                if (c >= m.no_cells) return;
                 const T w = a.ecw[k];
                 const T wx = w * tx, wy = w * ty, wz = w * tz;
                 p1 += a.g[3 * (int64_t)c] * wx + a.g[3 * (int64_t)c + 1] * wy + a.g[3 * (int64_t)c + 2] * wz;
+            };
+            if constexpr (MAXK > 0)
+            {
+#pragma unroll
+                for (int i = 0; i < MAXK; ++i)
+                    if (k0 + i < k1) term(k0 + i);
             }
+            else
+                for (int32_t k = k0; k < k1; ++k) term(k);
         }
         const T F = a.mcoef[e] * p0 + p1 + static_cast<T>(0);
         double y = static_cast<double>(F);
