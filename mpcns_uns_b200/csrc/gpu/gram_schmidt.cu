@@ -96,24 +96,65 @@ __device__ __forceinline__ bool grid_sum32(double v, double *part, unsigned *cou
 // (and so the resident warps) follow the column.  A thread adds its edges' products into its running
 // sums; the sums meet once, at the end, in the warp reduce-scatter and the grid tail.
 
+// Both passes stream NV (+2) vectors tile by tile: a block of kGsThreads threads takes tiles of kGsThreads
+// consecutive edges, and while it works on one tile the next tiles' values are already on their way into
+// shared memory (cp.async, kGsStages stages, each thread copying and reading only its own column: no block
+// barrier), so that a thread keeps many loads in flight without holding them in registers.  8-byte copies:
+// the basis vectors start at i * ldv, which need not be 16-byte aligned.
+constexpr int kGsThreads = 128;
+constexpr int kGsStages = 3; // tiles in flight per block: the one being read and kGsStages - 1 ahead
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
+{
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Pass 1: h_i = V_i . w (i < NV) into H(i, j), and |w|^2 into red[32], over the owned edges.  red holds 96
 // doubles: [0, 31) the re-orthogonalisation dots, [32] |w|^2 before the update, [64, 96) the last pass's sums.
+// Dynamic shared memory: kGsStages stages x (NV + 1) vectors x kGsThreads doubles.
 template <int NV>
-__global__ void __launch_bounds__(256) k_cgs_dots(Gate gt, const double *__restrict__ w, const double *__restrict__ V, int64_t ldv,
-                                                   int32_t n_owned, double *part, unsigned *counter, double *red, double *H, int mcols)
+__global__ void __launch_bounds__(kGsThreads) k_cgs_dots(Gate gt, const double *__restrict__ w, const double *__restrict__ V, int64_t ldv,
+                                                          int32_t n_owned, double *part, unsigned *counter, double *red, double *H, int mcols)
 {
     if (gt.off()) return;
-    constexpr int j = NV - 1;
+    constexpr int j = NV - 1, NVEC = NV + 1;
+    extern __shared__ double sm[];
+    const int tid = threadIdx.x;
+    const int64_t ntiles = (n_owned + kGsThreads - 1) / kGsThreads;
+    auto issue = [&](int64_t tile, int stage) {
+        const int64_t e = tile * kGsThreads + tid;
+        if (e < n_owned)
+        {
+            double *col = sm + (int64_t)stage * NVEC * kGsThreads + tid;
+#pragma unroll
+            for (int i = 0; i < NV; ++i) cp_async8(col + i * kGsThreads, V + i * ldv + e);
+            cp_async8(col + NV * kGsThreads, w + e);
+        }
+        cp_async_commit();
+    };
     double acc[NV + 1];
 #pragma unroll
     for (int i = 0; i <= NV; ++i) acc[i] = 0.0;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_owned; e += (int64_t)gridDim.x * blockDim.x)
-    {
-        const double we = w[e];
+    int64_t tile = blockIdx.x;
 #pragma unroll
-        for (int i = 0; i < NV; ++i) acc[i] += V[i * ldv + e] * we;
-        acc[NV] += we * we;
+    for (int q = 0; q < kGsStages - 1; ++q) issue(tile + q * gridDim.x, q);
+    for (int k = 0; tile < ntiles; ++k, tile += gridDim.x)
+    {
+        issue(tile + (kGsStages - 1) * (int64_t)gridDim.x, (k + kGsStages - 1) % kGsStages); // past the end: an empty group
+        cp_async_wait<kGsStages - 1>();
+        const int64_t e = tile * kGsThreads + tid;
+        if (e < n_owned)
+        {
+            const double *col = sm + (int64_t)(k % kGsStages) * NVEC * kGsThreads + tid;
+            const double we = col[NV * kGsThreads];
+#pragma unroll
+            for (int i = 0; i < NV; ++i) acc[i] += col[i * kGsThreads] * we;
+            acc[NV] += we * we;
+        }
     }
+    cp_async_wait<0>();
     double p[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) p[i] = i < NV ? acc[i] : (i == 31 ? acc[NV] : 0.0);
@@ -128,43 +169,65 @@ __global__ void __launch_bounds__(256) k_cgs_dots(Gate gt, const double *__restr
 // (|w|^2 < |w_before|^2 / 2, red[32] holds |w_before|^2 from pass 1) and the remaining components along
 // the basis are above round-off (|s| > 1e-12 |w|), it leaves s in red[0..j] and raises ctl->reorth; else it
 // stores H(j+1, j) = |w|.  Pass 3 (reorth == 1) runs only when raised: it adds c to H(:, j), stores
-// H(j+1, j) = |w| and lowers the flag.
+// H(j+1, j) = |w| and lowers the flag.  reverse: the tiles in descending order (the previous pass's tail is
+// in L2).  Dynamic shared memory: kGsStages stages x (NV + 2) vectors (the basis, w, pd) x kGsThreads doubles.
 template <int NV, bool F32>
-__global__ void __launch_bounds__(256) k_cgs_update(Gate gt, Ctl *ctl, int reorth, double *__restrict__ w, const double *__restrict__ V,
-                                                     int64_t ldv, int32_t n_all, int32_t n_owned, int reverse, double *part,
-                                                     unsigned *counter, double *red, double *H, int mcols, const double *__restrict__ pd,
-                                                     double *__restrict__ zs, float *__restrict__ zs32)
+__global__ void __launch_bounds__(kGsThreads) k_cgs_update(Gate gt, Ctl *ctl, int reorth, double *__restrict__ w, const double *__restrict__ V,
+                                                            int64_t ldv, int32_t n_all, int32_t n_owned, int reverse, double *part,
+                                                            unsigned *counter, double *red, double *H, int mcols,
+                                                            const double *__restrict__ pd, double *__restrict__ zs, float *__restrict__ zs32)
 {
     if (gt.off() || (reorth && !ctl->reorth)) return;
-    constexpr int j = NV - 1;
+    constexpr int j = NV - 1, NVEC = NV + 2;
+    extern __shared__ double sm[];
     __shared__ double csh[NV];
-    if (threadIdx.x < NV) csh[threadIdx.x] = reorth ? red[threadIdx.x] : H[threadIdx.x * mcols + j];
+    const int tid = threadIdx.x;
+    if (tid < NV) csh[tid] = reorth ? red[tid] : H[tid * mcols + j];
     __syncthreads();
-    double c[NV];
+    const int64_t ntiles = (n_all + kGsThreads - 1) / kGsThreads;
+    auto tile_of = [&](int64_t t) { return reverse ? ntiles - 1 - t : t; };
+    auto issue = [&](int64_t t, int stage) {
+        const int64_t e = t < ntiles ? tile_of(t) * kGsThreads + tid : n_all;
+        if (e < n_all)
+        {
+            double *col = sm + (int64_t)stage * NVEC * kGsThreads + tid;
 #pragma unroll
-    for (int i = 0; i < NV; ++i) c[i] = csh[i];
+            for (int i = 0; i < NV; ++i) cp_async8(col + i * kGsThreads, V + i * ldv + e);
+            cp_async8(col + NV * kGsThreads, w + e);
+            cp_async8(col + (NV + 1) * kGsThreads, pd + e);
+        }
+        cp_async_commit();
+    };
     double acc[NV + 1];
 #pragma unroll
     for (int i = 0; i <= NV; ++i) acc[i] = 0.0;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n_all; t += (int64_t)gridDim.x * blockDim.x)
+    int64_t t = blockIdx.x;
+#pragma unroll
+    for (int q = 0; q < kGsStages - 1; ++q) issue(t + q * gridDim.x, q);
+    for (int k = 0; t < ntiles; ++k, t += gridDim.x)
     {
-        const int64_t e = reverse ? n_all - 1 - t : t;
-        double v[NV];
-#pragma unroll
-        for (int i = 0; i < NV; ++i) v[i] = V[i * ldv + e];
-        double we = w[e];
-#pragma unroll
-        for (int i = 0; i < NV; ++i) we -= c[i] * v[i];
-        w[e] = we;
-        if (F32) zs32[e] = static_cast<float>(we * pd[e]);
-        else zs[e] = we * pd[e];
-        if (e < n_owned)
+        issue(t + (kGsStages - 1) * (int64_t)gridDim.x, (k + kGsStages - 1) % kGsStages);
+        cp_async_wait<kGsStages - 1>();
+        const int64_t e = tile_of(t) * kGsThreads + tid;
+        if (e < n_all)
         {
+            const double *col = sm + (int64_t)(k % kGsStages) * NVEC * kGsThreads + tid;
+            double we = col[NV * kGsThreads];
 #pragma unroll
-            for (int i = 0; i < NV; ++i) acc[i] += v[i] * we;
-            acc[NV] += we * we;
+            for (int i = 0; i < NV; ++i) we -= csh[i] * col[i * kGsThreads];
+            w[e] = we;
+            const double z = we * col[(NV + 1) * kGsThreads];
+            if (F32) zs32[e] = static_cast<float>(z);
+            else zs[e] = z;
+            if (e < n_owned)
+            {
+#pragma unroll
+                for (int i = 0; i < NV; ++i) acc[i] += col[i * kGsThreads] * we;
+                acc[NV] += we * we;
+            }
         }
     }
+    cp_async_wait<0>();
     double p[32];
 #pragma unroll
     for (int i = 0; i < 32; ++i) p[i] = i < NV ? acc[i] : (i == 31 ? acc[NV] : 0.0);
@@ -182,31 +245,40 @@ __global__ void __launch_bounds__(256) k_cgs_update(Gate gt, Ctl *ctl, int reort
         return;
     }
     if (reorth)
-        for (int i = 0; i < NV; ++i) H[i * mcols + j] += c[i];
+        for (int i = 0; i < NV; ++i) H[i * mcols + j] += csh[i];
     H[(j + 1) * mcols + j] = sqrt(nn);
     ctl->reorth = 0;
 }
 
 // Launchers of the instances for NV = 1..31, and their grids (resident blocks on every SM)
+constexpr size_t gs_smem(int nvec) { return size_t(kGsStages) * nvec * kGsThreads * sizeof(double); }
 template <int NV> void cgs_step(const CgsArgs &a, const int *grid, cudaStream_t s, int pass)
 {
     if (pass == 0)
-        k_cgs_dots<NV><<<grid[0], 256, 0, s>>>(a.gt, a.w, a.V, a.ldv, a.n_owned, a.part, a.counter, a.red, a.H, a.mcols);
+        k_cgs_dots<NV><<<grid[0], kGsThreads, gs_smem(NV + 1), s>>>(a.gt, a.w, a.V, a.ldv, a.n_owned, a.part, a.counter, a.red, a.H,
+                                                                    a.mcols);
     else if (a.zs32)
-        k_cgs_update<NV, true><<<grid[1], 256, 0, s>>>(a.gt, a.ctl, pass - 1, a.w, a.V, a.ldv, a.n_all, a.n_owned, pass == 1, a.part,
-                                                       a.counter, a.red, a.H, a.mcols, a.pd, nullptr, a.zs32);
+        k_cgs_update<NV, true><<<grid[1], kGsThreads, gs_smem(NV + 2), s>>>(a.gt, a.ctl, pass - 1, a.w, a.V, a.ldv, a.n_all, a.n_owned,
+                                                                            pass == 1, a.part, a.counter, a.red, a.H, a.mcols, a.pd,
+                                                                            nullptr, a.zs32);
     else
-        k_cgs_update<NV, false><<<grid[1], 256, 0, s>>>(a.gt, a.ctl, pass - 1, a.w, a.V, a.ldv, a.n_all, a.n_owned, pass == 1, a.part,
-                                                        a.counter, a.red, a.H, a.mcols, a.pd, a.zs, nullptr);
+        k_cgs_update<NV, false><<<grid[1], kGsThreads, gs_smem(NV + 2), s>>>(a.gt, a.ctl, pass - 1, a.w, a.V, a.ldv, a.n_all, a.n_owned,
+                                                                             pass == 1, a.part, a.counter, a.red, a.H, a.mcols, a.pd,
+                                                                             a.zs, nullptr);
 }
+// the instances' shared memory opted in, and their resident grids (the partials buffer holds kRedBlocks)
 template <int NV> void cgs_grids(int sms, int *grid)
 {
+    const int sd = static_cast<int>(gs_smem(NV + 1)), su = static_cast<int>(gs_smem(NV + 2));
+    MHD_CUDA(cudaFuncSetAttribute(k_cgs_dots<NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sd));
+    MHD_CUDA(cudaFuncSetAttribute(k_cgs_update<NV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, su));
+    MHD_CUDA(cudaFuncSetAttribute(k_cgs_update<NV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, su));
     int per = 0;
-    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cgs_dots<NV>, 256, 0));
+    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cgs_dots<NV>, kGsThreads, sd));
     grid[0] = std::max(1, std::min(kRedBlocks, sms * std::max(per, 1)));
-    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cgs_update<NV, false>, 256, 0));
+    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_cgs_update<NV, false>, kGsThreads, su));
     int per32 = 0;
-    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_cgs_update<NV, true>, 256, 0));
+    MHD_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per32, k_cgs_update<NV, true>, kGsThreads, su));
     grid[1] = std::max(1, std::min(kRedBlocks, sms * std::max(std::min(per, per32), 1)));
 }
 using CgsStepFn = void (*)(const CgsArgs &, const int *, cudaStream_t, int);
