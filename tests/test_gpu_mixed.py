@@ -128,3 +128,41 @@ def test_mixed_vs_fp64_ten_ions_wall_table():
     assert dm.div_b(P32)["max_rel"] < DIVB_TOL
     num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(Un, U64))
     assert np.sqrt(num / den) > 1e-6      # the table acts
+
+
+def test_config2_hundred_steps_accuracy():
+    """The bench's config-2 figures, asserted: the 14,155,776-cell two-ion shell with the J x B force and the
+    Strang-split gyration, 100 steps at CFL 0.4 (device CFL step in each precision) from the same state.
+    * the whole state within 1e-5 relative L2 of the FP64 step (north_star's bar), and H+ alone too;
+    * Na+, the trace ion whose first cell layer at the absorbing wall amplifies rounding, within 2x of what
+      the FP64 step itself departs by from a state perturbed by 1e-7 (single-precision input rounding):
+      the mixed step is as accurate as the problem's conditioning allows;
+    * Phi within 1e-5, and div B at FP64 round-off of the total field in both precisions."""
+    from mpcns_uns_b200 import gpu, workloads
+    wl = workloads.shell(64, 96, sources=True, device_geometry=True)
+    assert wl.mesh.n_cells == 14155776 and wl.lorentz
+    dm = gpu.DeviceMesh(wl.mesh)
+    n = 100
+
+    def run(precision, U0):
+        p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl,
+                            precision=precision, lorentz=wl.lorentz, induce_coeff=wl.induce_coeff, inver_MA2=wl.inver_MA2)
+        st = gpu.ResidentState(dm, p)
+        st.set(U0, wl.Phi, wl.PhiAdd)
+        for _ in range(n):
+            st.step(0.0, sync=False)
+        out = [st.U(s) for s in range(wl.n_species)], st.Phi()
+        del st
+        return out
+
+    U64, P64 = run("fp64", wl.U)
+    U32, P32 = run("mixed", wl.U)
+    rng = np.random.default_rng(7)
+    Up, _ = run("fp64", [u * (1 + 1e-7 * rng.uniform(-1, 1, u.size)) for u in wl.U])
+    num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(U32, U64))
+    den = sum(float(np.sum(b ** 2)) for b in U64)
+    assert np.sqrt(num / den) < L2_TOL
+    assert _l2(U32[0], U64[0]) < L2_TOL
+    assert _l2(U32[1], U64[1]) < 2 * _l2(Up[1], U64[1]), (_l2(U32[1], U64[1]), _l2(Up[1], U64[1]))
+    assert np.linalg.norm(P32 - P64) / np.linalg.norm(P64 + wl.PhiAdd) < L2_TOL
+    assert dm.div_b(P32, wl.PhiAdd)["max_rel"] < DIVB_TOL and dm.div_b(P64, wl.PhiAdd)["max_rel"] < DIVB_TOL
