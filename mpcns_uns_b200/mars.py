@@ -43,7 +43,11 @@ class MarsStep:
     inflow ghost state of each ion (n_species x 5).  wall: (faces, prims n_species x n_wall x 5), the wall
     ghost table.  neutral: neutral_stride densities per cell [cm^-3].  PhiAdd: the background face flux."""
 
-    def __init__(self, dmesh: gpu.DeviceMesh, scales: dict, freestream, wall, neutral, PhiAdd, masses=PARTICLE_MASS):
+    def __init__(self, dmesh: gpu.DeviceMesh, scales: dict, freestream, wall, neutral, PhiAdd, masses=PARTICLE_MASS,
+                 induction=None):
+        """induction: the Hall solve's GMRES settings (rtol, max_it, restart, precision; the reference's Config
+        defaults 1e-4, 100, 20, FP64 otherwise).  The solve runs when scales["hall"] is on and
+        scales["hall_scale"] > 0, as MarsSolver builds its ImplicitInduction: Hall only, no radial taper."""
         torch = gpu._torch()
         self.dm = dmesh
         self.sc = dict(scales)
@@ -59,6 +63,13 @@ class MarsStep:
         nc = dmesh.n_cells
         self.U = torch.zeros(self.nsp * 5 * nc, dtype=torch.float64, device="cuda")
         self.Phi = torch.zeros(dmesh.n_faces, dtype=torch.float64, device="cuda")
+        self.ind, self.last_solve = None, None
+        if self.sc.get("hall", 0) and self.sc.get("hall_scale", 0.0) > 0:
+            k = {"rtol": 1e-4, "max_it": 100, "restart": 20, "precision": "fp64", **(induction or {})}
+            self.ind = gpu.DeviceInduction(dmesh, None, hall=True, hall_coef=self.sc["hall_scale"], hall_r_min=0.0, hall_r_max=0.0,
+                                           rtol=k["rtol"], max_it=k["max_it"], restart=k["restart"], precision=k["precision"])
+            self.fluid = gpu.dev(np.asarray(dmesh.host["cell_material"]) == 0)
+            self.dirichlet = gpu.dev((np.asarray(dmesh.host["edge_mode"]) != 0).astype(np.int8))
 
     def set(self, U, Phi):
         self.U.copy_(gpu.dev(U).reshape(-1))
@@ -103,7 +114,11 @@ class MarsStep:
         return dm.edge_modes(sc["u_inf"], sc["B_imf"], E)
 
     def step(self, dt_max=1e300):
-        """MarsSolver::step without the photochemistry and the Hall solve; returns the step size."""
+        """MarsSolver::step (:705-744) without the photochemistry; returns the step size.  With the Hall term on,
+        the edge EMF is the implicit one of the semi-implicit induction solve (:723-735): the frozen total field
+        and n_e,eff of the fluid cells, wall and inflow edges held at their prescribed values, GMRES warm-started
+        from the previous step's correction; last_solve holds its (iterations, relative residual)."""
+        torch = gpu._torch()
         dm, sc = self.dm, self.sc
         q = self.prepare()
         dt = min(dm.mars_time_step(self.mp, sc["cfl"], self.U, q["W"], q["Btot"], q["uplus"]), dt_max)
@@ -112,6 +127,11 @@ class MarsStep:
         rhs = self.rhs(q)
         E = self.emf(q)
         dm.mars_advance(self.nsp, rhs, dt, self.U)
+        if self.ind is not None:
+            ne = torch.where(self.fluid, q["ne_eff"], torch.zeros_like(q["ne_eff"]))
+            self.ind.set_frozen_state(q["Btot"], ne)
+            E, it, rr = self.ind.solve(self.Phi, E, self.dirichlet, dt, warm=True)
+            self.last_solve = (it, rr)
         self.Phi = dm.faraday_update(E, self.Phi, dt)
         dm.mars_implicit_sources(self.mp, q["Btot"], self.neutral, dt, self.U)
         dm.mars_floors(self.mp, self.U)

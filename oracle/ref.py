@@ -78,6 +78,8 @@ def lib():
             ("ref_mars_floors", [vp], ctypes.c_int),
             ("ref_mars_emf", [vp, vp], ctypes.c_int),
             ("ref_mars_step_nochem", [vp, dbl, vp], ctypes.c_int),
+            ("ref_mars_set_induction", [vp, dbl, i32, i32], ctypes.c_int),
+            ("ref_mars_last_solve", [vp, vp, vp], None),
             ("ref_mars_wall_table", [vp, vp, vp], i32),
             ("ref_mars_boundary", [vp, vp, vp], None),
             ("ref_limited_gradients_wall", [vp, vp, i32, vp, i32, dbl, i32, vp, vp, vp], ctypes.c_int),
@@ -482,7 +484,7 @@ def read_fields(path):
 
 MARS_PARAM_NAMES = ("rho_ref", "n_ref", "p_ref", "time_ref", "kB", "L", "U", "q", "B", "mag_scale", "pressure_scale", "ne_floor",
                     "rho_floor", "p_floor", "gamma", "cfl", "sw_ux", "sw_uy", "sw_uz", "sw_Bx", "sw_By", "sw_Bz", "ambipolar", "hall",
-                    "second_order", "cuct", "rel_limit")
+                    "second_order", "cuct", "rel_limit", "hall_scale")
 
 
 class RefMars:
@@ -550,6 +552,16 @@ class RefMars:
 
     def floors(self):
         _check(lib().ref_mars_floors(self._h))
+
+    def set_induction(self, rtol, max_it, restart):
+        """The Hall solve's GMRES settings (rtol, iteration limit, restart)."""
+        _check(lib().ref_mars_set_induction(self._h, float(rtol), int(max_it), int(restart)))
+
+    def last_solve(self):
+        """(GMRES iterations, relative residual) of the last step's Hall solve."""
+        it, res = ctypes.c_int32(), ctypes.c_double()
+        lib().ref_mars_last_solve(self._h, ctypes.byref(it), ctypes.byref(res))
+        return it.value, res.value
 
     def step_nochem(self, dt_max=1e300):
         d = np.zeros(1)

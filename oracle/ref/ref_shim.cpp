@@ -973,6 +973,8 @@ void ref_fields_get(int32_t i, char *name, int32_t len, int32_t *dim, int32_t *n
 
 struct RefMars
 {
+    int last_it = 0;     // the Hall solve of the last step: GMRES iterations and relative residual
+    double last_res = 0;
     mars::MarsParams prm;
     std::unique_ptr<mars::MarsSolver> s;
     std::vector<double> rhs_sum; // scratch
@@ -1000,14 +1002,14 @@ void *ref_mars_create(void *mesh, int32_t n_overrides, const char *const *overri
 void ref_mars_free(void *h) { delete static_cast<RefMars *>(h); }
 
 // the scales in the order of MhdMarsParams: rho_ref n_ref p_ref time_ref kB L U q B mag_scale pressure_scale
-// ne_floor rho_floor p_floor gamma, then cfl sw_u(3) sw_B(3) ambipolar hall second_order cuct rel_limit
+// ne_floor rho_floor p_floor gamma, then cfl sw_u(3) sw_B(3) ambipolar hall second_order cuct rel_limit hall_scale
 void ref_mars_params(void *h, double *out)
 {
     const mars::MarsParams &q = static_cast<RefMars *>(h)->prm;
     const double v[] = {q.rho_ref, q.n, q.p_ref, q.time_ref, q.kB, q.L, q.U, q.q, q.B, q.mag_scale, q.pressure_scale, q.ne_floor,
                         q.rho_floor, q.p_floor, q.cfg.sc.gamma, q.cfg.cfl, q.sw_u.x, q.sw_u.y, q.sw_u.z, q.sw_B.x, q.sw_B.y, q.sw_B.z,
                         q.ambipolar ? 1.0 : 0.0, q.hall ? 1.0 : 0.0, q.cfg.second_order ? 1.0 : 0.0, q.cfg.ideal.cuct,
-                        q.cfg.recon_rel_limit};
+                        q.cfg.recon_rel_limit, q.hall_scale};
     std::memcpy(out, v, sizeof(v));
 }
 
@@ -1101,8 +1103,27 @@ int ref_mars_emf(void *h, double *E)
     });
 }
 
-// MarsSolver::step (:705-744) without the photochemistry (chemistry_), the Hall solve only if the solver
-// has it on: prepare, dt, fluxes and explicit sources, EMF, forward Euler, Faraday, implicit sources, floors
+// The Hall solve's GMRES settings (the reference's Config defaults otherwise: rtol 1e-4, 100 iterations,
+// restart 20), for comparisons at the solver's tolerance
+int ref_mars_set_induction(void *h, double rtol, int32_t max_it, int32_t restart)
+{
+    return guarded([&] {
+        mars::MarsSolver &s = *static_cast<RefMars *>(h)->s;
+        s.ind_.rtol_ = rtol;
+        s.ind_.max_it_ = max_it;
+        s.ind_.restart_ = std::max(2, static_cast<int>(restart));
+    });
+}
+
+void ref_mars_last_solve(void *h, int32_t *it, double *res)
+{
+    *it = static_cast<RefMars *>(h)->last_it;
+    *res = static_cast<RefMars *>(h)->last_res;
+}
+
+// MarsSolver::step (:705-744) without the photochemistry (chemistry_), with the Hall solve when the solver
+// has it on: prepare, dt, fluxes and explicit sources, EMF, forward Euler, Hall solve, Faraday, implicit
+// sources, floors
 int ref_mars_step_nochem(void *h, double dt_max, double *dt_used)
 {
     return guarded([&] {
@@ -1120,7 +1141,20 @@ int ref_mars_step_nochem(void *h, double dt_max, double *dt_used)
                 if (cx.cell_material[c] == kSolid) continue;
                 for (int m = 0; m < 5; ++m) s.U_[k][5 * static_cast<std::size_t>(c) + m] += dt * s.rhs_[k][5 * static_cast<std::size_t>(c) + m];
             }
-        if (s.ind_.active()) throw std::runtime_error("the checker's ten-ion step runs without the Hall term");
+        if (s.ind_.active()) // the Hall branch of MarsSolver::step (:723-735) as the reference runs it
+        {
+            std::vector<double> ne(cx.n_cells(), 0.0);
+            for (Id c = 0; c < cx.n_cells(); ++c)
+                if (cx.cell_material[c] == kFluid) ne[c] = s.ne_eff_[c];
+            s.ind_.set_frozen_state(s.Btot_.data(), ne.data());
+            std::vector<char> dir(cx.n_edges(), 0);
+            for (Id e = 0; e < cx.n_edges(); ++e) dir[e] = s.bc_.edge_mode[e] != 0;
+            std::vector<double> Eimp = E;
+            double res = 0;
+            static_cast<RefMars *>(h)->last_it = s.ind_.solve(s.Phi_.data(), E.data(), dir, dt, Eimp.data(), &res);
+            static_cast<RefMars *>(h)->last_res = res;
+            E.swap(Eimp);
+        }
         faraday_update(cx, s.active_, E.data(), s.Phi_.data(), dt);
         s.implicit_sources_(dt);
         s.floors_();

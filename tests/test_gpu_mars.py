@@ -21,13 +21,13 @@ if not ref.available():
 NS = 10
 
 
-def _setup(second_order=1, ambipolar=1, seed=0):
+def _setup(second_order=1, ambipolar=1, seed=0, hall=0, induction=None):
     from mpcns_uns_b200 import gpu, workloads
     from mpcns_uns_b200.mars import MarsStep
     from mpcns_uns_b200.mesh import HostMesh
     h = HostMesh.shell(4, 5, 1.04, 3.0, tets=True).compute_geometry()
     r = ref_twin(h, SHELL_TAGS)
-    m = ref.RefMars(r, ["is_Hall_Efield=0", f"second_order={second_order}", "CFL=0.4", f"is_Ambipolar_Efield={ambipolar}"])
+    m = ref.RefMars(r, [f"is_Hall_Efield={hall}", f"second_order={second_order}", "CFL=0.4", f"is_Ambipolar_Efield={ambipolar}"])
     P = m.params
     u_inf = (P["sw_ux"], P["sw_uy"], P["sw_uz"])
     B_imf = (P["sw_Bx"], P["sw_By"], P["sw_Bz"])
@@ -53,7 +53,9 @@ def _setup(second_order=1, ambipolar=1, seed=0):
     m.set("U", U)
     m.set("Phi", Phi)
     scales = dict(P, u_inf=u_inf, B_imf=B_imf)
-    st = MarsStep(dm, scales, m.freestream, m.wall_table(), m.get("neutral"), m.get("PhiAdd"))
+    if induction:
+        m.set_induction(induction["rtol"], induction["max_it"], induction["restart"])
+    st = MarsStep(dm, scales, m.freestream, m.wall_table(), m.get("neutral"), m.get("PhiAdd"), induction=induction)
     st.set(U, Phi)
     return h, m, st
 
@@ -141,3 +143,39 @@ def test_mars_step():
         _per_ion(_np(st.U), m.get("U"))
         assert rel_err(_np(st.Phi), m.get("Phi")) < TOL
     assert st.dm.div_b(st.Phi)["max_rel"] < 1e-12
+
+
+def test_mars_step_with_hall_solve():
+    """MarsSolver::step with the Hall term on (is_Hall_Efield=1): the implicit edge EMF of the semi-implicit
+    induction solve (ImplicitInduction with the solver's hall_scale, no taper, wall and inflow edges fixed,
+    warm start across steps) between the explicit update and Faraday.  Both sides run GMRES(20) to 1e-10:
+    the dot products round differently (block reductions against sequential sums), so the solve agrees to
+    its tolerance, not bit for bit; U and Phi after three steps to 1e-8, iterations within 2."""
+    ind = dict(rtol=1e-10, max_it=400, restart=20)
+    h, m, st = _setup(seed=5, hall=1, induction=ind)
+    assert m.params["hall"] == 1.0 and m.params["hall_scale"] > 0 and st.ind is not None
+    for k in range(3):
+        dt_ref = m.step_nochem()
+        dt = st.step()
+        assert abs(dt - dt_ref) <= 1e-12 * dt_ref
+        it_ref, rr_ref = m.last_solve()
+        it, rr = st.last_solve
+        assert rr <= 1e-10 and rr_ref <= 1e-10, (rr, rr_ref)
+        assert abs(it - it_ref) <= 2, (k, it, it_ref)
+        _per_ion(_np(st.U), m.get("U"), 1e-8)
+        assert rel_err(_np(st.Phi), m.get("Phi")) < 1e-8
+    assert st.dm.div_b(st.Phi)["max_rel"] < 1e-12
+
+
+def test_mars_step_hall_default_settings():
+    """The same step at the reference's own GMRES settings (rtol 1e-4, 100 iterations, restart 20): both
+    sides stop at the tolerance after the same number of iterations within 2, and the states agree to the
+    solve's tolerance."""
+    h, m, st = _setup(seed=6, hall=1)
+    for k in range(2):
+        m.step_nochem()
+        st.step()
+        it_ref, rr_ref = m.last_solve()
+        it, rr = st.last_solve
+        assert rr <= 1e-4 and rr_ref <= 1e-4 and abs(it - it_ref) <= 2, (it, it_ref, rr, rr_ref)
+        assert rel_err(_np(st.Phi), m.get("Phi")) < 1e-4
