@@ -9,6 +9,9 @@
  * all work is ordered on the handle's CUDA stream (mhd_gpu_mesh_stream) and calls return
  * when it is enqueued, except calls with host outputs, which synchronise.
  *
+ * An array argument may be NULL where it holds no entries (an empty rank: no cells, faces or edges); the
+ * call then does nothing for it, as the reference's loops run zero times.
+ *
  * Status: 0 ok, MHD_EINVAL bad argument, MHD_ECUDA CUDA error, MHD_ESTATE non-finite or
  * invalid state detected, MHD_ENOCONV GMRES stopped at max_it above rtol (the solution and
  * its relative residual are still returned).  mhd_gpu_last_error() gives the message of the

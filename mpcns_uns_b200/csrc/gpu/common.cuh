@@ -32,6 +32,8 @@ void set_last_error(const std::string &msg);
     do {                                                                                                       \
         if (!(cond)) throw ::mhd::ApiError(MHD_EINVAL, msg);                                                   \
     } while (0)
+// an array argument: required unless it holds no entries (an empty rank's vectors may have no storage)
+#define MHD_ARR(p, n) ((p) != nullptr || (n) == 0)
 #define MHD_LAUNCH_CHECK() MHD_CUDA(cudaGetLastError())
 
 template <class F> int guarded(F &&f)

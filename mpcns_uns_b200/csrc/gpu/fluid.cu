@@ -409,7 +409,7 @@ extern "C" {
 int mhd_gpu_to_prim(MhdMesh *mesh, const double *U, int32_t n, double gamma, double rho_floor, double p_floor, double *W)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && U && W && n >= 0, "bad argument");
+        MHD_REQUIRE(mesh && n >= 0 && MHD_ARR(U, n) && MHD_ARR(W, n), "bad argument");
         if (!n) return;
         k_to_prim<<<grid_for(n, 256), 256, 0, mesh->stream>>>(SField<const double>{U, 0, 5, 1}, SField<double>{W, 0, 5, 1}, n, 1,
                                                               gamma, rho_floor, p_floor);
@@ -421,7 +421,7 @@ int mhd_gpu_limited_gradients(MhdMesh *mesh, const double *W, int32_t species, c
                               double *grad)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && W && grad && fs, "bad argument");
+        MHD_REQUIRE(mesh && fs && MHD_ARR(W, mesh->v.nc) && MHD_ARR(grad, mesh->v.nc), "bad argument");
         MHD_REQUIRE(species >= 0, "negative species");
         const MeshView &m = mesh->v;
         if (!m.nc) return;
@@ -434,7 +434,7 @@ int mhd_gpu_limited_gradients_wall(MhdMesh *mesh, const double *W, int32_t speci
                                    int32_t n_wall, const int32_t *wall_faces, const double *wall_prims, double *grad)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && W && grad && fs, "bad argument");
+        MHD_REQUIRE(mesh && fs && MHD_ARR(W, mesh->v.nc) && MHD_ARR(grad, mesh->v.nc), "bad argument");
         MHD_REQUIRE(species >= 0, "negative species");
         MHD_REQUIRE(n_wall >= 0 && (!n_wall || (wall_faces && wall_prims)), "bad wall ghost table");
         const MeshView &m = mesh->v;
@@ -455,7 +455,7 @@ int mhd_gpu_flux_rhs_wall(MhdMesh *mesh, double gamma, int32_t species, const Mh
                           int32_t n_wall, const int32_t *wall_faces, const double *wall_prims, double *rhs)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && W && grad && rhs && fs, "bad argument");
+        MHD_REQUIRE(mesh && fs && MHD_ARR(W, mesh->v.nc) && MHD_ARR(grad, mesh->v.nc) && MHD_ARR(rhs, mesh->v.nc), "bad argument");
         MHD_REQUIRE(gamma > 1.0, "gamma must exceed 1");
         MHD_REQUIRE(n_wall >= 0 && (!n_wall || (wall_faces && wall_prims)), "bad wall ghost table");
         const MeshView &m = mesh->v;
@@ -480,7 +480,7 @@ int mhd_gpu_flux_rhs_wall(MhdMesh *mesh, double gamma, int32_t species, const Mh
 int mhd_gpu_flux_rhs(MhdMesh *mesh, double gamma, int32_t species, const MhdPrim *fs, const double *W, const double *grad, double *rhs)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && W && grad && rhs && fs, "bad argument");
+        MHD_REQUIRE(mesh && fs && MHD_ARR(W, mesh->v.nc) && MHD_ARR(grad, mesh->v.nc) && MHD_ARR(rhs, mesh->v.nc), "bad argument");
         MHD_REQUIRE(gamma > 1.0, "gamma must exceed 1");
         const MeshView &m = mesh->v;
         if (!m.nc) return;

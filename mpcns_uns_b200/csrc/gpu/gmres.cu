@@ -598,7 +598,7 @@ int mhd_gpu_induction_destroy(MhdInduction *I)
 int mhd_gpu_induction_set_frozen(MhdInduction *I, const double *B0, const double *ne_eff)
 {
     return guarded([&] {
-        MHD_REQUIRE(I && B0 && ne_eff, "null argument");
+        MHD_REQUIRE(I && MHD_ARR(B0, I->mesh->v.nc) && MHD_ARR(ne_eff, I->mesh->v.nc), "null argument");
         const MeshView &m = I->mesh->v;
         cudaStream_t s = I->mesh->stream;
         if (!m.nc) return;
@@ -616,7 +616,7 @@ int mhd_gpu_induction_set_frozen(MhdInduction *I, const double *B0, const double
 int mhd_gpu_induction_set_frozen_alpha(MhdInduction *I, const double *B0, const double *alpha)
 {
     return guarded([&] {
-        MHD_REQUIRE(I && B0 && alpha, "null argument");
+        MHD_REQUIRE(I && MHD_ARR(B0, I->mesh->v.nc) && MHD_ARR(alpha, I->mesh->v.nc), "null argument");
         const MeshView &m = I->mesh->v;
         cudaStream_t s = I->mesh->stream;
         if (!m.nc) return;
@@ -634,7 +634,7 @@ int mhd_gpu_induction_set_frozen_alpha(MhdInduction *I, const double *B0, const 
 int mhd_gpu_induction_apply_F(MhdInduction *I, const double *phi, double *out)
 {
     return guarded([&] {
-        MHD_REQUIRE(I && phi && out, "null argument");
+        MHD_REQUIRE(I && MHD_ARR(phi, I->mesh->v.ne) && MHD_ARR(out, I->mesh->v.ne), "null argument");
         op64(I, MatIn{}, phi, 0.0, out);
         MHD_LAUNCH_CHECK();
     });
@@ -643,7 +643,7 @@ int mhd_gpu_induction_apply_F(MhdInduction *I, const double *phi, double *out)
 int mhd_gpu_induction_apply_A(MhdInduction *I, const double *x, double dt, double *y)
 {
     return guarded([&] {
-        MHD_REQUIRE(I && x && y, "null argument");
+        MHD_REQUIRE(I && MHD_ARR(x, I->mesh->v.ne) && MHD_ARR(y, I->mesh->v.ne), "null argument");
         apply_plain(I, x, dt, y);
         MHD_LAUNCH_CHECK();
     });
@@ -654,7 +654,9 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
 {
     int status = MHD_OK;
     int rc = guarded([&] {
-        MHD_REQUIRE(I && Phi && Ee && dir && E, "null argument");
+        MHD_REQUIRE(I && MHD_ARR(Phi, I->mesh->v.nf) && MHD_ARR(Ee, I->mesh->v.ne) && MHD_ARR(dir, I->mesh->v.ne) &&
+                        MHD_ARR(E, I->mesh->v.ne),
+                    "null argument");
         const MeshView &m = I->mesh->v;
         cudaStream_t s = I->mesh->stream;
         const int32_t ne = m.ne;

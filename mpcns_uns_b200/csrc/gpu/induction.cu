@@ -596,7 +596,7 @@ extern "C" {
 int mhd_gpu_cell_vector(MhdMesh *mesh, const double *flux, int32_t ncells, double *out)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && flux && out, "bad argument");
+        MHD_REQUIRE(mesh && MHD_ARR(flux, mesh->v.nf) && MHD_ARR(out, ncells), "bad argument");
         MHD_REQUIRE(ncells >= 0 && ncells <= mesh->v.nc, "ncells out of range");
         if (!ncells) return;
         k_cell_vector<<<grid_for(ncells, 128), 128, 0, mesh->stream>>>(mesh->v, flux, ncells, out);
@@ -608,7 +608,9 @@ int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const do
                       double cuct, double *E)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && u && Bt && Bi && phi_tot && phi_ind && E, "bad argument");
+        MHD_REQUIRE(mesh && MHD_ARR(u, mesh->v.nc) && MHD_ARR(Bt, mesh->v.nc) && MHD_ARR(Bi, mesh->v.nc) && MHD_ARR(phi_tot, mesh->v.nf) &&
+                        MHD_ARR(phi_ind, mesh->v.nf) && MHD_ARR(E, mesh->v.ne),
+                    "bad argument");
         const MeshView &m = mesh->v;
         if (!m.nf) return;
         mesh->scratch_face3.alloc(3 * static_cast<size_t>(m.nf));
@@ -629,7 +631,7 @@ int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const do
 int mhd_gpu_edge_modes(MhdMesh *mesh, const double *u_inf, const double *B_imf, double *E)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && u_inf && B_imf && E, "bad argument");
+        MHD_REQUIRE(mesh && u_inf && B_imf && MHD_ARR(E, mesh->v.ne), "bad argument");
         if (!mesh->v.no_edges) return;
         const V3 ui = mk(u_inf[0], u_inf[1], u_inf[2]), bi = mk(B_imf[0], B_imf[1], B_imf[2]);
         const V3 Einf = -1.0 * cross(ui, bi);
@@ -641,7 +643,7 @@ int mhd_gpu_edge_modes(MhdMesh *mesh, const double *u_inf, const double *B_imf, 
 int mhd_gpu_faraday(MhdMesh *mesh, const double *E, double *B, double dt)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && E && B, "bad argument");
+        MHD_REQUIRE(mesh && MHD_ARR(E, mesh->v.ne) && MHD_ARR(B, mesh->v.nf), "bad argument");
         if (!mesh->v.nf) return;
         k_faraday<<<grid_for(mesh->v.nf, 256), 256, 0, mesh->stream>>>(mesh->v, E, nullptr, dt, B);
         MHD_LAUNCH_CHECK();
@@ -651,7 +653,7 @@ int mhd_gpu_faraday(MhdMesh *mesh, const double *E, double *B, double dt)
 int mhd_gpu_faraday_edge_dt(MhdMesh *mesh, const double *E, const double *dt_edge, double *B)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && E && B && dt_edge, "bad argument");
+        MHD_REQUIRE(mesh && MHD_ARR(E, mesh->v.ne) && MHD_ARR(B, mesh->v.nf) && MHD_ARR(dt_edge, mesh->v.ne), "bad argument");
         if (!mesh->v.nf) return;
         k_faraday<<<grid_for(mesh->v.nf, 256), 256, 0, mesh->stream>>>(mesh->v, E, dt_edge, 0.0, B);
         MHD_LAUNCH_CHECK();
@@ -661,7 +663,7 @@ int mhd_gpu_faraday_edge_dt(MhdMesh *mesh, const double *E, const double *dt_edg
 int mhd_gpu_div_b(MhdMesh *mesh, const double *B, const double *extra, double *host_out)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && B && host_out, "bad argument");
+        MHD_REQUIRE(mesh && host_out && MHD_ARR(B, mesh->v.nf), "bad argument");
         const MeshView &m = mesh->v;
         if (!m.no_cells)
         {
@@ -710,7 +712,7 @@ int mhd_gpu_alloc_calls(int64_t *out)
 int mhd_gpu_div_b_noalloc(MhdMesh *mesh, const double *B, const double *extra, double *host_out)
 {
     return guarded([&] {
-        MHD_REQUIRE(mesh && B && host_out, "bad argument");
+        MHD_REQUIRE(mesh && host_out && MHD_ARR(B, mesh->v.nf), "bad argument");
         const MeshView &m = mesh->v;
         if (!m.no_cells)
         {

@@ -540,7 +540,7 @@ int mhd_gpu_state_create(MhdMesh *mesh, const MhdStepParams *p, MhdState **out)
         st->mixed = p->precision == MHD_PREC_MIXED;
         if (st->mixed)
         {
-            MHD_REQUIRE(m.faces_per_cell == 4 && m.tri_faces, "mixed precision needs a tetrahedral mesh");
+            MHD_REQUIRE(!m.nc || (m.faces_per_cell == 4 && m.tri_faces), "mixed precision needs a tetrahedral mesh");
             MHD_REQUIRE(m.max_valence <= 8 && m.max_edge_cells <= 8, "mixed precision needs edge valence <= 8");
             mixed_setup(st);
         }
@@ -583,10 +583,18 @@ int mhd_gpu_state_destroy(MhdState *st)
     });
 }
 
+// entries of a field's host array (0 for an unknown field)
+static size_t field_count(const MhdState *st, int32_t field)
+{
+    const MeshView &m = st->mesh->v;
+    return field == MHD_FIELD_U ? 5 * (size_t)m.nc : field == MHD_FIELD_BADD ? 3 * (size_t)m.nc
+                                                                             : (field == MHD_FIELD_PHI || field == MHD_FIELD_PHIADD) ? (size_t)m.nf : 0;
+}
+
 int mhd_gpu_state_upload(MhdState *st, int32_t field, int32_t species, const double *host)
 {
     return guarded([&] {
-        MHD_REQUIRE(st && host, "null argument");
+        MHD_REQUIRE(st && MHD_ARR(host, field_count(st, field)), "null argument");
         const MeshView &m = st->mesh->v;
         cudaStream_t s = st->mesh->stream;
         if (field == MHD_FIELD_U)
@@ -598,10 +606,12 @@ int mhd_gpu_state_upload(MhdState *st, int32_t field, int32_t species, const dou
             MHD_LAUNCH_CHECK();
         }
         else if (field == MHD_FIELD_PHI)
-            MHD_CUDA(cudaMemcpyAsync(st->phi0.p, host, (size_t)m.nf * sizeof(double), cudaMemcpyHostToDevice, s));
+        {
+            if (m.nf) MHD_CUDA(cudaMemcpyAsync(st->phi0.p, host, (size_t)m.nf * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
         else if (field == MHD_FIELD_PHIADD)
         {
-            MHD_CUDA(cudaMemcpyAsync(st->phi_add.p, host, (size_t)m.nf * sizeof(double), cudaMemcpyHostToDevice, s));
+            if (m.nf) MHD_CUDA(cudaMemcpyAsync(st->phi_add.p, host, (size_t)m.nf * sizeof(double), cudaMemcpyHostToDevice, s));
             // BaddCell = reconstruct_cell_vector(PhiAdd) (MercuryUns/initial/Initial.cpp:82-83)
             if (m.nc) k_cell_vector_all<<<grid_for(m.nc, 128), 128, 0, s>>>(m, st->phi_add.p, st->badd.p);
             MHD_LAUNCH_CHECK();
@@ -616,7 +626,7 @@ int mhd_gpu_state_upload(MhdState *st, int32_t field, int32_t species, const dou
 int mhd_gpu_state_download(MhdState *st, int32_t field, int32_t species, double *host)
 {
     return guarded([&] {
-        MHD_REQUIRE(st && host, "null argument");
+        MHD_REQUIRE(st && MHD_ARR(host, field_count(st, field)), "null argument");
         const MeshView &m = st->mesh->v;
         cudaStream_t s = st->mesh->stream;
         if (field == MHD_FIELD_U)
@@ -628,11 +638,17 @@ int mhd_gpu_state_download(MhdState *st, int32_t field, int32_t species, double 
             MHD_CUDA(cudaMemcpyAsync(host, st->stage.p, 5 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToHost, s));
         }
         else if (field == MHD_FIELD_PHI)
-            MHD_CUDA(cudaMemcpyAsync(host, st->phi0.p, (size_t)m.nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        {
+            if (m.nf) MHD_CUDA(cudaMemcpyAsync(host, st->phi0.p, (size_t)m.nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
         else if (field == MHD_FIELD_PHIADD)
-            MHD_CUDA(cudaMemcpyAsync(host, st->phi_add.p, (size_t)m.nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        {
+            if (m.nf) MHD_CUDA(cudaMemcpyAsync(host, st->phi_add.p, (size_t)m.nf * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
         else if (field == MHD_FIELD_BADD)
-            MHD_CUDA(cudaMemcpyAsync(host, st->badd.p, 3 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+        {
+            if (m.nc) MHD_CUDA(cudaMemcpyAsync(host, st->badd.p, 3 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
         else
             MHD_REQUIRE(false, "unknown field");
         MHD_CUDA(cudaStreamSynchronize(s));

@@ -234,7 +234,7 @@ class HostMesh:
             return self._cache[name]
         n = ctypes.c_int64()
         p = lib().mhdm_array(self._h, name.encode(), ctypes.byref(n))
-        if not p or n.value < 0:
+        if n.value < 0 or (not p and n.value > 0):
             raise KeyError(name)
         if name.endswith("_ptr"):
             dt = np.int64

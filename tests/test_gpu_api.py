@@ -317,3 +317,38 @@ def test_div_b_worst_cell_after_renumbering():
         assert abs(g["max_rel"] - rr["max_rel"]) <= TOL * rr["max_rel"]
         assert g["worst_cell_gid"] == rr["worst_cell_gid"] and order[g["worst_cell"]] == rr["worst_cell_gid"]
         assert g["worst_cell"] != rr["worst_cell_gid"] or order[g["worst_cell"]] == g["worst_cell"]
+
+
+def test_empty_mesh_every_entry_point():
+    """A rank with no cells (a partition can leave one empty): every entry point accepts the empty mesh and
+    returns empty results without launching on empty grids, as the reference's loops run zero times."""
+    import torch
+    from mpcns_uns_b200 import gpu
+    h = HostMesh.from_cells(np.zeros((0, 3)), [])
+    h.compute_geometry()
+    h.boundary("outflow")
+    assert (h.n_cells, h.n_faces, h.n_edges) == (0, 0, 0)
+    dm = gpu.DeviceMesh(h)
+    e = np.zeros(0)
+    fs = (1.0, 0.0, 0.0, 0.0, 1.0)
+    W = dm.to_prim(e, 5.0 / 3.0)
+    g = dm.limited_gradients(W, 0, fs)
+    rhs = dm.fluid_flux_rhs(5.0 / 3.0, 0, fs, W, g)
+    B = dm.reconstruct_cell_vector(e)
+    E = dm.add_ideal_emf(e, e, e, e, e)
+    E = dm.edge_modes((1.0, 0.0, 0.0), (0.0, 0.0, 1.0), E)
+    Bn = dm.faraday_update(E, e, 0.1)
+    for a in (W, g, rhs, B, E, Bn):
+        assert int(torch.as_tensor(a).numel()) == 0
+    d = dm.div_b(e)
+    assert d["max_abs"] == 0.0
+    for precision in ("fp64", "mixed"):
+        p = gpu.step_params(1, 5.0 / 3.0, fs=[fs], precision=precision)
+        st = gpu.ResidentState(dm, p)
+        st.set([e], e, e)
+        assert st.step(1e-3) == 1e-3
+        assert st.U(0).size == 0 and st.Phi().size == 0
+    ind = gpu.DeviceInduction(dm, np.zeros(0), hall=True, hall_coef=1.0, rtol=1e-8)
+    ind.set_frozen_state(e, e)
+    E2, it, rr = ind.solve(e, e, np.zeros(0, np.int8), 1e-3)
+    assert int(E2.numel()) == 0
