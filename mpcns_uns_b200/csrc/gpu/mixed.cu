@@ -219,7 +219,6 @@ struct MxParams
     int8_t absorb[kMaxSpecies];
     float mass[kMaxSpecies];
     float M_ref;
-    int update_ng;              // species in the group of the flux records the update gathers
     int src_on;                 // two-ion J x B force (species 0 = H+, 1 = Na+)
     float inver_MA2, ne_floor;
     int ambi, chem;             // ambipolar force, chemistry terms (two-ion model)
@@ -909,7 +908,7 @@ __global__ void __launch_bounds__(128) k_mx_flux(MV m, MxParams p, int s0, int n
 template <bool GYR>
 __global__ void __launch_bounds__(128) k_mx_update(MV m, MxParams p, int s0, int ng, const float *__restrict__ F,
                                                    const double *__restrict__ Ub, double *__restrict__ Uo, const double *__restrict__ dtp,
-                                                   int stage2, const float4 *__restrict__ W, const float4 *__restrict__ G,
+                                                   int stage2, const float4 *__restrict__ G,
                                                    const float4 *__restrict__ bt, SrcParams sp, int gyr, const float4 *__restrict__ D,
                                                    const double *__restrict__ photo, const double *__restrict__ vst)
 {
@@ -1203,9 +1202,7 @@ void mixed_stage(MhdState *st, const double *Us, const double *phis, double *Uo,
         P.begin(KP_UPDATE, s);
         // the instance with the closing gyration fused carries its registers; the other stages use the lean one
         auto upd = gyrate_close && s0 == 0 ? k_mx_update<true> : k_mx_update<false>;
-        MxParams pu = p;
-        pu.update_ng = ng;
-        upd<<<gc, 128, 0, s>>>(m, pu, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, W4, st->g32.p, st->bt32.p, st->src,
+        upd<<<gc, 128, 0, s>>>(m, p, s0, ng, st->F32.p, Us, Uo, st->scal.p, stage2 ? 1 : 0, st->g32.p, st->bt32.p, st->src,
                                gyrate_close && s0 == 0 ? 1 : 0, st->src.ambi ? st->d32.p : nullptr,
                                st->src.chem && st->photo.n ? st->photo.p : nullptr, st->src.chem && st->vst.n ? st->vst.p : nullptr);
         MHD_LAUNCH_CHECK();
