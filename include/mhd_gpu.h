@@ -268,6 +268,39 @@ int mhd_gpu_induction_launches(MhdInduction *ind, int64_t *out);
 /* Gram-Schmidt second passes (re-orthogonalisations) the last solve ran; no GPU work. */
 int mhd_gpu_induction_last_solve_stats(MhdInduction *ind, int32_t *reorth_passes);
 
+/* Block-Jacobi ILU(0) preconditioner of I + dt M d1^T S2 d1 on the owned edges (couplings to other ranks
+ * and the Hall part dropped): Config::ind_ilu / ind_ilu_shift (Common/config/Config.h:38-39).  enable != 0
+ * builds the pattern (ImplicitInduction::build_precond_pattern, .cpp:209-242, on the host from the mesh's
+ * e2f / f2e rows, star2 and the handle's m_e) and makes every later solve factor it for its dt and
+ * Dirichlet flags (factor_precond, :247-275) and precondition with it (apply_precond, :277-297) in place of
+ * the Jacobi diagonal, as solve() does with use_ilu_ (:317-318, 337, 374).  The factorisation and the two
+ * triangular solves run on the device with the reference's arithmetic per row (bit-identical factors
+ * and results), one thread per row, rows taken in the order of their dependency levels; a wait on
+ * another row gives up after 2 s (MHD_ECUDA, "ILU(0) pass timed out"), which no valid input reaches.
+ * Rows longer than 64 entries are rejected (MHD_EINVAL).  Both precisions use the FP64 factors. */
+int mhd_gpu_induction_set_ilu(MhdInduction *ind, int32_t enable, double shift);
+/* factor_precond(dt, dir) alone (dirichlet: device int8 array, NULL: none); then apply_precond of a device
+ * vector v into z (n_edges each; z = 0 on the non-owned edges).  The pattern must have been built. */
+int mhd_gpu_induction_ilu_factor(MhdInduction *ind, double dt, const int8_t *dirichlet);
+int mhd_gpu_induction_ilu_apply(MhdInduction *ind, const int8_t *dirichlet, const double *v, double *z);
+/* Test hook of the bounded waits: the wait limit (0 < wait_s <= 2; 2 by default) and one row whose warp
+ * never raises its flag (-1: none), so that the rows reading it give up and the call returns MHD_ECUDA
+ * ("ILU(0) pass timed out") with the handle usable again. */
+int mhd_gpu_induction_ilu_debug(MhdInduction *ind, double wait_s, int32_t unpublished_row);
+/* Launch shape of the ILU(0) passes: about window_levels dependency levels of rows in flight (default 2)
+ * and at most max_backoff_ns between two polls of an unfinished row (default 512). */
+int mhd_gpu_induction_ilu_tune(MhdInduction *ind, int32_t window_levels, int32_t max_backoff_ns);
+/* Host copies of the pattern and the current factors (pc_ptr_ n_owned+1, pc_col_ / pc_coef_ / pc_val_
+ * nnz, pc_diag_ n_owned); any output may be NULL; *n_owned and *nnz receive the sizes. */
+int mhd_gpu_induction_ilu_arrays(MhdInduction *ind, int32_t *n_owned, int64_t *nnz, int64_t *ptr, int32_t *col, double *coef,
+                                 double *val, int64_t *diag);
+/* build_precond_pattern on host arrays (no GPU work): rows of the n_owned first edges of the signed CSR
+ * e2f (edge -> faces) and f2e (face -> edges) with star2 per face and m_e per edge.  Call with col and
+ * coef NULL to get ptr (n_owned + 1 entries), then again with both sized ptr[n_owned]. */
+int mhd_ilu_pattern(int32_t n_edges, int32_t n_owned, int32_t n_faces, const int64_t *e2f_ptr, const int32_t *e2f_idx,
+                    const int8_t *e2f_sgn, const int64_t *f2e_ptr, const int32_t *f2e_idx, const int8_t *f2e_sgn,
+                    const double *star2, const double *m_edge, int64_t *ptr, int32_t *col, double *coef);
+
 /* ------------------------------------------------------------------ resident state, fused step
  * The explicit step of mercury::Solver::step (MercuryUns/driver/Solver.cpp:481-516) restricted to
  * the hot path (prepare :94-125 without the current, rhs :132-169 without model sources, advance

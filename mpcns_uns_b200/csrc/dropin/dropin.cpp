@@ -22,7 +22,7 @@
 //
 // Not covered by the C-ABI, and reported as std::runtime_error (the reference's error convention): a
 // non-empty GhostFn (the ten-ion solver's wall table has its own entry points), the per-edge dt_edge form
-// of ImplicitInduction::solve, its implicit-ideal part, and the block-ILU(0) preconditioner.
+// of ImplicitInduction::solve and its implicit-ideal part.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -273,8 +273,8 @@ struct IndEntry
 {
     MhdInduction *ind = nullptr;
     MhdMesh *mesh = nullptr;
-    bool hall = false, resistive = false;
-    double hall_coef = 0, rtol = 0;
+    bool hall = false, resistive = false, ilu = false;
+    double hall_coef = 0, rtol = 0, shift = 0;
     int max_it = 0, restart = 0;
     std::vector<double> m;
     ~IndEntry()
@@ -291,15 +291,16 @@ int ImplicitInduction::solve(const double *Phi_n, const double *E_expl, const st
 {
     if (dt_edge) throw std::runtime_error("mhd_gpu drop-in: the per-edge dt_edge form of ImplicitInduction::solve is not in the C-ABI");
     if (ideal_) throw std::runtime_error("mhd_gpu drop-in: the implicit ideal part of ImplicitInduction is not in the C-ABI");
-    if (use_ilu_) throw std::runtime_error("mhd_gpu drop-in: the block-ILU(0) preconditioner is not in the C-ABI (Jacobi only)");
+    // the block-ILU(0) preconditioner where the object built its pattern (:102, :317)
+    const bool ilu = use_ilu_ && !pc_ptr_.empty();
     Entry &e = mhd_dropin::find(lm_.mesh.cx);
     IndEntry *ie = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_ind_mu);
         auto &slot = g_ind[this];
         if (slot && !(slot->mesh == e.mesh && slot->hall == hall_ && slot->resistive == resistive_ && slot->hall_coef == hall_coef_ &&
-                      slot->rtol == rtol_ && slot->max_it == max_it_ && slot->restart == restart_ &&
-                      (!resistive_ || slot->m == m_)))
+                      slot->rtol == rtol_ && slot->max_it == max_it_ && slot->restart == restart_ && slot->ilu == ilu &&
+                      (!ilu || slot->shift == shift_) && (!resistive_ || slot->m == m_)))
             slot.reset();
         if (!slot)
         {
@@ -311,6 +312,8 @@ int ImplicitInduction::solve(const double *Phi_n, const double *E_expl, const st
             slot->rtol = rtol_;
             slot->max_it = max_it_;
             slot->restart = restart_;
+            slot->ilu = ilu;
+            slot->shift = shift_;
             if (resistive_) slot->m = m_;
             MhdInductionParams p{};
             p.hall = hall_ ? 1 : 0;
@@ -323,6 +326,7 @@ int ImplicitInduction::solve(const double *Phi_n, const double *E_expl, const st
             p.hall_r_min = -1.0;
             p.hall_r_max = -1.0;
             mhd_dropin::ok(mhd_gpu_induction_create(e.mesh, &p, resistive_ ? m_.data() : nullptr, &slot->ind));
+            if (ilu) mhd_dropin::ok(mhd_gpu_induction_set_ilu(slot->ind, 1, shift_));
         }
         ie = slot.get();
     }

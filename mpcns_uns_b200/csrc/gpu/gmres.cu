@@ -11,7 +11,9 @@
 // reference's sequential sums, so GMRES iterates agree to the solver tolerance, not bit for bit.
 //
 // Fusions of the Arnoldi step (each keeps the reference's arithmetic per element):
-//   * the Jacobi preconditioner z = dir ? 0 : V_j / (1 + dt m d2) is applied while gathering z in d1;
+//   * the Jacobi preconditioner z = dir ? 0 : V_j / (1 + dt m d2) is applied while gathering z in d1
+//     (with the block ILU(0) preconditioner on, z = M^-1 V_j comes from the triangular solves of ilu.cu,
+//     which store V_j, and the matvec gathers z itself);
 //   * V_j = w / H(j, j-1) is formed lazily in the next matvec (the face pass gathers w / h, the edge
 //     pass stores V_j), so w is not re-read to normalise it;
 //   * the edge pass zeroes the Dirichlet rows of w and produces H(0, j) = w . V_0;
@@ -321,6 +323,27 @@ __global__ void k_vec_update(const Ctl *ctl, int32_t n, const double *V, const d
     z[e] = x0[e] + d;
 }
 
+// comb = sum_i y_i V_i (:357-362), the input of the ILU(0) correction
+__global__ void k_vec_comb(const Ctl *ctl, int32_t n, const double *V, const double *y, double *comb)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const int j = ctl->jend;
+    double s = 0.0;
+    for (int i = 0; i < j; ++i) s += y[i] * V[(int64_t)i * n + e];
+    comb[e] = s;
+}
+
+// delta += M^-1 comb (:374); z = x0 + delta for the true residual
+__global__ void k_vec_addz(int32_t n, const double *pz, const double *x0, double *delta, double *z)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const double d = delta[e] + pz[e];
+    delta[e] = d;
+    z[e] = x0[e] + d;
+}
+
 // E = x0 + delta, corr = dir ? 0 : E - E_expl (:379-381)
 __global__ void k_vec_final(int32_t n, const double *x0, const double *delta, const double *Ee, const int8_t *dir, double *E, double *corr)
 {
@@ -401,13 +424,23 @@ void enqueue_cycle(MhdInduction *I)
         gt.ctl = I->ctl.p;
         gt.j = j;
         MatIn in;
-        in.src = j == 0 ? V : I->w.p;
-        in.hs = j == 0 ? nullptr : I->nrm.p + j;
-        in.pd = I->pd.p;
-        if (I->mixed) in.zs32 = I->zs32.p;
-        else in.zs = I->zs.p;
+        const bool ilu = I->ilu.on;
+        if (ilu)
+        {
+            // z = M^-1 V_j (:337) by the two triangular solves, V_j = w / H(j, j-1) stored on the way
+            ilu_apply(I, gt, j == 0 ? V : I->w.p, j == 0 ? nullptr : I->nrm.p + j, I->dirc.p, j == 0 ? nullptr : V + (int64_t)j * ne);
+            in.x = I->ilu.z.p;
+        }
+        else
+        {
+            in.src = j == 0 ? V : I->w.p;
+            in.hs = j == 0 ? nullptr : I->nrm.p + j;
+            in.pd = I->pd.p;
+            if (I->mixed) in.zs32 = I->zs32.p;
+            else in.zs = I->zs.p;
+        }
         Fused fz;
-        fz.vout = j == 0 ? nullptr : V + (int64_t)j * ne;
+        fz.vout = j == 0 || ilu ? nullptr : V + (int64_t)j * ne;
         fz.dir = I->dirc.p;
         const bool cgs = mr <= kCgsMax;
         fz.v0 = cgs ? nullptr : V;
@@ -674,6 +707,7 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         apply_plain(I, I->x0.p, dt, I->Ax.p);                                                     // A x0
         IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
         IND_LAUNCH(I, KI_VECTOR, s, k_vec_pd<<<ge, 256, 0, s>>>(ne, dt, I->mcoef.p, I->d2.p, dir, I->pd.p, I->dirc.p));
+        if (I->ilu.on) ilu_factor(I, dt, dir); // (:317-318)
         dev_dot(I, I->b.p, I->b.p, 2, sc + 0);
         dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
         MHD_LAUNCH_CHECK();
@@ -698,8 +732,15 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
             else
                 enqueue_cycle(I);
             IND_LAUNCH(I, KI_SCALAR, s, k_backsub<<<1, 1, 0, s>>>(I->ctl.p, I->H.p, mr, I->gv.p, I->yv.p, sc + 2));
-            IND_LAUNCH(I, KI_VECTOR, s,
-                       k_vec_update<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p));
+            if (I->ilu.on)
+            {
+                IND_LAUNCH(I, KI_VECTOR, s, k_vec_comb<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->w.p));
+                ilu_apply(I, Gate{}, I->w.p, nullptr, dir, nullptr);
+                IND_LAUNCH(I, KI_VECTOR, s, k_vec_addz<<<ge, 256, 0, s>>>(ne, I->ilu.z.p, I->x0.p, I->delta.p, I->z.p));
+            }
+            else
+                IND_LAUNCH(I, KI_VECTOR, s,
+                           k_vec_update<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p));
             // true residual in FP64 (the outer iterative refinement of the mixed-precision solve)
             apply_plain(I, I->z.p, dt, I->Ax.p);
             IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
@@ -713,6 +754,7 @@ int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee
         IND_LAUNCH(I, KI_VECTOR, s, k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p));
         MHD_LAUNCH_CHECK();
         MHD_CUDA(cudaStreamSynchronize(s));
+        if (I->ilu.on) ilu_check(I);
         I->have_corr = true;
         if (iterations) *iterations = total;
         if (rel_res) *rel_res = beta / bnorm;

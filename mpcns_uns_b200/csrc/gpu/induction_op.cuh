@@ -16,9 +16,9 @@ namespace mhd
 constexpr int kRedBlocks = 8 * 148; // streaming reductions: 8 resident 256-thread blocks per SM
 
 // kernel classes of the solve, timed with CUDA events on the handle's stream when profiling is on
-enum IndKernel { KI_FACE = 0, KI_BCELL, KI_HALL, KI_EDGE, KI_MGS, KI_SCALAR, KI_VECTOR, KI_COUNT };
-const char *const kIndKernelNames[KI_COUNT] = {"face_d1",      "cell_field",    "hall_emf",     "edge_gather",
-                                               "gram_schmidt", "krylov_scalar", "krylov_vector"};
+enum IndKernel { KI_FACE = 0, KI_BCELL, KI_HALL, KI_EDGE, KI_MGS, KI_SCALAR, KI_VECTOR, KI_ILU, KI_COUNT };
+const char *const kIndKernelNames[KI_COUNT] = {"face_d1",      "cell_field",    "hall_emf",      "edge_gather",
+                                               "gram_schmidt", "krylov_scalar", "krylov_vector", "ilu"};
 
 // Device-side control of one restart cycle: the Arnoldi steps of a cycle are enqueued (or replayed as
 // one CUDA graph) without host round trips; a step whose predecessor met the tolerance, or that lies
@@ -57,6 +57,35 @@ struct CgsArgs
 void cgs_launch(int j, const CgsArgs &a, const int *grid, cudaStream_t s, int pass);
 // the resident grids of column k's passes (2 ints), for an SM count
 void cgs_grids_for(int k, int sms, int *grid);
+
+// ---------------------------------------------------------------- block-Jacobi ILU(0) (ilu.cu)
+// Control of the row-ordered passes (factorisation, lower and upper solve): rows are claimed in order
+// through `ticket`; a finished row raises its flag to the pass's epoch; the last block of a pass resets
+// the ticket and advances the epoch.  err != 0: a wait gave up (the pass's results are invalid).
+struct IluCtl
+{
+    unsigned ticket, done, epoch, err;
+};
+constexpr int kIluMaxRow = 64; // longest row accepted
+struct IluState
+{
+    bool built = false, on = false;
+    double shift = 0.3;   // Config::ind_ilu_shift
+    int32_t no = 0;       // owned edges (the rows)
+    int64_t nnz = 0;
+    int32_t depth_l = 0, depth_u = 0; // levels of the lower / upper dependency order
+    int32_t npos_l = 0, npos_u = 0;   // positions of the level orders (levels padded to whole warps)
+    int grid_l = 0, grid_u = 0;       // blocks of the passes: a few levels of rows in flight
+    int64_t resident = 0;             // blocks of a pass resident on the device at once
+    int32_t window_levels = 2;        // levels of rows in flight
+    unsigned backoff_ns = 512;        // longest pause between two polls
+    uint64_t wait_ns = 2000000000ull; // a wait on another row gives up after this long
+    int32_t unpublished = -1;         // test hook: a row that never raises its flag
+    DBuf<int32_t> ptr, col, diag, order_l, order_u;
+    DBuf<double> coef, val, y, z; // y, z: results of the lower and upper solves (z = M^-1 v)
+    DBuf<unsigned> flag;
+    DBuf<IluCtl> ctl;
+};
 
 // ---------------------------------------------------------------- operator
 // Input of a matvec: x_e directly (apply_A), or the preconditioned Krylov vector
@@ -319,6 +348,7 @@ struct MhdInduction
     mhd::DBuf<int8_t> dirc;
     mhd::DBuf<unsigned> counter;
     mhd::DBuf<mhd::Ctl> ctl;
+    mhd::IluState ilu;
     double *pinned = nullptr;
     mhd::EventProfiler<mhd::KI_COUNT> prof;
     int64_t launches = 0;
@@ -362,4 +392,13 @@ struct Fused
 
 // the Arnoldi matvec with the FP32 operator (gmres32.cu)
 void op32(MhdInduction *I, const MatIn &in, double dt, double *y, const Fused &fz);
+
+// ILU(0) passes on the handle's stream (ilu.cu): factor_precond (:247-275) for dt and the Dirichlet flags;
+// apply_precond (:277-297) of v = dir ? 0 : src / *hs (hs may be null) into I->ilu.z, storing src / *hs to
+// vout when given (the lazily normalised Krylov vector); gated by gt inside a restart cycle.  The result
+// stays valid until the next application.
+void ilu_factor(MhdInduction *I, double dt, const int8_t *dir);
+void ilu_apply(MhdInduction *I, const Gate &gt, const double *src, const double *hs, const int8_t *dir, double *vout);
+// MHD_ECUDA if a wait of an ILU(0) pass gave up since the last check (synchronises the stream)
+void ilu_check(MhdInduction *I);
 } // namespace mhd

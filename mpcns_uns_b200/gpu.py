@@ -114,6 +114,13 @@ _SIGS = {
     "mhd_gpu_induction_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
     "mhd_gpu_induction_last_solve_stats": ([vp, ctypes.POINTER(i32)], ctypes.c_int),
+    "mhd_gpu_induction_set_ilu": ([vp, i32, dbl], ctypes.c_int),
+    "mhd_gpu_induction_ilu_factor": ([vp, dbl, vp], ctypes.c_int),
+    "mhd_gpu_induction_ilu_apply": ([vp, vp, vp, vp], ctypes.c_int),
+    "mhd_gpu_induction_ilu_debug": ([vp, dbl, i32], ctypes.c_int),
+    "mhd_gpu_induction_ilu_tune": ([vp, i32, i32], ctypes.c_int),
+    "mhd_gpu_induction_ilu_arrays": ([vp, ctypes.POINTER(i32), ctypes.POINTER(i64), vp, vp, vp, vp, vp], ctypes.c_int),
+    "mhd_ilu_pattern": ([i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_tet_build": ([i32, i64, vp, vp, i32, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_tet_build_counts": ([vp, vp], ctypes.c_int),
     "mhd_gpu_tet_build_copy": ([vp, vp], ctypes.c_int),
@@ -928,6 +935,71 @@ class DeviceInduction:
         v = i32()
         check(lib().mhd_gpu_induction_last_solve_stats(self._h, ctypes.byref(v)))
         return v.value
+
+    def set_ilu(self, enable=True, shift=0.3):
+        """Config::ind_ilu / ind_ilu_shift: block-Jacobi ILU(0) in place of the Jacobi preconditioner
+        (ImplicitInduction.cpp:209-297); builds the pattern on the first call."""
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_set_ilu(self._h, int(bool(enable)), float(shift)))
+        self.mesh._leave()
+
+    def _dir(self, dirichlet):
+        torch = _torch()
+        if dirichlet is None:
+            return None
+        if isinstance(dirichlet, torch.Tensor):
+            return dirichlet.to(torch.int8).contiguous().cuda()
+        return dev(np.ascontiguousarray(dirichlet, np.int8))
+
+    def ilu_factor(self, dt, dirichlet=None):
+        """factor_precond (:247-275) for dt and the Dirichlet flags."""
+        d = self._dir(dirichlet)
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_ilu_factor(self._h, float(dt), None if d is None else ptr(d)))
+        self.mesh._leave()
+
+    def ilu_apply(self, v, dirichlet=None):
+        """apply_precond (:277-297) with the current factors -> z (CUDA float64)."""
+        torch = _torch()
+        v, d = dev(v), self._dir(dirichlet)
+        z = torch.empty(self.mesh.n_edges, dtype=torch.float64, device="cuda")
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_ilu_apply(self._h, None if d is None else ptr(d), ptr(v), ptr(z)))
+        self.mesh._leave()
+        return z
+
+    def ilu_debug(self, wait_s=2.0, unpublished_row=-1):
+        """Test hook of the ILU(0) passes' bounded waits (mhd_gpu_induction_ilu_debug)."""
+        check(lib().mhd_gpu_induction_ilu_debug(self._h, float(wait_s), int(unpublished_row)))
+
+    def ilu_tune(self, window_levels=2, max_backoff_ns=512):
+        """Launch shape of the ILU(0) passes (mhd_gpu_induction_ilu_tune)."""
+        check(lib().mhd_gpu_induction_ilu_tune(self._h, int(window_levels), int(max_backoff_ns)))
+
+    def ilu_arrays(self):
+        """{pc_ptr, pc_col, pc_coef, pc_val, pc_diag} of the pattern and the current factors (host)."""
+        no, nnz = i32(), i64()
+        check(lib().mhd_gpu_induction_ilu_arrays(self._h, ctypes.byref(no), ctypes.byref(nnz), None, None, None, None, None))
+        out = dict(pc_ptr=np.zeros(no.value + 1, np.int64), pc_col=np.zeros(nnz.value, np.int32), pc_coef=np.zeros(nnz.value),
+                   pc_val=np.zeros(nnz.value), pc_diag=np.zeros(no.value, np.int64))
+        check(lib().mhd_gpu_induction_ilu_arrays(self._h, ctypes.byref(no), ctypes.byref(nnz),
+                                                 *[out[k].ctypes.data_as(vp) for k in ("pc_ptr", "pc_col", "pc_coef", "pc_val",
+                                                                                         "pc_diag")]))
+        return out
+
+
+def ilu_pattern(n_edges, n_owned, n_faces, e2f, f2e, star2, m_edge):
+    """ImplicitInduction::build_precond_pattern (Common/induction/ImplicitInduction.cpp:209-242) on host arrays
+    (no GPU work): e2f and f2e as (ptr int64, idx int32, sgn int8) -> (pc_ptr, pc_col, pc_coef)."""
+    a = [np.ascontiguousarray(e2f[0], np.int64), np.ascontiguousarray(e2f[1], np.int32), np.ascontiguousarray(e2f[2], np.int8),
+         np.ascontiguousarray(f2e[0], np.int64), np.ascontiguousarray(f2e[1], np.int32), np.ascontiguousarray(f2e[2], np.int8),
+         np.ascontiguousarray(star2, np.float64), np.ascontiguousarray(m_edge, np.float64)]
+    pp = np.zeros(n_owned + 1, np.int64)
+    args = [int(n_edges), int(n_owned), int(n_faces)] + [x.ctypes.data_as(vp) for x in a]
+    check(lib().mhd_ilu_pattern(*args, pp.ctypes.data_as(vp), None, None))
+    col, coef = np.zeros(int(pp[-1]), np.int32), np.zeros(int(pp[-1]))
+    check(lib().mhd_ilu_pattern(*args, pp.ctypes.data_as(vp), col.ctypes.data_as(vp), coef.ctypes.data_as(vp)))
+    return pp, col, coef
 
 
 class ComplexOut(ctypes.Structure):

@@ -99,6 +99,7 @@ def lib():
             ("ref_ind_apply_F", [vp, vp, vp], None),
             ("ref_ind_apply_A", [vp, vp, dbl, vp], None),
             ("ref_ind_solve", [vp, vp, vp, vp, dbl, i32, vp, vp], i32),
+            ("ref_ind_precond", [vp, dbl, vp, vp, vp], i32),
             ("ref_rk2_step", [vp, ctypes.POINTER(StepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
             ("ref_add_sources", [vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp], None),
             ("ref_electron_pressure_gradient", [vp, vp, vp, vp], None),
@@ -420,10 +421,18 @@ class RefInduction:
         n = lib().ref_ind_array(self._h, name.encode(), None)
         if n < 0:
             raise KeyError(name)
-        dt = np.int64 if name == "ce_ptr" else np.int32 if name == "ce_edge" else np.float64
+        dt = np.int64 if name in ("ce_ptr", "pc_ptr", "pc_diag") else np.int32 if name in ("ce_edge", "pc_col") else np.float64
         a = np.zeros(n, dt)
         lib().ref_ind_array(self._h, name.encode(), _p(a))
         return a
+
+    def precond(self, dt, dirichlet, v):
+        """factor_precond(dt, dir) then apply_precond(v) (ImplicitInduction.cpp:247-297) -> z."""
+        d = np.ascontiguousarray(dirichlet, np.int8)
+        v = np.ascontiguousarray(v, np.float64)
+        z = np.zeros(self.mesh.n_edges)
+        _check(lib().ref_ind_precond(self._h, float(dt), _p(d), _p(v), _p(z)))
+        return z
 
     def set_frozen_state(self, B0, ne):
         B0 = np.ascontiguousarray(B0, np.float64)

@@ -574,6 +574,25 @@ void ref_ind_set_m(void *h, const double *m)
     RefInd *ri = static_cast<RefInd *>(h);
     std::copy(m, m + ri->ind->m_.size(), ri->ind->m_.begin());
     ri->ind->resistive_ = true;
+    // the constructor built the ILU(0) pattern from its own m_ (:102): build it again from these
+    if (ri->ind->use_ilu_ && !ri->ind->ideal_) ri->ind->build_precond_pattern();
+}
+
+// ImplicitInduction::factor_precond (:247-275) for dt and dir, then apply_precond (:277-297) of v into z
+// (both n_edges); the pattern must exist (ilu on).
+int ref_ind_precond(void *h, double dt, const int8_t *dir, const double *v, double *z)
+{
+    return guarded([&] {
+        ImplicitInduction &I = *static_cast<RefInd *>(h)->ind;
+        if (I.pc_ptr_.empty()) throw std::runtime_error("no ILU(0) pattern");
+        const size_t ne = I.m_.size();
+        std::vector<char> d(ne);
+        for (size_t e = 0; e < ne; ++e) d[e] = dir ? dir[e] : 0;
+        I.factor_precond(dt, d);
+        std::vector<double> vv(v, v + ne), zz(ne, 0.0);
+        I.apply_precond(vv, zz, d);
+        std::copy(zz.begin(), zz.end(), z);
+    });
 }
 
 int64_t ref_ind_array(void *h, const char *cname, void *out)
@@ -589,6 +608,11 @@ int64_t ref_ind_array(void *h, const char *cname, void *out)
     if (n == "ce_edge") return put(I.ce_edge_, out);
     if (n == "ce_wt") return put3(I.ce_wt_, out);
     if (n == "corr") return put(I.corr_, out);
+    if (n == "pc_ptr") return put(I.pc_ptr_, out);
+    if (n == "pc_col") return put(I.pc_col_, out);
+    if (n == "pc_coef") return put(I.pc_coef_, out);
+    if (n == "pc_val") return put(I.pc_val_, out);
+    if (n == "pc_diag") return put(I.pc_diag_, out);
     return -1;
 }
 

@@ -133,13 +133,16 @@ def test_induction_signatures(mesh):
         assert int(o[2]) == rr["worst_cell_gid"]
 
 
-def test_implicit_induction_solve_signature(mesh):
+@pytest.mark.parametrize("ilu", [False, True])
+def test_implicit_induction_solve_signature(mesh, ilu):
     """ImplicitInduction::solve on the reference's object: the drop-in hands the object's resistivity, Hall
-    coefficient per cell (alpha_ = taper hall_coef / n_e,eff) and frozen field to the device solve."""
+    coefficient per cell (alpha_ = taper hall_coef / n_e,eff) and frozen field to the device solve, with the
+    object's preconditioner (Jacobi, or block ILU(0) when its Config asked for it)."""
     r, (lm, geo, bc, cfg, st) = mesh
     rng = np.random.default_rng(73)
     nc, nf, ne = r.n_cells, r.n_faces, r.n_edges
-    ri = ref.RefInduction(r, hall=True, hall_coef=0.5, hall_r_min=-100.0, hall_r_max=-99.0, rtol=1e-10, max_it=200, restart=15)
+    ri = ref.RefInduction(r, hall=True, hall_coef=0.5, hall_r_min=-100.0, hall_r_max=-99.0, rtol=1e-10, max_it=200, restart=15,
+                          ilu=ilu)
     ri.set_m(rng.uniform(0.5, 2.0, ne) / np.asarray(r["star1"]))
     ri.set_frozen_state(rng.uniform(-1, 1, 3 * nc), rng.uniform(0.5, 2.0, nc))
     phi = rng.uniform(-1, 1, nf)
