@@ -19,7 +19,8 @@ induction solve (ImplicitInduction::solve) on the cubed-sphere shell r in [0.8, 
 x 6 tetrahedra (7,962,624 cells, 9,331,392 edge unknowns), eta = 1 below r = 1 and 1e-3 above, Hall
 on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, cold start, capped at
 --gmres-max-it iterations: seconds per solve in FP64 and mixed precision, per-kernel GB/s, and the
-reference's own solve on a bounded sample beside it.
+reference's own solve on a bounded sample beside it; its "ilu" object is the same FP64 solve with the
+block ILU(0) preconditioner against Jacobi, both capped at --gmres-ilu-max-it iterations.
 
 The "ten_ion" object (left out with --no-ten-ion, alone with --ten-ion-only): the ten-ion shell r in
 [1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background field: mixed and FP64 steps and
@@ -389,7 +390,51 @@ def bench_gmres(args, peak):
     out["speedup_mixed"] = out["fp64"]["s_per_solve"] / out["mixed"]["s_per_solve"]
     out["E_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(E["mixed"] - E["fp64"]) / np.linalg.norm(E["fp64"]))
     out["rel_res_ratio_mixed_vs_fp64"] = out["mixed"]["rel_res"] / out["fp64"]["rel_res"]
+    if args.gmres_ilu_max_it > 0:
+        out["ilu"] = bench_gmres_ilu(args, case, dm)
     return out
+
+
+def bench_gmres_ilu(args, case, dm):
+    """The same FP64 solve with the block ILU(0) preconditioner (Config::ind_ilu, shift 0.3) against Jacobi, both
+    capped at --gmres-ilu-max-it iterations: host pattern time, device time of one factorisation and of one
+    application (both triangular solves), seconds per capped solve and the residual each preconditioner reaches."""
+    import torch
+    from mpcns_uns_b200 import gpu
+    il = {"max_it": args.gmres_ilu_max_it, "shift": 0.3}
+    for ilu in (False, True):
+        di = gpu.DeviceInduction(dm, case.m_edge, hall=True, hall_coef=case.hall_coef, hall_r_min=case.hall_r_min,
+                                 hall_r_max=case.hall_r_max, rtol=1e-8, max_it=args.gmres_ilu_max_it, restart=30)
+        di.set_frozen_state(case.B0, case.ne)
+        if ilu:
+            t = time.time()
+            di.set_ilu(True, 0.3)
+            il["pattern_s"] = time.time() - t
+        di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)  # warm-up (captures the cycle graph)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(dm.stream)
+        _, it, rr = di.solve(case.Phi, case.E_expl, case.dirichlet, case.dt, False)
+        ev1.record(dm.stream)
+        ev1.synchronize()
+        il["ilu" if ilu else "jacobi"] = {"s_per_solve": ev0.elapsed_time(ev1) / 1e3, "iterations": it, "rel_res": rr}
+        if ilu:
+            d = torch.tensor(case.dirichlet, device="cuda")
+            v = torch.rand(case.mesh.n_edges, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+            evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            evs[0].record(dm.stream)
+            di.ilu_factor(case.dt, d)
+            evs[1].record(dm.stream)
+            di.ilu_apply(v, d)
+            evs[2].record(dm.stream)
+            evs[2].synchronize()
+            il["factor_ms"] = evs[0].elapsed_time(evs[1])
+            il["apply_ms"] = evs[1].elapsed_time(evs[2])
+        del di
+    log(f"[bench] ILU(0) {il['max_it']} iterations: {il['ilu']['s_per_solve']:.3f} s, rel_res {il['ilu']['rel_res']:.3e} "
+        f"(Jacobi {il['jacobi']['s_per_solve']:.3f} s, {il['jacobi']['rel_res']:.3e}); factor {il['factor_ms']:.1f} ms, "
+        f"apply {il['apply_ms']:.2f} ms")
+    return il
 
 
 def bench_adjoint(args):
@@ -612,6 +657,11 @@ def summary(out):
                        for p in ("fp64", "mixed")}
         sm["gmres"]["speedup_mixed"] = _r(g["speedup_mixed"])
         sm["gmres"]["cols"] = "s_per_solve, iterations, rel_res, Gram-Schmidt second passes"
+        il = g.get("ilu")
+        if il:
+            sm["gmres"]["ilu"] = {"it": il["max_it"], "s": [_r(il["ilu"]["s_per_solve"]), _r(il["jacobi"]["s_per_solve"])],
+                                  "rel_res": [_r(il["ilu"]["rel_res"], 3), _r(il["jacobi"]["rel_res"], 3)],
+                                  "factor_apply_ms": [_r(il["factor_ms"]), _r(il["apply_ms"])]}
     d = out.get("adjoint")
     if d:
         fd = d["fd"]
@@ -658,6 +708,7 @@ def main():
     ap.add_argument("--gmres-nr", type=int, default=96)
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
+    ap.add_argument("--gmres-ilu-max-it", type=int, default=60, help="block ILU(0) leg against Jacobi (0: skip)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ten-ion", action="store_true", help="leave out the ten-ion shell (config 5, 42.5M cells)")
     ap.add_argument("--ten-ion-only", action="store_true", help="run only the ten-ion section and print it as its own JSON line")
