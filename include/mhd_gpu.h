@@ -257,8 +257,22 @@ int mhd_gpu_induction_apply_A(MhdInduction *ind, const double *x, double dt, dou
  * rel_res set) when max_it is reached above rtol, which the reference reports without throwing. */
 int mhd_gpu_induction_solve(MhdInduction *ind, const double *Phi, const double *E_expl, const int8_t *dirichlet, double dt,
                             int32_t warm, double *E, int32_t *iterations, double *rel_res);
+/* ImplicitInduction::solve with the per-edge pseudo-time step dt_edge (device, one per edge; the steady mode's
+ * local time stepping, .h:48-50): the system (I + F d1 diag(dt_e)) E = E_expl + F(Phi^n), the Jacobi scaling
+ * 1 / (1 + dt_e m_e d2_e), no ILU(0) (:317).  Otherwise as mhd_gpu_induction_solve. */
+int mhd_gpu_induction_solve_dt_edge(MhdInduction *ind, const double *Phi, const double *E_expl, const int8_t *dirichlet,
+                                    const double *dt_edge, int32_t warm, double *E, int32_t *iterations, double *rel_res);
+/* Implicit ideal induction (Config::implicit_ideal, ImplicitInduction::set_ideal_state, :112-116): the part
+ * of the ideal UCT EMF that is linear in the induced flux for frozen cell velocities u (3 per cell) joins
+ * F on the edges with mask != 0 (:150-158), with UCT strength cuct (IdealParams::cuct).  u and mask are
+ * copied (device arrays); u = NULL switches the part off.  While it is on, solves use the Jacobi
+ * preconditioner (the reference builds no ILU(0) pattern then, :102) and the mixed-precision solve runs
+ * its Arnoldi matvecs with the FP64 operator.  ideal_linear (:118-124): that part alone, L(phi) on
+ * every owned edge (0 on the others). */
+int mhd_gpu_induction_set_ideal(MhdInduction *ind, const double *u_cell, const int8_t *mask, double cuct);
+int mhd_gpu_induction_ideal_linear(MhdInduction *ind, const double *phi, double *out);
 /* Per-kernel-class device time of the solve (CUDA events on the mesh stream while enabled; classes:
- * face_d1, cell_field, hall_emf, edge_gather, gram_schmidt, krylov_scalar, krylov_vector; a profiled solve
+ * face_d1, cell_field, hall_emf, edge_gather, gram_schmidt, krylov_scalar, krylov_vector, ilu, ideal_emf; a profiled solve
  * launches its kernels one by one instead of replaying the restart-cycle graph), read as
  * in mhd_gpu_state_profile_read; and the number of kernels the handle has launched. */
 int mhd_gpu_induction_profile(MhdInduction *ind, int32_t enable);

@@ -21,8 +21,7 @@
 // another made at the same address is recognised by its counts and storage and gets a new handle.
 //
 // Not covered by the C-ABI, and reported as std::runtime_error (the reference's error convention): a
-// non-empty GhostFn (the ten-ion solver's wall table has its own entry points), the per-edge dt_edge form
-// of ImplicitInduction::solve and its implicit-ideal part.
+// non-empty GhostFn (the ten-ion solver's wall table has its own entry points).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -90,7 +89,7 @@ struct Entry
     // without detach) shows up as different counts or storage and gets a new handle
     std::array<int64_t, 4> counts{};
     const void *storage[3] = {};
-    Buf b[8];
+    Buf b[10];
     std::vector<int32_t> e2n; // start and end node of every edge (the descriptor's edge_nodes)
     ~Entry()
     {
@@ -263,8 +262,9 @@ DivBReport div_b(const uns::CellComplex &cx, const double *B, const double *scal
 
 // ImplicitInduction::solve (ImplicitInduction.cpp:299-390) on the device: the handle is made on the first solve
 // from the object's resistivity m_, Hall switch and GMRES settings; every solve hands over the frozen state
-// the object holds (B0_ and alpha_ = taper * hall_coef / n_e,eff of set_frozen_state).  use_guess_ maps to the
-// warm start.
+// the object holds (B0_ and alpha_ = taper * hall_coef / n_e,eff of set_frozen_state), and its implicit ideal
+// part (u_ideal_, ideal_mask_ of set_ideal_state) where it has one.  use_guess_ maps to the warm start; dt_edge
+// to the per-edge form of the solve.
 namespace
 {
 // The device handle of an ImplicitInduction object, with the settings it was made from: an object made
@@ -289,8 +289,6 @@ std::unordered_map<const ImplicitInduction *, std::unique_ptr<IndEntry>> g_ind;
 int ImplicitInduction::solve(const double *Phi_n, const double *E_expl, const std::vector<char> &dirichlet, double dt, double *E,
                              double *rel_res, const double *dt_edge)
 {
-    if (dt_edge) throw std::runtime_error("mhd_gpu drop-in: the per-edge dt_edge form of ImplicitInduction::solve is not in the C-ABI");
-    if (ideal_) throw std::runtime_error("mhd_gpu drop-in: the implicit ideal part of ImplicitInduction is not in the C-ABI");
     // the block-ILU(0) preconditioner where the object built its pattern (:102, :317)
     const bool ilu = use_ilu_ && !pc_ptr_.empty();
     Entry &e = mhd_dropin::find(lm_.mesh.cx);
@@ -334,13 +332,23 @@ int ImplicitInduction::solve(const double *Phi_n, const double *E_expl, const st
     const size_t nc = cx.n_cells(), nf = cx.n_faces(), ne = cx.n_edges();
     const double *dB0 = e.up(0, B0_.data(), 3 * nc), *dal = e.up(1, alpha_.data(), nc);
     mhd_dropin::ok(mhd_gpu_induction_set_frozen_alpha(ie->ind, dB0, dal));
+    // the implicit ideal part where the object has its frozen velocities (set_ideal_state, :112-116)
+    if (ideal_ && u_ideal_)
+    {
+        const double *du = e.up(6, u_ideal_, 3 * nc);
+        const int8_t *dm = e.up(7, reinterpret_cast<const int8_t *>(ideal_mask_.data()), ne);
+        mhd_dropin::ok(mhd_gpu_induction_set_ideal(ie->ind, du, dm, ideal_prm_.cuct));
+    }
+    else
+        mhd_dropin::ok(mhd_gpu_induction_set_ideal(ie->ind, nullptr, nullptr, ideal_prm_.cuct));
     const double *dPhi = e.up(2, Phi_n, nf), *dEe = e.up(3, E_expl, ne);
     static_assert(sizeof(char) == sizeof(int8_t), "char is one byte");
     const int8_t *ddir = e.up(4, reinterpret_cast<const int8_t *>(dirichlet.data()), ne);
     double *dE = e.b[5].get<double>(ne);
     int32_t it = 0;
     double rr = 0;
-    const int rc = mhd_gpu_induction_solve(ie->ind, dPhi, dEe, ddir, dt, use_guess_ ? 1 : 0, dE, &it, &rr);
+    const int rc = dt_edge ? mhd_gpu_induction_solve_dt_edge(ie->ind, dPhi, dEe, ddir, e.up(8, dt_edge, ne), use_guess_ ? 1 : 0, dE, &it, &rr)
+                           : mhd_gpu_induction_solve(ie->ind, dPhi, dEe, ddir, dt, use_guess_ ? 1 : 0, dE, &it, &rr);
     if (rc != MHD_OK && rc != MHD_ENOCONV) mhd_dropin::ok(rc);
     e.down(E, dE, ne);
     if (rel_res) *rel_res = rr;

@@ -238,12 +238,14 @@ __global__ void k_vec_resid(int32_t n, const double *b, const double *Ax, const 
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) r[i] = dir[i] ? 0.0 : b[i] - Ax[i];
 }
-// pd = dir ? 0 : 1 / (1 + dt m d2)  (Jacobi, :315-316); dirc = the caller's Dirichlet flags, kept for the cycle
-__global__ void k_vec_pd(int32_t n, double dt, const double *mc, const double *d2, const int8_t *dir, double *pd, int8_t *dirc)
+// pd = dir ? 0 : 1 / (1 + dt m d2), dt_e in place of dt when given (Jacobi, :315-316); dirc = the caller's
+// Dirichlet flags, kept for the cycle
+__global__ void k_vec_pd(int32_t n, double dt, const double *dte, const double *mc, const double *d2, const int8_t *dir, double *pd,
+                         int8_t *dirc)
 {
     const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    pd[i] = dir[i] ? 0.0 : 1.0 / (1.0 + dt * mc[i] * d2[i]);
+    pd[i] = dir[i] ? 0.0 : 1.0 / (1.0 + (dte ? dte[i] : dt) * mc[i] * d2[i]);
     dirc[i] = dir[i];
 }
 // V0 = r / beta, and the face pass's input V0 * pd
@@ -362,42 +364,57 @@ namespace mhd
 {
 namespace
 {
-// y = F(phi) (no input in `in`, phi given) or y = A x; optional fused outputs as in EdgeArgs.
-void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, double *y, const Fused &fz = Fused{})
+// y = F(phi) (no input in `in`, phi given) or y = A x; optional fused outputs as in EdgeArgs.  only_ideal: the
+// ideal part alone (ImplicitInduction::ideal_linear, :118-124).
+void op64(MhdInduction *I, const MatIn &in, const double *phi_in, double dt, double *y, const Fused &fz = Fused{}, bool only_ideal = false)
 {
     const MeshView &m = I->mesh->v;
     cudaStream_t s = I->mesh->stream;
+    const bool resistive = I->resistive && !only_ideal, hall = I->hall && !only_ideal, ideal = I->ideal;
     const double *phi = phi_in;
     if (in.x || in.src)
     {
         if (m.nf)
             IND_LAUNCH(I, KI_FACE, s, (m.tri_faces ? k_ind_face<double, true> : k_ind_face<double, false>)<<<g1(m.nf), 256, 0, s>>>(
-                                          m, fz.gt, in, I->hall, I->resistive, I->phi.p, I->s2phi.p));
+                                          m, fz.gt, in, hall || ideal, resistive, I->phi.p, I->s2phi.p));
         phi = I->phi.p;
     }
-    else if (I->resistive && m.nf)
+    else if (resistive && m.nf)
         IND_LAUNCH(I, KI_FACE, s, k_ind_s2phi<<<g1(m.nf), 256, 0, s>>>(m, phi, I->s2phi.p));
-    if (I->hall && m.nc)
-    {
+    // the cell field from the face fluxes (:138-149), for the Hall and the ideal parts
+    if ((hall || ideal) && m.nc)
         IND_LAUNCH(I, KI_BCELL, s, (m.faces_per_cell == 4 ? k_ind_bcell<double, true> : k_ind_bcell<double, false>)<<<g1(m.nc), 256, 0, s>>>(
                                        m, fz.gt, I->recon.p, phi, I->bcell.p));
-        if (m.no_cells)
-            IND_LAUNCH(I, KI_HALL, s,
-                       (m.faces_per_cell == 4 ? k_ind_hall<true> : k_ind_hall<false>)<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot_nb.p, I->slot_sa.p, I->bcell.p, I->alpha.p, I->B0.p,
-                                                                 I->g.p));
+    // the ideal EMF of the frozen velocities and the cell field of phi (:150-158); masked in the edge pass
+    if (ideal && m.ne)
+    {
+        IND_LAUNCH(I, KI_IDEAL, s, MHD_CUDA(cudaMemsetAsync(I->ide.p, 0, (size_t)m.ne * sizeof(double), s)));
+        IND_LAUNCH(I, KI_IDEAL, s,
+                   ideal_emf_enqueue(m, I->u_ideal.p, I->bcell.p, I->bcell.p, phi, phi, I->cuct, I->face3.p, I->ide.p, s));
+        if (m.no_edges) ++I->launches; // the enqueue is two kernels
     }
+    if (hall && m.nc && m.no_cells)
+        IND_LAUNCH(I, KI_HALL, s,
+                   (m.faces_per_cell == 4 ? k_ind_hall<true> : k_ind_hall<false>)<<<g1(m.no_cells), 256, 0, s>>>(m, fz.gt, I->slot_nb.p, I->slot_sa.p, I->bcell.p, I->alpha.p, I->B0.p,
+                                                                 I->g.p));
     EdgeArgs<double> a;
-    a.resistive = I->resistive; a.hall = I->hall;
+    a.resistive = resistive; a.hall = hall;
+    if (ideal)
+    {
+        a.ide = I->ide.p;
+        a.imask = I->imask.p;
+    }
     a.s2phi = I->s2phi.p; a.g = I->g.p; a.mcoef = I->mcoef.p; a.ecw = m.ec_weight; a.tvec = m.edge_vec;
     a.in = in; a.dt = dt; a.dtp = fz.dtp; a.vout = fz.vout; a.dir = fz.dir; a.v0 = fz.v0; a.dot = fz.dot; a.gt = fz.gt;
     a.part = I->part.p; a.counter = I->counter.p; a.out = y;
     if (m.ne) IND_LAUNCH(I, KI_EDGE, s, (m.max_valence <= 8 && m.max_edge_cells <= 8 ? k_ind_edge<double, 8> : k_ind_edge<double, 0>)<<<I->edge_blocks, 256, 0, s>>>(m, a));
 }
 
-void apply_plain(MhdInduction *I, const double *x, double dt, double *y)
+void apply_plain(MhdInduction *I, const double *x, double dt, double *y, const double *dte = nullptr)
 {
     MatIn in;
     in.x = x;
+    in.dte = dte;
     op64(I, in, nullptr, dt, y);
 }
 
@@ -424,7 +441,8 @@ void enqueue_cycle(MhdInduction *I)
         gt.ctl = I->ctl.p;
         gt.j = j;
         MatIn in;
-        const bool ilu = I->ilu.on;
+        const bool ilu = I->mode == 2;
+        in.dte = I->mode == 1 ? I->dte.p : nullptr;
         if (ilu)
         {
             // z = M^-1 V_j (:337) by the two triangular solves, V_j = w / H(j, j-1) stored on the way
@@ -447,7 +465,8 @@ void enqueue_cycle(MhdInduction *I)
         fz.dot = cgs ? nullptr : H + j;
         fz.dtp = &I->ctl.p->dt;
         fz.gt = gt;
-        if (I->mixed) op32(I, in, 0.0, I->w.p, fz);
+        // the FP32 operator has no ideal part: the mixed solve uses the FP64 operator while it is on
+        if (I->mixed && !I->ideal) op32(I, in, 0.0, I->w.p, fz);
         else op64(I, in, nullptr, 0.0, I->w.p, fz);
         if (cgs)
         {
@@ -473,7 +492,8 @@ void enqueue_cycle(MhdInduction *I)
 // Capture the cycle once as a CUDA graph; a stream that cannot be captured keeps direct launches.
 void build_cycle_graph(MhdInduction *I)
 {
-    I->cycle_tried = true;
+    const int md = I->mode;
+    I->cycle_tried[md] = true;
     cudaStream_t s = I->mesh->stream;
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
     {
@@ -486,7 +506,7 @@ void build_cycle_graph(MhdInduction *I)
     I->capturing = false;
     cudaGraph_t graph = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s, &graph);
-    I->cycle_kernels = I->launches - l0;
+    I->cycle_kernels[md] = I->launches - l0;
     I->launches = l0;
     if (ce != cudaSuccess || !graph)
     {
@@ -502,7 +522,7 @@ void build_cycle_graph(MhdInduction *I)
         cudaGetLastError();
         return;
     }
-    I->cycle = exec;
+    I->cycle[md] = exec;
 }
 
 void host_read(MhdInduction *I, const double *dev, int n)
@@ -511,7 +531,111 @@ void host_read(MhdInduction *I, const double *dev, int n)
     MHD_CUDA(cudaMemcpyAsync(I->pinned, dev, n * sizeof(double), cudaMemcpyDeviceToHost, s));
     MHD_CUDA(cudaStreamSynchronize(s));
 }
+// ImplicitInduction::solve (:299-390); dte != null: the per-edge pseudo-time step (A x = x + F(d1 diag(dt_e) x),
+// Jacobi 1 / (1 + dt_e m d2), no ILU(0)), dt unused.
+int solve_impl(MhdInduction *I, const double *Phi, const double *Ee, const int8_t *dir, double dt, const double *dte_in, int32_t warm,
+               double *E, int32_t *iterations, double *rel_res)
+{
+    int status = MHD_OK;
+    int rc = guarded([&] {
+        MHD_REQUIRE(I && MHD_ARR(Phi, I->mesh->v.nf) && MHD_ARR(Ee, I->mesh->v.ne) && MHD_ARR(dir, I->mesh->v.ne) &&
+                        MHD_ARR(E, I->mesh->v.ne),
+                    "null argument");
+        const MeshView &m = I->mesh->v;
+        cudaStream_t s = I->mesh->stream;
+        const int32_t ne = m.ne;
+        if (iterations) *iterations = 0;
+        if (rel_res) *rel_res = 0.0;
+        if (ne == 0) return;
+        const int mr = I->p.restart;
+        const int ge = g1(ne);
+        const double *dte = nullptr;
+        if (dte_in)
+        {
+            I->dte.alloc(ne);
+            MHD_CUDA(cudaMemcpyAsync(I->dte.p, dte_in, (size_t)ne * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            dte = I->dte.p;
+        }
+        // the ILU(0) is built for a scalar dt (:317) and only without the ideal part (:102)
+        I->mode = dte ? 1 : (I->ilu.on && !I->ideal ? 2 : 0);
+        const double dtA = dte ? 1.0 : dt; // A x = x + dtA F(d1 [diag(dt_e)] x): d1 carries dt_e (:196)
+        if (!warm) I->have_corr = false;
+        I->last_reorth = 0;
+        double *sc = I->scal.p; // [0] |b|  [1] beta  [2] steps of the last cycle
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_x0<<<ge, 256, 0, s>>>(ne, Ee, I->have_corr ? I->corr.p : nullptr, dir, I->x0.p, I->delta.p));
+        op64(I, MatIn{}, Phi, 0.0, I->Fn.p);                                                      // F(Phi^n)
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_add<<<ge, 256, 0, s>>>(ne, Ee, I->Fn.p, I->b.p));     // b = E_expl + F(Phi^n)
+        apply_plain(I, I->x0.p, dtA, I->Ax.p, dte);                                               // A x0
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_pd<<<ge, 256, 0, s>>>(ne, dt, dte, I->mcoef.p, I->d2.p, dir, I->pd.p, I->dirc.p));
+        if (I->mode == 2) ilu_factor(I, dt, dir); // (:317-318)
+        dev_dot(I, I->b.p, I->b.p, 2, sc + 0);
+        dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
+        MHD_LAUNCH_CHECK();
+        host_read(I, sc + 0, 2);
+        const double bnorm = I->pinned[0];
+        double beta = I->pinned[1];
+        const double tol = I->p.rtol * bnorm;
+        int total = 0;
+        while (beta > tol && total < I->p.max_it)
+        {
+            IND_LAUNCH(I, KI_VECTOR, s,
+                       k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, I->V.p, I->pd.p, I->mixed ? nullptr : I->zs.p,
+                                                   I->mixed ? I->zs32.p : nullptr));
+            IND_LAUNCH(I, KI_SCALAR, s,
+                       k_cycle_init<<<1, 1, 0, s>>>(I->ctl.p, std::min(mr, I->p.max_it - total), tol, dtA, I->gv.p, mr + 1, sc + 1));
+            if (!I->prof.on && !I->cycle_tried[I->mode]) build_cycle_graph(I);
+            if (!I->prof.on && I->cycle[I->mode])
+            {
+                MHD_CUDA(cudaGraphLaunch(I->cycle[I->mode], s));
+                I->launches += I->cycle_kernels[I->mode];
+            }
+            else
+                enqueue_cycle(I);
+            IND_LAUNCH(I, KI_SCALAR, s, k_backsub<<<1, 1, 0, s>>>(I->ctl.p, I->H.p, mr, I->gv.p, I->yv.p, sc + 2));
+            if (I->mode == 2)
+            {
+                IND_LAUNCH(I, KI_VECTOR, s, k_vec_comb<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->w.p));
+                ilu_apply(I, Gate{}, I->w.p, nullptr, dir, nullptr);
+                IND_LAUNCH(I, KI_VECTOR, s, k_vec_addz<<<ge, 256, 0, s>>>(ne, I->ilu.z.p, I->x0.p, I->delta.p, I->z.p));
+            }
+            else
+                IND_LAUNCH(I, KI_VECTOR, s,
+                           k_vec_update<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p));
+            // true residual in FP64 (the outer iterative refinement of the mixed-precision solve)
+            apply_plain(I, I->z.p, dtA, I->Ax.p, dte);
+            IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
+            dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
+            MHD_LAUNCH_CHECK();
+            host_read(I, sc + 1, 3);
+            beta = I->pinned[0];
+            total += static_cast<int>(I->pinned[1]);
+            I->last_reorth += static_cast<int32_t>(I->pinned[2]);
+        }
+        IND_LAUNCH(I, KI_VECTOR, s, k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p));
+        MHD_LAUNCH_CHECK();
+        MHD_CUDA(cudaStreamSynchronize(s));
+        if (I->mode == 2) ilu_check(I);
+        I->have_corr = true;
+        if (iterations) *iterations = total;
+        if (rel_res) *rel_res = beta / bnorm;
+        if (beta > tol) status = MHD_ENOCONV;
+    });
+    return rc != MHD_OK ? rc : status;
+}
+
 } // namespace
+
+void drop_cycle_graphs(MhdInduction *I)
+{
+    MHD_CUDA(cudaStreamSynchronize(I->mesh->stream));
+    for (int k = 0; k < 3; ++k)
+    {
+        if (I->cycle[k]) MHD_CUDA(cudaGraphExecDestroy(I->cycle[k]));
+        I->cycle[k] = nullptr;
+        I->cycle_tried[k] = false;
+    }
+}
 } // namespace mhd
 
 extern "C" {
@@ -533,10 +657,9 @@ int mhd_gpu_induction_create(MhdMesh *mesh, const MhdInductionParams *p, const d
         I->mixed = p->precision == MHD_PREC_MIXED;
         I->edge_blocks = g1(m.ne);
         {
-            int dev = 0, sms = 0, per = 0;
+            int dev = 0, sms = 0;
             MHD_CUDA(cudaGetDevice(&dev));
             MHD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-            (void)per;
             for (int k = 0; k < kCgsMax; ++k) cgs_grids_for(k, sms, I->cgs_grid + 2 * k);
         }
         const size_t ne = m.ne, nf = m.nf, nc = m.nc;
@@ -685,82 +808,51 @@ int mhd_gpu_induction_apply_A(MhdInduction *I, const double *x, double dt, doubl
 int mhd_gpu_induction_solve(MhdInduction *I, const double *Phi, const double *Ee, const int8_t *dir, double dt, int32_t warm, double *E,
                             int32_t *iterations, double *rel_res)
 {
-    int status = MHD_OK;
-    int rc = guarded([&] {
-        MHD_REQUIRE(I && MHD_ARR(Phi, I->mesh->v.nf) && MHD_ARR(Ee, I->mesh->v.ne) && MHD_ARR(dir, I->mesh->v.ne) &&
-                        MHD_ARR(E, I->mesh->v.ne),
-                    "null argument");
+    return solve_impl(I, Phi, Ee, dir, dt, nullptr, warm, E, iterations, rel_res);
+}
+
+int mhd_gpu_induction_solve_dt_edge(MhdInduction *I, const double *Phi, const double *Ee, const int8_t *dir, const double *dt_edge,
+                                    int32_t warm, double *E, int32_t *iterations, double *rel_res)
+{
+    if (I && I->mesh && !MHD_ARR(dt_edge, I->mesh->v.ne))
+    {
+        set_last_error("null dt_edge");
+        return MHD_EINVAL;
+    }
+    return solve_impl(I, Phi, Ee, dir, 0.0, dt_edge, warm, E, iterations, rel_res);
+}
+
+int mhd_gpu_induction_set_ideal(MhdInduction *I, const double *u_cell, const int8_t *mask, double cuct)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I, "null induction handle");
         const MeshView &m = I->mesh->v;
+        const bool on = u_cell != nullptr;
+        MHD_REQUIRE(!on || (MHD_ARR(mask, m.ne) && std::isfinite(cuct)), "null mask or non-finite cuct");
         cudaStream_t s = I->mesh->stream;
-        const int32_t ne = m.ne;
-        if (iterations) *iterations = 0;
-        if (rel_res) *rel_res = 0.0;
-        if (ne == 0) return;
-        const int mr = I->p.restart;
-        const int ge = g1(ne);
-        if (!warm) I->have_corr = false;
-        I->last_reorth = 0;
-        double *sc = I->scal.p; // [0] |b|  [1] beta  [2] steps of the last cycle
-        IND_LAUNCH(I, KI_VECTOR, s, k_vec_x0<<<ge, 256, 0, s>>>(ne, Ee, I->have_corr ? I->corr.p : nullptr, dir, I->x0.p, I->delta.p));
-        op64(I, MatIn{}, Phi, 0.0, I->Fn.p);                                                      // F(Phi^n)
-        IND_LAUNCH(I, KI_VECTOR, s, k_vec_add<<<ge, 256, 0, s>>>(ne, Ee, I->Fn.p, I->b.p));     // b = E_expl + F(Phi^n)
-        apply_plain(I, I->x0.p, dt, I->Ax.p);                                                     // A x0
-        IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
-        IND_LAUNCH(I, KI_VECTOR, s, k_vec_pd<<<ge, 256, 0, s>>>(ne, dt, I->mcoef.p, I->d2.p, dir, I->pd.p, I->dirc.p));
-        if (I->ilu.on) ilu_factor(I, dt, dir); // (:317-318)
-        dev_dot(I, I->b.p, I->b.p, 2, sc + 0);
-        dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
-        MHD_LAUNCH_CHECK();
-        host_read(I, sc + 0, 2);
-        const double bnorm = I->pinned[0];
-        double beta = I->pinned[1];
-        const double tol = I->p.rtol * bnorm;
-        int total = 0;
-        while (beta > tol && total < I->p.max_it)
+        if (on)
         {
-            IND_LAUNCH(I, KI_VECTOR, s,
-                       k_vec_v0<<<ge, 256, 0, s>>>(ne, I->r.p, sc + 1, I->V.p, I->pd.p, I->mixed ? nullptr : I->zs.p,
-                                                   I->mixed ? I->zs32.p : nullptr));
-            IND_LAUNCH(I, KI_SCALAR, s,
-                       k_cycle_init<<<1, 1, 0, s>>>(I->ctl.p, std::min(mr, I->p.max_it - total), tol, dt, I->gv.p, mr + 1, sc + 1));
-            if (!I->prof.on && !I->cycle_tried) build_cycle_graph(I);
-            if (!I->prof.on && I->cycle)
-            {
-                MHD_CUDA(cudaGraphLaunch(I->cycle, s));
-                I->launches += I->cycle_kernels;
-            }
-            else
-                enqueue_cycle(I);
-            IND_LAUNCH(I, KI_SCALAR, s, k_backsub<<<1, 1, 0, s>>>(I->ctl.p, I->H.p, mr, I->gv.p, I->yv.p, sc + 2));
-            if (I->ilu.on)
-            {
-                IND_LAUNCH(I, KI_VECTOR, s, k_vec_comb<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->w.p));
-                ilu_apply(I, Gate{}, I->w.p, nullptr, dir, nullptr);
-                IND_LAUNCH(I, KI_VECTOR, s, k_vec_addz<<<ge, 256, 0, s>>>(ne, I->ilu.z.p, I->x0.p, I->delta.p, I->z.p));
-            }
-            else
-                IND_LAUNCH(I, KI_VECTOR, s,
-                           k_vec_update<<<ge, 256, 0, s>>>(I->ctl.p, ne, I->V.p, I->yv.p, I->pd.p, dir, I->x0.p, I->delta.p, I->z.p));
-            // true residual in FP64 (the outer iterative refinement of the mixed-precision solve)
-            apply_plain(I, I->z.p, dt, I->Ax.p);
-            IND_LAUNCH(I, KI_VECTOR, s, k_vec_resid<<<ge, 256, 0, s>>>(ne, I->b.p, I->Ax.p, dir, I->r.p));
-            dev_dot(I, I->r.p, I->r.p, 1, sc + 1);
-            MHD_LAUNCH_CHECK();
-            host_read(I, sc + 1, 3);
-            beta = I->pinned[0];
-            total += static_cast<int>(I->pinned[1]);
-            I->last_reorth += static_cast<int32_t>(I->pinned[2]);
+            I->u_ideal.alloc(std::max<size_t>(1, 3 * (size_t)m.nc));
+            I->imask.alloc(std::max<size_t>(1, (size_t)m.ne));
+            I->ide.alloc(std::max<size_t>(1, (size_t)m.ne));
+            I->face3.alloc(std::max<size_t>(1, 3 * (size_t)m.nf));
+            if (m.nc) MHD_CUDA(cudaMemcpyAsync(I->u_ideal.p, u_cell, 3 * (size_t)m.nc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+            if (m.ne) MHD_CUDA(cudaMemcpyAsync(I->imask.p, mask, (size_t)m.ne, cudaMemcpyDeviceToDevice, s));
+            I->cuct = cuct;
         }
-        IND_LAUNCH(I, KI_VECTOR, s, k_vec_final<<<ge, 256, 0, s>>>(ne, I->x0.p, I->delta.p, Ee, dir, E, I->corr.p));
-        MHD_LAUNCH_CHECK();
-        MHD_CUDA(cudaStreamSynchronize(s));
-        if (I->ilu.on) ilu_check(I);
-        I->have_corr = true;
-        if (iterations) *iterations = total;
-        if (rel_res) *rel_res = beta / bnorm;
-        if (beta > tol) status = MHD_ENOCONV;
+        // the captured restart cycles hold the other operator (and the mixed solve the other precision)
+        if (on != I->ideal) drop_cycle_graphs(I);
+        I->ideal = on;
     });
-    return rc != MHD_OK ? rc : status;
+}
+
+int mhd_gpu_induction_ideal_linear(MhdInduction *I, const double *phi, double *out)
+{
+    return guarded([&] {
+        MHD_REQUIRE(I && MHD_ARR(phi, I->mesh->v.nf) && MHD_ARR(out, I->mesh->v.ne), "null argument");
+        op64(I, MatIn{}, phi, 0.0, out, Fused{}, true);
+        MHD_LAUNCH_CHECK();
+    });
 }
 
 int mhd_gpu_induction_profile(MhdInduction *I, int32_t enable)

@@ -582,14 +582,8 @@ int mhd_gpu_induction_set_ilu(MhdInduction *I, int32_t enable, double shift)
         // the reference builds the pattern when the operator is active (:102)
         if (I->ilu.on && !I->ilu.built && (I->resistive || I->hall)) ilu_build(I);
         if (!I->ilu.built) I->ilu.on = false;
-        if (I->ilu.on != was && I->cycle)
-        {
-            // the captured restart cycle holds the other preconditioner: capture again at the next solve
-            MHD_CUDA(cudaStreamSynchronize(I->mesh->stream));
-            MHD_CUDA(cudaGraphExecDestroy(I->cycle));
-            I->cycle = nullptr;
-        }
-        if (I->ilu.on != was) I->cycle_tried = false;
+        // the captured restart cycles hold the other preconditioner: capture again at the next solve
+        if (I->ilu.on != was) drop_cycle_graphs(I);
     });
 }
 
@@ -613,13 +607,8 @@ int mhd_gpu_induction_ilu_tune(MhdInduction *I, int32_t window_levels, int32_t m
         I->ilu.window_levels = window_levels;
         I->ilu.backoff_ns = (unsigned)max_backoff_ns;
         if (I->ilu.built) ilu_grids(I->ilu);
-        // the captured restart cycle holds the old grids
-        if (I->cycle)
-        {
-            MHD_CUDA(cudaGraphExecDestroy(I->cycle));
-            I->cycle = nullptr;
-        }
-        I->cycle_tried = false;
+        // the captured restart cycles hold the old grids
+        drop_cycle_graphs(I);
     });
 }
 

@@ -587,6 +587,20 @@ void launch_cell_current(const MeshView &m, const double *B, double *J, cudaStre
     k_cell_current<<<grid_for(m.nc, 128), 128, 0, s>>>(m, B, J);
     MHD_LAUNCH_CHECK();
 }
+
+void ideal_emf_enqueue(const MeshView &m, const double *u, const double *Bt, const double *Bi, const double *phi_tot,
+                       const double *phi_ind, double cuct, double *face3, double *E, cudaStream_t s)
+{
+    if (!m.nf) return;
+    k_face_candidate<<<grid_for(m.nf, 128), 128, 0, s>>>(m, u, Bt, Bi, phi_tot, nullptr, face3, nullptr, nullptr);
+    if (m.no_edges)
+    {
+        if (m.max_valence <= 8)
+            k_edge_uct<8><<<grid_for(m.no_edges, 128), 128, 0, s>>>(m, face3, u, phi_ind, cuct, E);
+        else
+            k_edge_uct<kMaxValence><<<grid_for(m.no_edges, 128), 128, 0, s>>>(m, face3, u, phi_ind, cuct, E);
+    }
+}
 } // namespace mhd
 
 using namespace mhd;
@@ -614,17 +628,8 @@ int mhd_gpu_ideal_emf(MhdMesh *mesh, const double *u, const double *Bt, const do
         const MeshView &m = mesh->v;
         if (!m.nf) return;
         mesh->scratch_face3.alloc(3 * static_cast<size_t>(m.nf));
-        k_face_candidate<<<grid_for(m.nf, 128), 128, 0, mesh->stream>>>(m, u, Bt, Bi, phi_tot, nullptr, mesh->scratch_face3.p, nullptr,
-                                                                         nullptr);
+        ideal_emf_enqueue(m, u, Bt, Bi, phi_tot, phi_ind, cuct, mesh->scratch_face3.p, E, mesh->stream);
         MHD_LAUNCH_CHECK();
-        if (m.no_edges)
-        {
-            if (m.max_valence <= 8)
-                k_edge_uct<8><<<grid_for(m.no_edges, 128), 128, 0, mesh->stream>>>(m, mesh->scratch_face3.p, u, phi_ind, cuct, E);
-            else
-                k_edge_uct<kMaxValence><<<grid_for(m.no_edges, 128), 128, 0, mesh->stream>>>(m, mesh->scratch_face3.p, u, phi_ind, cuct, E);
-            MHD_LAUNCH_CHECK();
-        }
     });
 }
 

@@ -16,9 +16,9 @@ namespace mhd
 constexpr int kRedBlocks = 8 * 148; // streaming reductions: 8 resident 256-thread blocks per SM
 
 // kernel classes of the solve, timed with CUDA events on the handle's stream when profiling is on
-enum IndKernel { KI_FACE = 0, KI_BCELL, KI_HALL, KI_EDGE, KI_MGS, KI_SCALAR, KI_VECTOR, KI_ILU, KI_COUNT };
-const char *const kIndKernelNames[KI_COUNT] = {"face_d1",      "cell_field",    "hall_emf",      "edge_gather",
-                                               "gram_schmidt", "krylov_scalar", "krylov_vector", "ilu"};
+enum IndKernel { KI_FACE = 0, KI_BCELL, KI_HALL, KI_EDGE, KI_MGS, KI_SCALAR, KI_VECTOR, KI_ILU, KI_IDEAL, KI_COUNT };
+const char *const kIndKernelNames[KI_COUNT] = {"face_d1",      "cell_field",    "hall_emf",      "edge_gather", "gram_schmidt",
+                                               "krylov_scalar", "krylov_vector", "ilu",          "ideal_emf"};
 
 // Device-side control of one restart cycle: the Arnoldi steps of a cycle are enqueued (or replayed as
 // one CUDA graph) without host round trips; a step whose predecessor met the tolerance, or that lies
@@ -98,6 +98,7 @@ struct MatIn
     const double *src = nullptr, *hs = nullptr, *pd = nullptr;
     const double *zs = nullptr;
     const float *zs32 = nullptr;
+    const double *dte = nullptr; // per-edge pseudo-time step: Phi' = d1 diag(dt_e) x (:188)
 };
 
 template <class T> struct EdgeArgs
@@ -113,6 +114,8 @@ template <class T> struct EdgeArgs
     double *part = nullptr, *dot = nullptr;
     unsigned *counter = nullptr;
     double *out = nullptr;
+    const double *ide = nullptr;   // implicit ideal EMF of the owned edges (part2, :151-158) where imask is set
+    const int8_t *imask = nullptr;
     Gate gt;
 };
 } // namespace mhd
@@ -180,19 +183,29 @@ __global__ void k_ind_face(MeshView m, Gate gt, MatIn in, int hall, int resistiv
         if (in.zs32) { v0 = in.zs32[e0]; v1 = in.zs32[e1]; v2 = in.zs32[e2]; }
         else if (in.zs) { v0 = in.zs[e0]; v1 = in.zs[e1]; v2 = in.zs[e2]; }
         else { v0 = in.x[e0]; v1 = in.x[e1]; v2 = in.x[e2]; }
-        s += s0 * v0;
-        s += s1 * v1;
-        s += s2 * v2;
+        if (in.dte)
+        {
+            s += (s0 * in.dte[e0]) * v0;
+            s += (s1 * in.dte[e1]) * v1;
+            s += (s2 * in.dte[e2]) * v2;
+        }
+        else
+        {
+            s += s0 * v0;
+            s += s1 * v1;
+            s += s2 * v2;
+        }
     }
     else
     {
         const int32_t k0 = m.f2e_ptr[f], k1 = m.f2e_ptr[f + 1];
-        if (in.zs32)
-            for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * static_cast<double>(in.zs32[m.f2e_idx[k]]);
-        else if (in.zs)
-            for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.zs[m.f2e_idx[k]];
-        else
-            for (int32_t k = k0; k < k1; ++k) s += m.f2e_sgn[k] * in.x[m.f2e_idx[k]];
+        for (int32_t k = k0; k < k1; ++k)
+        {
+            const int32_t e = m.f2e_idx[k];
+            const double v = in.zs32 ? static_cast<double>(in.zs32[e]) : (in.zs ? in.zs[e] : in.x[e]);
+            const double sg = m.f2e_sgn[k];
+            s += (in.dte ? sg * in.dte[e] : sg) * v;
+        }
     }
     if ((in.zs || in.zs32) && in.hs) s = s / *in.hs;
     if (hall) phi[f] = static_cast<T>(s);
@@ -306,7 +319,8 @@ __global__ void __launch_bounds__(256) k_ind_edge(MeshView m, EdgeArgs<T> a)
             else
                 for (int32_t k = k0; k < k1; ++k) term(k);
         }
-        const T F = a.mcoef[e] * p0 + p1 + static_cast<T>(0);
+        const T p2 = (a.ide && a.imask[e]) ? static_cast<T>(a.ide[e]) : static_cast<T>(0);
+        const T F = a.mcoef[e] * p0 + p1 + p2;
         double y = static_cast<double>(F);
         if (a.in.src || a.in.x)
         {
@@ -353,14 +367,22 @@ struct MhdInduction
     mhd::EventProfiler<mhd::KI_COUNT> prof;
     int64_t launches = 0;
     int32_t last_reorth = 0; // Gram-Schmidt second passes of the last solve
-    // one restart cycle (mr Arnoldi steps) captured as a CUDA graph on the first unprofiled solve
-    cudaGraphExec_t cycle = nullptr;
-    bool cycle_tried = false;
-    int64_t cycle_kernels = 0;
+    // the implicit ideal part of F (set_ideal_state): cell velocities, edges that carry it, its UCT strength
+    bool ideal = false;
+    double cuct = 0.5;
+    mhd::DBuf<double> u_ideal, ide, face3, dte;
+    mhd::DBuf<int8_t> imask;
+    // one restart cycle (mr Arnoldi steps) captured as a CUDA graph on the first unprofiled solve of each
+    // kind (mode 0: Jacobi with a scalar dt; 1: Jacobi with the per-edge dt; 2: ILU(0))
+    int mode = 0;
+    cudaGraphExec_t cycle[3] = {nullptr, nullptr, nullptr};
+    bool cycle_tried[3] = {false, false, false};
+    int64_t cycle_kernels[3] = {0, 0, 0};
     bool capturing = false;
     ~MhdInduction()
     {
-        if (cycle) cudaGraphExecDestroy(cycle);
+        for (auto &g : cycle)
+            if (g) cudaGraphExecDestroy(g);
         if (pinned) cudaFreeHost(pinned);
     }
 };
@@ -401,4 +423,11 @@ void ilu_factor(MhdInduction *I, double dt, const int8_t *dir);
 void ilu_apply(MhdInduction *I, const Gate &gt, const double *src, const double *hs, const int8_t *dir, double *vout);
 // MHD_ECUDA if a wait of an ILU(0) pass gave up since the last check (synchronises the stream)
 void ilu_check(MhdInduction *I);
+// Drop the captured restart cycles (after a change of preconditioner, launch shape or operator parts);
+// synchronises the stream.
+void drop_cycle_graphs(MhdInduction *I);
+// The ideal UCT EMF added into E (owned edges) from u, B_tot, B_ind (3 per cell) and phi_tot, phi_ind
+// (per face), with face3 (3 per face) as the face candidates' scratch (induction.cu).
+void ideal_emf_enqueue(const MeshView &m, const double *u, const double *Bt, const double *Bi, const double *phi_tot,
+                       const double *phi_ind, double cuct, double *face3, double *E, cudaStream_t s);
 } // namespace mhd

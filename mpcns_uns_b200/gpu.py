@@ -115,6 +115,9 @@ _SIGS = {
     "mhd_gpu_induction_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
     "mhd_gpu_induction_last_solve_stats": ([vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_induction_set_ilu": ([vp, i32, dbl], ctypes.c_int),
+    "mhd_gpu_induction_solve_dt_edge": ([vp, vp, vp, vp, vp, i32, vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_induction_set_ideal": ([vp, vp, vp, dbl], ctypes.c_int),
+    "mhd_gpu_induction_ideal_linear": ([vp, vp, vp], ctypes.c_int),
     "mhd_gpu_induction_ilu_factor": ([vp, dbl, vp], ctypes.c_int),
     "mhd_gpu_induction_ilu_apply": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_induction_ilu_debug": ([vp, dbl, i32], ctypes.c_int),
@@ -917,6 +920,43 @@ class DeviceInduction:
         if rc != MHD_ENOCONV:
             check(rc)
         return E, it.value, rr.value
+
+    def solve_dt_edge(self, Phi, E_expl, dirichlet, dt_edge, warm=True, E=None):
+        """ImplicitInduction::solve with the per-edge pseudo-time step dt_edge (:299-390) -> (E, iterations, rel_res)."""
+        torch = _torch()
+        Phi, Ee, dte = dev(Phi), dev(E_expl), dev(dt_edge)
+        d = self._dir(dirichlet)
+        if E is None:
+            E = torch.empty(self.mesh.n_edges, dtype=torch.float64, device="cuda")
+        it, rr = i32(), dbl()
+        self.mesh._enter()
+        rc = lib().mhd_gpu_induction_solve_dt_edge(self._h, ptr(Phi), ptr(Ee), ptr(d), ptr(dte), int(bool(warm)), ptr(E),
+                                                   ctypes.byref(it), ctypes.byref(rr))
+        self.mesh._leave()
+        if rc != MHD_ENOCONV:
+            check(rc)
+        return E, it.value, rr.value
+
+    def set_ideal_state(self, u_cell, mask, cuct=0.5):
+        """ImplicitInduction::set_ideal_state (:112-116) with Config::implicit_ideal: u 3 per cell, mask 1 per edge
+        (None: the ideal part off)."""
+        if u_cell is None:
+            check(lib().mhd_gpu_induction_set_ideal(self._h, None, None, float(cuct)))
+            return
+        u, m = dev(u_cell), self._dir(mask)
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_set_ideal(self._h, ptr(u), ptr(m), float(cuct)))
+        self.mesh._leave()
+
+    def ideal_linear(self, phi):
+        """ImplicitInduction::ideal_linear (:118-124): the implicit ideal part alone."""
+        torch = _torch()
+        phi = dev(phi)
+        out = torch.empty(self.mesh.n_edges, dtype=torch.float64, device="cuda")
+        self.mesh._enter()
+        check(lib().mhd_gpu_induction_ideal_linear(self._h, ptr(phi), ptr(out)))
+        self.mesh._leave()
+        return out
 
     def profile(self, enable=True):
         check(lib().mhd_gpu_induction_profile(self._h, int(bool(enable))))

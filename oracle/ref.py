@@ -23,9 +23,9 @@ def available() -> bool:
 
 
 class IndParams(ctypes.Structure):
-    _fields_ = [("resistive", i32), ("hall", i32), ("max_it", i32), ("restart", i32), ("ilu", i32), ("pad", i32),
+    _fields_ = [("resistive", i32), ("hall", i32), ("max_it", i32), ("restart", i32), ("ilu", i32), ("implicit_ideal", i32),
                 ("inver_Rem", dbl), ("eta_r_inner", dbl), ("eta_r_outer", dbl), ("eta_width", dbl),
-                ("hall_coef", dbl), ("hall_r_min", dbl), ("hall_r_max", dbl), ("rtol", dbl), ("ilu_shift", dbl)]
+                ("hall_coef", dbl), ("hall_r_min", dbl), ("hall_r_max", dbl), ("rtol", dbl), ("ilu_shift", dbl), ("cuct", dbl)]
 
 
 class StepParams(ctypes.Structure):
@@ -100,6 +100,9 @@ def lib():
             ("ref_ind_apply_A", [vp, vp, dbl, vp], None),
             ("ref_ind_solve", [vp, vp, vp, vp, dbl, i32, vp, vp], i32),
             ("ref_ind_precond", [vp, dbl, vp, vp, vp], i32),
+            ("ref_ind_set_ideal", [vp, vp, vp], None),
+            ("ref_ind_ideal_linear", [vp, vp, vp], None),
+            ("ref_ind_solve_dte", [vp, vp, vp, vp, vp, i32, vp, vp], i32),
             ("ref_rk2_step", [vp, ctypes.POINTER(StepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
             ("ref_add_sources", [vp, ctypes.POINTER(StepParams), i32, vp, vp, vp, vp, vp, vp, vp, vp, dbl, vp], None),
             ("ref_electron_pressure_gradient", [vp, vp, vp, vp], None),
@@ -399,6 +402,8 @@ class RefInduction:
         p.hall_r_max = kw.get("hall_r_max", 1.012)
         p.rtol = kw.get("rtol", 1e-4)
         p.ilu_shift = kw.get("ilu_shift", 0.3)
+        p.implicit_ideal = int(kw.get("implicit_ideal", False))
+        p.cuct = kw.get("cuct", 0.5)
         self.mesh = mesh
         h = lib().ref_ind_create(mesh._h, ctypes.byref(p))
         if not h:
@@ -425,6 +430,30 @@ class RefInduction:
         a = np.zeros(n, dt)
         lib().ref_ind_array(self._h, name.encode(), _p(a))
         return a
+
+    def set_ideal_state(self, u_cell, mask):
+        """ImplicitInduction::set_ideal_state (:112-116): u 3 per cell, mask 1 per edge."""
+        u = np.ascontiguousarray(u_cell, np.float64)
+        m = np.ascontiguousarray(mask, np.int8)
+        lib().ref_ind_set_ideal(self._h, _p(u), _p(m))
+
+    def ideal_linear(self, phi):
+        """ImplicitInduction::ideal_linear (:118-124)."""
+        phi = np.ascontiguousarray(phi, np.float64)
+        o = np.zeros(self.mesh.n_edges)
+        lib().ref_ind_ideal_linear(self._h, _p(phi), _p(o))
+        return o
+
+    def solve_dt_edge(self, Phi, E_expl, dirichlet, dt_edge, warm=True):
+        """ImplicitInduction::solve with the per-edge step dt_edge (:299-390)."""
+        Phi = np.ascontiguousarray(Phi, np.float64)
+        Ee = np.ascontiguousarray(E_expl, np.float64)
+        d = np.ascontiguousarray(dirichlet, np.int8)
+        dte = np.ascontiguousarray(dt_edge, np.float64)
+        E = np.zeros(self.mesh.n_edges)
+        rr = ctypes.c_double()
+        it = lib().ref_ind_solve_dte(self._h, _p(Phi), _p(Ee), _p(d), _p(dte), int(warm), _p(E), ctypes.byref(rr))
+        return E, int(it), rr.value
 
     def precond(self, dt, dirichlet, v):
         """factor_precond(dt, dir) then apply_precond(v) (ImplicitInduction.cpp:247-297) -> z."""

@@ -115,4 +115,14 @@ int drv_ind_solve(void *ind, const double *Phi, const double *Ee, const int8_t *
         *it = static_cast<mhd::ImplicitInduction *>(ind)->solve(Phi, Ee, d, dt, E, rr);
     });
 }
+
+// the per-edge pseudo-time form of the same call
+int drv_ind_solve_dte(void *ind, const double *Phi, const double *Ee, const int8_t *dir, int64_t n_edges, const double *dt_edge, double *E,
+                      int32_t *it, double *rr)
+{
+    return guarded([&] {
+        std::vector<char> d(dir, dir + n_edges);
+        *it = static_cast<mhd::ImplicitInduction *>(ind)->solve(Phi, Ee, d, 0.0, E, rr, dt_edge);
+    });
+}
 } // extern "C"

@@ -521,8 +521,8 @@ double ref_local_time_step(void *h, double gamma, double cfl, double inver_MA2, 
 
 struct RefIndParams
 {
-    int32_t resistive, hall, max_it, restart, ilu, pad;
-    double inver_Rem, eta_r_inner, eta_r_outer, eta_width, hall_coef, hall_r_min, hall_r_max, rtol, ilu_shift;
+    int32_t resistive, hall, max_it, restart, ilu, implicit_ideal;
+    double inver_Rem, eta_r_inner, eta_r_outer, eta_width, hall_coef, hall_r_min, hall_r_max, rtol, ilu_shift, cuct;
 };
 
 struct RefInd
@@ -530,6 +530,7 @@ struct RefInd
     RefMesh *mesh;
     comm::Exchanger ex;
     std::unique_ptr<ImplicitInduction> ind;
+    std::vector<double> u_ideal; // the cell velocities set_ideal_state points to
     RefInd(RefMesh *m) : mesh(m), ex(MPI_COMM_SELF, m->lm) {}
 };
 
@@ -558,6 +559,8 @@ void *ref_ind_create(void *h, const RefIndParams *p)
         c.hall = p->hall != 0; c.sc.hall_coef = p->hall_coef; c.hall_r_min = p->hall_r_min; c.hall_r_max = p->hall_r_max;
         c.ind_rtol = p->rtol; c.ind_max_it = p->max_it; c.ind_restart = p->restart; c.ind_ilu = p->ilu != 0;
         c.ind_ilu_shift = p->ilu_shift;
+        c.implicit_ideal = p->implicit_ideal != 0;
+        c.ideal.cuct = p->cuct;
         auto *ri = new RefInd(r);
         ri->ind = std::make_unique<ImplicitInduction>(r->lm, r->geo, ri->ex, c);
         out = ri;
@@ -630,6 +633,33 @@ void ref_ind_apply_A(void *h, const double *x, double dt, double *y)
     std::vector<double> xv(x, x + ne), yv(ne);
     I.apply_A(xv, yv, dt);
     std::copy(yv.begin(), yv.end(), y);
+}
+
+// ImplicitInduction::set_ideal_state (:112-116): u 3 per cell (kept in the handle, the object holds a
+// pointer), mask 1 per edge
+void ref_ind_set_ideal(void *h, const double *u, const int8_t *mask)
+{
+    RefInd *ri = static_cast<RefInd *>(h);
+    ImplicitInduction &I = *ri->ind;
+    const size_t nc = I.alpha_.size(), ne = I.m_.size();
+    ri->u_ideal.assign(u, u + 3 * nc);
+    std::vector<char> mk(ne);
+    for (size_t e = 0; e < ne; ++e) mk[e] = mask[e];
+    I.set_ideal_state(ri->u_ideal.data(), mk);
+}
+
+// ImplicitInduction::ideal_linear (:118-124)
+void ref_ind_ideal_linear(void *h, const double *phi, double *out) { static_cast<RefInd *>(h)->ind->ideal_linear(phi, out); }
+
+// ImplicitInduction::solve with the per-edge pseudo-time step dt_edge (:299-390, system (I + F d1 diag(dt_e)) E)
+int32_t ref_ind_solve_dte(void *h, const double *Phi, const double *Eexpl, const int8_t *dir, const double *dt_edge, int32_t use_guess,
+                          double *E, double *rel_res)
+{
+    ImplicitInduction &I = *static_cast<RefInd *>(h)->ind;
+    if (!use_guess) I.corr_.clear();
+    std::vector<char> d(I.m_.size());
+    for (size_t e = 0; e < d.size(); ++e) d[e] = dir[e];
+    return I.solve(Phi, Eexpl, d, 0.0, E, rel_res, dt_edge);
 }
 
 // ImplicitInduction::solve (:299-390).  use_guess = 0 clears the warm start first.

@@ -42,7 +42,9 @@ def drv():
                            "drv_cell_vector": [vp, vp, vp, i32, vp], "drv_ideal_emf": [vp, vp, vp, vp, vp, vp, vp, dbl, vp],
                            "drv_faraday": [vp, vp, vp, dbl], "drv_faraday_edge_dt": [vp, vp, vp, vp],
                            "drv_div_b": [vp, vp, vp, vp],
-                           "drv_ind_solve": [vp, vp, vp, vp, ctypes.c_int64, dbl, vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)]}.items():
+                           "drv_ind_solve": [vp, vp, vp, vp, ctypes.c_int64, dbl, vp, ctypes.POINTER(i32), ctypes.POINTER(dbl)],
+                           "drv_ind_solve_dte": [vp, vp, vp, vp, ctypes.c_int64, vp, vp, ctypes.POINTER(i32),
+                                                 ctypes.POINTER(dbl)]}.items():
             getattr(L, name).argtypes = args
             getattr(L, name).restype = ctypes.c_int
         _drv = L
@@ -133,25 +135,34 @@ def test_induction_signatures(mesh):
         assert int(o[2]) == rr["worst_cell_gid"]
 
 
-@pytest.mark.parametrize("ilu", [False, True])
-def test_implicit_induction_solve_signature(mesh, ilu):
+@pytest.mark.parametrize("variant", ["jacobi", "ilu", "dt_edge", "ideal"])
+def test_implicit_induction_solve_signature(mesh, variant):
     """ImplicitInduction::solve on the reference's object: the drop-in hands the object's resistivity, Hall
     coefficient per cell (alpha_ = taper hall_coef / n_e,eff) and frozen field to the device solve, with the
-    object's preconditioner (Jacobi, or block ILU(0) when its Config asked for it)."""
+    object's preconditioner (Jacobi, or block ILU(0) when its Config asked for it), its per-edge pseudo-time
+    step when the call passes one, and its implicit ideal part (Config::implicit_ideal, set_ideal_state)."""
     r, (lm, geo, bc, cfg, st) = mesh
     rng = np.random.default_rng(73)
     nc, nf, ne = r.n_cells, r.n_faces, r.n_edges
     ri = ref.RefInduction(r, hall=True, hall_coef=0.5, hall_r_min=-100.0, hall_r_max=-99.0, rtol=1e-10, max_it=200, restart=15,
-                          ilu=ilu)
+                          ilu=variant == "ilu", implicit_ideal=variant == "ideal", cuct=0.5)
     ri.set_m(rng.uniform(0.5, 2.0, ne) / np.asarray(r["star1"]))
     ri.set_frozen_state(rng.uniform(-1, 1, 3 * nc), rng.uniform(0.5, 2.0, nc))
     phi = rng.uniform(-1, 1, nf)
     Ee = rng.uniform(-1, 1, ne)
     dirichlet = (np.asarray(r["edge_mode"]) == 2).astype(np.int8)
-    E_ref, it_ref, rr_ref = ri.solve(phi, Ee, dirichlet, 0.05, False)
+    if variant == "ideal":
+        ri.set_ideal_state(rng.uniform(-1, 1, 3 * nc), (np.asarray(r["edge_mode"]) == 0).astype(np.int8))
     E = np.zeros(ne)
     it, rr = i32(), dbl()
-    call(drv().drv_ind_solve, ri.object(), _p(phi), _p(Ee), _p(dirichlet), ne, 0.05, _p(E), ctypes.byref(it), ctypes.byref(rr))
+    if variant == "dt_edge":
+        dte = rng.uniform(0.02, 0.08, ne)
+        E_ref, it_ref, rr_ref = ri.solve_dt_edge(phi, Ee, dirichlet, dte, False)
+        call(drv().drv_ind_solve_dte, ri.object(), _p(phi), _p(Ee), _p(dirichlet), ne, _p(dte), _p(E), ctypes.byref(it),
+             ctypes.byref(rr))
+    else:
+        E_ref, it_ref, rr_ref = ri.solve(phi, Ee, dirichlet, 0.05, False)
+        call(drv().drv_ind_solve, ri.object(), _p(phi), _p(Ee), _p(dirichlet), ne, 0.05, _p(E), ctypes.byref(it), ctypes.byref(rr))
     assert rr.value <= 1e-10 and rr_ref <= 1e-10
     assert abs(it.value - it_ref) <= 2, (it.value, it_ref)
     assert rel_err(E, E_ref) <= 1e-8
