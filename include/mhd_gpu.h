@@ -301,9 +301,10 @@ int mhd_gpu_induction_ilu_apply(MhdInduction *ind, const int8_t *dirichlet, cons
  * never raises its flag (-1: none), so that the rows reading it give up and the call returns MHD_ECUDA
  * ("ILU(0) pass timed out") with the handle usable again. */
 int mhd_gpu_induction_ilu_debug(MhdInduction *ind, double wait_s, int32_t unpublished_row);
-/* Launch shape of the ILU(0) passes: about window_levels dependency levels of rows in flight (default 2)
- * and at most max_backoff_ns between two polls of an unfinished row (default 512). */
-int mhd_gpu_induction_ilu_tune(MhdInduction *ind, int32_t window_levels, int32_t max_backoff_ns);
+/* Launch shape of the ILU(0) passes: about window_levels dependency levels of rows in flight (default 8),
+ * spin_polls polls of unfinished rows without a pause (default 0), then pauses doubling from 32 ns to
+ * max_backoff_ns (default 128). */
+int mhd_gpu_induction_ilu_tune(MhdInduction *ind, int32_t window_levels, int32_t max_backoff_ns, int32_t spin_polls);
 /* Host copies of the pattern and the current factors (pc_ptr_ n_owned+1, pc_col_ / pc_coef_ / pc_val_
  * nnz, pc_diag_ n_owned); any output may be NULL; *n_owned and *nnz receive the sizes. */
 int mhd_gpu_induction_ilu_arrays(MhdInduction *ind, int32_t *n_owned, int64_t *nnz, int64_t *ptr, int32_t *col, double *coef,

@@ -42,14 +42,9 @@ struct IluView
     uint64_t wait_ns;    // a wait gives up after this long
     int32_t unpublished; // test hook: this row never raises its flag (-1: none)
     unsigned backoff;    // longest pause between two polls (ns)
+    unsigned spin;       // polls without a pause before the back-off starts
 };
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
-{
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
 __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p)
 {
     unsigned v;
@@ -68,32 +63,11 @@ __device__ __forceinline__ uint64_t global_ns()
     return t;
 }
 
-// Wait until row r of this pass is finished (its flag holds the pass's epoch), backing off from 32 ns to
-// `backoff` between polls.  Gives up, raising ctl->err, after P.wait_ns, and at once when another wait has
-// given up.
-__device__ __noinline__ void ilu_wait(const unsigned *flag, IluCtl *ctl, uint64_t wait_ns, unsigned backoff, unsigned ep)
-{
-    const uint64_t t0 = global_ns();
-    unsigned ns = 32;
-    for (unsigned it = 1;; ++it)
-    {
-        if (ld_acquire(flag) == ep) return;
-        __nanosleep(ns);
-        ns = ns < backoff ? 2 * ns : backoff;
-        if ((it & 15) == 0)
-        {
-            if (*(volatile unsigned *)&ctl->err) return;
-            if (global_ns() - t0 > wait_ns)
-            {
-                atomicOr(&ctl->err, 1u);
-                return;
-            }
-        }
-    }
-}
-
-// The flags of columns col[k0 .. k0+n) (n <= kIluChunk): loaded together, the unfinished ones waited for,
-// then one fence orders the caller's later loads of those rows' results after their release.
+// The flags of columns col[k0 .. k0+n) (n <= kIluChunk): loaded together, the unfinished ones polled
+// together until they are raised (every round one round trip for all of them: spin rounds without a
+// pause, then 32 ns doubling to P.backoff), then one fence orders the caller's later loads of those rows'
+// results after their release.  Gives up after P.wait_ns (raising ctl->err), and at once when another
+// wait has given up.
 __device__ __forceinline__ void ilu_wait_chunk(const IluView &P, int32_t k0, int n, unsigned ep, int32_t *c)
 {
     unsigned f[kIluChunk];
@@ -101,9 +75,36 @@ __device__ __forceinline__ void ilu_wait_chunk(const IluView &P, int32_t k0, int
     for (int u = 0; u < kIluChunk; ++u) c[u] = u < n ? __ldg(P.col + k0 + u) : 0;
 #pragma unroll
     for (int u = 0; u < kIluChunk; ++u) f[u] = u < n ? ld_relaxed(P.flag + c[u]) : ep;
+    unsigned pending = 0;
 #pragma unroll
     for (int u = 0; u < kIluChunk; ++u)
-        if (f[u] != ep) ilu_wait(P.flag + c[u], P.ctl, P.wait_ns, P.backoff, ep);
+        if (f[u] != ep) pending |= 1u << u;
+    // the unfinished rows polled together, one round trip per round for all of them
+    const uint64_t t0 = pending ? global_ns() : 0;
+    unsigned ns = 32;
+    for (unsigned it = 1; pending; ++it)
+    {
+        if (it > P.spin)
+        {
+            __nanosleep(ns);
+            ns = ns < P.backoff ? 2 * ns : P.backoff;
+        }
+#pragma unroll
+        for (int u = 0; u < kIluChunk; ++u)
+            if (pending & (1u << u)) f[u] = ld_relaxed(P.flag + c[u]);
+#pragma unroll
+        for (int u = 0; u < kIluChunk; ++u)
+            if ((pending & (1u << u)) && f[u] == ep) pending &= ~(1u << u);
+        if (pending && (it & 15) == 0)
+        {
+            if (*(volatile unsigned *)&P.ctl->err) break;
+            if (global_ns() - t0 > P.wait_ns)
+            {
+                atomicOr(&P.ctl->err, 1u);
+                break;
+            }
+        }
+    }
     fence_acq_rel();
 }
 
@@ -227,25 +228,33 @@ __device__ __forceinline__ void st_relaxed_f64(double *p, double v)
 }
 __device__ __forceinline__ bool unset(double v) { return __double_as_longlong(v) == kUnset; }
 
-// Poll the result of row r until it is set, backing off from 32 ns to P.backoff; gives up as ilu_wait does
-// (the unset value is returned then).
-__device__ __noinline__ double ilu_wait_value(const double *p, IluCtl *ctl, uint64_t wait_ns, unsigned backoff)
+// Poll the results of the pending rows c[u] (bits of `pending`) until all are set: every round reloads all
+// of them at once, then pauses (spin rounds without a pause, then 32 ns doubling to P.backoff).  Gives up
+// as ilu_wait_chunk does (the unset values stay then).
+__device__ __forceinline__ void ilu_poll_values(const IluView &P, const double *out, const int32_t *c, double *x, unsigned pending)
 {
     const uint64_t t0 = global_ns();
     unsigned ns = 32;
-    for (unsigned it = 1;; ++it)
+    for (unsigned it = 1; pending; ++it)
     {
-        const double v = ld_relaxed_f64(p);
-        if (!unset(v)) return v;
-        __nanosleep(ns);
-        ns = ns < backoff ? 2 * ns : backoff;
-        if ((it & 15) == 0)
+        if (it > P.spin)
         {
-            if (*(volatile unsigned *)&ctl->err) return v;
-            if (global_ns() - t0 > wait_ns)
+            __nanosleep(ns);
+            ns = ns < P.backoff ? 2 * ns : P.backoff;
+        }
+#pragma unroll
+        for (int u = 0; u < kIluChunk; ++u)
+            if (pending & (1u << u)) x[u] = ld_relaxed_f64(out + c[u]);
+#pragma unroll
+        for (int u = 0; u < kIluChunk; ++u)
+            if ((pending & (1u << u)) && !unset(x[u])) pending &= ~(1u << u);
+        if (pending && (it & 15) == 0)
+        {
+            if (*(volatile unsigned *)&P.ctl->err) return;
+            if (global_ns() - t0 > P.wait_ns)
             {
-                atomicOr(&ctl->err, 1u);
-                return v;
+                atomicOr(&P.ctl->err, 1u);
+                return;
             }
         }
     }
@@ -300,9 +309,12 @@ __global__ void __launch_bounds__(kIluThreads) k_ilu_trsv(Gate gt, IluView P, co
             }
 #pragma unroll
             for (int u = 0; u < kIluChunk; ++u) x[u] = u < n ? ld_relaxed_f64(out + c[u]) : 0.0;
+            // the unfinished rows polled together, one round trip per round for all of them
+            unsigned pending = 0;
 #pragma unroll
             for (int u = 0; u < kIluChunk; ++u)
-                if (u < n && unset(x[u])) x[u] = ilu_wait_value(out + c[u], P.ctl, P.wait_ns, P.backoff);
+                if (u < n && unset(x[u])) pending |= 1u << u;
+            if (pending) ilu_poll_values(P, out, c, x, pending);
 #pragma unroll
             for (int u = 0; u < kIluChunk; ++u)
                 if (u < n) acc = __dsub_rn(acc, __dmul_rn(a[u], x[u]));
@@ -327,7 +339,7 @@ __global__ void k_ilu_tail(Gate gt, int32_t no, int32_t ne, const double *src, c
 IluView view(MhdInduction *I)
 {
     IluState &L = I->ilu;
-    return IluView{L.no, L.ptr.p, L.col.p, L.diag.p, L.coef.p, L.val.p, L.flag.p, L.ctl.p, L.wait_ns, L.unpublished, L.backoff_ns};
+    return IluView{L.no, L.ptr.p, L.col.p, L.diag.p, L.coef.p, L.val.p, L.flag.p, L.ctl.p, L.wait_ns, L.unpublished, L.backoff_ns, L.spin_polls};
 }
 
 // build_precond_pattern (:209-242) for rows [r0, r1): counts per row and the rows' (column, coefficient) runs
@@ -597,15 +609,17 @@ int mhd_gpu_induction_ilu_debug(MhdInduction *I, double wait_s, int32_t unpublis
     });
 }
 
-int mhd_gpu_induction_ilu_tune(MhdInduction *I, int32_t window_levels, int32_t max_backoff_ns)
+int mhd_gpu_induction_ilu_tune(MhdInduction *I, int32_t window_levels, int32_t max_backoff_ns, int32_t spin_polls)
 {
     return guarded([&] {
         MHD_REQUIRE(I, "null induction handle");
         MHD_REQUIRE(window_levels >= 1 && window_levels <= 1024, "window_levels outside [1, 1024]");
         MHD_REQUIRE(max_backoff_ns >= 32 && max_backoff_ns <= 100000, "max_backoff_ns outside [32, 100000]");
+        MHD_REQUIRE(spin_polls >= 0 && spin_polls <= 100000, "spin_polls outside [0, 100000]");
         MHD_CUDA(cudaStreamSynchronize(I->mesh->stream));
         I->ilu.window_levels = window_levels;
         I->ilu.backoff_ns = (unsigned)max_backoff_ns;
+        I->ilu.spin_polls = (unsigned)spin_polls;
         if (I->ilu.built) ilu_grids(I->ilu);
         // the captured restart cycles hold the old grids
         drop_cycle_graphs(I);

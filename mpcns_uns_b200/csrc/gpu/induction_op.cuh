@@ -77,8 +77,9 @@ struct IluState
     int32_t npos_l = 0, npos_u = 0;   // positions of the level orders (levels padded to whole warps)
     int grid_l = 0, grid_u = 0;       // blocks of the passes: a few levels of rows in flight
     int64_t resident = 0;             // blocks of a pass resident on the device at once
-    int32_t window_levels = 2;        // levels of rows in flight
-    unsigned backoff_ns = 512;        // longest pause between two polls
+    int32_t window_levels = 8;        // levels of rows in flight
+    unsigned backoff_ns = 128;        // longest pause between two polls
+    unsigned spin_polls = 0;          // polls without a pause before the back-off
     uint64_t wait_ns = 2000000000ull; // a wait on another row gives up after this long
     int32_t unpublished = -1;         // test hook: a row that never raises its flag
     DBuf<int32_t> ptr, col, diag, order_l, order_u;

@@ -121,7 +121,7 @@ _SIGS = {
     "mhd_gpu_induction_ilu_factor": ([vp, dbl, vp], ctypes.c_int),
     "mhd_gpu_induction_ilu_apply": ([vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_induction_ilu_debug": ([vp, dbl, i32], ctypes.c_int),
-    "mhd_gpu_induction_ilu_tune": ([vp, i32, i32], ctypes.c_int),
+    "mhd_gpu_induction_ilu_tune": ([vp, i32, i32, i32], ctypes.c_int),
     "mhd_gpu_induction_ilu_arrays": ([vp, ctypes.POINTER(i32), ctypes.POINTER(i64), vp, vp, vp, vp, vp], ctypes.c_int),
     "mhd_ilu_pattern": ([i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
     "mhd_gpu_tet_build": ([i32, i64, vp, vp, i32, vp, vp, ctypes.POINTER(vp)], ctypes.c_int),
@@ -1012,9 +1012,9 @@ class DeviceInduction:
         """Test hook of the ILU(0) passes' bounded waits (mhd_gpu_induction_ilu_debug)."""
         check(lib().mhd_gpu_induction_ilu_debug(self._h, float(wait_s), int(unpublished_row)))
 
-    def ilu_tune(self, window_levels=2, max_backoff_ns=512):
+    def ilu_tune(self, window_levels=8, max_backoff_ns=128, spin_polls=0):
         """Launch shape of the ILU(0) passes (mhd_gpu_induction_ilu_tune)."""
-        check(lib().mhd_gpu_induction_ilu_tune(self._h, int(window_levels), int(max_backoff_ns)))
+        check(lib().mhd_gpu_induction_ilu_tune(self._h, int(window_levels), int(max_backoff_ns), int(spin_polls)))
 
     def ilu_arrays(self):
         """{pc_ptr, pc_col, pc_coef, pc_val, pc_diag} of the pattern and the current factors (host)."""
