@@ -376,6 +376,18 @@ int mhd_gpu_cfl_dt(MhdState *state, double dt_max, double *host_dt);
  * capped by dt_max is computed on the device.  dt_used (host, may be NULL) receives the step
  * and makes the call synchronous; with NULL the step is only enqueued (no host round trip). */
 int mhd_gpu_step_rk2(MhdState *state, double dt_fixed, double dt_max, double *dt_used);
+/* One semi-implicit step, mercury::Solver::step_first_order (MercuryUns/driver/Solver.cpp:228-277,
+ * Config::time_order = 1): prepare and the CFL step (or dt_fixed), with the J x B force the opening half-step
+ * gyration, the rhs and forward Euler of the fluid with floors, then the edge EMF from
+ * ImplicitInduction::solve on `ind` (made on the same mesh: its resistivity, Hall coefficient and GMRES
+ * settings) with the step's total cell field and n_e,eff of the fluid cells frozen, the inflow edges
+ * Dirichlet, the rhs's explicit EMF (ideal, ambipolar, boundary values) as E_expl and the warm start of
+ * the previous step, faraday_update with that EMF, and the closing half-step gyration.  FP64 two-ion state.
+ * Synchronous; dt_used, iterations and rel_res (host, may be NULL) receive the step and the solve's
+ * figures; MHD_ENOCONV when the solve stopped at max_it above rtol (the step is still taken, as the
+ * reference takes it). */
+int mhd_gpu_step_semi_implicit(MhdState *state, MhdInduction *ind, double dt_fixed, double dt_max, double *dt_used,
+                               int32_t *iterations, double *rel_res);
 
 /* mercury::add_sources (MercuryUns/fluid/MercurySources.cpp:13-63) for species 0 or 1 of the two-ion
  * model (params: n_species 2, mass[0..1], M_ref, ne_floor, inver_MA2, lorentz, ambipolar, chemistry and

@@ -626,6 +626,8 @@ int solve_impl(MhdInduction *I, const double *Phi, const double *Ee, const int8_
 
 } // namespace
 
+MhdMesh *induction_mesh(const MhdInduction *I) { return I->mesh; }
+
 void drop_cycle_graphs(MhdInduction *I)
 {
     MHD_CUDA(cudaStreamSynchronize(I->mesh->stream));

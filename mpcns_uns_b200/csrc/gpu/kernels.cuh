@@ -5,6 +5,9 @@
 
 namespace mhd
 {
+// gmres.cu: the mesh an induction handle was made on
+MhdMesh *induction_mesh(const MhdInduction *I);
+
 // fluid.cu
 void launch_limited_gradients(const MeshView &m, const FluidParams &p, SField<const double> W, SField<double> G, cudaStream_t s);
 void launch_face_flux(const MeshView &m, const FluidParams &p, SField<const double> W, SField<const double> G, double *F, cudaStream_t s);

@@ -50,6 +50,8 @@ struct MhdState
     mhd::DBuf<double> pn;   // nodal p_e of the ambipolar EMF
     mhd::DBuf<int8_t> pok;  // the node has fluid cells
     mhd::DBuf<double> photo, vst; // source fields of the chemistry terms (empty: absent)
+    mhd::DBuf<double> ne_eff, E_impl; // semi-implicit step: n_e,eff per cell, the implicit EMF per edge
+    mhd::DBuf<int8_t> dir_inflow;     // semi-implicit step: the Dirichlet (inflow) edges of the solve
     mhd::DBuf<float4> g32;  // mixed precision: face terms A_f x b_f of the cell current (per face)
     mhd::DBuf<float4> d32;  // mixed precision: face terms (p_R - p_L) A_f / 2 of grad p_e (per face)
     mhd::DBuf<int32_t> wall_slot; // the caller's Dirichlet wall states: slot per face (-1: ghost_state)

@@ -246,6 +246,21 @@ __global__ void __launch_bounds__(256) k_ct(MeshView m, const double *__restrict
     phio[f] = stage2 ? 0.5 * (phio[f] + v) : v;
 }
 
+// n_e,eff of the fluid cells, 0 elsewhere (Solver.cpp:257-259: mhd::Scales::numinfo of the two ions' densities)
+__global__ void k_ne_eff(MeshView m, SrcParams sp, SField<const double> W, double *__restrict__ ne)
+{
+    const int32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m.nc) return;
+    ne[c] = m.material[c] == 0 ? numinfo2(sp, W(0, c, 0), W(1, c, 0)).ne_eff : 0.0;
+}
+
+// the Dirichlet edges of the semi-implicit solve: the inflow edges (Solver.cpp:261-262)
+__global__ void k_inflow_dir(MeshView m, int8_t *__restrict__ dir)
+{
+    const int32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < m.ne) dir[e] = m.edge_mode[e] == 2 ? 1 : 0;
+}
+
 __global__ void k_aos_to_soa(const double *__restrict__ in, double *__restrict__ out, int32_t n, int ncomp)
 {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -322,7 +337,7 @@ void prepare_cfl(MhdState *st, const double *Us, const double *phis, bool cfl, d
 }
 
 void stage(MhdState *st, const double *Us, const double *phis, double *Uo, double *phio, bool stage2, bool cfl, double dt_max,
-           bool prepared = false)
+           bool prepared = false, bool ct = true)
 {
     MhdMesh *mesh = st->mesh;
     const MeshView &m = mesh->v;
@@ -392,7 +407,7 @@ void stage(MhdState *st, const double *Us, const double *phis, double *Uo, doubl
                            st->sw_edge, st->efgeo.n ? st->efgeo.p : nullptr, st->efgeo.n ? st->pa.p : nullptr);
     P.end(KP_EDGE_EMF, s);
     st->launches += (m.nf ? 1 : 0) + (m.ne ? 1 : 0);
-    if (m.nf)
+    if (ct && m.nf)
     {
         P.begin(KP_CT, s);
         k_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m, st->E.p, phis, phio, st->scal.p, stage2 ? 1 : 0);
@@ -762,6 +777,97 @@ int mhd_gpu_step_rk2(MhdState *st, double dt_fixed, double dt_max, double *dt_us
         if (split && m.no_cells && !st->mixed) ++st->launches; // the FP64 closing gyration
         if (dt_used) read_dt(st, dt_used);
     });
+}
+
+int mhd_gpu_step_semi_implicit(MhdState *st, MhdInduction *ind, double dt_fixed, double dt_max, double *dt_used, int32_t *iterations,
+                               double *rel_res)
+{
+    int status = MHD_OK;
+    const int rc = guarded([&] {
+        MHD_REQUIRE(st && ind, "null state or induction handle");
+        MHD_REQUIRE(dt_fixed > 0 || dt_max > 0, "need dt_fixed > 0 or dt_max > 0");
+        MHD_REQUIRE(!st->mixed, "the semi-implicit step runs on an FP64 state");
+        MHD_REQUIRE(st->nsp == 2, "the semi-implicit step is the two-ion model's");
+        MHD_REQUIRE(induction_mesh(ind) == st->mesh, "the induction handle belongs to another mesh");
+        MhdMesh *mesh = st->mesh;
+        const MeshView &m = mesh->v;
+        cudaStream_t s = mesh->stream;
+        const bool cfl = !(dt_fixed > 0);
+        if (!cfl)
+        {
+            k_set_dt<<<1, 1, 0, s>>>(st->scal.p, dt_fixed, st->flag.p);
+            MHD_LAUNCH_CHECK();
+            ++st->launches;
+        }
+        // Solver::step_first_order (Solver.cpp:228-277): prepare and the CFL step; with the J x B force the
+        // opening half-step gyration and prepare again
+        const bool split = st->src.on && st->src.induce > 0;
+        if (split)
+        {
+            prepare_cfl(st, st->U0.p, st->phi0.p, cfl, dt_max);
+            Reprepare rp;
+            rp.on = 1;
+            rp.fp = st->fp;
+            rp.mass = st->mass.p;
+            rp.M_ref = st->prm.M_ref;
+            rp.U = soa_cstate(st->U0.p, m.nc);
+            rp.W = soa_state(st->W.p, m.nc);
+            rp.up = st->up.p;
+            st->prof.begin(KP_GYRATE, s);
+            launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s, rp);
+            st->prof.end(KP_GYRATE, s);
+            st->launches += m.no_cells ? 1 : 0;
+        }
+        // rhs and forward Euler of the fluid with floors, in place; E = the explicit EMF (ideal, ambipolar,
+        // boundary values); no CT yet
+        stage(st, st->U0.p, st->phi0.p, st->U0.p, st->phi0.p, false, cfl && !split, dt_max, split, false);
+        // the implicit linear terms with the total EMF as the unknown (:250-266)
+        st->ne_eff.alloc(std::max<size_t>(1, (size_t)m.nc));
+        st->E_impl.alloc(std::max<size_t>(1, (size_t)m.ne));
+        if (!st->dir_inflow.n)
+        {
+            st->dir_inflow.alloc(std::max<size_t>(1, (size_t)m.ne));
+            if (m.ne) k_inflow_dir<<<grid_for(m.ne, 256), 256, 0, s>>>(m, st->dir_inflow.p);
+            ++st->launches;
+        }
+        if (m.nc)
+        {
+            k_ne_eff<<<grid_for(m.nc, 256), 256, 0, s>>>(m, st->src, soa_cstate(st->W.p, m.nc), st->ne_eff.p);
+            ++st->launches;
+        }
+        MHD_LAUNCH_CHECK();
+        double dt = 0.0;
+        read_dt(st, &dt);
+        int rcs = mhd_gpu_induction_set_frozen(ind, st->btot.p, st->ne_eff.p);
+        if (rcs != MHD_OK) throw ApiError(rcs, std::string("induction: ") + mhd_gpu_last_error());
+        int32_t it = 0;
+        double rr = 0.0;
+        rcs = mhd_gpu_induction_solve(ind, st->phi0.p, st->E.p, st->dir_inflow.p, dt, 1, st->E_impl.p, &it, &rr);
+        if (rcs != MHD_OK && rcs != MHD_ENOCONV) throw ApiError(rcs, std::string("induction: ") + mhd_gpu_last_error());
+        if (rcs == MHD_ENOCONV) status = MHD_ENOCONV;
+        if (iterations) *iterations = it;
+        if (rel_res) *rel_res = rr;
+        // faraday_update with the implicit EMF (:269), then the closing half-step gyration with the Btot of
+        // the step's prepare (:274)
+        if (m.nf)
+        {
+            st->prof.begin(KP_CT, s);
+            k_ct<<<grid_for(m.nf, 256), 256, 0, s>>>(m, st->E_impl.p, st->phi0.p, st->phi0.p, st->scal.p, 0);
+            MHD_LAUNCH_CHECK();
+            st->prof.end(KP_CT, s);
+            ++st->launches;
+        }
+        if (split)
+        {
+            st->prof.begin(KP_GYRATE, s);
+            launch_gyrate(m, st->src, st->btot.p, nullptr, st->scal.p, 0.5, st->U0.p, s);
+            st->prof.end(KP_GYRATE, s);
+            st->launches += m.no_cells ? 1 : 0;
+        }
+        if (dt_used) *dt_used = dt;
+        MHD_CUDA(cudaStreamSynchronize(s));
+    });
+    return rc != MHD_OK ? rc : status;
 }
 
 int mhd_gpu_state_profile(MhdState *st, int32_t enable)

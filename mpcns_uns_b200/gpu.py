@@ -69,6 +69,7 @@ _SIGS = {
     "mhd_gpu_state_device_ptr": ([vp, i32, ctypes.POINTER(vp)], ctypes.c_int),
     "mhd_gpu_cfl_dt": ([vp, dbl, ctypes.POINTER(dbl)], ctypes.c_int),
     "mhd_gpu_step_rk2": ([vp, dbl, dbl, ctypes.POINTER(dbl)], ctypes.c_int),
+    "mhd_gpu_step_semi_implicit": ([vp, vp, dbl, dbl, ctypes.POINTER(dbl), ctypes.POINTER(i32), ctypes.POINTER(dbl)], ctypes.c_int),
     "mhd_gpu_state_profile": ([vp, i32], ctypes.c_int),
     "mhd_gpu_state_profile_read": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32)], ctypes.c_int),
     "mhd_gpu_state_launches": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
@@ -596,6 +597,17 @@ class ResidentState:
         d = dbl()
         check(lib().mhd_gpu_step_rk2(self._h, float(dt), float(dt_max), ctypes.byref(d) if sync else None))
         return d.value if sync else None
+
+    def step_semi_implicit(self, induction, dt=0.0, dt_max=1e300):
+        """One semi-implicit step (Solver::step_first_order, time_order = 1): forward Euler of the fluid and the
+        EMF of ImplicitInduction::solve on `induction` (a DeviceInduction of the same mesh) -> (dt, iterations,
+        rel_res).  Like the reference, a solve stopped at max_it above rtol does not raise."""
+        d, it, rr = dbl(), i32(), dbl()
+        rc = lib().mhd_gpu_step_semi_implicit(self._h, induction._h, float(dt), float(dt_max), ctypes.byref(d), ctypes.byref(it),
+                                              ctypes.byref(rr))
+        if rc != MHD_ENOCONV:
+            check(rc)
+        return d.value, it.value, rr.value
 
     def profile(self, enable=True):
         check(lib().mhd_gpu_state_profile(self._h, int(bool(enable))))

@@ -35,7 +35,8 @@ class StepParams(ctypes.Structure):
                 ("induce_coeff", dbl), ("inver_MA2", dbl), ("m_res", ctypes.c_void_p), ("ambipolar", i32), ("chemistry", i32),
                 ("pressure_coef", dbl), ("a1_Na", dbl), ("a4", dbl), ("a5", dbl), ("a6", dbl), ("state_coeff_H", dbl),
                 ("state_coeff_Na", dbl), ("T_ref", dbl), ("Tn0", dbl), ("photo", ctypes.c_void_p), ("vst", ctypes.c_void_p),
-                ("n_wall", i32), ("pad2", i32), ("wall_faces", ctypes.c_void_p), ("wall_prims", ctypes.c_void_p)]
+                ("n_wall", i32), ("pad2", i32), ("wall_faces", ctypes.c_void_p), ("wall_prims", ctypes.c_void_p),
+                ("first_order", i32), ("ind_iterations", i32), ("ind", ctypes.c_void_p), ("ind_rel_res", dbl)]
 
 
 def lib():
@@ -381,6 +382,18 @@ class RefMesh:
         BaddCell = np.ascontiguousarray(BaddCell, np.float64)
         _check(lib().ref_rk2_step(self._h, ctypes.byref(params), ctypes.cast(arr, ctypes.c_void_p), _p(Phi), _p(PhiAdd),
                                   _p(BaddCell), dt))
+
+    def first_order_step(self, params: StepParams, ind, U_list, Phi, PhiAdd, BaddCell, dt):
+        """One semi-implicit step (Solver::step_first_order, MercuryUns/driver/Solver.cpp:228-277): forward
+        Euler of the fluid, then the EMF from ind's ImplicitInduction::solve (frozen total field and n_e,eff of
+        the step's prepare, inflow edges Dirichlet, the rhs's EMF as E_expl), CT with it, and with
+        params.lorentz the Strang-split gyration; U_list and Phi in place -> (iterations, rel_res)."""
+        params.first_order = 1
+        params.ind = ind._h
+        self.rk2_step(params, U_list, Phi, PhiAdd, BaddCell, dt)
+        params.first_order = 0
+        params.ind = None
+        return params.ind_iterations, params.ind_rel_res
 
 
 class RefInduction:

@@ -696,6 +696,11 @@ struct RefStepParams
     int32_t n_wall, pad2;
     const int32_t *wall_faces;
     const double *wall_prims;
+    // time_order = 1 (Solver::step_first_order, Solver.cpp:228-277): forward Euler of the fluid and the
+    // semi-implicit induction solve of `ind` (a RefInd handle) for the EMF; iterations and rel_res out
+    int32_t first_order, ind_iterations;
+    void *ind;
+    double ind_rel_res;
 };
 
 namespace
@@ -801,7 +806,7 @@ void floors(const RefStepParams &p, const CellComplex &cx, std::vector<double *>
 } // namespace
 
 // U[s]: 5 per cell (AoS) per species, updated in place; Phi: induced face flux, updated in place.
-int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
+int ref_rk2_step(void *h, RefStepParams *pp, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
 {
     RefMesh *r = static_cast<RefMesh *>(h);
     return guarded([&] {
@@ -920,6 +925,23 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
                 }
             }
             std::copy(phis, phis + nf, phio);
+            if (p.first_order)
+            {
+                // the implicit linear terms with the total EMF as the unknown (Solver.cpp:252-265): frozen total
+                // field and n_e,eff of the fluid cells, inflow edges Dirichlet, E_expl the rhs's EMF
+                ImplicitInduction &ind = *static_cast<RefInd *>(p.ind)->ind;
+                std::vector<double> ne(nc, 0.0);
+                for (Id c = 0; c < nc; ++c)
+                    if (cx.cell_material[c] == kFluid) ne[c] = scfg.sc.numinfo(w.W[0][5 * static_cast<size_t>(c)], w.W[1][5 * static_cast<size_t>(c)]).ne_eff;
+                ind.set_frozen_state(w.Btot.data(), ne.data());
+                std::vector<char> dir(cx.n_edges(), 0);
+                for (Id e = 0; e < cx.n_edges(); ++e) dir[e] = r->bc.edge_mode[e] == 2;
+                std::vector<double> Eimp(cx.n_edges());
+                double res = 0;
+                pp->ind_iterations = ind.solve(phis, w.E.data(), dir, dt, Eimp.data(), &res);
+                pp->ind_rel_res = res;
+                w.E = Eimp;
+            }
             faraday_update(cx, r->active, w.E.data(), phio, dt);
             floors(p, cx, Uo);
         };
@@ -943,6 +965,15 @@ int ref_rk2_step(void *h, const RefStepParams *pp, double *const *U, double *Phi
                 bt[3 * c] = bi[c].x + BaddCell[3 * c]; bt[3 * c + 1] = bi[c].y + BaddCell[3 * c + 1]; bt[3 * c + 2] = bi[c].z + BaddCell[3 * c + 2];
             }
             mercury::gyrate(r->lm, scfg, bt.data(), 0.5 * dt, U0[0], U0[1]);
+        }
+        if (p.first_order)
+        {
+            // one forward Euler stage in place; the closing half step with the Btot of its prepare (Solver.cpp:274)
+            stage(U0, Phi, U1, w.Phi1.data());
+            for (int k = 0; k < ns; ++k) std::copy(U1[k], U1[k] + 5 * static_cast<size_t>(nc), U0[k]);
+            std::copy(w.Phi1.begin(), w.Phi1.end(), Phi);
+            if (split) mercury::gyrate(r->lm, scfg, w.Btot.data(), 0.5 * dt, U0[0], U0[1]);
+            return;
         }
         stage(U0, Phi, U1, w.Phi1.data());
         stage(U1, w.Phi1.data(), U2, w.Phi2.data());
