@@ -22,6 +22,10 @@ on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, c
 reference's own solve on a bounded sample beside it; its "ilu" object is the same FP64 solve with the
 block ILU(0) preconditioner against Jacobi, both capped at --gmres-ilu-max-it iterations.
 
+The "semi_implicit" object (left out with --no-semi-implicit): the reference's default run mode, the
+semi-implicit step of Solver::step_first_order (forward Euler fluid, EMF from the Hall + resistive solve),
+on the same shell in FP64: wall milliseconds per synchronous step and the solve's iterations.
+
 The "ten_ion" object (left out with --no-ten-ion, alone with --ten-ion-only): the ten-ion shell r in
 [1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background field: mixed and FP64 steps and
 the mixed state's error after 50 steps.
@@ -547,6 +551,48 @@ def bench_adjoint(args):
     return out
 
 
+def bench_semi_implicit(args, wl, dm, new_state):
+    """The reference's default run mode (Config::time_order = 1, Solver::step_first_order) on the step's shell:
+    forward Euler of both ions with the J x B force and the Strang-split gyration, the EMF from the Hall +
+    resistive ImplicitInduction::solve (the reference's radial taper from r = 1 to 1.012, eta / star1 with
+    eta = 1e-2 below r = 1.2 and 1e-4 above, GMRES(30) to rtol 1e-8 capped at --si-max-it, warm start across
+    steps), CT with it; FP64, CFL step.  The Hall coefficient is set so that the initial CFL step is
+    --si-whistler-ratio times the explicit whistler limit of the initial state (the stiffness the implicit
+    treatment is for; config 3's ratio of 20 stagnates Jacobi GMRES).  Wall time of each synchronous step."""
+    import torch
+    from mpcns_uns_b200 import gpu, workloads
+    h = wl.mesh
+    st = new_state("fp64")
+    r_e = np.linalg.norm(np.asarray(h["edge_mid"]), axis=1)
+    m_edge = np.where(r_e < 1.2, 1e-2, 1e-4) / np.asarray(h["star1"])
+    # n_e,eff (M_ref 1, ne_floor 0.01) and |B_tot| of the initial state; whistler limit of hall_coef 1
+    nc = h.n_cells
+    ne = np.asarray(wl.U[0]).reshape(nc, 5)[:, 0] / wl.mass[0] + np.asarray(wl.U[1]).reshape(nc, 5)[:, 0] / wl.mass[1]
+    ne_eff = np.sqrt(ne * ne + 1e-4)
+    B = dm.reconstruct_cell_vector(np.asarray(wl.Phi) + np.asarray(wl.PhiAdd)).cpu().numpy()
+    dtw1 = workloads.whistler_dt(h, B, ne_eff, 1.0, 1.0)
+    hall_coef = args.si_whistler_ratio * dtw1 / st.cfl_dt()
+    di = gpu.DeviceInduction(dm, m_edge, hall=True, hall_coef=hall_coef, hall_r_min=1.0, hall_r_max=1.012, rtol=1e-8,
+                             max_it=args.si_max_it, restart=30)
+    st.step_semi_implicit(di)  # warm-up: the solve's tables and captured restart cycle
+    torch.cuda.synchronize()
+    ms, its, rrs, dts = [], [], [], []
+    for _ in range(args.si_steps):
+        t0 = time.perf_counter()
+        dt, it, rr = st.step_semi_implicit(di)
+        ms.append((time.perf_counter() - t0) * 1e3)
+        its.append(it)
+        rrs.append(rr)
+        dts.append(dt)
+    out = {"workload": wl.name, "cells": h.n_cells, "edges": h.n_edges, "steps": args.si_steps, "ms_per_step": float(np.median(ms)),
+           "iterations": its, "rel_res": rrs, "dt": dts, "max_it": args.si_max_it, "rtol": 1e-8, "restart": 30, "hall_coef": hall_coef,
+           "dt_over_whistler_limit": args.si_whistler_ratio,
+           "eta": "1e-2 for r < 1.2, 1e-4 above", "precision": "fp64"}
+    log(f"[bench] semi-implicit step: {out['ms_per_step']:.1f} ms per step, iterations {its}, rel_res {max(rrs):.2e}")
+    del di, st
+    return out
+
+
 def bench_ten_ion(args, peak):
     """Config 5: the ten-ion shell r in [1, 8], 6 x 96 x 96 x 128 x 6 tetrahedra (42.5M cells), crustal background
     field, no model sources: mixed and FP64 steps (CFL 0.4 on the device), per-kernel times, and the mixed state's
@@ -662,6 +708,9 @@ def summary(out):
             sm["gmres"]["ilu"] = {"it": il["max_it"], "s": [_r(il["ilu"]["s_per_solve"]), _r(il["jacobi"]["s_per_solve"])],
                                   "rel_res": [_r(il["ilu"]["rel_res"], 3), _r(il["jacobi"]["rel_res"], 3)],
                                   "factor_apply_ms": [_r(il["factor_ms"]), _r(il["apply_ms"])]}
+    si = out.get("semi_implicit")
+    if si:
+        sm["semi_implicit"] = {"ms": _r(si["ms_per_step"]), "it": si["iterations"], "rel_res": _r(max(si["rel_res"]), 3)}
     d = out.get("adjoint")
     if d:
         fd = d["fd"]
@@ -709,6 +758,10 @@ def main():
     ap.add_argument("--gmres-max-it", type=int, default=300)
     ap.add_argument("--gmres-solves", type=int, default=2)
     ap.add_argument("--gmres-ilu-max-it", type=int, default=60, help="block ILU(0) leg against Jacobi (0: skip)")
+    ap.add_argument("--no-semi-implicit", action="store_true", help="leave out the time_order = 1 step")
+    ap.add_argument("--si-steps", type=int, default=3)
+    ap.add_argument("--si-max-it", type=int, default=100)
+    ap.add_argument("--si-whistler-ratio", type=float, default=2.0)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-ten-ion", action="store_true", help="leave out the ten-ion shell (config 5, 42.5M cells)")
     ap.add_argument("--ten-ion-only", action="store_true", help="run only the ten-ion section and print it as its own JSON line")
@@ -908,7 +961,14 @@ def main():
     # the configuration sections run once, on a single-GPU run (under torchrun the replicas time the step only)
     if world > 1:
         args.no_gmres = args.no_adjoint = True
-        args.no_ten_ion = True
+        args.no_ten_ion = args.no_semi_implicit = True
+    si = None
+    if rank == 0 and not args.no_semi_implicit and wl.n_species == 2:
+        try:
+            si = bench_semi_implicit(args, wl, dm, new_state)
+        except Exception as e:  # reported, not required
+            log(f"[bench] semi-implicit step failed: {e}")
+        torch.cuda.empty_cache()
     if rank == 0 and not args.no_gmres:
         del st64, st32, st
         torch.cuda.empty_cache()
@@ -957,7 +1017,7 @@ def main():
                         "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
                "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "adjoint": adj, "ten_ion": ten}
+               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "semi_implicit": si, "adjoint": adj, "ten_ion": ten}
         out["summary"] = summary(out)
         print(json.dumps(out))
     if dist:
