@@ -226,8 +226,8 @@ int mhd_gpu_cell_current(MhdMesh *mesh, const double *B, double *J);
 /* ------------------------------------------------------------------ semi-implicit induction
  * mhd::ImplicitInduction (Common/induction/ImplicitInduction.h:27-94): the operator
  *   F(Phi) = M d1^T S2 Phi + H(Phi),  A x = x + dt F(d1 x)
- * and the restarted GMRES(m) with Givens rotations, Jacobi right preconditioner, true residual at
- * every restart and warm start (.cpp:299-390).  The reference orthogonalises with modified
+ * and the restarted GMRES(m) with Givens rotations, Jacobi right preconditioner (or block ILU(0):
+ * mhd_gpu_induction_set_ilu), true residual at every restart and warm start (.cpp:299-390).  The reference orthogonalises with modified
  * Gram-Schmidt; here (restart <= 31) classical Gram-Schmidt with a second pass where the first
  * cancelled and left components above round-off: the same Krylov space and Hessenberg matrix to
  * rounding, two or three passes over the basis per Arnoldi step (restart > 31: modified Gram-Schmidt).  The resistive
