@@ -834,8 +834,8 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
  * mhd::ImplicitInduction (Common/induction/ImplicitInduction.cpp): constructor tables (:10-103),
  * set_frozen_state (:105-111), apply_F (:127-183), apply_A (:185-198), dot_owned (:200-207) and the
  * restarted GMRES(m) with modified Gram-Schmidt, Givens rotations and the Jacobi right
- * preconditioner (:299-390).  The resistive coefficient m_e = eta_e / star1_e is an input (the
- * reference fills it from its tanh window). */
+ * preconditioner (:299-390), or the block-Jacobi ILU(0) (:209-297).  The resistive coefficient
+ * m_e = eta_e / star1_e is an input (the reference fills it from its tanh window). */
 struct OrInduction
 {
     const OrMesh *m;
@@ -845,6 +845,12 @@ struct OrInduction
     int64_t *ce_ptr;
     int32_t *ce_edge;
     double *phi, *bcell, *part, *tmp;
+    /* block-Jacobi ILU(0) of the owned edges (:209-297) */
+    int ilu;
+    double shift;
+    int64_t *pc_ptr, *pc_diag;
+    int32_t *pc_col;
+    double *pc_coef, *pc_val;
 };
 
 OrInduction *or_ind_create(const OrMesh *m, const OrIndParams *p, const double *m_edge)
@@ -952,7 +958,150 @@ void or_ind_free(OrInduction *s)
     if (!s) return;
     free(s->m_edge); free(s->taper); free(s->alpha); free(s->B0); free(s->recon); free(s->d2); free(s->ce_wt); free(s->corr);
     free(s->ce_ptr); free(s->ce_edge); free(s->phi); free(s->bcell); free(s->part); free(s->tmp);
+    free(s->pc_ptr); free(s->pc_diag); free(s->pc_col); free(s->pc_coef); free(s->pc_val);
     free(s);
+}
+
+/* build_precond_pattern (:209-242): per owned row e the entries (e2, m_e s_e,f s_e2,f star2_f) of every face of
+ * e and every owned edge e2 of that face, plus (e, 0), sorted by column (insertion sort: ties keep the
+ * gathering order), equal columns summed in that order */
+void or_ind_set_ilu(OrInduction *s, int32_t enable, double shift)
+{
+    const OrMesh *m = s->m;
+    const int32_t no = m->n_owned_edges;
+    s->shift = shift;
+    s->ilu = enable != 0 && (s->resistive || s->hall);
+    if (!s->ilu || s->pc_ptr) return;
+    int64_t cap = 1024, nnz = 0;
+    s->pc_ptr = (int64_t *)calloc((size_t)no + 1, sizeof(int64_t));
+    s->pc_col = (int32_t *)malloc((size_t)cap * sizeof(int32_t));
+    s->pc_coef = (double *)malloc((size_t)cap * sizeof(double));
+    int32_t rc[1024];
+    double rv[1024];
+    for (int32_t e = 0; e < no; ++e)
+    {
+        int n = 0;
+        rc[n] = e; rv[n] = 0.0; ++n;
+        for (int64_t kf = m->e2f_ptr[e]; kf < m->e2f_ptr[e + 1]; ++kf)
+        {
+            const int32_t f = m->e2f_idx[kf];
+            const double se = m->e2f_sgn[kf];
+            for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k)
+            {
+                const int32_t e2 = m->f2e_idx[k];
+                if (e2 >= no || n >= 1024) continue;
+                rc[n] = e2; rv[n] = s->m_edge[e] * se * m->f2e_sgn[k] * m->star2[f]; ++n;
+            }
+        }
+        for (int i = 1; i < n; ++i)
+        {
+            const int32_t c = rc[i];
+            const double v = rv[i];
+            int j = i - 1;
+            while (j >= 0 && rc[j] > c) { rc[j + 1] = rc[j]; rv[j + 1] = rv[j]; --j; }
+            rc[j + 1] = c; rv[j + 1] = v;
+        }
+        for (int i = 0; i < n;)
+        {
+            int j = i;
+            double sum = 0;
+            for (; j < n && rc[j] == rc[i]; ++j) sum += rv[j];
+            if (nnz == cap)
+            {
+                cap *= 2;
+                s->pc_col = (int32_t *)realloc(s->pc_col, (size_t)cap * sizeof(int32_t));
+                s->pc_coef = (double *)realloc(s->pc_coef, (size_t)cap * sizeof(double));
+            }
+            s->pc_col[nnz] = rc[i];
+            s->pc_coef[nnz] = sum;
+            ++nnz;
+            i = j;
+        }
+        s->pc_ptr[e + 1] = nnz;
+    }
+    s->pc_val = (double *)calloc((size_t)nnz + 1, sizeof(double));
+    s->pc_diag = (int64_t *)calloc((size_t)no + 1, sizeof(int64_t));
+    for (int32_t e = 0; e < no; ++e)
+        for (int64_t k = s->pc_ptr[e]; k < s->pc_ptr[e + 1]; ++k)
+            if (s->pc_col[k] == e) s->pc_diag[e] = k;
+}
+
+int64_t or_ind_ilu_pattern(OrInduction *s, int64_t *ptr, int32_t *col, double *coef)
+{
+    if (!s->pc_ptr) return -1;
+    const int32_t no = s->m->n_owned_edges;
+    const int64_t nnz = s->pc_ptr[no];
+    if (ptr) memcpy(ptr, s->pc_ptr, ((size_t)no + 1) * sizeof(int64_t));
+    if (col) memcpy(col, s->pc_col, (size_t)nnz * sizeof(int32_t));
+    if (coef) memcpy(coef, s->pc_coef, (size_t)nnz * sizeof(double));
+    return nnz;
+}
+
+/* factor_precond (:247-275): Dirichlet rows and columns removed, the relaxed diagonal, IKJ elimination with the
+ * breakdown guard */
+static void ilu_factor(OrInduction *s, double dt, const int8_t *dir)
+{
+    const int32_t no = s->m->n_owned_edges;
+    const int64_t *P = s->pc_ptr, *D = s->pc_diag;
+    const int32_t *C = s->pc_col;
+    double *V = s->pc_val;
+    for (int32_t e = 0; e < no; ++e)
+        for (int64_t k = P[e]; k < P[e + 1]; ++k)
+        {
+            const int32_t c = C[k];
+            const int de = dir && dir[e], dc = dir && dir[c];
+            V[k] = (de || dc) ? (c == e ? 1.0 : 0.0) : (c == e ? 1.0 : 0.0) + dt * s->pc_coef[k];
+            if (c == e && !de) V[k] += s->shift * dt * s->pc_coef[k];
+        }
+    int64_t *pos = (int64_t *)malloc(((size_t)s->m->n_edges + 1) * sizeof(int64_t));
+    for (int32_t e = 0; e <= s->m->n_edges; ++e) pos[e] = -1;
+    for (int32_t i = 0; i < no; ++i)
+    {
+        for (int64_t k = P[i]; k < P[i + 1]; ++k) pos[C[k]] = k;
+        for (int64_t kk = P[i]; kk < P[i + 1] && C[kk] < i; ++kk)
+        {
+            const int32_t k = C[kk];
+            V[kk] /= V[D[k]];
+            const double lik = V[kk];
+            for (int64_t jj = D[k] + 1; jj < P[k + 1]; ++jj)
+            {
+                const int64_t q = pos[C[jj]];
+                if (q >= 0) V[q] -= lik * V[jj];
+            }
+        }
+        if (!(fabs(V[D[i]]) > 1e-12)) V[D[i]] = 1.0;
+        for (int64_t k = P[i]; k < P[i + 1]; ++k) pos[C[k]] = -1;
+    }
+    free(pos);
+}
+
+/* apply_precond (:277-297): unit lower, then upper; z = 0 on the non-owned edges */
+static void ilu_apply(const OrInduction *s, const double *v, double *z, const int8_t *dir)
+{
+    const int32_t no = s->m->n_owned_edges, ne = s->m->n_edges;
+    const int64_t *P = s->pc_ptr, *D = s->pc_diag;
+    const int32_t *C = s->pc_col;
+    const double *V = s->pc_val;
+    for (int32_t i = 0; i < no; ++i)
+    {
+        double t = (dir && dir[i]) ? 0.0 : v[i];
+        for (int64_t k = P[i]; k < D[i]; ++k) t -= V[k] * z[C[k]];
+        z[i] = t;
+    }
+    for (int32_t i = no; i-- > 0;)
+    {
+        double t = z[i];
+        for (int64_t k = D[i] + 1; k < P[i + 1]; ++k) t -= V[k] * z[C[k]];
+        z[i] = (dir && dir[i]) ? 0.0 : t / V[D[i]];
+    }
+    for (int32_t e = no; e < ne; ++e) z[e] = 0.0;
+}
+
+void or_ind_ilu_precond(OrInduction *s, double dt, const int8_t *dir, const double *v, double *z)
+{
+    if (!s->pc_ptr) return;
+    ilu_factor(s, dt, dir);
+    ilu_apply(s, v, z, dir);
 }
 
 void or_ind_set_frozen(OrInduction *s, const double *B0, const double *ne)
@@ -1053,6 +1202,8 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
     or_ind_apply_A(s, x0, dt, Ax);
     for (int32_t e = 0; e < ne; ++e) r[e] = dir[e] ? 0.0 : b[e] - Ax[e];
     for (int32_t e = 0; e < ne; ++e) idg[e] = 1.0 / (1.0 + dt * s->m_edge[e] * s->d2[e]);
+    const int ilu = s->ilu && s->pc_ptr; /* (:317-318) */
+    if (ilu) ilu_factor(s, dt, dir);
     const double bnorm = sqrt(dmax(dot_owned(m, b, b), 1e-300));
     double beta = sqrt(dot_owned(m, r, r));
     int total = 0;
@@ -1065,7 +1216,8 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
         for (; j < mr && total < s->p.max_it; ++j, ++total)
         {
             const double *Vj = V + (size_t)j * (size_t)ne;
-            for (int32_t e = 0; e < ne; ++e) z[e] = dir[e] ? 0.0 : Vj[e] * idg[e];
+            if (ilu) ilu_apply(s, Vj, z, dir);
+            else for (int32_t e = 0; e < ne; ++e) z[e] = dir[e] ? 0.0 : Vj[e] * idg[e];
             or_ind_apply_A(s, z, dt, w);
             for (int32_t e = 0; e < ne; ++e)
                 if (dir[e]) w[e] = 0.0;
@@ -1108,7 +1260,13 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
             for (int i = 0; i < j; ++i) t += yv[i] * V[(size_t)i * (size_t)ne + e];
             comb[e] = t;
         }
-        for (int32_t e = 0; e < ne; ++e) delta[e] += dir[e] ? 0.0 : comb[e] * idg[e];
+        if (ilu)
+        {
+            ilu_apply(s, comb, z, dir);
+            for (int32_t e = 0; e < ne; ++e) delta[e] += z[e];
+        }
+        else
+            for (int32_t e = 0; e < ne; ++e) delta[e] += dir[e] ? 0.0 : comb[e] * idg[e];
         for (int32_t e = 0; e < ne; ++e) z[e] = x0[e] + delta[e];
         or_ind_apply_A(s, z, dt, Ax);
         for (int32_t e = 0; e < ne; ++e) r[e] = dir[e] ? 0.0 : b[e] - Ax[e];

@@ -92,4 +92,13 @@ void or_ind_apply_F(OrInduction *s, const double *phi, double *out);
 void or_ind_apply_A(OrInduction *s, const double *x, double dt, double *y);
 int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *E_expl, const int8_t *dir, double dt, int32_t warm, double *E,
                      double *rel_res);
+/* block-Jacobi ILU(0) (ImplicitInduction.cpp:209-297): enable builds the pattern of the owned rows and makes
+ * or_ind_solve factor and apply it in place of the Jacobi scaling.  Ties of the column sort keep the
+ * gathering order (the reference's std::sort leaves them in an order of its own), so the diagonal
+ * coefficients agree with the reference's to rounding and everything else bit for bit. */
+void or_ind_set_ilu(OrInduction *s, int32_t enable, double shift);
+/* the pattern (ptr n_owned + 1, col / coef nnz; NULL: skipped); returns nnz, -1 without a pattern */
+int64_t or_ind_ilu_pattern(OrInduction *s, int64_t *ptr, int32_t *col, double *coef);
+/* factor_precond(dt, dir) then apply_precond(v) -> z (n_edges each; dir may be NULL) */
+void or_ind_ilu_precond(OrInduction *s, double dt, const int8_t *dir, const double *v, double *z);
 #endif

@@ -100,6 +100,9 @@ def lib():
             ("or_ind_apply_F", [vp, vp, vp], None),
             ("or_ind_apply_A", [vp, vp, dbl, vp], None),
             ("or_ind_solve", [vp, vp, vp, vp, dbl, i32, vp, vp], i32),
+            ("or_ind_set_ilu", [vp, i32, dbl], None),
+            ("or_ind_ilu_pattern", [vp, vp, vp, vp], i64),
+            ("or_ind_ilu_precond", [vp, dbl, vp, vp, vp], None),
         ]:
             f = getattr(L, name)
             f.argtypes = args
@@ -263,7 +266,7 @@ class PortMesh:
 
 
 class PortInduction:
-    """The oracle's mhd::ImplicitInduction (Jacobi-preconditioned restarted GMRES)."""
+    """The oracle's mhd::ImplicitInduction (restarted GMRES, Jacobi or block ILU(0) preconditioner)."""
 
     def __init__(self, pm: PortMesh, m_edge=None, hall=False, hall_coef=0.0, hall_r_min=1.0, hall_r_max=1.012, rtol=1e-4,
                  max_it=100, restart=20):
@@ -288,6 +291,27 @@ class PortInduction:
         o = np.zeros(self.pm.n_edges)
         lib().or_ind_apply_A(self._h, _p(_f(x)), dt, _p(o))
         return o
+
+    def set_ilu(self, enable=True, shift=0.3):
+        """Config::ind_ilu / ind_ilu_shift: block-Jacobi ILU(0) in place of the Jacobi scaling."""
+        lib().or_ind_set_ilu(self._h, int(bool(enable)), float(shift))
+
+    def ilu_pattern(self):
+        """(pc_ptr, pc_col, pc_coef) of the owned rows."""
+        nnz = lib().or_ind_ilu_pattern(self._h, None, None, None)
+        if nnz < 0:
+            raise RuntimeError("no ILU(0) pattern")
+        ptr = np.zeros(self.pm.n_edges + 1, np.int64)
+        col, coef = np.zeros(nnz, np.int32), np.zeros(nnz)
+        lib().or_ind_ilu_pattern(self._h, _p(ptr), _p(col), _p(coef))
+        return ptr, col, coef
+
+    def precond(self, dt, dirichlet, v):
+        """factor_precond(dt, dir) then apply_precond(v) -> z."""
+        z = np.zeros(self.pm.n_edges)
+        d = np.ascontiguousarray(dirichlet, np.int8)
+        lib().or_ind_ilu_precond(self._h, dt, _p(d), _p(_f(v)), _p(z))
+        return z
 
     def solve(self, Phi, E_expl, dirichlet, dt, warm=True):
         E = np.zeros(self.pm.n_edges)
