@@ -743,7 +743,10 @@ void or_resistive_emf(const OrMesh *m, const double *m_res, const double *phi, d
     free(p0);
 }
 
-int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
+/* One step of the hot path: the SSP-RK2 step of Solver::step (ind NULL), or with ind the semi-implicit step of
+ * Solver::step_first_order (Solver.cpp:228-277): one forward Euler stage whose EMF is ind's solve */
+static int step_impl(const OrMesh *m, const OrStepParams *p, OrInduction *ind, double *const *U, double *Phi, const double *PhiAdd,
+                     const double *BaddCell, double dt, int32_t *iterations, double *rel_res)
 {
     const int32_t nc = m->n_cells, nf = m->n_faces, ne = m->n_edges, ns = p->n_species;
     const size_t c5 = 5 * (size_t)nc;
@@ -765,7 +768,10 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
         for (size_t i = 0; i < 3 * (size_t)nc; ++i) Bt[i] = Bi[i] + BaddCell[i];
         or_gyrate(m, p, Bt, 0.5 * dt, Us[0], Us[1]);
     }
-    for (int st = 0; st < 2; ++st)
+    double *Eimp = ind ? (double *)malloc(sizeof(double) * ((size_t)ne + 1)) : NULL;
+    double *nec = ind ? (double *)malloc(sizeof(double) * ((size_t)nc + 1)) : NULL;
+    int8_t *dirv = ind ? (int8_t *)malloc((size_t)ne + 1) : NULL;
+    for (int st = 0; st < (ind ? 1 : 2); ++st)
     {
         double *const *Ui = st == 0 ? Us : U1s;
         double *const *Uo = st == 0 ? U1s : U2s;
@@ -806,6 +812,20 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
         if (p->ambipolar) or_ambipolar_emf(m, p, W, W + c5, E); /* Solver.cpp:158 */
         or_edge_modes(m, p->u_inf, p->B_imf, E);
         if (p->m_res) or_resistive_emf(m, p->m_res, phis, E);
+        if (ind)
+        {
+            /* the implicit linear terms with the total EMF as the unknown (Solver.cpp:252-265): frozen total field
+             * and n_e,eff of the fluid cells, inflow edges Dirichlet, E_expl the rhs's EMF, warm start */
+            for (int32_t c = 0; c < nc; ++c)
+                nec[c] = m->cell_material[c] == 0 ? numinfo(p, W[5 * (size_t)c], W[c5 + 5 * (size_t)c]).ne_eff : 0.0;
+            for (int32_t e = 0; e < ne; ++e) dirv[e] = m->edge_mode[e] == 2;
+            or_ind_set_frozen(ind, Bt, nec);
+            double rr = 0;
+            const int32_t it = or_ind_solve(ind, phis, E, dirv, dt, 1, Eimp, &rr);
+            if (iterations) *iterations = it;
+            if (rel_res) *rel_res = rr;
+            memcpy(E, Eimp, sizeof(double) * (size_t)ne);
+        }
         for (int s = 0; s < ns; ++s)
         {
             memcpy(Uo[s], Ui[s], sizeof(double) * c5);
@@ -819,15 +839,39 @@ int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double
         or_faraday(m, E, NULL, dt, phio);
         floors(m, p, Uo);
     }
-    for (int s = 0; s < ns; ++s)
-        for (size_t i = 0; i < c5; ++i) U[s][i] = 0.5 * (U[s][i] + U2s[s][i]);
-    for (int32_t f = 0; f < nf; ++f) Phi[f] = 0.5 * (Phi[f] + P2[f]);
-    /* the closing half step with Btot of the stage-2 input (Solver.cpp:510) */
+    if (ind)
+    {
+        /* the forward Euler result; the closing half step with Btot of the step's prepare (Solver.cpp:274) */
+        for (int s = 0; s < ns; ++s) memcpy(U[s], U1s[s], sizeof(double) * c5);
+        memcpy(Phi, P1, sizeof(double) * (size_t)nf);
+    }
+    else
+    {
+        for (int s = 0; s < ns; ++s)
+            for (size_t i = 0; i < c5; ++i) U[s][i] = 0.5 * (U[s][i] + U2s[s][i]);
+        for (int32_t f = 0; f < nf; ++f) Phi[f] = 0.5 * (Phi[f] + P2[f]);
+    }
+    /* the closing half step with Btot of the last stage's input (Solver.cpp:510) */
     if (split) or_gyrate(m, p, Bt, 0.5 * dt, Us[0], Us[1]);
     free(Jc);
     free(dpe);
+    free(Eimp);
+    free(nec);
+    free(dirv);
     free(mem);
     return 0;
+}
+
+int or_rk2_step(const OrMesh *m, const OrStepParams *p, double *const *U, double *Phi, const double *PhiAdd, const double *BaddCell, double dt)
+{
+    return step_impl(m, p, NULL, U, Phi, PhiAdd, BaddCell, dt, NULL, NULL);
+}
+
+int or_first_order_step(const OrMesh *m, const OrStepParams *p, OrInduction *ind, double *const *U, double *Phi, const double *PhiAdd,
+                        const double *BaddCell, double dt, int32_t *iterations, double *rel_res)
+{
+    if (!ind || p->n_species != 2) return -1;
+    return step_impl(m, p, ind, U, Phi, PhiAdd, BaddCell, dt, iterations, rel_res);
 }
 
 /* ------------------------------------------------------------------ semi-implicit induction

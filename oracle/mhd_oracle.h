@@ -92,6 +92,12 @@ void or_ind_apply_F(OrInduction *s, const double *phi, double *out);
 void or_ind_apply_A(OrInduction *s, const double *x, double dt, double *y);
 int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *E_expl, const int8_t *dir, double dt, int32_t warm, double *E,
                      double *rel_res);
+/* one semi-implicit step, mercury::Solver::step_first_order (MercuryUns/driver/Solver.cpp:228-277): forward Euler of
+ * the fluid (with the opening and closing half-step gyration when lorentz is on), the EMF from ind's solve (frozen
+ * total field and n_e,eff of the step, inflow edges Dirichlet, the rhs's EMF as E_expl, warm start) and CT with it;
+ * two ions; -1 on bad arguments */
+int or_first_order_step(const OrMesh *m, const OrStepParams *p, OrInduction *ind, double *const *U, double *Phi, const double *PhiAdd,
+                        const double *BaddCell, double dt, int32_t *iterations, double *rel_res);
 /* block-Jacobi ILU(0) (ImplicitInduction.cpp:209-297): enable builds the pattern of the owned rows and makes
  * or_ind_solve factor and apply it in place of the Jacobi scaling.  Ties of the column sort keep the
  * gathering order (the reference's std::sort leaves them in an order of its own), so the diagonal

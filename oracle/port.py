@@ -90,6 +90,7 @@ def lib():
             ("or_cell_current", [P(OrMesh), vp, vp], None),
             ("or_local_time_step", [P(OrMesh), i32, vp, vp, dbl, dbl, dbl, dbl], dbl),
             ("or_rk2_step", [P(OrMesh), P(OrStepParams), vp, vp, vp, vp, dbl], ctypes.c_int),
+            ("or_first_order_step", [P(OrMesh), P(OrStepParams), vp, vp, vp, vp, vp, dbl, P(i32), P(dbl)], ctypes.c_int),
             ("or_add_sources", [P(OrMesh), P(OrStepParams), i32, vp, vp, vp, vp, vp, vp, vp, dbl, vp], None),
             ("or_electron_pressure_gradient", [P(OrMesh), vp, vp, vp], None),
             ("or_ambipolar_emf", [P(OrMesh), P(OrStepParams), vp, vp, vp], None),
@@ -263,6 +264,18 @@ class PortMesh:
         rc = lib().or_rk2_step(self.ref, ctypes.byref(p), ctypes.cast(arr, ctypes.c_void_p), _p(Phi), _p(_f(wl.PhiAdd)), _p(_f(Badd)), dt)
         if rc != 0:
             raise RuntimeError("oracle rk2 step failed")
+
+    def first_order_step(self, wl, ind, U_list, Phi, Badd, dt, lorentz=False, induce_coeff=0.0, inver_MA2=1.0):
+        """One semi-implicit step (Solver::step_first_order) with the EMF of ind's solve (a PortInduction of this
+        mesh); U_list and Phi updated in place -> (iterations, rel_res)."""
+        p = self.step_params(wl, None, lorentz, induce_coeff, inver_MA2)
+        arr = (ctypes.c_void_p * len(U_list))(*[u.ctypes.data for u in U_list])
+        it, rr = i32(), dbl()
+        rc = lib().or_first_order_step(self.ref, ctypes.byref(p), ind._h, ctypes.cast(arr, ctypes.c_void_p), _p(Phi), _p(_f(wl.PhiAdd)),
+                                       _p(_f(Badd)), dt, ctypes.byref(it), ctypes.byref(rr))
+        if rc != 0:
+            raise RuntimeError("oracle first-order step failed")
+        return it.value, rr.value
 
 
 class PortInduction:

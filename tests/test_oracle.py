@@ -304,3 +304,34 @@ def test_reference_built_shell_is_the_workload_shell(ncube, nr, n_solid):
     wh = workloads.shell_state(h, "h", 1.0, st, sources=True)
     wr = workloads.shell_state(r, "r", 1.0, st, sources=True)
     assert all(np.array_equal(a, b) for a, b in zip(wh.U, wr.U)) and np.array_equal(wh.PhiAdd, wr.PhiAdd)
+
+
+def test_semi_implicit_step():
+    """Solver::step_first_order (time_order = 1): forward Euler of both ions with the J x B force and the Strang-split
+    gyration, the EMF from the Hall + resistive ImplicitInduction::solve (warm start across steps), CT with it,
+    bit for bit against the reference's sequence; the solve's iterations and residual equal."""
+    from mpcns_uns_b200 import workloads
+    wl = workloads.shell(4, 5)
+    h = wl.mesh
+    r = ref_twin(h, SHELL_TAGS).boundary(*SHELL_BC)
+    o = port.PortMesh(h)
+    rp = _ref_params(wl, True, 1.0, 1.0)
+    r_e = np.linalg.norm(np.asarray(h["edge_mid"]), axis=1)
+    m_edge = np.where(r_e < 1.5, 1e-2, 1e-4) / np.asarray(h["star1"])
+    kw = dict(hall=True, hall_coef=0.5, hall_r_min=1.0, hall_r_max=1.6, rtol=1e-10, max_it=300, restart=30)
+    ri = ref.RefInduction(r, **kw)
+    ri.set_m(m_edge)
+    oi = port.PortInduction(o, m_edge, **kw)
+    Badd = r.cell_vector(wl.PhiAdd)
+    Uo = [np.array(u) for u in wl.U]
+    Ur = [np.array(u) for u in wl.U]
+    Po, Pr = np.array(wl.Phi), np.array(wl.Phi)
+    for _ in range(3):
+        W = [r.to_prim(u, wl.gamma) for u in Ur]
+        dt = r.local_time_step(wl.gamma, 0.4, 1.0, 1e-2, W[0], W[1], r.cell_vector(Pr) + Badd)
+        ito, rro = o.first_order_step(wl, oi, Uo, Po, Badd, dt, lorentz=True, induce_coeff=1.0, inver_MA2=1.0)
+        itr, rrr = r.first_order_step(rp, ri, Ur, Pr, wl.PhiAdd, Badd, dt)
+        assert ito == itr and rro == rrr and rrr <= 1e-10
+        for a, b in zip(Uo, Ur):
+            same(a, b)
+        same(Po, Pr)
