@@ -889,6 +889,11 @@ struct OrInduction
     int64_t *ce_ptr;
     int32_t *ce_edge;
     double *phi, *bcell, *part, *tmp;
+    /* the implicit ideal part (set_ideal_state, :112-116): frozen cell velocities, the edges that carry it */
+    int ideal;
+    double cuct;
+    double *u_ideal, *ide;
+    int8_t *imask;
     /* block-Jacobi ILU(0) of the owned edges (:209-297) */
     int ilu;
     double shift;
@@ -1003,6 +1008,7 @@ void or_ind_free(OrInduction *s)
     free(s->m_edge); free(s->taper); free(s->alpha); free(s->B0); free(s->recon); free(s->d2); free(s->ce_wt); free(s->corr);
     free(s->ce_ptr); free(s->ce_edge); free(s->phi); free(s->bcell); free(s->part); free(s->tmp);
     free(s->pc_ptr); free(s->pc_diag); free(s->pc_col); free(s->pc_coef); free(s->pc_val);
+    free(s->u_ideal); free(s->ide); free(s->imask);
     free(s);
 }
 
@@ -1155,19 +1161,19 @@ void or_ind_set_frozen(OrInduction *s, const double *B0, const double *ne)
     for (int32_t c = 0; c < nc; ++c) s->alpha[c] = (s->hall && ne[c] > 0) ? s->taper[c] * s->p.hall_coef / ne[c] : 0.0;
 }
 
-void or_ind_apply_F(OrInduction *s, const double *phi, double *out)
+/* apply_F (:127-183) with the resistive and Hall parts as given (ideal_linear, :118-124, turns both off) */
+static void apply_F_parts(OrInduction *s, const double *phi, double *out, int resistive, int hall)
 {
     const OrMesh *m = s->m;
     const int32_t ne = m->n_edges, nc = m->n_cells;
     memset(s->part, 0, 3 * (size_t)ne * sizeof(double));
-    if (s->resistive)
+    if (resistive)
         for (int32_t f = 0; f < m->n_faces; ++f)
         {
             const double v = m->star2[f] * phi[f];
             for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) s->part[3 * (int64_t)m->f2e_idx[k]] += m->f2e_sgn[k] * v;
         }
-    if (s->hall)
-    {
+    if (hall || s->ideal) /* the cell field from the face fluxes (:138-149) */
         for (int32_t c = 0; c < nc; ++c)
         {
             double b[3] = {0, 0, 0};
@@ -1178,6 +1184,14 @@ void or_ind_apply_F(OrInduction *s, const double *phi, double *out)
             }
             s->bcell[3 * (int64_t)c] = b[0]; s->bcell[3 * (int64_t)c + 1] = b[1]; s->bcell[3 * (int64_t)c + 2] = b[2];
         }
+    if (s->ideal) /* the ideal EMF of the frozen velocities and that field, on the masked edges (:150-158) */
+    {
+        memset(s->ide, 0, (size_t)ne * sizeof(double));
+        or_ideal_emf(m, s->u_ideal, s->bcell, s->bcell, phi, phi, s->cuct, s->ide);
+        for (int32_t e = 0; e < ne; ++e) s->part[3 * (int64_t)e + 2] = s->imask[e] ? s->ide[e] : 0.0;
+    }
+    if (hall)
+    {
         for (int32_t c = 0; c < m->n_owned_cells; ++c)
         {
             if (s->alpha[c] == 0.0) continue;
@@ -1203,18 +1217,45 @@ void or_ind_apply_F(OrInduction *s, const double *phi, double *out)
     for (int32_t e = 0; e < ne; ++e) out[e] = s->m_edge[e] * s->part[3 * (int64_t)e] + s->part[3 * (int64_t)e + 1] + s->part[3 * (int64_t)e + 2];
 }
 
-void or_ind_apply_A(OrInduction *s, const double *x, double dt, double *y)
+void or_ind_apply_F(OrInduction *s, const double *phi, double *out) { apply_F_parts(s, phi, out, s->resistive, s->hall); }
+
+void or_ind_ideal_linear(OrInduction *s, const double *phi, double *out) { apply_F_parts(s, phi, out, 0, 0); }
+
+void or_ind_set_ideal(OrInduction *s, const double *u_cell, const int8_t *mask, double cuct)
+{
+    const OrMesh *m = s->m;
+    s->ideal = u_cell != NULL;
+    if (!s->ideal) return;
+    if (!s->u_ideal)
+    {
+        s->u_ideal = (double *)calloc(3 * (size_t)m->n_cells + 1, sizeof(double));
+        s->ide = (double *)calloc((size_t)m->n_edges + 1, sizeof(double));
+        s->imask = (int8_t *)calloc((size_t)m->n_edges + 1, 1);
+    }
+    memcpy(s->u_ideal, u_cell, 3 * (size_t)m->n_cells * sizeof(double));
+    memcpy(s->imask, mask, (size_t)m->n_edges);
+    s->cuct = cuct;
+}
+
+/* apply_A (:185-198): y = x + dt F(d1 x), or with the per-edge step dte y = x + F(d1 diag(dte) x) */
+static void apply_A_dte(OrInduction *s, const double *x, double dt, const double *dte, double *y)
 {
     const OrMesh *m = s->m;
     for (int32_t f = 0; f < m->n_faces; ++f)
     {
         double v = 0;
-        for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) v += m->f2e_sgn[k] * x[m->f2e_idx[k]];
+        if (dte)
+            for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) v += m->f2e_sgn[k] * dte[m->f2e_idx[k]] * x[m->f2e_idx[k]];
+        else
+            for (int64_t k = m->f2e_ptr[f]; k < m->f2e_ptr[f + 1]; ++k) v += m->f2e_sgn[k] * x[m->f2e_idx[k]];
         s->phi[f] = v;
     }
     or_ind_apply_F(s, s->phi, s->tmp);
-    for (int32_t e = 0; e < m->n_edges; ++e) y[e] = x[e] + dt * s->tmp[e];
+    if (dte) for (int32_t e = 0; e < m->n_edges; ++e) y[e] = x[e] + s->tmp[e];
+    else for (int32_t e = 0; e < m->n_edges; ++e) y[e] = x[e] + dt * s->tmp[e];
 }
+
+void or_ind_apply_A(OrInduction *s, const double *x, double dt, double *y) { apply_A_dte(s, x, dt, NULL, y); }
 
 static double dot_owned(const OrMesh *m, const double *a, const double *b)
 {
@@ -1223,7 +1264,8 @@ static double dot_owned(const OrMesh *m, const double *a, const double *b)
     return s;
 }
 
-int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, const int8_t *dir, double dt, int32_t warm, double *E, double *rel_res)
+static int32_t solve_impl(OrInduction *s, const double *Phi, const double *Eexp, const int8_t *dir, double dt, const double *dte, int32_t warm,
+                          double *E, double *rel_res)
 {
     const OrMesh *m = s->m;
     const int32_t ne = m->n_edges, mr = s->p.restart < 2 ? 2 : s->p.restart;
@@ -1243,10 +1285,11 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
             if (!dir[e]) x0[e] += s->corr[e];
     or_ind_apply_F(s, Phi, Fn);
     for (int32_t e = 0; e < ne; ++e) b[e] = Eexp[e] + Fn[e];
-    or_ind_apply_A(s, x0, dt, Ax);
+    apply_A_dte(s, x0, dt, dte, Ax);
     for (int32_t e = 0; e < ne; ++e) r[e] = dir[e] ? 0.0 : b[e] - Ax[e];
-    for (int32_t e = 0; e < ne; ++e) idg[e] = 1.0 / (1.0 + dt * s->m_edge[e] * s->d2[e]);
-    const int ilu = s->ilu && s->pc_ptr; /* (:317-318) */
+    for (int32_t e = 0; e < ne; ++e) idg[e] = 1.0 / (1.0 + (dte ? dte[e] : dt) * s->m_edge[e] * s->d2[e]);
+    /* ILU(0) for a scalar dt (:317-318), built only without the ideal part (:102) */
+    const int ilu = s->ilu && s->pc_ptr && !dte && !s->ideal;
     if (ilu) ilu_factor(s, dt, dir);
     const double bnorm = sqrt(dmax(dot_owned(m, b, b), 1e-300));
     double beta = sqrt(dot_owned(m, r, r));
@@ -1262,7 +1305,7 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
             const double *Vj = V + (size_t)j * (size_t)ne;
             if (ilu) ilu_apply(s, Vj, z, dir);
             else for (int32_t e = 0; e < ne; ++e) z[e] = dir[e] ? 0.0 : Vj[e] * idg[e];
-            or_ind_apply_A(s, z, dt, w);
+            apply_A_dte(s, z, dt, dte, w);
             for (int32_t e = 0; e < ne; ++e)
                 if (dir[e]) w[e] = 0.0;
             for (int i = 0; i <= j; ++i)
@@ -1312,7 +1355,7 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
         else
             for (int32_t e = 0; e < ne; ++e) delta[e] += dir[e] ? 0.0 : comb[e] * idg[e];
         for (int32_t e = 0; e < ne; ++e) z[e] = x0[e] + delta[e];
-        or_ind_apply_A(s, z, dt, Ax);
+        apply_A_dte(s, z, dt, dte, Ax);
         for (int32_t e = 0; e < ne; ++e) r[e] = dir[e] ? 0.0 : b[e] - Ax[e];
         beta = sqrt(dot_owned(m, r, r));
     }
@@ -1324,4 +1367,15 @@ int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, cons
     free(x0); free(b); free(r); free(Ax); free(Fn); free(idg); free(delta); free(w); free(z); free(comb); free(V); free(H);
     free(cs); free(sn); free(g); free(yv);
     return total;
+}
+
+int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *Eexp, const int8_t *dir, double dt, int32_t warm, double *E, double *rel_res)
+{
+    return solve_impl(s, Phi, Eexp, dir, dt, NULL, warm, E, rel_res);
+}
+
+int32_t or_ind_solve_dte(OrInduction *s, const double *Phi, const double *Eexp, const int8_t *dir, const double *dte, int32_t warm, double *E,
+                         double *rel_res)
+{
+    return solve_impl(s, Phi, Eexp, dir, 0.0, dte, warm, E, rel_res);
 }

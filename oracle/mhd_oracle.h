@@ -92,6 +92,13 @@ void or_ind_apply_F(OrInduction *s, const double *phi, double *out);
 void or_ind_apply_A(OrInduction *s, const double *x, double dt, double *y);
 int32_t or_ind_solve(OrInduction *s, const double *Phi, const double *E_expl, const int8_t *dir, double dt, int32_t warm, double *E,
                      double *rel_res);
+/* solve with the per-edge pseudo-time step dte (:299-390 with dte_): A x = x + F(d1 diag(dte) x), Jacobi
+ * 1 / (1 + dte m d2), no ILU(0) */
+int32_t or_ind_solve_dte(OrInduction *s, const double *Phi, const double *E_expl, const int8_t *dir, const double *dte, int32_t warm,
+                         double *E, double *rel_res);
+/* the implicit ideal part (Config::implicit_ideal, set_ideal_state :112-116; u NULL: off) and ideal_linear (:118-124) */
+void or_ind_set_ideal(OrInduction *s, const double *u_cell, const int8_t *mask, double cuct);
+void or_ind_ideal_linear(OrInduction *s, const double *phi, double *out);
 /* one semi-implicit step, mercury::Solver::step_first_order (MercuryUns/driver/Solver.cpp:228-277): forward Euler of
  * the fluid (with the opening and closing half-step gyration when lorentz is on), the EMF from ind's solve (frozen
  * total field and n_e,eff of the step, inflow edges Dirichlet, the rhs's EMF as E_expl, warm start) and CT with it;

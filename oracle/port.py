@@ -102,6 +102,9 @@ def lib():
             ("or_ind_apply_A", [vp, vp, dbl, vp], None),
             ("or_ind_solve", [vp, vp, vp, vp, dbl, i32, vp, vp], i32),
             ("or_ind_set_ilu", [vp, i32, dbl], None),
+            ("or_ind_solve_dte", [vp, vp, vp, vp, vp, i32, vp, vp], i32),
+            ("or_ind_set_ideal", [vp, vp, vp, dbl], None),
+            ("or_ind_ideal_linear", [vp, vp, vp], None),
             ("or_ind_ilu_pattern", [vp, vp, vp, vp], i64),
             ("or_ind_ilu_precond", [vp, dbl, vp, vp, vp], None),
         ]:
@@ -303,6 +306,28 @@ class PortInduction:
     def apply_A(self, x, dt):
         o = np.zeros(self.pm.n_edges)
         lib().or_ind_apply_A(self._h, _p(_f(x)), dt, _p(o))
+        return o
+
+    def solve_dt_edge(self, Phi, E_expl, dirichlet, dt_edge, warm=True):
+        """solve with the per-edge pseudo-time step dt_edge -> (E, iterations, rel_res)."""
+        E = np.zeros(self.pm.n_edges)
+        rr = ctypes.c_double()
+        d = np.ascontiguousarray(dirichlet, np.int8)
+        it = lib().or_ind_solve_dte(self._h, _p(_f(Phi)), _p(_f(E_expl)), _p(d), _p(_f(dt_edge)), int(warm), _p(E), ctypes.byref(rr))
+        return E, int(it), rr.value
+
+    def set_ideal_state(self, u_cell, mask, cuct=0.5):
+        """Config::implicit_ideal with set_ideal_state: u 3 per cell, mask 1 per edge (None: the part off)."""
+        if u_cell is None:
+            lib().or_ind_set_ideal(self._h, None, None, float(cuct))
+            return
+        self._u = _f(u_cell)
+        self._mask = np.ascontiguousarray(mask, np.int8)
+        lib().or_ind_set_ideal(self._h, _p(self._u), _p(self._mask), float(cuct))
+
+    def ideal_linear(self, phi):
+        o = np.zeros(self.pm.n_edges)
+        lib().or_ind_ideal_linear(self._h, _p(_f(phi)), _p(o))
         return o
 
     def set_ilu(self, enable=True, shift=0.3):

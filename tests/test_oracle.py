@@ -335,3 +335,53 @@ def test_semi_implicit_step():
         for a, b in zip(Uo, Ur):
             same(a, b)
         same(Po, Pr)
+
+
+@pytest.mark.parametrize("case", ["box", "shell"])
+def test_induction_steady_mode_forms(case):
+    """The implicit ideal part of F (Config::implicit_ideal: set_ideal_state, ideal_linear, apply_F, apply_A)
+    and the per-edge pseudo-time step of solve (dt_edge), alone and together, bit for bit against the
+    reference: operator outputs, iterations, residuals and E."""
+    if case == "box":
+        h = HostMesh.box(6, 5, 4, tets=True, jitter=0.1, seed=8).compute_geometry().boundary(*MIXED_BOX_BC)
+        r = ref_twin(h, BOX_TAGS).boundary(*MIXED_BOX_BC)
+        taper = dict(hall_r_min=-100.0, hall_r_max=-99.0)
+    else:
+        h = HostMesh.shell(4, 4, 0.8, 5.0, 1.2, n_solid=1, tets=True).compute_geometry().boundary(*SHELL_BC)
+        r = ref_twin(h, SHELL_TAGS).boundary(*SHELL_BC)
+        taper = dict(hall_r_min=1.0, hall_r_max=1.6)
+    o = port.PortMesh(h)
+    rng = np.random.default_rng(17)
+    m_edge = rng.uniform(0.5, 2.0, h.n_edges) / np.asarray(h["star1"])
+    kw = dict(hall=True, hall_coef=0.5, rtol=1e-10, max_it=300, restart=15, **taper)
+    B0 = rng.uniform(-1, 1, 3 * h.n_cells)
+    ne = rng.uniform(0.5, 2.0, h.n_cells)
+    u = rng.uniform(-1, 1, 3 * h.n_cells)
+    mask = (np.asarray(h["edge_mode"]) == 0).astype(np.int8)
+    dirichlet = (np.asarray(h["edge_mode"]) == 2).astype(np.int8)
+    phi = rng.uniform(-1, 1, h.n_faces)
+    x = rng.uniform(-1, 1, h.n_edges)
+    Ee = rng.uniform(-1, 1, h.n_edges)
+    dte = rng.uniform(0.005, 0.05, h.n_edges)
+    for ideal in (False, True):
+        ri = ref.RefInduction(r, implicit_ideal=ideal, cuct=0.5, **kw)
+        ri.set_m(m_edge)
+        oi = port.PortInduction(o, m_edge, **kw)
+        ri.set_frozen_state(B0, ne)
+        oi.set_frozen_state(B0, ne)
+        if ideal:
+            ri.set_ideal_state(u, mask)
+            oi.set_ideal_state(u, mask, 0.5)
+            same(oi.ideal_linear(phi), ri.ideal_linear(phi))
+        same(oi.apply_F(phi), ri.apply_F(phi))
+        same(oi.apply_A(x, 0.05), ri.apply_A(x, 0.05))
+        for warm in (False, True):
+            Eo, ito, rro = oi.solve_dt_edge(phi, Ee, dirichlet, dte, warm)
+            Er, itr, rrr = ri.solve_dt_edge(phi, Ee, dirichlet, dte, warm)
+            assert ito == itr and rro == rrr and rrr <= 1e-10
+            same(Eo, Er)
+        if ideal:
+            Eo, ito, rro = oi.solve(phi, Ee, dirichlet, 0.02, False)
+            Er, itr, rrr = ri.solve(phi, Ee, dirichlet, 0.02, False)
+            assert ito == itr and rro == rrr and rrr <= 1e-10
+            same(Eo, Er)
