@@ -22,6 +22,9 @@ on, dt = 20 x the explicit whistler limit, GMRES(30) with Jacobi to rtol 1e-8, c
 reference's own solve on a bounded sample beside it; its "ilu" object is the same FP64 solve with the
 block ILU(0) preconditioner against Jacobi, both capped at --gmres-ilu-max-it iterations.
 
+The "config1" object (left out with --no-config1): config 1 itself, the 24,576-cell box of one ion, 20 steps at
+CFL 0.4 in FP64 and mixed precision (device ms per step, div B).
+
 The "semi_implicit" object (left out with --no-semi-implicit): the reference's default run mode, the
 semi-implicit step of Solver::step_first_order (forward Euler fluid, EMF from the Hall + resistive solve),
 on the same shell in FP64: wall milliseconds per synchronous step and the solve's iterations.
@@ -551,6 +554,43 @@ def bench_adjoint(args):
     return out
 
 
+def bench_config1(args):
+    """Config 1 itself, the reference's CPU-runnable case: the unit cube of 16^3 hexahedra x 6 tetrahedra (24,576
+    cells, interior nodes jittered, seed 0), one ion, 20 steps at CFL 0.4 with the device CFL step, outflow
+    everywhere; FP64 (reference-exact) and mixed precision, device time of the 20 steps after one warm-up step
+    from the same initial state, and div B after them.  A precision that fails is reported, not raised."""
+    import torch
+    from mpcns_uns_b200 import gpu, workloads
+    wl = workloads.box(16)
+    h = wl.mesh
+    dm = gpu.DeviceMesh(h)
+    out = {"workload": wl.name, "cells": h.n_cells, "steps": wl.steps, "cfl": wl.cfl, "n_species": wl.n_species}
+    for prec in ("fp64", "mixed"):
+        try:
+            p = gpu.step_params(wl.n_species, wl.gamma, fs=wl.fs, mass=wl.mass, u_inf=wl.u_inf, B_imf=wl.B_imf, cfl=wl.cfl,
+                                precision=prec)
+            st = gpu.ResidentState(dm, p)
+            st.set(wl.U, wl.Phi, wl.PhiAdd)
+            st.step(0.0)
+            st.set(wl.U, wl.Phi, wl.PhiAdd)
+            torch.cuda.synchronize()
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(dm.stream)
+            for _ in range(wl.steps):
+                st.step(0.0, sync=False)
+            ev1.record(dm.stream)
+            ev1.synchronize()
+            ms = ev0.elapsed_time(ev1) / wl.steps
+            out[prec] = {"ms_per_step": ms, "cell_updates_per_s": h.n_cells * wl.n_species * 2 / (ms / 1e3),
+                         "div_b_max_rel": dm.div_b(st.Phi())["max_rel"]}
+            del st
+        except Exception as e:  # reported, not required
+            out[prec] = {"error": str(e)[:200]}
+    log(f"[bench] config 1 ({h.n_cells} cells, {wl.steps} steps): " +
+        ", ".join(f"{k} {out[k].get('ms_per_step', float('nan')):.3f} ms/step" for k in ("fp64", "mixed")))
+    return out
+
+
 def bench_semi_implicit(args, wl, dm, new_state):
     """The reference's default run mode (Config::time_order = 1, Solver::step_first_order) on the step's shell:
     forward Euler of both ions with the J x B force and the Strang-split gyration, the EMF from the Hall +
@@ -708,6 +748,9 @@ def summary(out):
             sm["gmres"]["ilu"] = {"it": il["max_it"], "s": [_r(il["ilu"]["s_per_solve"]), _r(il["jacobi"]["s_per_solve"])],
                                   "rel_res": [_r(il["ilu"]["rel_res"], 3), _r(il["jacobi"]["rel_res"], 3)],
                                   "factor_apply_ms": [_r(il["factor_ms"]), _r(il["apply_ms"])]}
+    c1 = out.get("config1")
+    if c1:
+        sm["config1"] = {k: _r(c1[k].get("ms_per_step"), 3) for k in ("fp64", "mixed") if k in c1}
     si = out.get("semi_implicit")
     if si:
         sm["semi_implicit"] = {"ms": _r(si["ms_per_step"]), "it": si["iterations"], "rel_res": _r(max(si["rel_res"]), 3)}
@@ -759,6 +802,7 @@ def main():
     ap.add_argument("--gmres-solves", type=int, default=2)
     ap.add_argument("--gmres-ilu-max-it", type=int, default=60, help="block ILU(0) leg against Jacobi (0: skip)")
     ap.add_argument("--no-semi-implicit", action="store_true", help="leave out the time_order = 1 step")
+    ap.add_argument("--no-config1", action="store_true", help="leave out the 24,576-cell box (config 1)")
     ap.add_argument("--si-steps", type=int, default=3)
     ap.add_argument("--si-max-it", type=int, default=100)
     ap.add_argument("--si-whistler-ratio", type=float, default=2.0)
@@ -961,7 +1005,13 @@ def main():
     # the configuration sections run once, on a single-GPU run (under torchrun the replicas time the step only)
     if world > 1:
         args.no_gmres = args.no_adjoint = True
-        args.no_ten_ion = args.no_semi_implicit = True
+        args.no_ten_ion = args.no_semi_implicit = args.no_config1 = True
+    c1 = None
+    if rank == 0 and not args.no_config1 and args.config != "box":
+        try:
+            c1 = bench_config1(args)
+        except Exception as e:  # reported, not required
+            log(f"[bench] config 1 failed: {e}")
     si = None
     if rank == 0 and not args.no_semi_implicit and wl.n_species == 2:
         try:
@@ -1017,7 +1067,7 @@ def main():
                         "roofline": {"kernel": r64["kernel"], "achieved": r64["achieved"], "frac": r64["achieved"] / peak}},
                "accuracy_mixed_vs_fp64": acc,
                "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": io_bytes, "d2h_bytes_per_step": io_bytes},
-               "cpu_baseline": cpu, "clocks": clocks, "gmres": gm, "semi_implicit": si, "adjoint": adj, "ten_ion": ten}
+               "cpu_baseline": cpu, "clocks": clocks, "config1": c1, "gmres": gm, "semi_implicit": si, "adjoint": adj, "ten_ion": ten}
         out["summary"] = summary(out)
         print(json.dumps(out))
     if dist:
