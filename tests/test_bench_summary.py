@@ -19,6 +19,7 @@ def _line():
                   "ilu": {"max_it": 60, "ilu": {"s_per_solve": 0.73, "rel_res": 5.4e-4},
                           "jacobi": {"s_per_solve": 0.11, "rel_res": 8.4e-4}, "factor_ms": 62.3, "apply_ms": 9.1}},
         "semi_implicit": {"ms_per_step": 38.4, "iterations": [5, 5, 5], "rel_res": [4.1e-9, 3.9e-9, 4.0e-9]},
+        "config1": {"fp64": {"ms_per_step": 0.35}, "mixed": {"error": "reported, not raised"}},
         "adjoint": {"forward_s": 0.2, "forward_plus_backward_over_forward": 3.79, "dot_test_rel_err_max": 2.7e-15,
                     "fd": {"h=1e-06": fd, "h=1e-07": fd}},
         "ten_ion": {"mixed": {"ms_per_step": 105.5}, "fp64": {"ms_per_step": 325.5},
@@ -28,8 +29,9 @@ def _line():
 
 def test_summary_of_every_leg():
     sm = bench.summary(_line())
-    for key in ("acc", "gmres", "semi_implicit", "adjoint", "ten_ion"):
+    for key in ("acc", "gmres", "semi_implicit", "adjoint", "ten_ion", "config1"):
         assert key in sm, key
+    assert sm["config1"] == {"fp64": 0.35, "mixed": None}
     assert sm["gmres"]["ilu"]["factor_apply_ms"] == [62.3, 9.1]
     assert sm["semi_implicit"] == {"ms": 38.4, "it": [5, 5, 5], "rel_res": 4.1e-9}
     assert len(json.dumps({"summary": sm})) < 1400
@@ -37,7 +39,7 @@ def test_summary_of_every_leg():
 
 def test_summary_without_the_optional_legs():
     out = _line()
-    for key in ("accuracy_mixed_vs_fp64", "gmres", "semi_implicit", "adjoint", "ten_ion"):
+    for key in ("accuracy_mixed_vs_fp64", "gmres", "semi_implicit", "adjoint", "ten_ion", "config1"):
         out.pop(key)
     sm = bench.summary(out)
     assert set(sm) == {"mixed_ms", "fp64_ms", "speedup_mixed", "e2e", "roofline_frac", "roofline_kernel", "clocks_mhz"}
